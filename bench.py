@@ -1,0 +1,355 @@
+"""Benchmark of the DFSPH time step on B200 (one JSON line on rank 0).
+
+Workload (default): the 250,047-particle dam break (63^3 lattice, r = 0.0125 m, 4 x 2 x 2 m box,
+64,002 wall particles, CFL 0.4 with dt_max 5 ms, density tolerance 0.01 %, divergence 0.1 %),
+synthetic seeded input. A step is one DFSPHCUDA::step() equivalent: neighbour search, divergence
+solve, XSPH + gravity, CFL dt, pressure solve, position update.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 1..5]
+
+With N > 1 (torchrun) every rank runs an independent replica of the workload (the step does not
+shard across GPUs here) and the reported ms/step is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DFSPH ms/step & solver iters at rho-err<=0.01%, learned vs plain, 1 B200"
+UNIT = "ms/step"
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_scene(config: int):
+    from splishsplash_for_cuda_b200.scene import synthetic_scene
+
+    return synthetic_scene(config, cfl=True)
+
+
+# Algorithmic bytes per launch of each kernel (FP32 layout: float4 pos+mass, float4 vel, 4-byte
+# scalars, 4-byte neighbour indices, one packed 4-byte count word). Each particle's own data is
+# counted once per launch, neighbour data is other particles' own data (perfect reuse), and every
+# stored neighbour costs its 4-byte index. nf / nb are the mean fluid / boundary neighbour counts.
+def kernel_bytes(name: str, n: int, nb_particles: int, nf: float, nb: float) -> float:
+    nn = nf + nb
+    per = {
+        "density_alpha": 16 + 16 + 4 + 4 + 4 + 4 + 4 + 4 + 4 * nn,      # pos, vel, counts, kv r/w, rho, alpha, dadv
+        "divergence_jacobi": 16 + 4 + 4 + 4 + 4 + 16 + 16 + 4 * nn,     # pos, k, counts, kv r/w, vel r/w
+        "divergence_residual": 16 + 16 + 4 + 4 + 4 + 4 + 4 * nn,        # pos, vel, counts, alpha, dadv, k
+        "viscosity": 16 + 16 + 4 + 4 + 16 + 4 * nf,                      # pos, vel, counts, rho, acc
+        "pressure_warm_jacobi": 16 + 4 + 4 + 16 + 16 + 4 * nn,           # pos, kappa, counts, vel r/w
+        "pressure_residual": 16 + 16 + 4 + 4 + 4 + 4 + 4 + 4 + 4 * nn,   # pos, vel, counts, rho, alpha, kappa r/w, dadv, k
+        "pressure_jacobi": 16 + 4 + 4 + 16 + 16 + 4 * nn,                # pos, k, counts, vel r/w
+        "neighbor_build": 16 + 4 + 4 * nn,                               # pos, counts, lists written
+        "update_pos": 16 + 16 + 16,                                      # pos r/w, vel
+    }[name]
+    extra = 16 * nb_particles if name not in ("viscosity", "update_pos") else 0  # boundary pos+psi once
+    return per * n + extra
+
+
+def setup_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def reduce_max(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_reference_run(scene, steps: int, warmup: int, time_budget: float | None):
+    """Times the CPU reference of the step: the reference TimeStepDFSPH harness when it was built
+    (oracle/_ref/dfsph_ref), else the oracle's restatement of the GPU formulation. Returns
+    (ms_per_step, steps_timed, threads, kind)."""
+    ref_bin = ROOT / "oracle" / "_ref" / "dfsph_ref"
+    threads = os.cpu_count() or 1
+    if ref_bin.exists():
+        from oracle.ref_runner import run_reference
+
+        ms, done = run_reference(ref_bin, scene, steps, warmup, time_budget, threads)
+        return ms, done, threads, "reference"
+    from oracle import Oracle
+
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    o = Oracle(scene, 64)
+    for _ in range(warmup):
+        o.step()
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps:
+        o.step()
+        done += 1
+        if time_budget is not None and time.perf_counter() - t0 > time_budget and done >= 2:
+            break
+    ms = (time.perf_counter() - t0) * 1e3 / done
+    return ms, done, threads, "port"
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    scene = make_scene(args.config)
+    ms, done, threads, kind = cpu_reference_run(scene, args.steps, args.warmup, time_budget=args.ref_budget)
+    line = {
+        "metric": METRIC, "value": round(ms, 3), "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": done, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": scene.name, "fluid_particles": scene.n_fluid, "boundary_particles": scene.n_boundary,
+                   "parallelism": "cpu"},
+        "cpu_baseline": {"value": round(ms, 3), "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{done} steps after {args.warmup} warm-up steps of {scene.name}"},
+        "e2e": {"value": round(ms, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
+
+    scene = make_scene(args.config)
+    n = scene.n_fluid
+    d = DFSPHCUDA(scene, device=local, use_graphs=not args.host_loops)
+    d.set_param("timing", 0)
+    stream = torch.cuda.ExternalStream(d.stream_handle(), device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    for _ in range(args.warmup):
+        d.step()
+    d.synchronize()
+
+    def timed_steps(k, e2e=False, host=None):
+        tot = 0.0
+        iters, iters_v = [], []
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+        for s in range(k):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(s))  # 1 GiB... 256 MiB write: evicts L2 between timed steps
+                starts[s].record(stream)
+            if e2e:
+                d.update_fluid(host["x"], host["v"])
+            st = d.step()
+            if e2e:
+                host["x"][:] = d.positions()
+                host["v"][:] = d.velocities()
+            with torch.cuda.stream(stream):
+                ends[s].record(stream)
+            iters.append(st.iterations)
+            iters_v.append(st.iterations_v)
+        torch.cuda.synchronize(local)
+        for s in range(k):
+            tot += starts[s].elapsed_time(ends[s])
+        return tot, iters, iters_v
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize(local)
+    l0 = d.launch_count()
+    with ClockSampler(local) as clk:
+        total_ms, iters, iters_v = timed_steps(args.steps)
+    launches = d.launch_count() - l0
+    if world > 1:
+        dist.barrier()
+    ms = reduce_max(total_ms / args.steps, world)
+    agg_pps = reduce_sum(n * args.steps / (total_ms / 1e3), world)
+
+    # end-to-end through the public API with host buffers (pinned), copies inside the timed region
+    xh = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    vh = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    xh[:] = d.positions()
+    vh[:] = d.velocities()
+    e2e_total, _, _ = timed_steps(args.steps, e2e=True, host={"x": xh, "v": vh})
+    e2e_ms = reduce_max(e2e_total / args.steps, world)
+
+    # per-kernel device time with a cold L2 before each launch, for the roofline
+    counts = d.field("neighbor_counts")
+    nf, nbn = float(counts[:, 0].mean()), float(counts[:, 1].mean())
+    kt = {}
+    for name in ["pressure_jacobi", "pressure_residual", "divergence_jacobi", "divergence_residual",
+                 "density_alpha", "viscosity", "pressure_warm_jacobi", "neighbor_build", "update_pos"]:
+        vals = []
+        for _ in range(args.kernel_reps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            vals.append(d.time_kernel(name, 1))
+        kt[name] = float(np.median(vals))
+    mean_it, mean_itv = float(np.mean(iters)), float(np.mean(iters_v))
+    per_step_launches = {"pressure_jacobi": mean_it, "pressure_residual": mean_it + 1,
+                         "divergence_jacobi": mean_itv + 1, "divergence_residual": mean_itv + 1,
+                         "density_alpha": 1, "viscosity": 1, "pressure_warm_jacobi": 1, "neighbor_build": 1,
+                         "update_pos": 1}
+    share = {k: kt[k] * per_step_launches[k] for k in kt}
+    dom = max(share, key=share.get)
+    peak, peak_kind = _peaks()
+    alg = kernel_bytes(dom, n, scene.n_boundary, nf, nbn)
+    achieved = alg / (kt[dom] * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "ncu_traffic.json"
+    if tf.exists():
+        tj = json.loads(tf.read_text())
+        rec = tj.get("kernels", {}).get(dom)
+        if rec and rec.get("n_particles"):
+            traffic = rec["dram_bytes_per_launch"] * n / rec["n_particles"]
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ms_cpu, done, threads, kind = cpu_reference_run(scene, 10 ** 6, 1, time_budget=args.cpu_budget)
+        cpu = {"value": round(ms_cpu, 2), "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"{done} steps (after 1 warm-up) of {scene.name}, {args.cpu_budget:.0f} s budget"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(ms, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice + xoshiro256** jitter)",
+            "config": {"workload": scene.name, "fluid_particles": n, "boundary_particles": scene.n_boundary,
+                       "radius": scene.config.particleRadius, "cfl": "0.4, dt_max 5 ms",
+                       "max_error_pct": scene.config.maxError, "max_error_v_pct": scene.config.maxErrorV,
+                       "warm_start": "plain", "l2": "256 MiB write before every timed step",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "iterations_per_step": round(mean_it, 2), "iterations_v_per_step": round(mean_itv, 2),
+            "particle_steps_per_s": round(agg_pps, 1),
+            "e2e": {"value": round(e2e_ms, 4), "unit": UNIT, "h2d_bytes_per_step": n * 24, "d2h_bytes_per_step": n * 24},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": None if traffic is None else round(traffic),
+                         "algorithmic_bytes": round(alg), "ms_per_launch": round(kt[dom], 5)},
+            "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
+            "mean_neighbors": {"fluid": round(nf, 2), "boundary": round(nbn, 2)},
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    d.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--host-loops", action="store_true", help="solver loops driven from the host")
+    ap.add_argument("--kernel-reps", type=int, default=5)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-budget", type=float, default=120.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = setup_dist()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

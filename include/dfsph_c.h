@@ -1,0 +1,231 @@
+/*
+ * dfsph_c.h — C ABI of the B200-native DFSPH time step.
+ *
+ * One context (dfsph_ctx) holds the whole device state of one fluid set and one boundary set, the
+ * way SPH::DFSPHCData does in the reference (SPlisHSPlasH/DFSPH/DFSPH_c_arrays_structure.h:297-496),
+ * and exposes the seven host functions that SPH::DFSPHCUDA::step() calls
+ * (SPlisHSPlasH/DFSPH/DFSPH_CUDA.cpp:82-794, declared in SPlisHSPlasH/DFSPH/DFSPH_core_cuda.h:27-74),
+ * plus a fused dfsph_step() that runs them in the reference order on the context's own stream.
+ *
+ * Conventions
+ *  - Every entry point returns an int status: DFSPH_OK (0) or a negative DFSPH_E_* code. The
+ *    reference has no error channel (gpuAssert -> exit(), DFSPH_macro_cuda.h:22-29); this ABI never
+ *    exits and never traps. dfsph_last_error() gives a message for the last failing call.
+ *  - Host arrays are plain C arrays owned by the caller; every copy is explicit. Positions and
+ *    velocities are packed xyz triples (3 floats per particle).
+ *  - Particle order: the solver re-sorts particles every step (cell-sorted order). Unlike the
+ *    reference, each particle keeps a stable id (its index at upload); downloads are returned in
+ *    id order unless DFSPH_ORDER_SORTED is asked for.
+ *  - A context is used by one host thread at a time; several contexts may coexist.
+ */
+#ifndef DFSPH_C_H
+#define DFSPH_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DFSPH_ABI_VERSION 1
+
+/* Opaque solver context (one fluid set + one boundary set on one device). */
+typedef struct dfsph_ctx dfsph_ctx;
+
+/* ---- status codes ---------------------------------------------------------------------------- */
+#define DFSPH_OK 0
+#define DFSPH_E_INVALID (-1)  /* bad argument (null pointer, size out of range, unknown key)      */
+#define DFSPH_E_CUDA (-2)     /* a CUDA runtime call failed; see dfsph_last_error()               */
+#define DFSPH_E_STATE (-3)    /* call out of order (e.g. step before any fluid was uploaded)      */
+#define DFSPH_E_NOMEM (-4)    /* device allocation failed                                         */
+#define DFSPH_E_DEVICE (-5)   /* the device status word reports a fault of the data (see below)   */
+
+/* ---- device status word bits (dfsph_status) ---------------------------------------------------- */
+#define DFSPH_ST_NEIGHBOR_OVERFLOW 0x1u  /* a particle had more neighbours than neighbor_capacity   */
+#define DFSPH_ST_NONFINITE 0x2u          /* a fluid position was NaN/Inf                            */
+#define DFSPH_ST_ESCAPED 0x4u            /* a fluid particle left the cell grid                     */
+#define DFSPH_ST_PRESSURE_NOT_CONVERGED 0x8u    /* pressure solve stopped at max_iterations         */
+#define DFSPH_ST_DIVERGENCE_NOT_CONVERGED 0x10u /* divergence solve stopped at max_iterations_v     */
+#define DFSPH_ST_SORT_TIMEOUT 0x20u      /* a bounded wait in the radix sort gave up (no hang)      */
+#define DFSPH_ST_BOUNDARY_OVERFLOW 0x40u /* a boundary particle had too many boundary neighbours    */
+
+/* ---- scene / solver parameters ---------------------------------------------------------------- */
+/* Mirrors the "Configuration" keys of the reference JSON scene (Utilities/SceneLoader.cpp:39-160)
+ * and the solver members of SPH::TimeStep (SPlisHSPlasH/TimeStep.h:26-34). */
+typedef struct dfsph_scene {
+    double particle_radius;       /* r; kernel support radius = 4 r (FluidModel::setParticleRadius) */
+    double density0;              /* rest density rho0                                                */
+    double viscosity;             /* XSPH coefficient (Viscosity_XSPH)                                */
+    double gravitation[3];        /* m/s^2                                                            */
+    double time_step;             /* initial dt (TimeManager::getTimeStepSize)                        */
+    int32_t max_iterations;       /* pressure solve cap (m_maxIterations)                             */
+    double max_error;             /* pressure tolerance, percent of rho0 (m_maxError)                 */
+    int32_t max_iterations_v;     /* divergence solve cap (m_maxIterationsV)                          */
+    double max_error_v;           /* divergence tolerance, percent (m_maxErrorV)                      */
+    int32_t enable_divergence_solver; /* m_enableDivergenceSolver                                    */
+    int32_t cfl_method;           /* 0: fixed dt; 1: CFL (TimeStep::updateTimeStepSizeCFL semantics) */
+    double cfl_factor;            /* m_cflFactor                                                      */
+    double cfl_max_time_step;     /* m_cflMaxTimeStepSize                                             */
+    double cfl_min_time_step;     /* lower clamp of the CFL dt (reference passes 0.0001)              */
+    uint32_t fluid_capacity;      /* max fluid particles held by the context                          */
+    uint32_t boundary_capacity;   /* max boundary particles                                           */
+    uint32_t neighbor_capacity;   /* stored neighbours per fluid particle (fluid + boundary)          */
+    int32_t precision;            /* 32: FP32 kernels (product); 64: FP64 build of the same kernels   */
+    int32_t device;               /* CUDA device ordinal                                              */
+    int32_t use_graphs;           /* 1: solver loops run as CUDA-graph while-loops (no host sync)     */
+    double grid_min[3];           /* optional domain box for the cell grid; used when grid_min <      */
+    double grid_max[3];           /*   grid_max on every axis, otherwise the boundary bounding box    */
+} dfsph_scene;
+
+/* ---- per-step statistics ---------------------------------------------------------------------- */
+typedef struct dfsph_step_stats {
+    int32_t iterations;           /* pressure iterations (TimeStep::getIterationCount)               */
+    int32_t iterations_v;         /* divergence iterations (TimeStep::getIterationCountV)            */
+    double density_error;         /* final mean (rho_adv - rho0)^+ of the pressure solve [kg/m^3]    */
+    double divergence_error;      /* final mean clamped divergence of the divergence solve           */
+    double h;                     /* dt used by this step                                            */
+    double h_future;              /* dt chosen for the next step                                     */
+    uint32_t status;              /* DFSPH_ST_* bits raised during the step                          */
+    uint32_t num_fluid;           /* fluid particles                                                 */
+    double ms_total;              /* device time of the step (CUDA events), 0 if timing is off       */
+} dfsph_step_stats;
+
+/* ---- fields for upload / download -------------------------------------------------------------- */
+enum dfsph_field {
+    DFSPH_F_POSITION = 0,   /* 3 per particle */
+    DFSPH_F_VELOCITY = 1,   /* 3 */
+    DFSPH_F_MASS = 2,       /* 1 */
+    DFSPH_F_DENSITY = 3,    /* 1: rho from the density+alpha pass of the last step              */
+    DFSPH_F_FACTOR = 4,     /* 1: alpha (DFSPH factor); after a pressure solve it holds alpha/h_f */
+    DFSPH_F_DENSITY_ADV = 5,/* 1: last clamped residual (rho_adv - rho0)^+ or divergence         */
+    DFSPH_F_KAPPA = 6,      /* 1: pressure warm-start accumulator                                 */
+    DFSPH_F_KAPPA_V = 7,    /* 1: divergence warm-start accumulator                               */
+    DFSPH_F_ACCELERATION = 8, /* 3: non-pressure acceleration (gravity + XSPH)                     */
+    DFSPH_F_ID = 9,         /* 1 (uint32 in a float/double container is not allowed: use dtype 2) */
+    DFSPH_F_BOUNDARY_PSI = 10,      /* 1 per boundary particle: Akinci psi (boundary "mass")      */
+    DFSPH_F_BOUNDARY_POSITION = 11, /* 3 per boundary particle                                     */
+    DFSPH_F_NEIGHBOR_COUNTS = 12    /* 2 per fluid particle: fluid count, boundary count (dtype 2)  */
+};
+#define DFSPH_DTYPE_F32 0
+#define DFSPH_DTYPE_F64 1
+#define DFSPH_DTYPE_U32 2
+#define DFSPH_ORDER_ID 0
+#define DFSPH_ORDER_SORTED 1
+
+/* ---- lifetime ---------------------------------------------------------------------------------- */
+
+/* Fills *scene with the reference defaults (SPH::TimeStep::TimeStep, TimeStep.cpp:23-44; CFL off as
+ * in DFSPH_CUDA.cpp:299) and this library's capacities. */
+int dfsph_scene_defaults(dfsph_scene* scene);
+
+/* Replaces DFSPHCData::DFSPHCData(FluidModel*) (DFSPH_c_arrays_structure.cpp:852-944): allocates
+ * every device buffer for the capacities in *scene and a private CUDA stream. */
+int dfsph_create(const dfsph_scene* scene, dfsph_ctx** out);
+
+/* Replaces DFSPHCData::~DFSPHCData (DFSPH_c_arrays_structure.cpp:946-973). Null is accepted. */
+int dfsph_destroy(dfsph_ctx* ctx);
+
+/* Message of the last failing call on ctx (or of the last failing dfsph_create when ctx is null). */
+const char* dfsph_last_error(const dfsph_ctx* ctx);
+
+/* ---- state upload (DFSPHCData::reset, DFSPH_c_arrays_structure.cpp:975-1048) -------------------- */
+
+/* Static boundary particles (Akinci samples). Replaces boundaries_data->reset + initGridOffset +
+ * the boundary neighbour structure (DFSPH_c_arrays_structure.cpp:1005-1015, 1050-1098). The grid
+ * offset follows initGridOffset: offset = -(floor(min/H) - 5). When psi is null the Akinci psi
+ * (FluidModel::computeBoundaryPsi, FluidModel.cpp:233-258) is computed on the device in FP64;
+ * otherwise the given per-particle psi is used as boundary mass, as the reference uploads it. */
+int dfsph_set_boundary(dfsph_ctx* ctx, const float* xyz, const float* psi, uint32_t n);
+
+/* Moves the boundary: new positions (and velocities, nullable = zero) for the same n particles in
+ * the order of dfsph_set_boundary. psi is kept. The boundary cell structure is rebuilt. */
+int dfsph_move_boundary(dfsph_ctx* ctx, const float* xyz, const float* vxyz);
+
+/* Fluid particles (fluid_data->reset<FluidModel>). vxyz may be null (zero velocity). mass may be
+ * null: every particle then gets the reference default mass 0.8 * rho0 * (2r)^3
+ * (FluidModel::initMasses, FluidModel.cpp:94-107). Resets kappa, kappa_v and the dt history
+ * (h = h_future = h_past = time_step, h_ratio = 1) and assigns ids 0..n-1 in upload order. */
+int dfsph_upload_fluid(dfsph_ctx* ctx, const float* xyz, const float* vxyz, const float* mass, uint32_t n);
+
+/* Overwrites positions and velocities of the current n particles (given in id order) but keeps
+ * their warm-start accumulators and the dt history: the host-in-the-loop way to edit a running
+ * simulation without resetting it. */
+int dfsph_update_fluid(dfsph_ctx* ctx, const float* xyz, const float* vxyz);
+
+/* Copies a field to host memory. n_elems is the capacity of out in elements of dtype; the call
+ * fails with DFSPH_E_INVALID if it is too small. order: DFSPH_ORDER_ID or DFSPH_ORDER_SORTED. */
+int dfsph_download(dfsph_ctx* ctx, int field, int dtype, void* out, size_t n_elems, int order);
+
+/* Neighbour lists of every fluid particle, in id space: counts[2*id] fluid, counts[2*id+1]
+ * boundary; lists[id*cap + k] holds fluid neighbour ids first, then boundary indices (in the order
+ * given to dfsph_set_boundary). cap is the row length of lists and must be >= neighbor_capacity. */
+int dfsph_get_neighbors(dfsph_ctx* ctx, uint32_t* counts, uint32_t* lists, uint32_t cap);
+
+/* ---- one time step ----------------------------------------------------------------------------- */
+
+/* DFSPHCUDA::step() (DFSPH_CUDA.cpp:82-794) without rendering, dynamic bodies, open boundaries or
+ * the dynamic window: neighbour search -> divergence solve -> XSPH + gravity -> dt update ->
+ * velocity update -> pressure solve -> position update -> onSimulationStepEnd. stats may be null. */
+int dfsph_step(dfsph_ctx* ctx, dfsph_step_stats* stats);
+
+/* The seven host functions of DFSPH_core_cuda.h:27-74, for callers that drive the step themselves. */
+int dfsph_neighbors_search(dfsph_ctx* ctx, int sort);                     /* cuda_neighborsSearch */
+int dfsph_divergence_solve(dfsph_ctx* ctx, uint32_t max_iter, double max_error, int32_t* iters);
+int dfsph_external_forces(dfsph_ctx* ctx);                                /* cuda_externalForces  */
+int dfsph_update_time_step(dfsph_ctx* ctx, double h_future);              /* updateTimeStep       */
+int dfsph_cfl(dfsph_ctx* ctx, double min_dt, double cfl_factor, double max_dt); /* cuda_CFL       */
+int dfsph_update_vel(dfsph_ctx* ctx);                                     /* cuda_update_vel      */
+int dfsph_pressure_solve(dfsph_ctx* ctx, uint32_t max_iter, double max_error, int32_t* iters);
+int dfsph_update_pos(dfsph_ctx* ctx);                                     /* cuda_update_pos      */
+int dfsph_on_step_end(dfsph_ctx* ctx);                                    /* onSimulationStepEnd  */
+
+/* ---- parameters -------------------------------------------------------------------------------- */
+/* Keys: "viscosity", "density0", "max_error", "max_error_v", "max_iterations", "max_iterations_v",
+ * "enable_divergence_solver", "cfl_method", "cfl_factor", "cfl_max_time_step", "cfl_min_time_step",
+ * "time_step" (sets the dt the next dt update uses), "gravitation_x|y|z", "use_graphs",
+ * "h", "h_future", "h_past", "inv_h" (dt history of DFSPHCData), "timing" (1: record CUDA events). */
+int dfsph_set_param(dfsph_ctx* ctx, const char* key, double value);
+int dfsph_get_param(dfsph_ctx* ctx, const char* key, double* value);
+
+/* Device status word (DFSPH_ST_* bits accumulated since the last clear); clear != 0 resets it. */
+int dfsph_status(dfsph_ctx* ctx, uint32_t* status, int clear);
+
+/* Number of fluid particles currently held. */
+int dfsph_num_fluid(dfsph_ctx* ctx, uint32_t* n);
+
+/* Waits for all work queued on the context's stream. */
+int dfsph_synchronize(dfsph_ctx* ctx);
+
+/* Number of kernel launches the library issued on this context since creation (for accounting). */
+int dfsph_launch_count(dfsph_ctx* ctx, uint64_t* launches);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own work or events
+ * with the solver's. */
+int dfsph_get_stream(dfsph_ctx* ctx, void** stream);
+
+/* Kernels that dfsph_time_kernel can time (no reference counterpart: measurement support). */
+enum dfsph_kernel_id {
+    DFSPH_K_NEIGHBOR_BUILD = 0,
+    DFSPH_K_DENSITY_ALPHA = 1,
+    DFSPH_K_DIVERGENCE_JACOBI = 2,
+    DFSPH_K_DIVERGENCE_RESIDUAL = 3,
+    DFSPH_K_VISCOSITY = 4,
+    DFSPH_K_PRESSURE_WARM_JACOBI = 5,
+    DFSPH_K_PRESSURE_RESIDUAL = 6,
+    DFSPH_K_PRESSURE_JACOBI = 7,
+    DFSPH_K_UPDATE_POS = 8,
+    DFSPH_K_SORT_REORDER = 9,
+    DFSPH_K_COUNT = 10
+};
+
+/* Launches one kernel of the step `reps` times on the current state with CUDA events around each
+ * launch and returns the mean device time per launch in ms. The launches modify the state (the
+ * Jacobi kernels move velocities), so call it only when the simulation will not continue, e.g. at
+ * the end of a benchmark. */
+int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DFSPH_C_H */

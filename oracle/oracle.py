@@ -1,0 +1,226 @@
+"""ctypes wrapper of the CPU oracle (liboracle_dfsph.so). Test infrastructure only."""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle_dfsph.so"
+
+FIELD_IDS = {"position": (0, 3), "velocity": (1, 3), "mass": (2, 1), "density": (3, 1), "factor": (4, 1),
+             "density_adv": (5, 1), "kappa": (6, 1), "kappa_v": (7, 1), "acceleration": (8, 3),
+             "boundary_psi": (10, 1), "boundary_position": (11, 3)}
+
+
+class OracleParams(C.Structure):
+    _fields_ = [
+        ("particle_radius", C.c_double),
+        ("density0", C.c_double),
+        ("viscosity", C.c_double),
+        ("gravitation", C.c_double * 3),
+        ("time_step", C.c_double),
+        ("max_iterations", C.c_int32),
+        ("max_error", C.c_double),
+        ("max_iterations_v", C.c_int32),
+        ("max_error_v", C.c_double),
+        ("enable_divergence_solver", C.c_int32),
+        ("cfl_method", C.c_int32),
+        ("cfl_factor", C.c_double),
+        ("cfl_max_time_step", C.c_double),
+        ("cfl_min_time_step", C.c_double),
+        ("neighbor_capacity", C.c_uint32),
+        ("brute_force", C.c_int32),
+    ]
+
+
+def lib_path() -> Path:
+    return LIB
+
+
+def build(force: bool = False) -> Path:
+    """Builds liboracle_dfsph.so with the Makefile beside this file."""
+    if force or not LIB.exists() or LIB.stat().st_mtime < (HERE / "dfsph_oracle.cpp").stat().st_mtime:
+        subprocess.run(["make", "-C", str(HERE), "liboracle_dfsph.so"], check=True, capture_output=True)
+    return LIB
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        build()
+        lib = C.CDLL(str(LIB))
+        vp, fp, dp, up = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_uint32)
+        ip = C.POINTER(C.c_int32)
+        sig = {
+            "oracle_create": (vp, [C.c_int, C.POINTER(OracleParams)]),
+            "oracle_destroy": (None, [vp]),
+            "oracle_set_boundary": (C.c_int, [vp, fp, fp, C.c_uint32, dp]),
+            "oracle_set_boundary_velocity": (C.c_int, [vp, fp, fp]),
+            "oracle_set_fluid": (C.c_int, [vp, fp, fp, fp, C.c_uint32]),
+            "oracle_update_fluid": (C.c_int, [vp, dp, dp]),
+            "oracle_step": (C.c_int, [vp, ip, ip, dp, dp]),
+            "oracle_neighbors": (C.c_int, [vp]),
+            "oracle_divergence_solve": (C.c_int, [vp, C.c_int, C.c_double]),
+            "oracle_density_alpha": (C.c_int, [vp, C.c_int]),
+            "oracle_external_forces": (C.c_int, [vp]),
+            "oracle_update_time_step": (C.c_int, [vp, C.c_double]),
+            "oracle_update_vel": (C.c_int, [vp]),
+            "oracle_pressure_solve": (C.c_int, [vp, C.c_int, C.c_double]),
+            "oracle_update_pos": (C.c_int, [vp]),
+            "oracle_on_step_end": (C.c_int, [vp]),
+            "oracle_get": (C.c_int, [vp, C.c_int, dp]),
+            "oracle_get_scalar": (C.c_int, [vp, C.c_char_p, dp]),
+            "oracle_set_scalar": (C.c_int, [vp, C.c_char_p, C.c_double]),
+            "oracle_get_neighbors": (C.c_int, [vp, up, up, C.c_uint32]),
+            "oracle_kernel_values": (C.c_int, [C.c_double, dp, C.c_uint32, C.c_int, dp, dp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _f(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32).ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Oracle:
+    """CPU restatement of the DFSPH step on one scene (fluid in original order)."""
+
+    def __init__(self, scene, precision: int = 64, brute_force: bool = False, neighbor_capacity: int = 96,
+                 boundary_psi=None):
+        self.lib = _load()
+        cfg = scene.config
+        p = OracleParams()
+        p.particle_radius = cfg.particleRadius
+        p.density0 = cfg.density0
+        p.viscosity = cfg.viscosity
+        for a in range(3):
+            p.gravitation[a] = cfg.gravitation[a]
+        p.time_step = cfg.timeStepSize
+        p.max_iterations = cfg.maxIterations
+        p.max_error = cfg.maxError
+        p.max_iterations_v = cfg.maxIterationsV
+        p.max_error_v = cfg.maxErrorV
+        p.enable_divergence_solver = 1 if cfg.enableDivergenceSolver else 0
+        p.cfl_method = cfg.cflMethod
+        p.cfl_factor = cfg.cflFactor
+        p.cfl_max_time_step = cfg.cflMaxTimeStepSize
+        p.cfl_min_time_step = 0.0001
+        p.neighbor_capacity = neighbor_capacity
+        p.brute_force = 1 if brute_force else 0
+        self.params = p
+        self.h = self.lib.oracle_create(precision, C.byref(p))
+        if not self.h:
+            raise RuntimeError("oracle_create failed")
+        self.scene = scene
+        b = np.ascontiguousarray(scene.boundary, dtype=np.float32)
+        psi = None if boundary_psi is None else np.ascontiguousarray(boundary_psi, dtype=np.float32)
+        self._keep = (b, psi)
+        if self.lib.oracle_set_boundary(self.h, _f(b), _f(psi), b.shape[0], None) != 0:
+            raise RuntimeError("oracle_set_boundary failed")
+        x = np.ascontiguousarray(scene.fluid, dtype=np.float32)
+        v = None if scene.fluid_velocity is None else np.ascontiguousarray(scene.fluid_velocity, dtype=np.float32)
+        self.n = x.shape[0]
+        self.nb = b.shape[0]
+        self.lib.oracle_set_fluid(self.h, _f(x), _f(v), None, self.n)
+
+    def close(self):
+        if self.h:
+            self.lib.oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self):
+        it, itv = C.c_int32(), C.c_int32()
+        err, errv = C.c_double(), C.c_double()
+        overflow = self.lib.oracle_step(self.h, C.byref(it), C.byref(itv), C.byref(err), C.byref(errv))
+        return dict(iterations=it.value, iterations_v=itv.value, density_error=err.value,
+                    divergence_error=errv.value, overflow=bool(overflow))
+
+    def field(self, name: str) -> np.ndarray:
+        fid, comps = FIELD_IDS[name]
+        n = self.nb if name.startswith("boundary") else self.n
+        out = np.empty(n * comps, dtype=np.float64)
+        if self.lib.oracle_get(self.h, fid, out.ctypes.data_as(C.POINTER(C.c_double))) != 0:
+            raise KeyError(name)
+        return out.reshape(n, comps) if comps > 1 else out
+
+    def scalar(self, key: str) -> float:
+        v = C.c_double()
+        if self.lib.oracle_get_scalar(self.h, key.encode(), C.byref(v)) != 0:
+            raise KeyError(key)
+        return v.value
+
+    def set_scalar(self, key: str, value: float) -> None:
+        if self.lib.oracle_set_scalar(self.h, key.encode(), float(value)) != 0:
+            raise KeyError(key)
+
+    def neighbors(self, row: int = 96):
+        self.lib.oracle_neighbors(self.h)
+        return self.get_neighbors(row)
+
+    def get_neighbors(self, row: int = 96):
+        counts = np.zeros((self.n, 2), dtype=np.uint32)
+        lists = np.zeros((self.n, row), dtype=np.uint32)
+        self.lib.oracle_get_neighbors(self.h, counts.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                      lists.ctypes.data_as(C.POINTER(C.c_uint32)), row)
+        return counts, lists
+
+    def set_positions(self, xyz: np.ndarray, vxyz: np.ndarray | None = None) -> None:
+        x = np.ascontiguousarray(xyz, dtype=np.float64)
+        v = None if vxyz is None else np.ascontiguousarray(vxyz, dtype=np.float64)
+        self.lib.oracle_update_fluid(self.h, x.ctypes.data_as(C.POINTER(C.c_double)),
+                                     None if v is None else v.ctypes.data_as(C.POINTER(C.c_double)))
+
+    # piecewise phases
+    def divergence_solve(self, max_iter=None, max_error=None) -> int:
+        c = self.scene.config
+        return self.lib.oracle_divergence_solve(self.h, c.maxIterationsV if max_iter is None else max_iter,
+                                                c.maxErrorV if max_error is None else max_error)
+
+    def density_alpha(self, warm_v: bool = True):
+        self.lib.oracle_density_alpha(self.h, 1 if warm_v else 0)
+
+    def external_forces(self):
+        self.lib.oracle_external_forces(self.h)
+
+    def update_time_step(self, hf: float):
+        self.lib.oracle_update_time_step(self.h, hf)
+
+    def update_vel(self):
+        self.lib.oracle_update_vel(self.h)
+
+    def pressure_solve(self, max_iter=None, max_error=None) -> int:
+        c = self.scene.config
+        return self.lib.oracle_pressure_solve(self.h, c.maxIterations if max_iter is None else max_iter,
+                                              c.maxError if max_error is None else max_error)
+
+    def update_pos(self):
+        self.lib.oracle_update_pos(self.h)
+
+    def on_step_end(self):
+        self.lib.oracle_on_step_end(self.h)
+
+
+def kernel_values(H: float, r: np.ndarray, precision: int = 32):
+    lib = _load()
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    w = np.empty_like(r)
+    dw = np.empty_like(r)
+    dp = C.POINTER(C.c_double)
+    lib.oracle_kernel_values(H, r.ctypes.data_as(dp), r.size, precision, w.ctypes.data_as(dp), dw.ctypes.data_as(dp))
+    return w, dw

@@ -1,0 +1,213 @@
+// dfsph_common.cuh — types, SPH kernel functions, the canonical neighbour predicate and the
+// compensated sums shared by every device kernel of the DFSPH time step.
+//
+// Everything here is templated on the arithmetic type Real (float = product, double = the FP64
+// build of the same kernels used to state each field's FP32 error).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/dfsph_c.h"
+
+namespace dfsph {
+
+// ---------------------------------------------------------------------------------------------
+// Launch shapes. One thread per particle for the gathers (SPlisHSPlasH/DFSPH/DFSPH_define_cuda.h:6
+// uses 128); 256 threads keep 8 warps per block and let the FP64 residual reduction use one shared
+// array per block.
+constexpr int kBlock = 256;
+constexpr int kWarpsPerBlock = kBlock / 32;
+
+// Divergence and pressure minimum iteration counts of the reference GPU loops
+// (DFSPH_core_cuda.cu:828 and :1378).
+constexpr int kMinItersV = 3;
+constexpr int kMinItersP = 2;
+
+// Jacobi coefficient threshold m_eps (DFSPH_define_cuda.h:7); compared in double as the reference
+// does (float |k| promoted against the double literal 1.0e-5).
+constexpr double kEps = 1.0e-5;
+
+// Neighbour count below which a particle gets no divergence source (DFSPH_core_cuda.cu:340-351).
+constexpr uint32_t kMinNeighborsForDivergence = 20;
+
+// ---------------------------------------------------------------------------------------------
+// Vector helpers.
+template <class Real> struct V3 {
+    Real x, y, z;
+};
+template <class Real> __host__ __device__ inline V3<Real> v3(Real x, Real y, Real z) { return {x, y, z}; }
+
+template <class Real> struct Vec4Traits;
+template <> struct Vec4Traits<float> { using type = float4; };
+struct alignas(32) double4a { double x, y, z, w; };
+template <> struct Vec4Traits<double> { using type = double4a; };
+template <class Real> using Vec4 = typename Vec4Traits<Real>::type;
+
+template <class Real> __device__ __forceinline__ Vec4<Real> ld4(const Vec4<Real>* p) { return *p; }
+template <> __device__ __forceinline__ float4 ld4<float>(const float4* p) { return __ldg(p); }
+
+// ---------------------------------------------------------------------------------------------
+// Compensated (Kahan) accumulation of FP32 sums. For double the same code runs; the compensation
+// term is simply tiny.
+template <class Real> struct KSum {
+    Real s = Real(0), c = Real(0);
+    __device__ __forceinline__ void add(Real v) {
+        const Real y = v - c;
+        const Real t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ Real value() const { return s; }
+};
+template <class Real> struct KSum3 {
+    KSum<Real> x, y, z;
+    __device__ __forceinline__ void add(Real a, Real b, Real d) { x.add(a); y.add(b); z.add(d); }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Canonical pair predicate. The reference tests (pos_i - pos_j).squaredNorm() < H*H
+// (SPlisHSPlasH/DFSPH/DFSPH_macro_cuda.h:149, squaredNorm at SPlisHSPlasH/Vector.h:137). Its
+// rounding depends on how the compiler contracts x*x+y*y+z*z; this library fixes one order with
+// explicit round-to-nearest intrinsics so that the device kernels and the CPU oracle decide every
+// pair identically: d2 = fma(dz,dz, fma(dy,dy, dx*dx)), strict d2 < H*H.
+__device__ __forceinline__ bool pair_within(float xi, float yi, float zi, float xj, float yj, float zj, float H2) {
+    const float dx = __fsub_rn(xi, xj), dy = __fsub_rn(yi, yj), dz = __fsub_rn(zi, zj);
+    const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+    return d2 < H2;
+}
+__device__ __forceinline__ bool pair_within(double xi, double yi, double zi, double xj, double yj, double zj, double H2) {
+    // The FP64 build decides pairs on the FP32-rounded coordinates so that both builds use the same
+    // neighbour sets (positions enter both builds as the same float values).
+    return pair_within((float)xi, (float)yi, (float)zi, (float)xj, (float)yj, (float)zj, (float)H2);
+}
+
+// Cell coordinate along one axis: floor(x / H + offset), the reference's
+// (pos / kernelRadius) + gridOffset followed by toFloor (DFSPH_core_cuda.cu:1839-1841,
+// SPlisHSPlasH/Vector.h:157), in FP32 with an IEEE division.
+__device__ __forceinline__ int cell_coord(float x, float H, int offset) {
+    return (int)floorf(__fadd_rn(__fdiv_rn(x, H), (float)offset));
+}
+__device__ __forceinline__ int cell_coord(double x, double H, int offset) {
+    return cell_coord((float)x, (float)H, offset);
+}
+
+// 30-bit Morton key of 10-bit cell coordinates (x in the lowest bit of each triple).
+__host__ __device__ inline uint32_t spread_bits10(uint32_t v) {
+    v &= 0x3FFu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__host__ __device__ inline uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+    return spread_bits10(x) | (spread_bits10(y) << 1) | (spread_bits10(z) << 2);
+}
+__host__ __device__ inline uint32_t compact_bits10(uint32_t v) {
+    v &= 0x09249249u;
+    v = (v | (v >> 2)) & 0x030C30C3u;
+    v = (v | (v >> 4)) & 0x0300F00Fu;
+    v = (v | (v >> 8)) & 0x030000FFu;
+    v = (v | (v >> 16)) & 0x000003FFu;
+    return v;
+}
+constexpr uint32_t kEscapedKey = 0xFFFFFFFFu;  // sorts after every valid 30-bit Morton key
+
+// ---------------------------------------------------------------------------------------------
+// Cubic spline kernel (SPlisHSPlasH/DFSPH/SPH_kernels.h:20-100, CubicKernelPerso): W and grad W
+// with support H, k = 8/(pi H^3), l = 48/(pi H^3); grad W = 0 for |r| <= 1e-6.
+template <class Real> struct Cubic {
+    Real H, invH, k, l, W0;
+    __device__ __forceinline__ Real W_of_q(Real q) const {
+        if (q <= Real(1)) {
+            if (q <= Real(0.5)) {
+                const Real q2 = q * q;
+                const Real q3 = q2 * q;
+                return k * (Real(6) * q3 - Real(6) * q2 + Real(1));
+            }
+            const Real f = Real(1) - q;
+            return k * (Real(2) * f * f * f);
+        }
+        return Real(0);
+    }
+    __device__ __forceinline__ Real W(Real rx, Real ry, Real rz) const {
+        const Real rl = sqrt_(rx * rx + ry * ry + rz * rz);
+        return W_of_q(rl / H);
+    }
+    // Returns grad W(r) and W(r) from one square root.
+    __device__ __forceinline__ void gradW(Real rx, Real ry, Real rz, Real& gx, Real& gy, Real& gz) const {
+        const Real rl = sqrt_(rx * rx + ry * ry + rz * rz);
+        const Real q = rl / H;
+        gx = gy = gz = Real(0);
+        if (q <= Real(1) && (double)rl > 1.0e-6) {
+            const Real s = Real(1) / (rl * H);
+            Real c;
+            if (q <= Real(0.5)) {
+                c = l * q * (Real(3) * q - Real(2));
+            } else {
+                const Real f = Real(1) - q;
+                c = l * (-f * f);
+            }
+            gx = c * (rx * s);
+            gy = c * (ry * s);
+            gz = c * (rz * s);
+        }
+    }
+    __device__ __forceinline__ void W_gradW(Real rx, Real ry, Real rz, Real& w, Real& gx, Real& gy, Real& gz) const {
+        const Real rl = sqrt_(rx * rx + ry * ry + rz * rz);
+        const Real q = rl / H;
+        gx = gy = gz = Real(0);
+        w = W_of_q(q);
+        if (q <= Real(1) && (double)rl > 1.0e-6) {
+            const Real s = Real(1) / (rl * H);
+            Real c;
+            if (q <= Real(0.5)) {
+                c = l * q * (Real(3) * q - Real(2));
+            } else {
+                const Real f = Real(1) - q;
+                c = l * (-f * f);
+            }
+            gx = c * (rx * s);
+            gy = c * (ry * s);
+            gz = c * (rz * s);
+        }
+    }
+    static __device__ __forceinline__ float sqrt_(float v) { return sqrtf(v); }
+    static __device__ __forceinline__ double sqrt_(double v) { return sqrt(v); }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Per-launch parameters (passed by value). The dt history mirrors DFSPHCData
+// (DFSPH_c_arrays_structure.h:343-354, updateTimeStep/onSimulationStepEnd at .cpp:1100-1118).
+template <class Real> struct StepParams {
+    Cubic<Real> kern;
+    Real H2;              // H*H for the predicate (computed in float for both builds)
+    Real density0;
+    Real viscosity;
+    Real gx, gy, gz;
+    Real h, h_future, inv_h, inv_h_future, h_ratio_to_past, h_ratio_to_past2;
+    int off_x, off_y, off_z;     // grid offset (cells)
+    int dim_x, dim_y, dim_z;     // cell grid extent
+    uint32_t n_fluid;
+    uint32_t n_boundary;
+    uint32_t nbr_stride;         // row stride of the interleaved neighbour table
+    uint32_t nbr_cap;            // stored neighbours per particle
+    int boundary_moving;         // 1: boundary velocities are read (else zero)
+};
+
+// Device-side control block of one solver loop (divergence or pressure).
+struct LoopCtl {
+    double sum;          // last residual sum over all fluid particles (FP64)
+    double avg;          // sum / n
+    double eta;          // tolerance (absolute)
+    double init_avg;     // residual after the init pass
+    int32_t iter;        // iterations done
+    int32_t max_iter;
+    int32_t min_iter;
+    uint32_t cont;       // loop condition for the next iteration
+    uint32_t ticket;     // last-block election counter
+    uint32_t pad;
+};
+
+}  // namespace dfsph

@@ -1,0 +1,215 @@
+// io.cu — device-side packing between the caller's packed xyz arrays and the solver's SoA layout.
+//
+// Replaces load_UnifiedParticleSet_cuda / read_UnifiedParticleSet_cuda
+// (DFSPH_memory_management_cuda.cu:613-656), which copy AoS Vector3d arrays through managed memory.
+#include "io.cuh"
+
+namespace dfsph {
+
+namespace {
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock) unpack_fluid_kernel(const float* __restrict__ xyz,
+                                                              const float* __restrict__ vxyz,
+                                                              const float* __restrict__ mass, float default_mass,
+                                                              uint32_t n, Vec4<Real>* __restrict__ pos,
+                                                              Vec4<Real>* __restrict__ vel, Real* __restrict__ kappa,
+                                                              Real* __restrict__ kappaV, uint32_t* __restrict__ id) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec4<Real> x, v;
+    x.x = (Real)xyz[3 * i + 0];
+    x.y = (Real)xyz[3 * i + 1];
+    x.z = (Real)xyz[3 * i + 2];
+    x.w = (Real)(mass ? mass[i] : default_mass);
+    v.x = vxyz ? (Real)vxyz[3 * i + 0] : Real(0);
+    v.y = vxyz ? (Real)vxyz[3 * i + 1] : Real(0);
+    v.z = vxyz ? (Real)vxyz[3 * i + 2] : Real(0);
+    v.w = Real(0);
+    pos[i] = x;
+    vel[i] = v;
+    kappa[i] = Real(0);
+    kappaV[i] = Real(0);
+    id[i] = i;
+}
+
+// Overwrites positions/velocities of each slot from the caller's arrays indexed by particle id.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) update_fluid_kernel(const float* __restrict__ xyz,
+                                                              const float* __restrict__ vxyz, uint32_t n,
+                                                              const uint32_t* __restrict__ id,
+                                                              Vec4<Real>* __restrict__ pos,
+                                                              Vec4<Real>* __restrict__ vel) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = id[i];
+    Vec4<Real> x = pos[i];
+    x.x = (Real)xyz[3 * t + 0];
+    x.y = (Real)xyz[3 * t + 1];
+    x.z = (Real)xyz[3 * t + 2];
+    pos[i] = x;
+    Vec4<Real> v;
+    v.x = vxyz ? (Real)vxyz[3 * t + 0] : Real(0);
+    v.y = vxyz ? (Real)vxyz[3 * t + 1] : Real(0);
+    v.z = vxyz ? (Real)vxyz[3 * t + 2] : Real(0);
+    v.w = Real(0);
+    vel[i] = v;
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock) unpack_boundary_kernel(const float* __restrict__ xyz,
+                                                                 const float* __restrict__ psi, uint32_t n,
+                                                                 Vec4<Real>* __restrict__ bpos,
+                                                                 Vec4<Real>* __restrict__ bvel) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Vec4<Real> x;
+    x.x = (Real)xyz[3 * i + 0];
+    x.y = (Real)xyz[3 * i + 1];
+    x.z = (Real)xyz[3 * i + 2];
+    x.w = psi ? (Real)psi[i] : Real(0);
+    bpos[i] = x;
+    Vec4<Real> v;
+    v.x = v.y = v.z = v.w = Real(0);
+    bvel[i] = v;
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock) reorder_boundary_kernel(const uint32_t* __restrict__ perm, uint32_t n,
+                                                                  const Vec4<Real>* __restrict__ bpos_in,
+                                                                  const Vec4<Real>* __restrict__ bvel_in,
+                                                                  Vec4<Real>* __restrict__ bpos_out,
+                                                                  Vec4<Real>* __restrict__ bvel_out,
+                                                                  uint32_t* __restrict__ bid_out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t j = perm[i];
+    if (j >= n) j = i;  // only after a failed sort (flagged in the status word); stay in range
+    bpos_out[i] = bpos_in[j];
+    bvel_out[i] = bvel_in[j];
+    bid_out[i] = j;
+}
+
+// Moves boundary particles given in original order (bid maps sorted slot -> original index).
+template <class Real>
+__global__ void __launch_bounds__(kBlock) move_boundary_kernel(const float* __restrict__ xyz,
+                                                               const float* __restrict__ vxyz, uint32_t n,
+                                                               const uint32_t* __restrict__ bid,
+                                                               Vec4<Real>* __restrict__ bpos,
+                                                               Vec4<Real>* __restrict__ bvel) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = bid[i];
+    Vec4<Real> x = bpos[i];
+    x.x = (Real)xyz[3 * t + 0];
+    x.y = (Real)xyz[3 * t + 1];
+    x.z = (Real)xyz[3 * t + 2];
+    bpos[i] = x;
+    Vec4<Real> v;
+    v.x = vxyz ? (Real)vxyz[3 * t + 0] : Real(0);
+    v.y = vxyz ? (Real)vxyz[3 * t + 1] : Real(0);
+    v.z = vxyz ? (Real)vxyz[3 * t + 2] : Real(0);
+    v.w = Real(0);
+    bvel[i] = v;
+}
+
+// Field download: element c of slot i of src (stride src_stride Real elements) goes to
+// dst[(id ? id[i] : i) * comps + c], converted to Out.
+template <class Real, class Out>
+__global__ void __launch_bounds__(kBlock) pack_field_kernel(const Real* __restrict__ src, int src_stride, int comps,
+                                                            const uint32_t* __restrict__ id, uint32_t n,
+                                                            Out* __restrict__ dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = id ? id[i] : i;
+    for (int c = 0; c < comps; ++c) dst[(size_t)t * comps + c] = (Out)src[(size_t)i * src_stride + c];
+}
+
+__global__ void __launch_bounds__(kBlock) pack_u32_kernel(const uint32_t* __restrict__ src, int comps,
+                                                          const uint32_t* __restrict__ id, uint32_t n,
+                                                          uint32_t* __restrict__ dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = id ? id[i] : i;
+    for (int c = 0; c < comps; ++c) dst[(size_t)t * comps + c] = src[(size_t)i * comps + c];
+}
+
+__global__ void __launch_bounds__(kBlock) unpack_counts_kernel(const uint32_t* __restrict__ counts,
+                                                               const uint32_t* __restrict__ id, uint32_t n,
+                                                               uint32_t* __restrict__ dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = id ? id[i] : i;
+    dst[2 * (size_t)t + 0] = counts[i] & 0xFFFFu;
+    dst[2 * (size_t)t + 1] = counts[i] >> 16;
+}
+
+// Publishes a new device state block. The block travels as a kernel parameter, so the update is
+// ordered with the surrounding work on the stream and never reads host memory asynchronously.
+template <class Real> __global__ void set_state_kernel(DevState<Real>* __restrict__ dst, DevState<Real> v) { *dst = v; }
+
+}  // namespace
+
+template <class Real> void launch_set_state(DevState<Real>* dst, const DevState<Real>& v, cudaStream_t s) {
+    set_state_kernel<Real><<<1, 1, 0, s>>>(dst, v);
+}
+
+template <class Real>
+void launch_unpack_fluid(const float* xyz, const float* vxyz, const float* mass, float default_mass, uint32_t n,
+                         Vec4<Real>* pos, Vec4<Real>* vel, Real* kappa, Real* kappaV, uint32_t* id, cudaStream_t s) {
+    if (n)
+        unpack_fluid_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(xyz, vxyz, mass, default_mass, n, pos, vel, kappa,
+                                                                 kappaV, id);
+}
+template <class Real>
+void launch_update_fluid(const float* xyz, const float* vxyz, uint32_t n, const uint32_t* id, Vec4<Real>* pos,
+                         Vec4<Real>* vel, cudaStream_t s) {
+    if (n) update_fluid_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(xyz, vxyz, n, id, pos, vel);
+}
+template <class Real>
+void launch_unpack_boundary(const float* xyz, const float* psi, uint32_t n, Vec4<Real>* bpos, Vec4<Real>* bvel,
+                            cudaStream_t s) {
+    if (n) unpack_boundary_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(xyz, psi, n, bpos, bvel);
+}
+template <class Real>
+void launch_reorder_boundary(const uint32_t* perm, uint32_t n, const Vec4<Real>* bpos_in, const Vec4<Real>* bvel_in,
+                             Vec4<Real>* bpos_out, Vec4<Real>* bvel_out, uint32_t* bid_out, cudaStream_t s) {
+    if (n)
+        reorder_boundary_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(perm, n, bpos_in, bvel_in, bpos_out, bvel_out,
+                                                                     bid_out);
+}
+template <class Real>
+void launch_move_boundary(const float* xyz, const float* vxyz, uint32_t n, const uint32_t* bid, Vec4<Real>* bpos,
+                          Vec4<Real>* bvel, cudaStream_t s) {
+    if (n) move_boundary_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(xyz, vxyz, n, bid, bpos, bvel);
+}
+template <class Real, class Out>
+void launch_pack_field(const Real* src, int src_stride, int comps, const uint32_t* id, uint32_t n, Out* dst,
+                       cudaStream_t s) {
+    if (n) pack_field_kernel<Real, Out><<<grid_for(n), kBlock, 0, s>>>(src, src_stride, comps, id, n, dst);
+}
+void launch_pack_u32(const uint32_t* src, int comps, const uint32_t* id, uint32_t n, uint32_t* dst, cudaStream_t s) {
+    if (n) pack_u32_kernel<<<grid_for(n), kBlock, 0, s>>>(src, comps, id, n, dst);
+}
+void launch_unpack_counts(const uint32_t* counts, const uint32_t* id, uint32_t n, uint32_t* dst, cudaStream_t s) {
+    if (n) unpack_counts_kernel<<<grid_for(n), kBlock, 0, s>>>(counts, id, n, dst);
+}
+
+#define DFSPH_INSTANTIATE_IO(R)                                                                                      \
+    template void launch_set_state<R>(DevState<R>*, const DevState<R>&, cudaStream_t);                               \
+    template void launch_unpack_fluid<R>(const float*, const float*, const float*, float, uint32_t, Vec4<R>*,        \
+                                         Vec4<R>*, R*, R*, uint32_t*, cudaStream_t);                                 \
+    template void launch_update_fluid<R>(const float*, const float*, uint32_t, const uint32_t*, Vec4<R>*, Vec4<R>*,  \
+                                         cudaStream_t);                                                              \
+    template void launch_unpack_boundary<R>(const float*, const float*, uint32_t, Vec4<R>*, Vec4<R>*, cudaStream_t); \
+    template void launch_reorder_boundary<R>(const uint32_t*, uint32_t, const Vec4<R>*, const Vec4<R>*, Vec4<R>*,   \
+                                             Vec4<R>*, uint32_t*, cudaStream_t);                                     \
+    template void launch_move_boundary<R>(const float*, const float*, uint32_t, const uint32_t*, Vec4<R>*, Vec4<R>*, \
+                                          cudaStream_t);                                                             \
+    template void launch_pack_field<R, float>(const R*, int, int, const uint32_t*, uint32_t, float*, cudaStream_t);  \
+    template void launch_pack_field<R, double>(const R*, int, int, const uint32_t*, uint32_t, double*, cudaStream_t);
+
+DFSPH_INSTANTIATE_IO(float)
+DFSPH_INSTANTIATE_IO(double)
+
+}  // namespace dfsph

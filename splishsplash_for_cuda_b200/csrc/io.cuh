@@ -1,0 +1,30 @@
+// io.cuh — launch wrappers of io.cu.
+#pragma once
+#include "dfsph_state.cuh"
+
+namespace dfsph {
+
+template <class Real> void launch_set_state(DevState<Real>* dst, const DevState<Real>& v, cudaStream_t s);
+
+template <class Real>
+void launch_unpack_fluid(const float* xyz, const float* vxyz, const float* mass, float default_mass, uint32_t n,
+                         Vec4<Real>* pos, Vec4<Real>* vel, Real* kappa, Real* kappaV, uint32_t* id, cudaStream_t s);
+template <class Real>
+void launch_update_fluid(const float* xyz, const float* vxyz, uint32_t n, const uint32_t* id, Vec4<Real>* pos,
+                         Vec4<Real>* vel, cudaStream_t s);
+template <class Real>
+void launch_unpack_boundary(const float* xyz, const float* psi, uint32_t n, Vec4<Real>* bpos, Vec4<Real>* bvel,
+                            cudaStream_t s);
+template <class Real>
+void launch_reorder_boundary(const uint32_t* perm, uint32_t n, const Vec4<Real>* bpos_in, const Vec4<Real>* bvel_in,
+                             Vec4<Real>* bpos_out, Vec4<Real>* bvel_out, uint32_t* bid_out, cudaStream_t s);
+template <class Real>
+void launch_move_boundary(const float* xyz, const float* vxyz, uint32_t n, const uint32_t* bid, Vec4<Real>* bpos,
+                          Vec4<Real>* bvel, cudaStream_t s);
+template <class Real, class Out>
+void launch_pack_field(const Real* src, int src_stride, int comps, const uint32_t* id, uint32_t n, Out* dst,
+                       cudaStream_t s);
+void launch_pack_u32(const uint32_t* src, int comps, const uint32_t* id, uint32_t n, uint32_t* dst, cudaStream_t s);
+void launch_unpack_counts(const uint32_t* counts, const uint32_t* id, uint32_t n, uint32_t* dst, cudaStream_t s);
+
+}  // namespace dfsph

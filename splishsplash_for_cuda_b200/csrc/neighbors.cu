@@ -1,0 +1,275 @@
+// neighbors.cu — cell keys, fluid reorder, cell-start table, neighbour lists and boundary psi.
+//
+// Reference: cuda_neighborsSearch (DFSPH_core_cuda.cu:2651-3024) with
+// DFSPH_computeGridIdx_kernel (:1833-1848), DFSPH_CountingSortIds_kernel (:1851-1857),
+// cuda_sortData (:2057-2120) and DFSPH_neighborsSearch_kernel<true> (:2219-2517), which iterates
+// ITER_NEIGHBORS_FROM_STRUCTURE_LINEAR_ADVANCED (DFSPH_macro_cuda.h:136-155): every particle of the
+// 27 cells around the particle's cell is tested with squaredNorm < H^2, self excluded for the fluid.
+//
+// Differences by design: 30-bit Morton keys sorted by a stable in-house radix sort (sort.cu)
+// instead of a dense 256^3 histogram; a cell table sized to the scene's grid, cleared per step;
+// neighbour lists with a checked capacity (the reference writes past MAX_NEIGHBOURS = 90 unchecked).
+#include "dfsph_state.cuh"
+
+namespace dfsph {
+
+namespace {
+
+template <class Real>
+__device__ __forceinline__ bool particle_cell(Real x, Real y, Real z, const StepParams<Real>& p, int& cx, int& cy,
+                                              int& cz) {
+    if (!(isfinite(x) && isfinite(y) && isfinite(z))) return false;
+    cx = cell_coord(x, p.kern.H, p.off_x);
+    cy = cell_coord(y, p.kern.H, p.off_y);
+    cz = cell_coord(z, p.kern.H, p.off_z);
+    return cx >= 0 && cy >= 0 && cz >= 0 && cx < p.dim_x && cy < p.dim_y && cz < p.dim_z;
+}
+
+__device__ __forceinline__ uint32_t cell_linear(int cx, int cy, int cz, int dim_x, int dim_y) {
+    return (uint32_t)cx + (uint32_t)dim_x * ((uint32_t)cy + (uint32_t)dim_y * (uint32_t)cz);
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock) cell_keys_kernel(const Vec4<Real>* __restrict__ pos, uint32_t n,
+                                                           StepParams<Real> p, uint32_t* __restrict__ keys,
+                                                           uint32_t* __restrict__ status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Vec4<Real> x = pos[i];
+    int cx, cy, cz;
+    uint32_t key;
+    if (particle_cell(x.x, x.y, x.z, p, cx, cy, cz)) {
+        key = morton3((uint32_t)cx, (uint32_t)cy, (uint32_t)cz);
+    } else {
+        key = kEscapedKey;
+        const bool finite = isfinite(x.x) && isfinite(x.y) && isfinite(x.z);
+        atomicOr(status, finite ? DFSPH_ST_ESCAPED : (DFSPH_ST_NONFINITE | DFSPH_ST_ESCAPED));
+    }
+    keys[i] = key;
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock) reorder_fluid_kernel(
+    const uint32_t* __restrict__ perm, uint32_t n, const Vec4<Real>* __restrict__ pos_in,
+    const Vec4<Real>* __restrict__ vel_in, const Real* __restrict__ kappa_in, const Real* __restrict__ kappaV_in,
+    const uint32_t* __restrict__ id_in, Vec4<Real>* __restrict__ pos_out, Vec4<Real>* __restrict__ vel_out,
+    Real* __restrict__ kappa_out, Real* __restrict__ kappaV_out, uint32_t* __restrict__ id_out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t j = perm[i];
+    if (j >= n) j = i;  // only after a failed sort (flagged in the status word); stay in range
+    pos_out[i] = pos_in[j];
+    vel_out[i] = vel_in[j];
+    kappa_out[i] = kappa_in[j];
+    kappaV_out[i] = kappaV_in[j];
+    id_out[i] = id_in[j];
+}
+
+// Cell start/end from run boundaries of the sorted keys (replaces the dense histogram scan).
+__global__ void __launch_bounds__(kBlock) cell_bounds_kernel(const uint32_t* __restrict__ keys, uint32_t n, int dim_x,
+                                                             int dim_y, int dim_z, uint2* __restrict__ table) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t k = keys[i];
+    if (k == kEscapedKey) return;
+    const uint32_t cx = compact_bits10(k), cy = compact_bits10(k >> 1), cz = compact_bits10(k >> 2);
+    if (cx >= (uint32_t)dim_x || cy >= (uint32_t)dim_y || cz >= (uint32_t)dim_z) return;
+    const uint32_t lin = cell_linear((int)cx, (int)cy, (int)cz, dim_x, dim_y);
+    if (i == 0 || keys[i - 1] != k) table[lin].x = i;
+    if (i == n - 1 || keys[i + 1] != k) table[lin].y = i + 1;
+}
+
+// One thread per fluid particle: fluid neighbours (self excluded) then boundary neighbours, cells in
+// a fixed order (z, y, x from -1 to +1), particles of a cell in sorted order. Lists are written
+// interleaved (nbr[k * stride + i]) so that the gathers read them coalesced.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) build_neighbors_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+                                                                 const uint2* __restrict__ ftab,
+                                                                 const uint2* __restrict__ btab) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const StepParams<Real>& p = ds->p;
+    const Vec4<Real>* __restrict__ pos = ds->pos;
+    const Vec4<Real>* __restrict__ bpos = ds->bpos;
+    uint32_t* __restrict__ nbr = ds->nbr;
+    const uint32_t stride = p.nbr_stride, cap = p.nbr_cap;
+    const Vec4<Real> xi = pos[i];
+    int cx, cy, cz;
+    uint32_t nf = 0, nb = 0, total = 0;
+    bool overflow = false;
+    if (particle_cell(xi.x, xi.y, xi.z, p, cx, cy, cz)) {
+        const Real H2 = p.H2;
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int z = cz + dz;
+            if (z < 0 || z >= p.dim_z) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int y = cy + dy;
+                if (y < 0 || y >= p.dim_y) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int x = cx + dx;
+                    if (x < 0 || x >= p.dim_x) continue;
+                    const uint2 r = ftab[cell_linear(x, y, z, p.dim_x, p.dim_y)];
+                    for (uint32_t j = r.x; j < r.y; ++j) {
+                        if (j == i) continue;
+                        const Vec4<Real> xj = ld4<Real>(pos + j);
+                        if (pair_within(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z, H2)) {
+                            if (total < cap) {
+                                nbr[(size_t)total * stride + i] = j;
+                                ++total;
+                                ++nf;
+                            } else {
+                                overflow = true;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (p.n_boundary > 0) {
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int z = cz + dz;
+                if (z < 0 || z >= p.dim_z) continue;
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const int y = cy + dy;
+                    if (y < 0 || y >= p.dim_y) continue;
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        const int x = cx + dx;
+                        if (x < 0 || x >= p.dim_x) continue;
+                        const uint2 r = btab[cell_linear(x, y, z, p.dim_x, p.dim_y)];
+                        for (uint32_t j = r.x; j < r.y; ++j) {
+                            const Vec4<Real> xj = ld4<Real>(bpos + j);
+                            if (pair_within(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z, H2)) {
+                                if (total < cap) {
+                                    nbr[(size_t)total * stride + i] = j;
+                                    ++total;
+                                    ++nb;
+                                } else {
+                                    overflow = true;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (overflow) atomicOr(ds->status, DFSPH_ST_NEIGHBOR_OVERFLOW);
+    ds->counts[i] = nf | (nb << 16);
+}
+
+// Akinci boundary psi (FluidModel::computeBoundaryPsi, FluidModel.cpp:233-258):
+// psi_b = rho0 / (W0 + sum_{b' != b, |x_b - x_b'| < H} W(x_b - x_b')), accumulated in FP64.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) boundary_psi_kernel(const Vec4<Real>* __restrict__ bpos_in,
+                                                              Vec4<Real>* __restrict__ bpos_out, uint32_t nb,
+                                                              StepParams<Real> p, const uint2* __restrict__ btab,
+                                                              uint32_t* __restrict__ status) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const Vec4<Real> xb = bpos_in[b];
+    int cx, cy, cz;
+    const double H = (double)p.kern.H;
+    const double k = 8.0 / (3.14159265358979323846 * H * H * H);
+    double delta = k;  // W(0)
+    if (particle_cell(xb.x, xb.y, xb.z, p, cx, cy, cz)) {
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int z = cz + dz;
+            if (z < 0 || z >= p.dim_z) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int y = cy + dy;
+                if (y < 0 || y >= p.dim_y) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int x = cx + dx;
+                    if (x < 0 || x >= p.dim_x) continue;
+                    const uint2 r = btab[cell_linear(x, y, z, p.dim_x, p.dim_y)];
+                    for (uint32_t j = r.x; j < r.y; ++j) {
+                        if (j == b) continue;
+                        const Vec4<Real> xj = bpos_in[j];
+                        if (pair_within(xb.x, xb.y, xb.z, xj.x, xj.y, xj.z, p.H2)) {
+                            const double rx = (double)xb.x - (double)xj.x;
+                            const double ry = (double)xb.y - (double)xj.y;
+                            const double rz = (double)xb.z - (double)xj.z;
+                            const double q = sqrt(rx * rx + ry * ry + rz * rz) / H;
+                            double w = 0.0;
+                            if (q <= 1.0) {
+                                if (q <= 0.5) {
+                                    w = k * (6.0 * q * q * q - 6.0 * q * q + 1.0);
+                                } else {
+                                    const double f = 1.0 - q;
+                                    w = k * (2.0 * f * f * f);
+                                }
+                            }
+                            delta += w;
+                        }
+                    }
+                }
+            }
+        }
+    } else {
+        atomicOr(status, DFSPH_ST_BOUNDARY_OVERFLOW);
+    }
+    Vec4<Real> out = xb;
+    out.w = (Real)((double)p.density0 / delta);
+    bpos_out[b] = out;
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock) scatter_by_id_kernel(const uint32_t* __restrict__ id, uint32_t n,
+                                                               const Real* __restrict__ src, int comps,
+                                                               int src_stride, Real* __restrict__ dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = id[i];
+    for (int c = 0; c < comps; ++c) dst[(size_t)t * comps + c] = src[(size_t)i * src_stride + c];
+}
+
+}  // namespace
+
+template <class Real>
+void launch_cell_keys(const Vec4<Real>* pos, uint32_t n, const StepParams<Real>& p, uint32_t* keys, uint32_t* status,
+                      cudaStream_t s) {
+    if (n) cell_keys_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(pos, n, p, keys, status);
+}
+template <class Real>
+void launch_reorder_fluid(const uint32_t* perm, uint32_t n, const Vec4<Real>* pos_in, const Vec4<Real>* vel_in,
+                          const Real* kappa_in, const Real* kappaV_in, const uint32_t* id_in, Vec4<Real>* pos_out,
+                          Vec4<Real>* vel_out, Real* kappa_out, Real* kappaV_out, uint32_t* id_out, cudaStream_t s) {
+    if (n)
+        reorder_fluid_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(perm, n, pos_in, vel_in, kappa_in, kappaV_in, id_in,
+                                                                  pos_out, vel_out, kappa_out, kappaV_out, id_out);
+}
+void launch_cell_bounds(const uint32_t* sorted_keys, uint32_t n, int dim_x, int dim_y, int dim_z, uint2* table,
+                        cudaStream_t s) {
+    if (n) cell_bounds_kernel<<<grid_for(n), kBlock, 0, s>>>(sorted_keys, n, dim_x, dim_y, dim_z, table);
+}
+template <class Real>
+void launch_build_neighbors(const DevState<Real>* d, uint32_t n, const uint2* fluid_table, const uint2* boundary_table,
+                            cudaStream_t s) {
+    if (n) build_neighbors_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, fluid_table, boundary_table);
+}
+template <class Real>
+void launch_boundary_psi(const Vec4<Real>* bpos_in, Vec4<Real>* bpos_out, uint32_t nb, const StepParams<Real>& p,
+                         const uint2* boundary_table, uint32_t* status, cudaStream_t s) {
+    if (nb) boundary_psi_kernel<Real><<<grid_for(nb), kBlock, 0, s>>>(bpos_in, bpos_out, nb, p, boundary_table, status);
+}
+template <class Real>
+void launch_scatter_by_id(const uint32_t* id, uint32_t n, const Real* src, int comps, int src_stride, Real* dst,
+                          cudaStream_t s) {
+    if (n) scatter_by_id_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(id, n, src, comps, src_stride, dst);
+}
+
+#define DFSPH_INSTANTIATE_NEIGHBORS(R)                                                                               \
+    template void launch_cell_keys<R>(const Vec4<R>*, uint32_t, const StepParams<R>&, uint32_t*, uint32_t*,          \
+                                      cudaStream_t);                                                                 \
+    template void launch_reorder_fluid<R>(const uint32_t*, uint32_t, const Vec4<R>*, const Vec4<R>*, const R*,       \
+                                          const R*, const uint32_t*, Vec4<R>*, Vec4<R>*, R*, R*, uint32_t*,          \
+                                          cudaStream_t);                                                             \
+    template void launch_build_neighbors<R>(const DevState<R>*, uint32_t, const uint2*, const uint2*, cudaStream_t); \
+    template void launch_boundary_psi<R>(const Vec4<R>*, Vec4<R>*, uint32_t, const StepParams<R>&, const uint2*,     \
+                                         uint32_t*, cudaStream_t);                                                   \
+    template void launch_scatter_by_id<R>(const uint32_t*, uint32_t, const R*, int, int, R*, cudaStream_t);
+
+DFSPH_INSTANTIATE_NEIGHBORS(float)
+DFSPH_INSTANTIATE_NEIGHBORS(double)
+
+}  // namespace dfsph

@@ -1,0 +1,661 @@
+// solver.cu — the gather kernels of the DFSPH time step.
+//
+// Reference kernels (SPlisHSPlasH/DFSPH/DFSPH_core_cuda.cu):
+//   density + alpha + kappa_v warm start + divergence source  DFSPH_divergence_warmstart_init_kernel :221-237
+//   divergence Jacobi (warm start / iteration)                 divergenceSolveParticle :400-480, :495-517
+//   divergence residual                                        computeDensityChange :546-614, :618-709, :732-748
+//   XSPH viscosity + gravity                                   DFSPH_viscosityXSPH_kernel :1423-1507
+//   velocity update + kappa warm-start scaling                 DFSPH_update_vel_kernel :3047-3070
+//   pressure Jacobi (warm start / iteration)                   pressureSolveParticle :867-951, :965-980
+//   density residual                                           computeDensityAdv :1165-1214, :1217-1243, :1264-1284
+//   position update                                            DFSPH_update_pos_kernel :3127-3215
+// The residual sums that decide convergence (cub::DeviceReduce::Sum + blocking copy in the
+// reference, :774-781 and :1321-1325) are fused into the residual kernels as deterministic FP64
+// block reductions whose last block evaluates the loop condition on the device (and, inside a CUDA
+// graph, sets the while-node condition), so no host round trip happens per iteration.
+#include "dfsph_state.cuh"
+
+namespace dfsph {
+
+namespace {
+
+template <class Real> __device__ __forceinline__ Real rmax(Real a, Real b);
+template <> __device__ __forceinline__ float rmax<float>(float a, float b) { return fmaxf(a, b); }
+template <> __device__ __forceinline__ double rmax<double>(double a, double b) { return fmax(a, b); }
+
+__device__ __forceinline__ bool above_eps(float v) { return (double)fabsf(v) > kEps; }
+__device__ __forceinline__ bool above_eps(double v) { return fabs(v) > kEps; }
+
+__device__ __forceinline__ uint32_t fluid_count(uint32_t c) { return c & 0xFFFFu; }
+__device__ __forceinline__ uint32_t boundary_count(uint32_t c) { return c >> 16; }
+
+// Deterministic FP64 sum over the grid, then (last block) the loop decision. The partial of each
+// block is reduced in a fixed shuffle pattern and the last block adds the partials in block order.
+template <int kIsInit>
+__device__ void reduce_and_decide(double v, double* __restrict__ partials, LoopCtl* __restrict__ ctl, uint32_t n,
+                                  double eta, int min_it, int max_it, cudaGraphConditionalHandle handle,
+                                  bool use_handle) {
+    __shared__ double warp_sums[kWarpsPerBlock];
+    __shared__ bool is_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    if (lane == 0) warp_sums[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kWarpsPerBlock; ++w) s += warp_sums[w];
+        partials[blockIdx.x] = s;
+        __threadfence();
+        const uint32_t t = atomicAdd(&ctl->ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    double s = 0.0;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += ((volatile double*)partials)[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
+    __syncthreads();
+    if (lane == 0) warp_sums[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < kWarpsPerBlock; ++w) tot += warp_sums[w];
+        const double avg = n ? tot / (double)n : 0.0;
+        ctl->sum = tot;
+        uint32_t cont;
+        if (kIsInit) {
+            // The init pass fixes the tolerance and bounds of the loop that follows; the loop
+            // kernels (possibly replayed from a CUDA graph) read them back from the control block.
+            ctl->eta = eta;
+            ctl->min_iter = min_it;
+            ctl->max_iter = max_it;
+            ctl->init_avg = avg;
+            ctl->avg = 0.0;
+            ctl->iter = 0;
+            cont = (max_it > 0) ? 1u : 0u;
+        } else {
+            const int it = ctl->iter + 1;
+            ctl->iter = it;
+            ctl->avg = avg;
+            cont = ((avg > ctl->eta) || (it < ctl->min_iter)) && (it < ctl->max_iter) ? 1u : 0u;
+        }
+        ctl->cont = cont;
+        ctl->ticket = 0;
+        __threadfence();
+        if (use_handle) cudaGraphSetConditional(handle, cont);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// density + alpha + divergence source (+ kappa_v warm-start scaling), one pass over the neighbours.
+template <class Real, bool kWarmV, bool kFeatures>
+__global__ void __launch_bounds__(kBlock) density_alpha_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const StepParams<Real>& p = ds->p;
+    const Vec4<Real>* __restrict__ pos = ds->pos;
+    const Vec4<Real>* __restrict__ vel = ds->vel;
+    const Vec4<Real>* __restrict__ bpos = ds->bpos;
+    const Vec4<Real>* __restrict__ bvel = ds->bvel;
+    const uint32_t* __restrict__ nbr = ds->nbr;
+    const uint32_t stride = p.nbr_stride;
+    const Cubic<Real> K = p.kern;
+
+    if (kWarmV) ds->kappaV[i] = rmax<Real>(ds->kappaV[i] * p.h_ratio_to_past / Real(2), Real(-0.5));
+
+    const Vec4<Real> xi = pos[i];
+    const Vec4<Real> vi = vel[i];
+    const uint32_t c = ds->counts[i];
+    const uint32_t nf = fluid_count(c), nb = boundary_count(c);
+    KSum<Real> rho, sgk, drho;
+    KSum3<Real> gpi;
+    rho.add(xi.w * K.W0);
+    for (uint32_t k = 0; k < nf; ++k) {
+        const uint32_t j = nbr[(size_t)k * stride + i];
+        const Vec4<Real> xj = ld4<Real>(pos + j);
+        const Vec4<Real> vj = ld4<Real>(vel + j);
+        Real w, gx, gy, gz;
+        K.W_gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, w, gx, gy, gz);
+        rho.add(xj.w * w);
+        const Real px = xj.w * gx, py = xj.w * gy, pz = xj.w * gz;
+        sgk.add(px * px + py * py + pz * pz);
+        gpi.add(px, py, pz);
+        drho.add((vi.x - vj.x) * px + (vi.y - vj.y) * py + (vi.z - vj.z) * pz);
+    }
+    for (uint32_t k = nf; k < nf + nb; ++k) {
+        const uint32_t j = nbr[(size_t)k * stride + i];
+        const Vec4<Real> xj = ld4<Real>(bpos + j);
+        Real bvx = 0, bvy = 0, bvz = 0;
+        if (p.boundary_moving) {
+            const Vec4<Real> vb = ld4<Real>(bvel + j);
+            bvx = vb.x; bvy = vb.y; bvz = vb.z;
+        }
+        Real w, gx, gy, gz;
+        K.W_gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, w, gx, gy, gz);
+        rho.add(xj.w * w);
+        const Real px = xj.w * gx, py = xj.w * gy, pz = xj.w * gz;
+        sgk.add(px * px + py * py + pz * pz);
+        gpi.add(px, py, pz);
+        drho.add((vi.x - bvx) * px + (vi.y - bvy) * py + (vi.z - bvz) * pz);
+    }
+    const Real gx = gpi.x.value(), gy = gpi.y.value(), gz = gpi.z.value();
+    const Real sg = sgk.value() + (gx * gx + gy * gy + gz * gz);
+    const Real alpha = -p.inv_h / rmax<Real>(sg, Real(kEps));
+    const Real density = rho.value();
+    ds->factor[i] = alpha;
+    ds->density[i] = density;
+    uint32_t num = nf;
+    if (num < kMinNeighborsForDivergence) num += nb;
+    const Real dadv = (num < kMinNeighborsForDivergence) ? Real(0) : rmax<Real>(drho.value(), Real(0));
+    ds->densityAdv[i] = dadv;
+    if (kFeatures) {
+        float* f = ds->features + (size_t)i * 4;
+        f[0] = (float)((density - p.density0) / p.density0);
+        f[1] = (float)(dadv * alpha);
+        f[2] = (float)(nf + nb) * (1.0f / 64.0f);
+        f[3] = 0.0f;
+    }
+}
+
+// Divergence warm start (divergenceSolveParticle<true>, only where the source is positive,
+// DFSPH_core_cuda.cu:509-512): v_i += h * sum (kv_i + kv_j) m_j grad W_ij + h kv_i sum psi_b grad W_ib.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) divergence_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
+                                                                        uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!(ds->densityAdv[i] > Real(0))) return;
+    const StepParams<Real>& p = ds->p;
+    const Vec4<Real>* __restrict__ pos = ds->pos;
+    const Vec4<Real>* __restrict__ bpos = ds->bpos;
+    const Real* __restrict__ kv = ds->kappaV;
+    const uint32_t* __restrict__ nbr = ds->nbr;
+    const uint32_t stride = p.nbr_stride;
+    const Cubic<Real> K = p.kern;
+    const Real ki = kv[i];
+    const Vec4<Real> xi = pos[i];
+    const uint32_t c = ds->counts[i];
+    const uint32_t nf = fluid_count(c), nb = boundary_count(c);
+    KSum3<Real> acc;
+    for (uint32_t k = 0; k < nf; ++k) {
+        const uint32_t j = nbr[(size_t)k * stride + i];
+        const Real ks = ki + kv[j];
+        if (above_eps(ks)) {
+            const Vec4<Real> xj = ld4<Real>(pos + j);
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+            const Real s = ks * xj.w;
+            acc.add(s * gx, s * gy, s * gz);
+        }
+    }
+    if (above_eps(ki)) {
+        for (uint32_t k = nf; k < nf + nb; ++k) {
+            const uint32_t j = nbr[(size_t)k * stride + i];
+            const Vec4<Real> xj = ld4<Real>(bpos + j);
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+            const Real s = ki * xj.w;
+            acc.add(s * gx, s * gy, s * gz);
+        }
+    }
+    Vec4<Real> v = ds->vel[i];
+    v.x += acc.x.value() * p.h;
+    v.y += acc.y.value() * p.h;
+    v.z += acc.z.value() * p.h;
+    ds->vel[i] = v;
+}
+
+// Divergence residual (computeDensityChange): rho_dot_i = max(sum m_j (v_i - v_j).grad W_ij +
+// sum psi_b (v_i - v_b).grad W_ib, 0), 0 with fewer than 20 neighbours. Also stores
+// k_i = rho_dot_i * alpha_i for the next Jacobi pass. kInit additionally zeroes kappa_v
+// (DFSPH_divergence_init_kernel, :631-633).
+template <class Real, bool kInit>
+__global__ void __launch_bounds__(kBlock) divergence_residual_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+                                                                     double eta, int min_it, int max_it,
+                                                                     cudaGraphConditionalHandle handle,
+                                                                     bool use_handle) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double contrib = 0.0;
+    if (i < n) {
+        const StepParams<Real>& p = ds->p;
+        if (kInit) ds->kappaV[i] = Real(0);
+        const uint32_t c = ds->counts[i];
+        const uint32_t nf = fluid_count(c), nb = boundary_count(c);
+        uint32_t num = nf;
+        if (num < kMinNeighborsForDivergence) num += nb;
+        Real dadv = Real(0);
+        if (num >= kMinNeighborsForDivergence) {
+            const Vec4<Real>* __restrict__ pos = ds->pos;
+            const Vec4<Real>* __restrict__ vel = ds->vel;
+            const Vec4<Real>* __restrict__ bpos = ds->bpos;
+            const Vec4<Real>* __restrict__ bvel = ds->bvel;
+            const uint32_t* __restrict__ nbr = ds->nbr;
+            const uint32_t stride = p.nbr_stride;
+            const Cubic<Real> K = p.kern;
+            const Vec4<Real> xi = pos[i];
+            const Vec4<Real> vi = vel[i];
+            KSum<Real> s;
+            for (uint32_t k = 0; k < nf; ++k) {
+                const uint32_t j = nbr[(size_t)k * stride + i];
+                const Vec4<Real> xj = ld4<Real>(pos + j);
+                const Vec4<Real> vj = ld4<Real>(vel + j);
+                Real gx, gy, gz;
+                K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+                s.add(xj.w * ((vi.x - vj.x) * gx + (vi.y - vj.y) * gy + (vi.z - vj.z) * gz));
+            }
+            for (uint32_t k = nf; k < nf + nb; ++k) {
+                const uint32_t j = nbr[(size_t)k * stride + i];
+                const Vec4<Real> xj = ld4<Real>(bpos + j);
+                Real bvx = 0, bvy = 0, bvz = 0;
+                if (p.boundary_moving) {
+                    const Vec4<Real> vb = ld4<Real>(bvel + j);
+                    bvx = vb.x; bvy = vb.y; bvz = vb.z;
+                }
+                Real gx, gy, gz;
+                K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+                s.add(xj.w * ((vi.x - bvx) * gx + (vi.y - bvy) * gy + (vi.z - bvz) * gz));
+            }
+            dadv = rmax<Real>(s.value(), Real(0));
+        }
+        ds->densityAdv[i] = dadv;
+        ds->kcoef[i] = dadv * ds->factor[i];
+        contrib = (double)dadv;
+    }
+    reduce_and_decide<kInit ? 1 : 0>(contrib, ds->partials, ds->ctl + 0, n, eta, min_it, max_it, handle, use_handle);
+}
+
+// Divergence Jacobi iteration (divergenceSolveParticle<false>): k_i = rho_dot_i alpha_i,
+// kappa_v_i += k_i, v_i += h * [sum (k_i + k_j) m_j grad W_ij + k_i sum psi_b grad W_ib].
+template <class Real>
+__global__ void __launch_bounds__(kBlock) divergence_jacobi_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+                                                                   cudaGraphConditionalHandle handle, bool use_handle) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // Inside a graph while-loop the condition is cleared here and only set again by the last block
+    // of the residual pass that follows: a loop can end early but can never spin without bound.
+    if (use_handle && i == 0) cudaGraphSetConditional(handle, 0u);
+    if (i >= n) return;
+    const StepParams<Real>& p = ds->p;
+    const Vec4<Real>* __restrict__ pos = ds->pos;
+    const Vec4<Real>* __restrict__ bpos = ds->bpos;
+    const Real* __restrict__ kc = ds->kcoef;
+    const uint32_t* __restrict__ nbr = ds->nbr;
+    const uint32_t stride = p.nbr_stride;
+    const Cubic<Real> K = p.kern;
+    const Real ki = kc[i];
+    ds->kappaV[i] += ki;
+    const Vec4<Real> xi = pos[i];
+    const uint32_t c = ds->counts[i];
+    const uint32_t nf = fluid_count(c), nb = boundary_count(c);
+    KSum3<Real> acc;
+    for (uint32_t k = 0; k < nf; ++k) {
+        const uint32_t j = nbr[(size_t)k * stride + i];
+        const Real ks = ki + kc[j];
+        if (above_eps(ks)) {
+            const Vec4<Real> xj = ld4<Real>(pos + j);
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+            const Real s = ks * xj.w;
+            acc.add(s * gx, s * gy, s * gz);
+        }
+    }
+    if (above_eps(ki)) {
+        for (uint32_t k = nf; k < nf + nb; ++k) {
+            const uint32_t j = nbr[(size_t)k * stride + i];
+            const Vec4<Real> xj = ld4<Real>(bpos + j);
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+            const Real s = ki * xj.w;
+            acc.add(s * gx, s * gy, s * gz);
+        }
+    }
+    Vec4<Real> v = ds->vel[i];
+    v.x += acc.x.value() * p.h;
+    v.y += acc.y.value() * p.h;
+    v.z += acc.z.value() * p.h;
+    ds->vel[i] = v;
+}
+
+// XSPH viscosity + gravity: a_i = g - sum (inv_h * nu * m_j / rho_j) (v_i - v_j) W_ij over fluid
+// neighbours. With kCfl the block maximum of |v + a h|^2 is stored for the CFL time step.
+template <class Real, bool kCfl>
+__global__ void __launch_bounds__(kBlock) viscosity_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float vmag = 0.0f;
+    if (i < n) {
+        const StepParams<Real>& p = ds->p;
+        const Vec4<Real>* __restrict__ pos = ds->pos;
+        const Vec4<Real>* __restrict__ vel = ds->vel;
+        const Real* __restrict__ rho = ds->density;
+        const uint32_t* __restrict__ nbr = ds->nbr;
+        const uint32_t stride = p.nbr_stride;
+        const Cubic<Real> K = p.kern;
+        const Vec4<Real> xi = pos[i];
+        const Vec4<Real> vi = vel[i];
+        const uint32_t nf = fluid_count(ds->counts[i]);
+        const Real cvis = p.inv_h * p.viscosity;
+        KSum3<Real> a;
+        for (uint32_t k = 0; k < nf; ++k) {
+            const uint32_t j = nbr[(size_t)k * stride + i];
+            const Vec4<Real> xj = ld4<Real>(pos + j);
+            const Vec4<Real> vj = ld4<Real>(vel + j);
+            const Real w = K.W(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
+            const Real s = cvis * (xj.w / rho[j]);
+            a.add(-(s * (vi.x - vj.x)) * w, -(s * (vi.y - vj.y)) * w, -(s * (vi.z - vj.z)) * w);
+        }
+        Vec4<Real> out;
+        out.x = p.gx + a.x.value();
+        out.y = p.gy + a.y.value();
+        out.z = p.gz + a.z.value();
+        out.w = Real(0);
+        ds->acc[i] = out;
+        if (kCfl) {
+            const Real ux = vi.x + out.x * p.h, uy = vi.y + out.y * p.h, uz = vi.z + out.z * p.h;
+            vmag = (float)(ux * ux + uy * uy + uz * uz);
+        }
+    }
+    if (kCfl) {
+        __shared__ float wmax[kWarpsPerBlock];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vmag = fmaxf(vmag, __shfl_down_sync(0xFFFFFFFFu, vmag, o));
+        if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = vmag;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float m = 0.0f;
+            for (int w = 0; w < kWarpsPerBlock; ++w) m = fmaxf(m, wmax[w]);
+            ds->cfl_partials[blockIdx.x] = m;
+        }
+    }
+}
+
+// Maximum of the CFL partials into ctl[2].sum (one block).
+template <class Real>
+__global__ void __launch_bounds__(kBlock) cfl_reduce_kernel(const DevState<Real>* __restrict__ ds, uint32_t n_blocks) {
+    float m = 0.0f;
+    for (uint32_t b = threadIdx.x; b < n_blocks; b += blockDim.x) m = fmaxf(m, ds->cfl_partials[b]);
+    __shared__ float wmax[kWarpsPerBlock];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float r = 0.0f;
+        for (int w = 0; w < kWarpsPerBlock; ++w) r = fmaxf(r, wmax[w]);
+        ds->ctl[2].sum = (double)r;
+    }
+}
+
+// v_i += h a_i (DFSPH_update_vel_kernel); the kappa warm-start scaling of that kernel is applied
+// on the fly by the pressure warm start, which is the only reader of the scaled value.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) update_vel_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Real h = ds->p.h;
+    Vec4<Real> v = ds->vel[i];
+    const Vec4<Real> a = ds->acc[i];
+    v.x += h * a.x;
+    v.y += h * a.y;
+    v.z += h * a.z;
+    ds->vel[i] = v;
+    ds->kappa[i] = rmax<Real>(ds->kappa[i] * ds->p.h_ratio_to_past2, Real(-0.5));
+}
+
+// Pressure warm start (pressureSolveParticle<true>) fused with the velocity update: with
+// kFusedVel the particle first applies v_i += h a_i and uses kappa scaled by (h/h_future)^2 and
+// clamped at -0.5 (update_vel, :3061-3065), computed for the neighbours on the fly.
+template <class Real, bool kFusedVel>
+__global__ void __launch_bounds__(kBlock) pressure_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
+                                                                      uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const StepParams<Real>& p = ds->p;
+    const Vec4<Real>* __restrict__ pos = ds->pos;
+    const Vec4<Real>* __restrict__ bpos = ds->bpos;
+    const Real* __restrict__ kap = ds->kappa;
+    const uint32_t* __restrict__ nbr = ds->nbr;
+    const uint32_t stride = p.nbr_stride;
+    const Cubic<Real> K = p.kern;
+    const Real r2 = p.h_ratio_to_past2;
+    const Real ki = kFusedVel ? rmax<Real>(kap[i] * r2, Real(-0.5)) : kap[i];
+    const Vec4<Real> xi = pos[i];
+    const uint32_t c = ds->counts[i];
+    const uint32_t nf = fluid_count(c), nb = boundary_count(c);
+    KSum3<Real> acc;
+    for (uint32_t k = 0; k < nf; ++k) {
+        const uint32_t j = nbr[(size_t)k * stride + i];
+        const Real kj = kFusedVel ? rmax<Real>(kap[j] * r2, Real(-0.5)) : kap[j];
+        const Real ks = ki + kj;
+        if (above_eps(ks)) {
+            const Vec4<Real> xj = ld4<Real>(pos + j);
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+            const Real s = ks * xj.w;
+            acc.add(s * gx, s * gy, s * gz);
+        }
+    }
+    if (above_eps(ki)) {
+        for (uint32_t k = nf; k < nf + nb; ++k) {
+            const uint32_t j = nbr[(size_t)k * stride + i];
+            const Vec4<Real> xj = ld4<Real>(bpos + j);
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+            const Real s = ki * xj.w;
+            acc.add(s * gx, s * gy, s * gz);
+        }
+    }
+    Vec4<Real> v = ds->vel[i];
+    if (kFusedVel) {
+        const Vec4<Real> a = ds->acc[i];
+        v.x += p.h * a.x;
+        v.y += p.h * a.y;
+        v.z += p.h * a.z;
+    }
+    v.x += acc.x.value() * p.h_future;
+    v.y += acc.y.value() * p.h_future;
+    v.z += acc.z.value() * p.h_future;
+    ds->vel[i] = v;
+}
+
+// Density residual (computeDensityAdv): rho_adv_i = max(rho_i + h_f * [sum m_j (v_i - v_j).grad W_ij
+// + sum psi_b (v_i - v_b).grad W_ib] - rho0, 0); kappa_i += rho_adv_i alpha_i; k_i = rho_adv_i alpha_i.
+// kInit first scales alpha by 1/h_future and zeroes kappa (DFSPH_pressure_init_kernel, :1230-1238).
+template <class Real, bool kInit>
+__global__ void __launch_bounds__(kBlock) pressure_residual_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+                                                                   double eta, int min_it, int max_it,
+                                                                   cudaGraphConditionalHandle handle,
+                                                                   bool use_handle) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double contrib = 0.0;
+    if (i < n) {
+        const StepParams<Real>& p = ds->p;
+        Real alpha = ds->factor[i];
+        Real kap = Real(0);
+        if (kInit) {
+            alpha *= p.inv_h_future;
+            ds->factor[i] = alpha;
+        } else {
+            kap = ds->kappa[i];
+        }
+        const Vec4<Real>* __restrict__ pos = ds->pos;
+        const Vec4<Real>* __restrict__ vel = ds->vel;
+        const Vec4<Real>* __restrict__ bpos = ds->bpos;
+        const Vec4<Real>* __restrict__ bvel = ds->bvel;
+        const uint32_t* __restrict__ nbr = ds->nbr;
+        const uint32_t stride = p.nbr_stride;
+        const Cubic<Real> K = p.kern;
+        const Vec4<Real> xi = pos[i];
+        const Vec4<Real> vi = vel[i];
+        const uint32_t c = ds->counts[i];
+        const uint32_t nf = fluid_count(c), nb = boundary_count(c);
+        KSum<Real> s;
+        for (uint32_t k = 0; k < nf; ++k) {
+            const uint32_t j = nbr[(size_t)k * stride + i];
+            const Vec4<Real> xj = ld4<Real>(pos + j);
+            const Vec4<Real> vj = ld4<Real>(vel + j);
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+            s.add(xj.w * ((vi.x - vj.x) * gx + (vi.y - vj.y) * gy + (vi.z - vj.z) * gz));
+        }
+        for (uint32_t k = nf; k < nf + nb; ++k) {
+            const uint32_t j = nbr[(size_t)k * stride + i];
+            const Vec4<Real> xj = ld4<Real>(bpos + j);
+            Real bvx = 0, bvy = 0, bvz = 0;
+            if (p.boundary_moving) {
+                const Vec4<Real> vb = ld4<Real>(bvel + j);
+                bvx = vb.x; bvy = vb.y; bvz = vb.z;
+            }
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+            s.add(xj.w * ((vi.x - bvx) * gx + (vi.y - bvy) * gy + (vi.z - bvz) * gz));
+        }
+        const Real dadv = rmax<Real>(ds->density[i] + p.h_future * s.value() - p.density0, Real(0));
+        const Real kc = dadv * alpha;
+        ds->densityAdv[i] = dadv;
+        ds->kcoef[i] = kc;
+        ds->kappa[i] = kap + kc;
+        contrib = (double)dadv;
+    }
+    reduce_and_decide<kInit ? 1 : 0>(contrib, ds->partials, ds->ctl + 1, n, eta, min_it, max_it, handle, use_handle);
+}
+
+// Pressure Jacobi iteration (pressureSolveParticle<false>): v_i += h_f * [sum (k_i + k_j) m_j grad W_ij
+// + k_i sum psi_b grad W_ib] with k = rho_adv * alpha.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) pressure_jacobi_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+                                                                 cudaGraphConditionalHandle handle, bool use_handle) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (use_handle && i == 0) cudaGraphSetConditional(handle, 0u);  // see divergence_jacobi_kernel
+    if (i >= n) return;
+    const StepParams<Real>& p = ds->p;
+    const Vec4<Real>* __restrict__ pos = ds->pos;
+    const Vec4<Real>* __restrict__ bpos = ds->bpos;
+    const Real* __restrict__ kc = ds->kcoef;
+    const uint32_t* __restrict__ nbr = ds->nbr;
+    const uint32_t stride = p.nbr_stride;
+    const Cubic<Real> K = p.kern;
+    const Real ki = kc[i];
+    const Vec4<Real> xi = pos[i];
+    const uint32_t c = ds->counts[i];
+    const uint32_t nf = fluid_count(c), nb = boundary_count(c);
+    KSum3<Real> acc;
+    for (uint32_t k = 0; k < nf; ++k) {
+        const uint32_t j = nbr[(size_t)k * stride + i];
+        const Real ks = ki + kc[j];
+        if (above_eps(ks)) {
+            const Vec4<Real> xj = ld4<Real>(pos + j);
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+            const Real s = ks * xj.w;
+            acc.add(s * gx, s * gy, s * gz);
+        }
+    }
+    if (above_eps(ki)) {
+        for (uint32_t k = nf; k < nf + nb; ++k) {
+            const uint32_t j = nbr[(size_t)k * stride + i];
+            const Vec4<Real> xj = ld4<Real>(bpos + j);
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
+            const Real s = ki * xj.w;
+            acc.add(s * gx, s * gy, s * gz);
+        }
+    }
+    Vec4<Real> v = ds->vel[i];
+    v.x += acc.x.value() * p.h_future;
+    v.y += acc.y.value() * p.h_future;
+    v.z += acc.z.value() * p.h_future;
+    ds->vel[i] = v;
+}
+
+// x_i += h v_i (DFSPH_update_pos_kernel with border damping and wave cancelling off).
+template <class Real>
+__global__ void __launch_bounds__(kBlock) update_pos_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Real h = ds->p.h;
+    Vec4<Real> x = ds->pos[i];
+    const Vec4<Real> v = ds->vel[i];
+    x.x += h * v.x;
+    x.y += h * v.y;
+    x.z += h * v.z;
+    ds->pos[i] = x;
+}
+
+}  // namespace
+
+template <class Real> void launch_density_alpha(const DevState<Real>* d, uint32_t n, bool warm_v, cudaStream_t s) {
+    if (!n) return;
+    if (warm_v) density_alpha_kernel<Real, true, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    else density_alpha_kernel<Real, false, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+}
+template <class Real> void launch_divergence_warm_jacobi(const DevState<Real>* d, uint32_t n, cudaStream_t s) {
+    if (n) divergence_warm_jacobi_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n);
+}
+template <class Real>
+void launch_divergence_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
+                                cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s) {
+    const unsigned g = grid_for(n ? n : 1);
+    if (init) divergence_residual_kernel<Real, true><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
+    else divergence_residual_kernel<Real, false><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
+}
+template <class Real>
+void launch_divergence_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
+                              cudaStream_t s) {
+    if (n) divergence_jacobi_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
+}
+template <class Real> void launch_viscosity(const DevState<Real>* d, uint32_t n, bool cfl, cudaStream_t s) {
+    if (!n) return;
+    if (cfl) viscosity_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    else viscosity_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+}
+template <class Real> void launch_update_vel(const DevState<Real>* d, uint32_t n, cudaStream_t s) {
+    if (n) update_vel_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n);
+}
+template <class Real>
+void launch_pressure_warm_jacobi(const DevState<Real>* d, uint32_t n, bool fused_vel, cudaStream_t s) {
+    if (!n) return;
+    if (fused_vel) pressure_warm_jacobi_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    else pressure_warm_jacobi_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+}
+template <class Real>
+void launch_pressure_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
+                              cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s) {
+    const unsigned g = grid_for(n ? n : 1);
+    if (init) pressure_residual_kernel<Real, true><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
+    else pressure_residual_kernel<Real, false><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
+}
+template <class Real>
+void launch_pressure_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
+                            cudaStream_t s) {
+    if (n) pressure_jacobi_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
+}
+template <class Real> void launch_update_pos(const DevState<Real>* d, uint32_t n, cudaStream_t s) {
+    if (n) update_pos_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n);
+}
+template <class Real> void launch_cfl_reduce(const DevState<Real>* d, uint32_t n_blocks, cudaStream_t s) {
+    cfl_reduce_kernel<Real><<<1, kBlock, 0, s>>>(d, n_blocks);
+}
+
+#define DFSPH_INSTANTIATE_SOLVER(R)                                                                                  \
+    template void launch_density_alpha<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                        \
+    template void launch_divergence_warm_jacobi<R>(const DevState<R>*, uint32_t, cudaStream_t);                     \
+    template void launch_divergence_residual<R>(const DevState<R>*, uint32_t, bool, double, int, int,               \
+                                                cudaGraphConditionalHandle, bool, cudaStream_t);                     \
+    template void launch_divergence_jacobi<R>(const DevState<R>*, uint32_t, cudaGraphConditionalHandle, bool,       \
+                                              cudaStream_t);                                                         \
+    template void launch_viscosity<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                            \
+    template void launch_update_vel<R>(const DevState<R>*, uint32_t, cudaStream_t);                                 \
+    template void launch_pressure_warm_jacobi<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                 \
+    template void launch_pressure_residual<R>(const DevState<R>*, uint32_t, bool, double, int, int,                 \
+                                              cudaGraphConditionalHandle, bool, cudaStream_t);                       \
+    template void launch_pressure_jacobi<R>(const DevState<R>*, uint32_t, cudaGraphConditionalHandle, bool,         \
+                                            cudaStream_t);                                                           \
+    template void launch_update_pos<R>(const DevState<R>*, uint32_t, cudaStream_t);                                 \
+    template void launch_cfl_reduce<R>(const DevState<R>*, uint32_t, cudaStream_t);
+
+DFSPH_INSTANTIATE_SOLVER(float)
+DFSPH_INSTANTIATE_SOLVER(double)
+
+}  // namespace dfsph

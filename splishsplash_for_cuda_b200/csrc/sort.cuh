@@ -1,0 +1,20 @@
+// sort.cuh — interface of the in-house stable radix sort (sort.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dfsph {
+
+struct SortBuffers {
+    uint32_t* keys_a = nullptr;
+    uint32_t* vals_a = nullptr;
+    uint32_t* keys_b = nullptr;
+    uint32_t* vals_b = nullptr;
+    uint32_t* workspace = nullptr;  // radix_sort_workspace_words(n_max, 4) words
+};
+
+size_t radix_sort_workspace_words(uint32_t n_max, int passes);
+void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, cudaStream_t stream,
+                      uint32_t* status_word, uint64_t* launch_counter, uint32_t** keys_out, uint32_t** vals_out);
+
+}  // namespace dfsph

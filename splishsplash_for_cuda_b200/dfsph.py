@@ -1,0 +1,279 @@
+"""Host-side mirror of the reference solver interface for the DFSPH time step.
+
+`DFSPHCUDA` has the public surface of SPH::DFSPHCUDA (SPlisHSPlasH/DFSPH/DFSPH_CUDA.h:26-154) and of
+its base SPH::TimeStep (SPlisHSPlasH/TimeStep.h:79-103): step(), reset(), the iteration counters and
+the max error / max iteration / CFL / divergence-solver setters, all backed by the sm_100a kernels
+of libdfsph_b200.so through the C ABI. `DFSPHCData` exposes the state accessors the reference
+callers use (fluid particle count, dynamic data readback, dt history).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from .scene import Scene
+
+_f32p = C.POINTER(C.c_float)
+
+
+def _fptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_f32p)
+
+
+def scene_struct(scene: Scene, precision: int = 32, device: int = 0, use_graphs: bool = True,
+                 neighbor_capacity: int = 96, fluid_capacity: int | None = None,
+                 boundary_capacity: int | None = None) -> _capi.DfsphScene:
+    lib = _capi.load()
+    s = _capi.DfsphScene()
+    _capi.check(lib, None, lib.dfsph_scene_defaults(C.byref(s)))
+    cfg = scene.config
+    s.particle_radius = cfg.particleRadius
+    s.density0 = cfg.density0
+    s.viscosity = cfg.viscosity
+    for a in range(3):
+        s.gravitation[a] = cfg.gravitation[a]
+    s.time_step = cfg.timeStepSize
+    s.max_iterations = cfg.maxIterations
+    s.max_error = cfg.maxError
+    s.max_iterations_v = cfg.maxIterationsV
+    s.max_error_v = cfg.maxErrorV
+    s.enable_divergence_solver = 1 if cfg.enableDivergenceSolver else 0
+    s.cfl_method = cfg.cflMethod
+    s.cfl_factor = cfg.cflFactor
+    s.cfl_max_time_step = cfg.cflMaxTimeStepSize
+    s.fluid_capacity = max(1, fluid_capacity if fluid_capacity is not None else scene.n_fluid)
+    s.boundary_capacity = max(1, boundary_capacity if boundary_capacity is not None else scene.n_boundary)
+    s.neighbor_capacity = neighbor_capacity
+    s.precision = precision
+    s.device = device
+    s.use_graphs = 1 if use_graphs else 0
+    return s
+
+
+class DFSPHData:
+    """State accessors of one solver context (the parts of SPH::DFSPHCData callers read)."""
+
+    def __init__(self, owner: "DFSPHCUDA"):
+        self._o = owner
+
+    def getFluidParticlesCount(self) -> int:
+        n = C.c_uint32()
+        self._o._call(self._o._lib.dfsph_num_fluid(self._o._ctx, C.byref(n)))
+        return int(n.value)
+
+    def readDynamicData(self):
+        """Positions and velocities in particle-id order (DFSPHCData::readDynamicData)."""
+        return self._o.positions(), self._o.velocities()
+
+    @property
+    def h(self) -> float:
+        return self._o.get_param("h")
+
+    @property
+    def h_future(self) -> float:
+        return self._o.get_param("h_future")
+
+    @property
+    def h_past(self) -> float:
+        return self._o.get_param("h_past")
+
+    def updateTimeStep(self, h_future: float) -> None:
+        self._o._call(self._o._lib.dfsph_update_time_step(self._o._ctx, float(h_future)))
+
+    def onSimulationStepEnd(self) -> None:
+        self._o._call(self._o._lib.dfsph_on_step_end(self._o._ctx))
+
+
+class DFSPHCUDA:
+    """Drop-in for SPH::DFSPHCUDA over one scene (fluid + static box walls)."""
+
+    def __init__(self, scene: Scene, precision: int = 32, device: int = 0, use_graphs: bool = True,
+                 neighbor_capacity: int = 96, boundary_psi: np.ndarray | None = None,
+                 fluid_capacity: int | None = None):
+        self._lib = _capi.load()
+        self.scene = scene
+        self.precision = precision
+        self._struct = scene_struct(scene, precision, device, use_graphs, neighbor_capacity, fluid_capacity)
+        ctx = C.c_void_p()
+        code = self._lib.dfsph_create(C.byref(self._struct), C.byref(ctx))
+        if code != _capi.DFSPH_OK:
+            raise _capi.DfsphError(code, self._lib.dfsph_last_error(None).decode())
+        self._ctx = ctx
+        self._psi = None if boundary_psi is None else np.ascontiguousarray(boundary_psi, dtype=np.float32)
+        self.m_iterations = 0
+        self.m_iterationsV = 0
+        self.last_stats = None
+        self.m_data = DFSPHData(self)
+        self.reset()
+
+    # ---- lifetime ------------------------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            self._lib.dfsph_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _call(self, code: int) -> None:
+        _capi.check(self._lib, self._ctx, code)
+
+    def reset(self) -> None:
+        """DFSPHCUDA::reset (DFSPH_CUDA.cpp:796-817): reload boundary and fluid from the scene."""
+        b = np.ascontiguousarray(self.scene.boundary, dtype=np.float32)
+        self._call(self._lib.dfsph_set_boundary(self._ctx, _fptr(b), _fptr(self._psi), b.shape[0]))
+        x = np.ascontiguousarray(self.scene.fluid, dtype=np.float32)
+        v = None if self.scene.fluid_velocity is None else np.ascontiguousarray(self.scene.fluid_velocity,
+                                                                                 dtype=np.float32)
+        self._call(self._lib.dfsph_upload_fluid(self._ctx, _fptr(x), _fptr(v), None, x.shape[0]))
+        self.m_iterations = 0
+        self.m_iterationsV = 0
+
+    # ---- the time step ----------------------------------------------------------------------------
+    def step(self) -> _capi.DfsphStepStats:
+        st = _capi.DfsphStepStats()
+        self._call(self._lib.dfsph_step(self._ctx, C.byref(st)))
+        self.m_iterations = st.iterations
+        self.m_iterationsV = st.iterations_v
+        self.last_stats = st
+        return st
+
+    # piecewise host functions of DFSPH_core_cuda.h
+    def neighbors_search(self) -> None:
+        self._call(self._lib.dfsph_neighbors_search(self._ctx, 1))
+
+    def divergence_solve(self, max_iter: int | None = None, max_error: float | None = None) -> int:
+        it = C.c_int32()
+        self._call(self._lib.dfsph_divergence_solve(
+            self._ctx, self.getMaxIterationsV() if max_iter is None else max_iter,
+            self.getMaxErrorV() if max_error is None else max_error, C.byref(it)))
+        return int(it.value)
+
+    def external_forces(self) -> None:
+        self._call(self._lib.dfsph_external_forces(self._ctx))
+
+    def update_time_step(self, h_future: float) -> None:
+        self._call(self._lib.dfsph_update_time_step(self._ctx, h_future))
+
+    def update_vel(self) -> None:
+        self._call(self._lib.dfsph_update_vel(self._ctx))
+
+    def pressure_solve(self, max_iter: int | None = None, max_error: float | None = None) -> int:
+        it = C.c_int32()
+        self._call(self._lib.dfsph_pressure_solve(
+            self._ctx, self.getMaxIterations() if max_iter is None else max_iter,
+            self.getMaxError() if max_error is None else max_error, C.byref(it)))
+        return int(it.value)
+
+    def update_pos(self) -> None:
+        self._call(self._lib.dfsph_update_pos(self._ctx))
+
+    def on_step_end(self) -> None:
+        self._call(self._lib.dfsph_on_step_end(self._ctx))
+
+    # ---- TimeStep accessors ------------------------------------------------------------------------
+    def getIterationCount(self) -> int:
+        return self.m_iterations
+
+    def getIterationCountV(self) -> int:
+        return self.m_iterationsV
+
+    def get_param(self, key: str) -> float:
+        v = C.c_double()
+        self._call(self._lib.dfsph_get_param(self._ctx, key.encode(), C.byref(v)))
+        return float(v.value)
+
+    def set_param(self, key: str, value: float) -> None:
+        self._call(self._lib.dfsph_set_param(self._ctx, key.encode(), float(value)))
+
+    def getMaxError(self) -> float: return self.get_param("max_error")
+    def setMaxError(self, v: float) -> None: self.set_param("max_error", v)
+    def getMaxIterations(self) -> int: return int(self.get_param("max_iterations"))
+    def setMaxIterations(self, v: int) -> None: self.set_param("max_iterations", v)
+    def getMaxErrorV(self) -> float: return self.get_param("max_error_v")
+    def setMaxErrorV(self, v: float) -> None: self.set_param("max_error_v", v)
+    def getMaxIterationsV(self) -> int: return int(self.get_param("max_iterations_v"))
+    def setMaxIterationsV(self, v: int) -> None: self.set_param("max_iterations_v", v)
+    def getCflMethod(self) -> int: return int(self.get_param("cfl_method"))
+    def setCflMethod(self, v: int) -> None: self.set_param("cfl_method", v)
+    def getCflFactor(self) -> float: return self.get_param("cfl_factor")
+    def setCflFactor(self, v: float) -> None: self.set_param("cfl_factor", v)
+    def getCflMaxTimeStepSize(self) -> float: return self.get_param("cfl_max_time_step")
+    def setCflMaxTimeStepSize(self, v: float) -> None: self.set_param("cfl_max_time_step", v)
+    def getEnableDivergenceSolver(self) -> bool: return bool(self.get_param("enable_divergence_solver"))
+    def setEnableDivergenceSolver(self, v: bool) -> None: self.set_param("enable_divergence_solver", 1 if v else 0)
+    def getViscosity(self) -> float: return self.get_param("viscosity")
+    def setViscosity(self, v: float) -> None: self.set_param("viscosity", v)
+
+    # ---- state readback ----------------------------------------------------------------------------
+    def num_fluid(self) -> int:
+        return self.m_data.getFluidParticlesCount()
+
+    def field(self, name: str, dtype=np.float32, order: int = _capi.ORDER_ID) -> np.ndarray:
+        fid, comps = _capi.FIELDS[name]
+        n = int(self.get_param("num_boundary")) if name.startswith("boundary") else self.num_fluid()
+        if name in ("id", "neighbor_counts"):
+            out = np.empty(n * comps, dtype=np.uint32)
+            code = _capi.DTYPE_U32
+        else:
+            out = np.empty(n * comps, dtype=dtype)
+            code = _capi.DTYPE_F64 if np.dtype(dtype) == np.float64 else _capi.DTYPE_F32
+        self._call(self._lib.dfsph_download(self._ctx, fid, code, out.ctypes.data_as(C.c_void_p), out.size, order))
+        return out.reshape(n, comps) if comps > 1 else out
+
+    def positions(self, dtype=np.float32) -> np.ndarray:
+        return self.field("position", dtype)
+
+    def velocities(self, dtype=np.float32) -> np.ndarray:
+        return self.field("velocity", dtype)
+
+    def neighbors(self, row: int | None = None):
+        """(counts[N, 2], lists[N, row]) in particle-id space: fluid ids first, then boundary indices."""
+        n = self.num_fluid()
+        row = row or self._struct.neighbor_capacity
+        counts = np.zeros((n, 2), dtype=np.uint32)
+        lists = np.zeros((n, row), dtype=np.uint32)
+        self._call(self._lib.dfsph_get_neighbors(self._ctx, counts.ctypes.data_as(_capi._U),
+                                                 lists.ctypes.data_as(_capi._U), row))
+        return counts, lists
+
+    def status(self, clear: bool = False) -> int:
+        s = C.c_uint32()
+        self._call(self._lib.dfsph_status(self._ctx, C.byref(s), 1 if clear else 0))
+        return int(s.value)
+
+    def launch_count(self) -> int:
+        v = C.c_uint64()
+        self._call(self._lib.dfsph_launch_count(self._ctx, C.byref(v)))
+        return int(v.value)
+
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        self._call(self._lib.dfsph_get_stream(self._ctx, C.byref(p)))
+        return int(p.value or 0)
+
+    def time_kernel(self, name: str, reps: int = 5) -> float:
+        """Mean device ms per launch of one kernel of the step (modifies the state)."""
+        ms = C.c_double()
+        self._call(self._lib.dfsph_time_kernel(self._ctx, _capi.KERNELS.index(name), reps, C.byref(ms)))
+        return float(ms.value)
+
+    def synchronize(self) -> None:
+        self._call(self._lib.dfsph_synchronize(self._ctx))
+
+    def update_fluid(self, positions: np.ndarray, velocities: np.ndarray | None = None) -> None:
+        x = np.ascontiguousarray(positions, dtype=np.float32)
+        v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32)
+        self._call(self._lib.dfsph_update_fluid(self._ctx, _fptr(x), _fptr(v)))
+
+    def move_boundary(self, positions: np.ndarray, velocities: np.ndarray | None = None) -> None:
+        x = np.ascontiguousarray(positions, dtype=np.float32)
+        v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32)
+        self._call(self._lib.dfsph_move_boundary(self._ctx, _fptr(x), _fptr(v)))

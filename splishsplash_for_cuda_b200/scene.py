@@ -1,0 +1,267 @@
+"""Scenes for the DFSPH time step: the reference JSON scene format and seeded synthetic scenes.
+
+The JSON reader follows the keys of the reference SceneLoader (Utilities/SceneLoader.cpp:39-320):
+"Configuration" (timeStepSize, particleRadius, density0, viscosity, gravitation, cflMethod,
+cflFactor, cflMaxTimeStepSize, maxIterations, maxError, maxIterationsV, maxErrorV,
+enableDivergenceSolver), "FluidBlocks" (start/end boxes filled like DemoBase::createFluidBlocks,
+Demos/Common/DemoBase.cpp:539-603) and "RigidBodies". Wall bodies are sampled as a single-layer
+lattice of spacing 2r on the box surface instead of the Poisson-disk sampling of an OBJ mesh
+(Demos/StaticBoundaryDemo/main.cpp:466-468); a body whose "geometryFile" names a unit box is the
+box [translation - scale/2, translation + scale/2]. Extension keys (ignored by the reference):
+"seed" and "jitter" (uniform jitter amplitude as a fraction of r).
+"""
+from __future__ import annotations
+
+import json
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+_LANES = 1024
+
+
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    x = x + np.uint64(0x9E3779B97F4A7C15)
+    z = x
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def _rotl(x: np.ndarray, k: int) -> np.ndarray:
+    return (x << np.uint64(k)) | (x >> np.uint64(64 - k))
+
+
+def xoshiro_uniform(n: int, seed: int) -> np.ndarray:
+    """n doubles in [0, 1) from 1024 interleaved xoshiro256** streams (Blackman & Vigna); stream l
+    is seeded by four splitmix64 steps from seed * 1024 + l, and value i comes from stream i % 1024.
+    Vectorised over the streams, deterministic on every machine."""
+    if n <= 0:
+        return np.zeros(0, dtype=np.float64)
+    with np.errstate(over="ignore"):
+        x = np.uint64(seed & 0xFFFFFFFFFFFF) * np.uint64(_LANES) + np.arange(_LANES, dtype=np.uint64)
+        st = []
+        for _ in range(4):
+            x = x + np.uint64(0x9E3779B97F4A7C15)
+            st.append(_splitmix64(x))
+        s0, s1, s2, s3 = st
+        rounds = (n + _LANES - 1) // _LANES
+        out = np.empty((rounds, _LANES), dtype=np.uint64)
+        for r in range(rounds):
+            out[r] = _rotl(s1 * np.uint64(5), 7) * np.uint64(9)
+            t = s1 << np.uint64(17)
+            s2 = s2 ^ s0
+            s3 = s3 ^ s1
+            s1 = s1 ^ s2
+            s0 = s0 ^ s3
+            s2 = s2 ^ t
+            s3 = _rotl(s3, 45)
+    return (out.ravel()[:n] >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def _jitter(n: int, amplitude: float, seed: int) -> np.ndarray:
+    """(n, 3) array of U(-amplitude, +amplitude) per coordinate."""
+    if amplitude == 0.0 or n == 0:
+        return np.zeros((n, 3), dtype=np.float64)
+    u = xoshiro_uniform(3 * n, seed)
+    return ((2.0 * u - 1.0) * amplitude).reshape(n, 3)
+
+
+def fluid_block(box_min, box_max, radius: float) -> np.ndarray:
+    """Dense-mode fluid block of DemoBase::createFluidBlocks: steps = round(extent / 2r) - 1 per axis,
+    first particle at min + 2r, x outer, y middle, z inner loop order. Returns (n, 3) float64."""
+    diam = 2.0 * radius
+    mn = np.asarray(box_min, dtype=np.float64)
+    mx = np.asarray(box_max, dtype=np.float64)
+    steps = [int(round((mx[a] - mn[a]) / diam)) - 1 for a in range(3)]
+    steps = [max(s, 0) for s in steps]
+    start = mn + diam
+    i, j, k = np.meshgrid(np.arange(steps[0]), np.arange(steps[1]), np.arange(steps[2]), indexing="ij")
+    pts = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1).astype(np.float64) * diam + start
+    return pts
+
+
+def lattice_block(counts, radius: float, origin=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """counts[0] x counts[1] x counts[2] lattice of spacing 2r whose first particle sits at origin + 2r
+    (the fluid block [origin, origin + (counts + 1) 2r] of createFluidBlocks)."""
+    diam = 2.0 * radius
+    mn = np.asarray(origin, dtype=np.float64)
+    mx = mn + (np.asarray(counts, dtype=np.float64) + 1.0) * diam
+    return fluid_block(mn, mx, radius)
+
+
+def box_wall(box_min, box_max, spacing: float) -> np.ndarray:
+    """Single-layer surface lattice of an axis-aligned box: every lattice point of spacing `spacing`
+    from box_min to box_max with at least one coordinate on a face. Returns (B, 3) float64."""
+    mn = np.asarray(box_min, dtype=np.float64)
+    mx = np.asarray(box_max, dtype=np.float64)
+    cnt = [int(round((mx[a] - mn[a]) / spacing)) + 1 for a in range(3)]
+    pts = []
+    for a in range(3):
+        b, c = [d for d in range(3) if d != a]
+        for side in (0, cnt[a] - 1):
+            # faces perpendicular to axis a; skip points already produced by earlier axes' faces
+            ib = np.arange(cnt[b])
+            ic = np.arange(cnt[c])
+            if b < a:
+                ib = ib[1:-1]
+            if c < a:
+                ic = ic[1:-1]
+            gb, gc = np.meshgrid(ib, ic, indexing="ij")
+            face = np.empty((gb.size, 3), dtype=np.float64)
+            face[:, a] = side
+            face[:, b] = gb.ravel()
+            face[:, c] = gc.ravel()
+            pts.append(face)
+    idx = np.concatenate(pts, axis=0)
+    return idx * spacing + mn
+
+
+@dataclass
+class Configuration:
+    """The "Configuration" block of a reference scene (defaults of SPH::TimeStep, TimeStep.cpp:23-44)."""
+
+    timeStepSize: float = 0.001
+    particleRadius: float = 0.025
+    density0: float = 1000.0
+    viscosity: float = 0.01
+    gravitation: tuple = (0.0, -9.81, 0.0)
+    cflMethod: int = 0
+    cflFactor: float = 0.5
+    cflMaxTimeStepSize: float = 0.01
+    maxIterations: int = 100
+    maxError: float = 0.01
+    maxIterationsV: int = 100
+    maxErrorV: float = 0.1
+    enableDivergenceSolver: bool = True
+    simulationMethod: int = 6
+
+
+@dataclass
+class Scene:
+    config: Configuration
+    fluid: np.ndarray  # (N, 3) float32
+    boundary: np.ndarray  # (B, 3) float32
+    fluid_velocity: np.ndarray | None = None
+    name: str = "scene"
+    box_min: tuple | None = None
+    box_max: tuple | None = None
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_fluid(self) -> int:
+        return int(self.fluid.shape[0])
+
+    @property
+    def n_boundary(self) -> int:
+        return int(self.boundary.shape[0])
+
+
+def _readvec(v, default):
+    return tuple(float(x) for x in v) if v is not None else default
+
+
+def load_scene(path: str | Path) -> Scene:
+    """Reads a reference-format JSON scene."""
+    path = Path(path)
+    j = json.loads(path.read_text())
+    c = j.get("Configuration", {})
+    cfg = Configuration()
+    for key in ("timeStepSize", "particleRadius", "density0", "viscosity", "cflFactor", "cflMaxTimeStepSize",
+                "maxError", "maxErrorV"):
+        if key in c:
+            setattr(cfg, key, float(c[key]))
+    for key in ("cflMethod", "maxIterations", "maxIterationsV", "simulationMethod"):
+        if key in c:
+            setattr(cfg, key, int(c[key]))
+    if "enableDivergenceSolver" in c:
+        cfg.enableDivergenceSolver = bool(c["enableDivergenceSolver"])
+    cfg.gravitation = _readvec(c.get("gravitation"), cfg.gravitation)
+    r = cfg.particleRadius
+    seed = int(c.get("seed", 1))
+    jitter = float(c.get("jitter", 0.0))
+    fluid = []
+    for fb in j.get("FluidBlocks", []):
+        start = np.asarray(_readvec(fb.get("start"), (0.0, 0.0, 0.0)))
+        end = np.asarray(_readvec(fb.get("end"), (1.0, 1.0, 1.0)))
+        scale = np.asarray(_readvec(fb.get("scale"), (1.0, 1.0, 1.0)))
+        trans = np.asarray(_readvec(fb.get("translation"), (0.0, 0.0, 0.0)))
+        mn = np.minimum(start, end) * scale + trans
+        mx = np.maximum(start, end) * scale + trans
+        if int(fb.get("denseMode", 0)) != 0:
+            raise ValueError("only denseMode 0 fluid blocks are supported")
+        fluid.append(fluid_block(mn, mx, r))
+    fluid_arr = np.concatenate(fluid, axis=0) if fluid else np.zeros((0, 3))
+    fluid_arr = fluid_arr + _jitter(fluid_arr.shape[0], jitter * r, seed)
+    walls = []
+    bmin = bmax = None
+    for rb in j.get("RigidBodies", []):
+        scale = np.asarray(_readvec(rb.get("scale"), (1.0, 1.0, 1.0)))
+        trans = np.asarray(_readvec(rb.get("translation"), (0.0, 0.0, 0.0)))
+        geo = str(rb.get("geometryFile", ""))
+        if "box" not in geo.lower():
+            raise ValueError(f"only box rigid bodies are supported, got {geo!r}")
+        mn = trans - 0.5 * scale
+        mx = trans + 0.5 * scale
+        walls.append(box_wall(mn, mx, 2.0 * r))
+        bmin = mn if bmin is None else np.minimum(bmin, mn)
+        bmax = mx if bmax is None else np.maximum(bmax, mx)
+    wall_arr = np.concatenate(walls, axis=0) if walls else np.zeros((0, 3))
+    return Scene(
+        config=cfg,
+        fluid=fluid_arr.astype(np.float32),
+        boundary=wall_arr.astype(np.float32),
+        name=path.stem,
+        box_min=tuple(bmin) if bmin is not None else None,
+        box_max=tuple(bmax) if bmax is not None else None,
+    )
+
+
+# Synthetic scenes of the five benchmark configurations. Every box dimension is twice the stated
+# one because a lattice of spacing 2r with the stated particle counts does not fit the stated boxes
+# (e.g. 30 x 2r = 1.5 m of fluid for a 1 m box); N, r, spacing, h = 4r, mass, dt and tolerances are
+# kept as stated.
+SYNTHETIC = {
+    1: dict(name="dam_break_27k", counts=(30, 30, 30), radius=0.025, box=(2.0, 2.0, 2.0), seed=1,
+            max_error=0.01, cfl_max=0.005),
+    2: dict(name="dam_break_250k", counts=(63, 63, 63), radius=0.0125, box=(4.0, 2.0, 2.0), seed=2,
+            max_error=0.01, cfl_max=0.005),
+    3: dict(name="sloshing_1m", counts=(100, 100, 100), radius=0.01, box=(8.0, 4.0, 4.0), seed=3,
+            max_error=0.01, cfl_max=0.005),
+    4: dict(name="column_2m", counts=(100, 200, 100), radius=0.008, box=(6.0, 6.0, 6.0), seed=4,
+            max_error=0.005, cfl_max=0.008),
+    5: dict(name="wave_tank_4m", counts=(400, 100, 100), radius=0.01, box=(16.0, 4.0, 4.0), seed=5,
+            max_error=0.01, cfl_max=0.005),
+}
+
+
+def synthetic_scene(config: int, jitter: float = 0.01, time_step: float | None = None, cfl: bool = False,
+                    counts=None) -> Scene:
+    """Seeded synthetic scene of benchmark configuration `config` (1..5). counts overrides the lattice
+    size (same radius, box and seed) for reduced test cases."""
+    spec = SYNTHETIC[config]
+    r = spec["radius"]
+    cnt = tuple(counts) if counts is not None else spec["counts"]
+    fluid = lattice_block(cnt, r)
+    fluid = fluid + _jitter(fluid.shape[0], jitter * r, spec["seed"])
+    box = np.asarray(spec["box"], dtype=np.float64)
+    walls = box_wall((0.0, 0.0, 0.0), box, 2.0 * r)
+    cfg = Configuration(
+        timeStepSize=time_step if time_step is not None else spec["cfl_max"],
+        particleRadius=r,
+        density0=1000.0,
+        viscosity=0.01,
+        gravitation=(0.0, -9.81, 0.0),
+        cflMethod=1 if cfl else 0,
+        cflFactor=0.4,
+        cflMaxTimeStepSize=spec["cfl_max"],
+        maxIterations=100,
+        maxError=spec["max_error"],
+        maxIterationsV=100,
+        maxErrorV=0.1,
+        enableDivergenceSolver=True,
+    )
+    return Scene(config=cfg, fluid=fluid.astype(np.float32), boundary=walls.astype(np.float32),
+                 name=spec["name"] if counts is None else f"{spec['name']}_{'x'.join(map(str, cnt))}",
+                 box_min=(0.0, 0.0, 0.0), box_max=tuple(box), meta=dict(config=config, seed=spec["seed"]))

@@ -1,0 +1,29 @@
+"""Comparison helpers for per-particle fields."""
+import numpy as np
+
+
+def field_error(got: np.ndarray, ref: np.ndarray, floor_frac: float = 1e-3) -> float:
+    """Max over particles of |got - ref| / max(|ref|, floor), with floor = floor_frac * max|ref| over
+    the field: a relative error that does not blow up where the field itself is ~0 (e.g. kappa of
+    particles that need no pressure)."""
+    got = np.asarray(got, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    scale = np.max(np.abs(ref)) if ref.size else 0.0
+    floor = max(floor_frac * scale, 1e-300)
+    den = np.maximum(np.abs(ref), floor)
+    return float(np.max(np.abs(got - ref) / den)) if ref.size else 0.0
+
+
+def assert_field(name: str, got, ref, rtol: float, floor_frac: float = 1e-3):
+    err = field_error(got, ref, floor_frac)
+    assert err <= rtol, f"{name}: max relative error {err:.3e} > {rtol:.1e}"
+    return err
+
+
+def neighbor_sets(counts: np.ndarray, lists: np.ndarray):
+    """List of (fluid_set, boundary_set) frozensets per particle."""
+    out = []
+    for i in range(counts.shape[0]):
+        nf, nb = int(counts[i, 0]), int(counts[i, 1])
+        out.append((frozenset(lists[i, :nf].tolist()), frozenset(lists[i, nf:nf + nb].tolist())))
+    return out

@@ -1,0 +1,71 @@
+"""CPU tests of the C ABI boundary: the shared library loads, exports every symbol include/dfsph_c.h
+declares, the ctypes layouts match the header, and without a GPU the product fails loudly."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from splishsplash_for_cuda_b200 import _capi
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "dfsph_c.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dfsph_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_bound_symbols():
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    assert set(syms) == set(_capi.SIGNATURES), set(syms) ^ set(_capi.SIGNATURES)
+
+
+def test_library_exports_every_declared_symbol(cuda_lib):
+    for name in declared_symbols():
+        assert hasattr(cuda_lib, name), name
+
+
+def test_scene_defaults_match_reference_timestep(cuda_lib):
+    s = _capi.DfsphScene()
+    assert cuda_lib.dfsph_scene_defaults(C.byref(s)) == 0
+    # SPH::TimeStep::TimeStep (TimeStep.cpp:23-44)
+    assert s.max_iterations == 100 and s.max_iterations_v == 100
+    assert s.max_error == pytest.approx(0.01) and s.max_error_v == pytest.approx(0.1)
+    assert s.cfl_factor == pytest.approx(0.5) and s.cfl_max_time_step == pytest.approx(0.01)
+    assert s.precision == 32 and s.neighbor_capacity >= 90
+
+
+def test_struct_sizes_match_header(cuda_lib):
+    # dfsph_scene: 3 doubles, gravitation[3], dt, then mixed fields; checked against the C layout
+    # by compiling a probe would need a compiler at test time, so check the ctypes size is the
+    # natural C size of the declared field sequence.
+    assert C.sizeof(_capi.DfsphScene) % 8 == 0
+    assert C.sizeof(_capi.DfsphStepStats) == 56
+
+
+def test_create_without_gpu_fails_loudly(cuda_lib):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    s = _capi.DfsphScene()
+    cuda_lib.dfsph_scene_defaults(C.byref(s))
+    ctx = C.c_void_p()
+    code = cuda_lib.dfsph_create(C.byref(s), C.byref(ctx))
+    assert code in (_capi.DFSPH_E_CUDA, _capi.DFSPH_E_NOMEM)
+    assert not ctx.value
+    assert cuda_lib.dfsph_last_error(None)
+
+
+def test_invalid_arguments_rejected_before_cuda(cuda_lib):
+    s = _capi.DfsphScene()
+    cuda_lib.dfsph_scene_defaults(C.byref(s))
+    s.precision = 16
+    ctx = C.c_void_p()
+    assert cuda_lib.dfsph_create(C.byref(s), C.byref(ctx)) == _capi.DFSPH_E_INVALID
+    assert b"precision" in cuda_lib.dfsph_last_error(None)
+    assert cuda_lib.dfsph_step(None, None) == _capi.DFSPH_E_INVALID
+    assert cuda_lib.dfsph_destroy(None) == 0

@@ -1,0 +1,195 @@
+"""GPU parity tests: the sm_100a kernels, called through the C ABI, against the CPU oracle.
+
+Bars: neighbour sets bit-exact; one-step fields within 1e-5 relative of the FP64 oracle for the FP32
+build (relative error floored at 1e-3 of the field's max, see tests/_compare.py) and within 1e-9 for
+the FP64 build of the same kernels; identical iteration counts; bit-identical reruns."""
+import numpy as np
+import pytest
+
+from oracle import Oracle
+from splishsplash_for_cuda_b200 import _capi
+from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
+from splishsplash_for_cuda_b200.scene import synthetic_scene
+from tests._compare import assert_field, field_error, neighbor_sets
+
+pytestmark = pytest.mark.gpu
+
+FIELDS_ONE_STEP = ["density", "factor", "kappa", "kappa_v", "velocity", "position", "acceleration"]
+
+
+def _moving_scene(counts=(14, 14, 14), seed=7, vmax=0.5):
+    s = synthetic_scene(1, counts=counts)
+    rng = np.random.default_rng(seed)
+    s.fluid_velocity = rng.uniform(-vmax, vmax, size=s.fluid.shape).astype(np.float32)
+    return s
+
+
+@pytest.mark.parametrize("config,counts", [(1, (12, 12, 12)), (1, None), (2, (40, 30, 30)), (2, None)])
+def test_neighbor_sets_bit_exact(config, counts):
+    s = synthetic_scene(config, counts=counts)
+    d = DFSPHCUDA(s)
+    d.neighbors_search()
+    c, l = d.neighbors()
+    o = Oracle(s, 64)
+    co, lo = o.neighbors(row=l.shape[1])
+    assert d.status() & _capi.ST_NEIGHBOR_OVERFLOW == 0
+    assert np.array_equal(c, co)
+    assert neighbor_sets(c, l) == neighbor_sets(co, lo)
+
+
+def test_neighbor_sets_bit_exact_after_steps():
+    s = synthetic_scene(1, counts=(16, 16, 16), cfl=True)
+    d = DFSPHCUDA(s)
+    for _ in range(40):
+        d.step()
+    d.neighbors_search()
+    c, l = d.neighbors()
+    x = d.positions()
+    o = Oracle(s, 64)
+    o.set_positions(x.astype(np.float64))
+    co, lo = o.neighbors(row=l.shape[1])
+    assert np.array_equal(c, co)
+    assert neighbor_sets(c, l) == neighbor_sets(co, lo)
+
+
+def test_boundary_psi_matches_fp64_oracle():
+    s = synthetic_scene(1, counts=(8, 8, 8))
+    d = DFSPHCUDA(s)
+    o = Oracle(s, 64)
+    assert_field("psi", d.field("boundary_psi", np.float64), o.field("boundary_psi"), 1e-6)
+
+
+@pytest.mark.parametrize("scene_fn", [lambda: synthetic_scene(1, counts=(14, 14, 14)), _moving_scene,
+                                      lambda: synthetic_scene(1)])
+def test_one_step_fp32_matches_fp64_oracle(scene_fn):
+    s = scene_fn()
+    d = DFSPHCUDA(s)
+    o = Oracle(s, 64)
+    st = d.step()
+    ro = o.step()
+    assert st.iterations == ro["iterations"]
+    assert st.iterations_v == ro["iterations_v"]
+    assert st.density_error == pytest.approx(ro["density_error"], rel=1e-4, abs=1e-7)
+    for name in FIELDS_ONE_STEP:
+        assert_field(name, d.field(name, np.float64), o.field(name), 1e-5)
+
+
+def test_one_step_fp64_build_matches_fp64_oracle():
+    s = _moving_scene()
+    d = DFSPHCUDA(s, precision=64)
+    o = Oracle(s, 64)
+    st = d.step()
+    ro = o.step()
+    assert st.iterations == ro["iterations"] and st.iterations_v == ro["iterations_v"]
+    for name in FIELDS_ONE_STEP:
+        assert_field(name, d.field(name, np.float64), o.field(name), 1e-9)
+
+
+def test_ten_steps_lockstep_fields():
+    """Ten CFL steps: FP32 kernels vs FP64 oracle stay within 1e-4 (errors compound through the
+    warm starts) and take the same number of iterations."""
+    s = synthetic_scene(1, counts=(14, 14, 14), cfl=True)
+    d = DFSPHCUDA(s)
+    o = Oracle(s, 64)
+    for k in range(10):
+        st = d.step()
+        ro = o.step()
+        assert st.iterations == ro["iterations"], k
+        assert st.iterations_v == ro["iterations_v"], k
+    for name in ["position", "velocity", "density"]:
+        assert_field(name, d.field(name, np.float64), o.field(name), 1e-4)
+
+
+def test_rerun_bit_identical():
+    s = synthetic_scene(1, counts=(16, 16, 16), cfl=True)
+    a, b = DFSPHCUDA(s), DFSPHCUDA(s)
+    for _ in range(20):
+        a.step()
+        b.step()
+    assert np.array_equal(a.positions(), b.positions())
+    assert np.array_equal(a.velocities(), b.velocities())
+
+
+def test_graph_loop_equals_host_loop():
+    s = _moving_scene()
+    a, b = DFSPHCUDA(s, use_graphs=True), DFSPHCUDA(s, use_graphs=False)
+    for _ in range(5):
+        sa, sb = a.step(), b.step()
+        assert sa.iterations == sb.iterations and sa.iterations_v == sb.iterations_v
+    assert np.array_equal(a.positions(), b.positions())
+    assert np.array_equal(a.field("kappa"), b.field("kappa"))
+
+
+def test_piecewise_host_functions_equal_fused_step():
+    """The seven host functions of DFSPH_core_cuda.h called one by one give the fused step."""
+    s = _moving_scene()
+    a, b = DFSPHCUDA(s), DFSPHCUDA(s)
+    for _ in range(3):
+        a.step()
+        b.neighbors_search()
+        b.divergence_solve()
+        b.external_forces()
+        b.update_time_step(s.config.timeStepSize)
+        b.update_vel()
+        b.pressure_solve()
+        b.update_pos()
+        b.on_step_end()
+    assert np.array_equal(a.positions(), b.positions())
+    assert np.array_equal(a.velocities(), b.velocities())
+
+
+def test_cfl_time_step_matches_oracle():
+    s = _moving_scene(vmax=2.0)
+    s.config.cflMethod = 1
+    d = DFSPHCUDA(s)
+    o = Oracle(s, 64)
+    st = d.step()
+    o.step()
+    assert st.h_future == pytest.approx(o.scalar("h"), rel=1e-5)
+    assert st.h_future < s.config.cflMaxTimeStepSize
+
+
+def test_status_nonfinite_position_reported():
+    s = synthetic_scene(1, counts=(10, 10, 10))
+    s.fluid[5] = np.nan
+    d = DFSPHCUDA(s)
+    st = d.step()
+    assert st.status & _capi.ST_NONFINITE
+    x = d.positions()
+    finite = np.isfinite(x).all(axis=1)
+    assert finite.sum() == s.n_fluid - 1
+
+
+def test_status_neighbor_overflow_reported():
+    s = synthetic_scene(1, counts=(10, 10, 10))
+    d = DFSPHCUDA(s, neighbor_capacity=8)
+    st = d.step()
+    assert st.status & _capi.ST_NEIGHBOR_OVERFLOW
+    c, _ = d.neighbors(row=8)
+    assert c.sum(axis=1).max() <= 8
+
+
+def test_status_not_converged_reported():
+    s = synthetic_scene(1, counts=(14, 14, 14))
+    s.config.maxIterations = 2
+    s.config.maxError = 1e-9
+    d = DFSPHCUDA(s)
+    st = d.step()
+    assert st.iterations == 2
+    assert st.status & _capi.ST_PRESSURE_NOT_CONVERGED
+
+
+def test_field_download_orders_and_dtypes():
+    s = synthetic_scene(1, counts=(6, 7, 8))
+    d = DFSPHCUDA(s)
+    x32 = d.positions()
+    x64 = d.positions(np.float64)
+    assert np.array_equal(x32, s.fluid)
+    assert np.array_equal(x64, s.fluid.astype(np.float64))
+    d.step()
+    ids_sorted = d.field("id", order=_capi.ORDER_SORTED)
+    assert sorted(ids_sorted.tolist()) == list(range(s.n_fluid))
+    xs = d.field("position", order=_capi.ORDER_SORTED)
+    assert np.array_equal(xs, d.positions()[ids_sorted])
+    m = d.field("mass")
+    assert np.allclose(m, 0.8 * 1000 * (2 * s.config.particleRadius) ** 3)

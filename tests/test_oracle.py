@@ -1,0 +1,111 @@
+"""CPU tests of the oracle itself: kernel closed form, neighbour search (grid vs brute force), boundary
+psi, FP32 error budget, edge cases. No GPU."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import Oracle
+from oracle.oracle import kernel_values
+from splishsplash_for_cuda_b200.scene import synthetic_scene, Scene, Configuration, box_wall
+from tests._compare import field_error, neighbor_sets
+
+
+def cubic_closed_form(r, H):
+    """Cubic spline of SPH_kernels.h:42-94 in exact arithmetic (float64)."""
+    k = 8.0 / (math.pi * H ** 3)
+    l = 48.0 / (math.pi * H ** 3)
+    q = r / H
+    w = np.where(q <= 0.5, k * (6 * q ** 3 - 6 * q ** 2 + 1), np.where(q <= 1.0, k * 2 * (1 - q) ** 3, 0.0))
+    dw = np.where(q <= 0.5, l * q * (3 * q - 2) / H, np.where(q <= 1.0, -l * (1 - q) ** 2 / H, 0.0))
+    dw = np.where(r > 1e-6, dw, 0.0)
+    return w, dw
+
+
+@pytest.mark.parametrize("precision,rtol", [(64, 1e-12), (32, 2e-6)])
+def test_kernel_closed_form(oracle_lib, precision, rtol):
+    H = 0.1
+    r = np.linspace(0.0, 1.2 * H, 2001)
+    w, dw = kernel_values(H, r, precision)
+    we, dwe = cubic_closed_form(r, H)
+    scale_w, scale_dw = np.abs(we).max(), np.abs(dwe).max()
+    assert np.max(np.abs(w - we)) <= rtol * scale_w * 4
+    assert np.max(np.abs(dw - dwe)) <= rtol * scale_dw * 4
+    assert w[-1] == 0.0 and dw[-1] == 0.0
+    assert dw[0] == 0.0  # grad W = 0 at |r| <= 1e-6
+
+
+@pytest.mark.parametrize("counts,jitter", [((8, 8, 8), 0.01), ((12, 9, 7), 0.2), ((10, 10, 10), 0.0)])
+def test_grid_search_equals_brute_force(oracle_lib, counts, jitter):
+    s = synthetic_scene(1, counts=counts, jitter=jitter)
+    a = Oracle(s, 64)
+    b = Oracle(s, 64, brute_force=True)
+    ca, la = a.neighbors()
+    cb, lb = b.neighbors()
+    assert np.array_equal(ca, cb)
+    assert neighbor_sets(ca, la) == neighbor_sets(cb, lb)
+    # every stored fluid pair is symmetric
+    sets = neighbor_sets(ca, la)
+    for i, (f, _) in enumerate(sets):
+        for j in f:
+            assert i in sets[j][0]
+
+
+def test_boundary_psi_planar_lattice(oracle_lib):
+    """A flat single-layer lattice of spacing H/2: interior samples see W0 + 4 W(H/2) + 4 W(H/sqrt2)."""
+    r = 0.025
+    H = 4 * r
+    s = synthetic_scene(1, counts=(4, 4, 4))
+    o = Oracle(s, 64)
+    psi = o.field("boundary_psi")
+    k = 8 / (math.pi * H ** 3)
+    expected = 1000.0 / (k * (1 + 4 * 0.25 + 4 * 2 * (1 - math.sqrt(0.5)) ** 3))
+    assert np.isclose(np.median(psi), expected, rtol=1e-4)
+    assert psi.min() > 0 and psi.max() < 2 * expected
+
+
+def test_fp32_error_budget_one_step(oracle_lib):
+    s = synthetic_scene(1, counts=(14, 14, 14))
+    o64, o32 = Oracle(s, 64), Oracle(s, 32)
+    r64, r32 = o64.step(), o32.step()
+    assert r64["iterations"] == r32["iterations"]
+    assert r64["iterations_v"] == r32["iterations_v"]
+    for name, tol in [("density", 1e-6), ("factor", 1e-5), ("velocity", 1e-5), ("position", 1e-6), ("kappa", 1e-4)]:
+        err = field_error(o32.field(name), o64.field(name))
+        assert err < tol, (name, err)
+
+
+def test_dam_break_stays_bounded(oracle_lib):
+    """60 CFL steps of a small dam break: no particle leaves the box, density stays physical."""
+    s = synthetic_scene(1, counts=(10, 10, 10), cfl=True)
+    o = Oracle(s, 64)
+    for _ in range(60):
+        st = o.step()
+        assert not st["overflow"]
+    x = o.field("position")
+    assert x.min() > 0.0 and x.max() < 2.0
+    rho = o.field("density")
+    assert rho.max() < 1.2 * 1000.0
+    v = np.linalg.norm(o.field("velocity"), axis=1)
+    assert v.max() < 10.0
+
+
+def test_low_neighbour_particles_get_no_divergence_source(oracle_lib):
+    """A lone particle (< 20 neighbours) keeps rho_dot = 0 (DFSPH_core_cuda.cu:340-351)."""
+    cfg = Configuration(timeStepSize=0.001, particleRadius=0.025)
+    fluid = np.array([[1.0, 1.0, 1.0], [1.03, 1.0, 1.0]], dtype=np.float32)
+    s = Scene(config=cfg, fluid=fluid, boundary=box_wall((0, 0, 0), (2, 2, 2), 0.05).astype(np.float32),
+              fluid_velocity=np.array([[1.0, 0, 0], [-1.0, 0, 0]], dtype=np.float32))
+    o = Oracle(s, 64)
+    o.neighbors()
+    o.density_alpha(True)
+    assert np.all(o.field("density_adv") == 0.0)
+    rho = o.field("density")
+    assert np.all(rho > 0)
+
+
+def test_empty_fluid(oracle_lib):
+    s = synthetic_scene(1, counts=(0, 0, 0))
+    o = Oracle(s, 64)
+    st = o.step()
+    assert st["iterations"] == 0 and st["iterations_v"] == 0
