@@ -53,15 +53,18 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | None = None) -> Path:
-    """Compiles every csrc/*.cu for sm_100a and links libdfsph_b200.so. Returns the library path."""
-    OBJ.mkdir(exist_ok=True)
+def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | None = None,
+          out: Path | None = None, obj_dir: Path | None = None) -> Path:
+    """Compiles every csrc/*.cu for sm_100a and links libdfsph_b200.so (or `out`). Returns its path."""
+    OUT_ = Path(out) if out is not None else OUT
+    OBJ_ = Path(obj_dir) if obj_dir is not None else OBJ
+    OBJ_.mkdir(parents=True, exist_ok=True)
     headers = list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
     flags = NVCC_FLAGS + (extra_flags or [])
     jobs = []
     objs = []
     for src in sources():
-        obj = OBJ / (src.stem + ".o")
+        obj = OBJ_ / (src.stem + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
             jobs.append([nvcc(), *flags, "-c", str(src), "-o", str(obj)])
@@ -73,13 +76,13 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
                 sys.stderr.write(" ".join(cmd) + "\n" + res.stdout + res.stderr)
             if res.returncode != 0:
                 raise RuntimeError(f"nvcc failed for {cmd[-3]}")
-    if force or jobs or _stale(OUT, objs):
-        link = [nvcc(), *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-cudart", "static"]
+    if force or jobs or _stale(OUT_, objs):
+        link = [nvcc(), *ARCH, "-shared", "-o", str(OUT_), *map(str, objs), "-cudart", "static"]
         res = subprocess.run(link, capture_output=True, text=True)
         if res.returncode != 0:
             sys.stderr.write(" ".join(link) + "\n" + res.stdout + res.stderr)
             raise RuntimeError("link of libdfsph_b200.so failed")
-    return OUT
+    return OUT_
 
 
 def main() -> None:

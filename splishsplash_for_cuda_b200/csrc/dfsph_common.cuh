@@ -18,6 +18,11 @@ namespace dfsph {
 // array per block.
 constexpr int kBlock = 256;
 constexpr int kWarpsPerBlock = kBlock / 32;
+// Minimum resident blocks per SM asked of the compiler for the gather kernels (register cap).
+#ifndef DFSPH_MIN_BLOCKS
+#define DFSPH_MIN_BLOCKS 4
+#endif
+constexpr int kGatherMinBlocks = DFSPH_MIN_BLOCKS;
 
 // Divergence and pressure minimum iteration counts of the reference GPU loops
 // (DFSPH_core_cuda.cu:828 and :1378).
@@ -176,6 +181,37 @@ template <class Real> struct Cubic {
     static __device__ __forceinline__ float sqrt_(float v) { return sqrtf(v); }
     static __device__ __forceinline__ double sqrt_(double v) { return sqrt(v); }
 };
+
+// ---------------------------------------------------------------------------------------------
+// Batched neighbour visit. The neighbours [k0, k1) of particle i are taken kGatherBatch at a time:
+// first the batch's indices are loaded (coalesced rows of the interleaved table), then load(u, j)
+// issues every gather of the batch, then use(u) consumes them in list order. Keeping a batch of
+// independent gathers in flight per thread hides the latency that a one-at-a-time loop exposes,
+// while the summation order (and so every result bit) stays that of the plain loop. Slots past the
+// end of the list load `fallback` (an in-range index) and are not used.
+#ifndef DFSPH_GATHER_BATCH
+#define DFSPH_GATHER_BATCH 4
+#endif
+constexpr int kGatherBatch = DFSPH_GATHER_BATCH;
+constexpr uint32_t kNoNeighbor = 0xFFFFFFFFu;
+
+template <int B, class Load, class Use>
+__device__ __forceinline__ void visit_neighbors(const uint32_t* __restrict__ nbr, uint32_t stride, uint32_t i,
+                                                uint32_t k0, uint32_t k1, uint32_t fallback, Load&& load, Use&& use) {
+    for (uint32_t kb = k0; kb < k1; kb += B) {
+        uint32_t jj[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const uint32_t k = kb + u;
+            jj[u] = k < k1 ? __ldg(nbr + (size_t)k * stride + i) : kNoNeighbor;
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u) load(u, jj[u] == kNoNeighbor ? fallback : jj[u]);
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            if (kb + u < k1) use(u);
+    }
+}
 
 // ---------------------------------------------------------------------------------------------
 // Per-launch parameters (passed by value). The dt history mirrors DFSPHCData

@@ -90,16 +90,111 @@ __device__ void reduce_and_decide(double v, double* __restrict__ partials, LoopC
 }
 
 // ---------------------------------------------------------------------------------------------
+// Boundary neighbour data (position + psi, and the velocity when the boundary moves).
+template <class Real> struct BNbr {
+    Vec4<Real> x;
+    Real vx, vy, vz;
+};
+template <class Real>
+__device__ __forceinline__ void load_bnbr(BNbr<Real>& b, const Vec4<Real>* __restrict__ bpos,
+                                          const Vec4<Real>* __restrict__ bvel, uint32_t j, bool moving) {
+    b.x = ld4<Real>(bpos + j);
+    if (moving) {
+        const Vec4<Real> v = ld4<Real>(bvel + j);
+        b.vx = v.x; b.vy = v.y; b.vz = v.z;
+    } else {
+        b.vx = b.vy = b.vz = Real(0);
+    }
+}
+
+// Sum over fluid then boundary neighbours of m_j (v_i - v_j).grad W_ij, in list order.
+template <class Real>
+__device__ __forceinline__ Real velocity_divergence(const DevState<Real>* __restrict__ ds, const StepParams<Real>& p,
+                                                    uint32_t i, const Vec4<Real>& xi, const Vec4<Real>& vi,
+                                                    uint32_t nf, uint32_t nb) {
+    const Vec4<Real>* __restrict__ pos = ds->pos;
+    const Vec4<Real>* __restrict__ vel = ds->vel;
+    const uint32_t* __restrict__ nbr = ds->nbr;
+    const uint32_t stride = p.nbr_stride;
+    const Cubic<Real> K = p.kern;
+    KSum<Real> s;
+    Vec4<Real> xj[kGatherBatch], vj[kGatherBatch];
+    visit_neighbors<kGatherBatch>(
+        nbr, stride, i, 0, nf, i,
+        [&](int u, uint32_t j) {
+            xj[u] = ld4<Real>(pos + j);
+            vj[u] = ld4<Real>(vel + j);
+        },
+        [&](int u) {
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj[u].x, xi.y - xj[u].y, xi.z - xj[u].z, gx, gy, gz);
+            s.add(xj[u].w * ((vi.x - vj[u].x) * gx + (vi.y - vj[u].y) * gy + (vi.z - vj[u].z) * gz));
+        });
+    if (nb) {
+        const bool moving = p.boundary_moving != 0;
+        BNbr<Real> b[kGatherBatch];
+        visit_neighbors<kGatherBatch>(
+            nbr, stride, i, nf, nf + nb, 0u, [&](int u, uint32_t j) { load_bnbr(b[u], ds->bpos, ds->bvel, j, moving); },
+            [&](int u) {
+                Real gx, gy, gz;
+                K.gradW(xi.x - b[u].x.x, xi.y - b[u].x.y, xi.z - b[u].x.z, gx, gy, gz);
+                s.add(b[u].x.w * ((vi.x - b[u].vx) * gx + (vi.y - b[u].vy) * gy + (vi.z - b[u].vz) * gz));
+            });
+    }
+    return s.value();
+}
+
+// Jacobi velocity correction: sum over fluid neighbours of (k_i + k_j) m_j grad W_ij where
+// |k_i + k_j| > eps, plus (when |k_i| > eps) k_i sum over boundary neighbours of psi_b grad W_ib.
+// kof(j) returns k_j (a load, possibly transformed).
+template <class Real, class KOf>
+__device__ __forceinline__ void jacobi_sum(const DevState<Real>* __restrict__ ds, const StepParams<Real>& p, uint32_t i,
+                                           const Vec4<Real>& xi, Real ki, uint32_t nf, uint32_t nb, KOf&& kof,
+                                           KSum3<Real>& acc) {
+    const Vec4<Real>* __restrict__ pos = ds->pos;
+    const uint32_t* __restrict__ nbr = ds->nbr;
+    const uint32_t stride = p.nbr_stride;
+    const Cubic<Real> K = p.kern;
+    Vec4<Real> xj[kGatherBatch];
+    Real kj[kGatherBatch];
+    visit_neighbors<kGatherBatch>(
+        nbr, stride, i, 0, nf, i,
+        [&](int u, uint32_t j) {
+            xj[u] = ld4<Real>(pos + j);
+            kj[u] = kof(j);
+        },
+        [&](int u) {
+            const Real ks = ki + kj[u];
+            if (above_eps(ks)) {
+                Real gx, gy, gz;
+                K.gradW(xi.x - xj[u].x, xi.y - xj[u].y, xi.z - xj[u].z, gx, gy, gz);
+                const Real sc = ks * xj[u].w;
+                acc.add(sc * gx, sc * gy, sc * gz);
+            }
+        });
+    if (nb && above_eps(ki)) {
+        const Vec4<Real>* __restrict__ bpos = ds->bpos;
+        Vec4<Real> xb[kGatherBatch];
+        visit_neighbors<kGatherBatch>(
+            nbr, stride, i, nf, nf + nb, 0u, [&](int u, uint32_t j) { xb[u] = ld4<Real>(bpos + j); },
+            [&](int u) {
+                Real gx, gy, gz;
+                K.gradW(xi.x - xb[u].x, xi.y - xb[u].y, xi.z - xb[u].z, gx, gy, gz);
+                const Real sc = ki * xb[u].w;
+                acc.add(sc * gx, sc * gy, sc * gz);
+            });
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // density + alpha + divergence source (+ kappa_v warm-start scaling), one pass over the neighbours.
 template <class Real, bool kWarmV, bool kFeatures>
-__global__ void __launch_bounds__(kBlock) density_alpha_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
     const Vec4<Real>* __restrict__ pos = ds->pos;
     const Vec4<Real>* __restrict__ vel = ds->vel;
-    const Vec4<Real>* __restrict__ bpos = ds->bpos;
-    const Vec4<Real>* __restrict__ bvel = ds->bvel;
     const uint32_t* __restrict__ nbr = ds->nbr;
     const uint32_t stride = p.nbr_stride;
     const Cubic<Real> K = p.kern;
@@ -113,33 +208,31 @@ __global__ void __launch_bounds__(kBlock) density_alpha_kernel(const DevState<Re
     KSum<Real> rho, sgk, drho;
     KSum3<Real> gpi;
     rho.add(xi.w * K.W0);
-    for (uint32_t k = 0; k < nf; ++k) {
-        const uint32_t j = nbr[(size_t)k * stride + i];
-        const Vec4<Real> xj = ld4<Real>(pos + j);
-        const Vec4<Real> vj = ld4<Real>(vel + j);
+    auto accumulate = [&](const Vec4<Real>& xj, Real vx, Real vy, Real vz) {
         Real w, gx, gy, gz;
         K.W_gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, w, gx, gy, gz);
         rho.add(xj.w * w);
         const Real px = xj.w * gx, py = xj.w * gy, pz = xj.w * gz;
         sgk.add(px * px + py * py + pz * pz);
         gpi.add(px, py, pz);
-        drho.add((vi.x - vj.x) * px + (vi.y - vj.y) * py + (vi.z - vj.z) * pz);
+        drho.add((vi.x - vx) * px + (vi.y - vy) * py + (vi.z - vz) * pz);
+    };
+    {
+        Vec4<Real> xj[kGatherBatch], vj[kGatherBatch];
+        visit_neighbors<kGatherBatch>(
+            nbr, stride, i, 0, nf, i,
+            [&](int u, uint32_t j) {
+                xj[u] = ld4<Real>(pos + j);
+                vj[u] = ld4<Real>(vel + j);
+            },
+            [&](int u) { accumulate(xj[u], vj[u].x, vj[u].y, vj[u].z); });
     }
-    for (uint32_t k = nf; k < nf + nb; ++k) {
-        const uint32_t j = nbr[(size_t)k * stride + i];
-        const Vec4<Real> xj = ld4<Real>(bpos + j);
-        Real bvx = 0, bvy = 0, bvz = 0;
-        if (p.boundary_moving) {
-            const Vec4<Real> vb = ld4<Real>(bvel + j);
-            bvx = vb.x; bvy = vb.y; bvz = vb.z;
-        }
-        Real w, gx, gy, gz;
-        K.W_gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, w, gx, gy, gz);
-        rho.add(xj.w * w);
-        const Real px = xj.w * gx, py = xj.w * gy, pz = xj.w * gz;
-        sgk.add(px * px + py * py + pz * pz);
-        gpi.add(px, py, pz);
-        drho.add((vi.x - bvx) * px + (vi.y - bvy) * py + (vi.z - bvz) * pz);
+    if (nb) {
+        const bool moving = p.boundary_moving != 0;
+        BNbr<Real> b[kGatherBatch];
+        visit_neighbors<kGatherBatch>(
+            nbr, stride, i, nf, nf + nb, 0u, [&](int u, uint32_t j) { load_bnbr(b[u], ds->bpos, ds->bvel, j, moving); },
+            [&](int u) { accumulate(b[u].x, b[u].vx, b[u].vy, b[u].vz); });
     }
     const Real gx = gpi.x.value(), gy = gpi.y.value(), gz = gpi.z.value();
     const Real sg = sgk.value() + (gx * gx + gy * gy + gz * gz);
@@ -163,44 +256,18 @@ __global__ void __launch_bounds__(kBlock) density_alpha_kernel(const DevState<Re
 // Divergence warm start (divergenceSolveParticle<true>, only where the source is positive,
 // DFSPH_core_cuda.cu:509-512): v_i += h * sum (kv_i + kv_j) m_j grad W_ij + h kv_i sum psi_b grad W_ib.
 template <class Real>
-__global__ void __launch_bounds__(kBlock) divergence_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
                                                                         uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (!(ds->densityAdv[i] > Real(0))) return;
     const StepParams<Real>& p = ds->p;
-    const Vec4<Real>* __restrict__ pos = ds->pos;
-    const Vec4<Real>* __restrict__ bpos = ds->bpos;
     const Real* __restrict__ kv = ds->kappaV;
-    const uint32_t* __restrict__ nbr = ds->nbr;
-    const uint32_t stride = p.nbr_stride;
-    const Cubic<Real> K = p.kern;
     const Real ki = kv[i];
-    const Vec4<Real> xi = pos[i];
+    const Vec4<Real> xi = ds->pos[i];
     const uint32_t c = ds->counts[i];
-    const uint32_t nf = fluid_count(c), nb = boundary_count(c);
     KSum3<Real> acc;
-    for (uint32_t k = 0; k < nf; ++k) {
-        const uint32_t j = nbr[(size_t)k * stride + i];
-        const Real ks = ki + kv[j];
-        if (above_eps(ks)) {
-            const Vec4<Real> xj = ld4<Real>(pos + j);
-            Real gx, gy, gz;
-            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-            const Real s = ks * xj.w;
-            acc.add(s * gx, s * gy, s * gz);
-        }
-    }
-    if (above_eps(ki)) {
-        for (uint32_t k = nf; k < nf + nb; ++k) {
-            const uint32_t j = nbr[(size_t)k * stride + i];
-            const Vec4<Real> xj = ld4<Real>(bpos + j);
-            Real gx, gy, gz;
-            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-            const Real s = ki * xj.w;
-            acc.add(s * gx, s * gy, s * gz);
-        }
-    }
+    jacobi_sum<Real>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c), [&](uint32_t j) { return kv[j]; }, acc);
     Vec4<Real> v = ds->vel[i];
     v.x += acc.x.value() * p.h;
     v.y += acc.y.value() * p.h;
@@ -213,7 +280,7 @@ __global__ void __launch_bounds__(kBlock) divergence_warm_jacobi_kernel(const De
 // k_i = rho_dot_i * alpha_i for the next Jacobi pass. kInit additionally zeroes kappa_v
 // (DFSPH_divergence_init_kernel, :631-633).
 template <class Real, bool kInit>
-__global__ void __launch_bounds__(kBlock) divergence_residual_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_residual_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                      double eta, int min_it, int max_it,
                                                                      cudaGraphConditionalHandle handle,
                                                                      bool use_handle) {
@@ -228,37 +295,9 @@ __global__ void __launch_bounds__(kBlock) divergence_residual_kernel(const DevSt
         if (num < kMinNeighborsForDivergence) num += nb;
         Real dadv = Real(0);
         if (num >= kMinNeighborsForDivergence) {
-            const Vec4<Real>* __restrict__ pos = ds->pos;
-            const Vec4<Real>* __restrict__ vel = ds->vel;
-            const Vec4<Real>* __restrict__ bpos = ds->bpos;
-            const Vec4<Real>* __restrict__ bvel = ds->bvel;
-            const uint32_t* __restrict__ nbr = ds->nbr;
-            const uint32_t stride = p.nbr_stride;
-            const Cubic<Real> K = p.kern;
-            const Vec4<Real> xi = pos[i];
-            const Vec4<Real> vi = vel[i];
-            KSum<Real> s;
-            for (uint32_t k = 0; k < nf; ++k) {
-                const uint32_t j = nbr[(size_t)k * stride + i];
-                const Vec4<Real> xj = ld4<Real>(pos + j);
-                const Vec4<Real> vj = ld4<Real>(vel + j);
-                Real gx, gy, gz;
-                K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-                s.add(xj.w * ((vi.x - vj.x) * gx + (vi.y - vj.y) * gy + (vi.z - vj.z) * gz));
-            }
-            for (uint32_t k = nf; k < nf + nb; ++k) {
-                const uint32_t j = nbr[(size_t)k * stride + i];
-                const Vec4<Real> xj = ld4<Real>(bpos + j);
-                Real bvx = 0, bvy = 0, bvz = 0;
-                if (p.boundary_moving) {
-                    const Vec4<Real> vb = ld4<Real>(bvel + j);
-                    bvx = vb.x; bvy = vb.y; bvz = vb.z;
-                }
-                Real gx, gy, gz;
-                K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-                s.add(xj.w * ((vi.x - bvx) * gx + (vi.y - bvy) * gy + (vi.z - bvz) * gz));
-            }
-            dadv = rmax<Real>(s.value(), Real(0));
+            const Vec4<Real> xi = ds->pos[i];
+            const Vec4<Real> vi = ds->vel[i];
+            dadv = rmax<Real>(velocity_divergence<Real>(ds, p, i, xi, vi, nf, nb), Real(0));
         }
         ds->densityAdv[i] = dadv;
         ds->kcoef[i] = dadv * ds->factor[i];
@@ -270,7 +309,7 @@ __global__ void __launch_bounds__(kBlock) divergence_residual_kernel(const DevSt
 // Divergence Jacobi iteration (divergenceSolveParticle<false>): k_i = rho_dot_i alpha_i,
 // kappa_v_i += k_i, v_i += h * [sum (k_i + k_j) m_j grad W_ij + k_i sum psi_b grad W_ib].
 template <class Real>
-__global__ void __launch_bounds__(kBlock) divergence_jacobi_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_jacobi_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                    cudaGraphConditionalHandle handle, bool use_handle) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     // Inside a graph while-loop the condition is cleared here and only set again by the last block
@@ -278,39 +317,13 @@ __global__ void __launch_bounds__(kBlock) divergence_jacobi_kernel(const DevStat
     if (use_handle && i == 0) cudaGraphSetConditional(handle, 0u);
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
-    const Vec4<Real>* __restrict__ pos = ds->pos;
-    const Vec4<Real>* __restrict__ bpos = ds->bpos;
     const Real* __restrict__ kc = ds->kcoef;
-    const uint32_t* __restrict__ nbr = ds->nbr;
-    const uint32_t stride = p.nbr_stride;
-    const Cubic<Real> K = p.kern;
     const Real ki = kc[i];
     ds->kappaV[i] += ki;
-    const Vec4<Real> xi = pos[i];
+    const Vec4<Real> xi = ds->pos[i];
     const uint32_t c = ds->counts[i];
-    const uint32_t nf = fluid_count(c), nb = boundary_count(c);
     KSum3<Real> acc;
-    for (uint32_t k = 0; k < nf; ++k) {
-        const uint32_t j = nbr[(size_t)k * stride + i];
-        const Real ks = ki + kc[j];
-        if (above_eps(ks)) {
-            const Vec4<Real> xj = ld4<Real>(pos + j);
-            Real gx, gy, gz;
-            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-            const Real s = ks * xj.w;
-            acc.add(s * gx, s * gy, s * gz);
-        }
-    }
-    if (above_eps(ki)) {
-        for (uint32_t k = nf; k < nf + nb; ++k) {
-            const uint32_t j = nbr[(size_t)k * stride + i];
-            const Vec4<Real> xj = ld4<Real>(bpos + j);
-            Real gx, gy, gz;
-            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-            const Real s = ki * xj.w;
-            acc.add(s * gx, s * gy, s * gz);
-        }
-    }
+    jacobi_sum<Real>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c), [&](uint32_t j) { return kc[j]; }, acc);
     Vec4<Real> v = ds->vel[i];
     v.x += acc.x.value() * p.h;
     v.y += acc.y.value() * p.h;
@@ -321,7 +334,7 @@ __global__ void __launch_bounds__(kBlock) divergence_jacobi_kernel(const DevStat
 // XSPH viscosity + gravity: a_i = g - sum (inv_h * nu * m_j / rho_j) (v_i - v_j) W_ij over fluid
 // neighbours. With kCfl the block maximum of |v + a h|^2 is stored for the CFL time step.
 template <class Real, bool kCfl>
-__global__ void __launch_bounds__(kBlock) viscosity_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) viscosity_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     float vmag = 0.0f;
     if (i < n) {
@@ -329,22 +342,26 @@ __global__ void __launch_bounds__(kBlock) viscosity_kernel(const DevState<Real>*
         const Vec4<Real>* __restrict__ pos = ds->pos;
         const Vec4<Real>* __restrict__ vel = ds->vel;
         const Real* __restrict__ rho = ds->density;
-        const uint32_t* __restrict__ nbr = ds->nbr;
-        const uint32_t stride = p.nbr_stride;
         const Cubic<Real> K = p.kern;
         const Vec4<Real> xi = pos[i];
         const Vec4<Real> vi = vel[i];
         const uint32_t nf = fluid_count(ds->counts[i]);
         const Real cvis = p.inv_h * p.viscosity;
         KSum3<Real> a;
-        for (uint32_t k = 0; k < nf; ++k) {
-            const uint32_t j = nbr[(size_t)k * stride + i];
-            const Vec4<Real> xj = ld4<Real>(pos + j);
-            const Vec4<Real> vj = ld4<Real>(vel + j);
-            const Real w = K.W(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z);
-            const Real s = cvis * (xj.w / rho[j]);
-            a.add(-(s * (vi.x - vj.x)) * w, -(s * (vi.y - vj.y)) * w, -(s * (vi.z - vj.z)) * w);
-        }
+        Vec4<Real> xj[kGatherBatch], vj[kGatherBatch];
+        Real rj[kGatherBatch];
+        visit_neighbors<kGatherBatch>(
+            ds->nbr, p.nbr_stride, i, 0, nf, i,
+            [&](int u, uint32_t j) {
+                xj[u] = ld4<Real>(pos + j);
+                vj[u] = ld4<Real>(vel + j);
+                rj[u] = rho[j];
+            },
+            [&](int u) {
+                const Real w = K.W(xi.x - xj[u].x, xi.y - xj[u].y, xi.z - xj[u].z);
+                const Real sc = cvis * (xj[u].w / rj[u]);
+                a.add(-(sc * (vi.x - vj[u].x)) * w, -(sc * (vi.y - vj[u].y)) * w, -(sc * (vi.z - vj[u].z)) * w);
+            });
         Vec4<Real> out;
         out.x = p.gx + a.x.value();
         out.y = p.gy + a.y.value();
@@ -407,45 +424,19 @@ __global__ void __launch_bounds__(kBlock) update_vel_kernel(const DevState<Real>
 // kFusedVel the particle first applies v_i += h a_i and uses kappa scaled by (h/h_future)^2 and
 // clamped at -0.5 (update_vel, :3061-3065), computed for the neighbours on the fly.
 template <class Real, bool kFusedVel>
-__global__ void __launch_bounds__(kBlock) pressure_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
                                                                       uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
-    const Vec4<Real>* __restrict__ pos = ds->pos;
-    const Vec4<Real>* __restrict__ bpos = ds->bpos;
     const Real* __restrict__ kap = ds->kappa;
-    const uint32_t* __restrict__ nbr = ds->nbr;
-    const uint32_t stride = p.nbr_stride;
-    const Cubic<Real> K = p.kern;
     const Real r2 = p.h_ratio_to_past2;
     const Real ki = kFusedVel ? rmax<Real>(kap[i] * r2, Real(-0.5)) : kap[i];
-    const Vec4<Real> xi = pos[i];
+    const Vec4<Real> xi = ds->pos[i];
     const uint32_t c = ds->counts[i];
-    const uint32_t nf = fluid_count(c), nb = boundary_count(c);
     KSum3<Real> acc;
-    for (uint32_t k = 0; k < nf; ++k) {
-        const uint32_t j = nbr[(size_t)k * stride + i];
-        const Real kj = kFusedVel ? rmax<Real>(kap[j] * r2, Real(-0.5)) : kap[j];
-        const Real ks = ki + kj;
-        if (above_eps(ks)) {
-            const Vec4<Real> xj = ld4<Real>(pos + j);
-            Real gx, gy, gz;
-            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-            const Real s = ks * xj.w;
-            acc.add(s * gx, s * gy, s * gz);
-        }
-    }
-    if (above_eps(ki)) {
-        for (uint32_t k = nf; k < nf + nb; ++k) {
-            const uint32_t j = nbr[(size_t)k * stride + i];
-            const Vec4<Real> xj = ld4<Real>(bpos + j);
-            Real gx, gy, gz;
-            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-            const Real s = ki * xj.w;
-            acc.add(s * gx, s * gy, s * gz);
-        }
-    }
+    jacobi_sum<Real>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c),
+                     [&](uint32_t j) { return kFusedVel ? rmax<Real>(kap[j] * r2, Real(-0.5)) : kap[j]; }, acc);
     Vec4<Real> v = ds->vel[i];
     if (kFusedVel) {
         const Vec4<Real> a = ds->acc[i];
@@ -463,7 +454,7 @@ __global__ void __launch_bounds__(kBlock) pressure_warm_jacobi_kernel(const DevS
 // + sum psi_b (v_i - v_b).grad W_ib] - rho0, 0); kappa_i += rho_adv_i alpha_i; k_i = rho_adv_i alpha_i.
 // kInit first scales alpha by 1/h_future and zeroes kappa (DFSPH_pressure_init_kernel, :1230-1238).
 template <class Real, bool kInit>
-__global__ void __launch_bounds__(kBlock) pressure_residual_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_residual_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                    double eta, int min_it, int max_it,
                                                                    cudaGraphConditionalHandle handle,
                                                                    bool use_handle) {
@@ -479,39 +470,11 @@ __global__ void __launch_bounds__(kBlock) pressure_residual_kernel(const DevStat
         } else {
             kap = ds->kappa[i];
         }
-        const Vec4<Real>* __restrict__ pos = ds->pos;
-        const Vec4<Real>* __restrict__ vel = ds->vel;
-        const Vec4<Real>* __restrict__ bpos = ds->bpos;
-        const Vec4<Real>* __restrict__ bvel = ds->bvel;
-        const uint32_t* __restrict__ nbr = ds->nbr;
-        const uint32_t stride = p.nbr_stride;
-        const Cubic<Real> K = p.kern;
-        const Vec4<Real> xi = pos[i];
-        const Vec4<Real> vi = vel[i];
+        const Vec4<Real> xi = ds->pos[i];
+        const Vec4<Real> vi = ds->vel[i];
         const uint32_t c = ds->counts[i];
-        const uint32_t nf = fluid_count(c), nb = boundary_count(c);
-        KSum<Real> s;
-        for (uint32_t k = 0; k < nf; ++k) {
-            const uint32_t j = nbr[(size_t)k * stride + i];
-            const Vec4<Real> xj = ld4<Real>(pos + j);
-            const Vec4<Real> vj = ld4<Real>(vel + j);
-            Real gx, gy, gz;
-            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-            s.add(xj.w * ((vi.x - vj.x) * gx + (vi.y - vj.y) * gy + (vi.z - vj.z) * gz));
-        }
-        for (uint32_t k = nf; k < nf + nb; ++k) {
-            const uint32_t j = nbr[(size_t)k * stride + i];
-            const Vec4<Real> xj = ld4<Real>(bpos + j);
-            Real bvx = 0, bvy = 0, bvz = 0;
-            if (p.boundary_moving) {
-                const Vec4<Real> vb = ld4<Real>(bvel + j);
-                bvx = vb.x; bvy = vb.y; bvz = vb.z;
-            }
-            Real gx, gy, gz;
-            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-            s.add(xj.w * ((vi.x - bvx) * gx + (vi.y - bvy) * gy + (vi.z - bvz) * gz));
-        }
-        const Real dadv = rmax<Real>(ds->density[i] + p.h_future * s.value() - p.density0, Real(0));
+        const Real sdiv = velocity_divergence<Real>(ds, p, i, xi, vi, fluid_count(c), boundary_count(c));
+        const Real dadv = rmax<Real>(ds->density[i] + p.h_future * sdiv - p.density0, Real(0));
         const Real kc = dadv * alpha;
         ds->densityAdv[i] = dadv;
         ds->kcoef[i] = kc;
@@ -524,44 +487,18 @@ __global__ void __launch_bounds__(kBlock) pressure_residual_kernel(const DevStat
 // Pressure Jacobi iteration (pressureSolveParticle<false>): v_i += h_f * [sum (k_i + k_j) m_j grad W_ij
 // + k_i sum psi_b grad W_ib] with k = rho_adv * alpha.
 template <class Real>
-__global__ void __launch_bounds__(kBlock) pressure_jacobi_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_jacobi_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                  cudaGraphConditionalHandle handle, bool use_handle) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (use_handle && i == 0) cudaGraphSetConditional(handle, 0u);  // see divergence_jacobi_kernel
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
-    const Vec4<Real>* __restrict__ pos = ds->pos;
-    const Vec4<Real>* __restrict__ bpos = ds->bpos;
     const Real* __restrict__ kc = ds->kcoef;
-    const uint32_t* __restrict__ nbr = ds->nbr;
-    const uint32_t stride = p.nbr_stride;
-    const Cubic<Real> K = p.kern;
     const Real ki = kc[i];
-    const Vec4<Real> xi = pos[i];
+    const Vec4<Real> xi = ds->pos[i];
     const uint32_t c = ds->counts[i];
-    const uint32_t nf = fluid_count(c), nb = boundary_count(c);
     KSum3<Real> acc;
-    for (uint32_t k = 0; k < nf; ++k) {
-        const uint32_t j = nbr[(size_t)k * stride + i];
-        const Real ks = ki + kc[j];
-        if (above_eps(ks)) {
-            const Vec4<Real> xj = ld4<Real>(pos + j);
-            Real gx, gy, gz;
-            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-            const Real s = ks * xj.w;
-            acc.add(s * gx, s * gy, s * gz);
-        }
-    }
-    if (above_eps(ki)) {
-        for (uint32_t k = nf; k < nf + nb; ++k) {
-            const uint32_t j = nbr[(size_t)k * stride + i];
-            const Vec4<Real> xj = ld4<Real>(bpos + j);
-            Real gx, gy, gz;
-            K.gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, gx, gy, gz);
-            const Real s = ki * xj.w;
-            acc.add(s * gx, s * gy, s * gz);
-        }
-    }
+    jacobi_sum<Real>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c), [&](uint32_t j) { return kc[j]; }, acc);
     Vec4<Real> v = ds->vel[i];
     v.x += acc.x.value() * p.h_future;
     v.y += acc.y.value() * p.h_future;

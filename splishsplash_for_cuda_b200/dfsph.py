@@ -26,8 +26,8 @@ def _fptr(a: np.ndarray | None):
 
 def scene_struct(scene: Scene, precision: int = 32, device: int = 0, use_graphs: bool = True,
                  neighbor_capacity: int = 96, fluid_capacity: int | None = None,
-                 boundary_capacity: int | None = None) -> _capi.DfsphScene:
-    lib = _capi.load()
+                 boundary_capacity: int | None = None, lib_path: str | None = None) -> _capi.DfsphScene:
+    lib = _capi.load(lib_path)
     s = _capi.DfsphScene()
     _capi.check(lib, None, lib.dfsph_scene_defaults(C.byref(s)))
     cfg = scene.config
@@ -93,11 +93,12 @@ class DFSPHCUDA:
 
     def __init__(self, scene: Scene, precision: int = 32, device: int = 0, use_graphs: bool = True,
                  neighbor_capacity: int = 96, boundary_psi: np.ndarray | None = None,
-                 fluid_capacity: int | None = None):
-        self._lib = _capi.load()
+                 fluid_capacity: int | None = None, lib_path: str | None = None):
+        self._lib = _capi.load(lib_path)
         self.scene = scene
         self.precision = precision
-        self._struct = scene_struct(scene, precision, device, use_graphs, neighbor_capacity, fluid_capacity)
+        self._struct = scene_struct(scene, precision, device, use_graphs, neighbor_capacity, fluid_capacity,
+                                    lib_path=lib_path)
         ctx = C.c_void_p()
         code = self._lib.dfsph_create(C.byref(self._struct), C.byref(ctx))
         if code != _capi.DFSPH_OK:

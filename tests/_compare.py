@@ -8,10 +8,16 @@ def field_error(got: np.ndarray, ref: np.ndarray, floor_frac: float = 1e-3) -> f
     particles that need no pressure)."""
     got = np.asarray(got, dtype=np.float64)
     ref = np.asarray(ref, dtype=np.float64)
-    scale = np.max(np.abs(ref)) if ref.size else 0.0
-    floor = max(floor_frac * scale, 1e-300)
-    den = np.maximum(np.abs(ref), floor)
-    return float(np.max(np.abs(got - ref) / den)) if ref.size else 0.0
+    if ref.size == 0:
+        return 0.0
+    if ref.ndim == 2:  # vector fields: per-particle norm of the difference over the norm of the value
+        diff = np.linalg.norm(got - ref, axis=1)
+        mag = np.linalg.norm(ref, axis=1)
+    else:
+        diff = np.abs(got - ref)
+        mag = np.abs(ref)
+    floor = max(floor_frac * float(mag.max()), 1e-300)
+    return float(np.max(diff / np.maximum(mag, floor)))
 
 
 def assert_field(name: str, got, ref, rtol: float, floor_frac: float = 1e-3):

@@ -59,9 +59,10 @@ def test_boundary_psi_matches_fp64_oracle():
     assert_field("psi", d.field("boundary_psi", np.float64), o.field("boundary_psi"), 1e-6)
 
 
-@pytest.mark.parametrize("scene_fn", [lambda: synthetic_scene(1, counts=(14, 14, 14)), _moving_scene,
-                                      lambda: synthetic_scene(1)])
+@pytest.mark.parametrize("scene_fn", [lambda: synthetic_scene(1, counts=(14, 14, 14)), lambda: synthetic_scene(1),
+                                      lambda: synthetic_scene(2, counts=(40, 30, 30), cfl=True)])
 def test_one_step_fp32_matches_fp64_oracle(scene_fn):
+    """Physical scenes (dam breaks from rest): every field within 1e-5 of the FP64 oracle."""
     s = scene_fn()
     d = DFSPHCUDA(s)
     o = Oracle(s, 64)
@@ -72,6 +73,20 @@ def test_one_step_fp32_matches_fp64_oracle(scene_fn):
     assert st.density_error == pytest.approx(ro["density_error"], rel=1e-4, abs=1e-7)
     for name in FIELDS_ONE_STEP:
         assert_field(name, d.field(name, np.float64), o.field(name), 1e-5)
+
+
+def test_one_step_stress_scene_within_fp32_budget():
+    """Random velocities of +-0.5 m/s make the divergence sums cancel heavily; there the FP32 error
+    itself is ~1e-4. The device kernels must stay within twice the error of the FP32 oracle (the same
+    formulation in plain compensated FP32 on the CPU), both measured against the FP64 oracle."""
+    s = _moving_scene()
+    d = DFSPHCUDA(s)
+    o64, o32 = Oracle(s, 64), Oracle(s, 32)
+    st, r64, _ = d.step(), o64.step(), o32.step()
+    assert st.iterations == r64["iterations"] and st.iterations_v == r64["iterations_v"]
+    for name in FIELDS_ONE_STEP:
+        budget = field_error(o32.field(name), o64.field(name))
+        assert_field(name, d.field(name, np.float64), o64.field(name), max(1e-5, 2.0 * budget))
 
 
 def test_one_step_fp64_build_matches_fp64_oracle():
