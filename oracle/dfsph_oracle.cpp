@@ -55,6 +55,16 @@ template <class Real> struct Kahan {
     Real value() const { return s; }
 };
 
+template <class Real> struct Neumaier {
+    Real s = 0, c = 0;
+    void add(Real v) {
+        const Real t = s + v;
+        c += (std::fabs(s) >= std::fabs(v)) ? ((s - t) + v) : ((v - t) + s);
+        s = t;
+    }
+    Real value() const { return s + c; }
+};
+
 template <class Real> struct Cubic {
     Real H = 0, k = 0, l = 0, W0 = 0;
     void set(double Hd) {
@@ -299,7 +309,10 @@ template <class Real> struct Oracle {
         for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
             const uint32_t i = (uint32_t)ii;
             if (warm_v) kapv[i] = std::max<Real>(kapv[i] * hr / Real(2), Real(-0.5));
-            Kahan<Real> r, sgk, dr, gx, gy, gz;
+            // rho - rho0 accumulated directly (the device kernels do the same; see density_alpha_kernel)
+            Neumaier<Real> r;
+            Kahan<Real> sgk, dr, gx, gy, gz;
+            r.add((Real)-prm.density0);
             r.add(m[i] * K.W0);
             const Real xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
             const Real vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2];
@@ -326,7 +339,7 @@ template <class Real> struct Oracle {
             const Real Gx = gx.value(), Gy = gy.value(), Gz = gz.value();
             const Real sg = sgk.value() + (Gx * Gx + Gy * Gy + Gz * Gz);
             alpha[i] = -invh / std::max<Real>(sg, (Real)kEps);
-            rho[i] = r.value();
+            rho[i] = r.value();  // rho - rho0
             uint32_t num = (uint32_t)nf[i].size();
             if (num < kMinNeighbors) num += (uint32_t)nbd[i].size();
             dadv[i] = (num < kMinNeighbors) ? Real(0) : std::max<Real>(dr.value(), Real(0));
@@ -436,7 +449,7 @@ template <class Real> struct Oracle {
             Kahan<Real> ax, ay, az;
             for (uint32_t j : nf[i]) {
                 const Real w = K.W(xi - x[3 * j], yi - x[3 * j + 1], zi - x[3 * j + 2]);
-                const Real s = cvis * (m[j] / rho[j]);
+                const Real s = cvis * (m[j] / ((Real)prm.density0 + rho[j]));
                 ax.add(-(s * (vx - v[3 * j])) * w);
                 ay.add(-(s * (vy - v[3 * j + 1])) * w);
                 az.add(-(s * (vz - v[3 * j + 2])) * w);
@@ -475,7 +488,7 @@ template <class Real> struct Oracle {
     }
 
     double pressure_residual(bool init) {
-        const Real hf = (Real)h_future, r0 = (Real)prm.density0;
+        const Real hf = (Real)h_future;
 #pragma omp parallel for schedule(static)
         for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
             const uint32_t i = (uint32_t)ii;
@@ -483,7 +496,7 @@ template <class Real> struct Oracle {
                 alpha[i] *= (Real)inv_h_future;
                 kap[i] = 0;
             }
-            dadv[i] = std::max<Real>(rho[i] + hf * velocity_divergence(i) - r0, Real(0));
+            dadv[i] = std::max<Real>(rho[i] + hf * velocity_divergence(i), Real(0));  // rho[] = rho - rho0
             kc[i] = dadv[i] * alpha[i];
             kap[i] += kc[i];
         }
@@ -689,7 +702,10 @@ int oracle_get(void* h, int field, double* out) {
             case 0: return put(o.x);
             case 1: return put(o.v);
             case 2: return put(o.m);
-            case 3: return put(o.rho);
+            case 3: {  // density = rho0 + (rho - rho0)
+                for (size_t k = 0; k < o.rho.size(); ++k) out[k] = o.prm.density0 + (double)o.rho[k];
+                return 0;
+            }
             case 4: return put(o.alpha);
             case 5: return put(o.dadv);
             case 6: return put(o.kap);

@@ -725,6 +725,12 @@ public:
         const size_t bytes = (size_t)count * comps * (dtype == DFSPH_DTYPE_F32 ? 4 : 8);
         DF_CUDA(cudaMemcpyAsync(out, dl, bytes, cudaMemcpyDeviceToHost, stream));
         DF_CUDA(cudaStreamSynchronize(stream));
+        if (field == DFSPH_F_DENSITY) {  // the device keeps rho - rho0
+            if (dtype == DFSPH_DTYPE_F32)
+                for (uint32_t i = 0; i < count; ++i) ((float*)out)[i] = (float)(sc.density0 + ((float*)out)[i]);
+            else
+                for (uint32_t i = 0; i < count; ++i) ((double*)out)[i] = sc.density0 + ((double*)out)[i];
+        }
         return DFSPH_OK;
     }
 

@@ -65,6 +65,18 @@ template <class Real> struct KSum {
     }
     __device__ __forceinline__ Real value() const { return s; }
 };
+// Neumaier's variant: exact compensation whichever operand is larger. Used for the density
+// deviation rho - rho0, a sum whose terms (the rest density, the self term, ~30 neighbour terms of
+// up to a few hundred kg/m^3) cancel to a value ~1e3 times smaller than themselves.
+template <class Real> struct NSum {
+    Real s = Real(0), c = Real(0);
+    __device__ __forceinline__ void add(Real v) {
+        const Real t = s + v;
+        c += (fabs(s) >= fabs(v)) ? ((s - t) + v) : ((v - t) + s);
+        s = t;
+    }
+    __device__ __forceinline__ Real value() const { return s + c; }
+};
 template <class Real> struct KSum3 {
     KSum<Real> x, y, z;
     __device__ __forceinline__ void add(Real a, Real b, Real d) { x.add(a); y.add(b); z.add(d); }
@@ -122,8 +134,16 @@ constexpr uint32_t kEscapedKey = 0xFFFFFFFFu;  // sorts after every valid 30-bit
 // ---------------------------------------------------------------------------------------------
 // Cubic spline kernel (SPlisHSPlasH/DFSPH/SPH_kernels.h:20-100, CubicKernelPerso): W and grad W
 // with support H, k = 8/(pi H^3), l = 48/(pi H^3); grad W = 0 for |r| <= 1e-6.
+//   W(q)      = k (6 q^3 - 6 q^2 + 1)   for q <= 1/2,   2 k (1 - q)^3   for 1/2 < q <= 1
+//   grad W(r) = l q (3 q - 2) r / (|r| H)  for q <= 1/2,  -l (1 - q)^2 r / (|r| H)  for 1/2 < q <= 1
+// The reference evaluates q = |r| / H and 1 / (|r| H) with two divisions and a square root per pair;
+// here one reciprocal square root of |r|^2 and the precomputed 1/H give q and 1/(|r| H) with
+// multiplications only (a few ulp from the division form; the CPU oracle keeps the division form
+// and the parity tests bound the difference).
 template <class Real> struct Cubic {
     Real H, invH, k, l, W0;
+    static __device__ __forceinline__ float rsqrt_(float v) { return rsqrtf(v); }
+    static __device__ __forceinline__ double rsqrt_(double v) { return rsqrt(v); }
     __device__ __forceinline__ Real W_of_q(Real q) const {
         if (q <= Real(1)) {
             if (q <= Real(0.5)) {
@@ -136,50 +156,46 @@ template <class Real> struct Cubic {
         }
         return Real(0);
     }
+    // |r| <= 1e-6 (tested as |r|^2 <= 1e-12, the same cut-off up to rounding) gives grad W = 0 and
+    // W = W0 = W(0).
     __device__ __forceinline__ Real W(Real rx, Real ry, Real rz) const {
-        const Real rl = sqrt_(rx * rx + ry * ry + rz * rz);
-        return W_of_q(rl / H);
+        const Real r2 = rx * rx + ry * ry + rz * rz;
+        if (!(r2 > Real(1e-12))) return W0;
+        const Real q = r2 * rsqrt_(r2) * invH;
+        return W_of_q(q);
     }
-    // Returns grad W(r) and W(r) from one square root.
     __device__ __forceinline__ void gradW(Real rx, Real ry, Real rz, Real& gx, Real& gy, Real& gz) const {
-        const Real rl = sqrt_(rx * rx + ry * ry + rz * rz);
-        const Real q = rl / H;
+        const Real r2 = rx * rx + ry * ry + rz * rz;
         gx = gy = gz = Real(0);
-        if (q <= Real(1) && (double)rl > 1.0e-6) {
-            const Real s = Real(1) / (rl * H);
-            Real c;
-            if (q <= Real(0.5)) {
-                c = l * q * (Real(3) * q - Real(2));
-            } else {
-                const Real f = Real(1) - q;
-                c = l * (-f * f);
+        if (r2 > Real(1e-12)) {
+            const Real inv_rl = rsqrt_(r2);
+            const Real q = r2 * inv_rl * invH;
+            if (q <= Real(1)) {
+                const Real c = (q <= Real(0.5)) ? l * q * (Real(3) * q - Real(2)) : l * (-(Real(1) - q) * (Real(1) - q));
+                const Real f = c * inv_rl * invH;
+                gx = f * rx;
+                gy = f * ry;
+                gz = f * rz;
             }
-            gx = c * (rx * s);
-            gy = c * (ry * s);
-            gz = c * (rz * s);
         }
     }
     __device__ __forceinline__ void W_gradW(Real rx, Real ry, Real rz, Real& w, Real& gx, Real& gy, Real& gz) const {
-        const Real rl = sqrt_(rx * rx + ry * ry + rz * rz);
-        const Real q = rl / H;
+        const Real r2 = rx * rx + ry * ry + rz * rz;
         gx = gy = gz = Real(0);
-        w = W_of_q(q);
-        if (q <= Real(1) && (double)rl > 1.0e-6) {
-            const Real s = Real(1) / (rl * H);
-            Real c;
-            if (q <= Real(0.5)) {
-                c = l * q * (Real(3) * q - Real(2));
-            } else {
-                const Real f = Real(1) - q;
-                c = l * (-f * f);
+        w = W0;
+        if (r2 > Real(1e-12)) {
+            const Real inv_rl = rsqrt_(r2);
+            const Real q = r2 * inv_rl * invH;
+            w = W_of_q(q);
+            if (q <= Real(1)) {
+                const Real c = (q <= Real(0.5)) ? l * q * (Real(3) * q - Real(2)) : l * (-(Real(1) - q) * (Real(1) - q));
+                const Real f = c * inv_rl * invH;
+                gx = f * rx;
+                gy = f * ry;
+                gz = f * rz;
             }
-            gx = c * (rx * s);
-            gy = c * (ry * s);
-            gz = c * (rz * s);
         }
     }
-    static __device__ __forceinline__ float sqrt_(float v) { return sqrtf(v); }
-    static __device__ __forceinline__ double sqrt_(double v) { return sqrt(v); }
 };
 
 // ---------------------------------------------------------------------------------------------

@@ -20,7 +20,7 @@ template <class Real> struct DevState {
     Real* kappa;           // pressure warm-start accumulator
     Real* kappaV;          // divergence warm-start accumulator
     uint32_t* id;          // stable particle id
-    Real* density;
+    Real* density;         // density deviation rho - rho0 (stored instead of rho: see density_alpha_kernel)
     Real* factor;          // DFSPH alpha
     Real* densityAdv;      // clamped residual (divergence or density)
     Real* kcoef;           // densityAdv * factor, the Jacobi coefficient read by neighbours

@@ -23,7 +23,9 @@ template <class Real> __device__ __forceinline__ Real rmax(Real a, Real b);
 template <> __device__ __forceinline__ float rmax<float>(float a, float b) { return fmaxf(a, b); }
 template <> __device__ __forceinline__ double rmax<double>(double a, double b) { return fmax(a, b); }
 
-__device__ __forceinline__ bool above_eps(float v) { return (double)fabsf(v) > kEps; }
+// |v| > 1e-5 with v in float: identical to the reference's promotion of |v| to double against the
+// double literal, because no float lies strictly between 1e-5f and the next float above 1e-5.
+__device__ __forceinline__ bool above_eps(float v) { return fabsf(v) > 1.0e-5f; }
 __device__ __forceinline__ bool above_eps(double v) { return fabs(v) > kEps; }
 
 __device__ __forceinline__ uint32_t fluid_count(uint32_t c) { return c & 0xFFFFu; }
@@ -205,8 +207,13 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
     const Vec4<Real> vi = vel[i];
     const uint32_t c = ds->counts[i];
     const uint32_t nf = fluid_count(c), nb = boundary_count(c);
-    KSum<Real> rho, sgk, drho;
+    // rho - rho0 is accumulated directly (rest density first, then the self term and the neighbour
+    // terms) so that the density residual rho + h*div - rho0 of the pressure solve never subtracts
+    // two numbers of ~1e3 in FP32 (the reference forms rho, then rho + h*div - rho0).
+    NSum<Real> rho;
+    KSum<Real> sgk, drho;
     KSum3<Real> gpi;
+    rho.add(-p.density0);
     rho.add(xi.w * K.W0);
     auto accumulate = [&](const Vec4<Real>& xj, Real vx, Real vy, Real vz) {
         Real w, gx, gy, gz;
@@ -246,7 +253,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
     ds->densityAdv[i] = dadv;
     if (kFeatures) {
         float* f = ds->features + (size_t)i * 4;
-        f[0] = (float)((density - p.density0) / p.density0);
+        f[0] = (float)(density / p.density0);
         f[1] = (float)(dadv * alpha);
         f[2] = (float)(nf + nb) * (1.0f / 64.0f);
         f[3] = 0.0f;
@@ -341,7 +348,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) viscosity_kernel(con
         const StepParams<Real>& p = ds->p;
         const Vec4<Real>* __restrict__ pos = ds->pos;
         const Vec4<Real>* __restrict__ vel = ds->vel;
-        const Real* __restrict__ rho = ds->density;
+        const Real* __restrict__ rho = ds->density;  // rho - rho0
         const Cubic<Real> K = p.kern;
         const Vec4<Real> xi = pos[i];
         const Vec4<Real> vi = vel[i];
@@ -355,7 +362,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) viscosity_kernel(con
             [&](int u, uint32_t j) {
                 xj[u] = ld4<Real>(pos + j);
                 vj[u] = ld4<Real>(vel + j);
-                rj[u] = rho[j];
+                rj[u] = p.density0 + rho[j];
             },
             [&](int u) {
                 const Real w = K.W(xi.x - xj[u].x, xi.y - xj[u].y, xi.z - xj[u].z);
@@ -474,7 +481,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_residual_ke
         const Vec4<Real> vi = ds->vel[i];
         const uint32_t c = ds->counts[i];
         const Real sdiv = velocity_divergence<Real>(ds, p, i, xi, vi, fluid_count(c), boundary_count(c));
-        const Real dadv = rmax<Real>(ds->density[i] + p.h_future * sdiv - p.density0, Real(0));
+        const Real dadv = rmax<Real>(ds->density[i] + p.h_future * sdiv, Real(0));  // density[] = rho - rho0
         const Real kc = dadv * alpha;
         ds->densityAdv[i] = dadv;
         ds->kcoef[i] = kc;
