@@ -225,6 +225,21 @@ enum dfsph_kernel_id {
  * the end of a benchmark. */
 int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launch);
 
+/* Allocation-free stable sort of cell keys (no counterpart in the reference: it exists for callers
+ * that may not allocate device memory, e.g. a host framework that owns every allocation or a plugin
+ * handed fixed device buffers). All pointers are device pointers owned by the caller: keys_in[n] is
+ * read, keys_out[n] receives the keys in ascending order and perm_out[n] the original index of each
+ * sorted key (equal keys keep their input order), sorting on the low key_bits bits (1..32). The
+ * call performs no cudaMalloc/cudaFree: its scratch is a fixed device array built into the library
+ * (about 2.6 MB on every GPU that loads it, held until the process exits) and n is limited to
+ * 262,144 keys (larger n returns DFSPH_E_INVALID with a message in dfsph_last_error(NULL)). The
+ * first call on a device looks up that array's device address, so make it before any stream
+ * capture. Every call reuses the same array: calls that overlap on the GPU (other streams, other
+ * threads) race and must be serialised by the caller. The call runs on `stream` (a cudaStream_t,
+ * NULL = legacy default stream) and returns after the sort has finished. */
+int dfsph_sort_cell_keys_noalloc(const uint32_t* keys_in, uint32_t* keys_out, uint32_t* perm_out, uint32_t n,
+                                 int key_bits, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -118,7 +118,10 @@ SIGNATURES = {
     "dfsph_launch_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "dfsph_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "dfsph_time_kernel": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "dfsph_sort_cell_keys_noalloc": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_int, _P]),
 }
+
+NOALLOC_MAX_KEYS = 1 << 18
 
 KERNELS = ["neighbor_build", "density_alpha", "divergence_jacobi", "divergence_residual", "viscosity",
            "pressure_warm_jacobi", "pressure_residual", "pressure_jacobi", "update_pos", "sort_reorder"]

@@ -24,6 +24,8 @@ namespace dfsph {
 
 static thread_local std::string g_create_error;
 
+void set_global_error(const std::string& msg) { g_create_error = msg; }
+
 #define DF_CUDA(call)                                                                             \
     do {                                                                                          \
         cudaError_t e_ = (call);                                                                  \

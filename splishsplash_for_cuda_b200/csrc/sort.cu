@@ -11,6 +11,9 @@
 // decoupled look-back over earlier tiles. Tiles take their index from an atomic counter at start,
 // so a tile only ever waits on tiles that are already running; every wait is bounded and gives up
 // with DFSPH_ST_SORT_TIMEOUT instead of hanging.
+#include <mutex>
+#include <string>
+
 #include "dfsph_common.cuh"
 #include "sort.cuh"
 
@@ -196,4 +199,100 @@ void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, 
     *vals_out = in_a ? b.vals_a : b.vals_b;
 }
 
+// ---------------------------------------------------------------------------------------------------
+// Allocation-free variant of the cell-key sort.
+//
+// Some callers cannot allocate device memory at all: code that runs inside a host that owns every
+// allocation (a simulation framework with its own pool, a plugin that is handed device buffers and
+// must not grow the process's footprint, or code running where cudaMalloc would synchronise the
+// device). dfsph_sort_cell_keys_noalloc serves them: the caller passes the input keys and the output
+// buffers, and the sort's scratch (digit histograms, look-back tile flags, one ping-pong key/payload
+// pair) lives in the file-scope device array below, of a fixed maximum size. Every GPU that loads
+// this library holds the array until the process exits.
+namespace {
+constexpr uint32_t kNoAllocMaxKeys = 1u << 18;  // 262,144 keys per call
+constexpr size_t kNoAllocTiles = (kNoAllocMaxKeys + kSortTile - 1) / kSortTile;
+// layout (32-bit words): [0,4) tile counters, [4,8) status word, [8,1032) digit histograms,
+// [1032,2056) digit offsets, then 4 passes of tile look-back flags, then the ping-pong keys and
+// payloads. Everything before the ping-pong pair is cleared at the start of every call.
+constexpr size_t kNoAllocCounters = 0, kNoAllocStatus = 4, kNoAllocHist = 8, kNoAllocOffsets = 1032;
+constexpr size_t kNoAllocTileFlags = 2056;
+constexpr size_t kNoAllocClearWords = kNoAllocTileFlags + 4 * kNoAllocTiles * 256;
+constexpr size_t kNoAllocWords = kNoAllocClearWords + 2 * (size_t)kNoAllocMaxKeys;
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+uint32_t* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+int noalloc_fail(int code, const std::string& msg) {
+    set_global_error(msg);  // reported by dfsph_last_error(NULL)
+    return code;
+}
+}  // namespace
+
 }  // namespace dfsph
+
+extern "C" int dfsph_sort_cell_keys_noalloc(const uint32_t* keys_in, uint32_t* keys_out, uint32_t* perm_out,
+                                            uint32_t n, int key_bits, void* stream) {
+    using namespace dfsph;
+    if (n > kNoAllocMaxKeys)
+        return noalloc_fail(DFSPH_E_INVALID, "dfsph_sort_cell_keys_noalloc: n = " + std::to_string(n) +
+                                                 " exceeds the maximum of " + std::to_string(kNoAllocMaxKeys) + " keys");
+    if (key_bits < 1 || key_bits > 32) return noalloc_fail(DFSPH_E_INVALID, "key_bits must be in [1, 32]");
+    if (n == 0) return DFSPH_OK;
+    if (!keys_in || !keys_out || !perm_out) return noalloc_fail(DFSPH_E_INVALID, "null device buffer");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_fail(DFSPH_E_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return noalloc_fail(DFSPH_E_INVALID, "device ordinal out of range");
+    uint32_t* scratch = nullptr;
+    {
+        // First call on this device: resolve the device address of the scratch array (the host-side
+        // name g_noalloc_scratch is only a stand-in and must never be handed to a kernel).
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess)
+                return noalloc_fail(DFSPH_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_noalloc_ptr[dev] = (uint32_t*)p;
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int passes = (key_bits + 7) / 8;
+    const size_t tiles = (n + kSortTile - 1) / kSortTile;
+    uint32_t* counters = scratch + kNoAllocCounters;
+    uint32_t* status = scratch + kNoAllocStatus;
+    uint32_t* hist = scratch + kNoAllocHist;
+    uint32_t* offsets = scratch + kNoAllocOffsets;
+    uint32_t* flags = scratch + kNoAllocTileFlags;
+    uint32_t* pk = scratch + kNoAllocClearWords;  // ping-pong keys
+    uint32_t* pv = pk + kNoAllocMaxKeys;           // ping-pong payloads
+    e = cudaMemsetAsync(scratch, 0, kNoAllocClearWords * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return noalloc_fail(DFSPH_E_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+    int hist_blocks = (int)((n + kSortThreads * 16 - 1) / (kSortThreads * 16));
+    if (hist_blocks > 148 * 4) hist_blocks = 148 * 4;
+    histogram_kernel<<<hist_blocks, kSortThreads, 0, s>>>(keys_in, n, passes, hist);
+    scan_kernel<<<1, 256, 0, s>>>(hist, passes, offsets);
+    // The last pass must write the caller's buffers: with an odd pass count the first pass writes
+    // them, with an even count the first pass writes the scratch pair.
+    const uint32_t* kin = keys_in;
+    const uint32_t* vin = nullptr;  // iota payloads on the first pass
+    bool to_out = (passes & 1) == 1;
+    for (int p = 0; p < passes; ++p) {
+        uint32_t* kout = to_out ? keys_out : pk;
+        uint32_t* vout = to_out ? perm_out : pv;
+        onesweep_kernel<<<(unsigned)tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, 8 * p, offsets + p * 256,
+                                                                flags + (size_t)p * tiles * 256, counters + p, status);
+        kin = kout;
+        vin = vout;
+        to_out = !to_out;
+    }
+    uint32_t st = 0;
+    e = cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return noalloc_fail(DFSPH_E_CUDA, std::string("sort: ") + cudaGetErrorString(e));
+    if (st & DFSPH_ST_SORT_TIMEOUT) return noalloc_fail(DFSPH_E_DEVICE, "sort look-back gave up (output unspecified)");
+    return DFSPH_OK;
+}

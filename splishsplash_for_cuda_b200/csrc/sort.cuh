@@ -1,6 +1,7 @@
 // sort.cuh — interface of the in-house stable radix sort (sort.cu).
 #pragma once
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 namespace dfsph {
@@ -14,6 +15,10 @@ struct SortBuffers {
 };
 
 size_t radix_sort_workspace_words(uint32_t n_max, int passes);
+
+// Message slot of dfsph_last_error(NULL): errors of calls that have no context (dfsph_create and
+// the allocation-free entry points). Thread-local.
+void set_global_error(const std::string& msg);
 void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, cudaStream_t stream,
                       uint32_t* status_word, uint64_t* launch_counter, uint32_t** keys_out, uint32_t** vals_out);
 
