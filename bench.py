@@ -15,7 +15,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -39,51 +38,71 @@ def _peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """Samples SM clocks and clock-event (throttle) reasons through NVML every few milliseconds while
+    the timed region runs. Read-only (never changes a clock or a setting)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
-
-    def __init__(self, device: int):
+    def __init__(self, device: int, period_s: float = 0.002):
         self.device = device
-        self.rows = []
-        self.proc = None
+        self.period = period_s
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._nvml = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self._nvml = (pynvml, h)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self._sample()
+            self._thread = threading.Thread(target=self._loop, daemon=True)
+            self._thread.start()
+        except Exception:
+            self._nvml = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                self.rows.append(parts)
+    def _sample(self):
+        pynvml, h = self._nvml
+        self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+        names = {pynvml.nvmlClocksEventReasonHwSlowdown: "hw_slowdown",
+                 pynvml.nvmlClocksEventReasonHwThermalSlowdown: "hw_thermal_slowdown",
+                 pynvml.nvmlClocksEventReasonSwThermalSlowdown: "sw_thermal_slowdown",
+                 pynvml.nvmlClocksEventReasonSwPowerCap: "sw_power_cap",
+                 pynvml.nvmlClocksEventReasonHwPowerBrakeSlowdown: "hw_power_brake_slowdown"}
+        for bit, name in names.items():
+            if r & bit:
+                self.reasons.add(name)
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception:
+                break
+            time.sleep(self.period)
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=2)
+        if self._nvml:
             try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+                self._sample()
+                self._nvml[0].nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
-        if not self.rows:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml"}
 
 
 def make_scene(config: int):
@@ -227,8 +246,8 @@ def run_ours(args, world, rank, local):
                 d.update_fluid(host["x"], host["v"])
             st = d.step()
             if e2e:
-                host["x"][:] = d.positions()
-                host["v"][:] = d.velocities()
+                d.field("position", out=host["x"])
+                d.field("velocity", out=host["v"])
             with torch.cuda.stream(stream):
                 ends[s].record(stream)
             iters.append(st.iterations)

@@ -217,17 +217,27 @@ class DFSPHCUDA:
     def num_fluid(self) -> int:
         return self.m_data.getFluidParticlesCount()
 
-    def field(self, name: str, dtype=np.float32, order: int = _capi.ORDER_ID) -> np.ndarray:
+    def field(self, name: str, dtype=np.float32, order: int = _capi.ORDER_ID,
+              out: np.ndarray | None = None) -> np.ndarray:
+        """Downloads one field (shape (n,) or (n, comps)). `out`, when given, must be a C-contiguous
+        array of the right size and dtype (e.g. pinned host memory) and is filled in place."""
         fid, comps = _capi.FIELDS[name]
-        n = int(self.get_param("num_boundary")) if name.startswith("boundary") else self.num_fluid()
+        if out is None:
+            n = int(self.get_param("num_boundary")) if name.startswith("boundary") else self.num_fluid()
+            out = np.empty((n, comps) if comps > 1 else n, dtype=np.uint32 if name in ("id", "neighbor_counts")
+                           else dtype)
+        if not out.flags.c_contiguous:
+            raise ValueError("out must be C-contiguous")
         if name in ("id", "neighbor_counts"):
-            out = np.empty(n * comps, dtype=np.uint32)
             code = _capi.DTYPE_U32
+            if out.dtype != np.uint32:
+                raise ValueError("id and neighbor_counts download as uint32")
         else:
-            out = np.empty(n * comps, dtype=dtype)
-            code = _capi.DTYPE_F64 if np.dtype(dtype) == np.float64 else _capi.DTYPE_F32
+            code = _capi.DTYPE_F64 if out.dtype == np.float64 else _capi.DTYPE_F32
+            if out.dtype not in (np.float32, np.float64):
+                raise ValueError("float fields download as float32 or float64")
         self._call(self._lib.dfsph_download(self._ctx, fid, code, out.ctypes.data_as(C.c_void_p), out.size, order))
-        return out.reshape(n, comps) if comps > 1 else out
+        return out
 
     def positions(self, dtype=np.float32) -> np.ndarray:
         return self.field("position", dtype)
