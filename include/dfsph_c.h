@@ -89,6 +89,8 @@ typedef struct dfsph_step_stats {
     uint32_t status;              /* DFSPH_ST_* bits raised during the step                          */
     uint32_t num_fluid;           /* fluid particles                                                 */
     double ms_total;              /* device time of the step (CUDA events), 0 if timing is off       */
+    uint32_t warm_start;          /* learned warm start used: bit 0 divergence, bit 1 pressure       */
+    uint32_t trained;             /* 1 if the warm-start network was trained at the end of the step  */
 } dfsph_step_stats;
 
 /* ---- fields for upload / download -------------------------------------------------------------- */
@@ -184,7 +186,19 @@ int dfsph_on_step_end(dfsph_ctx* ctx);                                    /* onS
 /* Keys: "viscosity", "density0", "max_error", "max_error_v", "max_iterations", "max_iterations_v",
  * "enable_divergence_solver", "cfl_method", "cfl_factor", "cfl_max_time_step", "cfl_min_time_step",
  * "time_step" (sets the dt the next dt update uses), "gravitation_x|y|z", "use_graphs",
- * "h", "h_future", "h_past", "inv_h" (dt history of DFSPHCData), "timing" (1: record CUDA events). */
+ * "h", "h_future", "h_past", "inv_h" (dt history of DFSPHCData), "timing" (1: record CUDA events).
+ *
+ * Learned warm start (no reference counterpart; off by default, dfsph_step only):
+ * "learned_warm_start" (1: on), "warm_start_probe" (1: per solve, keep the learned candidate only if
+ * its initial residual sum |rho_adv - rho0| (divergence: |rho_dot|) is not above the plain
+ * candidate's, default 1), "warm_start_damping" (in (0, 1]: the learned warm start raises the
+ * reference's to at most this fraction of the predicted needed pressure, default 0.95),
+ * "train_interval" (steps between online trainings, default 50; 0: never), "train_start" (first
+ * training step, default 1), "train_iters" (Adam steps per training, default 20), "train_batch"
+ * (particles per training batch, 1..65536, default 4096), "learning_rate" (default 1e-3), "mlp_seed"
+ * (re-initialises the network).
+ * Read-only: "mlp_ready", "mlp_trainings", "mlp_adam_steps", "mlp_loss" (last batch loss),
+ * "learned_solves_v|p" (solves that had a learned candidate), "learned_kept_v|p" (solves that kept it). */
 int dfsph_set_param(dfsph_ctx* ctx, const char* key, double value);
 int dfsph_get_param(dfsph_ctx* ctx, const char* key, double* value);
 
@@ -224,6 +238,35 @@ enum dfsph_kernel_id {
  * Jacobi kernels move velocities), so call it only when the simulation will not continue, e.g. at
  * the end of a benchmark. */
 int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launch);
+
+/* ---- learned warm-start network (no reference counterpart) -------------------------------------
+ * A per-particle MLP, inputs x[8] = [(rho - rho0)/rho0, rho_dot * alpha, neighbours / 64,
+ * kappa_total_prev, kappa_v_total_prev, 0, 0, 0] (each multiplied by in_scale[i]), two hidden layers
+ * of 64 ReLU units, outputs y[2] = corrections to the previous step's total kappa and kappa_v in units
+ * of out_scale. Parameters, FP32, row-major [out][in]: W1[64][8] b1[64] W2[64][64] b2[64] W3[2][64]
+ * b3[2]. Inference runs on BF16 tensor cores with FP32 accumulation; training in FP32. Batches of
+ * host data hold at most 65536 samples. The loss is the mean over samples of the summed squared
+ * output errors. */
+#define DFSPH_MLP_INPUTS 8
+#define DFSPH_MLP_OUTPUTS 2
+#define DFSPH_MLP_PARAMS 4866
+int dfsph_mlp_get_params(dfsph_ctx* ctx, float* params, size_t n);
+/* Loads weights (resets the Adam moments) and marks the network ready for the warm start. */
+int dfsph_mlp_set_params(dfsph_ctx* ctx, const float* params, size_t n);
+int dfsph_mlp_get_scales(dfsph_ctx* ctx, float* in_scale, float* out_scale);
+/* Sets the input / output scales (otherwise set from the first online training batch). */
+int dfsph_mlp_set_scales(dfsph_ctx* ctx, const float* in_scale, const float* out_scale);
+/* y[2 i + o] = network output o of sample i (tensor-core inference path). */
+int dfsph_mlp_forward(dfsph_ctx* ctx, const float* x, uint32_t n, float* y);
+/* Gradient of the loss of targets t[2 i + o] w.r.t. the parameters (FP32), without an update;
+ * grad (DFSPH_MLP_PARAMS floats) and loss may be null. */
+int dfsph_mlp_gradient(dfsph_ctx* ctx, const float* x, const float* t, uint32_t n, float* grad, double* loss);
+/* iters Adam steps (beta1 0.9, beta2 0.999, eps 1e-8) on one batch; loss = loss before the last step. */
+int dfsph_mlp_train(dfsph_ctx* ctx, const float* x, const float* t, uint32_t n, int32_t iters, double learning_rate,
+                    double* loss);
+/* Re-initialises the weights from a seed (He-uniform hidden layers, zero output layer and biases),
+ * clears the scales and the Adam state; the warm start is plain until the next training. */
+int dfsph_mlp_reset(dfsph_ctx* ctx, uint32_t seed);
 
 /* Allocation-free stable sort of cell keys (no counterpart in the reference: it exists for callers
  * that may not allocate device memory, e.g. a host framework that owns every allocation or a plugin

@@ -82,6 +82,8 @@ class DfsphStepStats(C.Structure):
         ("status", C.c_uint32),
         ("num_fluid", C.c_uint32),
         ("ms_total", C.c_double),
+        ("warm_start", C.c_uint32),
+        ("trained", C.c_uint32),
     ]
 
 
@@ -118,8 +120,18 @@ SIGNATURES = {
     "dfsph_launch_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "dfsph_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "dfsph_time_kernel": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "dfsph_mlp_get_params": (C.c_int, [_P, _F, C.c_size_t]),
+    "dfsph_mlp_set_params": (C.c_int, [_P, _F, C.c_size_t]),
+    "dfsph_mlp_get_scales": (C.c_int, [_P, _F, _F]),
+    "dfsph_mlp_set_scales": (C.c_int, [_P, _F, _F]),
+    "dfsph_mlp_forward": (C.c_int, [_P, _F, C.c_uint32, _F]),
+    "dfsph_mlp_gradient": (C.c_int, [_P, _F, _F, C.c_uint32, _F, C.POINTER(C.c_double)]),
+    "dfsph_mlp_train": (C.c_int, [_P, _F, _F, C.c_uint32, C.c_int32, C.c_double, C.POINTER(C.c_double)]),
+    "dfsph_mlp_reset": (C.c_int, [_P, C.c_uint32]),
     "dfsph_sort_cell_keys_noalloc": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_int, _P]),
 }
+
+MLP_INPUTS, MLP_OUTPUTS, MLP_PARAMS = 8, 2, 4866
 
 NOALLOC_MAX_KEYS = 1 << 18
 

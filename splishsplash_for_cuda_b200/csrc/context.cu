@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -16,6 +17,7 @@
 
 #include "dfsph_state.cuh"
 #include "io.cuh"
+#include "mlp.cuh"
 #include "sort.cuh"
 
 struct dfsph_ctx;
@@ -103,10 +105,34 @@ public:
     bool use_graphs = true;
     cudaGraphExec_t g_loop[2] = {nullptr, nullptr};  // [0] divergence, [1] pressure
     uint32_t g_loop_n[2] = {0, 0};
+    bool g_loop_keep = false;  // the loop graphs store unclamped residuals (learned warm start)
     bool vel_updated = false;  // dfsph_update_vel ran since the last external-force pass
 
     int last_iters = 0, last_iters_v = 0;
     double last_err = 0, last_err_v = 0;
+
+    // Learned warm start (mlp.cuh). The network buffers are allocated on first use, the
+    // per-particle buffers when the mode is first enabled; the plain path touches neither.
+    static constexpr uint32_t kMaxTrainBatch = 1u << 16;
+    bool learned = false, mlp_ready = false, scales_set = false, probe = true;
+    Real* kappaT[2] = {nullptr, nullptr};
+    Real* kappaVT[2] = {nullptr, nullptr};
+    Real *kappaW = nullptr, *kappaVW = nullptr, *kappaP = nullptr, *kappaVP = nullptr;
+    Vec4<Real>* velP = nullptr;
+    Real *resid = nullptr, *residV = nullptr;
+    float *features = nullptr, *pred = nullptr, *tx = nullptr, *tt = nullptr;
+    MlpDev mlp{};
+    MlpScales h_scales{};
+    uint32_t mlp_seed = 1234567u;
+    int train_interval = 50, train_start = 1, train_iters = 20;
+    uint32_t train_batch = 4096;
+    double lr = 1e-3;
+    double damping = 0.95;  // learned warm start: at most damping x the predicted needed coefficient
+    int adam_t = 0;
+    uint64_t lsteps = 0, trainings = 0, kept_v = 0, kept_p = 0, solves_v = 0, solves_p = 0;
+    double hr_used = 1.0, r2_used = 1.0;  // dt ratios the two warm starts of this step used
+    uint32_t forced_warm = 0;             // learned candidates used without a probe this step
+    bool step_trained = false;
 
     // ------------------------------------------------------------------------------------------
     template <class T> int dalloc(T** p, size_t count) {
@@ -152,16 +178,16 @@ public:
         DF_TRY(dalloc(&sb.vals_a, nmax));
         DF_TRY(dalloc(&sb.vals_b, nmax));
         DF_TRY(dalloc(&sb.workspace, radix_sort_workspace_words(nmax, 4)));
-        DF_TRY(dalloc(&partials, grid_for(nmax) + 1));
+        DF_TRY(dalloc(&partials, 2 * ((size_t)grid_for(nmax) + 1)));  // two sums per block at most
         DF_TRY(dalloc(&cfl_partials, grid_for(nmax) + 1));
-        DF_TRY(dalloc(&ctl, 3));
+        DF_TRY(dalloc(&ctl, 4));
         DF_TRY(dalloc(&status, 4));
         DF_TRY(dalloc(&stage, (size_t)nmax * 7));
         DF_CUDA(cudaMalloc(&dl, (size_t)nmax * 3 * sizeof(double)));
         DF_CUDA(cudaMalloc((void**)&ds, sizeof(DevState<Real>)));
         DF_CUDA(cudaMallocHost((void**)&h_ctl, 3 * sizeof(LoopCtl)));
         DF_CUDA(cudaMallocHost((void**)&h_status, 4 * sizeof(uint32_t)));
-        DF_CUDA(cudaMemsetAsync(ctl, 0, 3 * sizeof(LoopCtl), stream));
+        DF_CUDA(cudaMemsetAsync(ctl, 0, 4 * sizeof(LoopCtl), stream));
         DF_CUDA(cudaMemsetAsync(status, 0, 4 * sizeof(uint32_t), stream));
         DF_CUDA(cudaMemsetAsync(counts, 0, Nc * sizeof(uint32_t), stream));
         DF_CUDA(cudaEventCreate(&ev0));
@@ -185,6 +211,13 @@ public:
         f(density); f(factor); f(densityAdv); f(kcoef); f(acc); f(counts); f(nbr); f(bid);
         f(sb.keys_a); f(sb.keys_b); f(sb.vals_a); f(sb.vals_b); f(sb.workspace);
         f(partials); f(cfl_partials); f(ctl); f(status); f(stage); f(dl); f(ds); f(ftab); f(btab);
+        for (int b = 0; b < 2; ++b) {
+            f(kappaT[b]); f(kappaVT[b]);
+        }
+        f(kappaW); f(kappaVW); f(kappaP); f(kappaVP); f(velP); f(resid); f(residV); f(features); f(pred); f(tx);
+        f(tt);
+        f(mlp.params); f(mlp.adam_m); f(mlp.adam_v); f(mlp.grad); f(mlp.partials);
+        f(mlp.w1_bf16); f(mlp.w2_bf16); f(mlp.w3_bf16); f(mlp.scales); f(mlp.loss);
         if (h_ctl) cudaFreeHost(h_ctl);
         if (h_status) cudaFreeHost(h_status);
         if (ev0) cudaEventDestroy(ev0);
@@ -251,8 +284,20 @@ public:
         hs.ctl = ctl;
         hs.status = status;
         hs.cfl_partials = cfl_partials;
-        hs.features = nullptr;
-        hs.predicted = nullptr;
+        hs.features = features;
+        hs.pred = pred;
+        hs.kappaT = kappaT[cur];
+        hs.kappaVT = kappaVT[cur];
+        hs.kappaW = kappaW;
+        hs.kappaVW = kappaVW;
+        hs.kappaP = kappaP;
+        hs.kappaVP = kappaVP;
+        hs.velP = velP;
+        hs.resid = resid;
+        hs.residV = residV;
+        hs.out_scale = mlp.scales ? reinterpret_cast<const float*>(reinterpret_cast<const char*>(mlp.scales) +
+                                                                  offsetof(MlpScales, out_scale))
+                                  : nullptr;
         launch_set_state<Real>(ds, hs, stream);
         launches += 1;
         DF_CUDA(cudaGetLastError());
@@ -418,6 +463,8 @@ public:
             launches += 1;
             DF_CUDA(cudaMemsetAsync(counts, 0, (size_t)count * sizeof(uint32_t), stream));
         }
+        if (kappaT[0]) DF_TRY(clear_totals());
+        lsteps = 0;
         reset_dt();
         DF_TRY(sync_state());
         DF_CUDA(cudaStreamSynchronize(stream));
@@ -450,6 +497,10 @@ public:
         const int nx = 1 - cur;
         launch_reorder_fluid<Real>(perm, n, pos[cur], vel[cur], kappa[cur], kappaV[cur], id[cur], pos[nx], vel[nx],
                                    kappa[nx], kappaV[nx], id[nx], stream);
+        if (learned) {
+            launch_reorder_pair<Real>(perm, n, kappaT[cur], kappaVT[cur], kappaT[nx], kappaVT[nx], stream);
+            launches += 1;
+        }
         cur = nx;
         DF_CUDA(cudaMemsetAsync(ftab, 0, cells * sizeof(uint2), stream));
         launch_cell_bounds(skeys, n, dim[0], dim[1], dim[2], ftab, stream);
@@ -486,10 +537,10 @@ public:
         DF_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         if (kind == 0) {
             launch_divergence_jacobi<Real>(ds, n, handle, true, stream);
-            launch_divergence_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream);
+            launch_divergence_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream, g_loop_keep);
         } else {
             launch_pressure_jacobi<Real>(ds, n, handle, true, stream);
-            launch_pressure_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream);
+            launch_pressure_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream, g_loop_keep);
         }
         cudaGraph_t captured = nullptr;
         DF_CUDA(cudaStreamEndCapture(stream, &captured));
@@ -504,9 +555,13 @@ public:
 
     // Runs the iterations of one solver loop after its init pass. Graph mode: one graph launch,
     // no host round trip. Host mode: one small readback per iteration (what the reference does).
-    int run_loop(int kind, int max_iter) {
+    int run_loop(int kind, int max_iter, bool keep = false) {
         if (max_iter <= 0) return DFSPH_OK;
         if (use_graphs) {
+            if (keep != g_loop_keep) {
+                DF_TRY(invalidate_graphs());
+                g_loop_keep = keep;
+            }
             if (!g_loop[kind] || g_loop_n[kind] != n) DF_TRY(build_loop_graph(kind));
             DF_CUDA(cudaGraphLaunch(g_loop[kind], stream));
             launches += 1;
@@ -516,10 +571,10 @@ public:
         while (cont) {
             if (kind == 0) {
                 launch_divergence_jacobi<Real>(ds, n, 0, false, stream);
-                launch_divergence_residual<Real>(ds, n, false, 0.0, 0, 0, 0, false, stream);
+                launch_divergence_residual<Real>(ds, n, false, 0.0, 0, 0, 0, false, stream, keep);
             } else {
                 launch_pressure_jacobi<Real>(ds, n, 0, false, stream);
-                launch_pressure_residual<Real>(ds, n, false, 0.0, 0, 0, 0, false, stream);
+                launch_pressure_residual<Real>(ds, n, false, 0.0, 0, 0, 0, false, stream, keep);
             }
             launches += 2;
             DF_CUDA(cudaMemcpyAsync(h_ctl + kind, ctl + kind, sizeof(LoopCtl), cudaMemcpyDeviceToHost, stream));
@@ -529,30 +584,76 @@ public:
         return DFSPH_OK;
     }
 
-    // cuda_divergenceSolve (DFSPH_core_cuda.cu:785-861).
-    int divergence_solve(int max_iter, double max_error) {
+    // cuda_divergenceSolve (DFSPH_core_cuda.cu:785-861). lp: learned warm start (dfsph_step only).
+    int divergence_solve(int max_iter, double max_error, bool lp = false) {
         if (!n) return DFSPH_OK;
         DF_CUDA(cudaMemsetAsync(&ctl[0].ticket, 0, sizeof(uint32_t), stream));
-        launch_density_alpha<Real>(ds, n, true, stream);
-        launch_divergence_warm_jacobi<Real>(ds, n, stream);
         const double eta = max_error * 0.01 * sc.density0 / h;
-        launch_divergence_residual<Real>(ds, n, true, eta, kMinItersV, max_iter, 0, false, stream);
-        launches += 3;
-        DF_TRY(run_loop(0, max_iter));
+        if (!lp) {
+            launch_density_alpha<Real>(ds, n, true, false, stream);
+            launch_divergence_warm_jacobi<Real>(ds, n, nullptr, nullptr, stream);
+            launch_divergence_residual<Real>(ds, n, true, eta, kMinItersV, max_iter, 0, false, stream);
+            launches += 3;
+        } else {
+            const bool use = mlp_ready;
+            launch_density_alpha<Real>(ds, n, false, true, stream);
+            if (use) launch_mlp_forward(mlp, features, n, pred, stream);
+            hr_used = h_ratio;
+            launch_warm_values<Real>(ds, n, 0, use, damping, stream);
+            launches += use ? 3 : 2;
+            if (use && probe) {  // plain candidate: velocities into velP, initial residual into ctl[3]
+                DF_CUDA(cudaMemsetAsync(&ctl[3].ticket, 0, sizeof(uint32_t), stream));
+                launch_divergence_warm_jacobi<Real>(ds, n, kappaVP, velP, stream);
+                launch_probe_residual<Real>(ds, n, 0, velP, stream);
+                launches += 2;
+            }
+            launch_divergence_warm_jacobi<Real>(ds, n, kappaVW, nullptr, stream);
+            launch_divergence_residual<Real>(ds, n, true, eta, kMinItersV, max_iter, 0, false, stream, true);
+            launches += 2;
+            if (use && probe) {
+                launch_fallback_residual<Real>(ds, n, 0, eta, kMinItersV, max_iter, stream);
+                launches += 1;
+            }
+            if (use && !probe) forced_warm |= 1u;
+            if (use) ++solves_v;
+        }
+        DF_TRY(run_loop(0, max_iter, lp));
         DF_CUDA(cudaGetLastError());
         return DFSPH_OK;
     }
 
     // cuda_pressureSolve (DFSPH_core_cuda.cu:1338-1419); with fused_vel the velocity update of
     // cuda_update_vel is applied inside the warm-start pass.
-    int pressure_solve(int max_iter, double max_error, bool fused_vel) {
+    int pressure_solve(int max_iter, double max_error, bool fused_vel, bool lp = false) {
         if (!n) return DFSPH_OK;
         DF_CUDA(cudaMemsetAsync(&ctl[1].ticket, 0, sizeof(uint32_t), stream));
-        launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, stream);
         const double eta = max_error * 0.01 * sc.density0;
-        launch_pressure_residual<Real>(ds, n, true, eta, kMinItersP, max_iter, 0, false, stream);
-        launches += 2;
-        DF_TRY(run_loop(1, max_iter));
+        if (!lp) {
+            launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, nullptr, nullptr, stream);
+            launch_pressure_residual<Real>(ds, n, true, eta, kMinItersP, max_iter, 0, false, stream);
+            launches += 2;
+        } else {
+            const bool use = mlp_ready;
+            r2_used = h_ratio2;
+            launch_warm_values<Real>(ds, n, 1, use, damping, stream);
+            launches += 1;
+            if (use && probe) {
+                DF_CUDA(cudaMemsetAsync(&ctl[3].ticket, 0, sizeof(uint32_t), stream));
+                launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, kappaP, velP, stream);
+                launch_probe_residual<Real>(ds, n, 1, velP, stream);
+                launches += 2;
+            }
+            launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, kappaW, nullptr, stream);
+            launch_pressure_residual<Real>(ds, n, true, eta, kMinItersP, max_iter, 0, false, stream, true);
+            launches += 2;
+            if (use && probe) {
+                launch_fallback_residual<Real>(ds, n, 1, eta, kMinItersP, max_iter, stream);
+                launches += 1;
+            }
+            if (use && !probe) forced_warm |= 2u;
+            if (use) ++solves_p;
+        }
+        DF_TRY(run_loop(1, max_iter, lp));
         DF_CUDA(cudaGetLastError());
         return DFSPH_OK;
     }
@@ -618,7 +719,7 @@ public:
     // Reads the loop control blocks and the status word (one synchronisation).
     int collect(bool div_ran, int max_iter_v, int max_iter) {
         DF_CUDA(cudaMemcpyAsync(h_ctl, ctl, 2 * sizeof(LoopCtl), cudaMemcpyDeviceToHost, stream));
-        DF_CUDA(cudaMemcpyAsync(h_status, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaMemcpyAsync(h_status, status, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         DF_CUDA(cudaStreamSynchronize(stream));
         last_iters = n ? h_ctl[1].iter : 0;
         last_err = h_ctl[1].avg;
@@ -638,13 +739,25 @@ public:
         DF_CHECK(grid_ready, DFSPH_E_STATE, "step before any boundary or fluid upload");
         if (timing) DF_CUDA(cudaEventRecord(ev0, stream));
         const double h_used = h;
+        const bool lp = learned && n > 0;
+        forced_warm = 0;
+        step_trained = false;
+        if (lp) DF_CUDA(cudaMemsetAsync(status + 2, 0, sizeof(uint32_t), stream));
         DF_TRY(neighbors_search());
         const bool div = sc.enable_divergence_solver != 0;
         if (div) {
-            DF_TRY(divergence_solve(sc.max_iterations_v, sc.max_error_v));
+            DF_TRY(divergence_solve(sc.max_iterations_v, sc.max_error_v, lp));
         } else if (n) {
-            launch_density_alpha<Real>(ds, n, false, stream);
+            launch_density_alpha<Real>(ds, n, false, lp, stream);
             launches += 1;
+            if (lp) {  // no divergence solve: its warm-start arrays stay zero
+                DF_CUDA(cudaMemsetAsync(kappaVW, 0, (size_t)n * sizeof(Real), stream));
+                DF_CUDA(cudaMemsetAsync(kappaV[cur], 0, (size_t)n * sizeof(Real), stream));
+                if (mlp_ready) {
+                    launch_mlp_forward(mlp, features, n, pred, stream);
+                    launches += 1;
+                }
+            }
         }
         const bool use_cfl = sc.cfl_method != 0;
         DF_TRY(external_forces(use_cfl));
@@ -653,12 +766,26 @@ public:
         } else {
             DF_TRY(update_time_step(time_step));
         }
-        DF_TRY(pressure_solve(sc.max_iterations, sc.max_error, true));
+        DF_TRY(pressure_solve(sc.max_iterations, sc.max_error, true, lp));
         DF_TRY(update_pos());
+        if (lp) {
+            const bool due = train_interval > 0 &&
+                             (lsteps == (uint64_t)train_start ||
+                              (lsteps > (uint64_t)train_start && (lsteps - train_start) % train_interval == 0));
+            if (due && train_iters > 0) DF_TRY(train_online(div));
+            launch_totals<Real>(ds, n, div, stream);
+            launches += 1;
+            ++lsteps;
+        }
         const double h_next = h_future;
         DF_TRY(on_step_end());
         if (timing) DF_CUDA(cudaEventRecord(ev1, stream));
         DF_TRY(collect(div, sc.max_iterations_v, sc.max_iterations));
+        if (lp) {
+            const uint32_t w = (h_status[2] | forced_warm) & 3u;
+            if (w & 1u) ++kept_v;
+            if (w & 2u) ++kept_p;
+        }
         if (st) {
             st->iterations = last_iters;
             st->iterations_v = last_iters_v;
@@ -668,6 +795,8 @@ public:
             st->h_future = h_next;
             st->status = h_status[0];
             st->num_fluid = n;
+            st->warm_start = lp ? ((h_status[2] | forced_warm) & 3u) : 0u;
+            st->trained = step_trained ? 1u : 0u;
             st->ms_total = 0.0;
             if (timing) {
                 float ms = 0.0f;
@@ -675,6 +804,258 @@ public:
                 st->ms_total = ms;
             }
         }
+        return DFSPH_OK;
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Learned warm start: buffers, training, host-facing network calls.
+    int ensure_mlp() {
+        if (mlp.params) return DFSPH_OK;
+        DF_TRY(dalloc(&mlp.params, kMlpParams));
+        DF_TRY(dalloc(&mlp.adam_m, kMlpParams));
+        DF_TRY(dalloc(&mlp.adam_v, kMlpParams));
+        DF_TRY(dalloc(&mlp.grad, kMlpParams));
+        DF_TRY(dalloc(&mlp.partials, mlp_partials_floats(kMaxTrainBatch)));
+        DF_TRY(dalloc(&mlp.w1_bf16, kMlpHidden * 16));
+        DF_TRY(dalloc(&mlp.w2_bf16, kMlpHidden * kMlpHidden));
+        DF_TRY(dalloc(&mlp.w3_bf16, 8 * kMlpHidden));
+        DF_TRY(dalloc(&mlp.scales, 1));
+        DF_TRY(dalloc(&mlp.loss, 1));
+        DF_TRY(dalloc(&tx, (size_t)kMaxTrainBatch * kMlpIn));
+        DF_TRY(dalloc(&tt, (size_t)kMaxTrainBatch * kMlpOut));
+        DF_TRY(mlp_reset(mlp_seed));
+        return sync_state();
+    }
+
+    int upload_scales() {
+        DF_CUDA(cudaMemcpyAsync(mlp.scales, &h_scales, sizeof(MlpScales), cudaMemcpyHostToDevice, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));  // h_scales may change right after
+        return DFSPH_OK;
+    }
+
+    int mlp_reset(uint32_t seed) {
+        mlp_seed = seed;
+        for (int i = 0; i < kMlpIn; ++i) h_scales.in_scale[i] = i < 5 ? 1.0f : 0.0f;
+        for (int o = 0; o < kMlpOut; ++o) h_scales.out_scale[o] = 1.0f;
+        DF_TRY(upload_scales());
+        launch_mlp_init(mlp, seed, stream);
+        launch_mlp_pack(mlp, stream);
+        DF_CUDA(cudaMemsetAsync(mlp.loss, 0, sizeof(double), stream));
+        launches += 2;
+        adam_t = 0;
+        mlp_ready = false;
+        scales_set = false;
+        DF_CUDA(cudaGetLastError());
+        return DFSPH_OK;
+    }
+
+    int clear_totals() {
+        for (int b = 0; b < 2; ++b) {
+            DF_CUDA(cudaMemsetAsync(kappaT[b], 0, (size_t)Nc * sizeof(Real), stream));
+            DF_CUDA(cudaMemsetAsync(kappaVT[b], 0, (size_t)Nc * sizeof(Real), stream));
+        }
+        return DFSPH_OK;
+    }
+
+    int enable_learned(bool on) {
+        if (on && !learned) {
+            DF_TRY(ensure_mlp());
+            if (!kappaT[0]) {
+                for (int b = 0; b < 2; ++b) {
+                    DF_TRY(dalloc(&kappaT[b], Nc));
+                    DF_TRY(dalloc(&kappaVT[b], Nc));
+                }
+                DF_TRY(dalloc(&kappaW, Nc));
+                DF_TRY(dalloc(&kappaVW, Nc));
+                DF_TRY(dalloc(&kappaP, Nc));
+                DF_TRY(dalloc(&kappaVP, Nc));
+                DF_TRY(dalloc(&velP, Nc));
+                DF_TRY(dalloc(&resid, Nc));
+                DF_TRY(dalloc(&residV, Nc));
+                DF_TRY(dalloc(&features, (size_t)Nc * kMlpIn));
+                DF_TRY(dalloc(&pred, (size_t)Nc * kMlpOut));
+            }
+            DF_TRY(clear_totals());
+            lsteps = 0;
+        }
+        learned = on;
+        return sync_state();
+    }
+
+    // Normalisation that follows the data: inputs scaled to unit RMS, outputs in units of the
+    // targets' RMS, from the current training batch. A scale is replaced when it is unset or off by
+    // more than 2x, and the first / last layer are rescaled with it so that the network computes
+    // the same function in physical units (the Adam state restarts).
+    int adapt_scales(uint32_t B, uint32_t offset, bool div) {
+        std::vector<float> x((size_t)B * kMlpIn), t((size_t)B * kMlpOut);
+        DF_CUDA(cudaMemcpyAsync(x.data(), tx, x.size() * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaMemcpyAsync(t.data(), tt, t.size() * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        auto rms = [&](const std::vector<float>& v, int stride, int c, double mul) {
+            double acc = 0.0;
+            for (uint32_t k = 0; k < B; ++k) {
+                const double e = (double)v[(size_t)k * stride + c] * mul;
+                acc += e * e;
+            }
+            return std::sqrt(acc / (double)B);
+        };
+        MlpScales ns = h_scales;
+        bool changed = false;
+        for (int i = 0; i < 5; ++i) {
+            const double r = rms(x, kMlpIn, i, 1.0);
+            if (!(r > 1e-30) || !std::isfinite(r)) continue;
+            const double ratio = (1.0 / r) / (double)h_scales.in_scale[i];
+            if (!scales_set || ratio > 2.0 || ratio < 0.5) {
+                ns.in_scale[i] = (float)(1.0 / r);
+                changed = true;
+            }
+        }
+        for (int o = 0; o < kMlpOut; ++o) {
+            const double r = rms(t, kMlpOut, o, (double)h_scales.out_scale[o]);  // raw target RMS
+            if (!(r > 1e-30) || !std::isfinite(r)) continue;
+            const double ratio = r / (double)h_scales.out_scale[o];
+            if (!scales_set || ratio > 2.0 || ratio < 0.5) {
+                ns.out_scale[o] = (float)r;
+                changed = true;
+            }
+        }
+        scales_set = true;
+        if (!changed) return DFSPH_OK;
+        std::vector<float> prm(kMlpParams);
+        DF_CUDA(cudaMemcpyAsync(prm.data(), mlp.params, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        for (int j = 0; j < kMlpHidden; ++j)
+            for (int i = 0; i < kMlpIn; ++i)
+                if (ns.in_scale[i] != 0.0f)
+                    prm[kW1 + j * kMlpIn + i] *= h_scales.in_scale[i] / ns.in_scale[i];
+        for (int o = 0; o < kMlpOut; ++o) {
+            const float f = h_scales.out_scale[o] / ns.out_scale[o];
+            for (int j = 0; j < kMlpHidden; ++j) prm[kW3 + o * kMlpHidden + j] *= f;
+            prm[kB3 + o] *= f;
+        }
+        DF_CUDA(cudaMemcpyAsync(mlp.params, prm.data(), kMlpParams * sizeof(float), cudaMemcpyHostToDevice, stream));
+        DF_CUDA(cudaMemsetAsync(mlp.adam_m, 0, kMlpParams * sizeof(float), stream));
+        DF_CUDA(cudaMemsetAsync(mlp.adam_v, 0, kMlpParams * sizeof(float), stream));
+        adam_t = 0;
+        h_scales = ns;
+        DF_TRY(upload_scales());  // synchronises: prm goes out of scope
+        launch_gather_training<Real>(ds, n, B, offset, r2_used, hr_used, div, tx, tt, stream);  // targets / new scale
+        launches += 1;
+        return DFSPH_OK;
+    }
+
+    // One online training round at the end of a step: a batch of this step's (features, needed
+    // coefficients) pairs, train_iters Adam steps, then the BF16 inference copies.
+    int train_online(bool div) {
+        uint32_t B = std::min<uint32_t>(std::min<uint32_t>(train_batch, kMaxTrainBatch), n);
+        if (!B) return DFSPH_OK;
+        const uint32_t offset = (uint32_t)((lsteps * 2654435761ull) % n);
+        launch_gather_training<Real>(ds, n, B, offset, r2_used, hr_used, div, tx, tt, stream);
+        launches += 1;
+        DF_TRY(adapt_scales(B, offset, div));
+        for (int it = 0; it < train_iters; ++it)
+            launch_mlp_train_step(mlp, tx, tt, B, 1, (float)lr, 0.9f, 0.999f, 1e-8f, ++adam_t, stream);
+        launch_mlp_pack(mlp, stream);
+        launches += 1 + 2ull * (uint64_t)train_iters;
+        mlp_ready = true;
+        step_trained = true;
+        ++trainings;
+        DF_CUDA(cudaGetLastError());
+        return DFSPH_OK;
+    }
+
+    int stage_batch(const float* x, const float* t, uint32_t B) {
+        DF_CHECK(B > 0 && B <= kMaxTrainBatch, DFSPH_E_INVALID, "batch must be in [1, 65536]");
+        DF_CHECK(x, DFSPH_E_INVALID, "null inputs");
+        DF_TRY(ensure_mlp());
+        DF_CUDA(cudaMemcpyAsync(tx, x, (size_t)B * kMlpIn * sizeof(float), cudaMemcpyHostToDevice, stream));
+        if (t) DF_CUDA(cudaMemcpyAsync(tt, t, (size_t)B * kMlpOut * sizeof(float), cudaMemcpyHostToDevice, stream));
+        return DFSPH_OK;
+    }
+
+    int mlp_get_params(float* out, size_t count) {
+        DF_CHECK(out && count >= (size_t)kMlpParams, DFSPH_E_INVALID, "output needs DFSPH_MLP_PARAMS floats");
+        DF_TRY(ensure_mlp());
+        DF_CUDA(cudaMemcpyAsync(out, mlp.params, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        return DFSPH_OK;
+    }
+
+    int mlp_set_params(const float* in, size_t count) {
+        DF_CHECK(in && count >= (size_t)kMlpParams, DFSPH_E_INVALID, "input needs DFSPH_MLP_PARAMS floats");
+        DF_TRY(ensure_mlp());
+        DF_CUDA(cudaMemcpyAsync(mlp.params, in, kMlpParams * sizeof(float), cudaMemcpyHostToDevice, stream));
+        DF_CUDA(cudaMemsetAsync(mlp.adam_m, 0, kMlpParams * sizeof(float), stream));
+        DF_CUDA(cudaMemsetAsync(mlp.adam_v, 0, kMlpParams * sizeof(float), stream));
+        launch_mlp_pack(mlp, stream);
+        launches += 1;
+        DF_CUDA(cudaStreamSynchronize(stream));
+        adam_t = 0;
+        mlp_ready = true;
+        return DFSPH_OK;
+    }
+
+    int mlp_get_scales(float* in_scale, float* out_scale) {
+        DF_CHECK(in_scale && out_scale, DFSPH_E_INVALID, "null output");
+        DF_TRY(ensure_mlp());
+        std::memcpy(in_scale, h_scales.in_scale, sizeof(h_scales.in_scale));
+        std::memcpy(out_scale, h_scales.out_scale, sizeof(h_scales.out_scale));
+        return DFSPH_OK;
+    }
+
+    int mlp_set_scales(const float* in_scale, const float* out_scale) {
+        DF_CHECK(in_scale && out_scale, DFSPH_E_INVALID, "null input");
+        DF_TRY(ensure_mlp());
+        for (int o = 0; o < kMlpOut; ++o)
+            DF_CHECK(std::isfinite(out_scale[o]) && out_scale[o] != 0.0f, DFSPH_E_INVALID,
+                     "output scales must be finite and non-zero");
+        std::memcpy(h_scales.in_scale, in_scale, sizeof(h_scales.in_scale));
+        std::memcpy(h_scales.out_scale, out_scale, sizeof(h_scales.out_scale));
+        DF_TRY(upload_scales());
+        scales_set = true;
+        return DFSPH_OK;
+    }
+
+    int mlp_forward_host(const float* x, uint32_t B, float* y) {
+        DF_CHECK(y, DFSPH_E_INVALID, "null output");
+        DF_TRY(stage_batch(x, nullptr, B));
+        launch_mlp_forward(mlp, tx, B, tt, stream);
+        launches += 1;
+        DF_CUDA(cudaMemcpyAsync(y, tt, (size_t)B * kMlpOut * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        DF_CUDA(cudaGetLastError());
+        return DFSPH_OK;
+    }
+
+    int mlp_gradient_host(const float* x, const float* t, uint32_t B, float* grad, double* loss) {
+        DF_CHECK(t, DFSPH_E_INVALID, "null targets");
+        DF_TRY(stage_batch(x, t, B));
+        launch_mlp_train_step(mlp, tx, tt, B, 0, 0.0f, 0.9f, 0.999f, 1e-8f, 1, stream);
+        launches += 2;
+        if (grad)
+            DF_CUDA(cudaMemcpyAsync(grad, mlp.grad, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        double l = 0.0;
+        DF_CUDA(cudaMemcpyAsync(&l, mlp.loss, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        DF_CUDA(cudaGetLastError());
+        if (loss) *loss = l;
+        return DFSPH_OK;
+    }
+
+    int mlp_train_host(const float* x, const float* t, uint32_t B, int iters, double rate, double* loss) {
+        DF_CHECK(t, DFSPH_E_INVALID, "null targets");
+        DF_CHECK(iters > 0 && rate > 0 && std::isfinite(rate), DFSPH_E_INVALID, "iters and rate must be > 0");
+        DF_TRY(stage_batch(x, t, B));
+        for (int it = 0; it < iters; ++it)
+            launch_mlp_train_step(mlp, tx, tt, B, 1, (float)rate, 0.9f, 0.999f, 1e-8f, ++adam_t, stream);
+        launch_mlp_pack(mlp, stream);
+        launches += 1 + 2ull * (uint64_t)iters;
+        double l = 0.0;
+        DF_CUDA(cudaMemcpyAsync(&l, mlp.loss, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        DF_CUDA(cudaGetLastError());
+        if (loss) *loss = l;
+        mlp_ready = true;
         return DFSPH_OK;
     }
 
@@ -782,6 +1163,28 @@ public:
         else if (k == "h_past") { h_past = v; dt_changed = true; }
         else if (k == "inv_h") { inv_h = v; dt_changed = true; }
         else if (k == "timing") timing = v != 0;
+        else if (k == "learned_warm_start") return enable_learned(v != 0);
+        else if (k == "warm_start_probe") probe = v != 0;
+        else if (k == "warm_start_damping") {
+            DF_CHECK(v > 0 && v <= 1, DFSPH_E_INVALID, "warm_start_damping must be in (0, 1]");
+            damping = v;
+        }
+        else if (k == "train_interval") { DF_CHECK(v >= 0, DFSPH_E_INVALID, "train_interval must be >= 0"); train_interval = (int)v; }
+        else if (k == "train_start") { DF_CHECK(v >= 0, DFSPH_E_INVALID, "train_start must be >= 0"); train_start = (int)v; }
+        else if (k == "train_iters") { DF_CHECK(v >= 0, DFSPH_E_INVALID, "train_iters must be >= 0"); train_iters = (int)v; }
+        else if (k == "train_batch") {
+            DF_CHECK(v >= 1 && v <= kMaxTrainBatch, DFSPH_E_INVALID, "train_batch must be in [1, 65536]");
+            train_batch = (uint32_t)v;
+        }
+        else if (k == "learning_rate") { DF_CHECK(v > 0, DFSPH_E_INVALID, "learning_rate must be > 0"); lr = v; }
+        else if (k == "mlp_seed") {
+            DF_CHECK(v >= 0 && v < 4294967296.0, DFSPH_E_INVALID, "mlp_seed must fit 32 bits");
+            if (!mlp.params) {
+                mlp_seed = (uint32_t)v;
+                return DFSPH_OK;
+            }
+            return mlp_reset((uint32_t)v);
+        }
         else DF_CHECK(false, DFSPH_E_INVALID, "unknown parameter key: " + k);
         (void)dt_changed;
         return sync_state();
@@ -819,6 +1222,30 @@ public:
         else if (k == "sort_passes") *v = key_passes;
         else if (k == "iterations") *v = last_iters;
         else if (k == "iterations_v") *v = last_iters_v;
+        else if (k == "learned_warm_start") *v = learned ? 1 : 0;
+        else if (k == "warm_start_probe") *v = probe ? 1 : 0;
+        else if (k == "warm_start_damping") *v = damping;
+        else if (k == "train_interval") *v = train_interval;
+        else if (k == "train_start") *v = train_start;
+        else if (k == "train_iters") *v = train_iters;
+        else if (k == "train_batch") *v = train_batch;
+        else if (k == "learning_rate") *v = lr;
+        else if (k == "mlp_seed") *v = mlp_seed;
+        else if (k == "mlp_ready") *v = mlp_ready ? 1 : 0;
+        else if (k == "mlp_trainings") *v = (double)trainings;
+        else if (k == "mlp_adam_steps") *v = adam_t;
+        else if (k == "learned_kept_v") *v = (double)kept_v;
+        else if (k == "learned_kept_p") *v = (double)kept_p;
+        else if (k == "learned_solves_v") *v = (double)solves_v;
+        else if (k == "learned_solves_p") *v = (double)solves_p;
+        else if (k == "mlp_loss") {
+            double l = 0.0;
+            if (mlp.loss) {
+                DF_CUDA(cudaMemcpyAsync(&l, mlp.loss, sizeof(double), cudaMemcpyDeviceToHost, stream));
+                DF_CUDA(cudaStreamSynchronize(stream));
+            }
+            *v = l;
+        }
         else DF_CHECK(false, DFSPH_E_INVALID, "unknown parameter key: " + k);
         return DFSPH_OK;
     }
@@ -826,13 +1253,15 @@ public:
     void launch_kernel(int k) {
         switch (k) {
             case DFSPH_K_NEIGHBOR_BUILD: launch_build_neighbors<Real>(ds, n, ftab, btab, stream); break;
-            case DFSPH_K_DENSITY_ALPHA: launch_density_alpha<Real>(ds, n, false, stream); break;
+            case DFSPH_K_DENSITY_ALPHA: launch_density_alpha<Real>(ds, n, false, false, stream); break;
             case DFSPH_K_DIVERGENCE_JACOBI: launch_divergence_jacobi<Real>(ds, n, 0, false, stream); break;
             case DFSPH_K_DIVERGENCE_RESIDUAL:
                 launch_divergence_residual<Real>(ds, n, false, 0.0, 0, 0, 0, false, stream);
                 break;
             case DFSPH_K_VISCOSITY: launch_viscosity<Real>(ds, n, false, stream); break;
-            case DFSPH_K_PRESSURE_WARM_JACOBI: launch_pressure_warm_jacobi<Real>(ds, n, false, stream); break;
+            case DFSPH_K_PRESSURE_WARM_JACOBI:
+                launch_pressure_warm_jacobi<Real>(ds, n, false, nullptr, nullptr, stream);
+                break;
             case DFSPH_K_PRESSURE_RESIDUAL:
                 launch_pressure_residual<Real>(ds, n, false, 0.0, 0, 0, 0, false, stream);
                 break;
@@ -859,12 +1288,17 @@ public:
                 const int nx = 1 - cur;
                 launch_reorder_fluid<Real>(perm, n, pos[cur], vel[cur], kappa[cur], kappaV[cur], id[cur], pos[nx],
                                            vel[nx], kappa[nx], kappaV[nx], id[nx], stream);
+                if (learned) {
+                    launch_reorder_pair<Real>(perm, n, kappaT[cur], kappaVT[cur], kappaT[nx], kappaVT[nx], stream);
+                    launches += 1;
+                }
                 DF_CUDA(cudaMemsetAsync(ftab, 0, cells * sizeof(uint2), stream));
                 launch_cell_bounds(skeys, n, dim[0], dim[1], dim[2], ftab, stream);
                 cur = nx;
                 launches += 3;
                 launch_set_state<Real>(ds, (hs.pos = pos[cur], hs.vel = vel[cur], hs.kappa = kappa[cur],
-                                            hs.kappaV = kappaV[cur], hs.id = id[cur], hs), stream);
+                                            hs.kappaV = kappaV[cur], hs.id = id[cur], hs.kappaT = kappaT[cur],
+                                            hs.kappaVT = kappaVT[cur], hs), stream);
             } else {
                 launch_kernel(k);
             }
@@ -1082,6 +1516,36 @@ int dfsph_get_stream(dfsph_ctx* ctx, void** stream) {
 }
 int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launch) {
     DFSPH_DISPATCH(ctx, time_kernel(kernel, reps, ms_per_launch));
+}
+int dfsph_mlp_get_params(dfsph_ctx* ctx, float* params, size_t n) { DFSPH_DISPATCH(ctx, mlp_get_params(params, n)); }
+int dfsph_mlp_set_params(dfsph_ctx* ctx, const float* params, size_t n) {
+    DFSPH_DISPATCH(ctx, mlp_set_params(params, n));
+}
+int dfsph_mlp_get_scales(dfsph_ctx* ctx, float* in_scale, float* out_scale) {
+    DFSPH_DISPATCH(ctx, mlp_get_scales(in_scale, out_scale));
+}
+int dfsph_mlp_set_scales(dfsph_ctx* ctx, const float* in_scale, const float* out_scale) {
+    DFSPH_DISPATCH(ctx, mlp_set_scales(in_scale, out_scale));
+}
+int dfsph_mlp_forward(dfsph_ctx* ctx, const float* x, uint32_t n, float* y) {
+    DFSPH_DISPATCH(ctx, mlp_forward_host(x, n, y));
+}
+int dfsph_mlp_gradient(dfsph_ctx* ctx, const float* x, const float* t, uint32_t n, float* grad, double* loss) {
+    DFSPH_DISPATCH(ctx, mlp_gradient_host(x, t, n, grad, loss));
+}
+int dfsph_mlp_train(dfsph_ctx* ctx, const float* x, const float* t, uint32_t n, int32_t iters, double learning_rate,
+                    double* loss) {
+    DFSPH_DISPATCH(ctx, mlp_train_host(x, t, n, iters, learning_rate, loss));
+}
+int dfsph_mlp_reset(dfsph_ctx* ctx, uint32_t seed) {
+    if (!ctx) return DFSPH_E_INVALID;
+    cudaSetDevice(ctx->device);
+    if (ctx->f32) {
+        const int r = ctx->f32->ensure_mlp();
+        return r != DFSPH_OK ? r : ctx->f32->mlp_reset(seed);
+    }
+    const int r = ctx->f64->ensure_mlp();
+    return r != DFSPH_OK ? r : ctx->f64->mlp_reset(seed);
 }
 int dfsph_launch_count(dfsph_ctx* ctx, uint64_t* launches) {
     if (!ctx || !launches) return DFSPH_E_INVALID;

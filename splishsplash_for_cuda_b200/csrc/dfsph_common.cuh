@@ -260,6 +260,7 @@ struct LoopCtl {
     uint32_t cont;       // loop condition for the next iteration
     uint32_t ticket;     // last-block election counter
     uint32_t pad;
+    double aux;          // second sum of an init pass that reduces two values (learned warm start)
 };
 
 }  // namespace dfsph

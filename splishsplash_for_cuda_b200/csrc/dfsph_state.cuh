@@ -32,12 +32,22 @@ template <class Real> struct DevState {
     const Vec4<Real>* bvel;  // vx, vy, vz, (unused)
     // reductions and control
     double* partials;      // one FP64 partial per block
-    LoopCtl* ctl;          // [0] divergence loop, [1] pressure loop, [2] CFL / misc
-    uint32_t* status;      // DFSPH_ST_* bits
+    LoopCtl* ctl;          // [0] divergence loop, [1] pressure loop, [2] CFL / misc, [3] candidate probe
+    uint32_t* status;      // [0] DFSPH_ST_* bits, [1] scratch, [2] learned warm start kept (bit 0 div, 1 pressure)
     float* cfl_partials;   // per-block max |v + a h|^2
-    // learned warm start (null when off)
-    float* features;       // 4 per particle, written by the density+alpha pass
-    float* predicted;      // 2 per particle: kappa, kappa_v predictions
+    // learned warm start (see mlp.cuh)
+    float* features;       // kMlpIn per particle, written by the density+alpha pass
+    float* pred;           // 2 per particle: network outputs (normalised corrections)
+    Real* kappaT;          // previous step's total applied kappa (warm start + corrections)
+    Real* kappaVT;         // previous step's total applied kappa_v
+    Real* kappaW;          // warm-start value used by this step's pressure solve
+    Real* kappaVW;         // warm-start value used by this step's divergence solve
+    Real* kappaP;          // plain (reference) pressure warm-start candidate
+    Real* kappaVP;         // plain (reference) divergence warm-start candidate
+    Vec4<Real>* velP;      // velocities after the plain candidate's warm-start pass (probe)
+    Real* resid;           // unclamped density residual of the last pressure pass (null: not kept)
+    Real* residV;          // unclamped divergence residual of the last divergence pass (null: not kept)
+    const float* out_scale;  // 2 floats: scales of the network outputs
 };
 
 // ---- launch wrappers (neighbors.cu) ----------------------------------------------------------------
@@ -48,6 +58,10 @@ template <class Real>
 void launch_reorder_fluid(const uint32_t* perm, uint32_t n, const Vec4<Real>* pos_in, const Vec4<Real>* vel_in,
                           const Real* kappa_in, const Real* kappaV_in, const uint32_t* id_in, Vec4<Real>* pos_out,
                           Vec4<Real>* vel_out, Real* kappa_out, Real* kappaV_out, uint32_t* id_out, cudaStream_t s);
+// Reorders two more per-particle arrays by the same permutation (learned warm-start totals).
+template <class Real>
+void launch_reorder_pair(const uint32_t* perm, uint32_t n, const Real* a_in, const Real* b_in, Real* a_out,
+                         Real* b_out, cudaStream_t s);
 void launch_cell_bounds(const uint32_t* sorted_keys, uint32_t n, int dim_x, int dim_y, int dim_z, uint2* table,
                         cudaStream_t s);
 template <class Real>
@@ -61,20 +75,55 @@ void launch_scatter_by_id(const uint32_t* id, uint32_t n, const Real* src, int c
                           cudaStream_t s);
 
 // ---- launch wrappers (solver.cu) ------------------------------------------------------------------
-template <class Real> void launch_density_alpha(const DevState<Real>* d, uint32_t n, bool warm_v, cudaStream_t s);
-template <class Real> void launch_divergence_warm_jacobi(const DevState<Real>* d, uint32_t n, cudaStream_t s);
+// warm_v: scale kappa_v into the reference warm start; features: write the MLP inputs instead.
+template <class Real>
+void launch_density_alpha(const DevState<Real>* d, uint32_t n, bool warm_v, bool features, cudaStream_t s);
+// kw: warm-start coefficients (null = kappa_v); vout: output velocities (null = in place).
+template <class Real>
+void launch_divergence_warm_jacobi(const DevState<Real>* d, uint32_t n, const Real* kw, Vec4<Real>* vout,
+                                   cudaStream_t s);
+// Sum of the divergence (which = 0) or density (which = 1) residual of velocities `vel`, into ctl[3]
+// (no other write): the initial residual of a warm-start candidate.
+template <class Real>
+void launch_probe_residual(const DevState<Real>* d, uint32_t n, int which, const Vec4<Real>* vel, cudaStream_t s);
+// Warm-start candidates: which = 0 divergence (kappa_v), 1 pressure (kappa). Writes the plain
+// (reference) candidate to kappaVP / kappaP and, when learned, the learned one to kappa_v + kappaVW /
+// kappaW (otherwise the plain one there too).
+template <class Real>
+void launch_warm_values(const DevState<Real>* d, uint32_t n, int which, bool learned, double damping,
+                        cudaStream_t s);
+// kappaT / kappaVT = the pressure / divergence coefficients this step's solves needed: applied
+// totals (warm start + corrections) less the excess the unclamped final residuals show.
+template <class Real> void launch_totals(const DevState<Real>* d, uint32_t n, bool div_ran, cudaStream_t s);
+// Training pairs of `batch` particles spread over [0, n): x = features, t = targets
+// [(needed kappa)/r2 - kappaT_prev, (needed kappa_v)/hr - kappaVT_prev] / out_scale.
+template <class Real>
+void launch_gather_training(const DevState<Real>* d, uint32_t n, uint32_t batch, uint32_t offset, double r2, double hr,
+                            bool div_ran, float* x, float* t, cudaStream_t s);
+// keep: also store the unclamped residual in residV (learned warm start).
 template <class Real>
 void launch_divergence_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
-                                cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s);
+                                cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s, bool keep = false);
 template <class Real>
 void launch_divergence_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
                               cudaStream_t s);
 template <class Real> void launch_viscosity(const DevState<Real>* d, uint32_t n, bool cfl, cudaStream_t s);
 template <class Real> void launch_update_vel(const DevState<Real>* d, uint32_t n, cudaStream_t s);
-template <class Real> void launch_pressure_warm_jacobi(const DevState<Real>* d, uint32_t n, bool fused_vel, cudaStream_t s);
+// kw null: kappa scaled by (h/h_f)^2 and clamped (reference warm start); otherwise the given final
+// warm-start coefficients. vout: output velocities (null = in place).
+template <class Real>
+void launch_pressure_warm_jacobi(const DevState<Real>* d, uint32_t n, bool fused_vel, const Real* kw,
+                                 Vec4<Real>* vout, cudaStream_t s);
+// keep: also store the unclamped residual in resid (learned warm start).
 template <class Real>
 void launch_pressure_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
-                              cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s);
+                              cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s, bool keep = false);
+// Fallback init pass of the learned warm start (which = 0 divergence, 1 pressure): if the plain
+// candidate's probed residual (ctl[3]) is below the learned candidate's init residual, installs the
+// plain candidate and redoes the init pass; otherwise records the learned one as kept (status[2]).
+template <class Real>
+void launch_fallback_residual(const DevState<Real>* d, uint32_t n, int which, double eta, int min_it, int max_it,
+                              cudaStream_t s);
 template <class Real>
 void launch_pressure_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
                             cudaStream_t s);

@@ -65,6 +65,19 @@ __global__ void __launch_bounds__(kBlock) reorder_fluid_kernel(
     id_out[i] = id_in[j];
 }
 
+template <class Real>
+__global__ void __launch_bounds__(kBlock) reorder_pair_kernel(const uint32_t* __restrict__ perm, uint32_t n,
+                                                              const Real* __restrict__ a_in,
+                                                              const Real* __restrict__ b_in, Real* __restrict__ a_out,
+                                                              Real* __restrict__ b_out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t j = perm[i];
+    if (j >= n) j = i;
+    a_out[i] = a_in[j];
+    b_out[i] = b_in[j];
+}
+
 // Cell start/end from run boundaries of the sorted keys (replaces the dense histogram scan).
 __global__ void __launch_bounds__(kBlock) cell_bounds_kernel(const uint32_t* __restrict__ keys, uint32_t n, int dim_x,
                                                              int dim_y, int dim_z, uint2* __restrict__ table) {
@@ -238,6 +251,11 @@ void launch_reorder_fluid(const uint32_t* perm, uint32_t n, const Vec4<Real>* po
         reorder_fluid_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(perm, n, pos_in, vel_in, kappa_in, kappaV_in, id_in,
                                                                   pos_out, vel_out, kappa_out, kappaV_out, id_out);
 }
+template <class Real>
+void launch_reorder_pair(const uint32_t* perm, uint32_t n, const Real* a_in, const Real* b_in, Real* a_out,
+                         Real* b_out, cudaStream_t s) {
+    if (n) reorder_pair_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(perm, n, a_in, b_in, a_out, b_out);
+}
 void launch_cell_bounds(const uint32_t* sorted_keys, uint32_t n, int dim_x, int dim_y, int dim_z, uint2* table,
                         cudaStream_t s) {
     if (n) cell_bounds_kernel<<<grid_for(n), kBlock, 0, s>>>(sorted_keys, n, dim_x, dim_y, dim_z, table);
@@ -265,6 +283,7 @@ void launch_scatter_by_id(const uint32_t* id, uint32_t n, const Real* src, int c
                                           const R*, const uint32_t*, Vec4<R>*, Vec4<R>*, R*, R*, uint32_t*,          \
                                           cudaStream_t);                                                             \
     template void launch_build_neighbors<R>(const DevState<R>*, uint32_t, const uint2*, const uint2*, cudaStream_t); \
+    template void launch_reorder_pair<R>(const uint32_t*, uint32_t, const R*, const R*, R*, R*, cudaStream_t);       \
     template void launch_boundary_psi<R>(const Vec4<R>*, Vec4<R>*, uint32_t, const StepParams<R>&, const uint2*,     \
                                          uint32_t*, cudaStream_t);                                                   \
     template void launch_scatter_by_id<R>(const uint32_t*, uint32_t, const R*, int, int, R*, cudaStream_t);

@@ -22,6 +22,9 @@ namespace {
 template <class Real> __device__ __forceinline__ Real rmax(Real a, Real b);
 template <> __device__ __forceinline__ float rmax<float>(float a, float b) { return fmaxf(a, b); }
 template <> __device__ __forceinline__ double rmax<double>(double a, double b) { return fmax(a, b); }
+template <class Real> __device__ __forceinline__ Real rmin(Real a, Real b);
+template <> __device__ __forceinline__ float rmin<float>(float a, float b) { return fminf(a, b); }
+template <> __device__ __forceinline__ double rmin<double>(double a, double b) { return fmin(a, b); }
 
 // |v| > 1e-5 with v in float: identical to the reference's promotion of |v| to double against the
 // double literal, because no float lies strictly between 1e-5f and the next float above 1e-5.
@@ -33,21 +36,34 @@ __device__ __forceinline__ uint32_t boundary_count(uint32_t c) { return c >> 16;
 
 // Deterministic FP64 sum over the grid, then (last block) the loop decision. The partial of each
 // block is reduced in a fixed shuffle pattern and the last block adds the partials in block order.
-template <int kIsInit>
+// kAux also sums a second value (block partials after the first gridDim.x) into ctl->aux.
+template <int kIsInit, bool kAux = false>
 __device__ void reduce_and_decide(double v, double* __restrict__ partials, LoopCtl* __restrict__ ctl, uint32_t n,
                                   double eta, int min_it, int max_it, cudaGraphConditionalHandle handle,
-                                  bool use_handle) {
+                                  bool use_handle, double aux = 0.0) {
     __shared__ double warp_sums[kWarpsPerBlock];
+    __shared__ double warp_aux[kAux ? kWarpsPerBlock : 1];
     __shared__ bool is_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
-    if (lane == 0) warp_sums[warp] = v;
+    if (kAux) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) aux += __shfl_down_sync(0xFFFFFFFFu, aux, o);
+    }
+    if (lane == 0) {
+        warp_sums[warp] = v;
+        if (kAux) warp_aux[warp] = aux;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double s = 0.0;
+        double s = 0.0, a = 0.0;
         for (int w = 0; w < kWarpsPerBlock; ++w) s += warp_sums[w];
         partials[blockIdx.x] = s;
+        if (kAux) {
+            for (int w = 0; w < kWarpsPerBlock; ++w) a += warp_aux[w];
+            partials[gridDim.x + blockIdx.x] = a;
+        }
         __threadfence();
         const uint32_t t = atomicAdd(&ctl->ticket, 1u);
         is_last = (t == gridDim.x - 1);
@@ -55,16 +71,31 @@ __device__ void reduce_and_decide(double v, double* __restrict__ partials, LoopC
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    double s = 0.0;
-    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += ((volatile double*)partials)[b];
+    double s = 0.0, a = 0.0;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        s += ((volatile double*)partials)[b];
+        if (kAux) a += ((volatile double*)partials)[gridDim.x + b];
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
+    if (kAux) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xFFFFFFFFu, a, o);
+    }
     __syncthreads();
-    if (lane == 0) warp_sums[warp] = s;
+    if (lane == 0) {
+        warp_sums[warp] = s;
+        if (kAux) warp_aux[warp] = a;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         double tot = 0.0;
         for (int w = 0; w < kWarpsPerBlock; ++w) tot += warp_sums[w];
+        if (kAux) {
+            double ta = 0.0;
+            for (int w = 0; w < kWarpsPerBlock; ++w) ta += warp_aux[w];
+            ctl->aux = ta;
+        }
         const double avg = n ? tot / (double)n : 0.0;
         ctl->sum = tot;
         uint32_t cont;
@@ -113,9 +144,8 @@ __device__ __forceinline__ void load_bnbr(BNbr<Real>& b, const Vec4<Real>* __res
 template <class Real>
 __device__ __forceinline__ Real velocity_divergence(const DevState<Real>* __restrict__ ds, const StepParams<Real>& p,
                                                     uint32_t i, const Vec4<Real>& xi, const Vec4<Real>& vi,
-                                                    uint32_t nf, uint32_t nb) {
+                                                    uint32_t nf, uint32_t nb, const Vec4<Real>* __restrict__ vel) {
     const Vec4<Real>* __restrict__ pos = ds->pos;
-    const Vec4<Real>* __restrict__ vel = ds->vel;
     const uint32_t* __restrict__ nbr = ds->nbr;
     const uint32_t stride = p.nbr_stride;
     const Cubic<Real> K = p.kern;
@@ -190,8 +220,12 @@ __device__ __forceinline__ void jacobi_sum(const DevState<Real>* __restrict__ ds
 
 // ---------------------------------------------------------------------------------------------
 // density + alpha + divergence source (+ kappa_v warm-start scaling), one pass over the neighbours.
-template <class Real, bool kWarmV, bool kFeatures>
-__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+// warm_v and features are runtime flags so that every mode runs the same machine code for the
+// density and alpha arithmetic (the learned mode with a plain warm start reproduces the plain mode
+// bit for bit).
+template <class Real>
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+                                                                               bool warm_v, bool features) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
@@ -201,7 +235,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
     const uint32_t stride = p.nbr_stride;
     const Cubic<Real> K = p.kern;
 
-    if (kWarmV) ds->kappaV[i] = rmax<Real>(ds->kappaV[i] * p.h_ratio_to_past / Real(2), Real(-0.5));
+    if (warm_v) ds->kappaV[i] = rmax<Real>(ds->kappaV[i] * p.h_ratio_to_past / Real(2), Real(-0.5));
 
     const Vec4<Real> xi = pos[i];
     const Vec4<Real> vi = vel[i];
@@ -251,12 +285,11 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
     if (num < kMinNeighborsForDivergence) num += nb;
     const Real dadv = (num < kMinNeighborsForDivergence) ? Real(0) : rmax<Real>(drho.value(), Real(0));
     ds->densityAdv[i] = dadv;
-    if (kFeatures) {
-        float* f = ds->features + (size_t)i * 4;
-        f[0] = (float)(density / p.density0);
-        f[1] = (float)(dadv * alpha);
-        f[2] = (float)(nf + nb) * (1.0f / 64.0f);
-        f[3] = 0.0f;
+    if (features) {  // inputs of the warm-start MLP (mlp.cuh)
+        float4* f = reinterpret_cast<float4*>(ds->features + (size_t)i * 8);
+        f[0] = make_float4((float)(density / p.density0), (float)(dadv * alpha), (float)(nf + nb) * (1.0f / 64.0f),
+                           (float)ds->kappaT[i]);
+        f[1] = make_float4((float)ds->kappaVT[i], 0.0f, 0.0f, 0.0f);
     }
 }
 
@@ -264,12 +297,16 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
 // DFSPH_core_cuda.cu:509-512): v_i += h * sum (kv_i + kv_j) m_j grad W_ij + h kv_i sum psi_b grad W_ib.
 template <class Real>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
-                                                                        uint32_t n) {
+                                                                        uint32_t n, const Real* __restrict__ kw,
+                                                                        Vec4<Real>* __restrict__ vout) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    if (!(ds->densityAdv[i] > Real(0))) return;
+    if (!(ds->densityAdv[i] > Real(0))) {
+        if (vout) vout[i] = ds->vel[i];  // a candidate's velocity buffer holds every particle
+        return;
+    }
     const StepParams<Real>& p = ds->p;
-    const Real* __restrict__ kv = ds->kappaV;
+    const Real* __restrict__ kv = kw ? kw : ds->kappaV;
     const Real ki = kv[i];
     const Vec4<Real> xi = ds->pos[i];
     const uint32_t c = ds->counts[i];
@@ -279,38 +316,66 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_warm_jaco
     v.x += acc.x.value() * p.h;
     v.y += acc.y.value() * p.h;
     v.z += acc.z.value() * p.h;
-    ds->vel[i] = v;
+    (vout ? vout : ds->vel)[i] = v;
+}
+
+// Residual pass modes: a loop iteration, the init pass, and the fallback init pass of the learned
+// warm start (runs only if the plain candidate's probed residual, ctl[3], beat the learned
+// candidate's init residual; it then installs the plain candidate: velocities from velP, warm
+// coefficients from the plain array, and redoes the init on them).
+constexpr int kLoop = 0, kInitPass = 1, kFallback = 2;
+
+// True in every block of a fallback pass when the plain candidate is to replace the learned one:
+// when the learned candidate's sum |r| (its init pass, ctl[slot].aux) exceeds the plain one's
+// (probe, ctl[3].sum). Both sums are final before the launch; a NaN also falls back.
+template <class Real>
+__device__ __forceinline__ bool take_fallback(const DevState<Real>* __restrict__ ds, int slot, uint32_t bit) {
+    const double plain = ds->ctl[3].sum, learned = ds->ctl[slot].aux;
+    const bool fb = !(learned <= plain);
+    if (!fb && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(ds->status + 2, bit);
+    return fb;
 }
 
 // Divergence residual (computeDensityChange): rho_dot_i = max(sum m_j (v_i - v_j).grad W_ij +
 // sum psi_b (v_i - v_b).grad W_ib, 0), 0 with fewer than 20 neighbours. Also stores
-// k_i = rho_dot_i * alpha_i for the next Jacobi pass. kInit additionally zeroes kappa_v
+// k_i = rho_dot_i * alpha_i for the next Jacobi pass. The init pass additionally zeroes kappa_v
 // (DFSPH_divergence_init_kernel, :631-633).
-template <class Real, bool kInit>
+template <class Real, int kMode, bool kKeep>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_residual_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                      double eta, int min_it, int max_it,
                                                                      cudaGraphConditionalHandle handle,
                                                                      bool use_handle) {
+    if (kMode == kFallback && !take_fallback(ds, 0, 1u)) return;  // uniform over the grid
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    double contrib = 0.0;
+    const Vec4<Real>* __restrict__ vel = kMode == kFallback ? ds->velP : ds->vel;
+    double contrib = 0.0, aux = 0.0;
     if (i < n) {
         const StepParams<Real>& p = ds->p;
-        if (kInit) ds->kappaV[i] = Real(0);
+        if (kMode != kLoop) ds->kappaV[i] = Real(0);
+        if (kMode == kFallback) {
+            ds->vel[i] = vel[i];
+            ds->kappaVW[i] = ds->kappaVP[i];
+        }
         const uint32_t c = ds->counts[i];
         const uint32_t nf = fluid_count(c), nb = boundary_count(c);
         uint32_t num = nf;
         if (num < kMinNeighborsForDivergence) num += nb;
-        Real dadv = Real(0);
+        Real raw = Real(0);
         if (num >= kMinNeighborsForDivergence) {
             const Vec4<Real> xi = ds->pos[i];
-            const Vec4<Real> vi = ds->vel[i];
-            dadv = rmax<Real>(velocity_divergence<Real>(ds, p, i, xi, vi, nf, nb), Real(0));
+            const Vec4<Real> vi = vel[i];
+            raw = velocity_divergence<Real>(ds, p, i, xi, vi, nf, nb, vel);
         }
+        const Real dadv = rmax<Real>(raw, Real(0));
+        if (kKeep) ds->residV[i] = raw;  // learned warm start only
+        aux = fabs((double)raw);
         ds->densityAdv[i] = dadv;
         ds->kcoef[i] = dadv * ds->factor[i];
         contrib = (double)dadv;
     }
-    reduce_and_decide<kInit ? 1 : 0>(contrib, ds->partials, ds->ctl + 0, n, eta, min_it, max_it, handle, use_handle);
+    // The learned init pass also sums |r| (unclamped) for the fallback decision.
+    reduce_and_decide<kMode != kLoop ? 1 : 0, kKeep && kMode == kInitPass>(
+        contrib, ds->partials, ds->ctl + 0, n, eta, min_it, max_it, handle, use_handle, aux);
 }
 
 // Divergence Jacobi iteration (divergenceSolveParticle<false>): k_i = rho_dot_i alpha_i,
@@ -432,18 +497,22 @@ __global__ void __launch_bounds__(kBlock) update_vel_kernel(const DevState<Real>
 // clamped at -0.5 (update_vel, :3061-3065), computed for the neighbours on the fly.
 template <class Real, bool kFusedVel>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
-                                                                      uint32_t n) {
+                                                                      uint32_t n, const Real* __restrict__ kw,
+                                                                      Vec4<Real>* __restrict__ vout) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
-    const Real* __restrict__ kap = ds->kappa;
+    // kw given: final warm-start coefficients; otherwise the reference's kappa, scaled by
+    // (h/h_future)^2 and clamped when the velocity update is fused in (update_vel, :3061-3065).
+    const bool scale = kFusedVel && kw == nullptr;
+    const Real* __restrict__ kap = kw ? kw : ds->kappa;
     const Real r2 = p.h_ratio_to_past2;
-    const Real ki = kFusedVel ? rmax<Real>(kap[i] * r2, Real(-0.5)) : kap[i];
+    const Real ki = scale ? rmax<Real>(kap[i] * r2, Real(-0.5)) : kap[i];
     const Vec4<Real> xi = ds->pos[i];
     const uint32_t c = ds->counts[i];
     KSum3<Real> acc;
     jacobi_sum<Real>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c),
-                     [&](uint32_t j) { return kFusedVel ? rmax<Real>(kap[j] * r2, Real(-0.5)) : kap[j]; }, acc);
+                     [&](uint32_t j) { return scale ? rmax<Real>(kap[j] * r2, Real(-0.5)) : kap[j]; }, acc);
     Vec4<Real> v = ds->vel[i];
     if (kFusedVel) {
         const Vec4<Real> a = ds->acc[i];
@@ -454,41 +523,50 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_warm_jacobi
     v.x += acc.x.value() * p.h_future;
     v.y += acc.y.value() * p.h_future;
     v.z += acc.z.value() * p.h_future;
-    ds->vel[i] = v;
+    (vout ? vout : ds->vel)[i] = v;
 }
 
 // Density residual (computeDensityAdv): rho_adv_i = max(rho_i + h_f * [sum m_j (v_i - v_j).grad W_ij
 // + sum psi_b (v_i - v_b).grad W_ib] - rho0, 0); kappa_i += rho_adv_i alpha_i; k_i = rho_adv_i alpha_i.
 // kInit first scales alpha by 1/h_future and zeroes kappa (DFSPH_pressure_init_kernel, :1230-1238).
-template <class Real, bool kInit>
+template <class Real, int kMode, bool kKeep>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_residual_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                    double eta, int min_it, int max_it,
                                                                    cudaGraphConditionalHandle handle,
                                                                    bool use_handle) {
+    if (kMode == kFallback && !take_fallback(ds, 1, 2u)) return;  // uniform over the grid
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    double contrib = 0.0;
+    const Vec4<Real>* __restrict__ vel = kMode == kFallback ? ds->velP : ds->vel;
+    double contrib = 0.0, aux = 0.0;
     if (i < n) {
         const StepParams<Real>& p = ds->p;
-        Real alpha = ds->factor[i];
+        Real alpha = ds->factor[i];  // the fallback pass finds alpha already scaled by its init pass
         Real kap = Real(0);
-        if (kInit) {
+        if (kMode == kInitPass) {
             alpha *= p.inv_h_future;
             ds->factor[i] = alpha;
-        } else {
+        } else if (kMode == kLoop) {
             kap = ds->kappa[i];
+        } else {
+            ds->vel[i] = vel[i];
+            ds->kappaW[i] = ds->kappaP[i];
         }
         const Vec4<Real> xi = ds->pos[i];
-        const Vec4<Real> vi = ds->vel[i];
+        const Vec4<Real> vi = vel[i];
         const uint32_t c = ds->counts[i];
-        const Real sdiv = velocity_divergence<Real>(ds, p, i, xi, vi, fluid_count(c), boundary_count(c));
-        const Real dadv = rmax<Real>(ds->density[i] + p.h_future * sdiv, Real(0));  // density[] = rho - rho0
+        const Real sdiv = velocity_divergence<Real>(ds, p, i, xi, vi, fluid_count(c), boundary_count(c), vel);
+        const Real raw = ds->density[i] + p.h_future * sdiv;  // density[] = rho - rho0
+        const Real dadv = rmax<Real>(raw, Real(0));
+        if (kKeep) ds->resid[i] = raw;  // learned warm start only
+        aux = fabs((double)raw);
         const Real kc = dadv * alpha;
         ds->densityAdv[i] = dadv;
         ds->kcoef[i] = kc;
         ds->kappa[i] = kap + kc;
         contrib = (double)dadv;
     }
-    reduce_and_decide<kInit ? 1 : 0>(contrib, ds->partials, ds->ctl + 1, n, eta, min_it, max_it, handle, use_handle);
+    reduce_and_decide<kMode != kLoop ? 1 : 0, kKeep && kMode == kInitPass>(
+        contrib, ds->partials, ds->ctl + 1, n, eta, min_it, max_it, handle, use_handle, aux);
 }
 
 // Pressure Jacobi iteration (pressureSolveParticle<false>): v_i += h_f * [sum (k_i + k_j) m_j grad W_ij
@@ -527,22 +605,161 @@ __global__ void __launch_bounds__(kBlock) update_pos_kernel(const DevState<Real>
     ds->pos[i] = x;
 }
 
+// Initial residual of a warm-start candidate whose velocities are `vel`, as sum |r| of the unclamped
+// residuals (probe: the sum goes to ctl[3], nothing else is written). which = 0: divergence
+// (computeDensityChange), 1: density. The solver's own criterion clamps r at 0 and so cannot see an
+// over-pressured candidate (r < 0 everywhere it pushes too hard); |r| sees both directions.
+template <class Real, int kWhich>
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) probe_residual_kernel(const DevState<Real>* __restrict__ ds,
+                                                                              uint32_t n,
+                                                                              const Vec4<Real>* __restrict__ vel) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double contrib = 0.0;
+    if (i < n) {
+        const StepParams<Real>& p = ds->p;
+        const uint32_t c = ds->counts[i];
+        const uint32_t nf = fluid_count(c), nb = boundary_count(c);
+        if (kWhich == 0) {
+            uint32_t num = nf;
+            if (num < kMinNeighborsForDivergence) num += nb;
+            if (num >= kMinNeighborsForDivergence)
+                contrib = fabs((double)velocity_divergence<Real>(ds, p, i, ds->pos[i], vel[i], nf, nb, vel));
+        } else {
+            const Real sdiv = velocity_divergence<Real>(ds, p, i, ds->pos[i], vel[i], nf, nb, vel);
+            contrib = fabs((double)(ds->density[i] + p.h_future * sdiv));
+        }
+    }
+    reduce_and_decide<1>(contrib, ds->partials, ds->ctl + 3, n, 0.0, 0, 1, 0, false);
+}
+
+// Warm-start candidates (see launch_warm_values). kappa <= 0 is pressure, so min() takes the larger
+// pressure. The learned candidate raises the reference warm start to `damping` times the predicted
+// needed coefficient (the previous step's needed value plus the network's correction, scaled by the
+// dt ratio like the reference's warm start, in the reference's range [-0.5, 0]) wherever that is the
+// larger pressure, and keeps the reference warm start elsewhere. A clamped-residual Jacobi solve only
+// ever adds pressure, so from a warm start between the reference's and the needed pressure it ends
+// where the reference's solve ends (the needed pressure, or the reference warm start where that is
+// already larger); damping < 1 keeps a prediction error from overshooting the needed pressure.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) warm_values_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+                                                             int which, bool learned, Real damping) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const StepParams<Real>& p = ds->p;
+    if (which == 0) {
+        const Real plain = rmax<Real>(ds->kappaV[i] * p.h_ratio_to_past / Real(2), Real(-0.5));
+        Real use = plain;
+        if (learned) {
+            const Real corr = (Real)ds->out_scale[1] * (Real)ds->pred[2 * (size_t)i + 1];
+            const Real need = rmin<Real>(rmax<Real>((ds->kappaVT[i] + corr) * p.h_ratio_to_past, Real(-0.5)), Real(0));
+            use = rmin<Real>(plain, damping * need);
+        }
+        ds->kappaVP[i] = plain;
+        ds->kappaV[i] = use;
+        ds->kappaVW[i] = use;
+    } else {
+        const Real plain = rmax<Real>(ds->kappa[i] * p.h_ratio_to_past2, Real(-0.5));
+        Real use = plain;
+        if (learned) {
+            const Real corr = (Real)ds->out_scale[0] * (Real)ds->pred[2 * (size_t)i];
+            const Real need = rmin<Real>(rmax<Real>((ds->kappaT[i] + corr) * p.h_ratio_to_past2, Real(-0.5)), Real(0));
+            use = rmin<Real>(plain, damping * need);
+        }
+        ds->kappaP[i] = plain;
+        ds->kappaW[i] = use;
+    }
+}
+
+// Pressure each solve actually needed, per particle: the applied total (warm start + corrections)
+// less one Jacobi estimate of its excess, kept in the reference's range of coefficients [-0.5, 0]
+// (kappa <= 0 is pressure; no solve applies tension). A solve only ever adds pressure (its residuals
+// are clamped at zero), so an over-pressured warm start passes through unchanged; the unclamped
+// final residual r < 0 measures the excess and min(r, 0) * alpha removes it (alpha of the pressure
+// solve is already divided by h_future, the divergence solve's alpha is factor * h_future here).
+// Free-surface particles have r << 0 from their missing neighbours: the clamp at 0 leaves them
+// without pressure rather than under tension.
+template <class Real>
+__device__ __forceinline__ Real clamp_kappa(Real k) {
+    return rmin<Real>(rmax<Real>(k, Real(-0.5)), Real(0));
+}
+template <class Real>
+__device__ __forceinline__ void needed_totals(const DevState<Real>* __restrict__ ds, uint32_t i, bool div_ran,
+                                              Real& kt, Real& kvt) {
+    const Real f = ds->factor[i];
+    kt = clamp_kappa(ds->kappaW[i] + ds->kappa[i] + rmin<Real>(ds->resid[i], Real(0)) * f);
+    kvt = div_ran ? clamp_kappa(ds->kappaVW[i] + ds->kappaV[i] +
+                                rmin<Real>(ds->residV[i], Real(0)) * (f * ds->p.h_future))
+                  : Real(0);
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock) totals_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+                                                        bool div_ran) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Real kt, kvt;
+    needed_totals(ds, i, div_ran, kt, kvt);
+    ds->kappaT[i] = kt;
+    ds->kappaVT[i] = kvt;
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock) gather_training_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+                                                                 uint32_t batch, uint32_t offset, double r2, double hr,
+                                                                 bool div_ran, float* __restrict__ x,
+                                                                 float* __restrict__ t) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= batch) return;
+    const uint32_t i = (uint32_t)(((uint64_t)k * n / batch + offset) % n);
+    const float4* f = reinterpret_cast<const float4*>(ds->features + (size_t)i * 8);
+    reinterpret_cast<float4*>(x + (size_t)k * 8)[0] = f[0];
+    reinterpret_cast<float4*>(x + (size_t)k * 8)[1] = f[1];
+    Real kt, kvt;
+    needed_totals(ds, i, div_ran, kt, kvt);
+    const double tot = (double)kt, totv = (double)kvt;
+    t[2 * (size_t)k] = (float)((tot / r2 - (double)ds->kappaT[i]) / (double)ds->out_scale[0]);
+    t[2 * (size_t)k + 1] = (float)((totv / hr - (double)ds->kappaVT[i]) / (double)ds->out_scale[1]);
+}
+
 }  // namespace
 
-template <class Real> void launch_density_alpha(const DevState<Real>* d, uint32_t n, bool warm_v, cudaStream_t s) {
+template <class Real>
+void launch_density_alpha(const DevState<Real>* d, uint32_t n, bool warm_v, bool features, cudaStream_t s) {
     if (!n) return;
-    if (warm_v) density_alpha_kernel<Real, true, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
-    else density_alpha_kernel<Real, false, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    density_alpha_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, warm_v && !features, features);
 }
-template <class Real> void launch_divergence_warm_jacobi(const DevState<Real>* d, uint32_t n, cudaStream_t s) {
-    if (n) divergence_warm_jacobi_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n);
+template <class Real>
+void launch_divergence_warm_jacobi(const DevState<Real>* d, uint32_t n, const Real* kw, Vec4<Real>* vout,
+                                   cudaStream_t s) {
+    if (n) divergence_warm_jacobi_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, kw, vout);
+}
+template <class Real>
+void launch_probe_residual(const DevState<Real>* d, uint32_t n, int which, const Vec4<Real>* vel, cudaStream_t s) {
+    const unsigned g = grid_for(n ? n : 1);
+    if (which == 0) probe_residual_kernel<Real, 0><<<g, kBlock, 0, s>>>(d, n, vel);
+    else probe_residual_kernel<Real, 1><<<g, kBlock, 0, s>>>(d, n, vel);
+}
+template <class Real>
+void launch_warm_values(const DevState<Real>* d, uint32_t n, int which, bool learned, double damping,
+                        cudaStream_t s) {
+    if (n) warm_values_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, which, learned, (Real)damping);
+}
+template <class Real> void launch_totals(const DevState<Real>* d, uint32_t n, bool div_ran, cudaStream_t s) {
+    if (n) totals_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, div_ran);
+}
+template <class Real>
+void launch_gather_training(const DevState<Real>* d, uint32_t n, uint32_t batch, uint32_t offset, double r2, double hr,
+                            bool div_ran, float* x, float* t, cudaStream_t s) {
+    if (n && batch)
+        gather_training_kernel<Real><<<grid_for(batch), kBlock, 0, s>>>(d, n, batch, offset, r2, hr, div_ran, x, t);
 }
 template <class Real>
 void launch_divergence_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
-                                cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s) {
+                                cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s, bool keep) {
     const unsigned g = grid_for(n ? n : 1);
-    if (init) divergence_residual_kernel<Real, true><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
-    else divergence_residual_kernel<Real, false><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
+    auto k = init ? (keep ? divergence_residual_kernel<Real, kInitPass, true> : divergence_residual_kernel<Real, kInitPass, false>)
+                  : (keep ? divergence_residual_kernel<Real, kLoop, true> : divergence_residual_kernel<Real, kLoop, false>);
+    k<<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
 }
 template <class Real>
 void launch_divergence_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
@@ -558,17 +775,28 @@ template <class Real> void launch_update_vel(const DevState<Real>* d, uint32_t n
     if (n) update_vel_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n);
 }
 template <class Real>
-void launch_pressure_warm_jacobi(const DevState<Real>* d, uint32_t n, bool fused_vel, cudaStream_t s) {
+void launch_pressure_warm_jacobi(const DevState<Real>* d, uint32_t n, bool fused_vel, const Real* kw,
+                                 Vec4<Real>* vout, cudaStream_t s) {
     if (!n) return;
-    if (fused_vel) pressure_warm_jacobi_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n);
-    else pressure_warm_jacobi_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    if (fused_vel) pressure_warm_jacobi_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n, kw, vout);
+    else pressure_warm_jacobi_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n, kw, vout);
 }
 template <class Real>
 void launch_pressure_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
-                              cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s) {
+                              cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s, bool keep) {
     const unsigned g = grid_for(n ? n : 1);
-    if (init) pressure_residual_kernel<Real, true><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
-    else pressure_residual_kernel<Real, false><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
+    auto k = init ? (keep ? pressure_residual_kernel<Real, kInitPass, true> : pressure_residual_kernel<Real, kInitPass, false>)
+                  : (keep ? pressure_residual_kernel<Real, kLoop, true> : pressure_residual_kernel<Real, kLoop, false>);
+    k<<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
+}
+template <class Real>
+void launch_fallback_residual(const DevState<Real>* d, uint32_t n, int which, double eta, int min_it, int max_it,
+                              cudaStream_t s) {
+    const unsigned g = grid_for(n ? n : 1);
+    if (which == 0)
+        divergence_residual_kernel<Real, kFallback, true><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, 0, false);
+    else
+        pressure_residual_kernel<Real, kFallback, true><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, 0, false);
 }
 template <class Real>
 void launch_pressure_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
@@ -583,17 +811,24 @@ template <class Real> void launch_cfl_reduce(const DevState<Real>* d, uint32_t n
 }
 
 #define DFSPH_INSTANTIATE_SOLVER(R)                                                                                  \
-    template void launch_density_alpha<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                        \
-    template void launch_divergence_warm_jacobi<R>(const DevState<R>*, uint32_t, cudaStream_t);                     \
+    template void launch_density_alpha<R>(const DevState<R>*, uint32_t, bool, bool, cudaStream_t);                  \
+    template void launch_divergence_warm_jacobi<R>(const DevState<R>*, uint32_t, const R*, Vec4<R>*, cudaStream_t); \
+    template void launch_probe_residual<R>(const DevState<R>*, uint32_t, int, const Vec4<R>*, cudaStream_t);        \
+    template void launch_warm_values<R>(const DevState<R>*, uint32_t, int, bool, double, cudaStream_t);             \
+    template void launch_totals<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                               \
+    template void launch_gather_training<R>(const DevState<R>*, uint32_t, uint32_t, uint32_t, double, double, bool, \
+                                            float*, float*, cudaStream_t);                                           \
     template void launch_divergence_residual<R>(const DevState<R>*, uint32_t, bool, double, int, int,               \
-                                                cudaGraphConditionalHandle, bool, cudaStream_t);                     \
+                                                cudaGraphConditionalHandle, bool, cudaStream_t, bool);               \
     template void launch_divergence_jacobi<R>(const DevState<R>*, uint32_t, cudaGraphConditionalHandle, bool,       \
                                               cudaStream_t);                                                         \
     template void launch_viscosity<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                            \
     template void launch_update_vel<R>(const DevState<R>*, uint32_t, cudaStream_t);                                 \
-    template void launch_pressure_warm_jacobi<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                 \
+    template void launch_pressure_warm_jacobi<R>(const DevState<R>*, uint32_t, bool, const R*, Vec4<R>*,            \
+                                                 cudaStream_t);                                                      \
     template void launch_pressure_residual<R>(const DevState<R>*, uint32_t, bool, double, int, int,                 \
-                                              cudaGraphConditionalHandle, bool, cudaStream_t);                       \
+                                              cudaGraphConditionalHandle, bool, cudaStream_t, bool);                 \
+    template void launch_fallback_residual<R>(const DevState<R>*, uint32_t, int, double, int, int, cudaStream_t);   \
     template void launch_pressure_jacobi<R>(const DevState<R>*, uint32_t, cudaGraphConditionalHandle, bool,         \
                                             cudaStream_t);                                                           \
     template void launch_update_pos<R>(const DevState<R>*, uint32_t, cudaStream_t);                                 \

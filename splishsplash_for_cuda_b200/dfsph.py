@@ -288,3 +288,70 @@ class DFSPHCUDA:
         x = np.ascontiguousarray(positions, dtype=np.float32)
         v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32)
         self._call(self._lib.dfsph_move_boundary(self._ctx, _fptr(x), _fptr(v)))
+
+    # ---- learned warm start (no reference counterpart) ------------------------------------------
+    def set_learned_warm_start(self, on: bool = True, probe: bool = True, train_interval: int | None = None,
+                               train_iters: int | None = None, train_batch: int | None = None,
+                               learning_rate: float | None = None) -> None:
+        """Switches the MLP warm start of both solvers on or off (step() only). With probe, each solve
+        keeps the learned candidate only if its initial residual is not above the reference warm
+        start's. The network trains online every `train_interval` steps."""
+        for key, val in (("train_interval", train_interval), ("train_iters", train_iters),
+                         ("train_batch", train_batch), ("learning_rate", learning_rate)):
+            if val is not None:
+                self.set_param(key, val)
+        self.set_param("warm_start_probe", 1 if probe else 0)
+        self.set_param("learned_warm_start", 1 if on else 0)
+
+    def mlp_params(self) -> np.ndarray:
+        out = np.empty(_capi.MLP_PARAMS, dtype=np.float32)
+        self._call(self._lib.dfsph_mlp_get_params(self._ctx, _fptr(out), out.size))
+        return out
+
+    def set_mlp_params(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float32).ravel()
+        self._call(self._lib.dfsph_mlp_set_params(self._ctx, _fptr(p), p.size))
+
+    def mlp_scales(self) -> tuple[np.ndarray, np.ndarray]:
+        a = np.empty(_capi.MLP_INPUTS, dtype=np.float32)
+        b = np.empty(_capi.MLP_OUTPUTS, dtype=np.float32)
+        self._call(self._lib.dfsph_mlp_get_scales(self._ctx, _fptr(a), _fptr(b)))
+        return a, b
+
+    def set_mlp_scales(self, in_scale: np.ndarray, out_scale: np.ndarray) -> None:
+        a = np.ascontiguousarray(in_scale, dtype=np.float32)
+        b = np.ascontiguousarray(out_scale, dtype=np.float32)
+        if a.size != _capi.MLP_INPUTS or b.size != _capi.MLP_OUTPUTS:
+            raise ValueError("scales need 8 input and 2 output entries")
+        self._call(self._lib.dfsph_mlp_set_scales(self._ctx, _fptr(a), _fptr(b)))
+
+    def mlp_forward(self, x: np.ndarray) -> np.ndarray:
+        """Network outputs of samples x[n, 8] through the tensor-core inference path."""
+        xs = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, _capi.MLP_INPUTS)
+        y = np.empty((xs.shape[0], _capi.MLP_OUTPUTS), dtype=np.float32)
+        self._call(self._lib.dfsph_mlp_forward(self._ctx, _fptr(xs), xs.shape[0], _fptr(y)))
+        return y
+
+    def mlp_gradient(self, x: np.ndarray, t: np.ndarray) -> tuple[np.ndarray, float]:
+        xs = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, _capi.MLP_INPUTS)
+        ts = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, _capi.MLP_OUTPUTS)
+        if xs.shape[0] != ts.shape[0]:
+            raise ValueError("inputs and targets differ in length")
+        g = np.empty(_capi.MLP_PARAMS, dtype=np.float32)
+        loss = C.c_double()
+        self._call(self._lib.dfsph_mlp_gradient(self._ctx, _fptr(xs), _fptr(ts), xs.shape[0], _fptr(g),
+                                                C.byref(loss)))
+        return g, float(loss.value)
+
+    def mlp_train(self, x: np.ndarray, t: np.ndarray, iters: int, learning_rate: float = 1e-3) -> float:
+        xs = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, _capi.MLP_INPUTS)
+        ts = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, _capi.MLP_OUTPUTS)
+        if xs.shape[0] != ts.shape[0]:
+            raise ValueError("inputs and targets differ in length")
+        loss = C.c_double()
+        self._call(self._lib.dfsph_mlp_train(self._ctx, _fptr(xs), _fptr(ts), xs.shape[0], int(iters),
+                                             float(learning_rate), C.byref(loss)))
+        return float(loss.value)
+
+    def mlp_reset(self, seed: int = 1234567) -> None:
+        self._call(self._lib.dfsph_mlp_reset(self._ctx, int(seed)))

@@ -43,7 +43,7 @@ def test_struct_sizes_match_header(cuda_lib):
     # by compiling a probe would need a compiler at test time, so check the ctypes size is the
     # natural C size of the declared field sequence.
     assert C.sizeof(_capi.DfsphScene) % 8 == 0
-    assert C.sizeof(_capi.DfsphStepStats) == 56
+    assert C.sizeof(_capi.DfsphStepStats) == 64
 
 
 def test_create_without_gpu_fails_loudly(cuda_lib):

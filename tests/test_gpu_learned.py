@@ -1,0 +1,176 @@
+"""GPU tests of the learned warm start: the network kernels against the FP64 restatement in
+oracle/mlp_oracle.py (gradient, Adam, initialisation, tensor-core inference), the fallback to the
+reference warm start, and the ablation on a stiff workload (a resting 10 x 40 x 10 column).
+
+Bars: gradient within 1e-4 (relative, per parameter block) of the FP64 gradient, the FP32
+accumulation over up to 4096 samples being the only difference; Adam updates within 2 % of the
+learning rate per parameter; inference within 2e-3 (relative to the output norm) of the same
+arithmetic with BF16 inputs, weights and activations, and within 3e-2 of FP64; initialisation
+bit-exact."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+from splishsplash_for_cuda_b200 import _capi
+from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
+from splishsplash_for_cuda_b200.scene import column_scene, synthetic_scene
+
+pytestmark = pytest.mark.gpu
+
+
+def _net():
+    return DFSPHCUDA(synthetic_scene(1, counts=(6, 6, 6)))
+
+
+def _case(n, seed=0, pscale=0.3):
+    rng = np.random.default_rng(seed)
+    p = (rng.normal(size=M.N_PARAMS) * pscale).astype(np.float32)
+    s = rng.uniform(0.5, 2.0, size=M.N_IN).astype(np.float32)
+    x = rng.normal(size=(n, M.N_IN)).astype(np.float32)
+    x[:, 5:] = 0.0
+    t = rng.normal(size=(n, M.N_OUT)).astype(np.float32)
+    return p, s, x, t
+
+
+BLOCKS = [(M.W1, M.B1), (M.B1, M.W2), (M.W2, M.B2), (M.B2, M.W3), (M.W3, M.B3), (M.B3, M.N_PARAMS)]
+
+
+def test_mlp_init_matches_oracle(cuda_lib):
+    d = _net()
+    for seed in (1, 99):
+        d.mlp_reset(seed)
+        assert np.array_equal(d.mlp_params(), M.init_params(seed))
+    assert d.get_param("mlp_ready") == 0
+
+
+@pytest.mark.parametrize("n", [1, 127, 1000, 4096])
+def test_mlp_gradient_matches_oracle(cuda_lib, n):
+    p, s, x, t = _case(n, seed=n)
+    d = _net()
+    d.set_mlp_params(p)
+    d.set_mlp_scales(s, np.ones(2, np.float32))
+    g, loss = d.mlp_gradient(x, t)
+    lo, go = M.loss_and_grad(p, s, x, t)
+    assert abs(loss - lo) <= 1e-5 * lo
+    for a, b in BLOCKS:
+        ref = go[a:b]
+        err = np.linalg.norm(g[a:b] - ref) / max(np.linalg.norm(ref), 1e-30)
+        assert err < 1e-4, (a, b, err)
+
+
+def test_mlp_adam_matches_oracle(cuda_lib):
+    p, s, x, t = _case(1000, seed=5)
+    d = _net()
+    d.set_mlp_params(p)
+    d.set_mlp_scales(s, np.ones(2, np.float32))
+    lr = 1e-3
+    d.mlp_train(x, t, iters=3, learning_rate=lr)
+    got = d.mlp_params().astype(np.float64)
+    q, m, v = p.astype(np.float64), np.zeros(M.N_PARAMS), np.zeros(M.N_PARAMS)
+    for k in range(1, 4):
+        _, g = M.loss_and_grad(q.astype(np.float32), s, x, t)
+        q, m, v = M.adam(q, m, v, g, lr, k)
+    assert np.abs(got - q).max() <= 0.02 * lr
+    moved = got - p
+    assert np.linalg.norm(moved - (q - p)) <= 1e-2 * np.linalg.norm(q - p)
+
+
+@pytest.mark.parametrize("n", [16, 1000, 65536])
+def test_mlp_tensor_core_forward(cuda_lib, n):
+    p, s, x, _ = _case(n, seed=11)
+    d = _net()
+    d.set_mlp_params(p)
+    d.set_mlp_scales(s, np.ones(2, np.float32))
+    y = d.mlp_forward(x)
+    yb = M.forward_bf16(p, s, x)
+    y64 = M.forward(p, s, x)
+    assert np.linalg.norm(y - yb) <= 2e-3 * np.linalg.norm(yb)
+    assert np.linalg.norm(y - y64) <= 3e-2 * np.linalg.norm(y64)
+
+
+def test_mlp_training_reduces_loss(cuda_lib):
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=(4096, M.N_IN)).astype(np.float32)
+    x[:, 5:] = 0
+    t = np.stack([np.tanh(x[:, 0] - 0.5 * x[:, 3]), 0.3 * x[:, 1] * x[:, 4]], axis=1).astype(np.float32)
+    d = _net()
+    d.mlp_reset(4)
+    _, l0 = d.mlp_gradient(x, t)
+    d.mlp_train(x, t, iters=300, learning_rate=3e-3)
+    _, l1 = d.mlp_gradient(x, t)
+    assert l1 < 0.2 * l0
+
+
+def _run(scene, steps, learned, **kw):
+    d = DFSPHCUDA(scene)
+    if learned:
+        d.set_learned_warm_start(True, **kw)
+    its, itv, warm, st_bits = [], [], [], 0
+    for _ in range(steps):
+        st = d.step()
+        its.append(st.iterations)
+        itv.append(st.iterations_v)
+        warm.append(st.warm_start)
+        st_bits |= st.status
+    return d, np.array(its), np.array(itv), np.array(warm), st_bits
+
+
+def test_learned_mode_is_plain_before_training(cuda_lib):
+    """With no trained network the learned mode runs the reference warm start: bit-identical states."""
+    s = column_scene(counts=(8, 20, 8), time_step=0.002)
+    a, ia, va, _, _ = _run(s, 30, False)
+    b, ib, vb, wb, _ = _run(s, 30, True, train_interval=0)
+    assert np.array_equal(ia, ib) and np.array_equal(va, vb) and not wb.any()
+    assert np.array_equal(a.positions(), b.positions())
+    assert np.array_equal(a.velocities(), b.velocities())
+
+
+def test_fallback_restores_reference_warm_start(cuda_lib):
+    """A network that predicts the largest pressure everywhere loses every probe once the fluid
+    settles (its over-pressure shows as expansion, r < 0, in sum |r|): the step falls back to the
+    reference warm start and the states stay bit-identical to the plain mode. (A candidate can tie
+    the plain one, e.g. a divergence candidate while no particle has a positive source, or before
+    any contact with the floor: the tie keeps the learned one, which then changes nothing.)"""
+    s = column_scene(counts=(8, 20, 8), time_step=0.002)
+    a, ia, va, _, _ = _run(s, 30, False)
+    d = DFSPHCUDA(s)
+    d.set_learned_warm_start(True, train_interval=0)
+    p = np.zeros(M.N_PARAMS, np.float32)
+    p[M.B3:] = -50.0
+    d.set_mlp_params(p)
+    d.set_mlp_scales(np.ones(8, np.float32), np.ones(2, np.float32))
+    ib, vb = [], []
+    for _ in range(30):
+        st = d.step()
+        ib.append(st.iterations)
+        vb.append(st.iterations_v)
+        assert st.warm_start & 2 == 0
+    assert d.get_param("learned_solves_p") == 30 and d.get_param("learned_kept_p") == 0
+    assert d.get_param("learned_solves_v") == 30
+    assert np.array_equal(ia, ib) and np.array_equal(va, vb)
+    assert np.array_equal(a.positions(), d.positions())
+
+
+def test_learned_warm_start_cuts_iterations_on_stiff_column(cuda_lib):
+    """Ablation: same scene, same tolerance, reference warm start vs learned warm start. Both solve
+    every step to the tolerance; after the column settles the learned one needs >= 30 % fewer
+    pressure iterations."""
+    s = column_scene(counts=(10, 40, 10), time_step=0.002, max_error=0.01)
+    steps = 300
+    p, ip, vp, _, bits_p = _run(s, steps, False)
+    d, il, vl, wl, bits_l = _run(s, steps, True, train_interval=25)
+    assert bits_l & (_capi.ST_PRESSURE_NOT_CONVERGED | _capi.ST_NONFINITE) == 0
+    assert np.isfinite(d.positions()).all()
+    win = slice(150, steps)
+    mp, ml = ip[win].mean(), il[win].mean()
+    print(f"pressure iterations plain {mp:.2f} learned {ml:.2f}; divergence {vp[win].mean():.2f} "
+          f"{vl[win].mean():.2f}; learned kept p {d.get_param('learned_kept_p'):.0f}/"
+          f"{d.get_param('learned_solves_p'):.0f} v {d.get_param('learned_kept_v'):.0f}/"
+          f"{d.get_param('learned_solves_v'):.0f}; trainings {d.get_param('mlp_trainings'):.0f} "
+          f"loss {d.get_param('mlp_loss'):.3g}")
+    assert ml <= 0.7 * mp
+    assert d.get_param("mlp_trainings") >= 10
+    # Same fluid: mean density and the column top within a few percent of the plain run.
+    rp, rl = p.field("density").astype(np.float64), d.field("density").astype(np.float64)
+    assert abs(rl.mean() - rp.mean()) <= 0.05 * rp.mean()
+    assert abs(d.positions()[:, 1].max() - p.positions()[:, 1].max()) <= 0.25 * p.positions()[:, 1].max()
