@@ -217,6 +217,47 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def learned_ablation(local, steps: int, counts=(40, 40, 40)):
+    """Plain vs learned warm start on a stiff workload: a resting column (40 particles high) at the
+    reference's default 0.01 % tolerance. Both runs take `steps` steps from the same state; the
+    second half is measured (the column has settled by then). ms/step is the device time of each
+    step (CUDA events inside dfsph_step), online training rounds included."""
+    from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
+    from splishsplash_for_cuda_b200.scene import column_scene
+
+    scene = column_scene(counts=counts, time_step=0.002, max_error=0.01)
+    out = {"workload": scene.name, "fluid_particles": scene.n_fluid, "steps": steps,
+           "measured_steps": f"{steps // 2}..{steps - 1}", "max_error_pct": 0.01}
+    for mode in ("plain", "learned"):
+        d = DFSPHCUDA(scene, device=local)
+        d.set_param("timing", 1)
+        if mode == "learned":
+            d.set_learned_warm_start(True)
+        its, itv, ms, bits = [], [], [], 0
+        for _ in range(steps):
+            st = d.step()
+            its.append(st.iterations)
+            itv.append(st.iterations_v)
+            ms.append(st.ms_total)
+            bits |= st.status
+        w = slice(steps // 2, steps)
+        rec = {"pressure_iterations": round(float(np.mean(its[w])), 2),
+               "divergence_iterations": round(float(np.mean(itv[w])), 2),
+               "ms_per_step": round(float(np.mean(ms[w])), 4), "status_bits": int(bits)}
+        if mode == "learned":
+            rec.update(trainings=int(d.get_param("mlp_trainings")),
+                       kept_pressure=int(d.get_param("learned_kept_p")),
+                       solves_pressure=int(d.get_param("learned_solves_p")),
+                       kept_divergence=int(d.get_param("learned_kept_v")),
+                       damping=d.get_param("warm_start_damping"))
+        out[mode] = rec
+        d.close()
+    out["pressure_iteration_reduction"] = round(1 - out["learned"]["pressure_iterations"]
+                                                / out["plain"]["pressure_iterations"], 4)
+    out["ms_per_step_reduction"] = round(1 - out["learned"]["ms_per_step"] / out["plain"]["ms_per_step"], 4)
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -315,6 +356,10 @@ def run_ours(args, world, rank, local):
         cpu = {"value": round(ms_cpu, 2), "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"{done} steps (after 1 warm-up) of {scene.name}, {args.cpu_budget:.0f} s budget"}
 
+    ablation = None
+    if rank == 0 and world == 1 and args.ablation_steps > 0:
+        ablation = learned_ablation(local, args.ablation_steps)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(ms, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -337,6 +382,7 @@ def run_ours(args, world, rank, local):
             "mean_neighbors": {"fluid": round(nf, 2), "boundary": round(nbn, 2)},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "learned_warm_start": ablation,
         }
         print(json.dumps(line), flush=True)
     d.close()
@@ -354,6 +400,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ablation-steps", type=int, default=300,
+                    help="steps per mode of the plain vs learned warm-start comparison (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -209,11 +209,36 @@ template <class Real> struct Cubic {
 #define DFSPH_GATHER_BATCH 4
 #endif
 constexpr int kGatherBatch = DFSPH_GATHER_BATCH;
+#ifndef DFSPH_PREFETCH_IDX
+#define DFSPH_PREFETCH_IDX 1
+#endif
 constexpr uint32_t kNoNeighbor = 0xFFFFFFFFu;
 
 template <int B, class Load, class Use>
 __device__ __forceinline__ void visit_neighbors(const uint32_t* __restrict__ nbr, uint32_t stride, uint32_t i,
                                                 uint32_t k0, uint32_t k1, uint32_t fallback, Load&& load, Use&& use) {
+#if DFSPH_PREFETCH_IDX
+    // The index loads of the next batch are issued before the gathers of this one, so that their
+    // latency (a coalesced stream, usually from DRAM) overlaps the dependent gathers.
+    uint32_t jj[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) jj[u] = (k0 + u) < k1 ? __ldg(nbr + (size_t)(k0 + u) * stride + i) : kNoNeighbor;
+    for (uint32_t kb = k0; kb < k1; kb += B) {
+        uint32_t jn[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const uint32_t k = kb + B + u;
+            jn[u] = k < k1 ? __ldg(nbr + (size_t)k * stride + i) : kNoNeighbor;
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u) load(u, jj[u] == kNoNeighbor ? fallback : jj[u]);
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            if (kb + u < k1) use(u);
+#pragma unroll
+        for (int u = 0; u < B; ++u) jj[u] = jn[u];
+    }
+#else
     for (uint32_t kb = k0; kb < k1; kb += B) {
         uint32_t jj[B];
 #pragma unroll
@@ -227,6 +252,7 @@ __device__ __forceinline__ void visit_neighbors(const uint32_t* __restrict__ nbr
         for (int u = 0; u < B; ++u)
             if (kb + u < k1) use(u);
     }
+#endif
 }
 
 // ---------------------------------------------------------------------------------------------
