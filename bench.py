@@ -217,9 +217,9 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def learned_ablation(local, steps: int, counts=(40, 40, 40)):
-    """Plain vs learned warm start on a stiff workload: a resting column (40 particles high) at the
-    reference's default 0.01 % tolerance. Both runs take `steps` steps from the same state; the
+def learned_ablation(local, steps: int, counts=(64, 64, 64)):
+    """Plain vs learned warm start on a stiff workload: a resting column (64 x 64 x 64 = 262,144
+    particles, 64 high, r = 0.008 m, fixed dt 2 ms) at the reference's default 0.01 % tolerance. Both runs take `steps` steps from the same state; the
     second half is measured (the column has settled by then). ms/step is the device time of each
     step (CUDA events inside dfsph_step), online training rounds included."""
     from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
