@@ -187,6 +187,14 @@ class Oracle:
                                      None if v is None else v.ctypes.data_as(C.POINTER(C.c_double)))
 
     # piecewise phases
+    def move_boundary(self, xyz: np.ndarray, vxyz: np.ndarray | None = None) -> None:
+        """New boundary positions (and velocities) in upload order; psi is kept."""
+        x = np.ascontiguousarray(xyz, dtype=np.float32)
+        v = None if vxyz is None else np.ascontiguousarray(vxyz, dtype=np.float32)
+        self._moved = (x, v)
+        if self.lib.oracle_set_boundary_velocity(self.h, _f(x), _f(v)) != 0:
+            raise RuntimeError("oracle_set_boundary_velocity failed")
+
     def divergence_solve(self, max_iter=None, max_error=None) -> int:
         c = self.scene.config
         return self.lib.oracle_divergence_solve(self.h, c.maxIterationsV if max_iter is None else max_iter,

@@ -222,3 +222,64 @@ def test_field_download_orders_and_dtypes():
     assert np.array_equal(xs, d.positions()[ids_sorted])
     m = d.field("mass")
     assert np.allclose(m, 0.8 * 1000 * (2 * s.config.particleRadius) ** 3)
+
+
+def test_moving_boundary_lockstep_with_oracle():
+    """Walls translated each step with their velocity (the boundary velocity enters rho_dot and
+    rho_adv, psi is kept): FP32 kernels vs FP64 oracle over five steps."""
+    s = synthetic_scene(1, counts=(12, 12, 12))
+    d = DFSPHCUDA(s)
+    o = Oracle(s, 64)
+    b0 = s.boundary.astype(np.float64)
+    vel = np.zeros_like(b0)
+    vel[:, 0] = 0.2 * np.sign(b0[:, 0] - b0[:, 0].mean())  # the two x walls move apart
+    t = 0.0
+    for k in range(5):
+        bx = (b0 + vel * t).astype(np.float32)
+        bv = vel.astype(np.float32)
+        d.move_boundary(bx, bv)
+        o.move_boundary(bx, bv)
+        st = d.step()
+        ro = o.step()
+        assert st.iterations == ro["iterations"] and st.iterations_v == ro["iterations_v"], k
+        t += st.h
+    for name in ["position", "velocity", "density"]:
+        check_field(name, d.field(name, np.float64), o.field(name), 1e-4)
+
+
+def test_empty_and_single_particle_fluid():
+    s = synthetic_scene(1, counts=(4, 4, 4))
+    d = DFSPHCUDA(s)
+    d.reset()
+    from splishsplash_for_cuda_b200.scene import Scene
+    empty = Scene(config=s.config, fluid=np.zeros((0, 3), np.float32), boundary=s.boundary)
+    e = DFSPHCUDA(empty, fluid_capacity=16)
+    st = e.step()
+    assert st.num_fluid == 0 and st.iterations == 0 and st.status == 0
+    one = Scene(config=s.config, fluid=s.fluid[:1].copy(), boundary=s.boundary)
+    g = DFSPHCUDA(one)
+    o = Oracle(one, 64)
+    for _ in range(3):
+        sg, so = g.step(), o.step()
+        assert sg.iterations == so["iterations"]
+    check_field("position", g.field("position", np.float64), o.field("position"), 1e-6)
+
+
+def test_thousand_steps_bounded_drift():
+    """1000 CFL steps of the 27k dam break: FP32 build vs FP64 build of the same kernels. The flow
+    is chaotic, so particle-wise agreement is not expected; the aggregate state must stay close:
+    every solve converges, no particle escapes, the centres of mass agree within 1 % of the box
+    height and the kinetic energies within 10 % (measured: 0.25 % and 3.3 % after 1000 steps)."""
+    s = synthetic_scene(1, cfl=True)
+    a, b = DFSPHCUDA(s, precision=32), DFSPHCUDA(s, precision=64)
+    bits = 0
+    for _ in range(1000):
+        bits |= a.step().status
+        b.step()
+    assert bits & (_capi.ST_ESCAPED | _capi.ST_NONFINITE | _capi.ST_PRESSURE_NOT_CONVERGED) == 0
+    xa, xb = a.positions().astype(np.float64), b.positions().astype(np.float64)
+    va, vb = a.velocities().astype(np.float64), b.velocities().astype(np.float64)
+    span = float(np.ptp(s.boundary[:, 1]))
+    assert np.abs(xa.mean(0) - xb.mean(0)).max() <= 0.01 * span
+    ka, kb = (va ** 2).sum(1).mean(), (vb ** 2).sum(1).mean()
+    assert abs(ka - kb) <= 0.1 * max(ka, kb)
