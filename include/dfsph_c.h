@@ -107,7 +107,8 @@ enum dfsph_field {
     DFSPH_F_ID = 9,         /* 1 (uint32 in a float/double container is not allowed: use dtype 2) */
     DFSPH_F_BOUNDARY_PSI = 10,      /* 1 per boundary particle: Akinci psi (boundary "mass")      */
     DFSPH_F_BOUNDARY_POSITION = 11, /* 3 per boundary particle                                     */
-    DFSPH_F_NEIGHBOR_COUNTS = 12    /* 2 per fluid particle: fluid count, boundary count (dtype 2)  */
+    DFSPH_F_NEIGHBOR_COUNTS = 12,   /* 2 per fluid particle: fluid count, boundary count (dtype 2)  */
+    DFSPH_F_BOUNDARY_VELOCITY = 13  /* 3 per boundary particle (zero for a static boundary)         */
 };
 #define DFSPH_DTYPE_F32 0
 #define DFSPH_DTYPE_F64 1
@@ -238,6 +239,22 @@ enum dfsph_kernel_id {
  * Jacobi kernels move velocities), so call it only when the simulation will not continue, e.g. at
  * the end of a benchmark. */
 int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launch);
+
+/* ---- snapshots in the reference's text format ----------------------------------------------------
+ * DFSPHCUDA::handleSimulationSave / handleSimulationLoad (SPlisHSPlasH/DFSPH/DFSPH_CUDA.cpp:1885-1979)
+ * with UnifiedParticleSet::write_to_file / load_from_file (DFSPH_c_arrays_structure.cpp:424-600):
+ * dir/fluid_file.txt and dir/boundaries_file.txt hold a header line "N has_factor_computation
+ * velocity_impacted_by_fluid_solver is_dynamic_object" ("N 1 1 0" for the fluid, "N 0 0 0" for a
+ * static boundary) and one line "mass x y z vx vy vz" per particle (the boundary's mass column is its
+ * psi); dir/general_data.txt holds the time step. Values are written with 9 significant digits (the
+ * reference writes 6; both read either). Loading a boundary recomputes psi, as the reference does
+ * (computeRigidBodiesParticlesMass); loading the fluid sets h = h_future = h_past to the stored step
+ * and clears the warm starts (the format does not hold them). what: DFSPH_SNAP_FLUID |
+ * DFSPH_SNAP_BOUNDARY. dir must exist. */
+#define DFSPH_SNAP_FLUID 1
+#define DFSPH_SNAP_BOUNDARY 2
+int dfsph_save_snapshot(dfsph_ctx* ctx, const char* dir, int what);
+int dfsph_load_snapshot(dfsph_ctx* ctx, const char* dir, int what, int load_velocities);
 
 /* ---- learned warm-start network (no reference counterpart) -------------------------------------
  * A per-particle MLP, inputs x[8] = [(rho - rho0)/rho0, rho_dot * alpha, neighbours / 64,

@@ -39,6 +39,7 @@ FIELDS = {
     "boundary_psi": (10, 1),
     "boundary_position": (11, 3),
     "neighbor_counts": (12, 2),
+    "boundary_velocity": (13, 3),
 }
 DTYPE_F32, DTYPE_F64, DTYPE_U32 = 0, 1, 2
 ORDER_ID, ORDER_SORTED = 0, 1
@@ -120,6 +121,8 @@ SIGNATURES = {
     "dfsph_launch_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "dfsph_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "dfsph_time_kernel": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "dfsph_save_snapshot": (C.c_int, [_P, C.c_char_p, C.c_int]),
+    "dfsph_load_snapshot": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int]),
     "dfsph_mlp_get_params": (C.c_int, [_P, _F, C.c_size_t]),
     "dfsph_mlp_set_params": (C.c_int, [_P, _F, C.c_size_t]),
     "dfsph_mlp_get_scales": (C.c_int, [_P, _F, _F]),
@@ -132,6 +135,7 @@ SIGNATURES = {
 }
 
 MLP_INPUTS, MLP_OUTPUTS, MLP_PARAMS = 8, 2, 4866
+SNAP_FLUID, SNAP_BOUNDARY = 1, 2
 
 NOALLOC_MAX_KEYS = 1 << 18
 

@@ -11,7 +11,10 @@
 #include <cstdio>
 #include <cstddef>
 #include <cstring>
+#include <fstream>
+#include <iomanip>
 #include <memory>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -1085,6 +1088,10 @@ public:
                 src = (const Real*)bpos[0]; sstride = 4; comps = 3; count = nb;
                 idmap = (order == DFSPH_ORDER_ID) ? bid : nullptr;
                 break;
+            case DFSPH_F_BOUNDARY_VELOCITY:
+                src = (const Real*)bvel[0]; sstride = 4; comps = 3; count = nb;
+                idmap = (order == DFSPH_ORDER_ID) ? bid : nullptr;
+                break;
             case DFSPH_F_ID:
             case DFSPH_F_NEIGHBOR_COUNTS: {
                 DF_CHECK(dtype == DFSPH_DTYPE_U32, DFSPH_E_INVALID, "id and neighbour counts download as u32");
@@ -1113,6 +1120,98 @@ public:
                 for (uint32_t i = 0; i < count; ++i) ((float*)out)[i] = (float)(sc.density0 + ((float*)out)[i]);
             else
                 for (uint32_t i = 0; i < count; ++i) ((double*)out)[i] = sc.density0 + ((double*)out)[i];
+        }
+        return DFSPH_OK;
+    }
+
+    // ---- snapshots (reference text format, see dfsph_c.h) -----------------------------------------
+    static std::string join(const char* dir, const char* name) {
+        std::string d(dir);
+        if (!d.empty() && d.back() != '/') d += '/';
+        return d + name;
+    }
+
+    int write_set(const std::string& path, bool boundary) {
+        const uint32_t count = boundary ? nb : n;
+        std::vector<float> x((size_t)count * 3), v((size_t)count * 3), m(count);
+        if (count) {
+            DF_TRY(download(boundary ? DFSPH_F_BOUNDARY_POSITION : DFSPH_F_POSITION, DFSPH_DTYPE_F32, x.data(),
+                            x.size(), DFSPH_ORDER_ID));
+            DF_TRY(download(boundary ? DFSPH_F_BOUNDARY_VELOCITY : DFSPH_F_VELOCITY, DFSPH_DTYPE_F32, v.data(),
+                            v.size(), DFSPH_ORDER_ID));
+            DF_TRY(download(boundary ? DFSPH_F_BOUNDARY_PSI : DFSPH_F_MASS, DFSPH_DTYPE_F32, m.data(), m.size(),
+                            DFSPH_ORDER_ID));
+        }
+        std::ofstream f(path, std::ios::trunc);
+        DF_CHECK(f.is_open(), DFSPH_E_INVALID, "cannot open " + path + " for writing");
+        f << std::setprecision(9);
+        f << count << (boundary ? " 0 0 0" : " 1 1 0") << "\n";
+        for (uint32_t i = 0; i < count; ++i)
+            f << m[i] << " " << x[3 * i] << " " << x[3 * i + 1] << " " << x[3 * i + 2] << " " << v[3 * i] << " "
+              << v[3 * i + 1] << " " << v[3 * i + 2] << " \n";
+        DF_CHECK(f.good(), DFSPH_E_INVALID, "write failed: " + path);
+        return DFSPH_OK;
+    }
+
+    // Reads a particle file (UnifiedParticleSet::load_from_file); a dynamic-body line is skipped.
+    int read_set(const std::string& path, std::vector<float>& m, std::vector<float>& x, std::vector<float>& v) {
+        std::ifstream f(path);
+        DF_CHECK(f.is_open(), DFSPH_E_INVALID, "cannot open " + path);
+        long long count = -1;
+        int has_factor = 0, vel_impacted = 0, dynamic = 0;
+        f >> count >> has_factor >> vel_impacted >> dynamic;
+        DF_CHECK(f.good() && count >= 0 && count <= (long long)UINT32_MAX, DFSPH_E_INVALID, "bad header in " + path);
+        if (dynamic) {  // position, velocity, quaternion (v, s), angular velocity of the rigid body
+            double skip;
+            for (int k = 0; k < 13; ++k) f >> skip;
+        }
+        m.resize((size_t)count);
+        x.resize((size_t)count * 3);
+        v.resize((size_t)count * 3);
+        for (long long i = 0; i < count; ++i) {
+            f >> m[i] >> x[3 * i] >> x[3 * i + 1] >> x[3 * i + 2] >> v[3 * i] >> v[3 * i + 1] >> v[3 * i + 2];
+            DF_CHECK(!f.fail(), DFSPH_E_INVALID, "truncated particle file " + path);
+        }
+        return DFSPH_OK;
+    }
+
+    int save_snapshot(const char* dir, int what) {
+        DF_CHECK(dir, DFSPH_E_INVALID, "null directory");
+        if (what & DFSPH_SNAP_FLUID) {
+            DF_TRY(write_set(join(dir, "fluid_file.txt"), false));
+            std::ofstream g(join(dir, "general_data.txt"), std::ios::trunc);
+            DF_CHECK(g.is_open(), DFSPH_E_INVALID, "cannot write general_data.txt");
+            g << std::setprecision(17) << h;
+        }
+        if (what & DFSPH_SNAP_BOUNDARY) DF_TRY(write_set(join(dir, "boundaries_file.txt"), true));
+        return DFSPH_OK;
+    }
+
+    int load_snapshot(const char* dir, int what, bool load_velocities) {
+        DF_CHECK(dir, DFSPH_E_INVALID, "null directory");
+        std::vector<float> m, x, v;
+        if (what & DFSPH_SNAP_BOUNDARY) {
+            DF_TRY(read_set(join(dir, "boundaries_file.txt"), m, x, v));
+            DF_CHECK(x.size() / 3 <= Bc, DFSPH_E_INVALID, "boundary file exceeds boundary_capacity");
+            DF_TRY(set_boundary(x.data(), nullptr, (uint32_t)(x.size() / 3)));  // psi recomputed
+            if (load_velocities && !x.empty()) {
+                bool any = false;
+                for (float e : v) any = any || e != 0.0f;
+                if (any) DF_TRY(move_boundary(x.data(), v.data()));
+            }
+        }
+        if (what & DFSPH_SNAP_FLUID) {
+            DF_TRY(read_set(join(dir, "fluid_file.txt"), m, x, v));
+            DF_CHECK(x.size() / 3 <= Nc, DFSPH_E_INVALID, "fluid file exceeds fluid_capacity");
+            std::ifstream g(join(dir, "general_data.txt"));
+            double hs = 0.0;
+            DF_CHECK(g.is_open() && (g >> hs) && hs > 0 && std::isfinite(hs), DFSPH_E_INVALID,
+                     "general_data.txt missing or without a positive time step");
+            DF_TRY(upload_fluid(x.data(), load_velocities ? v.data() : nullptr, m.data(), (uint32_t)(x.size() / 3)));
+            // updateTimeStep(h) + onSimulationStepEnd() twice: h = h_future = h_past = stored step
+            time_step = hs;
+            reset_dt();
+            DF_TRY(sync_state());
         }
         return DFSPH_OK;
     }
@@ -1516,6 +1615,10 @@ int dfsph_get_stream(dfsph_ctx* ctx, void** stream) {
 }
 int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launch) {
     DFSPH_DISPATCH(ctx, time_kernel(kernel, reps, ms_per_launch));
+}
+int dfsph_save_snapshot(dfsph_ctx* ctx, const char* dir, int what) { DFSPH_DISPATCH(ctx, save_snapshot(dir, what)); }
+int dfsph_load_snapshot(dfsph_ctx* ctx, const char* dir, int what, int load_velocities) {
+    DFSPH_DISPATCH(ctx, load_snapshot(dir, what, load_velocities != 0));
 }
 int dfsph_mlp_get_params(dfsph_ctx* ctx, float* params, size_t n) { DFSPH_DISPATCH(ctx, mlp_get_params(params, n)); }
 int dfsph_mlp_set_params(dfsph_ctx* ctx, const float* params, size_t n) {

@@ -289,6 +289,16 @@ class DFSPHCUDA:
         v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32)
         self._call(self._lib.dfsph_move_boundary(self._ctx, _fptr(x), _fptr(v)))
 
+    # ---- snapshots (DFSPHCUDA::handleSimulationSave / handleSimulationLoad) ----------------------
+    def save_snapshot(self, folder, fluid: bool = True, boundary: bool = True) -> None:
+        """Writes fluid_file.txt, general_data.txt and boundaries_file.txt (reference text format)."""
+        what = (_capi.SNAP_FLUID if fluid else 0) | (_capi.SNAP_BOUNDARY if boundary else 0)
+        self._call(self._lib.dfsph_save_snapshot(self._ctx, str(folder).encode(), what))
+
+    def load_snapshot(self, folder, fluid: bool = True, boundary: bool = True, load_velocities: bool = True) -> None:
+        what = (_capi.SNAP_FLUID if fluid else 0) | (_capi.SNAP_BOUNDARY if boundary else 0)
+        self._call(self._lib.dfsph_load_snapshot(self._ctx, str(folder).encode(), what, 1 if load_velocities else 0))
+
     # ---- learned warm start (no reference counterpart) ------------------------------------------
     def set_learned_warm_start(self, on: bool = True, probe: bool = True, train_interval: int | None = None,
                                train_iters: int | None = None, train_batch: int | None = None,

@@ -287,3 +287,30 @@ def column_scene(counts=(10, 80, 10), radius: float = 0.008, time_step: float = 
     return Scene(config=cfg, fluid=fluid.astype(np.float32), boundary=walls.astype(np.float32),
                  name=f"column_{'x'.join(map(str, cnt))}", box_min=(0.0, 0.0, 0.0), box_max=tuple(box),
                  meta=dict(seed=seed))
+
+
+def read_particle_file(path):
+    """Reads a particle file of the reference's snapshot format (UnifiedParticleSet::load_from_file,
+    DFSPH_c_arrays_structure.cpp:488-600): header "N has_factor velocity_impacted is_dynamic", for a
+    dynamic body one line of 13 rigid-body values, then N lines "mass x y z vx vy vz". Returns
+    (mass (N,), position (N, 3), velocity (N, 3), header flags (3,))."""
+    tok = Path(path).read_text().split()
+    n = int(tok[0])
+    flags = tuple(int(t) for t in tok[1:4])
+    k = 4 + (13 if flags[2] else 0)
+    vals = np.asarray(tok[k:k + 7 * n], dtype=np.float64)
+    if vals.size != 7 * n:
+        raise ValueError(f"{path}: expected {n} particle lines")
+    vals = vals.reshape(n, 7)
+    return vals[:, 0].copy(), vals[:, 1:4].copy(), vals[:, 4:7].copy(), flags
+
+
+def write_particle_file(path, mass, position, velocity=None, flags=(1, 1, 0)):
+    """Writes a particle file of the reference's snapshot format (UnifiedParticleSet::write_to_file,
+    DFSPH_c_arrays_structure.cpp:424-486), 9 significant digits."""
+    m = np.asarray(mass, dtype=np.float64).reshape(-1)
+    x = np.asarray(position, dtype=np.float64).reshape(-1, 3)
+    v = np.zeros_like(x) if velocity is None else np.asarray(velocity, dtype=np.float64).reshape(-1, 3)
+    lines = [f"{m.size} {flags[0]} {flags[1]} {flags[2]}"]
+    lines += [" ".join(f"{e:.9g}" for e in (m[i], *x[i], *v[i])) + " " for i in range(m.size)]
+    Path(path).write_text("\n".join(lines) + "\n")

@@ -1,0 +1,70 @@
+"""Snapshot files in the reference's text format (DFSPHCUDA::handleSimulationSave / Load,
+SPlisHSPlasH/DFSPH/DFSPH_CUDA.cpp:1885-1979; UnifiedParticleSet::write_to_file / load_from_file,
+DFSPH_c_arrays_structure.cpp:424-600). The fixture under tests/golden/snapshot is written by hand in
+that format (a 3-particle fluid; a 2-particle boundary with the dynamic-body line)."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from splishsplash_for_cuda_b200.scene import read_particle_file, synthetic_scene, write_particle_file
+
+SNAP = Path(__file__).resolve().parent / "golden" / "snapshot"
+
+
+def test_reads_reference_format_fixture():
+    m, x, v, flags = read_particle_file(SNAP / "fluid_file.txt")
+    assert flags == (1, 1, 0) and m.shape == (3,) and np.allclose(x[1], [0.15, 0.2, 0.3])
+    assert np.allclose(v[2], [0.0, -0.49, 0.002])
+    m, x, v, flags = read_particle_file(SNAP / "boundaries_file.txt")
+    assert flags == (0, 0, 1) and np.allclose(m, [0.5, 0.5]) and np.allclose(x[1], [0.05, 0, 0])
+
+
+def test_round_trip_is_exact_for_float32(tmp_path):
+    s = synthetic_scene(1, counts=(5, 5, 5))
+    rng = np.random.default_rng(0)
+    v = rng.normal(size=s.fluid.shape).astype(np.float32)
+    m = np.full(s.n_fluid, 0.0125, np.float32)
+    write_particle_file(tmp_path / "f.txt", m, s.fluid, v)
+    m2, x2, v2, flags = read_particle_file(tmp_path / "f.txt")
+    assert flags == (1, 1, 0)
+    assert np.array_equal(x2.astype(np.float32), s.fluid) and np.array_equal(v2.astype(np.float32), v)
+
+
+@pytest.mark.gpu
+def test_device_snapshot_save_load(cuda_lib, tmp_path):
+    from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
+
+    s = synthetic_scene(1, counts=(12, 12, 12), cfl=True)
+    a = DFSPHCUDA(s)
+    for _ in range(10):
+        a.step()
+    a.save_snapshot(tmp_path)
+    m, x, v, flags = read_particle_file(tmp_path / "fluid_file.txt")
+    assert flags == (1, 1, 0)
+    assert np.array_equal(x.astype(np.float32), a.positions()) and np.array_equal(v.astype(np.float32), a.velocities())
+    assert np.array_equal(m.astype(np.float32), a.field("mass"))
+    mb, xb, _, bflags = read_particle_file(tmp_path / "boundaries_file.txt")
+    assert bflags == (0, 0, 0) and np.array_equal(xb.astype(np.float32), a.field("boundary_position"))
+    h = float((tmp_path / "general_data.txt").read_text())
+    assert h == a.get_param("h")
+    b = DFSPHCUDA(s)
+    b.load_snapshot(tmp_path)
+    assert np.array_equal(b.positions(), a.positions()) and np.array_equal(b.velocities(), a.velocities())
+    assert b.get_param("h") == h and b.get_param("h_future") == h and b.get_param("h_past") == h
+    assert np.allclose(b.field("boundary_psi"), a.field("boundary_psi"), rtol=1e-6)
+    st = b.step()
+    assert st.status == 0
+
+
+@pytest.mark.gpu
+def test_device_loads_reference_format_fixture(cuda_lib):
+    from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
+
+    s = synthetic_scene(1, counts=(4, 4, 4))
+    d = DFSPHCUDA(s)
+    d.load_snapshot(SNAP, boundary=False)
+    _, x, v, _ = read_particle_file(SNAP / "fluid_file.txt")
+    assert d.num_fluid() == 3
+    assert np.array_equal(d.positions(), x.astype(np.float32)) and np.array_equal(d.velocities(), v.astype(np.float32))
+    assert d.get_param("h") == 0.00125
