@@ -108,7 +108,9 @@ enum dfsph_field {
     DFSPH_F_BOUNDARY_PSI = 10,      /* 1 per boundary particle: Akinci psi (boundary "mass")      */
     DFSPH_F_BOUNDARY_POSITION = 11, /* 3 per boundary particle                                     */
     DFSPH_F_NEIGHBOR_COUNTS = 12,   /* 2 per fluid particle: fluid count, boundary count (dtype 2)  */
-    DFSPH_F_BOUNDARY_VELOCITY = 13  /* 3 per boundary particle (zero for a static boundary)         */
+    DFSPH_F_BOUNDARY_VELOCITY = 13, /* 3 per boundary particle (zero for a static boundary)         */
+    DFSPH_F_BOUNDARY_FORCE = 14     /* 3 per boundary particle: force of the fluid during the last step
+                                       (set_param "boundary_forces" 1; DFSPH_core_cuda.cu:467-477) */
 };
 #define DFSPH_DTYPE_F32 0
 #define DFSPH_DTYPE_F64 1
@@ -187,7 +189,10 @@ int dfsph_on_step_end(dfsph_ctx* ctx);                                    /* onS
 /* Keys: "viscosity", "density0", "max_error", "max_error_v", "max_iterations", "max_iterations_v",
  * "enable_divergence_solver", "cfl_method", "cfl_factor", "cfl_max_time_step", "cfl_min_time_step",
  * "time_step" (sets the dt the next dt update uses), "gravitation_x|y|z", "use_graphs",
- * "h", "h_future", "h_past", "inv_h" (dt history of DFSPHCData), "timing" (1: record CUDA events).
+ * "h", "h_future", "h_past", "inv_h" (dt history of DFSPHCData), "timing" (1: record CUDA events),
+ * "boundary_forces" (1: accumulate the fluid's force on every boundary particle in each Jacobi pass,
+ * -m_i k_i psi_b grad W_ib summed over both solves of a step, as the reference does for dynamic
+ * bodies; cleared by each neighbour search; atomics, so the summation order varies).
  *
  * Learned warm start (no reference counterpart; off by default, dfsph_step only):
  * "learned_warm_start" (1: on), "warm_start_probe" (1: per solve, keep the learned candidate only if

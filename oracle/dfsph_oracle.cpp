@@ -128,6 +128,10 @@ template <class Real> struct Oracle {
     // boundary
     uint32_t nb = 0;
     std::vector<Real> bx, bv, psi;
+    // Force of the fluid on each boundary particle, summed over the Jacobi passes of a step
+    // (DFSPH_core_cuda.cu:467-477, :937-946: -m_i k_i psi_b grad W_ib), when enabled.
+    bool bforce_on = false;
+    std::vector<double> bF;
     bool boundary_moving = false;
     // neighbours
     std::vector<std::vector<uint32_t>> nf, nbd;
@@ -218,6 +222,7 @@ template <class Real> struct Oracle {
     }
 
     void neighbors() {
+        if (bforce_on) bF.assign(3 * (size_t)nb, 0.0);
         const std::vector<float> fp = fpos(), fb = fbpos();
         nf.assign(n, {});
         nbd.assign(n, {});
@@ -348,7 +353,7 @@ template <class Real> struct Oracle {
 
     // Jacobi velocity correction with coefficient k (per particle); dt is h or h_future.
     template <class KF, class Skip>
-    void jacobi(KF&& kof, Real dt, Skip&& skip) {
+    void jacobi(KF&& kof, Real dt, Skip&& skip, bool forces = true) {
         std::vector<Real> dv(3 * (size_t)n, 0);
 #pragma omp parallel for schedule(static)
         for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
@@ -372,6 +377,15 @@ template <class Real> struct Oracle {
                     K.gradW(xi - bx[3 * j], yi - bx[3 * j + 1], zi - bx[3 * j + 2], g0, g1, g2);
                     const Real s = ki * psi[j];
                     ax.add(s * g0); ay.add(s * g1); az.add(s * g2);
+                    if (bforce_on && forces) {
+                        const double f = -(double)m[i] * (double)s;
+#pragma omp atomic
+                        bF[3 * (size_t)j] += f * (double)g0;
+#pragma omp atomic
+                        bF[3 * (size_t)j + 1] += f * (double)g1;
+#pragma omp atomic
+                        bF[3 * (size_t)j + 2] += f * (double)g2;
+                    }
                 }
             }
             dv[3 * i] = ax.value() * dt;
@@ -713,6 +727,7 @@ int oracle_get(void* h, int field, double* out) {
             case 8: return put(o.a);
             case 10: return put(o.psi);
             case 11: return put(o.bx);
+            case 14: return o.bforce_on ? put(o.bF) : -1;
             default: return -1;
         }
     })());
@@ -749,6 +764,10 @@ int oracle_set_scalar(void* h, const char* key, double v) {
         else if (k == "h_future") o.h_future = v;
         else if (k == "inv_h") o.inv_h = v;
         else if (k == "time_step") o.time_step = v;
+        else if (k == "boundary_forces") {
+            o.bforce_on = v != 0;
+            if (o.bforce_on) o.bF.assign(3 * (size_t)o.nb, 0.0);
+        }
         else return -1;
         return 0;
     })());

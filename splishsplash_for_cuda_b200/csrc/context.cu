@@ -89,6 +89,8 @@ public:
     size_t cells = 0;
     Vec4<Real>* bpos[2] = {nullptr, nullptr};
     Vec4<Real>* bvel[2] = {nullptr, nullptr};
+    Real* bforce = nullptr;  // boundary forces (4 per particle, sorted order), allocated when enabled
+    bool boundary_forces = false;
     uint32_t* bid = nullptr;
     double* partials = nullptr;
     LoopCtl* ctl = nullptr;
@@ -211,7 +213,7 @@ public:
         for (int b = 0; b < 2; ++b) {
             f(pos[b]); f(vel[b]); f(kappa[b]); f(kappaV[b]); f(id[b]); f(bpos[b]); f(bvel[b]);
         }
-        f(density); f(factor); f(densityAdv); f(kcoef); f(acc); f(counts); f(nbr); f(bid);
+        f(density); f(factor); f(densityAdv); f(kcoef); f(acc); f(counts); f(nbr); f(bid); f(bforce);
         f(sb.keys_a); f(sb.keys_b); f(sb.vals_a); f(sb.vals_b); f(sb.workspace);
         f(partials); f(cfl_partials); f(ctl); f(status); f(stage); f(dl); f(ds); f(ftab); f(btab);
         for (int b = 0; b < 2; ++b) {
@@ -287,6 +289,7 @@ public:
         hs.ctl = ctl;
         hs.status = status;
         hs.cfl_partials = cfl_partials;
+        hs.bforce = boundary_forces ? bforce : nullptr;
         hs.features = features;
         hs.pred = pred;
         hs.kappaT = kappaT[cur];
@@ -492,6 +495,9 @@ public:
     // the signature; unsorted searching is not offered).
     int neighbors_search() {
         DF_CHECK(grid_ready, DFSPH_E_STATE, "no grid: set a boundary or upload fluid first");
+        // forces on the boundary are per step (the reference clears them when it moves the dynamic
+        // bodies at the start of a step, DFSPH_core_cuda.cu:3413)
+        if (boundary_forces && nb) DF_CUDA(cudaMemsetAsync(bforce, 0, (size_t)nb * 4 * sizeof(Real), stream));
         if (!n) return DFSPH_OK;
         const StepParams<Real> p = params();
         launch_cell_keys<Real>(pos[cur], n, p, sb.keys_a, status, stream);
@@ -539,10 +545,10 @@ public:
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         DF_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         if (kind == 0) {
-            launch_divergence_jacobi<Real>(ds, n, handle, true, stream);
+            launch_divergence_jacobi<Real>(ds, n, handle, true, stream, boundary_forces);
             launch_divergence_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream, g_loop_keep);
         } else {
-            launch_pressure_jacobi<Real>(ds, n, handle, true, stream);
+            launch_pressure_jacobi<Real>(ds, n, handle, true, stream, boundary_forces);
             launch_pressure_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream, g_loop_keep);
         }
         cudaGraph_t captured = nullptr;
@@ -573,10 +579,10 @@ public:
         uint32_t cont = 1;
         while (cont) {
             if (kind == 0) {
-                launch_divergence_jacobi<Real>(ds, n, 0, false, stream);
+                launch_divergence_jacobi<Real>(ds, n, 0, false, stream, boundary_forces);
                 launch_divergence_residual<Real>(ds, n, false, 0.0, 0, 0, 0, false, stream, keep);
             } else {
-                launch_pressure_jacobi<Real>(ds, n, 0, false, stream);
+                launch_pressure_jacobi<Real>(ds, n, 0, false, stream, boundary_forces);
                 launch_pressure_residual<Real>(ds, n, false, 0.0, 0, 0, 0, false, stream, keep);
             }
             launches += 2;
@@ -594,7 +600,7 @@ public:
         const double eta = max_error * 0.01 * sc.density0 / h;
         if (!lp) {
             launch_density_alpha<Real>(ds, n, true, false, stream);
-            launch_divergence_warm_jacobi<Real>(ds, n, nullptr, nullptr, stream);
+            launch_divergence_warm_jacobi<Real>(ds, n, nullptr, nullptr, stream, boundary_forces);
             launch_divergence_residual<Real>(ds, n, true, eta, kMinItersV, max_iter, 0, false, stream);
             launches += 3;
         } else {
@@ -610,7 +616,7 @@ public:
                 launch_probe_residual<Real>(ds, n, 0, velP, stream);
                 launches += 2;
             }
-            launch_divergence_warm_jacobi<Real>(ds, n, kappaVW, nullptr, stream);
+            launch_divergence_warm_jacobi<Real>(ds, n, kappaVW, nullptr, stream, boundary_forces);
             launch_divergence_residual<Real>(ds, n, true, eta, kMinItersV, max_iter, 0, false, stream, true);
             launches += 2;
             if (use && probe) {
@@ -632,7 +638,7 @@ public:
         DF_CUDA(cudaMemsetAsync(&ctl[1].ticket, 0, sizeof(uint32_t), stream));
         const double eta = max_error * 0.01 * sc.density0;
         if (!lp) {
-            launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, nullptr, nullptr, stream);
+            launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, nullptr, nullptr, stream, boundary_forces);
             launch_pressure_residual<Real>(ds, n, true, eta, kMinItersP, max_iter, 0, false, stream);
             launches += 2;
         } else {
@@ -646,7 +652,7 @@ public:
                 launch_probe_residual<Real>(ds, n, 1, velP, stream);
                 launches += 2;
             }
-            launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, kappaW, nullptr, stream);
+            launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, kappaW, nullptr, stream, boundary_forces);
             launch_pressure_residual<Real>(ds, n, true, eta, kMinItersP, max_iter, 0, false, stream, true);
             launches += 2;
             if (use && probe) {
@@ -1092,6 +1098,11 @@ public:
                 src = (const Real*)bvel[0]; sstride = 4; comps = 3; count = nb;
                 idmap = (order == DFSPH_ORDER_ID) ? bid : nullptr;
                 break;
+            case DFSPH_F_BOUNDARY_FORCE:
+                DF_CHECK(bforce, DFSPH_E_STATE, "boundary forces are off (set_param boundary_forces 1)");
+                src = bforce; sstride = 4; comps = 3; count = nb;
+                idmap = (order == DFSPH_ORDER_ID) ? bid : nullptr;
+                break;
             case DFSPH_F_ID:
             case DFSPH_F_NEIGHBOR_COUNTS: {
                 DF_CHECK(dtype == DFSPH_DTYPE_U32, DFSPH_E_INVALID, "id and neighbour counts download as u32");
@@ -1264,6 +1275,14 @@ public:
         else if (k == "timing") timing = v != 0;
         else if (k == "learned_warm_start") return enable_learned(v != 0);
         else if (k == "warm_start_probe") probe = v != 0;
+        else if (k == "boundary_forces") {
+            if (v != 0 && !bforce) {
+                DF_TRY(dalloc(&bforce, (size_t)Bc * 4));
+                DF_CUDA(cudaMemsetAsync(bforce, 0, (size_t)Bc * 4 * sizeof(Real), stream));
+            }
+            boundary_forces = v != 0;
+            invalidate_graphs();  // the loop graphs read the DevState block; rebuilt for clarity
+        }
         else if (k == "warm_start_damping") {
             DF_CHECK(v > 0 && v <= 1, DFSPH_E_INVALID, "warm_start_damping must be in (0, 1]");
             damping = v;
@@ -1323,6 +1342,7 @@ public:
         else if (k == "iterations_v") *v = last_iters_v;
         else if (k == "learned_warm_start") *v = learned ? 1 : 0;
         else if (k == "warm_start_probe") *v = probe ? 1 : 0;
+        else if (k == "boundary_forces") *v = boundary_forces ? 1 : 0;
         else if (k == "warm_start_damping") *v = damping;
         else if (k == "train_interval") *v = train_interval;
         else if (k == "train_start") *v = train_start;

@@ -30,6 +30,7 @@ template <class Real> struct DevState {
     // boundary, cell-sorted order
     const Vec4<Real>* bpos;  // x, y, z, psi
     const Vec4<Real>* bvel;  // vx, vy, vz, (unused)
+    Real* bforce;            // fx, fy, fz, - per boundary particle (null: not accumulated)
     // reductions and control
     double* partials;      // one FP64 partial per block
     LoopCtl* ctl;          // [0] divergence loop, [1] pressure loop, [2] CFL / misc, [3] candidate probe
@@ -81,7 +82,7 @@ void launch_density_alpha(const DevState<Real>* d, uint32_t n, bool warm_v, bool
 // kw: warm-start coefficients (null = kappa_v); vout: output velocities (null = in place).
 template <class Real>
 void launch_divergence_warm_jacobi(const DevState<Real>* d, uint32_t n, const Real* kw, Vec4<Real>* vout,
-                                   cudaStream_t s);
+                                   cudaStream_t s, bool forces = false);
 // Sum of the divergence (which = 0) or density (which = 1) residual of velocities `vel`, into ctl[3]
 // (no other write): the initial residual of a warm-start candidate.
 template <class Real>
@@ -106,14 +107,14 @@ void launch_divergence_residual(const DevState<Real>* d, uint32_t n, bool init, 
                                 cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s, bool keep = false);
 template <class Real>
 void launch_divergence_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
-                              cudaStream_t s);
+                              cudaStream_t s, bool forces = false);
 template <class Real> void launch_viscosity(const DevState<Real>* d, uint32_t n, bool cfl, cudaStream_t s);
 template <class Real> void launch_update_vel(const DevState<Real>* d, uint32_t n, cudaStream_t s);
 // kw null: kappa scaled by (h/h_f)^2 and clamped (reference warm start); otherwise the given final
 // warm-start coefficients. vout: output velocities (null = in place).
 template <class Real>
 void launch_pressure_warm_jacobi(const DevState<Real>* d, uint32_t n, bool fused_vel, const Real* kw,
-                                 Vec4<Real>* vout, cudaStream_t s);
+                                 Vec4<Real>* vout, cudaStream_t s, bool forces = false);
 // keep: also store the unclamped residual in resid (learned warm start).
 template <class Real>
 void launch_pressure_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
@@ -126,7 +127,7 @@ void launch_fallback_residual(const DevState<Real>* d, uint32_t n, int which, do
                               cudaStream_t s);
 template <class Real>
 void launch_pressure_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
-                            cudaStream_t s);
+                            cudaStream_t s, bool forces = false);
 template <class Real> void launch_update_pos(const DevState<Real>* d, uint32_t n, cudaStream_t s);
 template <class Real> void launch_cfl_reduce(const DevState<Real>* d, uint32_t n_blocks, cudaStream_t s);
 

@@ -178,11 +178,13 @@ __device__ __forceinline__ Real velocity_divergence(const DevState<Real>* __rest
 
 // Jacobi velocity correction: sum over fluid neighbours of (k_i + k_j) m_j grad W_ij where
 // |k_i + k_j| > eps, plus (when |k_i| > eps) k_i sum over boundary neighbours of psi_b grad W_ib.
-// kof(j) returns k_j (a load, possibly transformed).
-template <class Real, class KOf>
+// kof(j) returns k_j (a load, possibly transformed). With boundary forces on (kForces, and at run
+// time `forces`), each boundary term also adds -m_i k_i psi_b grad W_ib to the boundary particle's force,
+// as the reference does for dynamic bodies (DFSPH_core_cuda.cu:467-477, :937-946).
+template <class Real, bool kForces = false, class KOf>
 __device__ __forceinline__ void jacobi_sum(const DevState<Real>* __restrict__ ds, const StepParams<Real>& p, uint32_t i,
                                            const Vec4<Real>& xi, Real ki, uint32_t nf, uint32_t nb, KOf&& kof,
-                                           KSum3<Real>& acc) {
+                                           KSum3<Real>& acc, bool forces = true) {
     const Vec4<Real>* __restrict__ pos = ds->pos;
     const uint32_t* __restrict__ nbr = ds->nbr;
     const uint32_t stride = p.nbr_stride;
@@ -206,14 +208,27 @@ __device__ __forceinline__ void jacobi_sum(const DevState<Real>* __restrict__ ds
         });
     if (nb && above_eps(ki)) {
         const Vec4<Real>* __restrict__ bpos = ds->bpos;
+        Real* __restrict__ bf = (kForces && forces) ? ds->bforce : nullptr;
         Vec4<Real> xb[kGatherBatch];
+        uint32_t jb[kGatherBatch];
         visit_neighbors<kGatherBatch>(
-            nbr, stride, i, nf, nf + nb, 0u, [&](int u, uint32_t j) { xb[u] = ld4<Real>(bpos + j); },
+            nbr, stride, i, nf, nf + nb, 0u,
+            [&](int u, uint32_t j) {
+                xb[u] = ld4<Real>(bpos + j);
+                jb[u] = j;
+            },
             [&](int u) {
                 Real gx, gy, gz;
                 K.gradW(xi.x - xb[u].x, xi.y - xb[u].y, xi.z - xb[u].z, gx, gy, gz);
                 const Real sc = ki * xb[u].w;
                 acc.add(sc * gx, sc * gy, sc * gz);
+                if (kForces && bf) {
+                    const Real f = -xi.w * sc;
+                    Real* fb = bf + 4 * (size_t)jb[u];
+                    atomicAdd(fb, f * gx);
+                    atomicAdd(fb + 1, f * gy);
+                    atomicAdd(fb + 2, f * gz);
+                }
             });
     }
 }
@@ -295,7 +310,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
 
 // Divergence warm start (divergenceSolveParticle<true>, only where the source is positive,
 // DFSPH_core_cuda.cu:509-512): v_i += h * sum (kv_i + kv_j) m_j grad W_ij + h kv_i sum psi_b grad W_ib.
-template <class Real>
+template <class Real, bool kForces>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
                                                                         uint32_t n, const Real* __restrict__ kw,
                                                                         Vec4<Real>* __restrict__ vout) {
@@ -311,7 +326,8 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_warm_jaco
     const Vec4<Real> xi = ds->pos[i];
     const uint32_t c = ds->counts[i];
     KSum3<Real> acc;
-    jacobi_sum<Real>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c), [&](uint32_t j) { return kv[j]; }, acc);
+    jacobi_sum<Real, kForces>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c), [&](uint32_t j) { return kv[j]; },
+                              acc, vout == nullptr);  // a candidate pass (vout set) adds no boundary force
     Vec4<Real> v = ds->vel[i];
     v.x += acc.x.value() * p.h;
     v.y += acc.y.value() * p.h;
@@ -380,7 +396,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_residual_
 
 // Divergence Jacobi iteration (divergenceSolveParticle<false>): k_i = rho_dot_i alpha_i,
 // kappa_v_i += k_i, v_i += h * [sum (k_i + k_j) m_j grad W_ij + k_i sum psi_b grad W_ib].
-template <class Real>
+template <class Real, bool kForces>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_jacobi_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                    cudaGraphConditionalHandle handle, bool use_handle) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -395,7 +411,8 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_jacobi_ke
     const Vec4<Real> xi = ds->pos[i];
     const uint32_t c = ds->counts[i];
     KSum3<Real> acc;
-    jacobi_sum<Real>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c), [&](uint32_t j) { return kc[j]; }, acc);
+    jacobi_sum<Real, kForces>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c), [&](uint32_t j) { return kc[j]; },
+                              acc);
     Vec4<Real> v = ds->vel[i];
     v.x += acc.x.value() * p.h;
     v.y += acc.y.value() * p.h;
@@ -495,7 +512,7 @@ __global__ void __launch_bounds__(kBlock) update_vel_kernel(const DevState<Real>
 // Pressure warm start (pressureSolveParticle<true>) fused with the velocity update: with
 // kFusedVel the particle first applies v_i += h a_i and uses kappa scaled by (h/h_future)^2 and
 // clamped at -0.5 (update_vel, :3061-3065), computed for the neighbours on the fly.
-template <class Real, bool kFusedVel>
+template <class Real, bool kFusedVel, bool kForces>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
                                                                       uint32_t n, const Real* __restrict__ kw,
                                                                       Vec4<Real>* __restrict__ vout) {
@@ -511,8 +528,9 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_warm_jacobi
     const Vec4<Real> xi = ds->pos[i];
     const uint32_t c = ds->counts[i];
     KSum3<Real> acc;
-    jacobi_sum<Real>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c),
-                     [&](uint32_t j) { return scale ? rmax<Real>(kap[j] * r2, Real(-0.5)) : kap[j]; }, acc);
+    jacobi_sum<Real, kForces>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c),
+                              [&](uint32_t j) { return scale ? rmax<Real>(kap[j] * r2, Real(-0.5)) : kap[j]; }, acc,
+                              vout == nullptr);  // a candidate pass (vout set) adds no boundary force
     Vec4<Real> v = ds->vel[i];
     if (kFusedVel) {
         const Vec4<Real> a = ds->acc[i];
@@ -571,7 +589,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_residual_ke
 
 // Pressure Jacobi iteration (pressureSolveParticle<false>): v_i += h_f * [sum (k_i + k_j) m_j grad W_ij
 // + k_i sum psi_b grad W_ib] with k = rho_adv * alpha.
-template <class Real>
+template <class Real, bool kForces>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_jacobi_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                  cudaGraphConditionalHandle handle, bool use_handle) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -583,7 +601,8 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_jacobi_kern
     const Vec4<Real> xi = ds->pos[i];
     const uint32_t c = ds->counts[i];
     KSum3<Real> acc;
-    jacobi_sum<Real>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c), [&](uint32_t j) { return kc[j]; }, acc);
+    jacobi_sum<Real, kForces>(ds, p, i, xi, ki, fluid_count(c), boundary_count(c), [&](uint32_t j) { return kc[j]; },
+                              acc);
     Vec4<Real> v = ds->vel[i];
     v.x += acc.x.value() * p.h_future;
     v.y += acc.y.value() * p.h_future;
@@ -730,8 +749,10 @@ void launch_density_alpha(const DevState<Real>* d, uint32_t n, bool warm_v, bool
 }
 template <class Real>
 void launch_divergence_warm_jacobi(const DevState<Real>* d, uint32_t n, const Real* kw, Vec4<Real>* vout,
-                                   cudaStream_t s) {
-    if (n) divergence_warm_jacobi_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, kw, vout);
+                                   cudaStream_t s, bool forces) {
+    if (!n) return;
+    if (forces) divergence_warm_jacobi_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n, kw, vout);
+    else divergence_warm_jacobi_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n, kw, vout);
 }
 template <class Real>
 void launch_probe_residual(const DevState<Real>* d, uint32_t n, int which, const Vec4<Real>* vel, cudaStream_t s) {
@@ -763,8 +784,10 @@ void launch_divergence_residual(const DevState<Real>* d, uint32_t n, bool init, 
 }
 template <class Real>
 void launch_divergence_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
-                              cudaStream_t s) {
-    if (n) divergence_jacobi_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
+                              cudaStream_t s, bool forces) {
+    if (!n) return;
+    if (forces) divergence_jacobi_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
+    else divergence_jacobi_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
 }
 template <class Real> void launch_viscosity(const DevState<Real>* d, uint32_t n, bool cfl, cudaStream_t s) {
     if (!n) return;
@@ -776,10 +799,16 @@ template <class Real> void launch_update_vel(const DevState<Real>* d, uint32_t n
 }
 template <class Real>
 void launch_pressure_warm_jacobi(const DevState<Real>* d, uint32_t n, bool fused_vel, const Real* kw,
-                                 Vec4<Real>* vout, cudaStream_t s) {
+                                 Vec4<Real>* vout, cudaStream_t s, bool forces) {
     if (!n) return;
-    if (fused_vel) pressure_warm_jacobi_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n, kw, vout);
-    else pressure_warm_jacobi_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n, kw, vout);
+    const unsigned g = grid_for(n);
+    if (forces) {
+        if (fused_vel) pressure_warm_jacobi_kernel<Real, true, true><<<g, kBlock, 0, s>>>(d, n, kw, vout);
+        else pressure_warm_jacobi_kernel<Real, false, true><<<g, kBlock, 0, s>>>(d, n, kw, vout);
+    } else {
+        if (fused_vel) pressure_warm_jacobi_kernel<Real, true, false><<<g, kBlock, 0, s>>>(d, n, kw, vout);
+        else pressure_warm_jacobi_kernel<Real, false, false><<<g, kBlock, 0, s>>>(d, n, kw, vout);
+    }
 }
 template <class Real>
 void launch_pressure_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
@@ -800,8 +829,10 @@ void launch_fallback_residual(const DevState<Real>* d, uint32_t n, int which, do
 }
 template <class Real>
 void launch_pressure_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
-                            cudaStream_t s) {
-    if (n) pressure_jacobi_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
+                            cudaStream_t s, bool forces) {
+    if (!n) return;
+    if (forces) pressure_jacobi_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
+    else pressure_jacobi_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
 }
 template <class Real> void launch_update_pos(const DevState<Real>* d, uint32_t n, cudaStream_t s) {
     if (n) update_pos_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n);
@@ -812,7 +843,8 @@ template <class Real> void launch_cfl_reduce(const DevState<Real>* d, uint32_t n
 
 #define DFSPH_INSTANTIATE_SOLVER(R)                                                                                  \
     template void launch_density_alpha<R>(const DevState<R>*, uint32_t, bool, bool, cudaStream_t);                  \
-    template void launch_divergence_warm_jacobi<R>(const DevState<R>*, uint32_t, const R*, Vec4<R>*, cudaStream_t); \
+    template void launch_divergence_warm_jacobi<R>(const DevState<R>*, uint32_t, const R*, Vec4<R>*, cudaStream_t,  \
+                                                   bool);                                                            \
     template void launch_probe_residual<R>(const DevState<R>*, uint32_t, int, const Vec4<R>*, cudaStream_t);        \
     template void launch_warm_values<R>(const DevState<R>*, uint32_t, int, bool, double, cudaStream_t);             \
     template void launch_totals<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                               \
@@ -821,16 +853,16 @@ template <class Real> void launch_cfl_reduce(const DevState<Real>* d, uint32_t n
     template void launch_divergence_residual<R>(const DevState<R>*, uint32_t, bool, double, int, int,               \
                                                 cudaGraphConditionalHandle, bool, cudaStream_t, bool);               \
     template void launch_divergence_jacobi<R>(const DevState<R>*, uint32_t, cudaGraphConditionalHandle, bool,       \
-                                              cudaStream_t);                                                         \
+                                              cudaStream_t, bool);                                                   \
     template void launch_viscosity<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                            \
     template void launch_update_vel<R>(const DevState<R>*, uint32_t, cudaStream_t);                                 \
     template void launch_pressure_warm_jacobi<R>(const DevState<R>*, uint32_t, bool, const R*, Vec4<R>*,            \
-                                                 cudaStream_t);                                                      \
+                                                 cudaStream_t, bool);                                                \
     template void launch_pressure_residual<R>(const DevState<R>*, uint32_t, bool, double, int, int,                 \
                                               cudaGraphConditionalHandle, bool, cudaStream_t, bool);                 \
     template void launch_fallback_residual<R>(const DevState<R>*, uint32_t, int, double, int, int, cudaStream_t);   \
     template void launch_pressure_jacobi<R>(const DevState<R>*, uint32_t, cudaGraphConditionalHandle, bool,         \
-                                            cudaStream_t);                                                           \
+                                            cudaStream_t, bool);                                                     \
     template void launch_update_pos<R>(const DevState<R>*, uint32_t, cudaStream_t);                                 \
     template void launch_cfl_reduce<R>(const DevState<R>*, uint32_t, cudaStream_t);
 

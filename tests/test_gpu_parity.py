@@ -283,3 +283,27 @@ def test_thousand_steps_bounded_drift():
     assert np.abs(xa.mean(0) - xb.mean(0)).max() <= 0.01 * span
     ka, kb = (va ** 2).sum(1).mean(), (vb ** 2).sum(1).mean()
     assert abs(ka - kb) <= 0.1 * max(ka, kb)
+
+
+def test_boundary_forces_match_oracle():
+    """Boundary forces (-m_i k_i psi_b grad W_ib over every Jacobi pass of a step, accumulated with
+    atomics): FP32 kernels vs FP64 oracle in lockstep, and the settled column's weight on the
+    boundary. Bar 1e-3 on the force field: FP32 terms of both signs accumulate over ~50 passes."""
+    from splishsplash_for_cuda_b200.scene import column_scene
+
+    s = column_scene(counts=(6, 12, 6), time_step=0.002)
+    d = DFSPHCUDA(s)
+    d.set_param("boundary_forces", 1)
+    o = Oracle(s, 64)
+    o.set_scalar("boundary_forces", 1)
+    for k in range(20):
+        st, ro = d.step(), o.step()
+        assert st.iterations == ro["iterations"], k
+    check_field("boundary_force", d.field("boundary_force", np.float64), o.field("boundary_force"), 1e-3)
+    weight = float(d.field("mass", np.float64).sum()) * 9.81
+    fy = []
+    for k in range(230):
+        d.step()
+        if k >= 180:
+            fy.append(d.field("boundary_force", np.float64)[:, 1].sum())
+    assert abs(np.mean(fy) + weight) <= 0.05 * weight

@@ -109,3 +109,20 @@ def test_empty_fluid(oracle_lib):
     o = Oracle(s, 64)
     st = o.step()
     assert st["iterations"] == 0 and st["iterations_v"] == 0
+
+
+def test_boundary_force_balances_weight_at_rest(oracle_lib):
+    """The fluid's force on the boundary (summed over the Jacobi passes of a step) carries the weight
+    of a settled column: sum F_y = -M g within 5 % averaged over 50 steps."""
+    from splishsplash_for_cuda_b200.scene import column_scene
+
+    s = column_scene(counts=(6, 12, 6), time_step=0.002)
+    o = Oracle(s, 64)
+    o.set_scalar("boundary_forces", 1)
+    weight = o.field("mass").sum() * 9.81
+    fy = []
+    for k in range(250):
+        o.step()
+        if k >= 200:
+            fy.append(o.field("boundary_force")[:, 1].sum())
+    assert abs(np.mean(fy) + weight) <= 0.05 * weight
