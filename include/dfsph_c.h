@@ -192,7 +192,10 @@ int dfsph_on_step_end(dfsph_ctx* ctx);                                    /* onS
  * "h", "h_future", "h_past", "inv_h" (dt history of DFSPHCData), "timing" (1: record CUDA events),
  * "boundary_forces" (1: accumulate the fluid's force on every boundary particle in each Jacobi pass,
  * -m_i k_i psi_b grad W_ib summed over both solves of a step, as the reference does for dynamic
- * bodies; cleared by each neighbour search; atomics, so the summation order varies).
+ * bodies; cleared by each neighbour search; atomics, so the summation order varies),
+ * "sort_withhold_tile" (failure-detection tests: the fluid sort's tile with this id never publishes
+ * its look-back flags, so the bounded waits of the tiles after it run out, about a second, and the
+ * step reports DFSPH_ST_SORT_TIMEOUT with an unspecified particle order; -1 turns it off).
  *
  * Learned warm start (no reference counterpart; off by default, dfsph_step only):
  * "learned_warm_start" (1: on), "warm_start_probe" (1: per solve, keep the learned candidate only if

@@ -70,6 +70,7 @@ public:
     bool grid_ready = false;
     bool boundary_moving = false;
     int key_passes = 4;
+    uint32_t sort_withheld_tile = kNoWithheldTile;  // failure-detection test hook (see sort.cuh)
     int off[3] = {0, 0, 0}, dim[3] = {0, 0, 0};
 
     DevState<Real> hs{};
@@ -502,7 +503,7 @@ public:
         const StepParams<Real> p = params();
         launch_cell_keys<Real>(pos[cur], n, p, sb.keys_a, status, stream);
         uint32_t *skeys, *perm;
-        radix_sort_pairs(sb, n, key_passes, true, stream, status, &launches, &skeys, &perm);
+        radix_sort_pairs(sb, n, key_passes, true, stream, status, &launches, &skeys, &perm, sort_withheld_tile);
         const int nx = 1 - cur;
         launch_reorder_fluid<Real>(perm, n, pos[cur], vel[cur], kappa[cur], kappaV[cur], id[cur], pos[nx], vel[nx],
                                    kappa[nx], kappaV[nx], id[nx], stream);
@@ -1275,6 +1276,7 @@ public:
         else if (k == "timing") timing = v != 0;
         else if (k == "learned_warm_start") return enable_learned(v != 0);
         else if (k == "warm_start_probe") probe = v != 0;
+        else if (k == "sort_withhold_tile") sort_withheld_tile = v < 0 ? kNoWithheldTile : (uint32_t)v;
         else if (k == "boundary_forces") {
             if (v != 0 && !bforce) {
                 DF_TRY(dalloc(&bforce, (size_t)Bc * 4));

@@ -70,7 +70,8 @@ __device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) { *(volatil
 __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
     const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
     uint32_t* __restrict__ vout, uint32_t n, int shift, const uint32_t* __restrict__ digit_offsets,
-    uint32_t* __restrict__ tile_status, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status_word) {
+    uint32_t* __restrict__ tile_status, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status_word,
+    uint32_t withheld_tile) {
     __shared__ uint32_t warp_hist[kSortWarps][256];
     __shared__ uint32_t digit_base[256];
     __shared__ uint32_t s_tile;
@@ -113,10 +114,13 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
         }
         uint32_t* my = tile_status + (size_t)tile * 256 + d;
         uint32_t exclusive = 0;
+        // A withheld tile (failure-detection tests only) never publishes: its successors' bounded
+        // look-back runs out and raises DFSPH_ST_SORT_TIMEOUT.
+        const bool publish = tile != withheld_tile;
         if (tile == 0) {
-            st_volatile(my, kFlagPrefix | total);
+            if (publish) st_volatile(my, kFlagPrefix | total);
         } else {
-            st_volatile(my, kFlagAggregate | total);
+            if (publish) st_volatile(my, kFlagAggregate | total);
             int look = (int)tile - 1;
             int spins = 0;
             while (look >= 0) {
@@ -134,7 +138,7 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
                 if (flag == kFlagPrefix) break;
                 --look;
             }
-            st_volatile(my, kFlagPrefix | ((exclusive + total) & kCountMask));
+            if (publish) st_volatile(my, kFlagPrefix | ((exclusive + total) & kCountMask));
         }
         digit_base[d] = digit_offsets[d] + exclusive;
     }
@@ -164,7 +168,8 @@ size_t radix_sort_workspace_words(uint32_t n_max, int passes) {
 // the first pass takes iota payloads when iota_values is set. The result is returned through
 // *keys_out / *vals_out and lies in set a after an even number of passes, else in set b.
 void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, cudaStream_t stream,
-                      uint32_t* status_word, uint64_t* launch_counter, uint32_t** keys_out, uint32_t** vals_out) {
+                      uint32_t* status_word, uint64_t* launch_counter, uint32_t** keys_out, uint32_t** vals_out,
+                      uint32_t withheld_tile) {
     if (n == 0 || passes == 0) {
         *keys_out = b.keys_a;
         *vals_out = b.vals_a;
@@ -191,7 +196,7 @@ void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, 
         uint32_t* vout = even ? b.vals_b : b.vals_a;
         onesweep_kernel<<<(unsigned)tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, 8 * p, offsets + p * 256,
                                                                    status + (size_t)p * tiles * 256, counters + p,
-                                                                   status_word);
+                                                                   status_word, withheld_tile);
         *launch_counter += 1;
     }
     const bool in_a = (passes & 1) == 0;
@@ -284,7 +289,8 @@ extern "C" int dfsph_sort_cell_keys_noalloc(const uint32_t* keys_in, uint32_t* k
         uint32_t* kout = to_out ? keys_out : pk;
         uint32_t* vout = to_out ? perm_out : pv;
         onesweep_kernel<<<(unsigned)tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, 8 * p, offsets + p * 256,
-                                                                flags + (size_t)p * tiles * 256, counters + p, status);
+                                                                flags + (size_t)p * tiles * 256, counters + p, status,
+                                                                kNoWithheldTile);
         kin = kout;
         vin = vout;
         to_out = !to_out;

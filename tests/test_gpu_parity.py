@@ -208,6 +208,26 @@ def test_status_not_converged_reported():
     assert st.status & _capi.ST_PRESSURE_NOT_CONVERGED
 
 
+def test_sort_wait_limit_reports_timeout_and_context_recovers():
+    """Failure detection without a GPU fault: one tile of the fluid sort withholds its look-back
+    flags (a flag that nothing sets), so the bounded waits of the tiles after it run out (about a
+    second each). The step returns with DFSPH_ST_SORT_TIMEOUT instead of hanging; every write stayed
+    in range, so after a reset the same context steps exactly like a fresh one."""
+    s = synthetic_scene(1, counts=(20, 20, 20))  # 8000 particles: 4 sort tiles
+    d = DFSPHCUDA(s)
+    d.set_param("sort_withhold_tile", 1)
+    st = d.step()
+    assert st.status & _capi.ST_SORT_TIMEOUT
+    d.set_param("sort_withhold_tile", -1)
+    d.reset()
+    d.status(clear=True)
+    ref = DFSPHCUDA(s)
+    for _ in range(3):
+        a, b = d.step(), ref.step()
+        assert a.status == 0 and a.iterations == b.iterations
+    assert np.array_equal(d.positions(), ref.positions())
+
+
 def test_field_download_orders_and_dtypes():
     s = synthetic_scene(1, counts=(6, 7, 8))
     d = DFSPHCUDA(s)
