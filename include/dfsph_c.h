@@ -264,6 +264,15 @@ int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launc
 int dfsph_save_snapshot(dfsph_ctx* ctx, const char* dir, int what);
 int dfsph_load_snapshot(dfsph_ctx* ctx, const char* dir, int what, int load_velocities);
 
+/* Binary checkpoint of the complete solver state (no reference counterpart; the text snapshot above
+ * drops the warm starts and the particle order): particles in their current internal order with
+ * kappa and kappa_v, the boundary with psi, the dt history, the grid, the scene parameters and, when
+ * the learned warm start is on, its totals, network weights, Adam state and scales. Loading into a
+ * context created with at least the same capacities, the same neighbor_capacity and precision
+ * resumes bit-identically. */
+int dfsph_checkpoint_save(dfsph_ctx* ctx, const char* path);
+int dfsph_checkpoint_load(dfsph_ctx* ctx, const char* path);
+
 /* ---- learned warm-start network (no reference counterpart) -------------------------------------
  * A per-particle MLP, inputs x[8] = [(rho - rho0)/rho0, rho_dot * alpha, neighbours / 64,
  * kappa_total_prev, kappa_v_total_prev, 0, 0, 0] (each multiplied by in_scale[i]), two hidden layers

@@ -124,6 +124,8 @@ SIGNATURES = {
     "dfsph_time_kernel": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "dfsph_save_snapshot": (C.c_int, [_P, C.c_char_p, C.c_int]),
     "dfsph_load_snapshot": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int]),
+    "dfsph_checkpoint_save": (C.c_int, [_P, C.c_char_p]),
+    "dfsph_checkpoint_load": (C.c_int, [_P, C.c_char_p]),
     "dfsph_mlp_get_params": (C.c_int, [_P, _F, C.c_size_t]),
     "dfsph_mlp_set_params": (C.c_int, [_P, _F, C.c_size_t]),
     "dfsph_mlp_get_scales": (C.c_int, [_P, _F, _F]),

@@ -315,7 +315,6 @@ public:
     // (DFSPH_c_arrays_structure.cpp:1050-1098): offset = -(floor(min / H) - 5).
     int set_grid(const float mn[3], const float mx[3]) {
         const float H = (float)(4.0 * sc.particle_radius);
-        int maxdim = 1;
         for (int a = 0; a < 3; ++a) {
             DF_CHECK(std::isfinite(mn[a]) && std::isfinite(mx[a]) && mx[a] >= mn[a], DFSPH_E_INVALID,
                      "invalid grid bounding box");
@@ -325,8 +324,13 @@ public:
             dim[a] = fmax + off[a] + 6;
             DF_CHECK(dim[a] <= 1024, DFSPH_E_INVALID,
                      "domain too large: more than 1024 cells of size 4r along one axis");
-            maxdim = std::max(maxdim, dim[a]);
         }
+        return alloc_grid();
+    }
+
+    // Cell tables for the current off / dim (also used when a checkpoint restores them).
+    int alloc_grid() {
+        const int maxdim = std::max(dim[0], std::max(dim[1], dim[2]));
         int bits = 1;
         while ((1 << bits) < maxdim) ++bits;
         key_passes = std::min(4, (3 * bits + 1 + 7) / 8);
@@ -1136,6 +1140,172 @@ public:
         return DFSPH_OK;
     }
 
+    // ---- binary checkpoint: the complete solver state, for exact resume ---------------------------
+    // Layout: magic, version, sizeof(Real), counts, the scene block, dt history, grid, then the
+    // fluid arrays in their current (cell-sorted) order, the boundary arrays in sorted order with
+    // their upload indices, and the learned warm-start state when the mode is on. Restoring the
+    // internal order (not just the particles) is what makes a resumed run bit-identical.
+    static constexpr char kCkptMagic[8] = {'D', 'F', 'S', 'P', 'H', 'C', 'K', '1'};
+
+    template <class T> int dev_to_file(std::ofstream& f, const T* d, size_t count) {
+        std::vector<T> h(count);
+        if (count) {
+            DF_CUDA(cudaMemcpyAsync(h.data(), d, count * sizeof(T), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+        }
+        f.write(reinterpret_cast<const char*>(h.data()), (std::streamsize)(count * sizeof(T)));
+        return DFSPH_OK;
+    }
+    template <class T> int file_to_dev(std::ifstream& f, T* d, size_t count) {
+        std::vector<T> h(count);
+        f.read(reinterpret_cast<char*>(h.data()), (std::streamsize)(count * sizeof(T)));
+        DF_CHECK((bool)f, DFSPH_E_INVALID, "truncated checkpoint");
+        if (count) {
+            DF_CUDA(cudaMemcpyAsync(d, h.data(), count * sizeof(T), cudaMemcpyHostToDevice, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+        }
+        return DFSPH_OK;
+    }
+    template <class T> static void put(std::ofstream& f, const T& v) { f.write(reinterpret_cast<const char*>(&v), sizeof(T)); }
+    template <class T> static bool get(std::ifstream& f, T& v) { return (bool)f.read(reinterpret_cast<char*>(&v), sizeof(T)); }
+
+    int save_checkpoint(const char* path) {
+        DF_CHECK(path, DFSPH_E_INVALID, "null path");
+        DF_CHECK(grid_ready, DFSPH_E_STATE, "nothing to checkpoint");
+        std::ofstream f(path, std::ios::binary | std::ios::trunc);
+        DF_CHECK(f.is_open(), DFSPH_E_INVALID, std::string("cannot open ") + path);
+        f.write(kCkptMagic, 8);
+        put(f, (int32_t)1);
+        put(f, (int32_t)sizeof(Real));
+        put(f, n);
+        put(f, nb);
+        put(f, sc);
+        for (double v : {h, h_future, h_past, inv_h, inv_h_future, h_ratio, h_ratio2, time_step}) put(f, v);
+        for (int a = 0; a < 3; ++a) put(f, (int32_t)off[a]);
+        for (int a = 0; a < 3; ++a) put(f, (int32_t)dim[a]);
+        put(f, (int32_t)(boundary_moving ? 1 : 0));
+        put(f, (int32_t)(learned ? 1 : 0));
+        DF_TRY(dev_to_file(f, pos[cur], n));
+        DF_TRY(dev_to_file(f, vel[cur], n));
+        DF_TRY(dev_to_file(f, kappa[cur], n));
+        DF_TRY(dev_to_file(f, kappaV[cur], n));
+        DF_TRY(dev_to_file(f, id[cur], n));
+        DF_TRY(dev_to_file(f, bpos[0], nb));
+        DF_TRY(dev_to_file(f, bvel[0], nb));
+        DF_TRY(dev_to_file(f, bid, nb));
+        if (learned) {
+            DF_TRY(dev_to_file(f, kappaT[cur], n));
+            DF_TRY(dev_to_file(f, kappaVT[cur], n));
+            DF_TRY(dev_to_file(f, mlp.params, (size_t)kMlpParams));
+            DF_TRY(dev_to_file(f, mlp.adam_m, (size_t)kMlpParams));
+            DF_TRY(dev_to_file(f, mlp.adam_v, (size_t)kMlpParams));
+            put(f, h_scales);
+            for (int32_t v : {adam_t, (int32_t)mlp_ready, (int32_t)scales_set, (int32_t)probe, train_interval,
+                              train_start, train_iters, (int32_t)train_batch})
+                put(f, v);
+            for (double v : {lr, damping}) put(f, v);
+            for (uint64_t v : {lsteps, trainings, kept_v, kept_p, solves_v, solves_p}) put(f, v);
+            put(f, mlp_seed);
+        }
+        DF_CHECK(f.good(), DFSPH_E_INVALID, std::string("write failed: ") + path);
+        return DFSPH_OK;
+    }
+
+    int load_checkpoint(const char* path) {
+        DF_CHECK(path, DFSPH_E_INVALID, "null path");
+        std::ifstream f(path, std::ios::binary);
+        DF_CHECK(f.is_open(), DFSPH_E_INVALID, std::string("cannot open ") + path);
+        char magic[8];
+        f.read(magic, 8);
+        DF_CHECK(f && std::memcmp(magic, kCkptMagic, 8) == 0, DFSPH_E_INVALID, "not a DFSPH checkpoint");
+        int32_t version = 0, rbytes = 0;
+        uint32_t cn = 0, cnb = 0;
+        dfsph_scene csc{};
+        DF_CHECK(get(f, version) && version == 1 && get(f, rbytes) && get(f, cn) && get(f, cnb) && get(f, csc),
+                 DFSPH_E_INVALID, "bad checkpoint header");
+        DF_CHECK(rbytes == (int32_t)sizeof(Real), DFSPH_E_INVALID, "checkpoint precision differs from the context's");
+        DF_CHECK(cn <= Nc && cnb <= Bc, DFSPH_E_INVALID, "checkpoint exceeds the context's capacities");
+        DF_CHECK(csc.neighbor_capacity == sc.neighbor_capacity, DFSPH_E_INVALID, "neighbor_capacity differs");
+        double dt[8];
+        for (double& v : dt) DF_CHECK(get(f, v), DFSPH_E_INVALID, "truncated checkpoint");
+        int32_t g[6], moving = 0, was_learned = 0;
+        for (int32_t& v : g) DF_CHECK(get(f, v), DFSPH_E_INVALID, "truncated checkpoint");
+        DF_CHECK(get(f, moving) && get(f, was_learned), DFSPH_E_INVALID, "truncated checkpoint");
+        // scene parameters of the run; this context keeps its own capacities, device and graph mode
+        csc.fluid_capacity = sc.fluid_capacity;
+        csc.boundary_capacity = sc.boundary_capacity;
+        csc.device = sc.device;
+        csc.use_graphs = sc.use_graphs;
+        sc = csc;
+        for (int a = 0; a < 3; ++a) {
+            off[a] = g[a];
+            dim[a] = g[3 + a];
+            DF_CHECK(dim[a] > 0 && dim[a] <= 1024, DFSPH_E_INVALID, "bad grid in checkpoint");
+        }
+        DF_TRY(alloc_grid());
+        grid_ready = true;
+        invalidate_graphs();
+        n = cn;
+        nb = cnb;
+        cur = 0;
+        DF_TRY(file_to_dev(f, pos[0], n));
+        DF_TRY(file_to_dev(f, vel[0], n));
+        DF_TRY(file_to_dev(f, kappa[0], n));
+        DF_TRY(file_to_dev(f, kappaV[0], n));
+        DF_TRY(file_to_dev(f, id[0], n));
+        DF_TRY(file_to_dev(f, bpos[1], nb));  // sorted order; re-sorting keeps it and rebuilds the table
+        DF_TRY(file_to_dev(f, bvel[1], nb));
+        std::vector<uint32_t> saved_bid(nb);
+        f.read(reinterpret_cast<char*>(saved_bid.data()), (std::streamsize)(nb * sizeof(uint32_t)));
+        DF_CHECK((bool)f, DFSPH_E_INVALID, "truncated checkpoint");
+        if (nb) {
+            DF_TRY(sort_boundary(false));
+            DF_CUDA(cudaMemcpyAsync(bid, saved_bid.data(), nb * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        }
+        boundary_moving = moving != 0;
+        DF_CUDA(cudaMemsetAsync(counts, 0, (size_t)Nc * sizeof(uint32_t), stream));
+        DF_CUDA(cudaMemsetAsync(status, 0, 4 * sizeof(uint32_t), stream));
+        if (was_learned) {
+            learned = false;
+            DF_TRY(enable_learned(true));
+            DF_TRY(file_to_dev(f, kappaT[0], n));
+            DF_TRY(file_to_dev(f, kappaVT[0], n));
+            DF_TRY(file_to_dev(f, mlp.params, (size_t)kMlpParams));
+            DF_TRY(file_to_dev(f, mlp.adam_m, (size_t)kMlpParams));
+            DF_TRY(file_to_dev(f, mlp.adam_v, (size_t)kMlpParams));
+            int32_t iv[8];
+            double dv[2];
+            uint64_t uv[6];
+            DF_CHECK(get(f, h_scales), DFSPH_E_INVALID, "truncated checkpoint");
+            for (int32_t& v : iv) DF_CHECK(get(f, v), DFSPH_E_INVALID, "truncated checkpoint");
+            for (double& v : dv) DF_CHECK(get(f, v), DFSPH_E_INVALID, "truncated checkpoint");
+            for (uint64_t& v : uv) DF_CHECK(get(f, v), DFSPH_E_INVALID, "truncated checkpoint");
+            DF_CHECK(get(f, mlp_seed), DFSPH_E_INVALID, "truncated checkpoint");
+            adam_t = iv[0];
+            mlp_ready = iv[1] != 0;
+            scales_set = iv[2] != 0;
+            probe = iv[3] != 0;
+            train_interval = iv[4];
+            train_start = iv[5];
+            train_iters = iv[6];
+            train_batch = (uint32_t)iv[7];
+            lr = dv[0];
+            damping = dv[1];
+            lsteps = uv[0]; trainings = uv[1]; kept_v = uv[2]; kept_p = uv[3]; solves_v = uv[4]; solves_p = uv[5];
+            DF_TRY(upload_scales());
+            launch_mlp_pack(mlp, stream);
+            launches += 1;
+        } else if (learned) {
+            DF_TRY(enable_learned(false));
+        }
+        h = dt[0]; h_future = dt[1]; h_past = dt[2]; inv_h = dt[3]; inv_h_future = dt[4];
+        h_ratio = dt[5]; h_ratio2 = dt[6]; time_step = dt[7];
+        use_graphs = sc.use_graphs != 0;
+        DF_TRY(sync_state());
+        DF_CUDA(cudaStreamSynchronize(stream));
+        return DFSPH_OK;
+    }
+
     // ---- snapshots (reference text format, see dfsph_c.h) -----------------------------------------
     static std::string join(const char* dir, const char* name) {
         std::string d(dir);
@@ -1639,6 +1809,8 @@ int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launc
     DFSPH_DISPATCH(ctx, time_kernel(kernel, reps, ms_per_launch));
 }
 int dfsph_save_snapshot(dfsph_ctx* ctx, const char* dir, int what) { DFSPH_DISPATCH(ctx, save_snapshot(dir, what)); }
+int dfsph_checkpoint_save(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, save_checkpoint(path)); }
+int dfsph_checkpoint_load(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, load_checkpoint(path)); }
 int dfsph_load_snapshot(dfsph_ctx* ctx, const char* dir, int what, int load_velocities) {
     DFSPH_DISPATCH(ctx, load_snapshot(dir, what, load_velocities != 0));
 }

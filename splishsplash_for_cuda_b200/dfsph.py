@@ -299,6 +299,13 @@ class DFSPHCUDA:
         what = (_capi.SNAP_FLUID if fluid else 0) | (_capi.SNAP_BOUNDARY if boundary else 0)
         self._call(self._lib.dfsph_load_snapshot(self._ctx, str(folder).encode(), what, 1 if load_velocities else 0))
 
+    def checkpoint_save(self, path) -> None:
+        """Binary checkpoint of the complete state (exact resume)."""
+        self._call(self._lib.dfsph_checkpoint_save(self._ctx, str(path).encode()))
+
+    def checkpoint_load(self, path) -> None:
+        self._call(self._lib.dfsph_checkpoint_load(self._ctx, str(path).encode()))
+
     # ---- learned warm start (no reference counterpart) ------------------------------------------
     def set_learned_warm_start(self, on: bool = True, probe: bool = True, train_interval: int | None = None,
                                train_iters: int | None = None, train_batch: int | None = None,
