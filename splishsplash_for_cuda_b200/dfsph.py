@@ -91,11 +91,15 @@ class DFSPHData:
 class DFSPHCUDA:
     """Drop-in for SPH::DFSPHCUDA over one scene (fluid + static box walls)."""
 
-    def __init__(self, scene: Scene, precision: int = 32, device: int = 0, use_graphs: bool = True,
+    def __init__(self, scene: Scene, precision: int | None = None, device: int = 0, use_graphs: bool = True,
                  neighbor_capacity: int = 96, boundary_psi: np.ndarray | None = None,
                  fluid_capacity: int | None = None, lib_path: str | None = None):
+        """precision None takes the scene's (Configuration "precision", default 32); the scene's
+        "learnedWarmStart" block, when present, configures the learned warm start."""
         self._lib = _capi.load(lib_path)
         self.scene = scene
+        if precision is None:
+            precision = int(getattr(scene.config, "precision", 32) or 32)
         self.precision = precision
         self._struct = scene_struct(scene, precision, device, use_graphs, neighbor_capacity, fluid_capacity,
                                     lib_path=lib_path)
@@ -110,6 +114,13 @@ class DFSPHCUDA:
         self.last_stats = None
         self.m_data = DFSPHData(self)
         self.reset()
+        lws = getattr(scene.config, "learnedWarmStart", None)
+        if lws and lws.get("enabled", True):
+            if "damping" in lws:
+                self.set_param("warm_start_damping", float(lws["damping"]))
+            self.set_learned_warm_start(True, probe=bool(lws.get("probe", True)),
+                                        train_interval=lws.get("trainInterval"), train_iters=lws.get("trainIters"),
+                                        train_batch=lws.get("trainBatch"), learning_rate=lws.get("learningRate"))
 
     # ---- lifetime ------------------------------------------------------------------------------
     def close(self) -> None:

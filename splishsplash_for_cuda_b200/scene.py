@@ -136,6 +136,11 @@ class Configuration:
     maxErrorV: float = 0.1
     enableDivergenceSolver: bool = True
     simulationMethod: int = 6
+    # extensions (keys the reference does not read): arithmetic precision of the solver (32 / 64) and
+    # the learned warm start ({"enabled": true, "trainInterval": 50, "trainIters": 20,
+    # "trainBatch": 4096, "learningRate": 1e-3, "damping": 0.95, "probe": true})
+    precision: int = 32
+    learnedWarmStart: dict | None = None
 
 
 @dataclass
@@ -177,6 +182,19 @@ def load_scene(path: str | Path) -> Scene:
             setattr(cfg, key, int(c[key]))
     if "enableDivergenceSolver" in c:
         cfg.enableDivergenceSolver = bool(c["enableDivergenceSolver"])
+    if "precision" in c:
+        cfg.precision = int(c["precision"])
+        if cfg.precision not in (32, 64):
+            raise ValueError("precision must be 32 or 64")
+    lws = c.get("learnedWarmStart")
+    if lws is not None:
+        if not isinstance(lws, dict):
+            raise ValueError("learnedWarmStart must be an object")
+        unknown = set(lws) - {"enabled", "trainInterval", "trainIters", "trainBatch", "learningRate", "damping",
+                              "probe"}
+        if unknown:
+            raise ValueError(f"unknown learnedWarmStart keys: {sorted(unknown)}")
+        cfg.learnedWarmStart = dict(lws)
     cfg.gravitation = _readvec(c.get("gravitation"), cfg.gravitation)
     r = cfg.particleRadius
     seed = int(c.get("seed", 1))
