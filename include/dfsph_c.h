@@ -171,7 +171,11 @@ int dfsph_get_neighbors(dfsph_ctx* ctx, uint32_t* counts, uint32_t* lists, uint3
 
 /* DFSPHCUDA::step() (DFSPH_CUDA.cpp:82-794) without rendering, dynamic bodies, open boundaries or
  * the dynamic window: neighbour search -> divergence solve -> XSPH + gravity -> dt update ->
- * velocity update -> pressure solve -> position update -> onSimulationStepEnd. stats may be null. */
+ * velocity update -> pressure solve -> position update -> onSimulationStepEnd. The whole step runs on
+ * the device, dt updates (CFL) included. With stats the call waits for the step and fills them; with
+ * stats null it only enqueues the step and returns (no read-back): dfsph_synchronize waits, and
+ * dfsph_status / dfsph_get_param ("iterations_sum", "iterations_v_sum", "h", ...) read the results
+ * (non-converged solves raise their status bits on the device). */
 int dfsph_step(dfsph_ctx* ctx, dfsph_step_stats* stats);
 
 /* The seven host functions of DFSPH_core_cuda.h:27-74, for callers that drive the step themselves. */
@@ -190,6 +194,8 @@ int dfsph_on_step_end(dfsph_ctx* ctx);                                    /* onS
  * "enable_divergence_solver", "cfl_method", "cfl_factor", "cfl_max_time_step", "cfl_min_time_step",
  * "time_step" (sets the dt the next dt update uses), "gravitation_x|y|z", "use_graphs",
  * "h", "h_future", "h_past", "inv_h" (dt history of DFSPHCData), "timing" (1: record CUDA events),
+ * "iterations_sum" (setting it clears the counters; reading it gives the pressure iterations of all
+ * solves since, "iterations_v_sum" the divergence iterations),
  * "boundary_forces" (1: accumulate the fluid's force on every boundary particle in each Jacobi pass,
  * -m_i k_i psi_b grad W_ib summed over both solves of a step, as the reference does for dynamic
  * bodies; cleared by each neighbour search; atomics, so the summation order varies),

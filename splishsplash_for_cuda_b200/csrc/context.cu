@@ -105,9 +105,14 @@ public:
     bool timing = false;
     uint64_t launches = 0;
 
-    // dt history (DFSPHCData h, h_future, h_past, h_ratio_to_past(2), invH, invH_future)
+    // dt history (DFSPHCData h, h_future, h_past, h_ratio_to_past(2), invH, invH_future). The device
+    // block dtd is authoritative (the dt updates of a step run on the device); these are host mirrors,
+    // refreshed by every read-back (collect, pull_dt) and pushed by push_dt.
     double h = 0, h_future = 0, h_past = 0, inv_h = 0, inv_h_future = 0, h_ratio = 1, h_ratio2 = 1;
     double time_step = 0;
+    double* dtd = nullptr;
+    double* h_dt = nullptr;  // pinned mirror of dtd
+    bool dt_stale = false;   // the device changed dtd since the last read-back
     bool use_graphs = true;
     cudaGraphExec_t g_loop[2] = {nullptr, nullptr};  // [0] divergence, [1] pressure
     uint32_t g_loop_n[2] = {0, 0};
@@ -136,7 +141,6 @@ public:
     double damping = 0.95;  // learned warm start: at most damping x the predicted needed coefficient
     int adam_t = 0;
     uint64_t lsteps = 0, trainings = 0, kept_v = 0, kept_p = 0, solves_v = 0, solves_p = 0;
-    double hr_used = 1.0, r2_used = 1.0;  // dt ratios the two warm starts of this step used
     uint32_t forced_warm = 0;             // learned candidates used without a probe this step
     bool step_trained = false;
 
@@ -193,6 +197,8 @@ public:
         DF_CUDA(cudaMalloc((void**)&ds, sizeof(DevState<Real>)));
         DF_CUDA(cudaMallocHost((void**)&h_ctl, 3 * sizeof(LoopCtl)));
         DF_CUDA(cudaMallocHost((void**)&h_status, 4 * sizeof(uint32_t)));
+        DF_TRY(dalloc(&dtd, kDtSlots));
+        DF_CUDA(cudaMallocHost((void**)&h_dt, kDtSlots * sizeof(double)));
         DF_CUDA(cudaMemsetAsync(ctl, 0, 4 * sizeof(LoopCtl), stream));
         DF_CUDA(cudaMemsetAsync(status, 0, 4 * sizeof(uint32_t), stream));
         DF_CUDA(cudaMemsetAsync(counts, 0, Nc * sizeof(uint32_t), stream));
@@ -200,8 +206,9 @@ public:
         DF_CUDA(cudaEventCreate(&ev1));
         time_step = s.time_step;
         use_graphs = s.use_graphs != 0;
+        DF_TRY(sync_state());
         reset_dt();
-        return sync_state();
+        return DFSPH_OK;
     }
 
     void release() {
@@ -226,6 +233,8 @@ public:
         f(mlp.w1_bf16); f(mlp.w2_bf16); f(mlp.w3_bf16); f(mlp.scales); f(mlp.loss);
         if (h_ctl) cudaFreeHost(h_ctl);
         if (h_status) cudaFreeHost(h_status);
+        if (h_dt) cudaFreeHost(h_dt);
+        f(dtd);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -236,6 +245,30 @@ public:
         h = h_future = h_past = time_step;
         inv_h = inv_h_future = 1.0 / time_step;
         h_ratio = h_ratio2 = 1.0;
+        push_dt();
+    }
+
+    // Host mirrors -> device dt block (and the Real copies the kernels read).
+    void push_dt() {
+        DtArgs a{};
+        a.v[kDtH] = h; a.v[kDtHFuture] = h_future; a.v[kDtHPast] = h_past; a.v[kDtInvH] = inv_h;
+        a.v[kDtInvHFuture] = inv_h_future; a.v[kDtRatio] = h_ratio; a.v[kDtRatio2] = h_ratio2;
+        a.v[kDtFixed] = time_step; a.v[kDtRatioUsedV] = h_ratio; a.v[kDtRatio2UsedP] = h_ratio2;
+        launch_dt<Real>(ds, 0, a, stream);
+        launches += 1;
+        dt_stale = false;
+    }
+    void mirror_dt() {
+        h = h_dt[kDtH]; h_future = h_dt[kDtHFuture]; h_past = h_dt[kDtHPast]; inv_h = h_dt[kDtInvH];
+        inv_h_future = h_dt[kDtInvHFuture]; h_ratio = h_dt[kDtRatio]; h_ratio2 = h_dt[kDtRatio2];
+        dt_stale = false;
+    }
+    int pull_dt() {
+        if (!dt_stale) return DFSPH_OK;
+        DF_CUDA(cudaMemcpyAsync(h_dt, dtd, kDtSlots * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        mirror_dt();
+        return DFSPH_OK;
     }
 
     // Parameters of the kernels derived from the scene and the dt history.
@@ -290,6 +323,7 @@ public:
         hs.ctl = ctl;
         hs.status = status;
         hs.cfl_partials = cfl_partials;
+        hs.dtd = dtd;
         hs.bforce = boundary_forces ? bforce : nullptr;
         hs.features = features;
         hs.pred = pred;
@@ -602,7 +636,7 @@ public:
     int divergence_solve(int max_iter, double max_error, bool lp = false) {
         if (!n) return DFSPH_OK;
         DF_CUDA(cudaMemsetAsync(&ctl[0].ticket, 0, sizeof(uint32_t), stream));
-        const double eta = max_error * 0.01 * sc.density0 / h;
+        const double eta = max_error * 0.01 * sc.density0;  // divided by the device's h in the init pass
         if (!lp) {
             launch_density_alpha<Real>(ds, n, true, false, stream);
             launch_divergence_warm_jacobi<Real>(ds, n, nullptr, nullptr, stream, boundary_forces);
@@ -612,7 +646,6 @@ public:
             const bool use = mlp_ready;
             launch_density_alpha<Real>(ds, n, false, true, stream);
             if (use) launch_mlp_forward(mlp, features, n, pred, stream);
-            hr_used = h_ratio;
             launch_warm_values<Real>(ds, n, 0, use, damping, stream);
             launches += use ? 3 : 2;
             if (use && probe) {  // plain candidate: velocities into velP, initial residual into ctl[3]
@@ -648,7 +681,6 @@ public:
             launches += 2;
         } else {
             const bool use = mlp_ready;
-            r2_used = h_ratio2;
             launch_warm_values<Real>(ds, n, 1, use, damping, stream);
             launches += 1;
             if (use && probe) {
@@ -681,29 +713,33 @@ public:
         return DFSPH_OK;
     }
 
+    // DFSPHCData::updateTimeStep (DFSPH_c_arrays_structure.cpp:1100-1112), on the device; hf <= 0
+    // takes the fixed time step.
     int update_time_step(double hf) {
         DF_CHECK(hf > 0 && std::isfinite(hf), DFSPH_E_INVALID, "time step must be finite and > 0");
-        h_future = hf;
-        inv_h_future = 1.0 / hf;
-        h_ratio = h / hf;
-        h_ratio2 = (h * h) / (hf * hf);
-        return sync_state();
+        DtArgs a{};
+        a.v[0] = hf;
+        launch_dt<Real>(ds, 1, a, stream);
+        launches += 1;
+        dt_stale = true;
+        DF_CUDA(cudaGetLastError());
+        return DFSPH_OK;
     }
 
-    // cuda_CFL (DFSPH_core_cuda.cu:3321-3394): dt = cfl * 0.4 * 2r / sqrt(max |v + a h|^2), clamped.
+    // cuda_CFL (DFSPH_core_cuda.cu:3321-3394): dt = cfl * 0.4 * 2r / sqrt(max |v + a h|^2), clamped,
+    // reduced and applied on the device (no host round trip).
     int cfl(double min_dt, double factor_, double max_dt) {
-        double vmax = 0.0;
-        if (n) {
-            launch_cfl_reduce<Real>(ds, grid_for(n), stream);
-            launches += 1;
-            DF_CUDA(cudaMemcpyAsync(h_ctl + 2, ctl + 2, sizeof(LoopCtl), cudaMemcpyDeviceToHost, stream));
-            DF_CUDA(cudaStreamSynchronize(stream));
-            vmax = h_ctl[2].sum;
-        }
-        double hn = factor_ * 0.4 * (2.0 * sc.particle_radius / std::sqrt(vmax));
-        hn = std::min(hn, max_dt);
-        hn = std::max(hn, min_dt);
-        return update_time_step(hn);
+        launch_cfl_reduce<Real>(ds, n ? grid_for(n) : 0, stream);
+        DtArgs a{};
+        a.v[0] = factor_;
+        a.v[1] = min_dt;
+        a.v[2] = max_dt;
+        a.v[3] = 2.0 * sc.particle_radius;
+        launch_dt<Real>(ds, 2, a, stream);
+        launches += 2;
+        dt_stale = true;
+        DF_CUDA(cudaGetLastError());
+        return DFSPH_OK;
     }
 
     int update_vel() {
@@ -724,17 +760,20 @@ public:
     }
 
     int on_step_end() {
-        h_past = h;
-        h = h_future;
-        inv_h = inv_h_future;
-        return sync_state();
+        launch_dt<Real>(ds, 3, DtArgs{}, stream);
+        launches += 1;
+        dt_stale = true;
+        DF_CUDA(cudaGetLastError());
+        return DFSPH_OK;
     }
 
     // Reads the loop control blocks and the status word (one synchronisation).
     int collect(bool div_ran, int max_iter_v, int max_iter) {
         DF_CUDA(cudaMemcpyAsync(h_ctl, ctl, 2 * sizeof(LoopCtl), cudaMemcpyDeviceToHost, stream));
         DF_CUDA(cudaMemcpyAsync(h_status, status, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaMemcpyAsync(h_dt, dtd, kDtSlots * sizeof(double), cudaMemcpyDeviceToHost, stream));
         DF_CUDA(cudaStreamSynchronize(stream));
+        mirror_dt();
         last_iters = n ? h_ctl[1].iter : 0;
         last_err = h_ctl[1].avg;
         last_iters_v = (div_ran && n) ? h_ctl[0].iter : 0;
@@ -752,7 +791,6 @@ public:
     int step(dfsph_step_stats* st) {
         DF_CHECK(grid_ready, DFSPH_E_STATE, "step before any boundary or fluid upload");
         if (timing) DF_CUDA(cudaEventRecord(ev0, stream));
-        const double h_used = h;
         const bool lp = learned && n > 0;
         forced_warm = 0;
         step_trained = false;
@@ -791,9 +829,9 @@ public:
             launches += 1;
             ++lsteps;
         }
-        const double h_next = h_future;
         DF_TRY(on_step_end());
         if (timing) DF_CUDA(cudaEventRecord(ev1, stream));
+        if (!st) return DFSPH_OK;  // asynchronous step: nothing read back, the host does not wait
         DF_TRY(collect(div, sc.max_iterations_v, sc.max_iterations));
         if (lp) {
             const uint32_t w = (h_status[2] | forced_warm) & 3u;
@@ -805,8 +843,8 @@ public:
             st->iterations_v = last_iters_v;
             st->density_error = last_err;
             st->divergence_error = last_err_v;
-            st->h = h_used;
-            st->h_future = h_next;
+            st->h = h_past;  // after onSimulationStepEnd: the step's dt is h_past, the next one h
+            st->h_future = h;
             st->status = h_status[0];
             st->num_fluid = n;
             st->warm_start = lp ? ((h_status[2] | forced_warm) & 3u) : 0u;
@@ -953,7 +991,7 @@ public:
         adam_t = 0;
         h_scales = ns;
         DF_TRY(upload_scales());  // synchronises: prm goes out of scope
-        launch_gather_training<Real>(ds, n, B, offset, r2_used, hr_used, div, tx, tt, stream);  // targets / new scale
+        launch_gather_training<Real>(ds, n, B, offset, div, tx, tt, stream);  // targets / new scale
         launches += 1;
         return DFSPH_OK;
     }
@@ -964,7 +1002,7 @@ public:
         uint32_t B = std::min<uint32_t>(std::min<uint32_t>(train_batch, kMaxTrainBatch), n);
         if (!B) return DFSPH_OK;
         const uint32_t offset = (uint32_t)((lsteps * 2654435761ull) % n);
-        launch_gather_training<Real>(ds, n, B, offset, r2_used, hr_used, div, tx, tt, stream);
+        launch_gather_training<Real>(ds, n, B, offset, div, tx, tt, stream);
         launches += 1;
         DF_TRY(adapt_scales(B, offset, div));
         for (int it = 0; it < train_iters; ++it)
@@ -1172,6 +1210,7 @@ public:
     int save_checkpoint(const char* path) {
         DF_CHECK(path, DFSPH_E_INVALID, "null path");
         DF_CHECK(grid_ready, DFSPH_E_STATE, "nothing to checkpoint");
+        DF_TRY(pull_dt());
         std::ofstream f(path, std::ios::binary | std::ios::trunc);
         DF_CHECK(f.is_open(), DFSPH_E_INVALID, std::string("cannot open ") + path);
         f.write(kCkptMagic, 8);
@@ -1301,6 +1340,7 @@ public:
         h = dt[0]; h_future = dt[1]; h_past = dt[2]; inv_h = dt[3]; inv_h_future = dt[4];
         h_ratio = dt[5]; h_ratio2 = dt[6]; time_step = dt[7];
         use_graphs = sc.use_graphs != 0;
+        push_dt();
         DF_TRY(sync_state());
         DF_CUDA(cudaStreamSynchronize(stream));
         return DFSPH_OK;
@@ -1359,6 +1399,7 @@ public:
 
     int save_snapshot(const char* dir, int what) {
         DF_CHECK(dir, DFSPH_E_INVALID, "null directory");
+        DF_TRY(pull_dt());
         if (what & DFSPH_SNAP_FLUID) {
             DF_TRY(write_set(join(dir, "fluid_file.txt"), false));
             std::ofstream g(join(dir, "general_data.txt"), std::ios::trunc);
@@ -1434,15 +1475,24 @@ public:
         else if (k == "cfl_factor") sc.cfl_factor = v;
         else if (k == "cfl_max_time_step") sc.cfl_max_time_step = v;
         else if (k == "cfl_min_time_step") sc.cfl_min_time_step = v;
-        else if (k == "time_step") { DF_CHECK(v > 0, DFSPH_E_INVALID, "time_step must be > 0"); time_step = v; }
+        else if (k == "time_step") {
+            DF_CHECK(v > 0, DFSPH_E_INVALID, "time_step must be > 0");
+            DF_TRY(pull_dt());
+            time_step = v;
+            dt_changed = true;
+        }
         else if (k == "gravitation_x") sc.gravitation[0] = v;
         else if (k == "gravitation_y") sc.gravitation[1] = v;
         else if (k == "gravitation_z") sc.gravitation[2] = v;
         else if (k == "use_graphs") { use_graphs = v != 0; }
-        else if (k == "h") { h = v; dt_changed = true; }
-        else if (k == "h_future") { h_future = v; dt_changed = true; }
-        else if (k == "h_past") { h_past = v; dt_changed = true; }
-        else if (k == "inv_h") { inv_h = v; dt_changed = true; }
+        else if (k == "h") { DF_TRY(pull_dt()); h = v; dt_changed = true; }
+        else if (k == "h_future") { DF_TRY(pull_dt()); h_future = v; dt_changed = true; }
+        else if (k == "h_past") { DF_TRY(pull_dt()); h_past = v; dt_changed = true; }
+        else if (k == "inv_h") { DF_TRY(pull_dt()); inv_h = v; dt_changed = true; }
+        else if (k == "iterations_sum") {  // clears both loops' iteration counters
+            DF_CUDA(cudaMemsetAsync(&ctl[0].iter_sum, 0, sizeof(uint32_t), stream));
+            DF_CUDA(cudaMemsetAsync(&ctl[1].iter_sum, 0, sizeof(uint32_t), stream));
+        }
         else if (k == "timing") timing = v != 0;
         else if (k == "learned_warm_start") return enable_learned(v != 0);
         else if (k == "warm_start_probe") probe = v != 0;
@@ -1476,12 +1526,22 @@ public:
             return mlp_reset((uint32_t)v);
         }
         else DF_CHECK(false, DFSPH_E_INVALID, "unknown parameter key: " + k);
-        (void)dt_changed;
+        if (dt_changed) push_dt();
         return sync_state();
     }
 
     int get_param(const std::string& k, double* v) {
         DF_CHECK(v, DFSPH_E_INVALID, "null output");
+        if (k == "h" || k == "h_future" || k == "h_past" || k == "inv_h" || k == "h_ratio_to_past" ||
+            k == "h_ratio_to_past2")
+            DF_TRY(pull_dt());
+        if (k == "iterations_sum" || k == "iterations_v_sum") {
+            LoopCtl c[2];
+            DF_CUDA(cudaMemcpyAsync(c, ctl, 2 * sizeof(LoopCtl), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+            *v = k == "iterations_sum" ? c[1].iter_sum : c[0].iter_sum;
+            return DFSPH_OK;
+        }
         if (k == "viscosity") *v = sc.viscosity;
         else if (k == "density0") *v = sc.density0;
         else if (k == "max_error") *v = sc.max_error;

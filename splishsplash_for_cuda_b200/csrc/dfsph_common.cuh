@@ -285,7 +285,7 @@ struct LoopCtl {
     int32_t min_iter;
     uint32_t cont;       // loop condition for the next iteration
     uint32_t ticket;     // last-block election counter
-    uint32_t pad;
+    uint32_t iter_sum;   // iterations of every loop ended since the counter was last cleared
     double aux;          // second sum of an init pass that reduces two values (learned warm start)
 };
 

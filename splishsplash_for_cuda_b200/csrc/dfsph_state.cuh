@@ -34,6 +34,7 @@ template <class Real> struct DevState {
     // reductions and control
     double* partials;      // one FP64 partial per block
     LoopCtl* ctl;          // [0] divergence loop, [1] pressure loop, [2] CFL / misc, [3] candidate probe
+    double* dtd;           // dt history in FP64 (see DtSlot); the kernels read their Real copies in p
     uint32_t* status;      // [0] DFSPH_ST_* bits, [1] scratch, [2] learned warm start kept (bit 0 div, 1 pressure)
     float* cfl_partials;   // per-block max |v + a h|^2
     // learned warm start (see mlp.cuh)
@@ -99,8 +100,8 @@ template <class Real> void launch_totals(const DevState<Real>* d, uint32_t n, bo
 // Training pairs of `batch` particles spread over [0, n): x = features, t = targets
 // [(needed kappa)/r2 - kappaT_prev, (needed kappa_v)/hr - kappaVT_prev] / out_scale.
 template <class Real>
-void launch_gather_training(const DevState<Real>* d, uint32_t n, uint32_t batch, uint32_t offset, double r2, double hr,
-                            bool div_ran, float* x, float* t, cudaStream_t s);
+void launch_gather_training(const DevState<Real>* d, uint32_t n, uint32_t batch, uint32_t offset, bool div_ran, float* x,
+                            float* t, cudaStream_t s);
 // keep: also store the unclamped residual in residV (learned warm start).
 template <class Real>
 void launch_divergence_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,

@@ -146,12 +146,57 @@ __global__ void __launch_bounds__(kBlock) unpack_counts_kernel(const uint32_t* _
 
 // Publishes a new device state block. The block travels as a kernel parameter, so the update is
 // ordered with the surrounding work on the stream and never reads host memory asynchronously.
-template <class Real> __global__ void set_state_kernel(DevState<Real>* __restrict__ dst, DevState<Real> v) { *dst = v; }
+template <class Real> __global__ void set_state_kernel(DevState<Real>* __restrict__ dst, DevState<Real> v) {
+    const StepParams<Real>& o = dst->p;  // dt fields stay as the device has them
+    v.p.h = o.h;
+    v.p.h_future = o.h_future;
+    v.p.inv_h = o.inv_h;
+    v.p.inv_h_future = o.inv_h_future;
+    v.p.h_ratio_to_past = o.h_ratio_to_past;
+    v.p.h_ratio_to_past2 = o.h_ratio_to_past2;
+    *dst = v;
+}
+
+template <class Real> __global__ void dt_kernel(DevState<Real>* __restrict__ ds, int op, DtArgs a) {
+    double* t = ds->dtd;
+    StepParams<Real>& p = ds->p;
+    if (op == 0) {
+        for (int k = 0; k < kDtSlots; ++k) t[k] = a.v[k];
+    } else if (op == 1 || op == 2) {
+        double hf;
+        if (op == 1) {
+            hf = a.v[0] > 0.0 ? a.v[0] : t[kDtFixed];
+        } else {
+            const double vmax2 = ds->ctl[2].sum;
+            hf = a.v[0] * 0.4 * (a.v[3] / sqrt(vmax2));
+            hf = (a.v[2] < hf) ? a.v[2] : hf;  // std::min(hf, max), NaN as std::min treats it
+            hf = (hf < a.v[1]) ? a.v[1] : hf;  // std::max(hf, min)
+        }
+        const double h = t[kDtH];
+        t[kDtHFuture] = hf;
+        t[kDtInvHFuture] = 1.0 / hf;
+        t[kDtRatio] = h / hf;
+        t[kDtRatio2] = (h * h) / (hf * hf);
+    } else {  // op 3
+        t[kDtHPast] = t[kDtH];
+        t[kDtH] = t[kDtHFuture];
+        t[kDtInvH] = t[kDtInvHFuture];
+    }
+    p.h = (Real)t[kDtH];
+    p.h_future = (Real)t[kDtHFuture];
+    p.inv_h = (Real)t[kDtInvH];
+    p.inv_h_future = (Real)t[kDtInvHFuture];
+    p.h_ratio_to_past = (Real)t[kDtRatio];
+    p.h_ratio_to_past2 = (Real)t[kDtRatio2];
+}
 
 }  // namespace
 
 template <class Real> void launch_set_state(DevState<Real>* dst, const DevState<Real>& v, cudaStream_t s) {
     set_state_kernel<Real><<<1, 1, 0, s>>>(dst, v);
+}
+template <class Real> void launch_dt(DevState<Real>* d, int op, const DtArgs& a, cudaStream_t s) {
+    dt_kernel<Real><<<1, 1, 0, s>>>(d, op, a);
 }
 
 template <class Real>
@@ -197,6 +242,7 @@ void launch_unpack_counts(const uint32_t* counts, const uint32_t* id, uint32_t n
 
 #define DFSPH_INSTANTIATE_IO(R)                                                                                      \
     template void launch_set_state<R>(DevState<R>*, const DevState<R>&, cudaStream_t);                               \
+    template void launch_dt<R>(DevState<R>*, int, const DtArgs&, cudaStream_t);                                       \
     template void launch_unpack_fluid<R>(const float*, const float*, const float*, float, uint32_t, Vec4<R>*,        \
                                          Vec4<R>*, R*, R*, uint32_t*, cudaStream_t);                                 \
     template void launch_update_fluid<R>(const float*, const float*, uint32_t, const uint32_t*, Vec4<R>*, Vec4<R>*,  \

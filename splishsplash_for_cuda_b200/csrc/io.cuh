@@ -4,7 +4,22 @@
 
 namespace dfsph {
 
+// Publishes the host's DevState block. The dt fields of p are kept from the device: the dt history
+// lives on the device (DtSlot) and only launch_dt changes it.
 template <class Real> void launch_set_state(DevState<Real>* dst, const DevState<Real>& v, cudaStream_t s);
+
+// Slots of the FP64 dt block (DevState::dtd).
+enum DtSlot { kDtH = 0, kDtHFuture, kDtHPast, kDtInvH, kDtInvHFuture, kDtRatio, kDtRatio2, kDtFixed, kDtRatioUsedV,
+              kDtRatio2UsedP, kDtSlots };
+struct DtArgs {
+    double v[kDtSlots];
+};
+// op 0: set every slot from a; op 1: h_future = a.v[0] (or the fixed step kDtFixed if a.v[0] <= 0);
+// op 2: CFL (cuda_CFL, DFSPH_core_cuda.cu:3321-3394): h_future = factor 0.4 diameter / sqrt(max |v + a h|^2)
+// from ctl[2].sum, clamped to [min, max] (a.v = factor, min, max, diameter); op 3: onSimulationStepEnd.
+// Ops 1 and 2 then set 1/h_future and the ratios (DFSPHCData::updateTimeStep,
+// DFSPH_c_arrays_structure.cpp:1100-1112), all in FP64, and refresh the Real copies in p.
+template <class Real> void launch_dt(DevState<Real>* d, int op, const DtArgs& a, cudaStream_t s);
 
 template <class Real>
 void launch_unpack_fluid(const float* xyz, const float* vxyz, const float* mass, float default_mass, uint32_t n,

@@ -14,6 +14,7 @@
 // block reductions whose last block evaluates the loop condition on the device (and, inside a CUDA
 // graph, sets the while-node condition), so no host round trip happens per iteration.
 #include "dfsph_state.cuh"
+#include "io.cuh"
 
 namespace dfsph {
 
@@ -37,10 +38,14 @@ __device__ __forceinline__ uint32_t boundary_count(uint32_t c) { return c >> 16;
 // Deterministic FP64 sum over the grid, then (last block) the loop decision. The partial of each
 // block is reduced in a fixed shuffle pattern and the last block adds the partials in block order.
 // kAux also sums a second value (block partials after the first gridDim.x) into ctl->aux.
+// A loop pass that ends its loop adds its iteration count to ctl->iter_sum and, if the loop ran out
+// of iterations above the tolerance, raises nc_bit in *status (so a step needs no host read to
+// report a non-converged solve).
 template <int kIsInit, bool kAux = false>
 __device__ void reduce_and_decide(double v, double* __restrict__ partials, LoopCtl* __restrict__ ctl, uint32_t n,
                                   double eta, int min_it, int max_it, cudaGraphConditionalHandle handle,
-                                  bool use_handle, double aux = 0.0) {
+                                  bool use_handle, double aux = 0.0, uint32_t* status = nullptr,
+                                  uint32_t nc_bit = 0) {
     __shared__ double warp_sums[kWarpsPerBlock];
     __shared__ double warp_aux[kAux ? kWarpsPerBlock : 1];
     __shared__ bool is_last;
@@ -114,6 +119,10 @@ __device__ void reduce_and_decide(double v, double* __restrict__ partials, LoopC
             ctl->iter = it;
             ctl->avg = avg;
             cont = ((avg > ctl->eta) || (it < ctl->min_iter)) && (it < ctl->max_iter) ? 1u : 0u;
+            if (!cont) {
+                ctl->iter_sum += (uint32_t)it;
+                if (status && it >= ctl->max_iter && avg > ctl->eta) atomicOr(status, nc_bit);
+            }
         }
         ctl->cont = cont;
         ctl->ticket = 0;
@@ -361,6 +370,9 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_residual_
                                                                      double eta, int min_it, int max_it,
                                                                      cudaGraphConditionalHandle handle,
                                                                      bool use_handle) {
+    // The init passes receive the tolerance per unit of h (maxErrorV 0.01 rho0 / h): h is the
+    // device's (the dt history lives on the device).
+    if (kMode != kLoop) eta = eta / ds->dtd[kDtH];
     if (kMode == kFallback && !take_fallback(ds, 0, 1u)) return;  // uniform over the grid
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const Vec4<Real>* __restrict__ vel = kMode == kFallback ? ds->velP : ds->vel;
@@ -391,7 +403,8 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_residual_
     }
     // The learned init pass also sums |r| (unclamped) for the fallback decision.
     reduce_and_decide<kMode != kLoop ? 1 : 0, kKeep && kMode == kInitPass>(
-        contrib, ds->partials, ds->ctl + 0, n, eta, min_it, max_it, handle, use_handle, aux);
+        contrib, ds->partials, ds->ctl + 0, n, eta, min_it, max_it, handle, use_handle, aux, ds->status,
+        DFSPH_ST_DIVERGENCE_NOT_CONVERGED);
 }
 
 // Divergence Jacobi iteration (divergenceSolveParticle<false>): k_i = rho_dot_i alpha_i,
@@ -584,7 +597,8 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_residual_ke
         contrib = (double)dadv;
     }
     reduce_and_decide<kMode != kLoop ? 1 : 0, kKeep && kMode == kInitPass>(
-        contrib, ds->partials, ds->ctl + 1, n, eta, min_it, max_it, handle, use_handle, aux);
+        contrib, ds->partials, ds->ctl + 1, n, eta, min_it, max_it, handle, use_handle, aux, ds->status,
+        DFSPH_ST_PRESSURE_NOT_CONVERGED);
 }
 
 // Pressure Jacobi iteration (pressureSolveParticle<false>): v_i += h_f * [sum (k_i + k_j) m_j grad W_ij
@@ -665,6 +679,7 @@ __global__ void __launch_bounds__(kBlock) warm_values_kernel(const DevState<Real
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
+    if (i == 0) ds->dtd[which == 0 ? kDtRatioUsedV : kDtRatio2UsedP] = ds->dtd[which == 0 ? kDtRatio : kDtRatio2];
     if (which == 0) {
         const Real plain = rmax<Real>(ds->kappaV[i] * p.h_ratio_to_past / Real(2), Real(-0.5));
         Real use = plain;
@@ -724,11 +739,11 @@ __global__ void __launch_bounds__(kBlock) totals_kernel(const DevState<Real>* __
 
 template <class Real>
 __global__ void __launch_bounds__(kBlock) gather_training_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
-                                                                 uint32_t batch, uint32_t offset, double r2, double hr,
-                                                                 bool div_ran, float* __restrict__ x,
-                                                                 float* __restrict__ t) {
+                                                                 uint32_t batch, uint32_t offset, bool div_ran,
+                                                                 float* __restrict__ x, float* __restrict__ t) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= batch) return;
+    const double r2 = ds->dtd[kDtRatio2UsedP], hr = ds->dtd[kDtRatioUsedV];  // dt ratios the warm starts used
     const uint32_t i = (uint32_t)(((uint64_t)k * n / batch + offset) % n);
     const float4* f = reinterpret_cast<const float4*>(ds->features + (size_t)i * 8);
     reinterpret_cast<float4*>(x + (size_t)k * 8)[0] = f[0];
@@ -769,10 +784,9 @@ template <class Real> void launch_totals(const DevState<Real>* d, uint32_t n, bo
     if (n) totals_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, div_ran);
 }
 template <class Real>
-void launch_gather_training(const DevState<Real>* d, uint32_t n, uint32_t batch, uint32_t offset, double r2, double hr,
-                            bool div_ran, float* x, float* t, cudaStream_t s) {
-    if (n && batch)
-        gather_training_kernel<Real><<<grid_for(batch), kBlock, 0, s>>>(d, n, batch, offset, r2, hr, div_ran, x, t);
+void launch_gather_training(const DevState<Real>* d, uint32_t n, uint32_t batch, uint32_t offset, bool div_ran, float* x,
+                            float* t, cudaStream_t s) {
+    if (n && batch) gather_training_kernel<Real><<<grid_for(batch), kBlock, 0, s>>>(d, n, batch, offset, div_ran, x, t);
 }
 template <class Real>
 void launch_divergence_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
@@ -848,8 +862,8 @@ template <class Real> void launch_cfl_reduce(const DevState<Real>* d, uint32_t n
     template void launch_probe_residual<R>(const DevState<R>*, uint32_t, int, const Vec4<R>*, cudaStream_t);        \
     template void launch_warm_values<R>(const DevState<R>*, uint32_t, int, bool, double, cudaStream_t);             \
     template void launch_totals<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                               \
-    template void launch_gather_training<R>(const DevState<R>*, uint32_t, uint32_t, uint32_t, double, double, bool, \
-                                            float*, float*, cudaStream_t);                                           \
+    template void launch_gather_training<R>(const DevState<R>*, uint32_t, uint32_t, uint32_t, bool, float*, float*, \
+                                            cudaStream_t);                                                           \
     template void launch_divergence_residual<R>(const DevState<R>*, uint32_t, bool, double, int, int,               \
                                                 cudaGraphConditionalHandle, bool, cudaStream_t, bool);               \
     template void launch_divergence_jacobi<R>(const DevState<R>*, uint32_t, cudaGraphConditionalHandle, bool,       \

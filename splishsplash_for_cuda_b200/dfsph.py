@@ -158,6 +158,11 @@ class DFSPHCUDA:
         return st
 
     # piecewise host functions of DFSPH_core_cuda.h
+    def step_async(self) -> None:
+        """Enqueues one time step without waiting or reading anything back (dfsph_step with null
+        stats); synchronize() waits, status() and get_param() read the results."""
+        self._call(self._lib.dfsph_step(self._ctx, None))
+
     def neighbors_search(self) -> None:
         self._call(self._lib.dfsph_neighbors_search(self._ctx, 1))
 

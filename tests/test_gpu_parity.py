@@ -327,3 +327,23 @@ def test_boundary_forces_match_oracle():
         if k >= 180:
             fy.append(d.field("boundary_force", np.float64)[:, 1].sum())
     assert abs(np.mean(fy) + weight) <= 0.05 * weight
+
+
+def test_async_steps_equal_waiting_steps():
+    """The step runs on the device, CFL dt included: enqueued steps without read-back give the same
+    state, dt history and iteration totals as steps that wait for their statistics."""
+    s = synthetic_scene(1, counts=(16, 16, 16), cfl=True)
+    a, b = DFSPHCUDA(s), DFSPHCUDA(s)
+    b.set_param("iterations_sum", 0)
+    its = itv = 0
+    for _ in range(12):
+        st = a.step()
+        its += st.iterations
+        itv += st.iterations_v
+        b.step_async()
+    b.synchronize()
+    assert b.get_param("iterations_sum") == its and b.get_param("iterations_v_sum") == itv
+    for key in ("h", "h_future", "h_past"):
+        assert a.get_param(key) == b.get_param(key)
+    assert np.array_equal(a.positions(), b.positions()) and np.array_equal(a.velocities(), b.velocities())
+    assert b.status() == 0
