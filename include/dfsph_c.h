@@ -270,6 +270,21 @@ int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launc
 int dfsph_save_snapshot(dfsph_ctx* ctx, const char* dir, int what);
 int dfsph_load_snapshot(dfsph_ctx* ctx, const char* dir, int what, int load_velocities);
 
+/* Partio particle files (Houdini BGEO version 5, gzip-compressed), the format of the reference's
+ * PartioReaderWriter (Utilities/PartioReaderWriter.cpp:8-66, 189-231).
+ * dfsph_export_bgeo replaces partioExport (Demos/StaticBoundaryDemo/main.cpp:485-496): the fluid's
+ * positions, velocities, pscale = particle radius and id = particle id, in particle-id order.
+ * dfsph_bgeo_write / dfsph_bgeo_read need no context (and no GPU): write count particles (vxyz may be
+ * null: no velocity attribute; radius 0: no pscale attribute); read positions and velocities
+ * (zeros when the file has none, untransformed) of a compressed or plain file. With xyz null,
+ * dfsph_bgeo_read only stores the particle count; otherwise capacity (particles) must hold it
+ * (DFSPH_E_INVALID if not). has_velocity (may be null) is set to 1 when the file has velocities.
+ * Errors of the context-free calls are reported by dfsph_last_error(NULL). */
+int dfsph_export_bgeo(dfsph_ctx* ctx, const char* path);
+int dfsph_bgeo_write(const char* path, const float* xyz, const float* vxyz, uint64_t count, float radius);
+int dfsph_bgeo_read(const char* path, float* xyz, float* vxyz, uint64_t capacity, uint64_t* count,
+                    int* has_velocity);
+
 /* Binary checkpoint of the complete solver state (no reference counterpart; the text snapshot above
  * drops the warm starts and the particle order): particles in their current internal order with
  * kappa and kappa_v, the boundary with psi, the dt history, the grid, the scene parameters and, when

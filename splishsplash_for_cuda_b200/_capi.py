@@ -125,6 +125,9 @@ SIGNATURES = {
     "dfsph_save_snapshot": (C.c_int, [_P, C.c_char_p, C.c_int]),
     "dfsph_load_snapshot": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int]),
     "dfsph_checkpoint_save": (C.c_int, [_P, C.c_char_p]),
+    "dfsph_export_bgeo": (C.c_int, [_P, C.c_char_p]),
+    "dfsph_bgeo_write": (C.c_int, [C.c_char_p, _P, _P, C.c_uint64, C.c_float]),
+    "dfsph_bgeo_read": (C.c_int, [C.c_char_p, _P, _P, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]),
     "dfsph_checkpoint_load": (C.c_int, [_P, C.c_char_p]),
     "dfsph_mlp_get_params": (C.c_int, [_P, _F, C.c_size_t]),
     "dfsph_mlp_set_params": (C.c_int, [_P, _F, C.c_size_t]),

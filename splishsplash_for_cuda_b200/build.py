@@ -2,8 +2,8 @@
 
 Usage: python -m splishsplash_for_cuda_b200.build [--force]
 
-Each CUDA translation unit is compiled with nvcc for sm_100a only, then linked into one shared
-library with the static CUDA runtime. The library has a plain C ABI (include/dfsph_c.h) and no
+Each CUDA translation unit is compiled with nvcc for sm_100a only (host-only C++ files with g++),
+then linked into one shared library with the static CUDA runtime and zlib (for .bgeo files). The library has a plain C ABI (include/dfsph_c.h) and no
 dependency on PyTorch.
 """
 from __future__ import annotations
@@ -42,8 +42,19 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libdfsph_b200.so")
 
 
+CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-I", str(ROOT / "include")]
+
+
+def cxx() -> str:
+    for cand in (os.environ.get("CXX"), shutil.which("g++"), "/usr/bin/g++"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("g++ not found")
+
+
 def sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu"))
+    """CUDA translation units (nvcc) and host-only C++ files (g++)."""
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:
@@ -59,15 +70,18 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
     OUT_ = Path(out) if out is not None else OUT
     OBJ_ = Path(obj_dir) if obj_dir is not None else OBJ
     OBJ_.mkdir(parents=True, exist_ok=True)
-    headers = list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((ROOT / "include").glob("*.h"))
     flags = NVCC_FLAGS + (extra_flags or [])
     jobs = []
     objs = []
     for src in sources():
-        obj = OBJ_ / (src.stem + ".o")
+        obj = OBJ_ / (src.stem + src.suffix.replace(".", "_") + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
-            jobs.append([nvcc(), *flags, "-c", str(src), "-o", str(obj)])
+            if src.suffix == ".cpp":
+                jobs.append([cxx(), *CXX_FLAGS, "-c", str(src), "-o", str(obj)])
+            else:
+                jobs.append([nvcc(), *flags, "-c", str(src), "-o", str(obj)])
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
             results = list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), jobs))
@@ -75,9 +89,9 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
             if verbose or res.returncode != 0:
                 sys.stderr.write(" ".join(cmd) + "\n" + res.stdout + res.stderr)
             if res.returncode != 0:
-                raise RuntimeError(f"nvcc failed for {cmd[-3]}")
+                raise RuntimeError(f"compile failed for {cmd[-3]}")
     if force or jobs or _stale(OUT_, objs):
-        link = [nvcc(), *ARCH, "-shared", "-o", str(OUT_), *map(str, objs), "-cudart", "static"]
+        link = [nvcc(), *ARCH, "-shared", "-o", str(OUT_), *map(str, objs), "-cudart", "static", "-lz"]
         res = subprocess.run(link, capture_output=True, text=True)
         if res.returncode != 0:
             sys.stderr.write(" ".join(link) + "\n" + res.stdout + res.stderr)

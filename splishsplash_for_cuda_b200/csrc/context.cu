@@ -18,6 +18,7 @@
 #include <string>
 #include <vector>
 
+#include "bgeo.h"
 #include "dfsph_state.cuh"
 #include "io.cuh"
 #include "mlp.cuh"
@@ -1207,6 +1208,19 @@ public:
     template <class T> static void put(std::ofstream& f, const T& v) { f.write(reinterpret_cast<const char*>(&v), sizeof(T)); }
     template <class T> static bool get(std::ifstream& f, T& v) { return (bool)f.read(reinterpret_cast<char*>(&v), sizeof(T)); }
 
+    // The fluid as a partio particle file (partioExport, Demos/StaticBoundaryDemo/main.cpp:485-496).
+    int export_bgeo(const char* path) {
+        DF_CHECK(path, DFSPH_E_INVALID, "null path");
+        std::vector<float> x((size_t)n * 3), v((size_t)n * 3);
+        if (n) {
+            DF_TRY(download(DFSPH_F_POSITION, DFSPH_DTYPE_F32, x.data(), x.size(), DFSPH_ORDER_ID));
+            DF_TRY(download(DFSPH_F_VELOCITY, DFSPH_DTYPE_F32, v.data(), v.size(), DFSPH_ORDER_ID));
+        }
+        std::string err;
+        DF_CHECK(bgeo_write(path, n, x.data(), v.data(), (float)sc.particle_radius, err), DFSPH_E_INVALID, err);
+        return DFSPH_OK;
+    }
+
     int save_checkpoint(const char* path) {
         DF_CHECK(path, DFSPH_E_INVALID, "null path");
         DF_CHECK(grid_ready, DFSPH_E_STATE, "nothing to checkpoint");
@@ -1870,6 +1884,39 @@ int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launc
 }
 int dfsph_save_snapshot(dfsph_ctx* ctx, const char* dir, int what) { DFSPH_DISPATCH(ctx, save_snapshot(dir, what)); }
 int dfsph_checkpoint_save(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, save_checkpoint(path)); }
+int dfsph_export_bgeo(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, export_bgeo(path)); }
+int dfsph_bgeo_write(const char* path, const float* xyz, const float* vxyz, uint64_t count, float radius) {
+    std::string err;
+    if (!path) err = "dfsph_bgeo_write: null path";
+    else if (dfsph::bgeo_write(path, count, xyz, vxyz, radius, err)) return DFSPH_OK;
+    dfsph::set_global_error(err);
+    return DFSPH_E_INVALID;
+}
+int dfsph_bgeo_read(const char* path, float* xyz, float* vxyz, uint64_t capacity, uint64_t* count, int* has_velocity) {
+    std::string err;
+    std::vector<float> x, v;
+    bool hv = false;
+    if (!path || !count) {
+        dfsph::set_global_error("dfsph_bgeo_read: null path or count");
+        return DFSPH_E_INVALID;
+    }
+    if (!dfsph::bgeo_read(path, x, v, hv, err)) {
+        dfsph::set_global_error(err);
+        return DFSPH_E_INVALID;
+    }
+    const uint64_t m = x.size() / 3;
+    *count = m;
+    if (has_velocity) *has_velocity = hv ? 1 : 0;
+    if (!xyz) return DFSPH_OK;
+    if (capacity < m) {
+        dfsph::set_global_error("dfsph_bgeo_read: " + std::to_string(m) + " particles exceed the capacity " +
+                                std::to_string(capacity));
+        return DFSPH_E_INVALID;
+    }
+    std::memcpy(xyz, x.data(), x.size() * sizeof(float));
+    if (vxyz) std::memcpy(vxyz, v.data(), v.size() * sizeof(float));
+    return DFSPH_OK;
+}
 int dfsph_checkpoint_load(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, load_checkpoint(path)); }
 int dfsph_load_snapshot(dfsph_ctx* ctx, const char* dir, int what, int load_velocities) {
     DFSPH_DISPATCH(ctx, load_snapshot(dir, what, load_velocities != 0));

@@ -322,6 +322,11 @@ class DFSPHCUDA:
     def checkpoint_load(self, path) -> None:
         self._call(self._lib.dfsph_checkpoint_load(self._ctx, str(path).encode()))
 
+    def export_bgeo(self, path) -> None:
+        """The fluid as a partio .bgeo file (positions, velocities, pscale, id), like the reference's
+        partioExport (Demos/StaticBoundaryDemo/main.cpp:485-496)."""
+        self._call(self._lib.dfsph_export_bgeo(self._ctx, str(path).encode()))
+
     # ---- learned warm start (no reference counterpart) ------------------------------------------
     def set_learned_warm_start(self, on: bool = True, probe: bool = True, train_interval: int | None = None,
                                train_iters: int | None = None, train_batch: int | None = None,

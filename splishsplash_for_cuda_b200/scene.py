@@ -4,7 +4,9 @@ The JSON reader follows the keys of the reference SceneLoader (Utilities/SceneLo
 "Configuration" (timeStepSize, particleRadius, density0, viscosity, gravitation, cflMethod,
 cflFactor, cflMaxTimeStepSize, maxIterations, maxError, maxIterationsV, maxErrorV,
 enableDivergenceSolver), "FluidBlocks" (start/end boxes filled like DemoBase::createFluidBlocks,
-Demos/Common/DemoBase.cpp:539-603) and "RigidBodies". Wall bodies are sampled as a single-layer
+Demos/Common/DemoBase.cpp:539-603), "FluidModels" (partio .bgeo particle files with translation,
+rotationAxis/rotationAngle and scale) and "RigidBodies" (box walls, or samples from a .bgeo
+"particleFile"). Wall bodies without a particle file are sampled as a single-layer
 lattice of spacing 2r on the box surface instead of the Poisson-disk sampling of an OBJ mesh
 (Demos/StaticBoundaryDemo/main.cpp:466-468); a body whose "geometryFile" names a unit box is the
 box [translation - scale/2, translation + scale/2]. Extension keys (ignored by the reference):
@@ -167,6 +169,11 @@ def _readvec(v, default):
     return tuple(float(x) for x in v) if v is not None else default
 
 
+def _scene_relative(scene_path: Path, file: str) -> Path:
+    f = Path(file)
+    return f if f.is_absolute() else scene_path.parent / f
+
+
 def load_scene(path: str | Path) -> Scene:
     """Reads a reference-format JSON scene."""
     path = Path(path)
@@ -212,11 +219,37 @@ def load_scene(path: str | Path) -> Scene:
         fluid.append(fluid_block(mn, mx, r))
     fluid_arr = np.concatenate(fluid, axis=0) if fluid else np.zeros((0, 3))
     fluid_arr = fluid_arr + _jitter(fluid_arr.shape[0], jitter * r, seed)
+    # FluidModels: particle files appended after the blocks (DemoBase::initFluidData,
+    # Demos/Common/DemoBase.cpp:514-534), x = R (s x) + t; velocities as stored.
+    fluid_vel = [np.zeros_like(fluid_arr)]
+    models = [fluid_arr]
+    any_vel = False
+    for fm in j.get("FluidModels", []):
+        if "particleFile" not in fm:
+            continue
+        x, v = read_bgeo(_scene_relative(path, fm["particleFile"]))
+        t, rot = _body_transform(fm)
+        sc = float(fm.get("scale", 1.0))
+        models.append((x.astype(np.float64) * sc) @ rot.T + t)
+        fluid_vel.append(np.zeros_like(x, dtype=np.float64) if v is None else v.astype(np.float64))
+        any_vel = any_vel or v is not None
+    fluid_arr = np.concatenate(models, axis=0)
     walls = []
     bmin = bmax = None
     for rb in j.get("RigidBodies", []):
         scale = np.asarray(_readvec(rb.get("scale"), (1.0, 1.0, 1.0)))
         trans = np.asarray(_readvec(rb.get("translation"), (0.0, 0.0, 0.0)))
+        if rb.get("particleFile"):
+            # boundary samples from a file (Demos/StaticBoundaryDemo/main.cpp:416-420): x = R (s0 x) + t
+            x, _ = read_bgeo(_scene_relative(path, rb["particleFile"]))
+            t, rot = _body_transform(rb)
+            pts = (x.astype(np.float64) * scale[0]) @ rot.T + t
+            walls.append(pts)
+            if pts.shape[0]:
+                mn, mx = pts.min(axis=0), pts.max(axis=0)
+                bmin = mn if bmin is None else np.minimum(bmin, mn)
+                bmax = mx if bmax is None else np.maximum(bmax, mx)
+            continue
         geo = str(rb.get("geometryFile", ""))
         if "box" not in geo.lower():
             raise ValueError(f"only box rigid bodies are supported, got {geo!r}")
@@ -230,6 +263,7 @@ def load_scene(path: str | Path) -> Scene:
         config=cfg,
         fluid=fluid_arr.astype(np.float32),
         boundary=wall_arr.astype(np.float32),
+        fluid_velocity=np.concatenate(fluid_vel, axis=0).astype(np.float32) if any_vel else None,
         name=path.stem,
         box_min=tuple(bmin) if bmin is not None else None,
         box_max=tuple(bmax) if bmax is not None else None,
@@ -305,6 +339,62 @@ def column_scene(counts=(10, 80, 10), radius: float = 0.008, time_step: float = 
     return Scene(config=cfg, fluid=fluid.astype(np.float32), boundary=walls.astype(np.float32),
                  name=f"column_{'x'.join(map(str, cnt))}", box_min=(0.0, 0.0, 0.0), box_max=tuple(box),
                  meta=dict(seed=seed))
+
+
+def read_bgeo(path):
+    """Reads a partio .bgeo particle file (Houdini BGEO v5, compressed or plain) through the library's
+    reader: (positions (N, 3) float32, velocities (N, 3) float32 or None when the file has none),
+    untransformed (PartioReaderWriter::readParticles, Utilities/PartioReaderWriter.cpp:8-66)."""
+    import ctypes as C
+
+    from . import _capi
+
+    lib = _capi.load()
+    n, hv = C.c_uint64(0), C.c_int(0)
+    bp = str(path).encode()
+    _capi.check(lib, None, lib.dfsph_bgeo_read(bp, None, None, 0, C.byref(n), C.byref(hv)))
+    x = np.zeros((n.value, 3), np.float32)
+    v = np.zeros((n.value, 3), np.float32)
+    _capi.check(lib, None, lib.dfsph_bgeo_read(bp, x.ctypes.data_as(C.c_void_p), v.ctypes.data_as(C.c_void_p),
+                                               n.value, C.byref(n), C.byref(hv)))
+    return x, (v if hv.value else None)
+
+
+def write_bgeo(path, position, velocity=None, radius: float = 0.0) -> None:
+    """Writes a gzip-compressed partio .bgeo file with the attributes of the reference's
+    PartioReaderWriter::writeParticles (Utilities/PartioReaderWriter.cpp:189-231): position,
+    velocity (when given), pscale (when radius != 0) and id."""
+    import ctypes as C
+
+    from . import _capi
+
+    lib = _capi.load()
+    x = np.ascontiguousarray(np.asarray(position, np.float32).reshape(-1, 3))
+    v = None if velocity is None else np.ascontiguousarray(np.asarray(velocity, np.float32).reshape(-1, 3))
+    if v is not None and v.shape != x.shape:
+        raise ValueError("velocity must have the shape of position")
+    _capi.check(lib, None, lib.dfsph_bgeo_write(str(path).encode(), x.ctypes.data_as(C.c_void_p),
+                                                None if v is None else v.ctypes.data_as(C.c_void_p),
+                                                x.shape[0], float(radius)))
+
+
+def angle_axis_matrix(axis, angle: float) -> np.ndarray:
+    """Rotation of `angle` radians about `axis` by the Rodrigues formula
+    R = cos(a) I + (1 - cos(a)) u u^T + sin(a) [u]x, with u taken as given (the scene's
+    rotationAxis, as Eigen's AngleAxis uses it in SceneLoader.cpp:228-233)."""
+    u = np.asarray(axis, np.float64).reshape(3)
+    c, s = np.cos(angle), np.sin(angle)
+    cross = np.array([[0.0, -u[2], u[1]], [u[2], 0.0, -u[0]], [-u[1], u[0], 0.0]])
+    return c * np.eye(3) + (1.0 - c) * np.outer(u, u) + s * cross
+
+
+def _body_transform(obj: dict):
+    t = np.asarray(_readvec(obj.get("translation"), (0.0, 0.0, 0.0)))
+    if obj.get("rotationAxis") is not None and obj.get("rotationAngle") is not None:
+        r = angle_axis_matrix(obj["rotationAxis"], float(obj["rotationAngle"]))
+    else:
+        r = np.eye(3)
+    return t, r
 
 
 def read_particle_file(path):
