@@ -49,6 +49,7 @@ typedef struct dfsph_ctx dfsph_ctx;
 #define DFSPH_ST_DIVERGENCE_NOT_CONVERGED 0x10u /* divergence solve stopped at max_iterations_v     */
 #define DFSPH_ST_SORT_TIMEOUT 0x20u      /* a bounded wait in the radix sort gave up (no hang)      */
 #define DFSPH_ST_BOUNDARY_OVERFLOW 0x40u /* a boundary particle had too many boundary neighbours    */
+#define DFSPH_ST_FLUID_CAPACITY 0x80u    /* an open-boundary inflow was cut at fluid_capacity        */
 
 /* ---- scene / solver parameters ---------------------------------------------------------------- */
 /* Mirrors the "Configuration" keys of the reference JSON scene (Utilities/SceneLoader.cpp:39-160)
@@ -284,6 +285,61 @@ int dfsph_export_bgeo(dfsph_ctx* ctx, const char* path);
 int dfsph_bgeo_write(const char* path, const float* xyz, const float* vxyz, uint64_t count, float radius);
 int dfsph_bgeo_read(const char* path, float* xyz, float* vxyz, uint64_t capacity, uint64_t* count,
                     int* has_velocity);
+
+/* ---- simple open boundary (OpenBoundariesSimpleInterface, OpenBoundariesSimple.{h,cu}) ----------
+ * Surfaces are the reference's BufferFluidSurface shapes (BufferFluidSurface.cu:421-900) with its
+ * type numbers; the triangle-mesh shape (3) is not offered. "Inside" follows isinside(): plane
+ * (x - origin) . normal >= 0; cuboid |x - center| < half_lengths component-wise; cylinder (axis y)
+ * |dy| <= half_lengths[1] and horizontal distance < radius; sphere distance < radius; star (axis y,
+ * `points` linear-sided points, the first along `direction`) |dy| <= half_lengths[1] and inside the
+ * star outline between radius_internal and radius. reversed != 0 swaps inside and outside. The
+ * normal used by the inflow is center - x (cylinder, sphere, star; negated when reversed,
+ * normalised) and zero for planes and cuboids. All surface arithmetic is FP32. */
+#define DFSPH_SURFACE_PLANE 0
+#define DFSPH_SURFACE_CUBOID 1
+#define DFSPH_SURFACE_CYLINDER 2
+#define DFSPH_SURFACE_SPHERE 4
+#define DFSPH_SURFACE_STAR 5
+typedef struct dfsph_surface {
+    int32_t type;            /* DFSPH_SURFACE_*                                                   */
+    int32_t reversed;        /* != 0: inside and outside swapped                                  */
+    float origin[3];         /* plane: a point of the plane                                       */
+    float normal[3];         /* plane: the side of the normal is inside                           */
+    float center[3];         /* cuboid, cylinder, sphere, star                                    */
+    float half_lengths[3];   /* cuboid; cylinder and star use [1] (half height along y)           */
+    float radius;            /* cylinder, sphere; star: outer radius                              */
+    float radius_internal;   /* star: inner radius                                                */
+    uint32_t points;         /* star: number of points (>= 1)                                     */
+    float direction[3];      /* star: direction of the first point (horizontal)                   */
+} dfsph_surface;
+
+/* OpenBoundariesSimpleInterface::init (OpenBoundariesSimple.cu:105-350): boundary is the simulation
+ * boundary, interior a slightly smaller copy (the reference uses 3 r less), fluid_surface the
+ * fluid's free surface (inside = below it). Of the n_samples inflow sample positions (a fluid at
+ * rest sampled in the same boundary, xyz[3 n]) the context keeps those outside `interior`, inside
+ * `fluid_surface` and inside the cell grid; n_kept (may be null) receives their count. Calling it
+ * again replaces the previous set. */
+int dfsph_open_boundary_init(dfsph_ctx* ctx, const dfsph_surface* boundary, const dfsph_surface* interior,
+                             const dfsph_surface* fluid_surface, const float* sample_xyz, uint32_t n_samples,
+                             uint32_t* n_kept);
+/* OpenBoundariesSimpleInterface::applyOpenBoundary (OpenBoundariesSimple.cu:495-620), called between
+ * steps. Inflow (use_inflow): every sample with no fluid particle of the 27 cells around it closer
+ * than allowed_distance becomes a fluid particle, with the kernel-and-mass-weighted velocity of its
+ * fluid neighbours (boundary neighbours add weight but no velocity), unless its density estimate
+ * exceeds allowed_density or that velocity points out of the boundary (v . normal < 0); new
+ * particles get the default fluid mass, kappa = kappa_v = 0 and the next ids, in sample order.
+ * allowed_distance and allowed_density must be > 0 when use_inflow != 0 (the reference exits
+ * otherwise). Outflow (use_outflow): particles outside `interior` and outside `fluid_surface` are
+ * removed; the remaining ids are renumbered densely in their previous order. Inflow beyond
+ * fluid_capacity is cut and raises DFSPH_ST_FLUID_CAPACITY. added / removed (may be null) receive
+ * the counts. Synchronises the context's stream. */
+int dfsph_open_boundary_apply(dfsph_ctx* ctx, double allowed_distance, double allowed_density, int use_inflow,
+                              int use_outflow, uint32_t* added, uint32_t* removed);
+/* The kept inflow samples (xyz[3 capacity]; xyz null: only the count), in sample order. */
+int dfsph_open_boundary_samples(dfsph_ctx* ctx, float* xyz, uint32_t capacity, uint32_t* count);
+/* Moves the three surfaces and the samples by delta[3] (the reference applies the dynamic window's
+ * displacement this way, OpenBoundariesSimple.cu:527-553). */
+int dfsph_open_boundary_shift(dfsph_ctx* ctx, const float* delta);
 
 /* Binary checkpoint of the complete solver state (no reference counterpart; the text snapshot above
  * drops the warm starts and the particle order): particles in their current internal order with

@@ -19,6 +19,9 @@
 //   pressure solve                     DFSPH_core_cuda.cu:867-951, 965-980, 1165-1243, 1264-1284, 1338-1419
 //   position update                    DFSPH_core_cuda.cu:3127-3215 (damping and wave cancelling off)
 //   CFL                                DFSPH_core_cuda.cu:3321-3394
+//   simple open boundary               OpenBoundariesSimple.cu:105-350 (init), 352-470 (inflow),
+//                                      475-492 (outflow), 495-620 (apply); surfaces
+//                                      BufferFluidSurface.cu:421-900 (isinside, getNormal)
 //
 // The pair predicate is the canonical FP32 form shared with the device code:
 // d2 = fma(dz, dz, fma(dy, dy, dx*dx)) on float coordinates, then d2 < H*H (H*H rounded to float).
@@ -104,6 +107,91 @@ template <class Real> struct Cubic {
     }
 };
 
+// Layout of the C ABI's dfsph_surface (restated; BufferFluidSurface's fields).
+struct Surface {
+    int32_t type, reversed;
+    float origin[3], normal[3], center[3], half_lengths[3];
+    float radius, radius_internal;
+    uint32_t points;
+    float direction[3];
+};
+
+// BufferFluidSurface::isinside / getNormal in FP32, each expression evaluated left to right.
+float sdot(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+float snorm(const float* a) { return std::sqrt(sdot(a, a)); }
+
+bool surface_inside(const Surface& S, const float* p) {
+    bool r = false;
+    float v[3];
+    switch (S.type) {
+        case 0:
+            for (int a = 0; a < 3; ++a) v[a] = p[a] - S.origin[a];
+            r = !(sdot(v, S.normal) < 0.0f);
+            break;
+        case 1:
+            for (int a = 0; a < 3; ++a) v[a] = std::fabs(p[a] - S.center[a]);
+            r = v[0] < S.half_lengths[0] && v[1] < S.half_lengths[1] && v[2] < S.half_lengths[2];
+            break;
+        case 2:
+        case 5: {
+            for (int a = 0; a < 3; ++a) v[a] = p[a] - S.center[a];
+            if (std::fabs(v[1]) > S.half_lengths[1]) break;
+            v[1] = 0.0f;
+            const float nv = snorm(v);
+            if (S.type == 2) {
+                r = nv < S.radius;
+                break;
+            }
+            if (nv < S.radius_internal) {
+                r = true;
+            } else if (nv > S.radius) {
+                r = false;
+            } else {
+                const float u[3] = {v[0] / nv, v[1] / nv, v[2] / nv};
+                const float alpha = std::acos(sdot(u, S.direction));
+                const float alpha0 = (2.0f * 3.14159265358979f) / (float)S.points;
+                float k = alpha / alpha0;
+                for (uint32_t it = 0; k > 1.0f && it <= S.points; ++it) k -= 1.0f;
+                const float x = k * alpha0;
+                const float half = alpha0 / 2.0f;
+                float a1 = 0.0f, r1 = S.radius, a2 = 0.0f + half, r2 = S.radius_internal;
+                if (x > half) {
+                    r1 = S.radius_internal;
+                    r2 = S.radius;
+                    a1 = a2;
+                    a2 = a1 + half;
+                }
+                const float x1 = r1 * std::cos(a1), y1 = r1 * std::sin(a1);
+                const float x2 = r2 * std::cos(a2), y2 = r2 * std::sin(a2);
+                const float m = (y2 - y1) / (x2 - x1);
+                const float c = -x1 * m + y1;
+                const float d = c / (-m * std::cos(x) + 1.0f * std::sin(x));
+                r = nv <= d;
+            }
+            break;
+        }
+        case 4:
+            for (int a = 0; a < 3; ++a) v[a] = p[a] - S.center[a];
+            r = snorm(v) < S.radius;
+            break;
+        default:
+            break;
+    }
+    return S.reversed ? !r : r;
+}
+
+void surface_normal(const Surface& S, const float* p, float* out) {
+    out[0] = out[1] = out[2] = 0.0f;
+    if (S.type == 2 || S.type == 4 || S.type == 5)
+        for (int a = 0; a < 3; ++a) out[a] = S.center[a] - p[a];
+    if (S.reversed)
+        for (int a = 0; a < 3; ++a) out[a] = -out[a];
+    if (!(out[0] == 0.0f && out[1] == 0.0f && out[2] == 0.0f)) {
+        const float nr = snorm(out);
+        for (int a = 0; a < 3; ++a) out[a] = out[a] / nr;
+    }
+}
+
 struct Params {
     double particle_radius, density0, viscosity, gravitation[3], time_step;
     int32_t max_iterations;
@@ -150,6 +238,135 @@ template <class Real> struct Oracle {
         time_step = p.time_step;
         reset_dt();
     }
+    // ---- simple open boundary ------------------------------------------------------------------
+    bool ob_ready = false;
+    Surface ob_b{}, ob_i{}, ob_s{};
+    std::vector<float> ob_x;  // kept samples
+
+    void ob_init(const Surface& b, const Surface& in, const Surface& sf, const float* xyz, uint32_t ns) {
+        ob_b = b;
+        ob_i = in;
+        ob_s = sf;
+        ob_x.clear();
+        for (uint32_t i = 0; i < ns; ++i) {
+            const float* p = xyz + 3 * (size_t)i;
+            int cx, cy, cz;
+            if (!surface_inside(in, p) && surface_inside(sf, p) && cell_of(p[0], p[1], p[2], cx, cy, cz))
+                ob_x.insert(ob_x.end(), p, p + 3);
+        }
+        ob_ready = true;
+    }
+
+    void ob_shift(const float* d) {
+        for (Surface* S : {&ob_b, &ob_i, &ob_s}) {
+            float* c = (S->type == 0) ? S->origin : S->center;
+            for (int a = 0; a < 3; ++a) c[a] += d[a];
+        }
+        for (size_t k = 0; k < ob_x.size(); ++k) ob_x[k] += d[k % 3];
+    }
+
+    // applyOpenBoundary: inflow decisions against the current fluid (all of them, in sample order),
+    // then the outflow over every particle, new ones included.
+    void ob_apply(double allowed_distance, double allowed_density, bool inflow, bool outflow, uint32_t capacity,
+                  uint32_t& added, uint32_t& removed, bool& clipped) {
+        added = removed = 0;
+        clipped = false;
+        const double d2r = 2.0 * prm.particle_radius;
+        const Real mass = (Real)(float)(0.8 * d2r * d2r * d2r * prm.density0);
+        if (inflow && !ob_x.empty()) {
+            const std::vector<float> fp = fpos(), fb = fbpos();
+            const Buckets bf = bucket(fp, n), bbk = bucket(fb, nb);
+            const uint32_t ns = (uint32_t)(ob_x.size() / 3);
+            std::vector<float> newx, newv;
+            for (uint32_t i = 0; i < ns; ++i) {
+                const float* sp = &ob_x[3 * (size_t)i];
+                const Real xi = sp[0], yi = sp[1], zi = sp[2];
+                Real min_d = Real(100);
+                bool any_cell = false;
+                for_cells(sp[0], sp[1], sp[2], [&](size_t c) {
+                    any_cell = true;
+                    for (uint32_t t = bf.start[c]; t < bf.start[c + 1]; ++t) {
+                        const uint32_t j = bf.items[t];
+                        const Real ex = xi - x[3 * j], ey = yi - x[3 * j + 1], ez = zi - x[3 * j + 2];
+                        const Real dd = std::sqrt(ex * ex + ey * ey + ez * ez);
+                        min_d = dd < min_d ? dd : min_d;
+                    }
+                });
+                if (!any_cell || !(min_d > (Real)(float)allowed_distance)) continue;
+                Real rho0 = K.W0 * mass, wsum = 0, vx = 0, vy = 0, vz = 0;
+                for_cells(sp[0], sp[1], sp[2], [&](size_t c) {
+                    for (uint32_t t = bf.start[c]; t < bf.start[c + 1]; ++t) {
+                        const uint32_t j = bf.items[t];
+                        const Real w = K.W(xi - x[3 * j], yi - x[3 * j + 1], zi - x[3 * j + 2]) * m[j];
+                        rho0 += w;
+                        vx += v[3 * j] * w;
+                        vy += v[3 * j + 1] * w;
+                        vz += v[3 * j + 2] * w;
+                        wsum += w;
+                    }
+                });
+                for_cells(sp[0], sp[1], sp[2], [&](size_t c) {
+                    for (uint32_t t = bbk.start[c]; t < bbk.start[c + 1]; ++t) {
+                        const uint32_t j = bbk.items[t];
+                        const Real w = K.W(xi - bx[3 * j], yi - bx[3 * j + 1], zi - bx[3 * j + 2]) * psi[j];
+                        wsum += w;
+                        rho0 += w;
+                    }
+                });
+                if (wsum > Real(0)) {
+                    vx /= wsum;
+                    vy /= wsum;
+                    vz /= wsum;
+                }
+                float nrm[3];
+                surface_normal(ob_b, sp, nrm);
+                const float vf[3] = {(float)vx, (float)vy, (float)vz};
+                if (rho0 > (Real)(float)allowed_density || sdot(vf, nrm) < 0.0f) continue;
+                newx.insert(newx.end(), sp, sp + 3);
+                newv.insert(newv.end(), vf, vf + 3);
+            }
+            uint32_t want = (uint32_t)(newx.size() / 3);
+            added = std::min<uint32_t>(want, capacity > n ? capacity - n : 0);
+            clipped = added < want;
+            for (uint32_t k = 0; k < added; ++k) {
+                for (int a3 = 0; a3 < 3; ++a3) {
+                    x.push_back((Real)newx[3 * k + a3]);
+                    v.push_back((Real)newv[3 * k + a3]);
+                    a.push_back(0);
+                }
+                m.push_back(mass);
+                for (auto* vec : {&rho, &alpha, &dadv, &kap, &kapv, &kc}) vec->push_back(0);
+            }
+            n += added;
+            nf.resize(n);
+            nbd.resize(n);
+        }
+        if (outflow && n) {
+            uint32_t w = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                const float p[3] = {(float)x[3 * i], (float)x[3 * i + 1], (float)x[3 * i + 2]};
+                if (!surface_inside(ob_i, p) && !surface_inside(ob_s, p)) continue;
+                if (w != i) {
+                    for (int a3 = 0; a3 < 3; ++a3) {
+                        x[3 * w + a3] = x[3 * i + a3];
+                        v[3 * w + a3] = v[3 * i + a3];
+                        a[3 * w + a3] = a[3 * i + a3];
+                    }
+                    for (auto* vec : {&m, &rho, &alpha, &dadv, &kap, &kapv, &kc}) (*vec)[w] = (*vec)[i];
+                }
+                ++w;
+            }
+            removed = n - w;
+            n = w;
+            x.resize(3 * (size_t)n);
+            v.resize(3 * (size_t)n);
+            a.resize(3 * (size_t)n);
+            for (auto* vec : {&m, &rho, &alpha, &dadv, &kap, &kapv, &kc}) vec->resize(n);
+            nf.resize(n);
+            nbd.resize(n);
+        }
+    }
+
     void reset_dt() {
         h = h_future = h_past = time_step;
         inv_h = inv_h_future = 1.0 / time_step;
@@ -689,6 +906,38 @@ int oracle_step(void* h, int32_t* iters, int32_t* iters_v, double* err, double* 
         if (err_v) *err_v = o.last_err_v;
         return (int)o.overflow;
     })());
+}
+
+int oracle_open_boundary_init(void* h, const Surface* b, const Surface* in, const Surface* sf, const float* xyz,
+                              uint32_t ns, uint32_t* kept) {
+    return ORACLE_DO(h, ([&] {
+        o.ob_init(*b, *in, *sf, xyz, ns);
+        if (kept) *kept = (uint32_t)(o.ob_x.size() / 3);
+        return 0;
+    })());
+}
+
+int oracle_open_boundary_apply(void* h, double dist, double rho, int inflow, int outflow, uint32_t capacity,
+                               uint32_t* added, uint32_t* removed) {
+    return ORACLE_DO(h, ([&] {
+        uint32_t ad = 0, rm = 0;
+        bool clipped = false;
+        o.ob_apply(dist, rho, inflow != 0, outflow != 0, capacity, ad, rm, clipped);
+        if (added) *added = ad;
+        if (removed) *removed = rm;
+        return clipped ? 1 : 0;
+    })());
+}
+
+int oracle_open_boundary_shift(void* h, const float* d) { return ORACLE_DO(h, (o.ob_shift(d), 0)); }
+
+// inside[i] and normal[3 i..] of the restated BufferFluidSurface::isinside / getNormal.
+int oracle_surface_eval(const Surface* s, const float* p, uint32_t n, uint8_t* inside, float* normal) {
+    for (uint32_t i = 0; i < n; ++i) {
+        inside[i] = surface_inside(*s, p + 3 * (size_t)i) ? 1 : 0;
+        surface_normal(*s, p + 3 * (size_t)i, normal + 3 * (size_t)i);
+    }
+    return 0;
 }
 
 // Piecewise phases, mirroring the C ABI of the device library.

@@ -36,6 +36,26 @@ class OracleParams(C.Structure):
     ]
 
 
+class OracleSurface(C.Structure):
+    """Same layout as the C ABI's dfsph_surface (restated)."""
+    _fields_ = [
+        ("type", C.c_int32),
+        ("reversed", C.c_int32),
+        ("origin", C.c_float * 3),
+        ("normal", C.c_float * 3),
+        ("center", C.c_float * 3),
+        ("half_lengths", C.c_float * 3),
+        ("radius", C.c_float),
+        ("radius_internal", C.c_float),
+        ("points", C.c_uint32),
+        ("direction", C.c_float * 3),
+    ]
+
+
+def _surface(s) -> OracleSurface:
+    return OracleSurface.from_buffer_copy(bytes(s))
+
+
 def lib_path() -> Path:
     return LIB
 
@@ -79,6 +99,12 @@ def _load():
             "oracle_set_scalar": (C.c_int, [vp, C.c_char_p, C.c_double]),
             "oracle_get_neighbors": (C.c_int, [vp, up, up, C.c_uint32]),
             "oracle_kernel_values": (C.c_int, [C.c_double, dp, C.c_uint32, C.c_int, dp, dp]),
+            "oracle_open_boundary_init": (C.c_int, [vp, C.POINTER(OracleSurface), C.POINTER(OracleSurface),
+                                                    C.POINTER(OracleSurface), fp, C.c_uint32, up]),
+            "oracle_open_boundary_apply": (C.c_int, [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_uint32, up,
+                                                     up]),
+            "oracle_open_boundary_shift": (C.c_int, [vp, fp]),
+            "oracle_surface_eval": (C.c_int, [C.POINTER(OracleSurface), fp, C.c_uint32, C.c_void_p, fp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -222,6 +248,39 @@ class Oracle:
 
     def on_step_end(self):
         self.lib.oracle_on_step_end(self.h)
+
+    # simple open boundary (surfaces: any ctypes structure with the dfsph_surface layout)
+    def open_boundary_init(self, boundary, interior, fluid_surface, samples) -> int:
+        x = np.ascontiguousarray(samples, dtype=np.float32).reshape(-1, 3)
+        self._ob = (_surface(boundary), _surface(interior), _surface(fluid_surface))
+        kept = C.c_uint32(0)
+        self.lib.oracle_open_boundary_init(self.h, *[C.byref(q) for q in self._ob], _f(x), x.shape[0],
+                                           C.byref(kept))
+        return kept.value
+
+    def open_boundary_apply(self, allowed_distance: float, allowed_density: float, use_inflow=True,
+                            use_outflow=True, capacity: int = 2 ** 32 - 1):
+        """Returns (added, removed, clipped)."""
+        a, r = C.c_uint32(0), C.c_uint32(0)
+        clipped = self.lib.oracle_open_boundary_apply(self.h, allowed_distance, allowed_density, int(use_inflow),
+                                                      int(use_outflow), capacity, C.byref(a), C.byref(r))
+        self.n = self.n + a.value - r.value
+        return a.value, r.value, bool(clipped)
+
+    def open_boundary_shift(self, delta) -> None:
+        self.lib.oracle_open_boundary_shift(self.h, _f(np.asarray(delta, np.float32).reshape(3)))
+
+
+def surface_eval(surface, points):
+    """(inside (n,) bool, normal (n, 3) float32) of the oracle's BufferFluidSurface restatement."""
+    lib = _load()
+    p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+    inside = np.zeros(p.shape[0], np.uint8)
+    normal = np.zeros((p.shape[0], 3), np.float32)
+    s = _surface(surface)
+    lib.oracle_surface_eval(C.byref(s), _f(p), p.shape[0], inside.ctypes.data_as(C.c_void_p),
+                            normal.ctypes.data_as(C.POINTER(C.c_float)))
+    return inside.astype(bool), normal
 
 
 def kernel_values(H: float, r: np.ndarray, precision: int = 32):

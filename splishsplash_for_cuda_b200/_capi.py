@@ -24,6 +24,25 @@ ST_PRESSURE_NOT_CONVERGED = 0x8
 ST_DIVERGENCE_NOT_CONVERGED = 0x10
 ST_SORT_TIMEOUT = 0x20
 ST_BOUNDARY_OVERFLOW = 0x40
+ST_FLUID_CAPACITY = 0x80
+
+SURFACE_PLANE, SURFACE_CUBOID, SURFACE_CYLINDER, SURFACE_SPHERE, SURFACE_STAR = 0, 1, 2, 4, 5
+
+
+class Surface(C.Structure):
+    """dfsph_surface (include/dfsph_c.h)."""
+    _fields_ = [
+        ("type", C.c_int32),
+        ("reversed", C.c_int32),
+        ("origin", C.c_float * 3),
+        ("normal", C.c_float * 3),
+        ("center", C.c_float * 3),
+        ("half_lengths", C.c_float * 3),
+        ("radius", C.c_float),
+        ("radius_internal", C.c_float),
+        ("points", C.c_uint32),
+        ("direction", C.c_float * 3),
+    ]
 
 FIELDS = {
     "position": (0, 3),
@@ -126,6 +145,12 @@ SIGNATURES = {
     "dfsph_load_snapshot": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int]),
     "dfsph_checkpoint_save": (C.c_int, [_P, C.c_char_p]),
     "dfsph_export_bgeo": (C.c_int, [_P, C.c_char_p]),
+    "dfsph_open_boundary_init": (C.c_int, [_P, C.POINTER(Surface), C.POINTER(Surface), C.POINTER(Surface), _P,
+                                           C.c_uint32, C.POINTER(C.c_uint32)]),
+    "dfsph_open_boundary_apply": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_uint32),
+                                            C.POINTER(C.c_uint32)]),
+    "dfsph_open_boundary_shift": (C.c_int, [_P, _P]),
+    "dfsph_open_boundary_samples": (C.c_int, [_P, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "dfsph_bgeo_write": (C.c_int, [C.c_char_p, _P, _P, C.c_uint64, C.c_float]),
     "dfsph_bgeo_read": (C.c_int, [C.c_char_p, _P, _P, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]),
     "dfsph_checkpoint_load": (C.c_int, [_P, C.c_char_p]),

@@ -22,6 +22,7 @@
 #include "dfsph_state.cuh"
 #include "io.cuh"
 #include "mlp.cuh"
+#include "open_boundary.cuh"
 #include "sort.cuh"
 
 struct dfsph_ctx;
@@ -145,6 +146,18 @@ public:
     uint32_t forced_warm = 0;             // learned candidates used without a probe this step
     bool step_trained = false;
 
+    // simple open boundary (OpenBoundariesSimple): surfaces, kept inflow samples and their scratch
+    bool ob_ready = false;
+    dfsph_surface ob_boundary{}, ob_interior{}, ob_surface{};
+    float4* ob_samples = nullptr;  // kept samples (x, y, z, 0)
+    float4* ob_vel = nullptr;      // per-sample candidate velocity (also the upload staging of init)
+    uint32_t* ob_flag = nullptr;
+    uint32_t* ob_rank = nullptr;
+    uint32_t* ob_scan = nullptr;   // scan scratch for max(sample capacity, fluid capacity) inputs
+    uint32_t* ob_total = nullptr;  // device scan totals
+    uint32_t* h_ob = nullptr;      // pinned copy of a scan total
+    uint32_t ob_ns = 0, ob_cap = 0;
+
     // ------------------------------------------------------------------------------------------
     template <class T> int dalloc(T** p, size_t count) {
         *p = nullptr;
@@ -232,6 +245,8 @@ public:
         f(tt);
         f(mlp.params); f(mlp.adam_m); f(mlp.adam_v); f(mlp.grad); f(mlp.partials);
         f(mlp.w1_bf16); f(mlp.w2_bf16); f(mlp.w3_bf16); f(mlp.scales); f(mlp.loss);
+        f(ob_samples); f(ob_vel); f(ob_flag); f(ob_rank); f(ob_scan); f(ob_total);
+        if (h_ob) cudaFreeHost(h_ob);
         if (h_ctl) cudaFreeHost(h_ctl);
         if (h_status) cudaFreeHost(h_status);
         if (h_dt) cudaFreeHost(h_dt);
@@ -539,6 +554,19 @@ public:
         // bodies at the start of a step, DFSPH_core_cuda.cu:3413)
         if (boundary_forces && nb) DF_CUDA(cudaMemsetAsync(bforce, 0, (size_t)nb * 4 * sizeof(Real), stream));
         if (!n) return DFSPH_OK;
+        DF_TRY(bin_fluid());
+        launch_build_neighbors<Real>(ds, n, ftab, btab, stream);
+        launches += 1;
+        DF_CUDA(cudaGetLastError());
+        return DFSPH_OK;
+    }
+
+    // Cell keys -> stable radix sort -> reorder (double buffer) -> cell table of the fluid.
+    int bin_fluid() {
+        if (!n) {
+            DF_CUDA(cudaMemsetAsync(ftab, 0, cells * sizeof(uint2), stream));
+            return sync_state();
+        }
         const StepParams<Real> p = params();
         launch_cell_keys<Real>(pos[cur], n, p, sb.keys_a, status, stream);
         uint32_t *skeys, *perm;
@@ -554,9 +582,171 @@ public:
         DF_CUDA(cudaMemsetAsync(ftab, 0, cells * sizeof(uint2), stream));
         launch_cell_bounds(skeys, n, dim[0], dim[1], dim[2], ftab, stream);
         DF_TRY(sync_state());
-        launch_build_neighbors<Real>(ds, n, ftab, btab, stream);
-        launches += 4;
+        launches += 3;
+        return DFSPH_OK;
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Simple open boundary (OpenBoundariesSimple.cu).
+    static bool surface_valid(const dfsph_surface& S) {
+        switch (S.type) {
+            case DFSPH_SURFACE_PLANE:
+            case DFSPH_SURFACE_CUBOID:
+            case DFSPH_SURFACE_CYLINDER:
+            case DFSPH_SURFACE_SPHERE:
+                return true;
+            case DFSPH_SURFACE_STAR:
+                return S.points >= 1;
+            default:
+                return false;
+        }
+    }
+
+    int open_boundary_init(const dfsph_surface* bnd, const dfsph_surface* interior, const dfsph_surface* surf,
+                           const float* xyz, uint32_t ns, uint32_t* n_kept) {
+        DF_CHECK(bnd && interior && surf, DFSPH_E_INVALID, "null surface");
+        DF_CHECK(surface_valid(*bnd) && surface_valid(*interior) && surface_valid(*surf), DFSPH_E_INVALID,
+                 "unsupported surface (types: plane 0, cuboid 1, cylinder 2, sphere 4, star 5 with points >= 1)");
+        DF_CHECK(xyz || ns == 0, DFSPH_E_INVALID, "null sample positions");
+        DF_CHECK(grid_ready, DFSPH_E_STATE, "no grid: set a boundary or upload fluid first");
+        if (ns > ob_cap || !ob_total) {
+            for (void* q : {(void*)ob_samples, (void*)ob_vel, (void*)ob_flag, (void*)ob_rank, (void*)ob_scan})
+                if (q) cudaFree(q);
+            ob_samples = ob_vel = nullptr;
+            ob_flag = ob_rank = ob_scan = nullptr;
+            ob_cap = std::max(ns, ob_cap);
+            DF_TRY(dalloc(&ob_samples, ob_cap));
+            DF_TRY(dalloc(&ob_vel, ob_cap));
+            DF_TRY(dalloc(&ob_flag, ob_cap));
+            DF_TRY(dalloc(&ob_rank, ob_cap));
+            DF_TRY(dalloc(&ob_scan, scan_scratch_words(std::max(ob_cap, Nc))));
+            if (!ob_total) DF_TRY(dalloc(&ob_total, 2));
+            if (!h_ob) DF_CUDA(cudaMallocHost((void**)&h_ob, 2 * sizeof(uint32_t)));
+        }
+        ob_boundary = *bnd;
+        ob_interior = *interior;
+        ob_surface = *surf;
+        ob_ns = 0;
+        if (ns) {
+            std::vector<float4> h(ns);
+            for (uint32_t i = 0; i < ns; ++i) h[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.f);
+            DF_CUDA(cudaMemcpyAsync(ob_vel, h.data(), (size_t)ns * sizeof(float4), cudaMemcpyHostToDevice, stream));
+            launch_open_boundary_select<Real>(ob_vel, ns, ob_interior, ob_surface, params(), ob_flag, stream);
+            exclusive_scan_u32(ob_flag, ob_rank, ns, ob_scan, ob_total, stream);
+            launch_compact_samples(ob_vel, ob_flag, ob_rank, ns, ob_samples, stream);
+            DF_CUDA(cudaMemcpyAsync(h_ob, ob_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+            DF_CUDA(cudaGetLastError());
+            ob_ns = h_ob[0];
+            launches += 5;
+        }
+        ob_ready = true;
+        if (n_kept) *n_kept = ob_ns;
+        return DFSPH_OK;
+    }
+
+    int open_boundary_samples(float* xyz, uint32_t capacity, uint32_t* count) {
+        DF_CHECK(count, DFSPH_E_INVALID, "null count");
+        DF_CHECK(ob_ready, DFSPH_E_STATE, "open boundary not initialised (dfsph_open_boundary_init)");
+        *count = ob_ns;
+        if (!xyz) return DFSPH_OK;
+        DF_CHECK(capacity >= ob_ns, DFSPH_E_INVALID, "capacity below the sample count");
+        std::vector<float4> h(ob_ns);
+        if (ob_ns) {
+            DF_CUDA(cudaMemcpyAsync(h.data(), ob_samples, (size_t)ob_ns * sizeof(float4), cudaMemcpyDeviceToHost,
+                                    stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+        }
+        for (uint32_t i = 0; i < ob_ns; ++i) {
+            xyz[3 * i] = h[i].x;
+            xyz[3 * i + 1] = h[i].y;
+            xyz[3 * i + 2] = h[i].z;
+        }
+        return DFSPH_OK;
+    }
+
+    int open_boundary_shift(const float* delta) {
+        DF_CHECK(delta, DFSPH_E_INVALID, "null delta");
+        DF_CHECK(ob_ready, DFSPH_E_STATE, "open boundary not initialised (dfsph_open_boundary_init)");
+        for (dfsph_surface* S : {&ob_boundary, &ob_interior, &ob_surface}) {
+            float* c = (S->type == DFSPH_SURFACE_PLANE) ? S->origin : S->center;
+            for (int a = 0; a < 3; ++a) c[a] += delta[a];
+        }
+        launch_shift_samples(ob_samples, ob_ns, delta[0], delta[1], delta[2], stream);
+        launches += ob_ns ? 1 : 0;
         DF_CUDA(cudaGetLastError());
+        return DFSPH_OK;
+    }
+
+    int open_boundary_apply(double allowed_distance, double allowed_density, bool inflow, bool outflow,
+                            uint32_t* added, uint32_t* removed) {
+        DF_CHECK(ob_ready, DFSPH_E_STATE, "open boundary not initialised (dfsph_open_boundary_init)");
+        if (inflow)
+            DF_CHECK(allowed_distance > 0 && allowed_density > 0, DFSPH_E_INVALID,
+                     "open boundary inflow needs allowed_distance > 0 and allowed_density > 0");
+        uint32_t n_add = 0, n_rm = 0;
+        bool clipped = false;
+        const uint32_t n0 = n;
+        if (inflow && ob_ns) {
+            DF_TRY(bin_fluid());
+            const double d = 2.0 * sc.particle_radius;
+            const Real mass = (Real)(float)(0.8 * d * d * d * sc.density0);
+            launch_inflow<Real>(ds, ob_samples, ob_ns, (float)allowed_distance, (float)allowed_density, mass,
+                                ob_boundary, ftab, btab, ob_flag, ob_vel, stream);
+            exclusive_scan_u32(ob_flag, ob_rank, ob_ns, ob_scan, ob_total, stream);
+            DF_CUDA(cudaMemcpyAsync(h_ob, ob_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+            const uint32_t want = h_ob[0];
+            n_add = std::min<uint32_t>(want, Nc - n);
+            clipped = n_add < want;
+            launch_append_inflow<Real>(ob_samples, ob_vel, ob_flag, ob_rank, ob_ns, n, Nc, mass, pos[cur], vel[cur],
+                                       kappa[cur], kappaV[cur], id[cur], learned ? kappaT[cur] : nullptr,
+                                       learned ? kappaVT[cur] : nullptr, stream);
+            n += n_add;
+            launches += 5;
+        }
+        if (outflow && n) {
+            uint32_t* alive = sb.keys_a;
+            uint32_t* dst = sb.vals_a;
+            launch_outflow_tag<Real>(pos[cur], n, ob_interior, ob_surface, alive, stream);
+            exclusive_scan_u32(alive, dst, n, ob_scan, ob_total, stream);
+            DF_CUDA(cudaMemcpyAsync(h_ob, ob_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+            const uint32_t kept = h_ob[0];
+            n_rm = n - kept;
+            launches += 4;
+            if (n_rm) {
+                const int nx = 1 - cur;
+                launch_compact_fluid<Real>(alive, dst, n, pos[cur], vel[cur], kappa[cur], kappaV[cur], id[cur],
+                                           learned ? kappaT[cur] : nullptr, learned ? kappaVT[cur] : nullptr,
+                                           pos[nx], vel[nx], kappa[nx], kappaV[nx], id[nx],
+                                           learned ? kappaT[nx] : nullptr, learned ? kappaVT[nx] : nullptr, stream);
+                // ids stay dense: survivors keep their relative id order
+                uint32_t* alive_by_id = sb.keys_b;
+                uint32_t* new_id = sb.vals_b;
+                launch_alive_by_id(id[cur], alive, n, alive_by_id, stream);
+                exclusive_scan_u32(alive_by_id, new_id, n, ob_scan, ob_total + 1, stream);
+                launch_renumber_ids(id[nx], kept, new_id, stream);
+                cur = nx;
+                n = kept;
+                launches += 6;
+            }
+        }
+        if (n != n0) {
+            invalidate_graphs();
+            DF_TRY(sync_state());
+        }
+        if (clipped) {
+            uint32_t st = 0;
+            DF_CUDA(cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+            st |= DFSPH_ST_FLUID_CAPACITY;
+            DF_CUDA(cudaMemcpyAsync(status, &st, sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        }
+        DF_CUDA(cudaStreamSynchronize(stream));
+        DF_CUDA(cudaGetLastError());
+        if (added) *added = n_add;
+        if (removed) *removed = n_rm;
         return DFSPH_OK;
     }
 
@@ -1885,6 +2075,20 @@ int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launc
 int dfsph_save_snapshot(dfsph_ctx* ctx, const char* dir, int what) { DFSPH_DISPATCH(ctx, save_snapshot(dir, what)); }
 int dfsph_checkpoint_save(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, save_checkpoint(path)); }
 int dfsph_export_bgeo(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, export_bgeo(path)); }
+int dfsph_open_boundary_init(dfsph_ctx* ctx, const dfsph_surface* boundary, const dfsph_surface* interior,
+                             const dfsph_surface* fluid_surface, const float* sample_xyz, uint32_t n_samples,
+                             uint32_t* n_kept) {
+    DFSPH_DISPATCH(ctx, open_boundary_init(boundary, interior, fluid_surface, sample_xyz, n_samples, n_kept));
+}
+int dfsph_open_boundary_apply(dfsph_ctx* ctx, double allowed_distance, double allowed_density, int use_inflow,
+                              int use_outflow, uint32_t* added, uint32_t* removed) {
+    DFSPH_DISPATCH(ctx, open_boundary_apply(allowed_distance, allowed_density, use_inflow != 0, use_outflow != 0,
+                                            added, removed));
+}
+int dfsph_open_boundary_shift(dfsph_ctx* ctx, const float* delta) { DFSPH_DISPATCH(ctx, open_boundary_shift(delta)); }
+int dfsph_open_boundary_samples(dfsph_ctx* ctx, float* xyz, uint32_t capacity, uint32_t* count) {
+    DFSPH_DISPATCH(ctx, open_boundary_samples(xyz, capacity, count));
+}
 int dfsph_bgeo_write(const char* path, const float* xyz, const float* vxyz, uint64_t count, float radius) {
     std::string err;
     if (!path) err = "dfsph_bgeo_write: null path";

@@ -300,6 +300,41 @@ class DFSPHCUDA:
         v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32)
         self._call(self._lib.dfsph_update_fluid(self._ctx, _fptr(x), _fptr(v)))
 
+    # ---- simple open boundary (OpenBoundariesSimpleInterface) ------------------------------------
+    def init_open_boundary(self, boundary, interior, fluid_surface, samples: np.ndarray) -> int:
+        """OpenBoundariesSimpleInterface::init: keeps the inflow samples outside `interior` and inside
+        `fluid_surface` (surfaces from splishsplash_for_cuda_b200.open_boundary); returns their count."""
+        x = np.ascontiguousarray(samples, dtype=np.float32).reshape(-1, 3)
+        kept = C.c_uint32(0)
+        self._call(self._lib.dfsph_open_boundary_init(self._ctx, C.byref(boundary), C.byref(interior),
+                                                      C.byref(fluid_surface), _fptr(x), x.shape[0], C.byref(kept)))
+        return kept.value
+
+    def apply_open_boundary(self, allowed_distance: float | None = None, allowed_density: float = 700.0,
+                            use_inflow: bool = True, use_outflow: bool = True) -> tuple[int, int]:
+        """OpenBoundariesSimpleInterface::applyOpenBoundary between steps; the defaults are the
+        reference driver's (DFSPH_CUDA.cpp:3903-3906: 1.75 r and 700). Returns (added, removed)."""
+        if allowed_distance is None:
+            allowed_distance = 1.75 * self.scene.config.particleRadius
+        added, removed = C.c_uint32(0), C.c_uint32(0)
+        self._call(self._lib.dfsph_open_boundary_apply(self._ctx, float(allowed_distance), float(allowed_density),
+                                                       int(use_inflow), int(use_outflow), C.byref(added),
+                                                       C.byref(removed)))
+        return added.value, removed.value
+
+    def open_boundary_samples(self) -> np.ndarray:
+        """The kept inflow samples (n, 3), in sample order."""
+        cnt = C.c_uint32(0)
+        self._call(self._lib.dfsph_open_boundary_samples(self._ctx, None, 0, C.byref(cnt)))
+        x = np.zeros((cnt.value, 3), np.float32)
+        self._call(self._lib.dfsph_open_boundary_samples(self._ctx, _fptr(x), cnt.value, C.byref(cnt)))
+        return x
+
+    def shift_open_boundary(self, delta) -> None:
+        """Moves the open boundary's surfaces and samples (dynamic-window displacement)."""
+        d = np.ascontiguousarray(delta, dtype=np.float32).reshape(3)
+        self._call(self._lib.dfsph_open_boundary_shift(self._ctx, _fptr(d)))
+
     def move_boundary(self, positions: np.ndarray, velocities: np.ndarray | None = None) -> None:
         x = np.ascontiguousarray(positions, dtype=np.float32)
         v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32)

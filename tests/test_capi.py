@@ -2,6 +2,8 @@
 declares, the ctypes layouts match the header, and without a GPU the product fails loudly."""
 import ctypes as C
 import re
+import shutil
+import subprocess
 from pathlib import Path
 
 import pytest
@@ -39,11 +41,36 @@ def test_scene_defaults_match_reference_timestep(cuda_lib):
 
 
 def test_struct_sizes_match_header(cuda_lib):
-    # dfsph_scene: 3 doubles, gravitation[3], dt, then mixed fields; checked against the C layout
-    # by compiling a probe would need a compiler at test time, so check the ctypes size is the
-    # natural C size of the declared field sequence.
     assert C.sizeof(_capi.DfsphScene) % 8 == 0
     assert C.sizeof(_capi.DfsphStepStats) == 64
+    assert C.sizeof(_capi.Surface) == 80
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="no C compiler")
+def test_struct_layouts_match_c_compiler(tmp_path):
+    """sizeof / offsetof of every struct of the header, from gcc, against the ctypes layouts."""
+    structs = {"dfsph_scene": _capi.DfsphScene, "dfsph_step_stats": _capi.DfsphStepStats,
+               "dfsph_surface": _capi.Surface}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dfsph_c.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            a, b, c = line.split()
+            got[(a, b)] = int(c)
+    for cname, cls in structs.items():
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
 
 
 def test_create_without_gpu_fails_loudly(cuda_lib):

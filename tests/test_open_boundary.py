@@ -1,0 +1,153 @@
+"""Simple open boundary on the CPU: the oracle's restatement of BufferFluidSurface against the
+reference's own class (fixtures made by tests/golden/open_boundary/make_surface_golden.py from
+SPlisHSPlasH/DFSPH/BufferFluidSurface.cu compiled as host code; the live pin when it is built), the
+reference's configuration table, and the oracle's inflow / outflow against a brute-force numpy
+restatement of OpenBoundariesSimple.cu:352-492 on a small tank. No GPU is needed."""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import Oracle
+from oracle.oracle import OracleSurface, surface_eval
+from splishsplash_for_cuda_b200 import open_boundary as ob
+from splishsplash_for_cuda_b200.scene import Configuration, Scene, box_wall, lattice_block
+
+GOLD = Path(__file__).resolve().parent / "golden" / "open_boundary" / "surfaces.npz"
+PIN = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "libsurface_pin.so"
+
+
+def test_oracle_surfaces_match_reference_fixture():
+    z = np.load(GOLD)
+    assert z["surfaces"].shape[0] == 22
+    for k in range(z["surfaces"].shape[0]):
+        s = OracleSurface.from_buffer_copy(z["surfaces"][k].tobytes())
+        inside, normal = surface_eval(s, z["points"][k])
+        assert np.array_equal(inside, z["inside"][k].astype(bool)), k
+        assert np.array_equal(normal, z["normal"][k]), k
+
+
+@pytest.mark.skipif(not PIN.exists(), reason="BufferFluidSurface compiled from the reference sources is not present")
+def test_oracle_surfaces_match_reference_live():
+    lib = C.CDLL(str(PIN))
+    lib.pin_surface_eval.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(99)
+    for s in [ob.cylinder((0.1, 0.0, 0.2), 0.5, 0.8, reversed=True), ob.star((0, 0, 0), 1.0, 2.0, 0.7, 6, (1, 0, 0)),
+              ob.cuboid((0, 0, 0), (0.5, 0.25, 2.0)), ob.plane((0, 0.3, 0), (0.1, 1.0, 0.2), reversed=True),
+              ob.sphere((1, 1, 1), 0.3)]:
+        p = rng.uniform(-2.5, 2.5, size=(5000, 3)).astype(np.float32)
+        ins = np.zeros(p.shape[0], np.uint8)
+        nrm = np.zeros((p.shape[0], 3), np.float32)
+        assert lib.pin_surface_eval(C.addressof(s), p.ctypes.data, p.shape[0], ins.ctypes.data, nrm.ctypes.data) == 0
+        oi, on = surface_eval(s, p)
+        assert np.array_equal(oi, ins.astype(bool)) and np.array_equal(on, nrm)
+
+
+def test_presets():
+    r = 0.01
+    b, i, s, name = ob.preset(0, r)
+    assert name == "inflowPositionsSet_cylinder.txt" and b.type == 2 and b.radius == 1.5
+    assert i.radius == np.float32(np.float32(1.5) - np.float32(3 * r))
+    assert s.type == 0 and tuple(s.normal) == (0.0, -1.0, 0.0) and tuple(s.origin) == (0.0, 1.0, 0.0)
+    b, i, _, _ = ob.preset(600, r)
+    assert b.type == 5 and b.points == 5 and b.radius == 3.5 and b.radius_internal == 2.0
+    b, i, _, name = ob.preset(1001, r)
+    assert b.type == 1 and tuple(i.center) == (0.0, 0.0, -1.0) and name.endswith("corridor.txt")
+    for c in (100, 200, 210, 220, 300, 400, 500):
+        ob.preset(c, r)
+    with pytest.raises(ValueError):
+        ob.preset(7, r)
+
+
+# ---- a small tank: fluid in one half, taller than the fluid surface ----------------------------
+R = 0.025
+
+
+def tank_scene(vx=0.0):
+    cfg = Configuration()
+    cfg.particleRadius = R
+    cfg.timeStepSize = 0.002
+    walls = box_wall((0.0, 0.0, 0.0), (1.0, 1.0, 0.5), 2 * R)
+    fluid = lattice_block((9, 13, 9), R)  # x, z in [0.05, 0.45], y up to 0.65
+    rng = np.random.default_rng(5)
+    fluid = fluid + rng.uniform(-0.01 * R, 0.01 * R, size=fluid.shape)
+    vel = np.zeros_like(fluid)
+    vel[:, 0] = vx * np.where(fluid[:, 2] < 0.25, 1.0, -1.0)
+    return Scene(config=cfg, fluid=fluid.astype(np.float32), boundary=walls.astype(np.float32),
+                 fluid_velocity=vel.astype(np.float32), name="tank")
+
+
+def tank_samples():
+    """The rest lattice of the whole tank with a 1 % r jitter (samples of a fluid at rest: an exact
+    lattice would put new particles at exactly H from each other, where the FP32 pair predicate of
+    the FP32 build and of the FP64 oracle's rounded positions can disagree)."""
+    x = lattice_block((19, 19, 9), R)
+    rng = np.random.default_rng(11)
+    return (x + rng.uniform(-0.01 * R, 0.01 * R, size=x.shape)).astype(np.float32)
+
+
+def tank_surfaces():
+    return (ob.cuboid((0.5, 0.5, 0.25), (0.5, 0.5, 0.25)), ob.cuboid((0.5, 0.5, 0.25), (0.425, 0.425, 0.175)),
+            ob.plane((0.0, 0.5, 0.0), (0.0, -1.0, 0.0)))
+
+
+def _W(r, H):
+    q = r / H
+    k = 8.0 / (np.pi * H ** 3)
+    return np.where(q <= 0.5, k * (6 * q ** 3 - 6 * q ** 2 + 1), np.where(q <= 1.0, k * 2 * (1 - q) ** 3, 0.0))
+
+
+def test_oracle_open_boundary_against_numpy():
+    s = tank_scene(vx=0.3)
+    o = Oracle(s, 64)
+    b, i, f = tank_surfaces()
+    samples = tank_samples()
+    kept = o.open_boundary_init(b, i, f, samples)
+    ins_i, _ = surface_eval(i, samples)
+    ins_f, _ = surface_eval(f, samples)
+    ks = samples[~ins_i & ins_f]
+    assert kept == ks.shape[0] > 0
+    # numpy restatement: brute force over the fluid (every particle within H matters; the reference's
+    # 27-cell iteration adds only particles beyond H, whose kernel weight is zero and which are
+    # farther than allowed_distance)
+    x = s.fluid.astype(np.float64)
+    v = s.fluid_velocity.astype(np.float64)
+    xb = s.boundary.astype(np.float64)
+    psi = o.field("boundary_psi")
+    H = 4 * R
+    m = np.float32(0.8 * (2 * R) ** 3 * 1000.0)
+    allowed = 1.75 * R
+    exp_x, exp_v = [], []
+    _, nrm = surface_eval(b, ks)
+    for q, nq in zip(ks.astype(np.float64), nrm):
+        d = np.linalg.norm(x - q, axis=1)
+        if d.size and d.min() <= np.float32(allowed):
+            continue
+        w = _W(d, H) * m
+        wb = _W(np.linalg.norm(xb - q, axis=1), H) * psi
+        rho = _W(0.0, H) * m + w.sum() + wb.sum()
+        ws = w.sum() + wb.sum()
+        vq = (w[:, None] * v).sum(0) / ws if ws > 0 else np.zeros(3)
+        if rho > 700.0 or float(np.dot(vq.astype(np.float32), nq)) < 0:
+            continue
+        exp_x.append(q)
+        exp_v.append(vq)
+    added, removed, clipped = o.open_boundary_apply(allowed, 700.0, True, False)
+    assert not clipped and added == len(exp_x) > 0 and removed == 0
+    xo, vo = o.field("position"), o.field("velocity")
+    assert np.array_equal(xo[:s.n_fluid], x) and np.array_equal(xo[s.n_fluid:], np.array(exp_x))
+    assert np.abs(vo[s.n_fluid:] - np.array(exp_v)).max() <= 1e-6 * max(1.0, np.abs(exp_v).max())
+    assert np.all(o.field("kappa")[s.n_fluid:] == 0)
+    # outflow: particles outside the interior and above the fluid surface, order kept
+    xo = o.field("position")
+    ii, _ = surface_eval(i, xo)
+    ff, _ = surface_eval(f, xo)
+    keep = ii | ff
+    assert (~keep).sum() > 0
+    a2, r2, _ = o.open_boundary_apply(allowed, 700.0, False, True)
+    assert a2 == 0 and r2 == int((~keep).sum())
+    assert np.array_equal(o.field("position"), xo[keep])
+    # the fluid still steps
+    o.step()
+    assert np.isfinite(o.field("position")).all()
