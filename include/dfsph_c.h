@@ -179,6 +179,15 @@ int dfsph_get_neighbors(dfsph_ctx* ctx, uint32_t* counts, uint32_t* lists, uint3
  * (non-converged solves raise their status bits on the device). */
 int dfsph_step(dfsph_ctx* ctx, dfsph_step_stats* stats);
 
+/* DFSPHCData::checkParticlesPositions (DFSPH_c_arrays_structure.cpp:1599, SPH_other_systems_cuda.cu:
+ * 1242-1328): counts the fluid particles with a coordinate outside the domain box (the boundary's
+ * bounding box, or grid_min / grid_max when given); mode 2 also removes them, keeping the order of
+ * the others and renumbering their ids densely; mode 0 only counts (the reference's mode 1 exits).
+ * A step called with stats ends with mode 2, as DFSPHCUDA::step does (DFSPH_CUDA.cpp:456), unless
+ * the parameter "remove_escaped" is 0; an asynchronous step (stats null) leaves them (a particle that
+ * leaves the cell grid is flagged DFSPH_ST_ESCAPED and keeps moving without neighbours). */
+int dfsph_check_particles_positions(dfsph_ctx* ctx, int mode, uint32_t* count);
+
 /* The seven host functions of DFSPH_core_cuda.h:27-74, for callers that drive the step themselves. */
 int dfsph_neighbors_search(dfsph_ctx* ctx, int sort);                     /* cuda_neighborsSearch */
 int dfsph_divergence_solve(dfsph_ctx* ctx, uint32_t max_iter, double max_error, int32_t* iters);
@@ -197,6 +206,8 @@ int dfsph_on_step_end(dfsph_ctx* ctx);                                    /* onS
  * "h", "h_future", "h_past", "inv_h" (dt history of DFSPHCData), "timing" (1: record CUDA events),
  * "iterations_sum" (setting it clears the counters; reading it gives the pressure iterations of all
  * solves since, "iterations_v_sum" the divergence iterations),
+ * "remove_escaped" (1, default: a step with stats removes particles outside the domain box),
+ * "escaped_removed" (read-only: particles removed that way so far),
  * "boundary_forces" (1: accumulate the fluid's force on every boundary particle in each Jacobi pass,
  * -m_i k_i psi_b grad W_ib summed over both solves of a step, as the reference does for dynamic
  * bodies; cleared by each neighbour search; atomics, so the summation order varies),

@@ -342,29 +342,48 @@ template <class Real> struct Oracle {
             nbd.resize(n);
         }
         if (outflow && n) {
-            uint32_t w = 0;
-            for (uint32_t i = 0; i < n; ++i) {
+            removed = compact([&](uint32_t i) {
                 const float p[3] = {(float)x[3 * i], (float)x[3 * i + 1], (float)x[3 * i + 2]};
-                if (!surface_inside(ob_i, p) && !surface_inside(ob_s, p)) continue;
-                if (w != i) {
-                    for (int a3 = 0; a3 < 3; ++a3) {
-                        x[3 * w + a3] = x[3 * i + a3];
-                        v[3 * w + a3] = v[3 * i + a3];
-                        a[3 * w + a3] = a[3 * i + a3];
-                    }
-                    for (auto* vec : {&m, &rho, &alpha, &dadv, &kap, &kapv, &kc}) (*vec)[w] = (*vec)[i];
-                }
-                ++w;
-            }
-            removed = n - w;
-            n = w;
-            x.resize(3 * (size_t)n);
-            v.resize(3 * (size_t)n);
-            a.resize(3 * (size_t)n);
-            for (auto* vec : {&m, &rho, &alpha, &dadv, &kap, &kapv, &kc}) vec->resize(n);
-            nf.resize(n);
-            nbd.resize(n);
+                return surface_inside(ob_i, p) || surface_inside(ob_s, p);
+            });
         }
+    }
+
+    // Keeps the particles with keep(i), in order; returns how many were removed.
+    template <class Keep> uint32_t compact(Keep&& keep) {
+        uint32_t w = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (!keep(i)) continue;
+            if (w != i) {
+                for (int a3 = 0; a3 < 3; ++a3) {
+                    x[3 * w + a3] = x[3 * i + a3];
+                    v[3 * w + a3] = v[3 * i + a3];
+                    a[3 * w + a3] = a[3 * i + a3];
+                }
+                for (auto* vec : {&m, &rho, &alpha, &dadv, &kap, &kapv, &kc}) (*vec)[w] = (*vec)[i];
+            }
+            ++w;
+        }
+        const uint32_t removed = n - w;
+        n = w;
+        x.resize(3 * (size_t)n);
+        v.resize(3 * (size_t)n);
+        a.resize(3 * (size_t)n);
+        for (auto* vec : {&m, &rho, &alpha, &dadv, &kap, &kapv, &kc}) vec->resize(n);
+        nf.resize(n);
+        nbd.resize(n);
+        return removed;
+    }
+
+    uint32_t remove_out_of_box() {
+        const uint32_t r = compact([&](uint32_t i) {
+            bool out = false;
+            for (int a3 = 0; a3 < 3; ++a3)
+                out = out || x[3 * i + a3] > (Real)bb_hi[a3] || x[3 * i + a3] < (Real)bb_lo[a3];
+            return !out;
+        });
+        escaped_removed += r;
+        return r;
     }
 
     void reset_dt() {
@@ -373,8 +392,16 @@ template <class Real> struct Oracle {
         h_ratio = h_ratio2 = 1.0;
     }
 
+    // domain box (initGridOffset's boundingBoxMin / Max) and the end-of-step removal of the
+    // particles outside it (checkParticlesPositions(2), SPH_other_systems_cuda.cu:1242-1328)
+    float bb_lo[3] = {0, 0, 0}, bb_hi[3] = {0, 0, 0};
+    bool remove_escaped = true;
+    uint64_t escaped_removed = 0;
+
     void set_grid(const float mn[3], const float mx[3]) {
         for (int a3 = 0; a3 < 3; ++a3) {
+            bb_lo[a3] = mn[a3];
+            bb_hi[a3] = mx[a3];
             const int fmin = (int)std::floor(mn[a3] / Hf);
             const int fmax = (int)std::floor(mx[a3] / Hf);
             off[a3] = -(fmin - 5);
@@ -788,6 +815,7 @@ template <class Real> struct Oracle {
         pressure_solve(prm.max_iterations, prm.max_error);
         update_pos();
         on_step_end();
+        if (remove_escaped) remove_out_of_box();
     }
 };
 
@@ -1001,6 +1029,8 @@ int oracle_get_scalar(void* h, const char* key, double* out) {
         else if (k == "grid_dim_x") *out = o.dim[0];
         else if (k == "grid_dim_y") *out = o.dim[1];
         else if (k == "grid_dim_z") *out = o.dim[2];
+        else if (k == "n") *out = o.n;
+        else if (k == "escaped_removed") *out = (double)o.escaped_removed;
         else return -1;
         return 0;
     })());
@@ -1017,6 +1047,7 @@ int oracle_set_scalar(void* h, const char* key, double v) {
             o.bforce_on = v != 0;
             if (o.bforce_on) o.bF.assign(3 * (size_t)o.nb, 0.0);
         }
+        else if (k == "remove_escaped") o.remove_escaped = v != 0;
         else return -1;
         return 0;
     })());

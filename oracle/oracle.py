@@ -174,6 +174,7 @@ class Oracle:
         it, itv = C.c_int32(), C.c_int32()
         err, errv = C.c_double(), C.c_double()
         overflow = self.lib.oracle_step(self.h, C.byref(it), C.byref(itv), C.byref(err), C.byref(errv))
+        self.n = int(self.scalar("n"))  # particles outside the domain box are removed at the step end
         return dict(iterations=it.value, iterations_v=itv.value, density_error=err.value,
                     divergence_error=errv.value, overflow=bool(overflow))
 

@@ -158,6 +158,11 @@ public:
     uint32_t* h_ob = nullptr;      // pinned copy of a scan total
     uint32_t ob_ns = 0, ob_cap = 0;
 
+    // end-of-step removal of particles outside the domain box (checkParticlesPositions(2))
+    float bb_lo[3] = {0, 0, 0}, bb_hi[3] = {0, 0, 0};
+    bool remove_escaped = true;
+    uint64_t escaped_removed = 0;
+
     // ------------------------------------------------------------------------------------------
     template <class T> int dalloc(T** p, size_t count) {
         *p = nullptr;
@@ -366,6 +371,8 @@ public:
     int set_grid(const float mn[3], const float mx[3]) {
         const float H = (float)(4.0 * sc.particle_radius);
         for (int a = 0; a < 3; ++a) {
+            bb_lo[a] = mn[a];  // initGridOffset keeps the box as boundingBoxMin / Max
+            bb_hi[a] = mx[a];
             DF_CHECK(std::isfinite(mn[a]) && std::isfinite(mx[a]) && mx[a] >= mn[a], DFSPH_E_INVALID,
                      "invalid grid bounding box");
             const int fmin = (int)std::floor(mn[a] / H);
@@ -678,6 +685,65 @@ public:
         return DFSPH_OK;
     }
 
+    // Stable removal of the particles with alive[i] == 0 (dst = exclusive scan of alive, kept
+    // survivors): the state moves to the other buffer; ids stay dense and keep their relative order.
+    int compact_fluid(const uint32_t* alive, const uint32_t* dst, uint32_t kept) {
+        const int nx = 1 - cur;
+        launch_compact_fluid<Real>(alive, dst, n, pos[cur], vel[cur], kappa[cur], kappaV[cur], id[cur],
+                                   learned ? kappaT[cur] : nullptr, learned ? kappaVT[cur] : nullptr, pos[nx],
+                                   vel[nx], kappa[nx], kappaV[nx], id[nx], learned ? kappaT[nx] : nullptr,
+                                   learned ? kappaVT[nx] : nullptr, stream);
+        uint32_t* alive_by_id = sb.keys_b;
+        uint32_t* new_id = sb.vals_b;
+        launch_alive_by_id(id[cur], alive, n, alive_by_id, stream);
+        exclusive_scan_u32(alive_by_id, new_id, n, ob_scan, ob_total + 1, stream);
+        launch_renumber_ids(id[nx], kept, new_id, stream);
+        cur = nx;
+        n = kept;
+        launches += 6;
+        return DFSPH_OK;
+    }
+
+    int ensure_scan_scratch() {
+        if (!ob_scan) DF_TRY(dalloc(&ob_scan, scan_scratch_words(std::max(ob_cap, Nc))));
+        if (!ob_total) DF_TRY(dalloc(&ob_total, 2));
+        if (!h_ob) DF_CUDA(cudaMallocHost((void**)&h_ob, 2 * sizeof(uint32_t)));
+        return DFSPH_OK;
+    }
+
+    // checkParticlesPositions (DFSPH_c_arrays_structure.cpp:1599, SPH_other_systems_cuda.cu:1283-1328):
+    // counts the fluid particles outside the domain box; mode 2 also removes them (stable).
+    int check_particles_positions(int mode, uint32_t* count) {
+        DF_CHECK(mode == 0 || mode == 2, DFSPH_E_INVALID, "mode must be 0 (count) or 2 (remove)");
+        uint32_t c = 0;
+        if (n && grid_ready) {
+            DF_TRY(ensure_scan_scratch());
+            DF_CUDA(cudaMemsetAsync(status + 3, 0, sizeof(uint32_t), stream));
+            launch_box_tag<Real>(pos[cur], n, bb_lo, bb_hi, sb.keys_a, status + 3, stream);
+            DF_CUDA(cudaMemcpyAsync(h_status + 3, status + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+            c = h_status[3];
+            launches += 1;
+            if (mode == 2 && c) DF_TRY(remove_tagged(c));
+        }
+        if (count) *count = c;
+        return DFSPH_OK;
+    }
+
+    // Removes the c particles whose sb.keys_a flag is 0.
+    int remove_tagged(uint32_t c) {
+        DF_TRY(ensure_scan_scratch());
+        exclusive_scan_u32(sb.keys_a, sb.vals_a, n, ob_scan, ob_total, stream);
+        launches += 3;
+        DF_TRY(compact_fluid(sb.keys_a, sb.vals_a, n - c));
+        escaped_removed += c;
+        invalidate_graphs();
+        DF_TRY(sync_state());
+        DF_CUDA(cudaStreamSynchronize(stream));
+        DF_CUDA(cudaGetLastError());
+        return DFSPH_OK;
+    }
+
     int open_boundary_apply(double allowed_distance, double allowed_density, bool inflow, bool outflow,
                             uint32_t* added, uint32_t* removed) {
         DF_CHECK(ob_ready, DFSPH_E_STATE, "open boundary not initialised (dfsph_open_boundary_init)");
@@ -715,22 +781,7 @@ public:
             const uint32_t kept = h_ob[0];
             n_rm = n - kept;
             launches += 4;
-            if (n_rm) {
-                const int nx = 1 - cur;
-                launch_compact_fluid<Real>(alive, dst, n, pos[cur], vel[cur], kappa[cur], kappaV[cur], id[cur],
-                                           learned ? kappaT[cur] : nullptr, learned ? kappaVT[cur] : nullptr,
-                                           pos[nx], vel[nx], kappa[nx], kappaV[nx], id[nx],
-                                           learned ? kappaT[nx] : nullptr, learned ? kappaVT[nx] : nullptr, stream);
-                // ids stay dense: survivors keep their relative id order
-                uint32_t* alive_by_id = sb.keys_b;
-                uint32_t* new_id = sb.vals_b;
-                launch_alive_by_id(id[cur], alive, n, alive_by_id, stream);
-                exclusive_scan_u32(alive_by_id, new_id, n, ob_scan, ob_total + 1, stream);
-                launch_renumber_ids(id[nx], kept, new_id, stream);
-                cur = nx;
-                n = kept;
-                launches += 6;
-            }
+            if (n_rm) DF_TRY(compact_fluid(alive, dst, kept));
         }
         if (n != n0) {
             invalidate_graphs();
@@ -961,7 +1012,7 @@ public:
     // Reads the loop control blocks and the status word (one synchronisation).
     int collect(bool div_ran, int max_iter_v, int max_iter) {
         DF_CUDA(cudaMemcpyAsync(h_ctl, ctl, 2 * sizeof(LoopCtl), cudaMemcpyDeviceToHost, stream));
-        DF_CUDA(cudaMemcpyAsync(h_status, status, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaMemcpyAsync(h_status, status, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         DF_CUDA(cudaMemcpyAsync(h_dt, dtd, kDtSlots * sizeof(double), cudaMemcpyDeviceToHost, stream));
         DF_CUDA(cudaStreamSynchronize(stream));
         mirror_dt();
@@ -1023,7 +1074,17 @@ public:
         DF_TRY(on_step_end());
         if (timing) DF_CUDA(cudaEventRecord(ev1, stream));
         if (!st) return DFSPH_OK;  // asynchronous step: nothing read back, the host does not wait
+        // DFSPHCUDA::step ends with checkParticlesPositions(2) (DFSPH_CUDA.cpp:456): the count comes
+        // back with the status words; the removal itself runs only when there is something to remove.
+        const bool tag = remove_escaped && n > 0;
+        if (tag) {
+            DF_TRY(ensure_scan_scratch());
+            DF_CUDA(cudaMemsetAsync(status + 3, 0, sizeof(uint32_t), stream));
+            launch_box_tag<Real>(pos[cur], n, bb_lo, bb_hi, sb.keys_a, status + 3, stream);
+            launches += 1;
+        }
         DF_TRY(collect(div, sc.max_iterations_v, sc.max_iterations));
+        if (tag && h_status[3]) DF_TRY(remove_tagged(h_status[3]));
         if (lp) {
             const uint32_t w = (h_status[2] | forced_warm) & 3u;
             if (w & 1u) ++kept_v;
@@ -1701,6 +1762,7 @@ public:
         else if (k == "learned_warm_start") return enable_learned(v != 0);
         else if (k == "warm_start_probe") probe = v != 0;
         else if (k == "sort_withhold_tile") sort_withheld_tile = v < 0 ? kNoWithheldTile : (uint32_t)v;
+        else if (k == "remove_escaped") remove_escaped = v != 0;
         else if (k == "boundary_forces") {
             if (v != 0 && !bforce) {
                 DF_TRY(dalloc(&bforce, (size_t)Bc * 4));
@@ -1779,6 +1841,8 @@ public:
         else if (k == "learned_warm_start") *v = learned ? 1 : 0;
         else if (k == "warm_start_probe") *v = probe ? 1 : 0;
         else if (k == "boundary_forces") *v = boundary_forces ? 1 : 0;
+        else if (k == "remove_escaped") *v = remove_escaped ? 1 : 0;
+        else if (k == "escaped_removed") *v = (double)escaped_removed;
         else if (k == "warm_start_damping") *v = damping;
         else if (k == "train_interval") *v = train_interval;
         else if (k == "train_start") *v = train_start;
@@ -2075,6 +2139,9 @@ int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launc
 int dfsph_save_snapshot(dfsph_ctx* ctx, const char* dir, int what) { DFSPH_DISPATCH(ctx, save_snapshot(dir, what)); }
 int dfsph_checkpoint_save(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, save_checkpoint(path)); }
 int dfsph_export_bgeo(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, export_bgeo(path)); }
+int dfsph_check_particles_positions(dfsph_ctx* ctx, int mode, uint32_t* count) {
+    DFSPH_DISPATCH(ctx, check_particles_positions(mode, count));
+}
 int dfsph_open_boundary_init(dfsph_ctx* ctx, const dfsph_surface* boundary, const dfsph_surface* interior,
                              const dfsph_surface* fluid_surface, const float* sample_xyz, uint32_t n_samples,
                              uint32_t* n_kept) {

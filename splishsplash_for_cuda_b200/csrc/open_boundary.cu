@@ -400,6 +400,21 @@ __global__ void __launch_bounds__(kBlock) compact_fluid_kernel(
     if (kVT_in) kVT_out[k] = kVT_in[i];
 }
 
+// checkParticlesPositions(2) (SPH_other_systems_cuda.cu:1242-1281): a particle with any coordinate
+// above the box maximum or below its minimum is removed (NaN coordinates compare false and stay).
+template <class Real>
+__global__ void __launch_bounds__(kBlock) box_tag_kernel(const Vec4<Real>* __restrict__ pos, uint32_t n, float lo_x,
+                                                         float lo_y, float lo_z, float hi_x, float hi_y, float hi_z,
+                                                         uint32_t* __restrict__ alive, uint32_t* __restrict__ count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Vec4<Real> x = pos[i];
+    const bool out = x.x > (Real)hi_x || x.y > (Real)hi_y || x.z > (Real)hi_z || x.x < (Real)lo_x ||
+                     x.y < (Real)lo_y || x.z < (Real)lo_z;
+    alive[i] = out ? 0u : 1u;
+    if (out) atomicAdd(count, 1u);
+}
+
 __global__ void __launch_bounds__(kBlock) alive_by_id_kernel(const uint32_t* __restrict__ id,
                                                              const uint32_t* __restrict__ alive, uint32_t n,
                                                              uint32_t* __restrict__ out) {
@@ -473,6 +488,13 @@ void launch_compact_fluid(const uint32_t* alive, const uint32_t* dst, uint32_t n
                                                                   id_in, kT_in, kVT_in, pos_out, vel_out, kappa_out,
                                                                   kappaV_out, id_out, kT_out, kVT_out);
 }
+template <class Real>
+void launch_box_tag(const Vec4<Real>* pos, uint32_t n, const float lo[3], const float hi[3], uint32_t* alive,
+                    uint32_t* count, cudaStream_t s) {
+    if (n)
+        box_tag_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(pos, n, lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], alive,
+                                                            count);
+}
 void launch_alive_by_id(const uint32_t* id, const uint32_t* alive, uint32_t n, uint32_t* alive_by_id, cudaStream_t s) {
     if (n) alive_by_id_kernel<<<grid_for(n), kBlock, 0, s>>>(id, alive, n, alive_by_id);
 }
@@ -492,7 +514,9 @@ void launch_renumber_ids(uint32_t* id, uint32_t n, const uint32_t* new_id, cudaS
                                         cudaStream_t);                                                            \
     template void launch_compact_fluid<R>(const uint32_t*, const uint32_t*, uint32_t, const Vec4<R>*,             \
                                           const Vec4<R>*, const R*, const R*, const uint32_t*, const R*, const R*, \
-                                          Vec4<R>*, Vec4<R>*, R*, R*, uint32_t*, R*, R*, cudaStream_t);
+                                          Vec4<R>*, Vec4<R>*, R*, R*, uint32_t*, R*, R*, cudaStream_t);       \
+    template void launch_box_tag<R>(const Vec4<R>*, uint32_t, const float*, const float*, uint32_t*, uint32_t*,   \
+                                    cudaStream_t);
 
 DFSPH_INSTANTIATE_OPEN_BOUNDARY(float)
 DFSPH_INSTANTIATE_OPEN_BOUNDARY(double)

@@ -58,6 +58,11 @@ void launch_compact_fluid(const uint32_t* alive, const uint32_t* dst, uint32_t n
                           const Real* kT_in, const Real* kVT_in, Vec4<Real>* pos_out, Vec4<Real>* vel_out,
                           Real* kappa_out, Real* kappaV_out, uint32_t* id_out, Real* kT_out, Real* kVT_out,
                           cudaStream_t s);
+// alive[i] = 0 (and *count += 1) for particles with a coordinate outside [lo, hi]
+// (checkParticlesPositions(2), SPH_other_systems_cuda.cu:1242-1281), 1 otherwise.
+template <class Real>
+void launch_box_tag(const Vec4<Real>* pos, uint32_t n, const float lo[3], const float hi[3], uint32_t* alive,
+                    uint32_t* count, cudaStream_t s);
 void launch_alive_by_id(const uint32_t* id, const uint32_t* alive, uint32_t n, uint32_t* alive_by_id, cudaStream_t s);
 void launch_renumber_ids(uint32_t* id, uint32_t n, const uint32_t* new_id, cudaStream_t s);
 

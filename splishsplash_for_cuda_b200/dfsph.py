@@ -300,6 +300,13 @@ class DFSPHCUDA:
         v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32)
         self._call(self._lib.dfsph_update_fluid(self._ctx, _fptr(x), _fptr(v)))
 
+    def checkParticlesPositions(self, mode: int = 2) -> int:
+        """DFSPHCData::checkParticlesPositions: the number of fluid particles outside the domain box;
+        mode 2 also removes them (mode 0 only counts)."""
+        c = C.c_uint32(0)
+        self._call(self._lib.dfsph_check_particles_positions(self._ctx, int(mode), C.byref(c)))
+        return c.value
+
     # ---- simple open boundary (OpenBoundariesSimpleInterface) ------------------------------------
     def init_open_boundary(self, boundary, interior, fluid_surface, samples: np.ndarray) -> int:
         """OpenBoundariesSimpleInterface::init: keeps the inflow samples outside `interior` and inside

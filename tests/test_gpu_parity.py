@@ -267,6 +267,42 @@ def test_moving_boundary_lockstep_with_oracle():
         check_field(name, d.field(name, np.float64), o.field(name), 1e-4)
 
 
+def test_particles_outside_domain_box_removed_like_reference():
+    """DFSPHCUDA::step ends with checkParticlesPositions(2): particles outside the boundary's box are
+    removed, the others keep their order (ids renumbered densely). Seven particles start outside the
+    walls, moving away."""
+    s = synthetic_scene(1, counts=(10, 10, 10))
+    s.fluid = s.fluid.copy()
+    s.fluid_velocity = np.zeros_like(s.fluid)
+    out = np.arange(3, 73, 10)
+    s.fluid[out] = np.array([-0.2, 0.5, 0.5], np.float32)
+    s.fluid[out, 1] += 0.06 * np.arange(7, dtype=np.float32)
+    s.fluid_velocity[out] = (-1.0, 0.0, 0.0)
+    d = DFSPHCUDA(s)
+    o = Oracle(s, 64)
+    for k in range(3):
+        st = d.step()
+        o.step()
+        assert st.num_fluid == o.n == s.n_fluid - 7, k
+    assert d.get_param("escaped_removed") == 7
+    keep = np.setdiff1d(np.arange(s.n_fluid), out)
+    assert np.abs(d.positions()[:, 0]).max() < 2.0
+    check_field("position", d.field("position", np.float64), o.field("position"), 1e-4)
+    # order kept: three steps moved every survivor by less than 2r from its start
+    assert np.abs(d.positions().astype(np.float64) - s.fluid[keep]).max() < 2 * s.config.particleRadius
+    # asynchronous steps leave them; the explicit call counts and removes
+    a = DFSPHCUDA(s)
+    a.step_async()
+    a.synchronize()
+    assert a.checkParticlesPositions(0) == 7 and a.num_fluid() == s.n_fluid
+    assert a.checkParticlesPositions(2) == 7 and a.num_fluid() == s.n_fluid - 7
+    assert a.checkParticlesPositions(0) == 0
+    a.set_param("remove_escaped", 0)
+    b = DFSPHCUDA(s)
+    b.set_param("remove_escaped", 0)
+    assert b.step().num_fluid == s.n_fluid
+
+
 def test_empty_and_single_particle_fluid():
     s = synthetic_scene(1, counts=(4, 4, 4))
     d = DFSPHCUDA(s)
