@@ -352,6 +352,15 @@ int dfsph_open_boundary_samples(dfsph_ctx* ctx, float* xyz, uint32_t capacity, u
  * displacement this way, OpenBoundariesSimple.cu:527-553). */
 int dfsph_open_boundary_shift(dfsph_ctx* ctx, const float* delta);
 
+/* Force and torque of the fluid on boundary bodies during the last step (needs "boundary_forces" 1):
+ * the per-particle forces the reference hands to its rigid-body solver (readDynamicObjectsData,
+ * DFSPH_c_arrays_structure.cpp:1177-1193), summed on the device. Body b is the range
+ * [first[b], first[b] + count[b]) of the boundary particles in the order given to dfsph_set_boundary;
+ * force_torque[6 b + 0..2] receives the force, [6 b + 3..5] the torque about centers[3 b..3 b + 2]
+ * (FP64, deterministic). Bodies move with dfsph_move_boundary. */
+int dfsph_body_wrench(dfsph_ctx* ctx, uint32_t n_bodies, const uint32_t* first, const uint32_t* count,
+                      const double* centers, double* force_torque);
+
 /* Binary checkpoint of the complete solver state (no reference counterpart; the text snapshot above
  * drops the warm starts and the particle order): particles in their current internal order with
  * kappa and kappa_v, the boundary with psi, the dt history, the grid, the scene parameters and, when

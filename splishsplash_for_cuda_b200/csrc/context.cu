@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "bgeo.h"
+#include "bodies.cuh"
 #include "dfsph_state.cuh"
 #include "io.cuh"
 #include "mlp.cuh"
@@ -250,7 +251,7 @@ public:
         f(tt);
         f(mlp.params); f(mlp.adam_m); f(mlp.adam_v); f(mlp.grad); f(mlp.partials);
         f(mlp.w1_bf16); f(mlp.w2_bf16); f(mlp.w3_bf16); f(mlp.scales); f(mlp.loss);
-        f(ob_samples); f(ob_vel); f(ob_flag); f(ob_rank); f(ob_scan); f(ob_total);
+        f(ob_samples); f(ob_vel); f(ob_flag); f(ob_rank); f(ob_scan); f(ob_total); f(wrench_buf);
         if (h_ob) cudaFreeHost(h_ob);
         if (h_ctl) cudaFreeHost(h_ctl);
         if (h_status) cudaFreeHost(h_status);
@@ -1459,6 +1460,45 @@ public:
     template <class T> static void put(std::ofstream& f, const T& v) { f.write(reinterpret_cast<const char*>(&v), sizeof(T)); }
     template <class T> static bool get(std::ifstream& f, T& v) { return (bool)f.read(reinterpret_cast<char*>(&v), sizeof(T)); }
 
+    // Force and torque of the fluid on boundary bodies (readDynamicObjectsData + the rigid-body
+    // solver's sum over the body's particles): bodies are ranges of the boundary upload order.
+    double* wrench_buf = nullptr;  // 6 Bc doubles (positions, forces in upload order) + bodies
+    size_t wrench_cap = 0;
+    int body_wrench(uint32_t nbod, const uint32_t* first, const uint32_t* count, const double* centers,
+                    double* out) {
+        DF_CHECK(bforce, DFSPH_E_STATE, "boundary forces are off (set_param boundary_forces 1)");
+        DF_CHECK(nbod == 0 || (first && count && centers && out), DFSPH_E_INVALID, "null body arrays");
+        for (uint32_t b = 0; b < nbod; ++b)
+            DF_CHECK((uint64_t)first[b] + count[b] <= nb, DFSPH_E_INVALID, "body range beyond the boundary particles");
+        if (!nbod) return DFSPH_OK;
+        const size_t need = 6 * (size_t)Bc + (size_t)nbod * (2 + 3 + 6);
+        if (need > wrench_cap) {
+            if (wrench_buf) cudaFree(wrench_buf);
+            wrench_buf = nullptr;
+            DF_TRY(dalloc(&wrench_buf, need));
+            wrench_cap = need;
+        }
+        double* xp = wrench_buf;
+        double* fp = wrench_buf + 3 * (size_t)Bc;
+        uint32_t* dfirst = (uint32_t*)(wrench_buf + 6 * (size_t)Bc);
+        uint32_t* dcount = dfirst + nbod;
+        double* dcent = wrench_buf + 6 * (size_t)Bc + nbod;  // 2 nbod uint32 = nbod doubles
+        double* dout = dcent + 3 * (size_t)nbod;
+        if (nb) {
+            launch_pack_field<Real, double>((const Real*)bpos[0], 4, 3, bid, nb, xp, stream);
+            launch_pack_field<Real, double>(bforce, 4, 3, bid, nb, fp, stream);
+        }
+        DF_CUDA(cudaMemcpyAsync(dfirst, first, nbod * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        DF_CUDA(cudaMemcpyAsync(dcount, count, nbod * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        DF_CUDA(cudaMemcpyAsync(dcent, centers, 3 * nbod * sizeof(double), cudaMemcpyHostToDevice, stream));
+        launch_body_wrench(xp, fp, dfirst, dcount, dcent, nbod, dout, stream);
+        DF_CUDA(cudaMemcpyAsync(out, dout, 6 * nbod * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        DF_CUDA(cudaGetLastError());
+        launches += nb ? 3 : 1;
+        return DFSPH_OK;
+    }
+
     // The fluid as a partio particle file (partioExport, Demos/StaticBoundaryDemo/main.cpp:485-496).
     int export_bgeo(const char* path) {
         DF_CHECK(path, DFSPH_E_INVALID, "null path");
@@ -2139,6 +2179,10 @@ int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launc
 int dfsph_save_snapshot(dfsph_ctx* ctx, const char* dir, int what) { DFSPH_DISPATCH(ctx, save_snapshot(dir, what)); }
 int dfsph_checkpoint_save(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, save_checkpoint(path)); }
 int dfsph_export_bgeo(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, export_bgeo(path)); }
+int dfsph_body_wrench(dfsph_ctx* ctx, uint32_t n_bodies, const uint32_t* first, const uint32_t* count,
+                      const double* centers, double* force_torque) {
+    DFSPH_DISPATCH(ctx, body_wrench(n_bodies, first, count, centers, force_torque));
+}
 int dfsph_check_particles_positions(dfsph_ctx* ctx, int mode, uint32_t* count) {
     DFSPH_DISPATCH(ctx, check_particles_positions(mode, count));
 }

@@ -300,6 +300,21 @@ class DFSPHCUDA:
         v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32)
         self._call(self._lib.dfsph_update_fluid(self._ctx, _fptr(x), _fptr(v)))
 
+    def body_wrench(self, first, count, centers) -> tuple[np.ndarray, np.ndarray]:
+        """Force (k, 3) and torque (k, 3) of the fluid during the last step on k boundary bodies,
+        body b being boundary particles first[b] .. first[b] + count[b] - 1 (upload order), torque
+        about centers[b]. Needs set_param("boundary_forces", 1)."""
+        f = np.ascontiguousarray(first, dtype=np.uint32).reshape(-1)
+        c = np.ascontiguousarray(count, dtype=np.uint32).reshape(-1)
+        ce = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
+        k = f.size
+        if c.size != k or ce.shape[0] != k:
+            raise ValueError("first, count and centers must describe the same bodies")
+        out = np.zeros((k, 6), np.float64)
+        self._call(self._lib.dfsph_body_wrench(self._ctx, k, f.ctypes.data, c.ctypes.data, ce.ctypes.data,
+                                               out.ctypes.data))
+        return out[:, :3].copy(), out[:, 3:].copy()
+
     def checkParticlesPositions(self, mode: int = 2) -> int:
         """DFSPHCData::checkParticlesPositions: the number of fluid particles outside the domain box;
         mode 2 also removes them (mode 0 only counts)."""
