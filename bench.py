@@ -217,25 +217,60 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def learned_ablation(local, steps: int, counts=(64, 64, 64)):
-    """Plain vs learned warm start on a stiff workload: a resting column (64 x 64 x 64 = 262,144
-    particles, 64 high, r = 0.008 m, fixed dt 2 ms) at the reference's default 0.01 % tolerance. Both runs take `steps` steps from the same state; the
-    second half is measured (the column has settled by then). ms/step is the device time of each
+ABLATION_WORKLOADS = ("column_64", "sloshing_1m", "column_2m")
+
+
+def ablation_scene(workload: str):
+    """Scenes of the plain vs learned comparison. column_64: a resting column (64 x 64 x 64 =
+    262,144 particles, r = 0.008 m, fixed dt 2 ms) at the reference's default 0.01 % tolerance;
+    sloshing_1m: the 1,000,000-particle sloshing tank (walls translating 0.1 sin(2 pi t / 2) m along
+    x), CFL; column_2m: the 2,000,000-particle column collapse at 0.005 % with dt_max 8 ms, CFL.
+    Returns (scene, wall motion or None)."""
+    from splishsplash_for_cuda_b200.scene import column_scene, synthetic_scene
+
+    if workload == "column_64":
+        return column_scene(counts=(64, 64, 64), time_step=0.002, max_error=0.01), None
+    if workload == "sloshing_1m":
+        scene = synthetic_scene(3, cfl=True)
+        b0 = scene.boundary.astype(np.float64)
+
+        def walls(t):
+            x = b0.copy()
+            x[:, 0] += 0.1 * np.sin(2 * np.pi * t / 2.0)
+            v = np.zeros_like(b0)
+            v[:, 0] = 0.1 * (2 * np.pi / 2.0) * np.cos(2 * np.pi * t / 2.0)
+            return x.astype(np.float32), v.astype(np.float32)
+
+        return scene, walls
+    if workload == "column_2m":
+        return synthetic_scene(4, cfl=True), None
+    raise ValueError(workload)
+
+
+def learned_ablation(local, steps: int, workload: str = "column_64"):
+    """Plain vs learned warm start on the same scene from the same state, each for `steps` steps;
+    the second half is measured (the flow has developed by then). ms/step is the device time of each
     step (CUDA events inside dfsph_step), online training rounds included."""
     from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
-    from splishsplash_for_cuda_b200.scene import column_scene
 
-    scene = column_scene(counts=counts, time_step=0.002, max_error=0.01)
-    out = {"workload": scene.name, "fluid_particles": scene.n_fluid, "steps": steps,
-           "measured_steps": f"{steps // 2}..{steps - 1}", "max_error_pct": 0.01}
+    scene, walls = ablation_scene(workload)
+    out = {"workload": scene.name if workload == "column_64" else workload, "fluid_particles": scene.n_fluid,
+           "steps": steps, "measured_steps": f"{steps // 2}..{steps - 1}",
+           "max_error_pct": scene.config.maxError, "moving_walls": walls is not None,
+           "cfl": bool(scene.config.cflMethod)}
     for mode in ("plain", "learned"):
         d = DFSPHCUDA(scene, device=local)
         d.set_param("timing", 1)
+        if walls is not None:  # the fluid follows the walls past the initial box: keep every particle
+            d.set_param("remove_escaped", 0)
         if mode == "learned":
             d.set_learned_warm_start(True)
-        its, itv, ms, bits = [], [], [], 0
+        its, itv, ms, bits, t = [], [], [], 0, 0.0
         for _ in range(steps):
+            if walls is not None:
+                d.move_boundary(*walls(t))
             st = d.step()
+            t += st.h
             its.append(st.iterations)
             itv.append(st.iterations_v)
             ms.append(st.ms_total)
@@ -243,12 +278,14 @@ def learned_ablation(local, steps: int, counts=(64, 64, 64)):
         w = slice(steps // 2, steps)
         rec = {"pressure_iterations": round(float(np.mean(its[w])), 2),
                "divergence_iterations": round(float(np.mean(itv[w])), 2),
-               "ms_per_step": round(float(np.mean(ms[w])), 4), "status_bits": int(bits)}
+               "ms_per_step": round(float(np.mean(ms[w])), 4), "status_bits": int(bits),
+               "simulated_s": round(t, 4)}
         if mode == "learned":
-            rec.update(trainings=int(d.get_param("mlp_trainings")),
-                       kept_pressure=int(d.get_param("learned_kept_p")),
-                       solves_pressure=int(d.get_param("learned_solves_p")),
+            solves = int(d.get_param("learned_solves_p"))
+            kept = int(d.get_param("learned_kept_p"))
+            rec.update(trainings=int(d.get_param("mlp_trainings")), kept_pressure=kept, solves_pressure=solves,
                        kept_divergence=int(d.get_param("learned_kept_v")),
+                       fallback_rate_pressure=round(1 - kept / solves, 4) if solves else None,
                        damping=d.get_param("warm_start_damping"))
         out[mode] = rec
         d.close()
@@ -362,7 +399,7 @@ def run_ours(args, world, rank, local):
 
     ablation = None
     if rank == 0 and world == 1 and args.ablation_steps > 0:
-        ablation = learned_ablation(local, args.ablation_steps)
+        ablation = learned_ablation(local, args.ablation_steps, args.ablation_workload)
 
     if rank == 0:
         line = {
@@ -407,12 +444,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ablation-steps", type=int, default=300,
                     help="steps per mode of the plain vs learned warm-start comparison (0: skip)")
+    ap.add_argument("--ablation-workload", choices=ABLATION_WORKLOADS, default="column_64")
+    ap.add_argument("--ablation-only", action="store_true",
+                    help="print only the plain vs learned comparison as one JSON line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = setup_dist()
     try:
-        if args.impl == "reference":
+        if args.ablation_only:
+            if rank == 0:
+                print(json.dumps({"learned_warm_start": learned_ablation(local, args.ablation_steps,
+                                                                         args.ablation_workload)}), flush=True)
+        elif args.impl == "reference":
             run_reference_arm(args, world, rank)
         else:
             run_ours(args, world, rank, local)

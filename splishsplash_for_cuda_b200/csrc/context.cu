@@ -134,6 +134,7 @@ public:
     Real *kappaW = nullptr, *kappaVW = nullptr, *kappaP = nullptr, *kappaVP = nullptr;
     Vec4<Real>* velP = nullptr;
     Real *resid = nullptr, *residV = nullptr;
+    Real *dadvP = nullptr, *kcP = nullptr, *rawP = nullptr;  // plain candidate of the dual init pass
     float *features = nullptr, *pred = nullptr, *tx = nullptr, *tt = nullptr;
     MlpDev mlp{};
     MlpScales h_scales{};
@@ -208,7 +209,7 @@ public:
         DF_TRY(dalloc(&sb.vals_a, nmax));
         DF_TRY(dalloc(&sb.vals_b, nmax));
         DF_TRY(dalloc(&sb.workspace, radix_sort_workspace_words(nmax, 4)));
-        DF_TRY(dalloc(&partials, 2 * ((size_t)grid_for(nmax) + 1)));  // two sums per block at most
+        DF_TRY(dalloc(&partials, 4 * ((size_t)grid_for(nmax) + 1)));  // two pairs of sums per block at most
         DF_TRY(dalloc(&cfl_partials, grid_for(nmax) + 1));
         DF_TRY(dalloc(&ctl, 4));
         DF_TRY(dalloc(&status, 4));
@@ -248,6 +249,7 @@ public:
             f(kappaT[b]); f(kappaVT[b]);
         }
         f(kappaW); f(kappaVW); f(kappaP); f(kappaVP); f(velP); f(resid); f(residV); f(features); f(pred); f(tx);
+        f(dadvP); f(kcP); f(rawP);
         f(tt);
         f(mlp.params); f(mlp.adam_m); f(mlp.adam_v); f(mlp.grad); f(mlp.partials);
         f(mlp.w1_bf16); f(mlp.w2_bf16); f(mlp.w3_bf16); f(mlp.scales); f(mlp.loss);
@@ -351,6 +353,9 @@ public:
         hs.pred = pred;
         hs.kappaT = kappaT[cur];
         hs.kappaVT = kappaVT[cur];
+        hs.dadvP = dadvP;
+        hs.kcP = kcP;
+        hs.rawP = rawP;
         hs.kappaW = kappaW;
         hs.kappaVW = kappaVW;
         hs.kappaP = kappaP;
@@ -891,18 +896,16 @@ public:
             if (use) launch_mlp_forward(mlp, features, n, pred, stream);
             launch_warm_values<Real>(ds, n, 0, use, damping, stream);
             launches += use ? 3 : 2;
-            if (use && probe) {  // plain candidate: velocities into velP, initial residual into ctl[3]
+            if (use && probe) {  // both candidates per pass, then the selection
                 DF_CUDA(cudaMemsetAsync(&ctl[3].ticket, 0, sizeof(uint32_t), stream));
-                launch_divergence_warm_jacobi<Real>(ds, n, kappaVP, velP, stream);
-                launch_probe_residual<Real>(ds, n, 0, velP, stream);
+                launch_warm_dual<Real>(ds, n, 0, false, stream, boundary_forces);
+                launch_residual_dual<Real>(ds, n, 0, eta, kMinItersV, max_iter, stream);
+                launch_select_candidate<Real>(ds, n, 0, stream);
+                launches += 3;
+            } else {
+                launch_divergence_warm_jacobi<Real>(ds, n, kappaVW, nullptr, stream, boundary_forces);
+                launch_divergence_residual<Real>(ds, n, true, eta, kMinItersV, max_iter, 0, false, stream, true);
                 launches += 2;
-            }
-            launch_divergence_warm_jacobi<Real>(ds, n, kappaVW, nullptr, stream, boundary_forces);
-            launch_divergence_residual<Real>(ds, n, true, eta, kMinItersV, max_iter, 0, false, stream, true);
-            launches += 2;
-            if (use && probe) {
-                launch_fallback_residual<Real>(ds, n, 0, eta, kMinItersV, max_iter, stream);
-                launches += 1;
             }
             if (use && !probe) forced_warm |= 1u;
             if (use) ++solves_v;
@@ -928,16 +931,14 @@ public:
             launches += 1;
             if (use && probe) {
                 DF_CUDA(cudaMemsetAsync(&ctl[3].ticket, 0, sizeof(uint32_t), stream));
-                launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, kappaP, velP, stream);
-                launch_probe_residual<Real>(ds, n, 1, velP, stream);
+                launch_warm_dual<Real>(ds, n, 1, fused_vel, stream, boundary_forces);
+                launch_residual_dual<Real>(ds, n, 1, eta, kMinItersP, max_iter, stream);
+                launch_select_candidate<Real>(ds, n, 1, stream);
+                launches += 3;
+            } else {
+                launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, kappaW, nullptr, stream, boundary_forces);
+                launch_pressure_residual<Real>(ds, n, true, eta, kMinItersP, max_iter, 0, false, stream, true);
                 launches += 2;
-            }
-            launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, kappaW, nullptr, stream, boundary_forces);
-            launch_pressure_residual<Real>(ds, n, true, eta, kMinItersP, max_iter, 0, false, stream, true);
-            launches += 2;
-            if (use && probe) {
-                launch_fallback_residual<Real>(ds, n, 1, eta, kMinItersP, max_iter, stream);
-                launches += 1;
             }
             if (use && !probe) forced_warm |= 2u;
             if (use) ++solves_p;
@@ -1177,6 +1178,9 @@ public:
                 DF_TRY(dalloc(&velP, Nc));
                 DF_TRY(dalloc(&resid, Nc));
                 DF_TRY(dalloc(&residV, Nc));
+                DF_TRY(dalloc(&dadvP, Nc));
+                DF_TRY(dalloc(&kcP, Nc));
+                DF_TRY(dalloc(&rawP, Nc));
                 DF_TRY(dalloc(&features, (size_t)Nc * kMlpIn));
                 DF_TRY(dalloc(&pred, (size_t)Nc * kMlpOut));
             }

@@ -49,6 +49,9 @@ template <class Real> struct DevState {
     Vec4<Real>* velP;      // velocities after the plain candidate's warm-start pass (probe)
     Real* resid;           // unclamped density residual of the last pressure pass (null: not kept)
     Real* residV;          // unclamped divergence residual of the last divergence pass (null: not kept)
+    Real* dadvP;           // plain candidate's clamped init residual (both candidates in one pass)
+    Real* kcP;             // plain candidate's Jacobi coefficient
+    Real* rawP;            // plain candidate's unclamped init residual
     const float* out_scale;  // 2 floats: scales of the network outputs
 };
 
@@ -120,6 +123,17 @@ void launch_pressure_warm_jacobi(const DevState<Real>* d, uint32_t n, bool fused
 template <class Real>
 void launch_pressure_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
                               cudaGraphConditionalHandle h, bool use_handle, cudaStream_t s, bool keep = false);
+// Both warm-start candidates in one pass (which = 0 divergence, 1 pressure): the plain candidate
+// (kappaVP / kappaP) into velP, the learned one (kappaVW / kappaW) into vel; then their init residuals
+// in one pass (learned into the solver's arrays and ctl[0 or 1], plain into dadvP / kcP / rawP and
+// ctl[3]); then the selection, which installs the plain candidate if the learned one's sum |r| is
+// larger. Replaces the probe + warm-start + init + fallback sequence with three launches.
+template <class Real>
+void launch_warm_dual(const DevState<Real>* d, uint32_t n, int which, bool fused_vel, cudaStream_t s, bool forces);
+template <class Real>
+void launch_residual_dual(const DevState<Real>* d, uint32_t n, int which, double eta, int min_it, int max_it,
+                          cudaStream_t s);
+template <class Real> void launch_select_candidate(const DevState<Real>* d, uint32_t n, int which, cudaStream_t s);
 // Fallback init pass of the learned warm start (which = 0 divergence, 1 pressure): if the plain
 // candidate's probed residual (ctl[3]) is below the learned candidate's init residual, installs the
 // plain candidate and redoes the init pass; otherwise records the learned one as kept (status[2]).

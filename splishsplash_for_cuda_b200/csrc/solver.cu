@@ -185,6 +185,49 @@ __device__ __forceinline__ Real velocity_divergence(const DevState<Real>* __rest
     return s.value();
 }
 
+// velocity_divergence for two velocity fields in one pass over the neighbours (positions and
+// indices loaded once); each sum is accumulated exactly as velocity_divergence would.
+template <class Real>
+__device__ __forceinline__ void velocity_divergence2(const DevState<Real>* __restrict__ ds, const StepParams<Real>& p,
+                                                     uint32_t i, const Vec4<Real>& xi, const Vec4<Real>& via,
+                                                     const Vec4<Real>& vib, uint32_t nf, uint32_t nb,
+                                                     const Vec4<Real>* __restrict__ vela,
+                                                     const Vec4<Real>* __restrict__ velb, Real& outa, Real& outb) {
+    const Vec4<Real>* __restrict__ pos = ds->pos;
+    const uint32_t* __restrict__ nbr = ds->nbr;
+    const uint32_t stride = p.nbr_stride;
+    const Cubic<Real> K = p.kern;
+    KSum<Real> sa, sb;
+    Vec4<Real> xj[kGatherBatch], va[kGatherBatch], vb[kGatherBatch];
+    visit_neighbors<kGatherBatch>(
+        nbr, stride, i, 0, nf, i,
+        [&](int u, uint32_t j) {
+            xj[u] = ld4<Real>(pos + j);
+            va[u] = ld4<Real>(vela + j);
+            vb[u] = ld4<Real>(velb + j);
+        },
+        [&](int u) {
+            Real gx, gy, gz;
+            K.gradW(xi.x - xj[u].x, xi.y - xj[u].y, xi.z - xj[u].z, gx, gy, gz);
+            sa.add(xj[u].w * ((via.x - va[u].x) * gx + (via.y - va[u].y) * gy + (via.z - va[u].z) * gz));
+            sb.add(xj[u].w * ((vib.x - vb[u].x) * gx + (vib.y - vb[u].y) * gy + (vib.z - vb[u].z) * gz));
+        });
+    if (nb) {
+        const bool moving = p.boundary_moving != 0;
+        BNbr<Real> b[kGatherBatch];
+        visit_neighbors<kGatherBatch>(
+            nbr, stride, i, nf, nf + nb, 0u, [&](int u, uint32_t j) { load_bnbr(b[u], ds->bpos, ds->bvel, j, moving); },
+            [&](int u) {
+                Real gx, gy, gz;
+                K.gradW(xi.x - b[u].x.x, xi.y - b[u].x.y, xi.z - b[u].x.z, gx, gy, gz);
+                sa.add(b[u].x.w * ((via.x - b[u].vx) * gx + (via.y - b[u].vy) * gy + (via.z - b[u].vz) * gz));
+                sb.add(b[u].x.w * ((vib.x - b[u].vx) * gx + (vib.y - b[u].vy) * gy + (vib.z - b[u].vz) * gz));
+            });
+    }
+    outa = sa.value();
+    outb = sb.value();
+}
+
 // Jacobi velocity correction: sum over fluid neighbours of (k_i + k_j) m_j grad W_ij where
 // |k_i + k_j| > eps, plus (when |k_i| > eps) k_i sum over boundary neighbours of psi_b grad W_ib.
 // kof(j) returns k_j (a load, possibly transformed). With boundary forces on (kForces, and at run
@@ -237,6 +280,78 @@ __device__ __forceinline__ void jacobi_sum(const DevState<Real>* __restrict__ ds
                     atomicAdd(fb, f * gx);
                     atomicAdd(fb + 1, f * gy);
                     atomicAdd(fb + 2, f * gz);
+                }
+            });
+    }
+}
+
+// Two warm-start candidates in one pass over the neighbours: the same sums as jacobi_sum for the
+// coefficients ka / kb (the plain and the learned candidate), each accumulated exactly as a
+// single-candidate pass would (the gradient is shared). Boundary forces, when on, follow candidate b
+// (the one applied in place).
+template <class Real, bool kForces = false, class KOfA, class KOfB>
+__device__ __forceinline__ void jacobi_sum2(const DevState<Real>* __restrict__ ds, const StepParams<Real>& p,
+                                            uint32_t i, const Vec4<Real>& xi, Real kia, Real kib, uint32_t nf,
+                                            uint32_t nb, KOfA&& kofa, KOfB&& kofb, KSum3<Real>& acca,
+                                            KSum3<Real>& accb) {
+    const Vec4<Real>* __restrict__ pos = ds->pos;
+    const uint32_t* __restrict__ nbr = ds->nbr;
+    const uint32_t stride = p.nbr_stride;
+    const Cubic<Real> K = p.kern;
+    Vec4<Real> xj[kGatherBatch];
+    Real kja[kGatherBatch], kjb[kGatherBatch];
+    visit_neighbors<kGatherBatch>(
+        nbr, stride, i, 0, nf, i,
+        [&](int u, uint32_t j) {
+            xj[u] = ld4<Real>(pos + j);
+            kja[u] = kofa(j);
+            kjb[u] = kofb(j);
+        },
+        [&](int u) {
+            const Real ksa = kia + kja[u], ksb = kib + kjb[u];
+            const bool ea = above_eps(ksa), eb = above_eps(ksb);
+            if (ea || eb) {
+                Real gx, gy, gz;
+                K.gradW(xi.x - xj[u].x, xi.y - xj[u].y, xi.z - xj[u].z, gx, gy, gz);
+                if (ea) {
+                    const Real sc = ksa * xj[u].w;
+                    acca.add(sc * gx, sc * gy, sc * gz);
+                }
+                if (eb) {
+                    const Real sc = ksb * xj[u].w;
+                    accb.add(sc * gx, sc * gy, sc * gz);
+                }
+            }
+        });
+    const bool ba = above_eps(kia), bb = above_eps(kib);
+    if (nb && (ba || bb)) {
+        const Vec4<Real>* __restrict__ bpos = ds->bpos;
+        Real* __restrict__ bf = kForces ? ds->bforce : nullptr;
+        Vec4<Real> xb[kGatherBatch];
+        uint32_t jb[kGatherBatch];
+        visit_neighbors<kGatherBatch>(
+            nbr, stride, i, nf, nf + nb, 0u,
+            [&](int u, uint32_t j) {
+                xb[u] = ld4<Real>(bpos + j);
+                jb[u] = j;
+            },
+            [&](int u) {
+                Real gx, gy, gz;
+                K.gradW(xi.x - xb[u].x, xi.y - xb[u].y, xi.z - xb[u].z, gx, gy, gz);
+                if (ba) {
+                    const Real sc = kia * xb[u].w;
+                    acca.add(sc * gx, sc * gy, sc * gz);
+                }
+                if (bb) {
+                    const Real sc = kib * xb[u].w;
+                    accb.add(sc * gx, sc * gy, sc * gz);
+                    if (kForces && bf) {
+                        const Real f = -xi.w * sc;
+                        Real* fb = bf + 4 * (size_t)jb[u];
+                        atomicAdd(fb, f * gx);
+                        atomicAdd(fb + 1, f * gy);
+                        atomicAdd(fb + 2, f * gz);
+                    }
                 }
             });
     }
@@ -665,6 +780,175 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) probe_residual_kerne
     reduce_and_decide<1>(contrib, ds->partials, ds->ctl + 3, n, 0.0, 0, 1, 0, false);
 }
 
+// ---- both warm-start candidates in one pass (learned warm start with the plain fallback) ---------
+// Two sets of compensated sums need more registers than the single-candidate passes' 64.
+constexpr int kDualMinBlocks = 2;
+// The plain candidate (kappaVP / kappaP) goes to velP, the learned one (kappaVW / kappaW) to vel in
+// place; each velocity is the one the single-candidate pass would produce.
+template <class Real, bool kForces>
+__global__ void __launch_bounds__(kBlock, kDualMinBlocks) divergence_warm_dual_kernel(
+    const DevState<Real>* __restrict__ ds, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!(ds->densityAdv[i] > Real(0))) {
+        ds->velP[i] = ds->vel[i];
+        return;
+    }
+    const StepParams<Real>& p = ds->p;
+    const Real* __restrict__ ka = ds->kappaVP;
+    const Real* __restrict__ kb = ds->kappaVW;
+    const Vec4<Real> xi = ds->pos[i];
+    const uint32_t c = ds->counts[i];
+    KSum3<Real> acca, accb;
+    jacobi_sum2<Real, kForces>(ds, p, i, xi, ka[i], kb[i], fluid_count(c), boundary_count(c),
+                               [&](uint32_t j) { return ka[j]; }, [&](uint32_t j) { return kb[j]; }, acca, accb);
+    const Vec4<Real> v0 = ds->vel[i];
+    Vec4<Real> va = v0, vb = v0;
+    va.x += acca.x.value() * p.h;
+    va.y += acca.y.value() * p.h;
+    va.z += acca.z.value() * p.h;
+    vb.x += accb.x.value() * p.h;
+    vb.y += accb.y.value() * p.h;
+    vb.z += accb.z.value() * p.h;
+    ds->velP[i] = va;
+    ds->vel[i] = vb;
+}
+
+template <class Real, bool kFusedVel, bool kForces>
+__global__ void __launch_bounds__(kBlock, kDualMinBlocks) pressure_warm_dual_kernel(
+    const DevState<Real>* __restrict__ ds, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const StepParams<Real>& p = ds->p;
+    const Real* __restrict__ ka = ds->kappaP;
+    const Real* __restrict__ kb = ds->kappaW;
+    const Vec4<Real> xi = ds->pos[i];
+    const uint32_t c = ds->counts[i];
+    KSum3<Real> acca, accb;
+    jacobi_sum2<Real, kForces>(ds, p, i, xi, ka[i], kb[i], fluid_count(c), boundary_count(c),
+                               [&](uint32_t j) { return ka[j]; }, [&](uint32_t j) { return kb[j]; }, acca, accb);
+    Vec4<Real> v = ds->vel[i];
+    if (kFusedVel) {
+        const Vec4<Real> a = ds->acc[i];
+        v.x += p.h * a.x;
+        v.y += p.h * a.y;
+        v.z += p.h * a.z;
+    }
+    Vec4<Real> va = v, vb = v;
+    va.x += acca.x.value() * p.h_future;
+    va.y += acca.y.value() * p.h_future;
+    va.z += acca.z.value() * p.h_future;
+    vb.x += accb.x.value() * p.h_future;
+    vb.y += accb.y.value() * p.h_future;
+    vb.z += accb.z.value() * p.h_future;
+    ds->velP[i] = va;
+    ds->vel[i] = vb;
+}
+
+// Init residual pass of both candidates: the learned one (vel) writes the solver's arrays and
+// reduces into ctl[slot] (sum of the clamped residuals, aux = sum |r|); the plain one (velP) writes
+// dadvP / kcP / rawP and reduces into ctl[3] the same way (separate block partials).
+template <class Real>
+__global__ void __launch_bounds__(kBlock, kDualMinBlocks) divergence_residual_dual_kernel(
+    const DevState<Real>* __restrict__ ds, uint32_t n, double eta, int min_it, int max_it) {
+    eta = eta / ds->dtd[kDtH];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double cb = 0.0, ab = 0.0, ca = 0.0, aa = 0.0;
+    if (i < n) {
+        const StepParams<Real>& p = ds->p;
+        ds->kappaV[i] = Real(0);
+        const uint32_t c = ds->counts[i];
+        const uint32_t nf = fluid_count(c), nb = boundary_count(c);
+        uint32_t num = nf;
+        if (num < kMinNeighborsForDivergence) num += nb;
+        Real rb = Real(0), ra = Real(0);
+        if (num >= kMinNeighborsForDivergence) {
+            const Vec4<Real> xi = ds->pos[i];
+            velocity_divergence2<Real>(ds, p, i, xi, ds->velP[i], ds->vel[i], nf, nb, ds->velP, ds->vel, ra, rb);
+        }
+        const Real alpha = ds->factor[i];
+        const Real db = rmax<Real>(rb, Real(0)), da = rmax<Real>(ra, Real(0));
+        ds->residV[i] = rb;
+        ds->densityAdv[i] = db;
+        ds->kcoef[i] = db * alpha;
+        ds->rawP[i] = ra;
+        ds->dadvP[i] = da;
+        ds->kcP[i] = da * alpha;
+        cb = (double)db;
+        ab = fabs((double)rb);
+        ca = (double)da;
+        aa = fabs((double)ra);
+    }
+    reduce_and_decide<1, true>(cb, ds->partials, ds->ctl + 0, n, eta, min_it, max_it, 0, false, ab);
+    __syncthreads();
+    reduce_and_decide<1, true>(ca, ds->partials + 2 * gridDim.x, ds->ctl + 3, n, eta, min_it, max_it, 0, false, aa);
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock, kDualMinBlocks) pressure_residual_dual_kernel(
+    const DevState<Real>* __restrict__ ds, uint32_t n, double eta, int min_it, int max_it) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double cb = 0.0, ab = 0.0, ca = 0.0, aa = 0.0;
+    if (i < n) {
+        const StepParams<Real>& p = ds->p;
+        const Real alpha = ds->factor[i] * p.inv_h_future;
+        ds->factor[i] = alpha;
+        const Vec4<Real> xi = ds->pos[i];
+        const uint32_t c = ds->counts[i];
+        const uint32_t nf = fluid_count(c), nb = boundary_count(c);
+        Real sa, sb;
+        velocity_divergence2<Real>(ds, p, i, xi, ds->velP[i], ds->vel[i], nf, nb, ds->velP, ds->vel, sa, sb);
+        const Real rb = ds->density[i] + p.h_future * sb, ra = ds->density[i] + p.h_future * sa;
+        const Real db = rmax<Real>(rb, Real(0)), da = rmax<Real>(ra, Real(0));
+        const Real kb = db * alpha, ka = da * alpha;
+        ds->resid[i] = rb;
+        ds->densityAdv[i] = db;
+        ds->kcoef[i] = kb;
+        ds->kappa[i] = Real(0) + kb;
+        ds->rawP[i] = ra;
+        ds->dadvP[i] = da;
+        ds->kcP[i] = ka;
+        cb = (double)db;
+        ab = fabs((double)rb);
+        ca = (double)da;
+        aa = fabs((double)ra);
+    }
+    reduce_and_decide<1, true>(cb, ds->partials, ds->ctl + 1, n, eta, min_it, max_it, 0, false, ab);
+    __syncthreads();
+    reduce_and_decide<1, true>(ca, ds->partials + 2 * gridDim.x, ds->ctl + 3, n, eta, min_it, max_it, 0, false, aa);
+}
+
+// Keeps the learned candidate unless its sum |r| exceeds the plain one's (or is NaN); otherwise
+// installs the plain candidate's velocities, warm coefficients, residual arrays and init sum.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) select_candidate_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
+                                                                  int which) {
+    const int slot = which == 0 ? 0 : 1;
+    const double learned = ds->ctl[slot].aux, plain = ds->ctl[3].aux;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (learned <= plain) {
+        if (i == 0) atomicOr(ds->status + 2, which == 0 ? 1u : 2u);
+        return;
+    }
+    if (i == 0) {  // (aux, the decision's input, stays: every block reads it)
+        LoopCtl* c = ds->ctl + slot;
+        c->sum = ds->ctl[3].sum;
+        c->init_avg = n ? ds->ctl[3].sum / (double)n : 0.0;
+    }
+    if (i >= n) return;
+    ds->vel[i] = ds->velP[i];
+    ds->densityAdv[i] = ds->dadvP[i];
+    ds->kcoef[i] = ds->kcP[i];
+    if (which == 0) {
+        ds->kappaVW[i] = ds->kappaVP[i];
+        ds->residV[i] = ds->rawP[i];
+    } else {
+        ds->kappaW[i] = ds->kappaP[i];
+        ds->kappa[i] = Real(0) + ds->kcP[i];  // as the init pass forms it (kappa = 0 + k)
+        ds->resid[i] = ds->rawP[i];
+    }
+}
+
 // Warm-start candidates (see launch_warm_values). kappa <= 0 is pressure, so min() takes the larger
 // pressure. The learned candidate raises the reference warm start to `damping` times the predicted
 // needed coefficient (the previous step's needed value plus the network's correction, scaled by the
@@ -833,6 +1117,30 @@ void launch_pressure_residual(const DevState<Real>* d, uint32_t n, bool init, do
     k<<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
 }
 template <class Real>
+void launch_warm_dual(const DevState<Real>* d, uint32_t n, int which, bool fused_vel, cudaStream_t s, bool forces) {
+    if (!n) return;
+    if (which == 0) {
+        if (forces) divergence_warm_dual_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n);
+        else divergence_warm_dual_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    } else if (fused_vel) {
+        if (forces) pressure_warm_dual_kernel<Real, true, true><<<grid_for(n), kBlock, 0, s>>>(d, n);
+        else pressure_warm_dual_kernel<Real, true, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    } else {
+        if (forces) pressure_warm_dual_kernel<Real, false, true><<<grid_for(n), kBlock, 0, s>>>(d, n);
+        else pressure_warm_dual_kernel<Real, false, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    }
+}
+template <class Real>
+void launch_residual_dual(const DevState<Real>* d, uint32_t n, int which, double eta, int min_it, int max_it,
+                          cudaStream_t s) {
+    if (!n) return;
+    if (which == 0) divergence_residual_dual_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, eta, min_it, max_it);
+    else pressure_residual_dual_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, eta, min_it, max_it);
+}
+template <class Real> void launch_select_candidate(const DevState<Real>* d, uint32_t n, int which, cudaStream_t s) {
+    select_candidate_kernel<Real><<<grid_for(n ? n : 1), kBlock, 0, s>>>(d, n, which);
+}
+template <class Real>
 void launch_fallback_residual(const DevState<Real>* d, uint32_t n, int which, double eta, int min_it, int max_it,
                               cudaStream_t s) {
     const unsigned g = grid_for(n ? n : 1);
@@ -875,6 +1183,9 @@ template <class Real> void launch_cfl_reduce(const DevState<Real>* d, uint32_t n
     template void launch_pressure_residual<R>(const DevState<R>*, uint32_t, bool, double, int, int,                 \
                                               cudaGraphConditionalHandle, bool, cudaStream_t, bool);                 \
     template void launch_fallback_residual<R>(const DevState<R>*, uint32_t, int, double, int, int, cudaStream_t);   \
+    template void launch_warm_dual<R>(const DevState<R>*, uint32_t, int, bool, cudaStream_t, bool);                  \
+    template void launch_residual_dual<R>(const DevState<R>*, uint32_t, int, double, int, int, cudaStream_t);        \
+    template void launch_select_candidate<R>(const DevState<R>*, uint32_t, int, cudaStream_t);                       \
     template void launch_pressure_jacobi<R>(const DevState<R>*, uint32_t, cudaGraphConditionalHandle, bool,         \
                                             cudaStream_t, bool);                                                     \
     template void launch_update_pos<R>(const DevState<R>*, uint32_t, cudaStream_t);                                 \
