@@ -96,3 +96,20 @@ def test_invalid_arguments_rejected_before_cuda(cuda_lib):
     assert b"precision" in cuda_lib.dfsph_last_error(None)
     assert cuda_lib.dfsph_step(None, None) == _capi.DFSPH_E_INVALID
     assert cuda_lib.dfsph_destroy(None) == 0
+
+
+@pytest.mark.parametrize("field,value,needle", [("neighbor_capacity", 0, "neighbor_capacity"),
+                                                ("neighbor_capacity", 70000, "neighbor_capacity"),
+                                                ("fluid_capacity", 0, "fluid_capacity"),
+                                                ("particle_radius", 0.0, "particle_radius"),
+                                                ("time_step", -1.0, "time_step")])
+def test_create_rejects_bad_scene_before_touching_the_device(cuda_lib, field, value, needle):
+    """Scene validation runs before any CUDA call: bad values give DFSPH_E_INVALID and a message
+    naming the field, also on a machine without a GPU."""
+    s = _capi.DfsphScene()
+    cuda_lib.dfsph_scene_defaults(C.byref(s))
+    setattr(s, field, value)
+    ctx = C.c_void_p()
+    assert cuda_lib.dfsph_create(C.byref(s), C.byref(ctx)) == _capi.DFSPH_E_INVALID
+    assert not ctx.value
+    assert needle in cuda_lib.dfsph_last_error(None).decode()
