@@ -376,17 +376,22 @@ public:
     // (DFSPH_c_arrays_structure.cpp:1050-1098): offset = -(floor(min / H) - 5).
     int set_grid(const float mn[3], const float mx[3]) {
         const float H = (float)(4.0 * sc.particle_radius);
-        for (int a = 0; a < 3; ++a) {
-            bb_lo[a] = mn[a];  // initGridOffset keeps the box as boundingBoxMin / Max
-            bb_hi[a] = mx[a];
+        int o[3], dm[3];
+        for (int a = 0; a < 3; ++a) {  // validated first: a rejected box leaves the grid unchanged
             DF_CHECK(std::isfinite(mn[a]) && std::isfinite(mx[a]) && mx[a] >= mn[a], DFSPH_E_INVALID,
                      "invalid grid bounding box");
             const int fmin = (int)std::floor(mn[a] / H);
             const int fmax = (int)std::floor(mx[a] / H);
-            off[a] = -(fmin - 5);
-            dim[a] = fmax + off[a] + 6;
-            DF_CHECK(dim[a] <= 1024, DFSPH_E_INVALID,
+            o[a] = -(fmin - 5);
+            dm[a] = fmax + o[a] + 6;
+            DF_CHECK(dm[a] <= 1024, DFSPH_E_INVALID,
                      "domain too large: more than 1024 cells of size 4r along one axis");
+        }
+        for (int a = 0; a < 3; ++a) {
+            off[a] = o[a];
+            dim[a] = dm[a];
+            bb_lo[a] = mn[a];  // initGridOffset keeps the box as boundingBoxMin / Max
+            bb_hi[a] = mx[a];
         }
         return alloc_grid();
     }

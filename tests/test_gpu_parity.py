@@ -304,9 +304,9 @@ def test_particles_outside_domain_box_removed_like_reference():
 
 
 def test_limits_are_errors_not_faults():
-    """Inputs past the context's limits return DFSPH_E_INVALID with a message: a domain wider than
-    1024 cells of 4r, more fluid than fluid_capacity, a download into a too-small buffer; the context
-    stays usable afterwards."""
+    """Inputs past the context's limits return DFSPH_E_INVALID with a message and change nothing: a
+    domain wider than 1024 cells of 4r, more fluid than fluid_capacity, a download into a too-small
+    buffer."""
     import ctypes as C
 
     s = synthetic_scene(1, counts=(6, 6, 6))
@@ -320,9 +320,11 @@ def test_limits_are_errors_not_faults():
     assert b"fluid_capacity" in lib.dfsph_last_error(d._ctx)
     small = np.zeros(3, np.float32)
     assert lib.dfsph_download(d._ctx, 0, 0, small.ctypes.data, 3, 0) == _capi.DFSPH_E_INVALID
-    d.reset()
-    st = d.step()
+    # nothing was changed by the rejected calls: the run continues as if they had not been made
+    ref = DFSPHCUDA(s)
+    st, sr = d.step(), ref.step()
     assert st.status == 0 and st.num_fluid == s.n_fluid
+    assert np.array_equal(d.positions(), ref.positions())
 
 
 def test_empty_and_single_particle_fluid():
