@@ -307,16 +307,16 @@ def test_limits_are_errors_not_faults():
     """Inputs past the context's limits return DFSPH_E_INVALID with a message and change nothing: a
     domain wider than 1024 cells of 4r, more fluid than fluid_capacity, a download into a too-small
     buffer."""
-    import ctypes as C
+    from splishsplash_for_cuda_b200.dfsph import _fptr
 
     s = synthetic_scene(1, counts=(6, 6, 6))
     d = DFSPHCUDA(s)
     lib = d._lib
     wide = np.array([[0.0, 0.0, 0.0], [1100 * 4 * s.config.particleRadius, 1.0, 1.0]], np.float32)
-    assert lib.dfsph_set_boundary(d._ctx, wide.ctypes.data, None, 2) == _capi.DFSPH_E_INVALID
+    assert lib.dfsph_set_boundary(d._ctx, _fptr(wide), None, 2) == _capi.DFSPH_E_INVALID
     assert b"domain too large" in lib.dfsph_last_error(d._ctx)
     more = np.zeros((s.n_fluid + 1, 3), np.float32)
-    assert lib.dfsph_upload_fluid(d._ctx, more.ctypes.data, None, None, s.n_fluid + 1) == _capi.DFSPH_E_INVALID
+    assert lib.dfsph_upload_fluid(d._ctx, _fptr(more), None, None, s.n_fluid + 1) == _capi.DFSPH_E_INVALID
     assert b"fluid_capacity" in lib.dfsph_last_error(d._ctx)
     small = np.zeros(3, np.float32)
     assert lib.dfsph_download(d._ctx, 0, 0, small.ctypes.data, 3, 0) == _capi.DFSPH_E_INVALID
