@@ -315,7 +315,8 @@ def run_ours(args, world, rank, local):
         """k steps, each bracketed by CUDA events on the solver's stream after a 256 MiB write that
         evicts L2. Steps are enqueued without host round trips (the step runs on the device, dt
         included); iterations come from the device counters. e2e: each step also uploads its inputs
-        from pinned host memory and reads positions and velocities back (which waits)."""
+        from pinned host memory and reads positions and velocities back (readDynamicData, which
+        waits)."""
         tot = 0.0
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
@@ -327,9 +328,8 @@ def run_ours(args, world, rank, local):
             if e2e:
                 d.update_fluid(host["x"], host["v"])
             d.step_async()
-            if e2e:
-                d.field("position", out=host["x"])
-                d.field("velocity", out=host["v"])
+            if e2e:  # DFSPHCData::readDynamicData: positions and velocities, one wait
+                d.m_data.readDynamicData(host["x"], host["v"])
             with torch.cuda.stream(stream):
                 ends[s].record(stream)
         torch.cuda.synchronize(local)

@@ -62,8 +62,7 @@ public:
         const size_t n = getFluidParticlesCount();
         pos.resize(3 * n);
         vel.resize(3 * n);
-        check(ctx_, dfsph_download(ctx_, DFSPH_F_POSITION, DFSPH_DTYPE_F32, pos.data(), pos.size(), DFSPH_ORDER_ID));
-        check(ctx_, dfsph_download(ctx_, DFSPH_F_VELOCITY, DFSPH_DTYPE_F32, vel.data(), vel.size(), DFSPH_ORDER_ID));
+        check(ctx_, dfsph_read_dynamic_data(ctx_, pos.data(), vel.data()));
     }
     void updateTimeStep(double h_future) { check(ctx_, dfsph_update_time_step(ctx_, h_future)); }
     void onSimulationStepEnd() { check(ctx_, dfsph_on_step_end(ctx_)); }

@@ -163,6 +163,10 @@ int dfsph_update_fluid(dfsph_ctx* ctx, const float* xyz, const float* vxyz);
  * fails with DFSPH_E_INVALID if it is too small. order: DFSPH_ORDER_ID or DFSPH_ORDER_SORTED. */
 int dfsph_download(dfsph_ctx* ctx, int field, int dtype, void* out, size_t n_elems, int order);
 
+/* DFSPHCData::readDynamicData (DFSPH_c_arrays_structure.cpp:1120-1150): positions and velocities
+ * (3 floats per particle each, particle-id order; either may be null) with a single wait. */
+int dfsph_read_dynamic_data(dfsph_ctx* ctx, float* xyz, float* vxyz);
+
 /* Neighbour lists of every fluid particle, in id space: counts[2*id] fluid, counts[2*id+1]
  * boundary; lists[id*cap + k] holds fluid neighbour ids first, then boundary indices (in the order
  * given to dfsph_set_boundary). cap is the row length of lists and must be >= neighbor_capacity. */

@@ -145,6 +145,7 @@ SIGNATURES = {
     "dfsph_load_snapshot": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int]),
     "dfsph_checkpoint_save": (C.c_int, [_P, C.c_char_p]),
     "dfsph_export_bgeo": (C.c_int, [_P, C.c_char_p]),
+    "dfsph_read_dynamic_data": (C.c_int, [_P, _P, _P]),
     "dfsph_body_wrench": (C.c_int, [_P, C.c_uint32, _P, _P, _P, _P]),
     "dfsph_check_particles_positions": (C.c_int, [_P, C.c_int, C.POINTER(C.c_uint32)]),
     "dfsph_open_boundary_init": (C.c_int, [_P, C.POINTER(Surface), C.POINTER(Surface), C.POINTER(Surface), _P,

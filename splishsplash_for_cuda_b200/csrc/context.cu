@@ -1469,6 +1469,22 @@ public:
     template <class T> static void put(std::ofstream& f, const T& v) { f.write(reinterpret_cast<const char*>(&v), sizeof(T)); }
     template <class T> static bool get(std::ifstream& f, T& v) { return (bool)f.read(reinterpret_cast<char*>(&v), sizeof(T)); }
 
+    // DFSPHCData::readDynamicData (DFSPH_c_arrays_structure.cpp:1120-1150): positions and velocities
+    // in id order with one wait (both packed, both copies queued, then one synchronisation).
+    int read_dynamic_data(float* xyz, float* vxyz) {
+        DF_CHECK(xyz || vxyz, DFSPH_E_INVALID, "null outputs");
+        if (!n) return DFSPH_OK;
+        float* px = (float*)dl;
+        float* pv = px + 3 * (size_t)n;
+        if (xyz) launch_pack_field<Real, float>((const Real*)pos[cur], 4, 3, id[cur], n, px, stream);
+        if (vxyz) launch_pack_field<Real, float>((const Real*)vel[cur], 4, 3, id[cur], n, pv, stream);
+        if (xyz) DF_CUDA(cudaMemcpyAsync(xyz, px, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        if (vxyz) DF_CUDA(cudaMemcpyAsync(vxyz, pv, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        launches += (xyz ? 1 : 0) + (vxyz ? 1 : 0);
+        return DFSPH_OK;
+    }
+
     // Force and torque of the fluid on boundary bodies (readDynamicObjectsData + the rigid-body
     // solver's sum over the body's particles): bodies are ranges of the boundary upload order.
     double* wrench_buf = nullptr;  // 6 Bc doubles (positions, forces in upload order) + bodies
@@ -2188,6 +2204,9 @@ int dfsph_time_kernel(dfsph_ctx* ctx, int kernel, int reps, double* ms_per_launc
 int dfsph_save_snapshot(dfsph_ctx* ctx, const char* dir, int what) { DFSPH_DISPATCH(ctx, save_snapshot(dir, what)); }
 int dfsph_checkpoint_save(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, save_checkpoint(path)); }
 int dfsph_export_bgeo(dfsph_ctx* ctx, const char* path) { DFSPH_DISPATCH(ctx, export_bgeo(path)); }
+int dfsph_read_dynamic_data(dfsph_ctx* ctx, float* xyz, float* vxyz) {
+    DFSPH_DISPATCH(ctx, read_dynamic_data(xyz, vxyz));
+}
 int dfsph_body_wrench(dfsph_ctx* ctx, uint32_t n_bodies, const uint32_t* first, const uint32_t* count,
                       const double* centers, double* force_torque) {
     DFSPH_DISPATCH(ctx, body_wrench(n_bodies, first, count, centers, force_torque));

@@ -65,9 +65,17 @@ class DFSPHData:
         self._o._call(self._o._lib.dfsph_num_fluid(self._o._ctx, C.byref(n)))
         return int(n.value)
 
-    def readDynamicData(self):
-        """Positions and velocities in particle-id order (DFSPHCData::readDynamicData)."""
-        return self._o.positions(), self._o.velocities()
+    def readDynamicData(self, out_positions: np.ndarray | None = None, out_velocities: np.ndarray | None = None):
+        """Positions and velocities (n, 3) float32 in particle-id order (DFSPHCData::readDynamicData),
+        read with one wait; the outputs may be given (C-contiguous float32, e.g. pinned memory)."""
+        n = self.getFluidParticlesCount()
+        x = np.empty((n, 3), np.float32) if out_positions is None else out_positions
+        v = np.empty((n, 3), np.float32) if out_velocities is None else out_velocities
+        for a in (x, v):
+            if a.dtype != np.float32 or not a.flags.c_contiguous or a.size != 3 * n:
+                raise ValueError("outputs must be C-contiguous float32 arrays of n x 3")
+        self._o._call(self._o._lib.dfsph_read_dynamic_data(self._o._ctx, x.ctypes.data, v.ctypes.data))
+        return x, v
 
     @property
     def h(self) -> float:

@@ -303,6 +303,19 @@ def test_particles_outside_domain_box_removed_like_reference():
     assert b.step().num_fluid == s.n_fluid
 
 
+def test_read_dynamic_data_equals_field_downloads():
+    s = synthetic_scene(1, counts=(10, 10, 10))
+    d = DFSPHCUDA(s)
+    for _ in range(3):
+        d.step()
+    x, v = d.m_data.readDynamicData()
+    assert np.array_equal(x, d.positions()) and np.array_equal(v, d.velocities())
+    xo = np.zeros_like(x)
+    vo = np.zeros_like(v)
+    d.m_data.readDynamicData(xo, vo)
+    assert np.array_equal(xo, x) and np.array_equal(vo, v)
+
+
 def test_limits_are_errors_not_faults():
     """Inputs past the context's limits return DFSPH_E_INVALID with a message and change nothing: a
     domain wider than 1024 cells of 4r, more fluid than fluid_capacity, a download into a too-small
