@@ -7,6 +7,7 @@
 // positions are first packed into upload order, so each body is a contiguous range, then one block
 // per body reduces its range in a fixed order (deterministic, FP64).
 #include "bodies.cuh"
+#include "dfsph_common.cuh"
 
 namespace dfsph {
 
@@ -20,6 +21,7 @@ __global__ void __launch_bounds__(kWrenchThreads) body_wrench_kernel(const doubl
                                                                      const uint32_t* __restrict__ count,
                                                                      const double* __restrict__ centers,
                                                                      double* __restrict__ out) {
+    DFSPH_PDL_ENTER;
     __shared__ double acc[6][kWrenchThreads];
     const uint32_t b = blockIdx.x;
     const double cx = centers[3 * b], cy = centers[3 * b + 1], cz = centers[3 * b + 2];
@@ -52,7 +54,7 @@ __global__ void __launch_bounds__(kWrenchThreads) body_wrench_kernel(const doubl
 
 void launch_body_wrench(const double* pos, const double* force, const uint32_t* first, const uint32_t* count,
                         const double* centers, uint32_t n_bodies, double* out, cudaStream_t s) {
-    if (n_bodies) body_wrench_kernel<<<n_bodies, kWrenchThreads, 0, s>>>(pos, force, first, count, centers, out);
+    if (n_bodies) launch_pdl(body_wrench_kernel, n_bodies, kWrenchThreads, 0, s, pos, force, first, count, centers, out);
 }
 
 }  // namespace dfsph

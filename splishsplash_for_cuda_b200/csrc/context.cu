@@ -836,6 +836,7 @@ public:
         DF_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         DF_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        g_pdl_off = true;  // the loop body is a graph: its kernel edges need no programmatic launch
         if (kind == 0) {
             launch_divergence_jacobi<Real>(ds, n, handle, true, stream, boundary_forces);
             launch_divergence_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream, g_loop_keep);
@@ -843,6 +844,7 @@ public:
             launch_pressure_jacobi<Real>(ds, n, handle, true, stream, boundary_forces);
             launch_pressure_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream, g_loop_keep);
         }
+        g_pdl_off = false;
         cudaGraph_t captured = nullptr;
         DF_CUDA(cudaStreamEndCapture(stream, &captured));
         cudaGraphExec_t exec = nullptr;

@@ -6,11 +6,45 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include "../../include/dfsph_c.h"
 
 namespace dfsph {
+
+// ---- programmatic dependent launch -------------------------------------------------------------
+// The kernels of a time step are launched with programmatic stream serialisation: the next kernel's
+// launch is processed while the previous grid's last blocks finish, instead of after the grid has
+// completed (about 2 us per kernel boundary on B200). Every kernel starts with pdl_wait(), which
+// blocks until the previous grid has completed and its writes are visible, so the ordering is the
+// plain stream order; each block signals its dependents when it ends (PdlTrigger). The attribute is
+// left off while a loop body is captured into a graph (g_pdl_off).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+struct PdlTrigger {
+    __device__ __forceinline__ ~PdlTrigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+};
+#define DFSPH_PDL_ENTER \
+    pdl_wait();         \
+    const PdlTrigger pdl_trigger_guard_ {}
+
+inline thread_local bool g_pdl_off = false;
+
+template <class... KArgs, class... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = g_pdl_off ? 0 : 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // ---------------------------------------------------------------------------------------------
 // Launch shapes. One thread per particle for the gathers (SPlisHSPlasH/DFSPH/DFSPH_define_cuda.h:6

@@ -15,6 +15,7 @@ __global__ void __launch_bounds__(kBlock) unpack_fluid_kernel(const float* __res
                                                               uint32_t n, Vec4<Real>* __restrict__ pos,
                                                               Vec4<Real>* __restrict__ vel, Real* __restrict__ kappa,
                                                               Real* __restrict__ kappaV, uint32_t* __restrict__ id) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Vec4<Real> x, v;
@@ -40,6 +41,7 @@ __global__ void __launch_bounds__(kBlock) update_fluid_kernel(const float* __res
                                                               const uint32_t* __restrict__ id,
                                                               Vec4<Real>* __restrict__ pos,
                                                               Vec4<Real>* __restrict__ vel) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t t = id[i];
@@ -61,6 +63,7 @@ __global__ void __launch_bounds__(kBlock) unpack_boundary_kernel(const float* __
                                                                  const float* __restrict__ psi, uint32_t n,
                                                                  Vec4<Real>* __restrict__ bpos,
                                                                  Vec4<Real>* __restrict__ bvel) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Vec4<Real> x;
@@ -81,6 +84,7 @@ __global__ void __launch_bounds__(kBlock) reorder_boundary_kernel(const uint32_t
                                                                   Vec4<Real>* __restrict__ bpos_out,
                                                                   Vec4<Real>* __restrict__ bvel_out,
                                                                   uint32_t* __restrict__ bid_out) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t j = perm[i];
@@ -97,6 +101,7 @@ __global__ void __launch_bounds__(kBlock) move_boundary_kernel(const float* __re
                                                                const uint32_t* __restrict__ bid,
                                                                Vec4<Real>* __restrict__ bpos,
                                                                Vec4<Real>* __restrict__ bvel) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t t = bid[i];
@@ -119,6 +124,7 @@ template <class Real, class Out>
 __global__ void __launch_bounds__(kBlock) pack_field_kernel(const Real* __restrict__ src, int src_stride, int comps,
                                                             const uint32_t* __restrict__ id, uint32_t n,
                                                             Out* __restrict__ dst) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t t = id ? id[i] : i;
@@ -128,6 +134,7 @@ __global__ void __launch_bounds__(kBlock) pack_field_kernel(const Real* __restri
 __global__ void __launch_bounds__(kBlock) pack_u32_kernel(const uint32_t* __restrict__ src, int comps,
                                                           const uint32_t* __restrict__ id, uint32_t n,
                                                           uint32_t* __restrict__ dst) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t t = id ? id[i] : i;
@@ -137,6 +144,7 @@ __global__ void __launch_bounds__(kBlock) pack_u32_kernel(const uint32_t* __rest
 __global__ void __launch_bounds__(kBlock) unpack_counts_kernel(const uint32_t* __restrict__ counts,
                                                                const uint32_t* __restrict__ id, uint32_t n,
                                                                uint32_t* __restrict__ dst) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t t = id ? id[i] : i;
@@ -147,6 +155,7 @@ __global__ void __launch_bounds__(kBlock) unpack_counts_kernel(const uint32_t* _
 // Publishes a new device state block. The block travels as a kernel parameter, so the update is
 // ordered with the surrounding work on the stream and never reads host memory asynchronously.
 template <class Real> __global__ void set_state_kernel(DevState<Real>* __restrict__ dst, DevState<Real> v) {
+    DFSPH_PDL_ENTER;
     const StepParams<Real>& o = dst->p;  // dt fields stay as the device has them
     v.p.h = o.h;
     v.p.h_future = o.h_future;
@@ -158,6 +167,7 @@ template <class Real> __global__ void set_state_kernel(DevState<Real>* __restric
 }
 
 template <class Real> __global__ void dt_kernel(DevState<Real>* __restrict__ ds, int op, DtArgs a) {
+    DFSPH_PDL_ENTER;
     double* t = ds->dtd;
     StepParams<Real>& p = ds->p;
     if (op == 0) {
@@ -193,51 +203,51 @@ template <class Real> __global__ void dt_kernel(DevState<Real>* __restrict__ ds,
 }  // namespace
 
 template <class Real> void launch_set_state(DevState<Real>* dst, const DevState<Real>& v, cudaStream_t s) {
-    set_state_kernel<Real><<<1, 1, 0, s>>>(dst, v);
+    launch_pdl(set_state_kernel<Real>, 1, 1, 0, s, dst, v);
 }
 template <class Real> void launch_dt(DevState<Real>* d, int op, const DtArgs& a, cudaStream_t s) {
-    dt_kernel<Real><<<1, 1, 0, s>>>(d, op, a);
+    launch_pdl(dt_kernel<Real>, 1, 1, 0, s, d, op, a);
 }
 
 template <class Real>
 void launch_unpack_fluid(const float* xyz, const float* vxyz, const float* mass, float default_mass, uint32_t n,
                          Vec4<Real>* pos, Vec4<Real>* vel, Real* kappa, Real* kappaV, uint32_t* id, cudaStream_t s) {
     if (n)
-        unpack_fluid_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(xyz, vxyz, mass, default_mass, n, pos, vel, kappa,
+        launch_pdl(unpack_fluid_kernel<Real>, grid_for(n), kBlock, 0, s, xyz, vxyz, mass, default_mass, n, pos, vel, kappa,
                                                                  kappaV, id);
 }
 template <class Real>
 void launch_update_fluid(const float* xyz, const float* vxyz, uint32_t n, const uint32_t* id, Vec4<Real>* pos,
                          Vec4<Real>* vel, cudaStream_t s) {
-    if (n) update_fluid_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(xyz, vxyz, n, id, pos, vel);
+    if (n) launch_pdl(update_fluid_kernel<Real>, grid_for(n), kBlock, 0, s, xyz, vxyz, n, id, pos, vel);
 }
 template <class Real>
 void launch_unpack_boundary(const float* xyz, const float* psi, uint32_t n, Vec4<Real>* bpos, Vec4<Real>* bvel,
                             cudaStream_t s) {
-    if (n) unpack_boundary_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(xyz, psi, n, bpos, bvel);
+    if (n) launch_pdl(unpack_boundary_kernel<Real>, grid_for(n), kBlock, 0, s, xyz, psi, n, bpos, bvel);
 }
 template <class Real>
 void launch_reorder_boundary(const uint32_t* perm, uint32_t n, const Vec4<Real>* bpos_in, const Vec4<Real>* bvel_in,
                              Vec4<Real>* bpos_out, Vec4<Real>* bvel_out, uint32_t* bid_out, cudaStream_t s) {
     if (n)
-        reorder_boundary_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(perm, n, bpos_in, bvel_in, bpos_out, bvel_out,
+        launch_pdl(reorder_boundary_kernel<Real>, grid_for(n), kBlock, 0, s, perm, n, bpos_in, bvel_in, bpos_out, bvel_out,
                                                                      bid_out);
 }
 template <class Real>
 void launch_move_boundary(const float* xyz, const float* vxyz, uint32_t n, const uint32_t* bid, Vec4<Real>* bpos,
                           Vec4<Real>* bvel, cudaStream_t s) {
-    if (n) move_boundary_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(xyz, vxyz, n, bid, bpos, bvel);
+    if (n) launch_pdl(move_boundary_kernel<Real>, grid_for(n), kBlock, 0, s, xyz, vxyz, n, bid, bpos, bvel);
 }
 template <class Real, class Out>
 void launch_pack_field(const Real* src, int src_stride, int comps, const uint32_t* id, uint32_t n, Out* dst,
                        cudaStream_t s) {
-    if (n) pack_field_kernel<Real, Out><<<grid_for(n), kBlock, 0, s>>>(src, src_stride, comps, id, n, dst);
+    if (n) launch_pdl(pack_field_kernel<Real, Out>, grid_for(n), kBlock, 0, s, src, src_stride, comps, id, n, dst);
 }
 void launch_pack_u32(const uint32_t* src, int comps, const uint32_t* id, uint32_t n, uint32_t* dst, cudaStream_t s) {
-    if (n) pack_u32_kernel<<<grid_for(n), kBlock, 0, s>>>(src, comps, id, n, dst);
+    if (n) launch_pdl(pack_u32_kernel, grid_for(n), kBlock, 0, s, src, comps, id, n, dst);
 }
 void launch_unpack_counts(const uint32_t* counts, const uint32_t* id, uint32_t n, uint32_t* dst, cudaStream_t s) {
-    if (n) unpack_counts_kernel<<<grid_for(n), kBlock, 0, s>>>(counts, id, n, dst);
+    if (n) launch_pdl(unpack_counts_kernel, grid_for(n), kBlock, 0, s, counts, id, n, dst);
 }
 
 #define DFSPH_INSTANTIATE_IO(R)                                                                                      \

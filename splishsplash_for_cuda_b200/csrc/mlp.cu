@@ -3,6 +3,7 @@
 #include <cuda_bf16.h>
 
 #include "mlp.cuh"
+#include "dfsph_common.cuh"
 
 namespace dfsph {
 
@@ -38,6 +39,7 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(const uint16_t* __rest
                                                           const MlpScales* __restrict__ scales,
                                                           const float* __restrict__ features, uint32_t n,
                                                           float* __restrict__ pred) {
+    DFSPH_PDL_ENTER;
     __shared__ uint32_t sW1[kMlpHidden * kS1];
     __shared__ uint32_t sW2[kMlpHidden * kS2];
     __shared__ uint32_t sW3[8 * kS2];
@@ -115,6 +117,7 @@ __global__ void __launch_bounds__(128) mlp_forward_kernel(const uint16_t* __rest
 
 __global__ void mlp_pack_kernel(const float* __restrict__ params, uint16_t* __restrict__ w1b,
                                 uint16_t* __restrict__ w2b, uint16_t* __restrict__ w3b) {
+    DFSPH_PDL_ENTER;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     auto bf = [](float v) {
         __nv_bfloat16 b = __float2bfloat16_rn(v);
@@ -141,6 +144,7 @@ __global__ void __launch_bounds__(kTrainBlock) mlp_train_partials_kernel(const f
                                                                         const float* __restrict__ x,
                                                                         const float* __restrict__ tgt, uint32_t batch,
                                                                         float* __restrict__ partials) {
+    DFSPH_PDL_ENTER;
     extern __shared__ float sm[];
     float* W1 = sm;                                 // [64][8]
     float* B1 = W1 + kMlpHidden * kMlpIn;           // [64]
@@ -229,6 +233,7 @@ __global__ void mlp_reduce_adam_kernel(float* __restrict__ params, float* __rest
                                        float* __restrict__ grad, const float* __restrict__ partials, int blocks,
                                        uint32_t batch, int adam, float lr, float beta1, float beta2, float eps,
                                        int step, double* __restrict__ loss) {
+    DFSPH_PDL_ENTER;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p > kMlpParams) return;
     double acc = 0.0;
@@ -261,6 +266,7 @@ __device__ __forceinline__ float hash_uniform(uint32_t seed, uint32_t i) {
 
 __global__ void mlp_init_kernel(float* __restrict__ params, float* __restrict__ m, float* __restrict__ v,
                                 uint32_t seed) {
+    DFSPH_PDL_ENTER;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= kMlpParams) return;
     float val = 0.0f;
@@ -286,11 +292,11 @@ void launch_mlp_forward(const MlpDev& m, const float* features, uint32_t n, floa
     if (!n) return;
     uint32_t tiles = (n + 63) / 64;
     if (tiles > 148 * 16) tiles = 148 * 16;
-    mlp_forward_kernel<<<tiles, 128, 0, s>>>(m.w1_bf16, m.w2_bf16, m.w3_bf16, m.params, m.scales, features, n, pred);
+    launch_pdl(mlp_forward_kernel, tiles, 128, 0, s, m.w1_bf16, m.w2_bf16, m.w3_bf16, m.params, m.scales, features, n, pred);
 }
 
 void launch_mlp_pack(const MlpDev& m, cudaStream_t s) {
-    mlp_pack_kernel<<<(kMlpHidden * kMlpHidden + 255) / 256, 256, 0, s>>>(m.params, m.w1_bf16, m.w2_bf16, m.w3_bf16);
+    launch_pdl(mlp_pack_kernel, (kMlpHidden * kMlpHidden + 255) / 256, 256, 0, s, m.params, m.w1_bf16, m.w2_bf16, m.w3_bf16);
 }
 
 static size_t train_smem_bytes() {
@@ -305,14 +311,14 @@ void launch_mlp_train_step(const MlpDev& m, const float* x, const float* t, uint
     const size_t smem = train_smem_bytes();
     // per device and idempotent: set on every call (the caller may switch devices)
     cudaFuncSetAttribute(mlp_train_partials_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    mlp_train_partials_kernel<<<blocks, kTrainBlock, smem, s>>>(m.params, m.scales, x, t, batch, m.partials);
-    mlp_reduce_adam_kernel<<<(kMlpParams + 1 + 255) / 256, 256, 0, s>>>(m.params, m.adam_m, m.adam_v, m.grad,
+    launch_pdl(mlp_train_partials_kernel, blocks, kTrainBlock, smem, s, m.params, m.scales, x, t, batch, m.partials);
+    launch_pdl(mlp_reduce_adam_kernel, (kMlpParams + 1 + 255) / 256, 256, 0, s, m.params, m.adam_m, m.adam_v, m.grad,
                                                                         m.partials, blocks, batch, adam, lr, beta1,
                                                                         beta2, eps, step, m.loss);
 }
 
 void launch_mlp_init(const MlpDev& m, uint32_t seed, cudaStream_t s) {
-    mlp_init_kernel<<<(kMlpParams + 255) / 256, 256, 0, s>>>(m.params, m.adam_m, m.adam_v, seed);
+    launch_pdl(mlp_init_kernel, (kMlpParams + 255) / 256, 256, 0, s, m.params, m.adam_m, m.adam_v, seed);
 }
 
 }  // namespace dfsph

@@ -33,6 +33,7 @@ template <class Real>
 __global__ void __launch_bounds__(kBlock) cell_keys_kernel(const Vec4<Real>* __restrict__ pos, uint32_t n,
                                                            StepParams<Real> p, uint32_t* __restrict__ keys,
                                                            uint32_t* __restrict__ status) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const Vec4<Real> x = pos[i];
@@ -54,6 +55,7 @@ __global__ void __launch_bounds__(kBlock) reorder_fluid_kernel(
     const Vec4<Real>* __restrict__ vel_in, const Real* __restrict__ kappa_in, const Real* __restrict__ kappaV_in,
     const uint32_t* __restrict__ id_in, Vec4<Real>* __restrict__ pos_out, Vec4<Real>* __restrict__ vel_out,
     Real* __restrict__ kappa_out, Real* __restrict__ kappaV_out, uint32_t* __restrict__ id_out) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t j = perm[i];
@@ -70,6 +72,7 @@ __global__ void __launch_bounds__(kBlock) reorder_pair_kernel(const uint32_t* __
                                                               const Real* __restrict__ a_in,
                                                               const Real* __restrict__ b_in, Real* __restrict__ a_out,
                                                               Real* __restrict__ b_out) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t j = perm[i];
@@ -81,6 +84,7 @@ __global__ void __launch_bounds__(kBlock) reorder_pair_kernel(const uint32_t* __
 // Cell start/end from run boundaries of the sorted keys (replaces the dense histogram scan).
 __global__ void __launch_bounds__(kBlock) cell_bounds_kernel(const uint32_t* __restrict__ keys, uint32_t n, int dim_x,
                                                              int dim_y, int dim_z, uint2* __restrict__ table) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t k = keys[i];
@@ -99,6 +103,7 @@ template <class Real>
 __global__ void __launch_bounds__(kBlock) build_neighbors_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                  const uint2* __restrict__ ftab,
                                                                  const uint2* __restrict__ btab) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
@@ -177,6 +182,7 @@ __global__ void __launch_bounds__(kBlock) boundary_psi_kernel(const Vec4<Real>* 
                                                               Vec4<Real>* __restrict__ bpos_out, uint32_t nb,
                                                               StepParams<Real> p, const uint2* __restrict__ btab,
                                                               uint32_t* __restrict__ status) {
+    DFSPH_PDL_ENTER;
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
     const Vec4<Real> xb = bpos_in[b];
@@ -230,6 +236,7 @@ template <class Real>
 __global__ void __launch_bounds__(kBlock) scatter_by_id_kernel(const uint32_t* __restrict__ id, uint32_t n,
                                                                const Real* __restrict__ src, int comps,
                                                                int src_stride, Real* __restrict__ dst) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t t = id[i];
@@ -241,39 +248,39 @@ __global__ void __launch_bounds__(kBlock) scatter_by_id_kernel(const uint32_t* _
 template <class Real>
 void launch_cell_keys(const Vec4<Real>* pos, uint32_t n, const StepParams<Real>& p, uint32_t* keys, uint32_t* status,
                       cudaStream_t s) {
-    if (n) cell_keys_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(pos, n, p, keys, status);
+    if (n) launch_pdl(cell_keys_kernel<Real>, grid_for(n), kBlock, 0, s, pos, n, p, keys, status);
 }
 template <class Real>
 void launch_reorder_fluid(const uint32_t* perm, uint32_t n, const Vec4<Real>* pos_in, const Vec4<Real>* vel_in,
                           const Real* kappa_in, const Real* kappaV_in, const uint32_t* id_in, Vec4<Real>* pos_out,
                           Vec4<Real>* vel_out, Real* kappa_out, Real* kappaV_out, uint32_t* id_out, cudaStream_t s) {
     if (n)
-        reorder_fluid_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(perm, n, pos_in, vel_in, kappa_in, kappaV_in, id_in,
+        launch_pdl(reorder_fluid_kernel<Real>, grid_for(n), kBlock, 0, s, perm, n, pos_in, vel_in, kappa_in, kappaV_in, id_in,
                                                                   pos_out, vel_out, kappa_out, kappaV_out, id_out);
 }
 template <class Real>
 void launch_reorder_pair(const uint32_t* perm, uint32_t n, const Real* a_in, const Real* b_in, Real* a_out,
                          Real* b_out, cudaStream_t s) {
-    if (n) reorder_pair_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(perm, n, a_in, b_in, a_out, b_out);
+    if (n) launch_pdl(reorder_pair_kernel<Real>, grid_for(n), kBlock, 0, s, perm, n, a_in, b_in, a_out, b_out);
 }
 void launch_cell_bounds(const uint32_t* sorted_keys, uint32_t n, int dim_x, int dim_y, int dim_z, uint2* table,
                         cudaStream_t s) {
-    if (n) cell_bounds_kernel<<<grid_for(n), kBlock, 0, s>>>(sorted_keys, n, dim_x, dim_y, dim_z, table);
+    if (n) launch_pdl(cell_bounds_kernel, grid_for(n), kBlock, 0, s, sorted_keys, n, dim_x, dim_y, dim_z, table);
 }
 template <class Real>
 void launch_build_neighbors(const DevState<Real>* d, uint32_t n, const uint2* fluid_table, const uint2* boundary_table,
                             cudaStream_t s) {
-    if (n) build_neighbors_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, fluid_table, boundary_table);
+    if (n) launch_pdl(build_neighbors_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, fluid_table, boundary_table);
 }
 template <class Real>
 void launch_boundary_psi(const Vec4<Real>* bpos_in, Vec4<Real>* bpos_out, uint32_t nb, const StepParams<Real>& p,
                          const uint2* boundary_table, uint32_t* status, cudaStream_t s) {
-    if (nb) boundary_psi_kernel<Real><<<grid_for(nb), kBlock, 0, s>>>(bpos_in, bpos_out, nb, p, boundary_table, status);
+    if (nb) launch_pdl(boundary_psi_kernel<Real>, grid_for(nb), kBlock, 0, s, bpos_in, bpos_out, nb, p, boundary_table, status);
 }
 template <class Real>
 void launch_scatter_by_id(const uint32_t* id, uint32_t n, const Real* src, int comps, int src_stride, Real* dst,
                           cudaStream_t s) {
-    if (n) scatter_by_id_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(id, n, src, comps, src_stride, dst);
+    if (n) launch_pdl(scatter_by_id_kernel<Real>, grid_for(n), kBlock, 0, s, id, n, src, comps, src_stride, dst);
 }
 
 #define DFSPH_INSTANTIATE_NEIGHBORS(R)                                                                               \

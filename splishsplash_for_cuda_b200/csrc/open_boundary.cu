@@ -162,6 +162,7 @@ __device__ uint32_t block_exclusive(uint32_t v, uint32_t* total) {
 
 __global__ void __launch_bounds__(kScanThreads) scan_tile_sums_kernel(const uint32_t* __restrict__ in, uint32_t n,
                                                                       uint32_t* __restrict__ sums) {
+    DFSPH_PDL_ENTER;
     __shared__ uint32_t tot;
     const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
     uint32_t s = 0;
@@ -175,6 +176,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_tile_sums_kernel(const uint
 // One block: exclusive scan of the tile sums in place, the grand total to *total.
 __global__ void __launch_bounds__(kScanThreads) scan_sums_kernel(uint32_t* __restrict__ sums, uint32_t tiles,
                                                                  uint32_t* __restrict__ total) {
+    DFSPH_PDL_ENTER;
     __shared__ uint32_t tot;
     uint32_t carry = 0;
     for (uint32_t base = 0; base < tiles; base += kScanTile) {
@@ -201,6 +203,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_sums_kernel(uint32_t* __res
 __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const uint32_t* __restrict__ in, uint32_t n,
                                                                   const uint32_t* __restrict__ sums,
                                                                   uint32_t* __restrict__ out) {
+    DFSPH_PDL_ENTER;
     __shared__ uint32_t tot;
     const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems], s = 0;
@@ -223,6 +226,7 @@ template <class Real>
 __global__ void __launch_bounds__(kBlock) select_kernel(const float4* __restrict__ samples, uint32_t ns,
                                                         dfsph_surface interior, dfsph_surface surface,
                                                         StepParams<Real> p, uint32_t* __restrict__ keep) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ns) return;
     const float4 s = samples[i];
@@ -238,12 +242,14 @@ __global__ void __launch_bounds__(kBlock) compact_samples_kernel(const float4* _
                                                                  const uint32_t* __restrict__ keep,
                                                                  const uint32_t* __restrict__ rank, uint32_t ns,
                                                                  float4* __restrict__ out) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < ns && keep[i]) out[rank[i]] = samples[i];
 }
 
 __global__ void __launch_bounds__(kBlock) shift_samples_kernel(float4* __restrict__ samples, uint32_t ns, float dx,
                                                                float dy, float dz) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ns) return;
     float4 s = samples[i];
@@ -260,6 +266,7 @@ __global__ void __launch_bounds__(kBlock) inflow_kernel(const DevState<Real>* __
                                                         dfsph_surface boundary, const uint2* __restrict__ ftab,
                                                         const uint2* __restrict__ btab, uint32_t* __restrict__ flag,
                                                         float4* __restrict__ vout) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ns) return;
     const StepParams<Real>& p = ds->p;
@@ -345,6 +352,7 @@ __global__ void __launch_bounds__(kBlock) append_kernel(const float4* __restrict
                                                         Vec4<Real>* __restrict__ vel, Real* __restrict__ kappa,
                                                         Real* __restrict__ kappaV, uint32_t* __restrict__ id,
                                                         Real* __restrict__ kT, Real* __restrict__ kVT) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ns || !flag[i]) return;
     const uint32_t r = rank[i];
@@ -373,6 +381,7 @@ template <class Real>
 __global__ void __launch_bounds__(kBlock) outflow_tag_kernel(const Vec4<Real>* __restrict__ pos, uint32_t n,
                                                              dfsph_surface interior, dfsph_surface surface,
                                                              uint32_t* __restrict__ alive) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const Vec4<Real> x = pos[i];
@@ -388,6 +397,7 @@ __global__ void __launch_bounds__(kBlock) compact_fluid_kernel(
     const Real* __restrict__ kVT_in, Vec4<Real>* __restrict__ pos_out, Vec4<Real>* __restrict__ vel_out,
     Real* __restrict__ kappa_out, Real* __restrict__ kappaV_out, uint32_t* __restrict__ id_out,
     Real* __restrict__ kT_out, Real* __restrict__ kVT_out) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !alive[i]) return;
     const uint32_t k = dst[i];
@@ -406,6 +416,7 @@ template <class Real>
 __global__ void __launch_bounds__(kBlock) box_tag_kernel(const Vec4<Real>* __restrict__ pos, uint32_t n, float lo_x,
                                                          float lo_y, float lo_z, float hi_x, float hi_y, float hi_z,
                                                          uint32_t* __restrict__ alive, uint32_t* __restrict__ count) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const Vec4<Real> x = pos[i];
@@ -418,6 +429,7 @@ __global__ void __launch_bounds__(kBlock) box_tag_kernel(const Vec4<Real>* __res
 __global__ void __launch_bounds__(kBlock) alive_by_id_kernel(const uint32_t* __restrict__ id,
                                                              const uint32_t* __restrict__ alive, uint32_t n,
                                                              uint32_t* __restrict__ out) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t k = id[i];
@@ -426,6 +438,7 @@ __global__ void __launch_bounds__(kBlock) alive_by_id_kernel(const uint32_t* __r
 
 __global__ void __launch_bounds__(kBlock) renumber_kernel(uint32_t* __restrict__ id, uint32_t n,
                                                           const uint32_t* __restrict__ new_id) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) id[i] = new_id[id[i]];
 }
@@ -439,29 +452,29 @@ void exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t*
         return;
     }
     const uint32_t tiles = (n + kScanTile - 1) / kScanTile;
-    scan_tile_sums_kernel<<<tiles, kScanThreads, 0, s>>>(in, n, scratch);
-    scan_sums_kernel<<<1, kScanThreads, 0, s>>>(scratch, tiles, total);
-    scan_apply_kernel<<<tiles, kScanThreads, 0, s>>>(in, n, scratch, out);
+    launch_pdl(scan_tile_sums_kernel, tiles, kScanThreads, 0, s, in, n, scratch);
+    launch_pdl(scan_sums_kernel, 1, kScanThreads, 0, s, scratch, tiles, total);
+    launch_pdl(scan_apply_kernel, tiles, kScanThreads, 0, s, in, n, scratch, out);
 }
 
 template <class Real>
 void launch_open_boundary_select(const float4* samples, uint32_t ns, dfsph_surface interior, dfsph_surface fluid_surface,
                                  const StepParams<Real>& p, uint32_t* keep, cudaStream_t s) {
-    if (ns) select_kernel<Real><<<grid_for(ns), kBlock, 0, s>>>(samples, ns, interior, fluid_surface, p, keep);
+    if (ns) launch_pdl(select_kernel<Real>, grid_for(ns), kBlock, 0, s, samples, ns, interior, fluid_surface, p, keep);
 }
 void launch_compact_samples(const float4* samples, const uint32_t* keep, const uint32_t* rank, uint32_t ns,
                             float4* out, cudaStream_t s) {
-    if (ns) compact_samples_kernel<<<grid_for(ns), kBlock, 0, s>>>(samples, keep, rank, ns, out);
+    if (ns) launch_pdl(compact_samples_kernel, grid_for(ns), kBlock, 0, s, samples, keep, rank, ns, out);
 }
 void launch_shift_samples(float4* samples, uint32_t ns, float dx, float dy, float dz, cudaStream_t s) {
-    if (ns) shift_samples_kernel<<<grid_for(ns), kBlock, 0, s>>>(samples, ns, dx, dy, dz);
+    if (ns) launch_pdl(shift_samples_kernel, grid_for(ns), kBlock, 0, s, samples, ns, dx, dy, dz);
 }
 template <class Real>
 void launch_inflow(const DevState<Real>* d, const float4* samples, uint32_t ns, float allowed_distance,
                    float allowed_density, Real mass, dfsph_surface boundary, const uint2* fluid_table,
                    const uint2* boundary_table, uint32_t* flag, float4* vel, cudaStream_t s) {
     if (ns)
-        inflow_kernel<Real><<<grid_for(ns), kBlock, 0, s>>>(d, samples, ns, allowed_distance, allowed_density, mass,
+        launch_pdl(inflow_kernel<Real>, grid_for(ns), kBlock, 0, s, d, samples, ns, allowed_distance, allowed_density, mass,
                                                             boundary, fluid_table, boundary_table, flag, vel);
 }
 template <class Real>
@@ -469,13 +482,13 @@ void launch_append_inflow(const float4* samples, const float4* svel, const uint3
                           uint32_t ns, uint32_t n, uint32_t capacity, Real mass, Vec4<Real>* pos, Vec4<Real>* vel,
                           Real* kappa, Real* kappaV, uint32_t* id, Real* kappaT, Real* kappaVT, cudaStream_t s) {
     if (ns && n < capacity)
-        append_kernel<Real><<<grid_for(ns), kBlock, 0, s>>>(samples, svel, flag, rank, ns, n, capacity, mass, pos, vel,
+        launch_pdl(append_kernel<Real>, grid_for(ns), kBlock, 0, s, samples, svel, flag, rank, ns, n, capacity, mass, pos, vel,
                                                             kappa, kappaV, id, kappaT, kappaVT);
 }
 template <class Real>
 void launch_outflow_tag(const Vec4<Real>* pos, uint32_t n, dfsph_surface interior, dfsph_surface fluid_surface,
                         uint32_t* alive, cudaStream_t s) {
-    if (n) outflow_tag_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(pos, n, interior, fluid_surface, alive);
+    if (n) launch_pdl(outflow_tag_kernel<Real>, grid_for(n), kBlock, 0, s, pos, n, interior, fluid_surface, alive);
 }
 template <class Real>
 void launch_compact_fluid(const uint32_t* alive, const uint32_t* dst, uint32_t n, const Vec4<Real>* pos_in,
@@ -484,7 +497,7 @@ void launch_compact_fluid(const uint32_t* alive, const uint32_t* dst, uint32_t n
                           Real* kappa_out, Real* kappaV_out, uint32_t* id_out, Real* kT_out, Real* kVT_out,
                           cudaStream_t s) {
     if (n)
-        compact_fluid_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(alive, dst, n, pos_in, vel_in, kappa_in, kappaV_in,
+        launch_pdl(compact_fluid_kernel<Real>, grid_for(n), kBlock, 0, s, alive, dst, n, pos_in, vel_in, kappa_in, kappaV_in,
                                                                   id_in, kT_in, kVT_in, pos_out, vel_out, kappa_out,
                                                                   kappaV_out, id_out, kT_out, kVT_out);
 }
@@ -492,14 +505,14 @@ template <class Real>
 void launch_box_tag(const Vec4<Real>* pos, uint32_t n, const float lo[3], const float hi[3], uint32_t* alive,
                     uint32_t* count, cudaStream_t s) {
     if (n)
-        box_tag_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(pos, n, lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], alive,
+        launch_pdl(box_tag_kernel<Real>, grid_for(n), kBlock, 0, s, pos, n, lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], alive,
                                                             count);
 }
 void launch_alive_by_id(const uint32_t* id, const uint32_t* alive, uint32_t n, uint32_t* alive_by_id, cudaStream_t s) {
-    if (n) alive_by_id_kernel<<<grid_for(n), kBlock, 0, s>>>(id, alive, n, alive_by_id);
+    if (n) launch_pdl(alive_by_id_kernel, grid_for(n), kBlock, 0, s, id, alive, n, alive_by_id);
 }
 void launch_renumber_ids(uint32_t* id, uint32_t n, const uint32_t* new_id, cudaStream_t s) {
-    if (n) renumber_kernel<<<grid_for(n), kBlock, 0, s>>>(id, n, new_id);
+    if (n) launch_pdl(renumber_kernel, grid_for(n), kBlock, 0, s, id, n, new_id);
 }
 
 #define DFSPH_INSTANTIATE_OPEN_BOUNDARY(R)                                                                        \

@@ -365,6 +365,7 @@ __device__ __forceinline__ void jacobi_sum2(const DevState<Real>* __restrict__ d
 template <class Real>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                                bool warm_v, bool features) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
@@ -438,6 +439,7 @@ template <class Real, bool kForces>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
                                                                         uint32_t n, const Real* __restrict__ kw,
                                                                         Vec4<Real>* __restrict__ vout) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (!(ds->densityAdv[i] > Real(0))) {
@@ -485,6 +487,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_residual_
                                                                      double eta, int min_it, int max_it,
                                                                      cudaGraphConditionalHandle handle,
                                                                      bool use_handle) {
+    DFSPH_PDL_ENTER;
     // The init passes receive the tolerance per unit of h (maxErrorV 0.01 rho0 / h): h is the
     // device's (the dt history lives on the device).
     if (kMode != kLoop) eta = eta / ds->dtd[kDtH];
@@ -527,6 +530,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_residual_
 template <class Real, bool kForces>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_jacobi_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                    cudaGraphConditionalHandle handle, bool use_handle) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     // Inside a graph while-loop the condition is cleared here and only set again by the last block
     // of the residual pass that follows: a loop can end early but can never spin without bound.
@@ -552,6 +556,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) divergence_jacobi_ke
 // neighbours. With kCfl the block maximum of |v + a h|^2 is stored for the CFL time step.
 template <class Real, bool kCfl>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) viscosity_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     float vmag = 0.0f;
     if (i < n) {
@@ -607,6 +612,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) viscosity_kernel(con
 // Maximum of the CFL partials into ctl[2].sum (one block).
 template <class Real>
 __global__ void __launch_bounds__(kBlock) cfl_reduce_kernel(const DevState<Real>* __restrict__ ds, uint32_t n_blocks) {
+    DFSPH_PDL_ENTER;
     float m = 0.0f;
     for (uint32_t b = threadIdx.x; b < n_blocks; b += blockDim.x) m = fmaxf(m, ds->cfl_partials[b]);
     __shared__ float wmax[kWarpsPerBlock];
@@ -625,6 +631,7 @@ __global__ void __launch_bounds__(kBlock) cfl_reduce_kernel(const DevState<Real>
 // on the fly by the pressure warm start, which is the only reader of the scaled value.
 template <class Real>
 __global__ void __launch_bounds__(kBlock) update_vel_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const Real h = ds->p.h;
@@ -644,6 +651,7 @@ template <class Real, bool kFusedVel, bool kForces>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_warm_jacobi_kernel(const DevState<Real>* __restrict__ ds,
                                                                       uint32_t n, const Real* __restrict__ kw,
                                                                       Vec4<Real>* __restrict__ vout) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
@@ -680,6 +688,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_residual_ke
                                                                    double eta, int min_it, int max_it,
                                                                    cudaGraphConditionalHandle handle,
                                                                    bool use_handle) {
+    DFSPH_PDL_ENTER;
     if (kMode == kFallback && !take_fallback(ds, 1, 2u)) return;  // uniform over the grid
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const Vec4<Real>* __restrict__ vel = kMode == kFallback ? ds->velP : ds->vel;
@@ -721,6 +730,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_residual_ke
 template <class Real, bool kForces>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_jacobi_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                  cudaGraphConditionalHandle handle, bool use_handle) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (use_handle && i == 0) cudaGraphSetConditional(handle, 0u);  // see divergence_jacobi_kernel
     if (i >= n) return;
@@ -742,6 +752,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) pressure_jacobi_kern
 // x_i += h v_i (DFSPH_update_pos_kernel with border damping and wave cancelling off).
 template <class Real>
 __global__ void __launch_bounds__(kBlock) update_pos_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const Real h = ds->p.h;
@@ -761,6 +772,7 @@ template <class Real, int kWhich>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) probe_residual_kernel(const DevState<Real>* __restrict__ ds,
                                                                               uint32_t n,
                                                                               const Vec4<Real>* __restrict__ vel) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double contrib = 0.0;
     if (i < n) {
@@ -788,6 +800,7 @@ constexpr int kDualMinBlocks = 2;
 template <class Real, bool kForces>
 __global__ void __launch_bounds__(kBlock, kDualMinBlocks) divergence_warm_dual_kernel(
     const DevState<Real>* __restrict__ ds, uint32_t n) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (!(ds->densityAdv[i] > Real(0))) {
@@ -817,6 +830,7 @@ __global__ void __launch_bounds__(kBlock, kDualMinBlocks) divergence_warm_dual_k
 template <class Real, bool kFusedVel, bool kForces>
 __global__ void __launch_bounds__(kBlock, kDualMinBlocks) pressure_warm_dual_kernel(
     const DevState<Real>* __restrict__ ds, uint32_t n) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
@@ -851,6 +865,7 @@ __global__ void __launch_bounds__(kBlock, kDualMinBlocks) pressure_warm_dual_ker
 template <class Real>
 __global__ void __launch_bounds__(kBlock, kDualMinBlocks) divergence_residual_dual_kernel(
     const DevState<Real>* __restrict__ ds, uint32_t n, double eta, int min_it, int max_it) {
+    DFSPH_PDL_ENTER;
     eta = eta / ds->dtd[kDtH];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double cb = 0.0, ab = 0.0, ca = 0.0, aa = 0.0;
@@ -887,6 +902,7 @@ __global__ void __launch_bounds__(kBlock, kDualMinBlocks) divergence_residual_du
 template <class Real>
 __global__ void __launch_bounds__(kBlock, kDualMinBlocks) pressure_residual_dual_kernel(
     const DevState<Real>* __restrict__ ds, uint32_t n, double eta, int min_it, int max_it) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double cb = 0.0, ab = 0.0, ca = 0.0, aa = 0.0;
     if (i < n) {
@@ -923,6 +939,7 @@ __global__ void __launch_bounds__(kBlock, kDualMinBlocks) pressure_residual_dual
 template <class Real>
 __global__ void __launch_bounds__(kBlock) select_candidate_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                   int which) {
+    DFSPH_PDL_ENTER;
     const int slot = which == 0 ? 0 : 1;
     const double learned = ds->ctl[slot].aux, plain = ds->ctl[3].aux;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -960,6 +977,7 @@ __global__ void __launch_bounds__(kBlock) select_candidate_kernel(const DevState
 template <class Real>
 __global__ void __launch_bounds__(kBlock) warm_values_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                              int which, bool learned, Real damping) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const StepParams<Real>& p = ds->p;
@@ -1013,6 +1031,7 @@ __device__ __forceinline__ void needed_totals(const DevState<Real>* __restrict__
 template <class Real>
 __global__ void __launch_bounds__(kBlock) totals_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                         bool div_ran) {
+    DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Real kt, kvt;
@@ -1025,6 +1044,7 @@ template <class Real>
 __global__ void __launch_bounds__(kBlock) gather_training_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                  uint32_t batch, uint32_t offset, bool div_ran,
                                                                  float* __restrict__ x, float* __restrict__ t) {
+    DFSPH_PDL_ENTER;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= batch) return;
     const double r2 = ds->dtd[kDtRatio2UsedP], hr = ds->dtd[kDtRatioUsedV];  // dt ratios the warm starts used
@@ -1044,33 +1064,33 @@ __global__ void __launch_bounds__(kBlock) gather_training_kernel(const DevState<
 template <class Real>
 void launch_density_alpha(const DevState<Real>* d, uint32_t n, bool warm_v, bool features, cudaStream_t s) {
     if (!n) return;
-    density_alpha_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, warm_v && !features, features);
+    launch_pdl(density_alpha_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, warm_v && !features, features);
 }
 template <class Real>
 void launch_divergence_warm_jacobi(const DevState<Real>* d, uint32_t n, const Real* kw, Vec4<Real>* vout,
                                    cudaStream_t s, bool forces) {
     if (!n) return;
-    if (forces) divergence_warm_jacobi_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n, kw, vout);
-    else divergence_warm_jacobi_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n, kw, vout);
+    if (forces) launch_pdl(divergence_warm_jacobi_kernel<Real, true>, grid_for(n), kBlock, 0, s, d, n, kw, vout);
+    else launch_pdl(divergence_warm_jacobi_kernel<Real, false>, grid_for(n), kBlock, 0, s, d, n, kw, vout);
 }
 template <class Real>
 void launch_probe_residual(const DevState<Real>* d, uint32_t n, int which, const Vec4<Real>* vel, cudaStream_t s) {
     const unsigned g = grid_for(n ? n : 1);
-    if (which == 0) probe_residual_kernel<Real, 0><<<g, kBlock, 0, s>>>(d, n, vel);
-    else probe_residual_kernel<Real, 1><<<g, kBlock, 0, s>>>(d, n, vel);
+    if (which == 0) launch_pdl(probe_residual_kernel<Real, 0>, g, kBlock, 0, s, d, n, vel);
+    else launch_pdl(probe_residual_kernel<Real, 1>, g, kBlock, 0, s, d, n, vel);
 }
 template <class Real>
 void launch_warm_values(const DevState<Real>* d, uint32_t n, int which, bool learned, double damping,
                         cudaStream_t s) {
-    if (n) warm_values_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, which, learned, (Real)damping);
+    if (n) launch_pdl(warm_values_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, which, learned, (Real)damping);
 }
 template <class Real> void launch_totals(const DevState<Real>* d, uint32_t n, bool div_ran, cudaStream_t s) {
-    if (n) totals_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, div_ran);
+    if (n) launch_pdl(totals_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, div_ran);
 }
 template <class Real>
 void launch_gather_training(const DevState<Real>* d, uint32_t n, uint32_t batch, uint32_t offset, bool div_ran, float* x,
                             float* t, cudaStream_t s) {
-    if (n && batch) gather_training_kernel<Real><<<grid_for(batch), kBlock, 0, s>>>(d, n, batch, offset, div_ran, x, t);
+    if (n && batch) launch_pdl(gather_training_kernel<Real>, grid_for(batch), kBlock, 0, s, d, n, batch, offset, div_ran, x, t);
 }
 template <class Real>
 void launch_divergence_residual(const DevState<Real>* d, uint32_t n, bool init, double eta, int min_it, int max_it,
@@ -1078,22 +1098,22 @@ void launch_divergence_residual(const DevState<Real>* d, uint32_t n, bool init, 
     const unsigned g = grid_for(n ? n : 1);
     auto k = init ? (keep ? divergence_residual_kernel<Real, kInitPass, true> : divergence_residual_kernel<Real, kInitPass, false>)
                   : (keep ? divergence_residual_kernel<Real, kLoop, true> : divergence_residual_kernel<Real, kLoop, false>);
-    k<<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
+    launch_pdl(k, g, kBlock, 0, s, d, n, eta, min_it, max_it, h, use_handle);
 }
 template <class Real>
 void launch_divergence_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
                               cudaStream_t s, bool forces) {
     if (!n) return;
-    if (forces) divergence_jacobi_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
-    else divergence_jacobi_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
+    if (forces) launch_pdl(divergence_jacobi_kernel<Real, true>, grid_for(n), kBlock, 0, s, d, n, h, use_handle);
+    else launch_pdl(divergence_jacobi_kernel<Real, false>, grid_for(n), kBlock, 0, s, d, n, h, use_handle);
 }
 template <class Real> void launch_viscosity(const DevState<Real>* d, uint32_t n, bool cfl, cudaStream_t s) {
     if (!n) return;
-    if (cfl) viscosity_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n);
-    else viscosity_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    if (cfl) launch_pdl(viscosity_kernel<Real, true>, grid_for(n), kBlock, 0, s, d, n);
+    else launch_pdl(viscosity_kernel<Real, false>, grid_for(n), kBlock, 0, s, d, n);
 }
 template <class Real> void launch_update_vel(const DevState<Real>* d, uint32_t n, cudaStream_t s) {
-    if (n) update_vel_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    if (n) launch_pdl(update_vel_kernel<Real>, grid_for(n), kBlock, 0, s, d, n);
 }
 template <class Real>
 void launch_pressure_warm_jacobi(const DevState<Real>* d, uint32_t n, bool fused_vel, const Real* kw,
@@ -1101,11 +1121,11 @@ void launch_pressure_warm_jacobi(const DevState<Real>* d, uint32_t n, bool fused
     if (!n) return;
     const unsigned g = grid_for(n);
     if (forces) {
-        if (fused_vel) pressure_warm_jacobi_kernel<Real, true, true><<<g, kBlock, 0, s>>>(d, n, kw, vout);
-        else pressure_warm_jacobi_kernel<Real, false, true><<<g, kBlock, 0, s>>>(d, n, kw, vout);
+        if (fused_vel) launch_pdl(pressure_warm_jacobi_kernel<Real, true, true>, g, kBlock, 0, s, d, n, kw, vout);
+        else launch_pdl(pressure_warm_jacobi_kernel<Real, false, true>, g, kBlock, 0, s, d, n, kw, vout);
     } else {
-        if (fused_vel) pressure_warm_jacobi_kernel<Real, true, false><<<g, kBlock, 0, s>>>(d, n, kw, vout);
-        else pressure_warm_jacobi_kernel<Real, false, false><<<g, kBlock, 0, s>>>(d, n, kw, vout);
+        if (fused_vel) launch_pdl(pressure_warm_jacobi_kernel<Real, true, false>, g, kBlock, 0, s, d, n, kw, vout);
+        else launch_pdl(pressure_warm_jacobi_kernel<Real, false, false>, g, kBlock, 0, s, d, n, kw, vout);
     }
 }
 template <class Real>
@@ -1114,53 +1134,53 @@ void launch_pressure_residual(const DevState<Real>* d, uint32_t n, bool init, do
     const unsigned g = grid_for(n ? n : 1);
     auto k = init ? (keep ? pressure_residual_kernel<Real, kInitPass, true> : pressure_residual_kernel<Real, kInitPass, false>)
                   : (keep ? pressure_residual_kernel<Real, kLoop, true> : pressure_residual_kernel<Real, kLoop, false>);
-    k<<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, h, use_handle);
+    launch_pdl(k, g, kBlock, 0, s, d, n, eta, min_it, max_it, h, use_handle);
 }
 template <class Real>
 void launch_warm_dual(const DevState<Real>* d, uint32_t n, int which, bool fused_vel, cudaStream_t s, bool forces) {
     if (!n) return;
     if (which == 0) {
-        if (forces) divergence_warm_dual_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n);
-        else divergence_warm_dual_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+        if (forces) launch_pdl(divergence_warm_dual_kernel<Real, true>, grid_for(n), kBlock, 0, s, d, n);
+        else launch_pdl(divergence_warm_dual_kernel<Real, false>, grid_for(n), kBlock, 0, s, d, n);
     } else if (fused_vel) {
-        if (forces) pressure_warm_dual_kernel<Real, true, true><<<grid_for(n), kBlock, 0, s>>>(d, n);
-        else pressure_warm_dual_kernel<Real, true, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+        if (forces) launch_pdl(pressure_warm_dual_kernel<Real, true, true>, grid_for(n), kBlock, 0, s, d, n);
+        else launch_pdl(pressure_warm_dual_kernel<Real, true, false>, grid_for(n), kBlock, 0, s, d, n);
     } else {
-        if (forces) pressure_warm_dual_kernel<Real, false, true><<<grid_for(n), kBlock, 0, s>>>(d, n);
-        else pressure_warm_dual_kernel<Real, false, false><<<grid_for(n), kBlock, 0, s>>>(d, n);
+        if (forces) launch_pdl(pressure_warm_dual_kernel<Real, false, true>, grid_for(n), kBlock, 0, s, d, n);
+        else launch_pdl(pressure_warm_dual_kernel<Real, false, false>, grid_for(n), kBlock, 0, s, d, n);
     }
 }
 template <class Real>
 void launch_residual_dual(const DevState<Real>* d, uint32_t n, int which, double eta, int min_it, int max_it,
                           cudaStream_t s) {
     if (!n) return;
-    if (which == 0) divergence_residual_dual_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, eta, min_it, max_it);
-    else pressure_residual_dual_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n, eta, min_it, max_it);
+    if (which == 0) launch_pdl(divergence_residual_dual_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, eta, min_it, max_it);
+    else launch_pdl(pressure_residual_dual_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, eta, min_it, max_it);
 }
 template <class Real> void launch_select_candidate(const DevState<Real>* d, uint32_t n, int which, cudaStream_t s) {
-    select_candidate_kernel<Real><<<grid_for(n ? n : 1), kBlock, 0, s>>>(d, n, which);
+    launch_pdl(select_candidate_kernel<Real>, grid_for(n ? n : 1), kBlock, 0, s, d, n, which);
 }
 template <class Real>
 void launch_fallback_residual(const DevState<Real>* d, uint32_t n, int which, double eta, int min_it, int max_it,
                               cudaStream_t s) {
     const unsigned g = grid_for(n ? n : 1);
     if (which == 0)
-        divergence_residual_kernel<Real, kFallback, true><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, 0, false);
+        launch_pdl(divergence_residual_kernel<Real, kFallback, true>, g, kBlock, 0, s, d, n, eta, min_it, max_it, 0, false);
     else
-        pressure_residual_kernel<Real, kFallback, true><<<g, kBlock, 0, s>>>(d, n, eta, min_it, max_it, 0, false);
+        launch_pdl(pressure_residual_kernel<Real, kFallback, true>, g, kBlock, 0, s, d, n, eta, min_it, max_it, 0, false);
 }
 template <class Real>
 void launch_pressure_jacobi(const DevState<Real>* d, uint32_t n, cudaGraphConditionalHandle h, bool use_handle,
                             cudaStream_t s, bool forces) {
     if (!n) return;
-    if (forces) pressure_jacobi_kernel<Real, true><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
-    else pressure_jacobi_kernel<Real, false><<<grid_for(n), kBlock, 0, s>>>(d, n, h, use_handle);
+    if (forces) launch_pdl(pressure_jacobi_kernel<Real, true>, grid_for(n), kBlock, 0, s, d, n, h, use_handle);
+    else launch_pdl(pressure_jacobi_kernel<Real, false>, grid_for(n), kBlock, 0, s, d, n, h, use_handle);
 }
 template <class Real> void launch_update_pos(const DevState<Real>* d, uint32_t n, cudaStream_t s) {
-    if (n) update_pos_kernel<Real><<<grid_for(n), kBlock, 0, s>>>(d, n);
+    if (n) launch_pdl(update_pos_kernel<Real>, grid_for(n), kBlock, 0, s, d, n);
 }
 template <class Real> void launch_cfl_reduce(const DevState<Real>* d, uint32_t n_blocks, cudaStream_t s) {
-    cfl_reduce_kernel<Real><<<1, kBlock, 0, s>>>(d, n_blocks);
+    launch_pdl(cfl_reduce_kernel<Real>, 1, kBlock, 0, s, d, n_blocks);
 }
 
 #define DFSPH_INSTANTIATE_SOLVER(R)                                                                                  \

@@ -31,6 +31,7 @@ constexpr int kSpinLimit = 1 << 22;
 
 __global__ void __launch_bounds__(kSortThreads) histogram_kernel(const uint32_t* __restrict__ keys, uint32_t n,
                                                                  int passes, uint32_t* __restrict__ hist) {
+    DFSPH_PDL_ENTER;
     __shared__ uint32_t sh[4][256];
     for (int t = threadIdx.x; t < 4 * 256; t += blockDim.x) (&sh[0][0])[t] = 0;
     __syncthreads();
@@ -48,6 +49,7 @@ __global__ void __launch_bounds__(kSortThreads) histogram_kernel(const uint32_t*
 // Exclusive scan of each pass's 256-bin histogram (one block of 256 threads).
 __global__ void __launch_bounds__(256) scan_kernel(const uint32_t* __restrict__ hist, int passes,
                                                    uint32_t* __restrict__ offsets) {
+    DFSPH_PDL_ENTER;
     __shared__ uint32_t s[256];
     for (int p = 0; p < passes; ++p) {
         const uint32_t v = hist[p * 256 + threadIdx.x];
@@ -72,6 +74,7 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
     uint32_t* __restrict__ vout, uint32_t n, int shift, const uint32_t* __restrict__ digit_offsets,
     uint32_t* __restrict__ tile_status, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status_word,
     uint32_t withheld_tile) {
+    DFSPH_PDL_ENTER;
     __shared__ uint32_t warp_hist[kSortWarps][256];
     __shared__ uint32_t digit_base[256];
     __shared__ uint32_t s_tile;
@@ -185,8 +188,8 @@ void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, 
     int hist_blocks = (int)((n + kSortThreads * 16 - 1) / (kSortThreads * 16));
     if (hist_blocks > 148 * 4) hist_blocks = 148 * 4;
     if (hist_blocks < 1) hist_blocks = 1;
-    histogram_kernel<<<hist_blocks, kSortThreads, 0, stream>>>(b.keys_a, n, passes, hist);
-    scan_kernel<<<1, 256, 0, stream>>>(hist, passes, offsets);
+    launch_pdl(histogram_kernel, hist_blocks, kSortThreads, 0, stream, b.keys_a, n, passes, hist);
+    launch_pdl(scan_kernel, 1, 256, 0, stream, hist, passes, offsets);
     *launch_counter += 2;
     for (int p = 0; p < passes; ++p) {
         const bool even = (p & 1) == 0;
@@ -194,7 +197,7 @@ void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, 
         const uint32_t* vin = (p == 0 && iota_values) ? nullptr : (even ? b.vals_a : b.vals_b);
         uint32_t* kout = even ? b.keys_b : b.keys_a;
         uint32_t* vout = even ? b.vals_b : b.vals_a;
-        onesweep_kernel<<<(unsigned)tiles, kSortThreads, 0, stream>>>(kin, vin, kout, vout, n, 8 * p, offsets + p * 256,
+        launch_pdl(onesweep_kernel, (unsigned)tiles, kSortThreads, 0, stream, kin, vin, kout, vout, n, 8 * p, offsets + p * 256,
                                                                    status + (size_t)p * tiles * 256, counters + p,
                                                                    status_word, withheld_tile);
         *launch_counter += 1;
@@ -278,8 +281,8 @@ extern "C" int dfsph_sort_cell_keys_noalloc(const uint32_t* keys_in, uint32_t* k
     if (e != cudaSuccess) return noalloc_fail(DFSPH_E_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
     int hist_blocks = (int)((n + kSortThreads * 16 - 1) / (kSortThreads * 16));
     if (hist_blocks > 148 * 4) hist_blocks = 148 * 4;
-    histogram_kernel<<<hist_blocks, kSortThreads, 0, s>>>(keys_in, n, passes, hist);
-    scan_kernel<<<1, 256, 0, s>>>(hist, passes, offsets);
+    launch_pdl(histogram_kernel, hist_blocks, kSortThreads, 0, s, keys_in, n, passes, hist);
+    launch_pdl(scan_kernel, 1, 256, 0, s, hist, passes, offsets);
     // The last pass must write the caller's buffers: with an odd pass count the first pass writes
     // them, with an even count the first pass writes the scratch pair.
     const uint32_t* kin = keys_in;
@@ -288,7 +291,7 @@ extern "C" int dfsph_sort_cell_keys_noalloc(const uint32_t* keys_in, uint32_t* k
     for (int p = 0; p < passes; ++p) {
         uint32_t* kout = to_out ? keys_out : pk;
         uint32_t* vout = to_out ? perm_out : pv;
-        onesweep_kernel<<<(unsigned)tiles, kSortThreads, 0, s>>>(kin, vin, kout, vout, n, 8 * p, offsets + p * 256,
+        launch_pdl(onesweep_kernel, (unsigned)tiles, kSortThreads, 0, s, kin, vin, kout, vout, n, 8 * p, offsets + p * 256,
                                                                 flags + (size_t)p * tiles * 256, counters + p, status,
                                                                 kNoWithheldTile);
         kin = kout;
