@@ -586,9 +586,12 @@ public:
             return sync_state();
         }
         const StepParams<Real> p = params();
-        launch_cell_keys<Real>(pos[cur], n, p, sb.keys_a, status, stream);
+        // the key pass also clears the fluid cell table and the sort's workspace (no memsets between
+        // the kernels of the step)
+        launch_cell_keys<Real>(pos[cur], n, p, sb.keys_a, status, stream, (uint32_t*)ftab, 2 * cells, sb.workspace,
+                               radix_sort_workspace_words(n, key_passes));
         uint32_t *skeys, *perm;
-        radix_sort_pairs(sb, n, key_passes, true, stream, status, &launches, &skeys, &perm, sort_withheld_tile);
+        radix_sort_pairs(sb, n, key_passes, true, stream, status, &launches, &skeys, &perm, sort_withheld_tile, true);
         const int nx = 1 - cur;
         launch_reorder_fluid<Real>(perm, n, pos[cur], vel[cur], kappa[cur], kappaV[cur], id[cur], pos[nx], vel[nx],
                                    kappa[nx], kappaV[nx], id[nx], stream);
@@ -597,7 +600,6 @@ public:
             launches += 1;
         }
         cur = nx;
-        DF_CUDA(cudaMemsetAsync(ftab, 0, cells * sizeof(uint2), stream));
         launch_cell_bounds(skeys, n, dim[0], dim[1], dim[2], ftab, stream);
         DF_TRY(sync_state());
         launches += 3;
@@ -890,7 +892,6 @@ public:
     // cuda_divergenceSolve (DFSPH_core_cuda.cu:785-861). lp: learned warm start (dfsph_step only).
     int divergence_solve(int max_iter, double max_error, bool lp = false) {
         if (!n) return DFSPH_OK;
-        DF_CUDA(cudaMemsetAsync(&ctl[0].ticket, 0, sizeof(uint32_t), stream));
         const double eta = max_error * 0.01 * sc.density0;  // divided by the device's h in the init pass
         if (!lp) {
             launch_density_alpha<Real>(ds, n, true, false, stream);
@@ -904,7 +905,6 @@ public:
             launch_warm_values<Real>(ds, n, 0, use, damping, stream);
             launches += use ? 3 : 2;
             if (use && probe) {  // both candidates per pass, then the selection
-                DF_CUDA(cudaMemsetAsync(&ctl[3].ticket, 0, sizeof(uint32_t), stream));
                 launch_warm_dual<Real>(ds, n, 0, false, stream, boundary_forces);
                 launch_residual_dual<Real>(ds, n, 0, eta, kMinItersV, max_iter, stream);
                 launch_select_candidate<Real>(ds, n, 0, stream);
@@ -926,7 +926,6 @@ public:
     // cuda_update_vel is applied inside the warm-start pass.
     int pressure_solve(int max_iter, double max_error, bool fused_vel, bool lp = false) {
         if (!n) return DFSPH_OK;
-        DF_CUDA(cudaMemsetAsync(&ctl[1].ticket, 0, sizeof(uint32_t), stream));
         const double eta = max_error * 0.01 * sc.density0;
         if (!lp) {
             launch_pressure_warm_jacobi<Real>(ds, n, fused_vel, nullptr, nullptr, stream, boundary_forces);
@@ -937,7 +936,6 @@ public:
             launch_warm_values<Real>(ds, n, 1, use, damping, stream);
             launches += 1;
             if (use && probe) {
-                DF_CUDA(cudaMemsetAsync(&ctl[3].ticket, 0, sizeof(uint32_t), stream));
                 launch_warm_dual<Real>(ds, n, 1, fused_vel, stream, boundary_forces);
                 launch_residual_dual<Real>(ds, n, 1, eta, kMinItersP, max_iter, stream);
                 launch_select_candidate<Real>(ds, n, 1, stream);

@@ -57,8 +57,11 @@ template <class Real> struct DevState {
 
 // ---- launch wrappers (neighbors.cu) ----------------------------------------------------------------
 template <class Real>
+// clear0 / clear1 (words0 / words1 32-bit words each, may be null / 0): buffers the same launch sets
+// to zero (the fluid cell table and the sort's workspace before a fluid binning).
 void launch_cell_keys(const Vec4<Real>* pos, uint32_t n, const StepParams<Real>& p, uint32_t* keys, uint32_t* status,
-                      cudaStream_t s);
+                      cudaStream_t s, uint32_t* clear0 = nullptr, size_t words0 = 0, uint32_t* clear1 = nullptr,
+                      size_t words1 = 0);
 template <class Real>
 void launch_reorder_fluid(const uint32_t* perm, uint32_t n, const Vec4<Real>* pos_in, const Vec4<Real>* vel_in,
                           const Real* kappa_in, const Real* kappaV_in, const uint32_t* id_in, Vec4<Real>* pos_out,

@@ -164,6 +164,10 @@ template <class Real> __global__ void set_state_kernel(DevState<Real>* __restric
     v.p.h_ratio_to_past = o.h_ratio_to_past;
     v.p.h_ratio_to_past2 = o.h_ratio_to_past2;
     *dst = v;
+    // The solver loops' last-block tickets start from zero (each reduction leaves them at zero too);
+    // resetting them here, with the state, saves a memset before every solve.
+    if (v.ctl)
+        for (int k = 0; k < 4; ++k) v.ctl[k].ticket = 0;
 }
 
 template <class Real> __global__ void dt_kernel(DevState<Real>* __restrict__ ds, int op, DtArgs a) {

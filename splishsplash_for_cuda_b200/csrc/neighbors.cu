@@ -32,9 +32,13 @@ __device__ __forceinline__ uint32_t cell_linear(int cx, int cy, int cz, int dim_
 template <class Real>
 __global__ void __launch_bounds__(kBlock) cell_keys_kernel(const Vec4<Real>* __restrict__ pos, uint32_t n,
                                                            StepParams<Real> p, uint32_t* __restrict__ keys,
-                                                           uint32_t* __restrict__ status) {
+                                                           uint32_t* __restrict__ status, uint32_t* __restrict__ z0,
+                                                           size_t w0, uint32_t* __restrict__ z1, size_t w1) {
     DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t k = i; k < w0; k += stride) z0[k] = 0u;  // optional buffers to clear (w = 0: none)
+    for (size_t k = i; k < w1; k += stride) z1[k] = 0u;
     if (i >= n) return;
     const Vec4<Real> x = pos[i];
     int cx, cy, cz;
@@ -247,8 +251,10 @@ __global__ void __launch_bounds__(kBlock) scatter_by_id_kernel(const uint32_t* _
 
 template <class Real>
 void launch_cell_keys(const Vec4<Real>* pos, uint32_t n, const StepParams<Real>& p, uint32_t* keys, uint32_t* status,
-                      cudaStream_t s) {
-    if (n) launch_pdl(cell_keys_kernel<Real>, grid_for(n), kBlock, 0, s, pos, n, p, keys, status);
+                      cudaStream_t s, uint32_t* clear0, size_t words0, uint32_t* clear1, size_t words1) {
+    if (n)
+        launch_pdl(cell_keys_kernel<Real>, grid_for(n), kBlock, 0, s, pos, n, p, keys, status, clear0, words0, clear1,
+                   words1);
 }
 template <class Real>
 void launch_reorder_fluid(const uint32_t* perm, uint32_t n, const Vec4<Real>* pos_in, const Vec4<Real>* vel_in,
@@ -285,7 +291,7 @@ void launch_scatter_by_id(const uint32_t* id, uint32_t n, const Real* src, int c
 
 #define DFSPH_INSTANTIATE_NEIGHBORS(R)                                                                               \
     template void launch_cell_keys<R>(const Vec4<R>*, uint32_t, const StepParams<R>&, uint32_t*, uint32_t*,          \
-                                      cudaStream_t);                                                                 \
+                                      cudaStream_t, uint32_t*, size_t, uint32_t*, size_t);                           \
     template void launch_reorder_fluid<R>(const uint32_t*, uint32_t, const Vec4<R>*, const Vec4<R>*, const R*,       \
                                           const R*, const uint32_t*, Vec4<R>*, Vec4<R>*, R*, R*, uint32_t*,          \
                                           cudaStream_t);                                                             \

@@ -172,7 +172,7 @@ size_t radix_sort_workspace_words(uint32_t n_max, int passes) {
 // *keys_out / *vals_out and lies in set a after an even number of passes, else in set b.
 void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, cudaStream_t stream,
                       uint32_t* status_word, uint64_t* launch_counter, uint32_t** keys_out, uint32_t** vals_out,
-                      uint32_t withheld_tile) {
+                      uint32_t withheld_tile, bool workspace_cleared) {
     if (n == 0 || passes == 0) {
         *keys_out = b.keys_a;
         *vals_out = b.vals_a;
@@ -184,7 +184,8 @@ void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, 
     uint32_t* hist = b.workspace + 4;
     uint32_t* offsets = hist + 1024;
     uint32_t* status = offsets + 1024;
-    cudaMemsetAsync(b.workspace, 0, radix_sort_workspace_words(n, passes) * sizeof(uint32_t), stream);
+    if (!workspace_cleared)
+        cudaMemsetAsync(b.workspace, 0, radix_sort_workspace_words(n, passes) * sizeof(uint32_t), stream);
     int hist_blocks = (int)((n + kSortThreads * 16 - 1) / (kSortThreads * 16));
     if (hist_blocks > 148 * 4) hist_blocks = 148 * 4;
     if (hist_blocks < 1) hist_blocks = 1;

@@ -23,8 +23,10 @@ void set_global_error(const std::string& msg);
 // successors' bounded waits run out and set DFSPH_ST_SORT_TIMEOUT; the output is then unspecified
 // but every write stays in range). kNoWithheldTile in normal use.
 constexpr uint32_t kNoWithheldTile = 0xFFFFFFFFu;
+// workspace_cleared: the caller has already zeroed radix_sort_workspace_words(n, passes) words of
+// the workspace on this stream (otherwise the sort clears them itself).
 void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, cudaStream_t stream,
                       uint32_t* status_word, uint64_t* launch_counter, uint32_t** keys_out, uint32_t** vals_out,
-                      uint32_t withheld_tile = kNoWithheldTile);
+                      uint32_t withheld_tile = kNoWithheldTile, bool workspace_cleared = false);
 
 }  // namespace dfsph
