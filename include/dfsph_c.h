@@ -50,6 +50,8 @@ typedef struct dfsph_ctx dfsph_ctx;
 #define DFSPH_ST_SORT_TIMEOUT 0x20u      /* a bounded wait in the radix sort gave up (no hang)      */
 #define DFSPH_ST_BOUNDARY_OVERFLOW 0x40u /* a boundary particle had too many boundary neighbours    */
 #define DFSPH_ST_FLUID_CAPACITY 0x80u    /* an open-boundary inflow was cut at fluid_capacity        */
+#define DFSPH_ST_MMA_TIMEOUT 0x100u      /* a bounded wait for the warm-start network's tensor-core MMA
+                                            gave up (no hang; that call's predictions are unspecified) */
 
 /* ---- scene / solver parameters ---------------------------------------------------------------- */
 /* Mirrors the "Configuration" keys of the reference JSON scene (Utilities/SceneLoader.cpp:39-160)

@@ -25,6 +25,7 @@ ST_DIVERGENCE_NOT_CONVERGED = 0x10
 ST_SORT_TIMEOUT = 0x20
 ST_BOUNDARY_OVERFLOW = 0x40
 ST_FLUID_CAPACITY = 0x80
+ST_MMA_TIMEOUT = 0x100
 
 SURFACE_PLANE, SURFACE_CUBOID, SURFACE_CYLINDER, SURFACE_SPHERE, SURFACE_STAR = 0, 1, 2, 4, 5
 

@@ -901,7 +901,7 @@ public:
         } else {
             const bool use = mlp_ready;
             launch_density_alpha<Real>(ds, n, false, true, stream);
-            if (use) launch_mlp_forward(mlp, features, n, pred, stream);
+            if (use) launch_mlp_forward(mlp, features, n, pred, status, stream);
             launch_warm_values<Real>(ds, n, 0, use, damping, stream);
             launches += use ? 3 : 2;
             if (use && probe) {  // both candidates per pass, then the selection
@@ -1055,7 +1055,7 @@ public:
                 DF_CUDA(cudaMemsetAsync(kappaVW, 0, (size_t)n * sizeof(Real), stream));
                 DF_CUDA(cudaMemsetAsync(kappaV[cur], 0, (size_t)n * sizeof(Real), stream));
                 if (mlp_ready) {
-                    launch_mlp_forward(mlp, features, n, pred, stream);
+                    launch_mlp_forward(mlp, features, n, pred, status, stream);
                     launches += 1;
                 }
             }
@@ -1333,7 +1333,7 @@ public:
     int mlp_forward_host(const float* x, uint32_t B, float* y) {
         DF_CHECK(y, DFSPH_E_INVALID, "null output");
         DF_TRY(stage_batch(x, nullptr, B));
-        launch_mlp_forward(mlp, tx, B, tt, stream);
+        launch_mlp_forward(mlp, tx, B, tt, status, stream);
         launches += 1;
         DF_CUDA(cudaMemcpyAsync(y, tt, (size_t)B * kMlpOut * sizeof(float), cudaMemcpyDeviceToHost, stream));
         DF_CUDA(cudaStreamSynchronize(stream));

@@ -14,105 +14,251 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
     return *reinterpret_cast<uint32_t*>(&v);
 }
 
-// D += A (16x16, row) * B (16x8, col) with BF16 inputs and FP32 accumulation.
-__device__ __forceinline__ void mma_bf16_16x8x16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                                 uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+// ---- inference on the 5th-generation tensor cores (tcgen05) -------------------------------------
+// One CTA of 128 threads evaluates tiles of 128 particles (the MMA's M): thread t owns particle row t
+// of the tile. Operands sit in shared memory in the canonical K-major, unswizzled UMMA layout
+// (core matrices of 8 rows x 16 bytes; LBO = byte distance between the two 8-element K halves of
+// one MMA's K = 16, SBO = distance between 8-row groups); one thread issues the MMAs, whose FP32
+// accumulators live in tensor memory (TMEM); each warp reads its 32 rows back with tcgen05.ld, adds
+// the bias, applies ReLU and stores the BF16 activations as the next layer's A operand.
+//   layer 1: [128 x 16] x [16 x 64]   (5 inputs + zero padding)  -> TMEM columns 0..63
+//   layer 2: [128 x 64] x [64 x 64]   (4 MMAs of K = 16)         -> TMEM columns 64..127
+//   layer 3: [128 x 64] x [64 x 16]   (2 outputs + zero padding) -> TMEM columns 0..15
+constexpr int kMmaM = 128;
+constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kSA = 0;                    // A operand: 128 x 64 BF16 = 16 KB
+constexpr uint32_t kSW1 = kSA + 16384;         // 64 x 16 BF16 = 2 KB
+constexpr uint32_t kSW2 = kSW1 + 2048;         // 64 x 64 BF16 = 8 KB
+constexpr uint32_t kSW3 = kSW2 + 8192;         // 16 x 64 BF16 = 2 KB
+constexpr uint32_t kSBias = kSW3 + 2048;       // b1[64], b2[64], b3[2], in_scale[8] (FP32)
+constexpr uint32_t kSBar = kSBias + 1024;      // mbarrier (8 B) + TMEM address slot (4 B)
+// Dynamic shared memory per CTA: the operands plus padding up to 56 KB, so that at most four CTAs
+// share an SM and their four 128-column TMEM allocations fit the SM's 512 columns (no CTA ever waits
+// in tcgen05.alloc).
+constexpr uint32_t kMlpSmem = 56 * 1024;
+constexpr uint32_t kMmaWaitLimit = 1u << 22;   // bounded mbarrier waits (a give-up raises a status bit)
+
+// Byte offset of element (r, k) of a K-major operand with 8-row groups of kchunks 16-byte chunks.
+__device__ __forceinline__ uint32_t umma_off(uint32_t r, uint32_t k, uint32_t kchunks) {
+    return (r >> 3) * (kchunks * 128u) + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
 }
 
-// Shared-memory row strides (32-bit words) chosen so that the 8 row-groups of a fragment load hit
-// distinct banks.
-constexpr int kS1 = 12;  // W1: 16 BF16 = 8 words per row, padded
-constexpr int kS2 = 36;  // W2 / W3: 64 BF16 = 32 words per row, padded
+// Shared-memory matrix descriptor (sm_100 layout): start address, LBO, SBO in 16-byte units,
+// version 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
 
-// One warp evaluates 16 particles per iteration: layer 1 (K = 16 with 5 real inputs), layer 2
-// (K = 64), layer 3 (N = 8 with 2 real outputs). The FP32 accumulator fragment of an m16n8 tile is
-// exactly the BF16 A-fragment layout of the next layer's k-chunk, so activations stay in registers.
-__global__ void __launch_bounds__(128) mlp_forward_kernel(const uint16_t* __restrict__ w1b,
-                                                          const uint16_t* __restrict__ w2b,
-                                                          const uint16_t* __restrict__ w3b,
-                                                          const float* __restrict__ params,
-                                                          const MlpScales* __restrict__ scales,
-                                                          const float* __restrict__ features, uint32_t n,
-                                                          float* __restrict__ pred) {
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, M x N.
+__device__ __forceinline__ uint32_t umma_idesc(uint32_t m, uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+// Waits for the mbarrier phase `parity`; false if the wait gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < kMmaWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Bias + ReLU of 64 accumulator columns of this thread's row (TMEM column `col`), stored as BF16
+// row r of the 128 x 64 A operand.
+__device__ __forceinline__ void epilogue64(uint32_t taddr_row, uint32_t col, const float* bias, unsigned char* sa,
+                                           uint32_t r) {
+#pragma unroll
+    for (int c0 = 0; c0 < 64; c0 += 16) {
+        float v[16];
+        tmem_ld16(taddr_row + col + c0, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int h = 0; h < 16; h += 8) {
+            uint4 chunk;
+            chunk.x = pack_bf16x2(fmaxf(v[h + 0] + bias[c0 + h + 0], 0.f), fmaxf(v[h + 1] + bias[c0 + h + 1], 0.f));
+            chunk.y = pack_bf16x2(fmaxf(v[h + 2] + bias[c0 + h + 2], 0.f), fmaxf(v[h + 3] + bias[c0 + h + 3], 0.f));
+            chunk.z = pack_bf16x2(fmaxf(v[h + 4] + bias[c0 + h + 4], 0.f), fmaxf(v[h + 5] + bias[c0 + h + 5], 0.f));
+            chunk.w = pack_bf16x2(fmaxf(v[h + 6] + bias[c0 + h + 6], 0.f), fmaxf(v[h + 7] + bias[c0 + h + 7], 0.f));
+            *reinterpret_cast<uint4*>(sa + umma_off(r, c0 + h, 8)) = chunk;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kMmaM) mlp_forward_kernel(const uint16_t* __restrict__ w1b,
+                                                            const uint16_t* __restrict__ w2b,
+                                                            const uint16_t* __restrict__ w3b,
+                                                            const float* __restrict__ params,
+                                                            const MlpScales* __restrict__ scales,
+                                                            const float* __restrict__ features, uint32_t n,
+                                                            float* __restrict__ pred, uint32_t* __restrict__ status) {
     DFSPH_PDL_ENTER;
-    __shared__ uint32_t sW1[kMlpHidden * kS1];
-    __shared__ uint32_t sW2[kMlpHidden * kS2];
-    __shared__ uint32_t sW3[8 * kS2];
-    __shared__ float sB1[kMlpHidden], sB2[kMlpHidden], sB3[8], sIn[kMlpIn];
-    const uint32_t* w1 = reinterpret_cast<const uint32_t*>(w1b);
-    const uint32_t* w2 = reinterpret_cast<const uint32_t*>(w2b);
-    const uint32_t* w3 = reinterpret_cast<const uint32_t*>(w3b);
-    for (int t = threadIdx.x; t < kMlpHidden * 8; t += blockDim.x) sW1[(t / 8) * kS1 + t % 8] = w1[t];
-    for (int t = threadIdx.x; t < kMlpHidden * 32; t += blockDim.x) sW2[(t / 32) * kS2 + t % 32] = w2[t];
-    for (int t = threadIdx.x; t < 8 * 32; t += blockDim.x) sW3[(t / 32) * kS2 + t % 32] = w3[t];
-    for (int t = threadIdx.x; t < kMlpHidden; t += blockDim.x) {
-        sB1[t] = params[kB1 + t];
-        sB2[t] = params[kB2 + t];
-    }
-    if (threadIdx.x < 8) sB3[threadIdx.x] = threadIdx.x < kMlpOut ? params[kB3 + threadIdx.x] : 0.0f;
-    if (threadIdx.x < kMlpIn) sIn[threadIdx.x] = scales->in_scale[threadIdx.x];
-    __syncthreads();
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* sa = smem + kSA;
+    float* sb1 = reinterpret_cast<float*>(smem + kSBias);
+    float* sb2 = sb1 + 64;
+    float* sb3 = sb2 + 64;
+    float* sin = sb3 + 2;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kSBar);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + kSBar + 8);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t s_base = (uint32_t)__cvta_generic_to_shared(smem);
+    const uint32_t bar_addr = s_base + kSBar;
 
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    for (uint32_t tile = (blockIdx.x * 4 + warp) * 16; tile < n; tile += gridDim.x * 4 * 16) {
-        const uint32_t r0 = tile + g, r1 = tile + g + 8;
-        float x00 = 0.f, x01 = 0.f, x10 = 0.f, x11 = 0.f;
-        if (r0 < n) {
-            const float2 f = *reinterpret_cast<const float2*>(features + (size_t)r0 * kMlpIn + 2 * q);
-            x00 = f.x * sIn[2 * q];
-            x01 = f.y * sIn[2 * q + 1];
-        }
-        if (r1 < n) {
-            const float2 f = *reinterpret_cast<const float2*>(features + (size_t)r1 * kMlpIn + 2 * q);
-            x10 = f.x * sIn[2 * q];
-            x11 = f.y * sIn[2 * q + 1];
-        }
-        const uint32_t a0 = pack_bf16x2(x00, x01), a1 = pack_bf16x2(x10, x11);
-        uint32_t h1[4][4];
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            float c[4];
-            c[0] = c[2] = sB1[8 * nt + 2 * q];
-            c[1] = c[3] = sB1[8 * nt + 2 * q + 1];
-            const uint32_t* row = sW1 + (8 * nt + g) * kS1;
-            mma_bf16_16x8x16(c, a0, a1, 0u, 0u, row[q], row[4 + q]);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) c[e] = fmaxf(c[e], 0.0f);
-            h1[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16x2(c[0], c[1]);
-            h1[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16x2(c[2], c[3]);
-        }
-        uint32_t h2[4][4];
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            float c[4];
-            c[0] = c[2] = sB2[8 * nt + 2 * q];
-            c[1] = c[3] = sB2[8 * nt + 2 * q + 1];
-            const uint32_t* row = sW2 + (8 * nt + g) * kS2;
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-                mma_bf16_16x8x16(c, h1[kk][0], h1[kk][1], h1[kk][2], h1[kk][3], row[8 * kk + q], row[8 * kk + 4 + q]);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) c[e] = fmaxf(c[e], 0.0f);
-            h2[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16x2(c[0], c[1]);
-            h2[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16x2(c[2], c[3]);
-        }
-        float c[4];
-        c[0] = c[2] = sB3[2 * q];
-        c[1] = c[3] = sB3[2 * q + 1];
-        const uint32_t* row = sW3 + g * kS2;
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk)
-            mma_bf16_16x8x16(c, h2[kk][0], h2[kk][1], h2[kk][2], h2[kk][3], row[8 * kk + q], row[8 * kk + 4 + q]);
-        if (q == 0) {  // columns 0 and 1 are the two outputs
-            if (r0 < n) *reinterpret_cast<float2*>(pred + 2 * (size_t)r0) = make_float2(c[0], c[1]);
-            if (r1 < n) *reinterpret_cast<float2*>(pred + 2 * (size_t)r1) = make_float2(c[2], c[3]);
-        }
+    // weights into the UMMA layout (B operands are [N][K], K-major)
+    for (uint32_t t = tid; t < 64 * 2; t += kMmaM) {  // W1: 64 rows x 2 chunks (K = 16)
+        const uint32_t r = t >> 1, c = t & 1;
+        *reinterpret_cast<uint4*>(smem + kSW1 + umma_off(r, 8 * c, 2)) =
+            *reinterpret_cast<const uint4*>(w1b + r * 16 + 8 * c);
     }
+    for (uint32_t t = tid; t < 64 * 8; t += kMmaM) {  // W2: 64 rows x 8 chunks
+        const uint32_t r = t >> 3, c = t & 7;
+        *reinterpret_cast<uint4*>(smem + kSW2 + umma_off(r, 8 * c, 8)) =
+            *reinterpret_cast<const uint4*>(w2b + r * 64 + 8 * c);
+    }
+    for (uint32_t t = tid; t < 16 * 8; t += kMmaM) {  // W3: 16 rows (8 stored, the rest zero) x 8 chunks
+        const uint32_t r = t >> 3, c = t & 7;
+        const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(smem + kSW3 + umma_off(r, 8 * c, 8)) =
+            r < 8 ? *reinterpret_cast<const uint4*>(w3b + r * 64 + 8 * c) : z;
+    }
+    if (tid < 64) {
+        sb1[tid] = params[kB1 + tid];
+        sb2[tid] = params[kB2 + tid];
+    }
+    if (tid < kMlpOut) sb3[tid] = params[kB3 + tid];
+    if (tid < kMlpIn) sin[tid] = scales->in_scale[tid];
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_addr) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {  // TMEM for the accumulators
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s_base + kSBar + 8),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t trow = tmem + ((warp * 32u) << 16);  // this warp's 32 TMEM lanes
+    const uint32_t idesc64 = umma_idesc(kMmaM, 64), idesc16 = umma_idesc(kMmaM, 16);
+    uint32_t phase = 0;
+    bool ok = true;
+
+    for (uint32_t tile = blockIdx.x; tile * kMmaM < n && ok; tile += gridDim.x) {
+        const uint32_t row = tile * kMmaM + tid;
+        // layer-1 operand: the scaled features, K padded to 16
+        {
+            float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (row < n) {
+                const float4 f0 = *reinterpret_cast<const float4*>(features + (size_t)row * kMlpIn);
+                const float4 f1 = *reinterpret_cast<const float4*>(features + (size_t)row * kMlpIn + 4);
+                x[0] = f0.x * sin[0]; x[1] = f0.y * sin[1]; x[2] = f0.z * sin[2]; x[3] = f0.w * sin[3];
+                x[4] = f1.x * sin[4]; x[5] = f1.y * sin[5]; x[6] = f1.z * sin[6]; x[7] = f1.w * sin[7];
+            }
+            uint4 c0;
+            c0.x = pack_bf16x2(x[0], x[1]);
+            c0.y = pack_bf16x2(x[2], x[3]);
+            c0.z = pack_bf16x2(x[4], x[5]);
+            c0.w = pack_bf16x2(x[6], x[7]);
+            *reinterpret_cast<uint4*>(sa + umma_off(tid, 0, 2)) = c0;
+            *reinterpret_cast<uint4*>(sa + umma_off(tid, 8, 2)) = make_uint4(0u, 0u, 0u, 0u);
+        }
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            umma_bf16(tmem + 0, umma_desc(s_base + kSA, 128, 256), umma_desc(s_base + kSW1, 128, 256), idesc64, 0);
+            umma_commit(bar_addr);
+        }
+        ok = __all_sync(0xFFFFFFFFu, mbar_wait(bar_addr, phase));  // warp-uniform for tcgen05.ld
+        phase ^= 1u;
+        tc_fence_after();
+        if (ok) epilogue64(trow, 0, sb1, sa, tid);  // layer-1 activations -> A operand (K = 64)
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0 && ok) {
+            tc_fence_after();
+            for (uint32_t k = 0; k < 4; ++k)
+                umma_bf16(tmem + 64, umma_desc(s_base + kSA + 256 * k, 128, 1024),
+                          umma_desc(s_base + kSW2 + 256 * k, 128, 1024), idesc64, k > 0);
+            umma_commit(bar_addr);
+        }
+        if (ok) ok = __all_sync(0xFFFFFFFFu, mbar_wait(bar_addr, phase));
+        phase ^= 1u;
+        tc_fence_after();
+        if (ok) epilogue64(trow, 64, sb2, sa, tid);  // layer-2 activations -> A operand
+        async_proxy_fence();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0 && ok) {
+            tc_fence_after();
+            for (uint32_t k = 0; k < 4; ++k)
+                umma_bf16(tmem + 0, umma_desc(s_base + kSA + 256 * k, 128, 1024),
+                          umma_desc(s_base + kSW3 + 256 * k, 128, 1024), idesc16, k > 0);
+            umma_commit(bar_addr);
+        }
+        if (ok) ok = __all_sync(0xFFFFFFFFu, mbar_wait(bar_addr, phase));
+        phase ^= 1u;
+        tc_fence_after();
+        if (ok) {
+            float v[16];
+            tmem_ld16(trow, v);
+            tmem_wait_ld();
+            if (row < n) *reinterpret_cast<float2*>(pred + 2 * (size_t)row) = make_float2(v[0] + sb3[0], v[1] + sb3[1]);
+        }
+        tc_fence_before();
+        __syncthreads();
+        ok = __syncthreads_and(ok);
+    }
+    if (!ok && tid == 0) atomicOr(status, DFSPH_ST_MMA_TIMEOUT);
+    // (a wait that gave up leaves at most one MMA group in flight: give it the same bounded time)
+    if (!ok && tid == 0) mbar_wait(bar_addr, phase ^ 1u);
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
 __global__ void mlp_pack_kernel(const float* __restrict__ params, uint16_t* __restrict__ w1b,
@@ -288,11 +434,14 @@ size_t mlp_partials_floats(uint32_t max_batch) {
     return blocks * (kMlpParams + 1);
 }
 
-void launch_mlp_forward(const MlpDev& m, const float* features, uint32_t n, float* pred, cudaStream_t s) {
+void launch_mlp_forward(const MlpDev& m, const float* features, uint32_t n, float* pred, uint32_t* status,
+                        cudaStream_t s) {
     if (!n) return;
-    uint32_t tiles = (n + 63) / 64;
-    if (tiles > 148 * 16) tiles = 148 * 16;
-    launch_pdl(mlp_forward_kernel, tiles, 128, 0, s, m.w1_bf16, m.w2_bf16, m.w3_bf16, m.params, m.scales, features, n, pred);
+    cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpSmem);
+    uint32_t tiles = (n + kMmaM - 1) / kMmaM;
+    if (tiles > 148 * 4) tiles = 148 * 4;  // persistent CTAs, at most four per SM (see kMlpSmem)
+    launch_pdl(mlp_forward_kernel, tiles, kMmaM, kMlpSmem, s, m.w1_bf16, m.w2_bf16, m.w3_bf16, m.params, m.scales,
+               features, n, pred, status);
 }
 
 void launch_mlp_pack(const MlpDev& m, cudaStream_t s) {

@@ -16,6 +16,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/dfsph_c.h"
+
 namespace dfsph {
 
 constexpr int kMlpIn = 8;       // 5 features + 3 zero pads
@@ -50,8 +52,11 @@ struct MlpDev {
     double* loss;         // last batch loss
 };
 
-// Inference: pred[2 i + o] = MLP(features[8 i ...] * in_scale)[o] for i < n, on tensor cores.
-void launch_mlp_forward(const MlpDev& m, const float* features, uint32_t n, float* pred, cudaStream_t s);
+// Inference: pred[2 i + o] = MLP(features[8 i ...] * in_scale)[o] for i < n, on the tcgen05 tensor
+// cores (accumulators in tensor memory). A bounded wait that gives up raises DFSPH_ST_MMA_TIMEOUT in
+// *status.
+void launch_mlp_forward(const MlpDev& m, const float* features, uint32_t n, float* pred, uint32_t* status,
+                        cudaStream_t s);
 // FP32 master weights -> BF16 inference copies.
 void launch_mlp_pack(const MlpDev& m, cudaStream_t s);
 // One training step on a batch: per-block forward/backward partial gradients, then a deterministic
