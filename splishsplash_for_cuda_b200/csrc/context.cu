@@ -67,6 +67,12 @@ public:
     std::string& err;
     dfsph_scene sc{};
     cudaStream_t stream = nullptr;
+    // Velocities given to update_fluid travel on a copy stream and are applied inside the next
+    // step's binning, after the sort (which does not read them): their upload overlaps the key pass
+    // and the radix sort. Any other call applies them first (flush_pending).
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_vel_ready = nullptr, ev_vel_free = nullptr;
+    bool pending_vel = false;
     uint32_t Nc = 0, Bc = 0, cap = 0, stride = 0;
     uint32_t n = 0, nb = 0;
     int cur = 0;
@@ -225,6 +231,9 @@ public:
         DF_CUDA(cudaMemsetAsync(counts, 0, Nc * sizeof(uint32_t), stream));
         DF_CUDA(cudaEventCreate(&ev0));
         DF_CUDA(cudaEventCreate(&ev1));
+        DF_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+        DF_CUDA(cudaEventCreateWithFlags(&ev_vel_ready, cudaEventDisableTiming));
+        DF_CUDA(cudaEventCreateWithFlags(&ev_vel_free, cudaEventDisableTiming));
         time_step = s.time_step;
         use_graphs = s.use_graphs != 0;
         DF_TRY(sync_state());
@@ -233,6 +242,7 @@ public:
     }
 
     void release() {
+        if (copy_stream) cudaStreamSynchronize(copy_stream);
         if (stream) cudaStreamSynchronize(stream);
         for (int k = 0; k < 2; ++k)
             if (g_loop[k]) cudaGraphExecDestroy(g_loop[k]);
@@ -262,6 +272,9 @@ public:
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+        if (ev_vel_ready) cudaEventDestroy(ev_vel_ready);
+        if (ev_vel_free) cudaEventDestroy(ev_vel_free);
         stream = nullptr;
     }
 
@@ -556,9 +569,37 @@ public:
         float* sx = stage;
         float* sv = stage + (size_t)n * 3;
         DF_CUDA(cudaMemcpyAsync(sx, xyz, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, stream));
-        if (vxyz) DF_CUDA(cudaMemcpyAsync(sv, vxyz, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, stream));
-        launch_update_fluid<Real>(sx, vxyz ? sv : nullptr, n, id[cur], pos[cur], vel[cur], stream);
+        if (!vxyz) {  // positions, velocities zero
+            launch_update_fluid<Real>(sx, nullptr, n, id[cur], pos[cur], vel[cur], stream, true);
+            launches += 1;
+            return DFSPH_OK;
+        }
+        launch_update_fluid<Real>(sx, nullptr, n, id[cur], pos[cur], vel[cur], stream, false);
+        // the staging area is free once the work queued so far has run
+        DF_CUDA(cudaEventRecord(ev_vel_free, stream));
+        DF_CUDA(cudaStreamWaitEvent(copy_stream, ev_vel_free, 0));
+        DF_CUDA(cudaMemcpyAsync(sv, vxyz, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, copy_stream));
+        DF_CUDA(cudaEventRecord(ev_vel_ready, copy_stream));
+        pending_vel = true;
         launches += 1;
+        return DFSPH_OK;
+    }
+
+    // Applies velocities uploaded by update_fluid (in id order) to the current particle order.
+    int flush_pending() {
+        if (!pending_vel) return DFSPH_OK;
+        pending_vel = false;
+        DF_CUDA(cudaStreamWaitEvent(stream, ev_vel_ready, 0));
+        launch_update_fluid<Real>(nullptr, stage + (size_t)n * 3, n, id[cur], pos[cur], vel[cur], stream, true);
+        launches += 1;
+        return DFSPH_OK;
+    }
+    // Every entry point but the step applies pending velocities first.
+    int enter() { return flush_pending(); }
+    int synchronize_all() {
+        DF_TRY(flush_pending());
+        DF_CUDA(cudaStreamSynchronize(copy_stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
         return DFSPH_OK;
     }
 
@@ -592,6 +633,7 @@ public:
                                radix_sort_workspace_words(n, key_passes));
         uint32_t *skeys, *perm;
         radix_sort_pairs(sb, n, key_passes, true, stream, status, &launches, &skeys, &perm, sort_withheld_tile, true);
+        DF_TRY(flush_pending());  // velocities uploaded during the key pass and the sort
         const int nx = 1 - cur;
         launch_reorder_fluid<Real>(perm, n, pos[cur], vel[cur], kappa[cur], kappaV[cur], id[cur], pos[nx], vel[nx],
                                    kappa[nx], kappaV[nx], id[nx], stream);
@@ -1039,6 +1081,7 @@ public:
 
     int step(dfsph_step_stats* st) {
         DF_CHECK(grid_ready, DFSPH_E_STATE, "step before any boundary or fluid upload");
+        if (!n) DF_TRY(flush_pending());
         if (timing) DF_CUDA(cudaEventRecord(ev0, stream));
         const bool lp = learned && n > 0;
         forced_warm = 0;
@@ -2023,6 +2066,18 @@ struct dfsph_ctx {
             (ctx)->err = "cudaSetDevice failed";                                               \
             return DFSPH_E_CUDA;                                                               \
         }                                                                                      \
+        const int pre = (ctx)->f32 ? (ctx)->f32->enter() : (ctx)->f64->enter();                \
+        if (pre != DFSPH_OK) return pre;                                                       \
+        return (ctx)->f32 ? (ctx)->f32->call : (ctx)->f64->call;                               \
+    } while (0)
+// The step applies velocities pending from dfsph_update_fluid inside its binning.
+#define DFSPH_DISPATCH_STEP(ctx, call)                                                         \
+    do {                                                                                       \
+        if (!(ctx)) return DFSPH_E_INVALID;                                                    \
+        if (cudaSetDevice((ctx)->device) != cudaSuccess) {                                     \
+            (ctx)->err = "cudaSetDevice failed";                                               \
+            return DFSPH_E_CUDA;                                                               \
+        }                                                                                      \
         return (ctx)->f32 ? (ctx)->f32->call : (ctx)->f64->call;                               \
     } while (0)
 
@@ -2137,7 +2192,7 @@ int dfsph_download(dfsph_ctx* ctx, int field, int dtype, void* out, size_t n_ele
 int dfsph_get_neighbors(dfsph_ctx* ctx, uint32_t* counts, uint32_t* lists, uint32_t cap) {
     DFSPH_DISPATCH(ctx, get_neighbors(counts, lists, cap));
 }
-int dfsph_step(dfsph_ctx* ctx, dfsph_step_stats* stats) { DFSPH_DISPATCH(ctx, step(stats)); }
+int dfsph_step(dfsph_ctx* ctx, dfsph_step_stats* stats) { DFSPH_DISPATCH_STEP(ctx, step(stats)); }
 int dfsph_neighbors_search(dfsph_ctx* ctx, int sort) {
     (void)sort;
     DFSPH_DISPATCH(ctx, neighbors_search());
@@ -2183,16 +2238,7 @@ int dfsph_num_fluid(dfsph_ctx* ctx, uint32_t* n) {
     *n = ctx->f32 ? ctx->f32->n : ctx->f64->n;
     return DFSPH_OK;
 }
-int dfsph_synchronize(dfsph_ctx* ctx) {
-    if (!ctx) return DFSPH_E_INVALID;
-    cudaSetDevice(ctx->device);
-    const cudaError_t e = cudaStreamSynchronize(ctx->f32 ? ctx->f32->stream : ctx->f64->stream);
-    if (e != cudaSuccess) {
-        ctx->err = std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e);
-        return DFSPH_E_CUDA;
-    }
-    return DFSPH_OK;
-}
+int dfsph_synchronize(dfsph_ctx* ctx) { DFSPH_DISPATCH(ctx, synchronize_all()); }
 int dfsph_get_stream(dfsph_ctx* ctx, void** stream) {
     if (!ctx || !stream) return DFSPH_E_INVALID;
     *stream = (void*)(ctx->f32 ? ctx->f32->stream : ctx->f64->stream);

@@ -40,16 +40,19 @@ __global__ void __launch_bounds__(kBlock) update_fluid_kernel(const float* __res
                                                               const float* __restrict__ vxyz, uint32_t n,
                                                               const uint32_t* __restrict__ id,
                                                               Vec4<Real>* __restrict__ pos,
-                                                              Vec4<Real>* __restrict__ vel) {
+                                                              Vec4<Real>* __restrict__ vel, bool set_vel) {
     DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t t = id[i];
-    Vec4<Real> x = pos[i];
-    x.x = (Real)xyz[3 * t + 0];
-    x.y = (Real)xyz[3 * t + 1];
-    x.z = (Real)xyz[3 * t + 2];
-    pos[i] = x;
+    if (xyz) {
+        Vec4<Real> x = pos[i];
+        x.x = (Real)xyz[3 * t + 0];
+        x.y = (Real)xyz[3 * t + 1];
+        x.z = (Real)xyz[3 * t + 2];
+        pos[i] = x;
+    }
+    if (!set_vel) return;
     Vec4<Real> v;
     v.x = vxyz ? (Real)vxyz[3 * t + 0] : Real(0);
     v.y = vxyz ? (Real)vxyz[3 * t + 1] : Real(0);
@@ -222,8 +225,8 @@ void launch_unpack_fluid(const float* xyz, const float* vxyz, const float* mass,
 }
 template <class Real>
 void launch_update_fluid(const float* xyz, const float* vxyz, uint32_t n, const uint32_t* id, Vec4<Real>* pos,
-                         Vec4<Real>* vel, cudaStream_t s) {
-    if (n) launch_pdl(update_fluid_kernel<Real>, grid_for(n), kBlock, 0, s, xyz, vxyz, n, id, pos, vel);
+                         Vec4<Real>* vel, cudaStream_t s, bool set_vel) {
+    if (n) launch_pdl(update_fluid_kernel<Real>, grid_for(n), kBlock, 0, s, xyz, vxyz, n, id, pos, vel, set_vel);
 }
 template <class Real>
 void launch_unpack_boundary(const float* xyz, const float* psi, uint32_t n, Vec4<Real>* bpos, Vec4<Real>* bvel,
@@ -260,7 +263,7 @@ void launch_unpack_counts(const uint32_t* counts, const uint32_t* id, uint32_t n
     template void launch_unpack_fluid<R>(const float*, const float*, const float*, float, uint32_t, Vec4<R>*,        \
                                          Vec4<R>*, R*, R*, uint32_t*, cudaStream_t);                                 \
     template void launch_update_fluid<R>(const float*, const float*, uint32_t, const uint32_t*, Vec4<R>*, Vec4<R>*,  \
-                                         cudaStream_t);                                                              \
+                                         cudaStream_t, bool);                                                        \
     template void launch_unpack_boundary<R>(const float*, const float*, uint32_t, Vec4<R>*, Vec4<R>*, cudaStream_t); \
     template void launch_reorder_boundary<R>(const uint32_t*, uint32_t, const Vec4<R>*, const Vec4<R>*, Vec4<R>*,   \
                                              Vec4<R>*, uint32_t*, cudaStream_t);                                     \

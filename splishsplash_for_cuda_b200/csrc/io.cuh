@@ -24,9 +24,11 @@ template <class Real> void launch_dt(DevState<Real>* d, int op, const DtArgs& a,
 template <class Real>
 void launch_unpack_fluid(const float* xyz, const float* vxyz, const float* mass, float default_mass, uint32_t n,
                          Vec4<Real>* pos, Vec4<Real>* vel, Real* kappa, Real* kappaV, uint32_t* id, cudaStream_t s);
+// Overwrites positions (xyz not null) and, with set_vel, velocities (zero for a null vxyz) of the
+// particles, both given in id order.
 template <class Real>
 void launch_update_fluid(const float* xyz, const float* vxyz, uint32_t n, const uint32_t* id, Vec4<Real>* pos,
-                         Vec4<Real>* vel, cudaStream_t s);
+                         Vec4<Real>* vel, cudaStream_t s, bool set_vel = true);
 template <class Real>
 void launch_unpack_boundary(const float* xyz, const float* psi, uint32_t n, Vec4<Real>* bpos, Vec4<Real>* bvel,
                             cudaStream_t s);
