@@ -103,6 +103,34 @@ __global__ void __launch_bounds__(kBlock) cell_bounds_kernel(const uint32_t* __r
 // One thread per fluid particle: fluid neighbours (self excluded) then boundary neighbours, cells in
 // a fixed order (z, y, x from -1 to +1), particles of a cell in sorted order. Lists are written
 // interleaved (nbr[k * stride + i]) so that the gathers read them coalesced.
+// Appends the candidates [j0, j1) of one cell that lie within H of particle i, in index order (the
+// fluid skips i itself). The positions are loaded kScanBatch at a time so that several loads are in
+// flight per thread; the tests and appends keep the order of a one-at-a-time loop.
+constexpr uint32_t kScanBatch = 4;
+template <class Real, bool kFluid>
+__device__ __forceinline__ void scan_cell(const Vec4<Real>* __restrict__ src, uint32_t j0, uint32_t j1, uint32_t i,
+                                          const Vec4<Real>& xi, Real H2, uint32_t* __restrict__ nbr, uint32_t stride,
+                                          uint32_t cap, uint32_t& total, uint32_t& cnt, bool& overflow) {
+    for (uint32_t jb = j0; jb < j1; jb += kScanBatch) {
+        Vec4<Real> xj[kScanBatch];
+#pragma unroll
+        for (uint32_t u = 0; u < kScanBatch; ++u) xj[u] = ld4<Real>(src + min(jb + u, j1 - 1));
+#pragma unroll
+        for (uint32_t u = 0; u < kScanBatch; ++u) {
+            const uint32_t j = jb + u;
+            if (j < j1 && (!kFluid || j != i) && pair_within(xi.x, xi.y, xi.z, xj[u].x, xj[u].y, xj[u].z, H2)) {
+                if (total < cap) {
+                    nbr[(size_t)total * stride + i] = j;
+                    ++total;
+                    ++cnt;
+                } else {
+                    overflow = true;
+                }
+            }
+        }
+    }
+}
+
 template <class Real>
 __global__ void __launch_bounds__(kBlock) build_neighbors_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                  const uint2* __restrict__ ftab,
@@ -131,19 +159,7 @@ __global__ void __launch_bounds__(kBlock) build_neighbors_kernel(const DevState<
                     const int x = cx + dx;
                     if (x < 0 || x >= p.dim_x) continue;
                     const uint2 r = ftab[cell_linear(x, y, z, p.dim_x, p.dim_y)];
-                    for (uint32_t j = r.x; j < r.y; ++j) {
-                        if (j == i) continue;
-                        const Vec4<Real> xj = ld4<Real>(pos + j);
-                        if (pair_within(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z, H2)) {
-                            if (total < cap) {
-                                nbr[(size_t)total * stride + i] = j;
-                                ++total;
-                                ++nf;
-                            } else {
-                                overflow = true;
-                            }
-                        }
-                    }
+                    scan_cell<Real, true>(pos, r.x, r.y, i, xi, H2, nbr, stride, cap, total, nf, overflow);
                 }
             }
         }
@@ -158,18 +174,7 @@ __global__ void __launch_bounds__(kBlock) build_neighbors_kernel(const DevState<
                         const int x = cx + dx;
                         if (x < 0 || x >= p.dim_x) continue;
                         const uint2 r = btab[cell_linear(x, y, z, p.dim_x, p.dim_y)];
-                        for (uint32_t j = r.x; j < r.y; ++j) {
-                            const Vec4<Real> xj = ld4<Real>(bpos + j);
-                            if (pair_within(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z, H2)) {
-                                if (total < cap) {
-                                    nbr[(size_t)total * stride + i] = j;
-                                    ++total;
-                                    ++nb;
-                                } else {
-                                    overflow = true;
-                                }
-                            }
-                        }
+                        scan_cell<Real, false>(bpos, r.x, r.y, i, xi, H2, nbr, stride, cap, total, nb, overflow);
                     }
                 }
             }
