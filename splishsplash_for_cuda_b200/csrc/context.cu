@@ -125,6 +125,7 @@ public:
     bool use_graphs = true;
     cudaGraphExec_t g_loop[2] = {nullptr, nullptr};  // [0] divergence, [1] pressure
     uint32_t g_loop_n[2] = {0, 0};
+    int g_loop_u[2] = {0, 0};  // iterations laid out before the while node
     bool g_loop_keep = false;  // the loop graphs store unclamped residuals (learned warm start)
     bool vel_updated = false;  // dfsph_update_vel ran since the last external-force pass
 
@@ -861,42 +862,77 @@ public:
             if (g_loop[k]) cudaGraphExecDestroy(g_loop[k]);
             g_loop[k] = nullptr;
             g_loop_n[k] = 0;
+            g_loop_u[k] = 0;
         }
         return DFSPH_OK;
     }
 
-    // A while-loop graph: body = Jacobi pass + residual pass whose last block sets the condition.
-    int build_loop_graph(int kind) {
+    // Loop graph: the first u iterations (those the loop always runs: u = min(minimum iterations,
+    // max_iter)) as plain kernel nodes, then a while node whose body is one more Jacobi pass +
+    // residual pass. Every residual's last block sets the condition (it = iterations so far:
+    // continue while the mean residual is above the tolerance or it < the minimum, and it <
+    // max_iter); the condition is 0 at each launch, so with u = max_iter the while node never runs.
+    int build_loop_graph(int kind, int u) {
         cudaGraph_t g = nullptr;
         DF_CUDA(cudaGraphCreate(&g, 0));
         cudaGraphConditionalHandle handle;
-        DF_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+        DF_CUDA(cudaGraphConditionalHandleCreate(&handle, g, u > 0 ? 0u : 1u, cudaGraphCondAssignDefault));
+        auto iteration = [&]() {
+            if (kind == 0) {
+                launch_divergence_jacobi<Real>(ds, n, handle, true, stream, boundary_forces);
+                launch_divergence_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream, g_loop_keep);
+            } else {
+                launch_pressure_jacobi<Real>(ds, n, handle, true, stream, boundary_forces);
+                launch_pressure_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream, g_loop_keep);
+            }
+        };
+        g_pdl_off = true;  // graph kernel edges need no programmatic launch
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        std::vector<cudaGraphNode_t> lead;
+        if (u > 0) {
+            DF_CUDA(cudaStreamBeginCaptureToGraph(stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            for (int k = 0; k < u; ++k) iteration();
+            cudaStreamCaptureStatus cs;
+            const cudaGraphNode_t* cdeps = nullptr;
+            size_t nc = 0;
+            const cudaError_t ei = cudaStreamGetCaptureInfo(stream, &cs, nullptr, nullptr, &cdeps, &nc);
+            if (ei == cudaSuccess) lead.assign(cdeps, cdeps + nc);
+            cudaGraph_t captured = nullptr;
+            const cudaError_t ee = cudaStreamEndCapture(stream, &captured);
+            if (ei != cudaSuccess || ee != cudaSuccess || lead.empty()) {
+                g_pdl_off = false;
+                cudaGraphDestroy(g);
+                err = "loop graph capture failed";
+                return DFSPH_E_CUDA;
+            }
+            deps = lead.data();
+            ndeps = lead.size();
+        }
         cudaGraphNodeParams cp{};
         cp.type = cudaGraphNodeTypeConditional;
         cp.conditional.handle = handle;
         cp.conditional.type = cudaGraphCondTypeWhile;
         cp.conditional.size = 1;
         cudaGraphNode_t node;
-        DF_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        DF_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        g_pdl_off = true;  // the loop body is a graph: its kernel edges need no programmatic launch
-        if (kind == 0) {
-            launch_divergence_jacobi<Real>(ds, n, handle, true, stream, boundary_forces);
-            launch_divergence_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream, g_loop_keep);
-        } else {
-            launch_pressure_jacobi<Real>(ds, n, handle, true, stream, boundary_forces);
-            launch_pressure_residual<Real>(ds, n, false, 0.0, 0, 0, handle, true, stream, g_loop_keep);
+        cudaError_t e = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
+        if (e == cudaSuccess) {
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                iteration();
+                cudaGraph_t captured = nullptr;
+                e = cudaStreamEndCapture(stream, &captured);
+            }
         }
         g_pdl_off = false;
-        cudaGraph_t captured = nullptr;
-        DF_CUDA(cudaStreamEndCapture(stream, &captured));
         cudaGraphExec_t exec = nullptr;
-        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
         DF_CUDA(e);
         g_loop[kind] = exec;
         g_loop_n[kind] = n;
+        g_loop_u[kind] = u;
         return DFSPH_OK;
     }
 
@@ -909,7 +945,12 @@ public:
                 DF_TRY(invalidate_graphs());
                 g_loop_keep = keep;
             }
-            if (!g_loop[kind] || g_loop_n[kind] != n) DF_TRY(build_loop_graph(kind));
+            const int u = std::min(kind == 0 ? kMinItersV : kMinItersP, max_iter);
+            if (!g_loop[kind] || g_loop_n[kind] != n || g_loop_u[kind] != u) {
+                if (g_loop[kind]) cudaGraphExecDestroy(g_loop[kind]);
+                g_loop[kind] = nullptr;
+                DF_TRY(build_loop_graph(kind, u));
+            }
             DF_CUDA(cudaGraphLaunch(g_loop[kind], stream));
             launches += 1;
             return DFSPH_OK;
