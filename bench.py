@@ -250,7 +250,9 @@ def ablation_scene(workload: str):
 def learned_ablation(local, steps: int, workload: str = "column_64"):
     """Plain vs learned warm start on the same scene from the same state, each for `steps` steps;
     the second half is measured (the flow has developed by then). ms/step is the device time of each
-    step (CUDA events inside dfsph_step), online training rounds included."""
+    step (CUDA events inside dfsph_step), online training rounds included. "gated" is the learned
+    warm start behind its cost gate (learned passes only while the plain solver needs at least one
+    iteration per step above the minimum counts; plain probe windows included in the average)."""
     from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
 
     scene, walls = ablation_scene(workload)
@@ -258,13 +260,13 @@ def learned_ablation(local, steps: int, workload: str = "column_64"):
            "steps": steps, "measured_steps": f"{steps // 2}..{steps - 1}",
            "max_error_pct": scene.config.maxError, "moving_walls": walls is not None,
            "cfl": bool(scene.config.cflMethod)}
-    for mode in ("plain", "learned"):
+    for mode in ("plain", "learned", "gated"):
         d = DFSPHCUDA(scene, device=local)
         d.set_param("timing", 1)
         if walls is not None:  # the fluid follows the walls past the initial box: keep every particle
             d.set_param("remove_escaped", 0)
-        if mode == "learned":
-            d.set_learned_warm_start(True)
+        if mode != "plain":
+            d.set_learned_warm_start(True, gate=mode == "gated")
         its, itv, ms, bits, t = [], [], [], 0, 0.0
         for _ in range(steps):
             if walls is not None:
@@ -280,6 +282,10 @@ def learned_ablation(local, steps: int, workload: str = "column_64"):
                "divergence_iterations": round(float(np.mean(itv[w])), 2),
                "ms_per_step": round(float(np.mean(ms[w])), 4), "status_bits": int(bits),
                "simulated_s": round(t, 4)}
+        if mode == "gated":
+            rec.update(learned_steps=int(d.get_param("gate_learned_steps")),
+                       plain_steps=int(d.get_param("gate_plain_steps")),
+                       last_excess_iterations=round(d.get_param("gate_last_excess"), 3))
         if mode == "learned":
             solves = int(d.get_param("learned_solves_p"))
             kept = int(d.get_param("learned_kept_p"))
@@ -292,6 +298,7 @@ def learned_ablation(local, steps: int, workload: str = "column_64"):
     out["pressure_iteration_reduction"] = round(1 - out["learned"]["pressure_iterations"]
                                                 / out["plain"]["pressure_iterations"], 4)
     out["ms_per_step_reduction"] = round(1 - out["learned"]["ms_per_step"] / out["plain"]["ms_per_step"], 4)
+    out["gated_ms_per_step_reduction"] = round(1 - out["gated"]["ms_per_step"] / out["plain"]["ms_per_step"], 4)
     return out
 
 

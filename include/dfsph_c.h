@@ -230,8 +230,16 @@ int dfsph_on_step_end(dfsph_ctx* ctx);                                    /* onS
  * training step, default 1), "train_iters" (Adam steps per training, default 20), "train_batch"
  * (particles per training batch, 1..65536, default 4096), "learning_rate" (default 1e-3), "mlp_seed"
  * (re-initialises the network).
+ * Cost gate of the learned warm start: "learned_gate" (1: the learned passes run only while the plain
+ * warm start needs at least "gate_margin" iterations per step, pressure + divergence, above the
+ * solves' minimum counts, default 1; setting the key restarts the schedule with a probe), measured on
+ * plain steps: a probe of 2 settling + "gate_window" (default 10) steps after every "gate_period"
+ * (default 200) learned steps, or every "gate_recheck" (default 50) steps while gated off. One host
+ * read of the iteration counters per decision.
  * Read-only: "mlp_ready", "mlp_trainings", "mlp_adam_steps", "mlp_loss" (last batch loss),
- * "learned_solves_v|p" (solves that had a learned candidate), "learned_kept_v|p" (solves that kept it). */
+ * "learned_solves_v|p" (solves that had a learned candidate), "learned_kept_v|p" (solves that kept it),
+ * "gate_learned_steps", "gate_plain_steps" (steps the gate ran with and without the learned passes),
+ * "gate_last_excess" (iterations per step above the minimum at the last decision; -1 before any). */
 int dfsph_set_param(dfsph_ctx* ctx, const char* key, double value);
 int dfsph_get_param(dfsph_ctx* ctx, const char* key, double* value);
 

@@ -153,6 +153,22 @@ public:
     int adam_t = 0;
     uint64_t lsteps = 0, trainings = 0, kept_v = 0, kept_p = 0, solves_v = 0, solves_p = 0;
     uint32_t forced_warm = 0;             // learned candidates used without a probe this step
+    // Cost gate of the learned warm start. The learned passes (features, inference, both candidates,
+    // training) cost about one to two gather passes per step, so they pay only while the plain warm
+    // start leaves at least gate_margin iterations (pressure + divergence per step) above the solves'
+    // minimum counts. The gate measures the plain solver on plain steps: a probe window of
+    // kGateSettle + gate_window plain steps (the first kGateSettle unmeasured: the plain warm start
+    // recovers from a learned step) after every gate_period learned steps, or every gate_recheck
+    // steps while it keeps the learned passes off.
+    static constexpr int kGateSettle = 2;
+    bool gate = false;
+    int gate_period = 200, gate_window = 10, gate_recheck = 50;
+    double gate_margin = 1.0;
+    enum GatePhase { kGateSettling = 0, kGateProbe, kGateLearned, kGatePlain };
+    int gate_phase = kGateLearned, gate_left = 0, gate_len = 0;
+    uint32_t gate_it0 = 0, gate_itv0 = 0;
+    uint64_t gate_learned_steps = 0, gate_plain_steps = 0;
+    double gate_last_excess = -1.0;
     bool step_trained = false;
 
     // simple open boundary (OpenBoundariesSimple): surfaces, kept inflow samples and their scratch
@@ -1120,11 +1136,57 @@ public:
         return DFSPH_OK;
     }
 
+    int gate_sums(uint32_t& it, uint32_t& itv) {
+        LoopCtl c[2];
+        DF_CUDA(cudaMemcpyAsync(c, ctl, 2 * sizeof(LoopCtl), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        it = c[1].iter_sum;
+        itv = c[0].iter_sum;
+        return DFSPH_OK;
+    }
+
+    // Advances the gate's schedule by one step; use_learned says whether this step runs the learned
+    // passes. One host read of the iteration counters per phase change.
+    int gate_step(bool& use_learned) {
+        if (gate_left <= 0) {
+            if (gate_phase == kGateLearned) {  // probe: settle, then measure the plain solver
+                gate_phase = kGateSettling;
+                gate_left = kGateSettle;
+            } else if (gate_phase == kGateSettling) {
+                DF_TRY(gate_sums(gate_it0, gate_itv0));
+                gate_phase = kGateProbe;
+                gate_left = gate_len = std::max(gate_window, 1);
+            } else {  // a measured plain phase ended: decide
+                uint32_t it, itv;
+                DF_TRY(gate_sums(it, itv));
+                const bool div = sc.enable_divergence_solver != 0;
+                const double dp = (double)(it - gate_it0) / gate_len, dv = (double)(itv - gate_itv0) / gate_len;
+                const double minp = std::min(kMinItersP, sc.max_iterations);
+                const double minv = std::min(kMinItersV, sc.max_iterations_v);
+                gate_last_excess = (dp - minp) + (div ? dv - minv : 0.0);
+                if (gate_last_excess >= gate_margin) {
+                    gate_phase = kGateLearned;
+                    gate_left = std::max(gate_period, 1);
+                } else {
+                    gate_phase = kGatePlain;
+                    gate_left = gate_len = std::max(gate_recheck, 1);
+                    gate_it0 = it;
+                    gate_itv0 = itv;
+                }
+            }
+        }
+        use_learned = gate_phase == kGateLearned;
+        --gate_left;
+        ++(use_learned ? gate_learned_steps : gate_plain_steps);
+        return DFSPH_OK;
+    }
+
     int step(dfsph_step_stats* st) {
         DF_CHECK(grid_ready, DFSPH_E_STATE, "step before any boundary or fluid upload");
         if (!n) DF_TRY(flush_pending());
+        bool lp = learned && n > 0;
+        if (lp && gate) DF_TRY(gate_step(lp));
         if (timing) DF_CUDA(cudaEventRecord(ev0, stream));
-        const bool lp = learned && n > 0;
         forced_warm = 0;
         step_trained = false;
         if (lp) DF_CUDA(cudaMemsetAsync(status + 2, 0, sizeof(uint32_t), stream));
@@ -1924,6 +1986,15 @@ public:
             DF_CHECK(v > 0 && v <= 1, DFSPH_E_INVALID, "warm_start_damping must be in (0, 1]");
             damping = v;
         }
+        else if (k == "learned_gate") {
+            gate = v != 0;
+            gate_phase = kGateLearned;  // the schedule starts with a probe window
+            gate_left = 0;
+        }
+        else if (k == "gate_period") { DF_CHECK(v >= 1, DFSPH_E_INVALID, "gate_period must be >= 1"); gate_period = (int)v; }
+        else if (k == "gate_window") { DF_CHECK(v >= 1, DFSPH_E_INVALID, "gate_window must be >= 1"); gate_window = (int)v; }
+        else if (k == "gate_recheck") { DF_CHECK(v >= 1, DFSPH_E_INVALID, "gate_recheck must be >= 1"); gate_recheck = (int)v; }
+        else if (k == "gate_margin") { DF_CHECK(v >= 0, DFSPH_E_INVALID, "gate_margin must be >= 0"); gate_margin = v; }
         else if (k == "train_interval") { DF_CHECK(v >= 0, DFSPH_E_INVALID, "train_interval must be >= 0"); train_interval = (int)v; }
         else if (k == "train_start") { DF_CHECK(v >= 0, DFSPH_E_INVALID, "train_start must be >= 0"); train_start = (int)v; }
         else if (k == "train_iters") { DF_CHECK(v >= 0, DFSPH_E_INVALID, "train_iters must be >= 0"); train_iters = (int)v; }
@@ -1993,6 +2064,14 @@ public:
         else if (k == "remove_escaped") *v = remove_escaped ? 1 : 0;
         else if (k == "escaped_removed") *v = (double)escaped_removed;
         else if (k == "warm_start_damping") *v = damping;
+        else if (k == "learned_gate") *v = gate ? 1 : 0;
+        else if (k == "gate_period") *v = gate_period;
+        else if (k == "gate_window") *v = gate_window;
+        else if (k == "gate_recheck") *v = gate_recheck;
+        else if (k == "gate_margin") *v = gate_margin;
+        else if (k == "gate_learned_steps") *v = (double)gate_learned_steps;
+        else if (k == "gate_plain_steps") *v = (double)gate_plain_steps;
+        else if (k == "gate_last_excess") *v = gate_last_excess;
         else if (k == "train_interval") *v = train_interval;
         else if (k == "train_start") *v = train_start;
         else if (k == "train_iters") *v = train_iters;

@@ -20,6 +20,12 @@ namespace dfsph {
 
 namespace {
 
+// Neighbours per batch in the passes that carry both warm-start candidates.
+#ifndef DFSPH_DUAL_BATCH
+#define DFSPH_DUAL_BATCH 2
+#endif
+constexpr int kDualBatch = DFSPH_DUAL_BATCH;
+
 template <class Real> __device__ __forceinline__ Real rmax(Real a, Real b);
 template <> __device__ __forceinline__ float rmax<float>(float a, float b) { return fmaxf(a, b); }
 template <> __device__ __forceinline__ double rmax<double>(double a, double b) { return fmax(a, b); }
@@ -198,8 +204,8 @@ __device__ __forceinline__ void velocity_divergence2(const DevState<Real>* __res
     const uint32_t stride = p.nbr_stride;
     const Cubic<Real> K = p.kern;
     KSum<Real> sa, sb;
-    Vec4<Real> xj[kGatherBatch], va[kGatherBatch], vb[kGatherBatch];
-    visit_neighbors<kGatherBatch>(
+    Vec4<Real> xj[kDualBatch], va[kDualBatch], vb[kDualBatch];
+    visit_neighbors<kDualBatch>(
         nbr, stride, i, 0, nf, i,
         [&](int u, uint32_t j) {
             xj[u] = ld4<Real>(pos + j);
@@ -214,8 +220,8 @@ __device__ __forceinline__ void velocity_divergence2(const DevState<Real>* __res
         });
     if (nb) {
         const bool moving = p.boundary_moving != 0;
-        BNbr<Real> b[kGatherBatch];
-        visit_neighbors<kGatherBatch>(
+        BNbr<Real> b[kDualBatch];
+        visit_neighbors<kDualBatch>(
             nbr, stride, i, nf, nf + nb, 0u, [&](int u, uint32_t j) { load_bnbr(b[u], ds->bpos, ds->bvel, j, moving); },
             [&](int u) {
                 Real gx, gy, gz;
@@ -298,9 +304,9 @@ __device__ __forceinline__ void jacobi_sum2(const DevState<Real>* __restrict__ d
     const uint32_t* __restrict__ nbr = ds->nbr;
     const uint32_t stride = p.nbr_stride;
     const Cubic<Real> K = p.kern;
-    Vec4<Real> xj[kGatherBatch];
-    Real kja[kGatherBatch], kjb[kGatherBatch];
-    visit_neighbors<kGatherBatch>(
+    Vec4<Real> xj[kDualBatch];
+    Real kja[kDualBatch], kjb[kDualBatch];
+    visit_neighbors<kDualBatch>(
         nbr, stride, i, 0, nf, i,
         [&](int u, uint32_t j) {
             xj[u] = ld4<Real>(pos + j);
@@ -327,9 +333,9 @@ __device__ __forceinline__ void jacobi_sum2(const DevState<Real>* __restrict__ d
     if (nb && (ba || bb)) {
         const Vec4<Real>* __restrict__ bpos = ds->bpos;
         Real* __restrict__ bf = kForces ? ds->bforce : nullptr;
-        Vec4<Real> xb[kGatherBatch];
-        uint32_t jb[kGatherBatch];
-        visit_neighbors<kGatherBatch>(
+        Vec4<Real> xb[kDualBatch];
+        uint32_t jb[kDualBatch];
+        visit_neighbors<kDualBatch>(
             nbr, stride, i, nf, nf + nb, 0u,
             [&](int u, uint32_t j) {
                 xb[u] = ld4<Real>(bpos + j);
@@ -793,8 +799,12 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) probe_residual_kerne
 }
 
 // ---- both warm-start candidates in one pass (learned warm start with the plain fallback) ---------
-// Two sets of compensated sums need more registers than the single-candidate passes' 64.
-constexpr int kDualMinBlocks = 2;
+// Two sets of compensated sums fit the single-candidate passes' 64 registers (4 CTAs per SM) with
+// two neighbours per batch: on 2 M particles this beats 2-3 CTAs per SM at batch 2-4 by 1-4 %.
+#ifndef DFSPH_DUAL_MIN_BLOCKS
+#define DFSPH_DUAL_MIN_BLOCKS 4
+#endif
+constexpr int kDualMinBlocks = DFSPH_DUAL_MIN_BLOCKS;
 // The plain candidate (kappaVP / kappaP) goes to velP, the learned one (kappaVW / kappaW) to vel in
 // place; each velocity is the one the single-candidate pass would produce.
 template <class Real, bool kForces>

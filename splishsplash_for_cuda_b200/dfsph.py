@@ -395,14 +395,24 @@ class DFSPHCUDA:
     # ---- learned warm start (no reference counterpart) ------------------------------------------
     def set_learned_warm_start(self, on: bool = True, probe: bool = True, train_interval: int | None = None,
                                train_iters: int | None = None, train_batch: int | None = None,
-                               learning_rate: float | None = None) -> None:
+                               learning_rate: float | None = None, gate: bool | None = None,
+                               gate_period: int | None = None, gate_window: int | None = None,
+                               gate_margin: float | None = None, gate_recheck: int | None = None) -> None:
         """Switches the MLP warm start of both solvers on or off (step() only). With probe, each solve
         keeps the learned candidate only if its initial residual is not above the reference warm
-        start's. The network trains online every `train_interval` steps."""
+        start's. The network trains online every `train_interval` steps. With gate, the learned passes
+        run only while the plain warm start needs at least `gate_margin` iterations per step above the
+        solves' minimum (measured on a plain probe window of `gate_window` steps after every
+        `gate_period` learned steps, or over every `gate_recheck` steps while the gate keeps them
+        off)."""
         for key, val in (("train_interval", train_interval), ("train_iters", train_iters),
-                         ("train_batch", train_batch), ("learning_rate", learning_rate)):
+                         ("train_batch", train_batch), ("learning_rate", learning_rate),
+                         ("gate_period", gate_period), ("gate_window", gate_window), ("gate_margin", gate_margin),
+                         ("gate_recheck", gate_recheck)):
             if val is not None:
                 self.set_param(key, val)
+        if gate is not None:
+            self.set_param("learned_gate", 1 if gate else 0)
         self.set_param("warm_start_probe", 1 if probe else 0)
         self.set_param("learned_warm_start", 1 if on else 0)
 

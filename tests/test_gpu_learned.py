@@ -179,3 +179,36 @@ def test_learned_warm_start_cuts_iterations_on_stiff_column(cuda_lib):
     rp, rl = p.field("density").astype(np.float64), d.field("density").astype(np.float64)
     assert abs(rl.mean() - rp.mean()) <= 0.05 * rp.mean()
     assert abs(d.positions()[:, 1].max() - p.positions()[:, 1].max()) <= 0.25 * p.positions()[:, 1].max()
+
+
+def test_gate_off_phases_run_the_plain_passes(cuda_lib):
+    """With a margin no solve reaches, the cost gate keeps the learned passes off after its first
+    probe window: the run is bit-identical to the plain mode, the network never trains, and every
+    step is counted as a plain step."""
+    s = column_scene(counts=(8, 20, 8), time_step=0.002)
+    a, ia, va, _, _ = _run(s, 60, False)
+    d, ib, vb, wb, _ = _run(s, 60, True, gate=True, gate_period=20, gate_window=4, gate_recheck=10,
+                            gate_margin=1e9)
+    assert np.array_equal(ia, ib) and np.array_equal(va, vb) and not wb.any()
+    assert np.array_equal(a.positions(), d.positions()) and np.array_equal(a.velocities(), d.velocities())
+    assert d.get_param("gate_learned_steps") == 0 and d.get_param("gate_plain_steps") == 60
+    assert d.get_param("mlp_trainings") == 0
+    assert d.get_param("gate_last_excess") >= 0.0
+
+
+def test_gate_turns_learned_passes_on_for_stiff_column(cuda_lib):
+    """Once the column has settled its plain solver needs ~20 pressure iterations above the minimum:
+    the gate runs the learned passes between its probe windows and keeps most of the iteration cut.
+    (While the column still falls the plain solver sits near the minimum, so the first probes keep
+    the learned passes off for a few re-check periods.)"""
+    s = column_scene(counts=(10, 40, 10), time_step=0.002, max_error=0.01)
+    steps = 300
+    _, ip, _, _, _ = _run(s, steps, False)
+    d, ig, _, wg, bits = _run(s, steps, True, train_interval=25, gate=True, gate_period=100, gate_window=5,
+                              gate_recheck=20)
+    assert bits & (_capi.ST_PRESSURE_NOT_CONVERGED | _capi.ST_NONFINITE) == 0
+    assert d.get_param("gate_last_excess") >= 1.0
+    learned_steps, plain_steps = d.get_param("gate_learned_steps"), d.get_param("gate_plain_steps")
+    assert learned_steps + plain_steps == steps and learned_steps >= steps // 2
+    win = slice(150, steps)
+    assert ig[win].mean() <= 0.75 * ip[win].mean()
