@@ -7,8 +7,9 @@ solve, XSPH + gravity, CFL dt, pressure solve, position update.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 1..5]
 
-With N > 1 (torchrun) every rank runs an independent replica of the workload (the step does not
-shard across GPUs here) and the reported ms/step is the maximum over ranks.
+With N > 1 (torchrun) every rank runs an independent replica of the workload (one B200 holds the
+largest configuration, so the step is not sharded across GPUs) and the reported ms/step is the
+maximum over ranks.
 """
 from __future__ import annotations
 
