@@ -212,3 +212,26 @@ def test_gate_turns_learned_passes_on_for_stiff_column(cuda_lib):
     assert learned_steps + plain_steps == steps and learned_steps >= steps // 2
     win = slice(150, steps)
     assert ig[win].mean() <= 0.75 * ip[win].mean()
+
+
+def test_gate_parameters_and_divergence_off(cuda_lib):
+    """Gate parameters are validated and read back; with the divergence solver off the gate measures
+    the pressure solve alone, and a gated-off run is still bit-identical to the plain mode."""
+    s = column_scene(counts=(8, 20, 8), time_step=0.002)
+    d = DFSPHCUDA(s)
+    for key, bad in (("gate_period", 0), ("gate_window", 0), ("gate_recheck", 0), ("gate_margin", -1)):
+        with pytest.raises(_capi.DfsphError) as e:
+            d.set_param(key, bad)
+        assert e.value.code == _capi.DFSPH_E_INVALID
+    d.set_learned_warm_start(True, gate=True, gate_period=7, gate_window=3, gate_recheck=5, gate_margin=1e9)
+    assert (d.get_param("learned_gate"), d.get_param("gate_period"), d.get_param("gate_window"),
+            d.get_param("gate_recheck"), d.get_param("gate_margin")) == (1, 7, 3, 5, 1e9)
+    assert d.get_param("gate_last_excess") == -1.0
+    a = DFSPHCUDA(s)
+    for x in (a, d):
+        x.setEnableDivergenceSolver(False)
+    for _ in range(20):
+        sa, sd = a.step(), d.step()
+        assert sa.iterations == sd.iterations and sd.iterations_v == 0 and sd.warm_start == 0
+    assert np.array_equal(a.positions(), d.positions())
+    assert d.get_param("gate_plain_steps") == 20 and d.get_param("gate_last_excess") >= 0.0
