@@ -158,7 +158,8 @@ int dfsph_upload_fluid(dfsph_ctx* ctx, const float* xyz, const float* vxyz, cons
 
 /* Overwrites positions and velocities of the current n particles (given in id order) but keeps
  * their warm-start accumulators and the dt history: the host-in-the-loop way to edit a running
- * simulation without resetting it (DFSPHCData's dynamic-data upload). vxyz null sets the velocities
+ * simulation without resetting it (the write-side counterpart of DFSPHCData::readDynamicData,
+ * DFSPH_c_arrays_structure.cpp:1120; the reference has no fluid upload between steps). vxyz null sets the velocities
  * to zero. The copies are asynchronous: from page-locked host memory the buffers must stay unchanged
  * until the next call that waits (dfsph_step with stats, a read, dfsph_synchronize). The velocities
  * travel on a second stream and are applied inside the next step's binning, after its sort, or by
