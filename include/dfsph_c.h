@@ -383,9 +383,10 @@ int dfsph_body_wrench(dfsph_ctx* ctx, uint32_t n_bodies, const uint32_t* first, 
 /* Binary checkpoint of the complete solver state (no reference counterpart; the text snapshot above
  * drops the warm starts and the particle order): particles in their current internal order with
  * kappa and kappa_v, the boundary with psi, the dt history, the grid, the scene parameters and, when
- * the learned warm start is on, its totals, network weights, Adam state and scales. Loading into a
- * context created with at least the same capacities, the same neighbor_capacity and precision
- * resumes bit-identically. */
+ * the learned warm start is on, its totals, network weights, Adam state, scales and cost-gate
+ * schedule. Loading into a context created with at least the same capacities, the same
+ * neighbor_capacity and precision resumes bit-identically. Files of format version 1 (no gate
+ * schedule) still load. */
 int dfsph_checkpoint_save(dfsph_ctx* ctx, const char* path);
 int dfsph_checkpoint_load(dfsph_ctx* ctx, const char* path);
 

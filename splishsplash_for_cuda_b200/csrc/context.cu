@@ -1690,7 +1690,7 @@ public:
         std::ofstream f(path, std::ios::binary | std::ios::trunc);
         DF_CHECK(f.is_open(), DFSPH_E_INVALID, std::string("cannot open ") + path);
         f.write(kCkptMagic, 8);
-        put(f, (int32_t)1);
+        put(f, (int32_t)2);
         put(f, (int32_t)sizeof(Real));
         put(f, n);
         put(f, nb);
@@ -1721,6 +1721,14 @@ public:
             for (double v : {lr, damping}) put(f, v);
             for (uint64_t v : {lsteps, trainings, kept_v, kept_p, solves_v, solves_p}) put(f, v);
             put(f, mlp_seed);
+            // cost gate (version 2): its schedule, and the iterations counted so far in its phase
+            uint32_t it = 0, itv = 0;
+            DF_TRY(gate_sums(it, itv));
+            for (int32_t v : {(int32_t)gate, gate_period, gate_window, gate_recheck, gate_phase, gate_left, gate_len})
+                put(f, v);
+            for (uint32_t v : {it - gate_it0, itv - gate_itv0}) put(f, v);
+            for (double v : {gate_margin, gate_last_excess}) put(f, v);
+            for (uint64_t v : {gate_learned_steps, gate_plain_steps}) put(f, v);
         }
         DF_CHECK(f.good(), DFSPH_E_INVALID, std::string("write failed: ") + path);
         return DFSPH_OK;
@@ -1736,7 +1744,8 @@ public:
         int32_t version = 0, rbytes = 0;
         uint32_t cn = 0, cnb = 0;
         dfsph_scene csc{};
-        DF_CHECK(get(f, version) && version == 1 && get(f, rbytes) && get(f, cn) && get(f, cnb) && get(f, csc),
+        DF_CHECK(get(f, version) && (version == 1 || version == 2) && get(f, rbytes) && get(f, cn) && get(f, cnb) &&
+                     get(f, csc),
                  DFSPH_E_INVALID, "bad checkpoint header");
         DF_CHECK(rbytes == (int32_t)sizeof(Real), DFSPH_E_INVALID, "checkpoint precision differs from the context's");
         DF_CHECK(cn <= Nc && cnb <= Bc, DFSPH_E_INVALID, "checkpoint exceeds the context's capacities");
@@ -1807,6 +1816,31 @@ public:
             lr = dv[0];
             damping = dv[1];
             lsteps = uv[0]; trainings = uv[1]; kept_v = uv[2]; kept_p = uv[3]; solves_v = uv[4]; solves_p = uv[5];
+            if (version >= 2) {
+                int32_t gi[7];
+                uint32_t part[2];
+                double gd[2];
+                uint64_t gu[2];
+                for (int32_t& v : gi) DF_CHECK(get(f, v), DFSPH_E_INVALID, "truncated checkpoint");
+                for (uint32_t& v : part) DF_CHECK(get(f, v), DFSPH_E_INVALID, "truncated checkpoint");
+                for (double& v : gd) DF_CHECK(get(f, v), DFSPH_E_INVALID, "truncated checkpoint");
+                for (uint64_t& v : gu) DF_CHECK(get(f, v), DFSPH_E_INVALID, "truncated checkpoint");
+                gate = gi[0] != 0;
+                gate_period = gi[1];
+                gate_window = gi[2];
+                gate_recheck = gi[3];
+                gate_phase = gi[4];
+                gate_left = gi[5];
+                gate_len = gi[6];
+                gate_margin = gd[0];
+                gate_last_excess = gd[1];
+                gate_learned_steps = gu[0];
+                gate_plain_steps = gu[1];
+                uint32_t it = 0, itv = 0;  // this context's counters: keep the phase's partial sums
+                DF_TRY(gate_sums(it, itv));
+                gate_it0 = it - part[0];
+                gate_itv0 = itv - part[1];
+            }
             DF_TRY(upload_scales());
             launch_mlp_pack(mlp, stream);
             launches += 1;
@@ -1966,6 +2000,12 @@ public:
         else if (k == "h_past") { DF_TRY(pull_dt()); h_past = v; dt_changed = true; }
         else if (k == "inv_h") { DF_TRY(pull_dt()); inv_h = v; dt_changed = true; }
         else if (k == "iterations_sum") {  // clears both loops' iteration counters
+            if (gate) {  // the gate's start counts move with the counters (its partial sums stay)
+                uint32_t it = 0, itv = 0;
+                DF_TRY(gate_sums(it, itv));
+                gate_it0 -= it;
+                gate_itv0 -= itv;
+            }
             DF_CUDA(cudaMemsetAsync(&ctl[0].iter_sum, 0, sizeof(uint32_t), stream));
             DF_CUDA(cudaMemsetAsync(&ctl[1].iter_sum, 0, sizeof(uint32_t), stream));
         }

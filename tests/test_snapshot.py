@@ -97,27 +97,55 @@ def test_device_loads_reference_format_fixture(cuda_lib):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("learned", [False, True])
-def test_checkpoint_resume_bit_identical(cuda_lib, tmp_path, learned):
+@pytest.mark.parametrize("mode", ["plain", "learned", "gated"])
+def test_checkpoint_resume_bit_identical(cuda_lib, tmp_path, mode):
     """A run saved after 10 steps and resumed in a fresh context continues bit-identically (internal
     particle order, warm starts, dt history and, in the learned mode, the network and Adam state
-    are part of the checkpoint)."""
+    are part of the checkpoint; with the cost gate, its schedule and the iterations counted so far in
+    its current phase, saved here in the middle of a phase)."""
     from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
 
     s = synthetic_scene(1, counts=(14, 14, 14), cfl=True)
     a = DFSPHCUDA(s)
-    if learned:
-        a.set_learned_warm_start(True, train_interval=4, train_batch=512)
+    gate = dict(gate=True, gate_period=4, gate_window=3, gate_recheck=5, gate_margin=0.0) if mode == "gated" else {}
+    if mode != "plain":
+        a.set_learned_warm_start(True, train_interval=4, train_batch=512, **gate)
     for _ in range(10):
         a.step()
     path = tmp_path / "run.ckpt"
     a.checkpoint_save(path)
     sa = [a.step() for _ in range(10)]
     b = DFSPHCUDA(s)
+    b.step()  # the resumed context's own counters differ from the saved run's
     b.checkpoint_load(path)
     sb = [b.step() for _ in range(10)]
+    if mode == "gated":
+        for key in ("gate_learned_steps", "gate_plain_steps", "gate_last_excess"):
+            assert a.get_param(key) == b.get_param(key), key
+        assert 0 < a.get_param("gate_learned_steps") < 20
     assert [x.iterations for x in sa] == [x.iterations for x in sb]
     assert [x.h for x in sa] == [x.h for x in sb]
     assert np.array_equal(a.positions(), b.positions()) and np.array_equal(a.velocities(), b.velocities())
-    if learned:
+    if mode != "plain":
         assert np.array_equal(a.mlp_params(), b.mlp_params())
+
+
+@pytest.mark.gpu
+def test_gate_ignores_counter_reset(cuda_lib):
+    """Clearing the user-visible iteration counters in the middle of a gate phase leaves the gate's
+    decisions, and so the run, unchanged."""
+    from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
+
+    s = synthetic_scene(1, counts=(14, 14, 14), cfl=True)
+    runs = []
+    for reset in (False, True):
+        d = DFSPHCUDA(s)
+        d.set_learned_warm_start(True, train_interval=4, train_batch=512, gate=True, gate_period=4, gate_window=3,
+                                 gate_recheck=5, gate_margin=0.5)
+        for k in range(24):
+            d.step()
+            if reset and k % 7 == 3:
+                d.set_param("iterations_sum", 0)
+        runs.append((d.get_param("gate_learned_steps"), d.get_param("gate_last_excess"), d.positions()))
+    assert runs[0][:2] == runs[1][:2]
+    assert np.array_equal(runs[0][2], runs[1][2])
