@@ -112,8 +112,13 @@ enum dfsph_field {
     DFSPH_F_BOUNDARY_POSITION = 11, /* 3 per boundary particle                                     */
     DFSPH_F_NEIGHBOR_COUNTS = 12,   /* 2 per fluid particle: fluid count, boundary count (dtype 2)  */
     DFSPH_F_BOUNDARY_VELOCITY = 13, /* 3 per boundary particle (zero for a static boundary)         */
-    DFSPH_F_BOUNDARY_FORCE = 14     /* 3 per boundary particle: force of the fluid during the last step
+    DFSPH_F_BOUNDARY_FORCE = 14,    /* 3 per boundary particle: force of the fluid during the last step
                                        (set_param "boundary_forces" 1; DFSPH_core_cuda.cu:467-477) */
+    DFSPH_F_FEATURES = 15           /* 5 per fluid particle, f32 only, learned mode: the warm-start
+                                       network's inputs from the last density + alpha pass,
+                                       (rho - rho0)/rho0, rho_dot * alpha, neighbours / 64, and the
+                                       previous step's needed kappa and kappa_v (no reference
+                                       counterpart) */
 };
 #define DFSPH_DTYPE_F32 0
 #define DFSPH_DTYPE_F64 1
@@ -421,16 +426,18 @@ int dfsph_mlp_reset(dfsph_ctx* ctx, uint32_t seed);
 
 /* Allocation-free stable sort of cell keys (no counterpart in the reference: it exists for callers
  * that may not allocate device memory, e.g. a host framework that owns every allocation or a plugin
- * handed fixed device buffers). All pointers are device pointers owned by the caller: keys_in[n] is
- * read, keys_out[n] receives the keys in ascending order and perm_out[n] the original index of each
- * sorted key (equal keys keep their input order), sorting on the low key_bits bits (1..32). The
- * call performs no cudaMalloc/cudaFree: its scratch is a fixed device array built into the library
- * (about 2.6 MB on every GPU that loads it, held until the process exits) and n is limited to
- * 262,144 keys (larger n returns DFSPH_E_INVALID with a message in dfsph_last_error(NULL)). The
- * first call on a device looks up that array's device address, so make it before any stream
- * capture. Every call reuses the same array: calls that overlap on the GPU (other streams, other
- * threads) race and must be serialised by the caller. The call runs on `stream` (a cudaStream_t,
- * NULL = legacy default stream) and returns after the sort has finished. */
+ * handed fixed device buffers). All pointers are device pointers owned by the caller and must not
+ * overlap (DFSPH_E_INVALID otherwise): keys_in[n] is read, keys_out[n] receives the input keys,
+ * unchanged, in ascending order of their low key_bits bits (1..32; the bits above are carried but
+ * do not order), and perm_out[n] the original index of each (equal low bits keep their input order).
+ * The call performs no cudaMalloc/cudaFree: its scratch is a fixed device array built into the
+ * library (about 2.6 MB on every GPU that loads it, held until the process exits) and n is limited
+ * to 262,144 keys (larger n returns DFSPH_E_INVALID with a message in dfsph_last_error(NULL)). Each
+ * call looks up that array's device address on the current device. Every call reuses the same
+ * array: calls that overlap on the GPU (other streams, other threads) race and must be serialised by
+ * the caller. The call runs on `stream` (a cudaStream_t, NULL = legacy default stream) and returns
+ * after the sort has finished; it ends with a host wait, so it cannot be made while the stream is
+ * being captured into a graph (DFSPH_E_STATE). */
 int dfsph_sort_cell_keys_noalloc(const uint32_t* keys_in, uint32_t* keys_out, uint32_t* perm_out, uint32_t n,
                                  int key_bits, void* stream);
 

@@ -107,6 +107,73 @@ template <class Real> struct Cubic {
     }
 };
 
+// Density terms m_j W_ij of the FP32 instance as double-float pairs (hi + lo), the same
+// error-free transformations as the device's density_term (dfsph_common.cuh): TwoSum, Fast2Sum and
+// the FMA product error on FP32 values. The FP64 instance evaluates the terms directly.
+struct F2 {
+    float h, l;
+};
+inline F2 f2_two_sum(float a, float b) {
+    const float s = a + b, bb = s - a;
+    return {s, (a - (s - bb)) + (b - bb)};
+}
+inline F2 f2_fast_two_sum(float a, float b) {
+    const float s = a + b;
+    return {s, b - (s - a)};
+}
+inline F2 f2_mul(F2 a, F2 b) {
+    const float p = a.h * b.h;
+    float e = std::fmaf(a.h, b.h, -p);
+    e = std::fmaf(a.h, b.l, e);
+    e = std::fmaf(a.l, b.h, e);
+    return f2_fast_two_sum(p, e);
+}
+inline F2 f2_mul_f(F2 a, float b) {
+    const float p = a.h * b;
+    return f2_fast_two_sum(p, std::fmaf(a.l, b, std::fmaf(a.h, b, -p)));
+}
+inline F2 f2_split(double v) {
+    const float h = (float)v;
+    return {h, (float)(v - (double)h)};
+}
+struct DensityTerms {
+    F2 ih2{}, k{}, k2{};
+    void set(double H) {
+        ih2 = f2_split(1.0 / (H * H));
+        k = f2_split(8.0 / (M_PI * H * H * H));
+        k2 = f2_split(16.0 / (M_PI * H * H * H));
+    }
+    // m W(r): |r|^2, q^2, q (one Newton correction of the FP32 root), the cubic and the product with
+    // m, each as a pair.
+    F2 term(float rx, float ry, float rz, float m) const {
+        const float a = rx * rx, b = ry * ry, c = rz * rz;
+        const float ea = std::fmaf(rx, rx, -a), eb = std::fmaf(ry, ry, -b), ec = std::fmaf(rz, rz, -c);
+        const F2 s1 = f2_two_sum(a, b), s2 = f2_two_sum(s1.h, c);
+        const F2 r2 = f2_fast_two_sum(s2.h, ((ea + eb) + ec) + (s1.l + s2.l));
+        const F2 q2 = f2_mul(r2, ih2);
+        if (q2.h > 1.0f) return {0.0f, 0.0f};
+        F2 W = k;
+        if (q2.h > 0.0f) {
+            const float qh = std::sqrt(q2.h);
+            const F2 q = f2_fast_two_sum(qh, (std::fmaf(-qh, qh, q2.h) + q2.l) * (0.5f / qh));
+            if (q.h > 1.0f) return {0.0f, 0.0f};
+            if (q.h <= 0.5f) {
+                F2 t = f2_two_sum(q.h, -1.0f);
+                t = f2_fast_two_sum(t.h, t.l + q.l);
+                const F2 v = f2_mul_f(f2_mul(q2, t), 6.0f);
+                F2 P = f2_two_sum(1.0f, v.h);
+                P = f2_fast_two_sum(P.h, P.l + v.l);
+                W = f2_mul(P, k);
+            } else {
+                F2 f = f2_two_sum(1.0f, -q.h);
+                f = f2_fast_two_sum(f.h, f.l - q.l);
+                W = f2_mul(f2_mul(f2_mul(f, f), f), k2);
+            }
+        }
+        return f2_mul_f(W, m);
+    }
+};
+
 // Layout of the C ABI's dfsph_surface (restated; BufferFluidSurface's fields).
 struct Surface {
     int32_t type, reversed;
@@ -207,12 +274,17 @@ struct Params {
 template <class Real> struct Oracle {
     Params prm{};
     Cubic<Real> K;
+    DensityTerms DT;
     float Hf = 0, H2f = 0;
     int off[3] = {0, 0, 0}, dim[3] = {0, 0, 0};
     bool grid = false;
     // fluid (original order)
     uint32_t n = 0;
     std::vector<Real> x, v, m, rho, alpha, dadv, kap, kapv, a, kc;
+    // Warm starts applied and last unclamped residuals of the step's two solves, for the coefficients
+    // each solve needed (the learned warm start's training targets and network inputs).
+    std::vector<Real> kw_p, kw_v, raw_p, raw_v;
+    bool div_ran = false;
     // boundary
     uint32_t nb = 0;
     std::vector<Real> bx, bv, psi;
@@ -233,6 +305,7 @@ template <class Real> struct Oracle {
     void init(const Params& p) {
         prm = p;
         K.set((double)(float)(4.0 * p.particle_radius));
+        DT.set((double)(float)(4.0 * p.particle_radius));
         Hf = (float)(4.0 * p.particle_radius);
         H2f = Hf * Hf;
         time_step = p.time_step;
@@ -560,16 +633,26 @@ template <class Real> struct Oracle {
             if (warm_v) kapv[i] = std::max<Real>(kapv[i] * hr / Real(2), Real(-0.5));
             // rho - rho0 accumulated directly (the device kernels do the same; see density_alpha_kernel)
             Neumaier<Real> r;
+            float r_lo = 0.0f;
             Kahan<Real> sgk, dr, gx, gy, gz;
             r.add((Real)-prm.density0);
-            r.add(m[i] * K.W0);
+            auto add_term = [&](Real rx, Real ry, Real rz, Real mj, Real w) {
+                if (sizeof(Real) == 4) {
+                    const F2 t = DT.term((float)rx, (float)ry, (float)rz, (float)mj);
+                    r.add((Real)t.h);
+                    r_lo += t.l;
+                } else {
+                    r.add(mj * w);
+                }
+            };
+            add_term(0, 0, 0, m[i], K.W0);
             const Real xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
             const Real vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2];
             for (uint32_t j : nf[i]) {
                 const Real rx = xi - x[3 * j], ry = yi - x[3 * j + 1], rz = zi - x[3 * j + 2];
                 Real w = K.W(rx, ry, rz), g0, g1, g2;
                 K.gradW(rx, ry, rz, g0, g1, g2);
-                r.add(m[j] * w);
+                add_term(rx, ry, rz, m[j], w);
                 const Real px = m[j] * g0, py = m[j] * g1, pz = m[j] * g2;
                 sgk.add(px * px + py * py + pz * pz);
                 gx.add(px); gy.add(py); gz.add(pz);
@@ -579,7 +662,7 @@ template <class Real> struct Oracle {
                 const Real rx = xi - bx[3 * j], ry = yi - bx[3 * j + 1], rz = zi - bx[3 * j + 2];
                 Real w = K.W(rx, ry, rz), g0, g1, g2;
                 K.gradW(rx, ry, rz, g0, g1, g2);
-                r.add(psi[j] * w);
+                add_term(rx, ry, rz, psi[j], w);
                 const Real px = psi[j] * g0, py = psi[j] * g1, pz = psi[j] * g2;
                 sgk.add(px * px + py * py + pz * pz);
                 gx.add(px); gy.add(py); gz.add(pz);
@@ -588,7 +671,7 @@ template <class Real> struct Oracle {
             const Real Gx = gx.value(), Gy = gy.value(), Gz = gz.value();
             const Real sg = sgk.value() + (Gx * Gx + Gy * Gy + Gz * Gz);
             alpha[i] = -invh / std::max<Real>(sg, (Real)kEps);
-            rho[i] = r.value();  // rho - rho0
+            rho[i] = r.value() + (Real)r_lo;  // rho - rho0
             uint32_t num = (uint32_t)nf[i].size();
             if (num < kMinNeighbors) num += (uint32_t)nbd[i].size();
             dadv[i] = (num < kMinNeighbors) ? Real(0) : std::max<Real>(dr.value(), Real(0));
@@ -666,7 +749,8 @@ template <class Real> struct Oracle {
             if (init) kapv[i] = 0;
             uint32_t num = (uint32_t)nf[i].size();
             if (num < kMinNeighbors) num += (uint32_t)nbd[i].size();
-            dadv[i] = (num < kMinNeighbors) ? Real(0) : std::max<Real>(velocity_divergence(i), Real(0));
+            raw_v[i] = (num < kMinNeighbors) ? Real(0) : velocity_divergence(i);
+            dadv[i] = std::max<Real>(raw_v[i], Real(0));
             kc[i] = dadv[i] * alpha[i];
         }
         double sum = 0;
@@ -681,6 +765,9 @@ template <class Real> struct Oracle {
             return 0;
         }
         density_alpha(true);
+        kw_v = kapv;
+        raw_v.assign(n, Real(0));
+        div_ran = true;
         jacobi([&](uint32_t j) { return kapv[j]; }, (Real)h, [&](uint32_t i) { return !(dadv[i] > Real(0)); });
         init_err_v = divergence_residual(true);
         const double eta = max_error * 0.01 * prm.density0 / h;
@@ -754,7 +841,8 @@ template <class Real> struct Oracle {
                 alpha[i] *= (Real)inv_h_future;
                 kap[i] = 0;
             }
-            dadv[i] = std::max<Real>(rho[i] + hf * velocity_divergence(i), Real(0));  // rho[] = rho - rho0
+            raw_p[i] = rho[i] + hf * velocity_divergence(i);  // rho[] = rho - rho0
+            dadv[i] = std::max<Real>(raw_p[i], Real(0));
             kc[i] = dadv[i] * alpha[i];
             kap[i] += kc[i];
         }
@@ -769,6 +857,8 @@ template <class Real> struct Oracle {
             last_err = 0;
             return 0;
         }
+        kw_p = kap;
+        raw_p.assign(n, Real(0));
         jacobi([&](uint32_t j) { return kap[j]; }, (Real)h_future, [](uint32_t) { return false; });
         init_err = pressure_residual(true);
         const double eta = max_error * 0.01 * prm.density0;
@@ -794,7 +884,22 @@ template <class Real> struct Oracle {
         inv_h = inv_h_future;
     }
 
+    // Pressure (which = 0) or divergence (1) coefficient the last solve needed, per particle
+    // (needed_totals of the device's solver.cu): the applied total, warm start plus corrections, less
+    // one Jacobi estimate min(r, 0) alpha of its excess, clamped to [-0.5, 0]. alpha here is the
+    // pressure solve's alpha / h_future; the divergence solve's alpha is that times h_future.
+    double needed(int which, uint32_t i) const {
+        auto clampk = [](double k) { return std::min(std::max(k, -0.5), 0.0); };
+        if (which == 0) {
+            if (kw_p.size() != n || raw_p.size() != n) return 0.0;
+            return clampk((double)(kw_p[i] + kap[i] + std::min<Real>(raw_p[i], Real(0)) * alpha[i]));
+        }
+        if (!div_ran || kw_v.size() != n || raw_v.size() != n) return 0.0;
+        return clampk((double)(kw_v[i] + kapv[i] + std::min<Real>(raw_v[i], Real(0)) * (alpha[i] * (Real)h_future)));
+    }
+
     void step() {
+        div_ran = false;
         neighbors();
         if (prm.enable_divergence_solver) divergence_solve(prm.max_iterations_v, prm.max_error_v);
         else {
@@ -1005,6 +1110,10 @@ int oracle_get(void* h, int field, double* out) {
             case 10: return put(o.psi);
             case 11: return put(o.bx);
             case 14: return o.bforce_on ? put(o.bF) : -1;
+            case 20:  // needed pressure coefficient of the last solve (not a C ABI field)
+            case 21:  // needed divergence coefficient
+                for (uint32_t i = 0; i < o.n; ++i) out[i] = o.needed(field - 20, i);
+                return 0;
             default: return -1;
         }
     })());

@@ -12,7 +12,8 @@ LIB = HERE / "liboracle_dfsph.so"
 
 FIELD_IDS = {"position": (0, 3), "velocity": (1, 3), "mass": (2, 1), "density": (3, 1), "factor": (4, 1),
              "density_adv": (5, 1), "kappa": (6, 1), "kappa_v": (7, 1), "acceleration": (8, 3),
-             "boundary_psi": (10, 1), "boundary_position": (11, 3), "boundary_force": (14, 3)}
+             "boundary_psi": (10, 1), "boundary_position": (11, 3), "boundary_force": (14, 3),
+             "kappa_needed": (20, 1), "kappa_v_needed": (21, 1)}
 
 
 class OracleParams(C.Structure):

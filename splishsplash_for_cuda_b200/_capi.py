@@ -61,6 +61,7 @@ FIELDS = {
     "neighbor_counts": (12, 2),
     "boundary_velocity": (13, 3),
     "boundary_force": (14, 3),
+    "features": (15, 5),
 }
 DTYPE_F32, DTYPE_F64, DTYPE_U32 = 0, 1, 2
 ORDER_ID, ORDER_SORTED = 0, 1

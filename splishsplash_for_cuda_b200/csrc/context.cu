@@ -136,6 +136,9 @@ public:
     // per-particle buffers when the mode is first enabled; the plain path touches neither.
     static constexpr uint32_t kMaxTrainBatch = 1u << 16;
     bool learned = false, mlp_ready = false, scales_set = false, probe = true;
+    // Ablation of the learned warm start: the needed-coefficient base with the network's correction
+    // fixed at zero (no inference, no training).
+    bool base_only = false;
     Real* kappaT[2] = {nullptr, nullptr};
     Real* kappaVT[2] = {nullptr, nullptr};
     Real *kappaW = nullptr, *kappaVW = nullptr, *kappaP = nullptr, *kappaVP = nullptr;
@@ -335,6 +338,13 @@ public:
         p.kern.k = (Real)(8.0 / (M_PI * H * H * H));
         p.kern.l = (Real)(48.0 / (M_PI * H * H * H));
         p.kern.W0 = p.kern.k;
+        auto split = [](double v, float& hi, float& lo) {
+            hi = (float)v;
+            lo = (float)(v - (double)hi);
+        };
+        split(1.0 / (H * H), p.kern.ih2_h, p.kern.ih2_l);
+        split(8.0 / (M_PI * H * H * H), p.kern.k_h, p.kern.k_l);
+        split(16.0 / (M_PI * H * H * H), p.kern.k2_h, p.kern.k2_l);
         p.H2 = (Real)(Hf * Hf);
         p.density0 = (Real)sc.density0;
         p.viscosity = (Real)sc.viscosity;
@@ -998,11 +1008,11 @@ public:
             launch_divergence_residual<Real>(ds, n, true, eta, kMinItersV, max_iter, 0, false, stream);
             launches += 3;
         } else {
-            const bool use = mlp_ready;
+            const bool infer = mlp_ready && !base_only, use = infer || base_only;
             launch_density_alpha<Real>(ds, n, false, true, stream);
-            if (use) launch_mlp_forward(mlp, features, n, pred, status, stream);
-            launch_warm_values<Real>(ds, n, 0, use, damping, stream);
-            launches += use ? 3 : 2;
+            if (infer) launch_mlp_forward(mlp, features, n, pred, status, stream);
+            launch_warm_values<Real>(ds, n, 0, use, infer, damping, stream);
+            launches += infer ? 3 : 2;
             if (use && probe) {  // both candidates per pass, then the selection
                 launch_warm_dual<Real>(ds, n, 0, false, stream, boundary_forces);
                 launch_residual_dual<Real>(ds, n, 0, eta, kMinItersV, max_iter, stream);
@@ -1031,8 +1041,8 @@ public:
             launch_pressure_residual<Real>(ds, n, true, eta, kMinItersP, max_iter, 0, false, stream);
             launches += 2;
         } else {
-            const bool use = mlp_ready;
-            launch_warm_values<Real>(ds, n, 1, use, damping, stream);
+            const bool infer = mlp_ready && !base_only, use = infer || base_only;
+            launch_warm_values<Real>(ds, n, 1, use, infer, damping, stream);
             launches += 1;
             if (use && probe) {
                 launch_warm_dual<Real>(ds, n, 1, fused_vel, stream, boundary_forces);
@@ -1200,7 +1210,7 @@ public:
             if (lp) {  // no divergence solve: its warm-start arrays stay zero
                 DF_CUDA(cudaMemsetAsync(kappaVW, 0, (size_t)n * sizeof(Real), stream));
                 DF_CUDA(cudaMemsetAsync(kappaV[cur], 0, (size_t)n * sizeof(Real), stream));
-                if (mlp_ready) {
+                if (mlp_ready && !base_only) {
                     launch_mlp_forward(mlp, features, n, pred, status, stream);
                     launches += 1;
                 }
@@ -1219,7 +1229,7 @@ public:
             const bool due = train_interval > 0 &&
                              (lsteps == (uint64_t)train_start ||
                               (lsteps > (uint64_t)train_start && (lsteps - train_start) % train_interval == 0));
-            if (due && train_iters > 0) DF_TRY(train_online(div));
+            if (due && train_iters > 0 && !base_only) DF_TRY(train_online(div));
             launch_totals<Real>(ds, n, div, stream);
             launches += 1;
             ++lsteps;
@@ -1554,6 +1564,18 @@ public:
                 src = bforce; sstride = 4; comps = 3; count = nb;
                 idmap = (order == DFSPH_ORDER_ID) ? bid : nullptr;
                 break;
+            case DFSPH_F_FEATURES: {
+                DF_CHECK(features, DFSPH_E_STATE, "warm-start features exist only after a learned-mode step");
+                DF_CHECK(dtype == DFSPH_DTYPE_F32, DFSPH_E_INVALID, "features download as f32");
+                DF_CHECK(n_elems >= (size_t)n * kMlpFeatures, DFSPH_E_INVALID, "output buffer too small");
+                if (!n) return DFSPH_OK;
+                launch_pack_field<float, float>(features, kMlpIn, kMlpFeatures, idmap, n, (float*)dl, stream);
+                launches += 1;
+                DF_CUDA(cudaMemcpyAsync(out, dl, (size_t)n * kMlpFeatures * sizeof(float), cudaMemcpyDeviceToHost,
+                                        stream));
+                DF_CUDA(cudaStreamSynchronize(stream));
+                return DFSPH_OK;
+            }
             case DFSPH_F_ID:
             case DFSPH_F_NEIGHBOR_COUNTS: {
                 DF_CHECK(dtype == DFSPH_DTYPE_U32, DFSPH_E_INVALID, "id and neighbour counts download as u32");
@@ -2012,6 +2034,7 @@ public:
         else if (k == "timing") timing = v != 0;
         else if (k == "learned_warm_start") return enable_learned(v != 0);
         else if (k == "warm_start_probe") probe = v != 0;
+        else if (k == "learned_base_only") base_only = v != 0;
         else if (k == "sort_withhold_tile") sort_withheld_tile = v < 0 ? kNoWithheldTile : (uint32_t)v;
         else if (k == "remove_escaped") remove_escaped = v != 0;
         else if (k == "boundary_forces") {
@@ -2100,6 +2123,7 @@ public:
         else if (k == "iterations_v") *v = last_iters_v;
         else if (k == "learned_warm_start") *v = learned ? 1 : 0;
         else if (k == "warm_start_probe") *v = probe ? 1 : 0;
+        else if (k == "learned_base_only") *v = base_only ? 1 : 0;
         else if (k == "boundary_forces") *v = boundary_forces ? 1 : 0;
         else if (k == "remove_escaped") *v = remove_escaped ? 1 : 0;
         else if (k == "escaped_removed") *v = (double)escaped_removed;

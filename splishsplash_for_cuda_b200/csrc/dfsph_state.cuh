@@ -98,7 +98,7 @@ void launch_probe_residual(const DevState<Real>* d, uint32_t n, int which, const
 // (reference) candidate to kappaVP / kappaP and, when learned, the learned one to kappa_v + kappaVW /
 // kappaW (otherwise the plain one there too).
 template <class Real>
-void launch_warm_values(const DevState<Real>* d, uint32_t n, int which, bool learned, double damping,
+void launch_warm_values(const DevState<Real>* d, uint32_t n, int which, bool learned, bool use_pred, double damping,
                         cudaStream_t s);
 // kappaT / kappaVT = the pressure / divergence coefficients this step's solves needed: applied
 // totals (warm start + corrections) less the excess the unclamped final residuals show.

@@ -3,6 +3,7 @@
 #include <cuda_bf16.h>
 
 #include "mlp.cuh"
+#include "mma_phases.h"
 #include "dfsph_common.cuh"
 
 namespace dfsph {
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(kMmaM) mlp_forward_kernel(const uint16_t* __re
     const uint32_t tmem = *tslot;
     const uint32_t trow = tmem + ((warp * 32u) << 16);  // this warp's 32 TMEM lanes
     const uint32_t idesc64 = umma_idesc(kMmaM, 64), idesc16 = umma_idesc(kMmaM, 16);
-    uint32_t phase = 0;
+    MmaPhases ph;  // tid 0's copy decides the drain below
     bool ok = true;
 
     for (uint32_t tile = blockIdx.x; tile * kMmaM < n && ok; tile += gridDim.x) {
@@ -211,8 +212,12 @@ __global__ void __launch_bounds__(kMmaM) mlp_forward_kernel(const uint16_t* __re
             umma_bf16(tmem + 0, umma_desc(s_base + kSA, 128, 256), umma_desc(s_base + kSW1, 128, 256), idesc64, 0);
             umma_commit(bar_addr);
         }
-        ok = __all_sync(0xFFFFFFFFu, mbar_wait(bar_addr, phase));  // warp-uniform for tcgen05.ld
-        phase ^= 1u;
+        {
+            ph.committed();
+            const bool done = mbar_wait(bar_addr, ph.phase);
+            ph.waited(done);
+            ok = __all_sync(0xFFFFFFFFu, done);  // warp-uniform for tcgen05.ld
+        }
         tc_fence_after();
         if (ok) epilogue64(trow, 0, sb1, sa, tid);  // layer-1 activations -> A operand (K = 64)
         async_proxy_fence();
@@ -225,8 +230,12 @@ __global__ void __launch_bounds__(kMmaM) mlp_forward_kernel(const uint16_t* __re
                           umma_desc(s_base + kSW2 + 256 * k, 128, 1024), idesc64, k > 0);
             umma_commit(bar_addr);
         }
-        if (ok) ok = __all_sync(0xFFFFFFFFu, mbar_wait(bar_addr, phase));
-        phase ^= 1u;
+        if (ok) {
+            ph.committed();
+            const bool done = mbar_wait(bar_addr, ph.phase);
+            ph.waited(done);
+            ok = __all_sync(0xFFFFFFFFu, done);
+        }
         tc_fence_after();
         if (ok) epilogue64(trow, 64, sb2, sa, tid);  // layer-2 activations -> A operand
         async_proxy_fence();
@@ -239,8 +248,12 @@ __global__ void __launch_bounds__(kMmaM) mlp_forward_kernel(const uint16_t* __re
                           umma_desc(s_base + kSW3 + 256 * k, 128, 1024), idesc16, k > 0);
             umma_commit(bar_addr);
         }
-        if (ok) ok = __all_sync(0xFFFFFFFFu, mbar_wait(bar_addr, phase));
-        phase ^= 1u;
+        if (ok) {
+            ph.committed();
+            const bool done = mbar_wait(bar_addr, ph.phase);
+            ph.waited(done);
+            ok = __all_sync(0xFFFFFFFFu, done);
+        }
         tc_fence_after();
         if (ok) {
             float v[16];
@@ -253,8 +266,10 @@ __global__ void __launch_bounds__(kMmaM) mlp_forward_kernel(const uint16_t* __re
         ok = __syncthreads_and(ok);
     }
     if (!ok && tid == 0) atomicOr(status, DFSPH_ST_MMA_TIMEOUT);
-    // (a wait that gave up leaves at most one MMA group in flight: give it the same bounded time)
-    if (!ok && tid == 0) mbar_wait(bar_addr, phase ^ 1u);
+    // A wait that gave up leaves at most one MMA group in flight: the one thread 0 committed and did
+    // not see complete. Give it the same bounded time before the tensor memory is freed.
+    uint32_t drain_parity;
+    if (tid == 0 && ph.drain(drain_parity)) mbar_wait(bar_addr, drain_parity);
     __syncthreads();
     tc_fence_after();
     if (warp == 0)

@@ -21,6 +21,7 @@
 namespace dfsph {
 
 constexpr int kMlpIn = 8;       // 5 features + 3 zero pads
+constexpr int kMlpFeatures = 5;
 constexpr int kMlpHidden = 64;
 constexpr int kMlpOut = 2;
 // parameter layout of the FP32 master copy (row-major [out][in])

@@ -13,6 +13,8 @@
 // reference, :774-781 and :1321-1325) are fused into the residual kernels as deterministic FP64
 // block reductions whose last block evaluates the loop condition on the device (and, inside a CUDA
 // graph, sets the while-node condition), so no host round trip happens per iteration.
+#include <type_traits>
+
 #include "dfsph_state.cuh"
 #include "io.cuh"
 
@@ -390,15 +392,30 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
     // rho - rho0 is accumulated directly (rest density first, then the self term and the neighbour
     // terms) so that the density residual rho + h*div - rho0 of the pressure solve never subtracts
     // two numbers of ~1e3 in FP32 (the reference forms rho, then rho + h*div - rho0).
+    // FP32 build: each density term m_j W_ij is formed as a double-float pair (density_term); the
+    // hi parts go to the compensated sum, the lo parts to rho_lo. FP64 build: plain terms.
+    constexpr bool kPairTerms = std::is_same<Real, float>::value;
     NSum<Real> rho;
+    float rho_lo = 0.0f;
     KSum<Real> sgk, drho;
     KSum3<Real> gpi;
     rho.add(-p.density0);
-    rho.add(xi.w * K.W0);
+    auto add_term = [&](Real rx, Real ry, Real rz, Real m, Real w) {
+        if constexpr (kPairTerms) {
+            const F2 t = density_term(K, rx, ry, rz, m);
+            rho.add(t.h);
+            rho_lo = __fadd_rn(rho_lo, t.l);
+        } else {
+            rho.add(m * w);
+        }
+    };
+    add_term(Real(0), Real(0), Real(0), xi.w, K.W0);
     auto accumulate = [&](const Vec4<Real>& xj, Real vx, Real vy, Real vz) {
         Real w, gx, gy, gz;
-        K.W_gradW(xi.x - xj.x, xi.y - xj.y, xi.z - xj.z, w, gx, gy, gz);
-        rho.add(xj.w * w);
+        const Real rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+        if constexpr (kPairTerms) K.gradW(rx, ry, rz, gx, gy, gz), w = Real(0);
+        else K.W_gradW(rx, ry, rz, w, gx, gy, gz);
+        add_term(rx, ry, rz, xj.w, w);
         const Real px = xj.w * gx, py = xj.w * gy, pz = xj.w * gz;
         sgk.add(px * px + py * py + pz * pz);
         gpi.add(px, py, pz);
@@ -424,7 +441,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
     const Real gx = gpi.x.value(), gy = gpi.y.value(), gz = gpi.z.value();
     const Real sg = sgk.value() + (gx * gx + gy * gy + gz * gz);
     const Real alpha = -p.inv_h / rmax<Real>(sg, Real(kEps));
-    const Real density = rho.value();
+    const Real density = rho.value() + Real(rho_lo);
     ds->factor[i] = alpha;
     ds->density[i] = density;
     uint32_t num = nf;
@@ -986,7 +1003,7 @@ __global__ void __launch_bounds__(kBlock) select_candidate_kernel(const DevState
 // already larger); damping < 1 keeps a prediction error from overshooting the needed pressure.
 template <class Real>
 __global__ void __launch_bounds__(kBlock) warm_values_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
-                                                             int which, bool learned, Real damping) {
+                                                             int which, bool learned, bool use_pred, Real damping) {
     DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -996,7 +1013,7 @@ __global__ void __launch_bounds__(kBlock) warm_values_kernel(const DevState<Real
         const Real plain = rmax<Real>(ds->kappaV[i] * p.h_ratio_to_past / Real(2), Real(-0.5));
         Real use = plain;
         if (learned) {
-            const Real corr = (Real)ds->out_scale[1] * (Real)ds->pred[2 * (size_t)i + 1];
+            const Real corr = use_pred ? (Real)ds->out_scale[1] * (Real)ds->pred[2 * (size_t)i + 1] : Real(0);
             const Real need = rmin<Real>(rmax<Real>((ds->kappaVT[i] + corr) * p.h_ratio_to_past, Real(-0.5)), Real(0));
             use = rmin<Real>(plain, damping * need);
         }
@@ -1007,7 +1024,7 @@ __global__ void __launch_bounds__(kBlock) warm_values_kernel(const DevState<Real
         const Real plain = rmax<Real>(ds->kappa[i] * p.h_ratio_to_past2, Real(-0.5));
         Real use = plain;
         if (learned) {
-            const Real corr = (Real)ds->out_scale[0] * (Real)ds->pred[2 * (size_t)i];
+            const Real corr = use_pred ? (Real)ds->out_scale[0] * (Real)ds->pred[2 * (size_t)i] : Real(0);
             const Real need = rmin<Real>(rmax<Real>((ds->kappaT[i] + corr) * p.h_ratio_to_past2, Real(-0.5)), Real(0));
             use = rmin<Real>(plain, damping * need);
         }
@@ -1090,9 +1107,9 @@ void launch_probe_residual(const DevState<Real>* d, uint32_t n, int which, const
     else launch_pdl(probe_residual_kernel<Real, 1>, g, kBlock, 0, s, d, n, vel);
 }
 template <class Real>
-void launch_warm_values(const DevState<Real>* d, uint32_t n, int which, bool learned, double damping,
+void launch_warm_values(const DevState<Real>* d, uint32_t n, int which, bool learned, bool use_pred, double damping,
                         cudaStream_t s) {
-    if (n) launch_pdl(warm_values_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, which, learned, (Real)damping);
+    if (n) launch_pdl(warm_values_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, which, learned, use_pred, (Real)damping);
 }
 template <class Real> void launch_totals(const DevState<Real>* d, uint32_t n, bool div_ran, cudaStream_t s) {
     if (n) launch_pdl(totals_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, div_ran);
@@ -1198,7 +1215,7 @@ template <class Real> void launch_cfl_reduce(const DevState<Real>* d, uint32_t n
     template void launch_divergence_warm_jacobi<R>(const DevState<R>*, uint32_t, const R*, Vec4<R>*, cudaStream_t,  \
                                                    bool);                                                            \
     template void launch_probe_residual<R>(const DevState<R>*, uint32_t, int, const Vec4<R>*, cudaStream_t);        \
-    template void launch_warm_values<R>(const DevState<R>*, uint32_t, int, bool, double, cudaStream_t);             \
+    template void launch_warm_values<R>(const DevState<R>*, uint32_t, int, bool, bool, double, cudaStream_t);       \
     template void launch_totals<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                               \
     template void launch_gather_training<R>(const DevState<R>*, uint32_t, uint32_t, uint32_t, bool, float*, float*, \
                                             cudaStream_t);                                                           \

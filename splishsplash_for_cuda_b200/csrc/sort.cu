@@ -11,7 +11,6 @@
 // decoupled look-back over earlier tiles. Tiles take their index from an atomic counter at start,
 // so a tile only ever waits on tiles that are already running; every wait is bounded and gives up
 // with DFSPH_ST_SORT_TIMEOUT instead of hanging.
-#include <mutex>
 #include <string>
 
 #include "dfsph_common.cuh"
@@ -29,14 +28,16 @@ constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1u;
 constexpr int kSpinLimit = 1 << 22;
 
+// Digits are taken from key & key_mask (all ones for the solver's keys).
 __global__ void __launch_bounds__(kSortThreads) histogram_kernel(const uint32_t* __restrict__ keys, uint32_t n,
-                                                                 int passes, uint32_t* __restrict__ hist) {
+                                                                 int passes, uint32_t key_mask,
+                                                                 uint32_t* __restrict__ hist) {
     DFSPH_PDL_ENTER;
     __shared__ uint32_t sh[4][256];
     for (int t = threadIdx.x; t < 4 * 256; t += blockDim.x) (&sh[0][0])[t] = 0;
     __syncthreads();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t k = keys[i];
+        const uint32_t k = keys[i] & key_mask;
         for (int p = 0; p < passes; ++p) atomicAdd(&sh[p][(k >> (8 * p)) & 255u], 1u);
     }
     __syncthreads();
@@ -71,7 +72,7 @@ __device__ __forceinline__ void st_volatile(uint32_t* p, uint32_t v) { *(volatil
 
 __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
     const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
-    uint32_t* __restrict__ vout, uint32_t n, int shift, const uint32_t* __restrict__ digit_offsets,
+    uint32_t* __restrict__ vout, uint32_t n, int shift, uint32_t key_mask, const uint32_t* __restrict__ digit_offsets,
     uint32_t* __restrict__ tile_status, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status_word,
     uint32_t withheld_tile) {
     DFSPH_PDL_ENTER;
@@ -95,7 +96,7 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
         const bool valid = idx < n;
         key[r] = valid ? kin[idx] : 0u;
         val[r] = valid ? (vin ? vin[idx] : idx) : 0u;
-        const uint32_t d = valid ? ((key[r] >> shift) & 255u) : 256u;
+        const uint32_t d = valid ? (((key[r] & key_mask) >> shift) & 255u) : 256u;
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
         const uint32_t prior = valid ? warp_hist[warp][d] : 0u;
         __syncwarp();
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(
     for (int r = 0; r < kSortItems; ++r) {
         const uint32_t idx = base + r * 32 + lane;
         if (idx < n) {
-            const uint32_t d = (key[r] >> shift) & 255u;
+            const uint32_t d = ((key[r] & key_mask) >> shift) & 255u;
             const uint32_t pos = digit_base[d] + warp_hist[warp][d] + rank[r];
             if (pos < n) {  // only false after a timed-out look-back; never write out of range
                 kout[pos] = key[r];
@@ -189,7 +190,7 @@ void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, 
     int hist_blocks = (int)((n + kSortThreads * 16 - 1) / (kSortThreads * 16));
     if (hist_blocks > 148 * 4) hist_blocks = 148 * 4;
     if (hist_blocks < 1) hist_blocks = 1;
-    launch_pdl(histogram_kernel, hist_blocks, kSortThreads, 0, stream, b.keys_a, n, passes, hist);
+    launch_pdl(histogram_kernel, hist_blocks, kSortThreads, 0, stream, b.keys_a, n, passes, 0xFFFFFFFFu, hist);
     launch_pdl(scan_kernel, 1, 256, 0, stream, hist, passes, offsets);
     *launch_counter += 2;
     for (int p = 0; p < passes; ++p) {
@@ -198,7 +199,8 @@ void radix_sort_pairs(SortBuffers& b, uint32_t n, int passes, bool iota_values, 
         const uint32_t* vin = (p == 0 && iota_values) ? nullptr : (even ? b.vals_a : b.vals_b);
         uint32_t* kout = even ? b.keys_b : b.keys_a;
         uint32_t* vout = even ? b.vals_b : b.vals_a;
-        launch_pdl(onesweep_kernel, (unsigned)tiles, kSortThreads, 0, stream, kin, vin, kout, vout, n, 8 * p, offsets + p * 256,
+        launch_pdl(onesweep_kernel, (unsigned)tiles, kSortThreads, 0, stream, kin, vin, kout, vout, n, 8 * p, 0xFFFFFFFFu,
+                   offsets + p * 256,
                                                                    status + (size_t)p * tiles * 256, counters + p,
                                                                    status_word, withheld_tile);
         *launch_counter += 1;
@@ -230,9 +232,6 @@ constexpr size_t kNoAllocClearWords = kNoAllocTileFlags + 4 * kNoAllocTiles * 25
 constexpr size_t kNoAllocWords = kNoAllocClearWords + 2 * (size_t)kNoAllocMaxKeys;
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-uint32_t* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 int noalloc_fail(int code, const std::string& msg) {
     set_global_error(msg);  // reported by dfsph_last_error(NULL)
     return code;
@@ -250,26 +249,30 @@ extern "C" int dfsph_sort_cell_keys_noalloc(const uint32_t* keys_in, uint32_t* k
     if (key_bits < 1 || key_bits > 32) return noalloc_fail(DFSPH_E_INVALID, "key_bits must be in [1, 32]");
     if (n == 0) return DFSPH_OK;
     if (!keys_in || !keys_out || !perm_out) return noalloc_fail(DFSPH_E_INVALID, "null device buffer");
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return noalloc_fail(DFSPH_E_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return noalloc_fail(DFSPH_E_INVALID, "device ordinal out of range");
-    uint32_t* scratch = nullptr;
-    {
-        // First call on this device: resolve the device address of the scratch array (the host-side
-        // name g_noalloc_scratch is only a stand-in and must never be handed to a kernel).
-        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_ptr[dev]) {
-            void* p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess)
-                return noalloc_fail(DFSPH_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            g_noalloc_ptr[dev] = (uint32_t*)p;
-        }
-        scratch = g_noalloc_ptr[dev];
-    }
+    // The passes read the input while they write the outputs (an odd pass count writes the caller's
+    // buffers on the first pass): overlapping buffers would race.
+    const auto overlap = [n](const void* a, const void* b) {
+        const uintptr_t pa = (uintptr_t)a, pb = (uintptr_t)b, len = (uintptr_t)n * sizeof(uint32_t);
+        return pa < pb + len && pb < pa + len;
+    };
+    if (overlap(keys_in, keys_out) || overlap(keys_in, perm_out) || overlap(keys_out, perm_out))
+        return noalloc_fail(DFSPH_E_INVALID, "keys_in, keys_out and perm_out must not overlap");
     cudaStream_t s = (cudaStream_t)stream;
+    // The call ends with a copy into host memory and a wait, neither of which a stream capture admits.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) return noalloc_fail(DFSPH_E_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+    if (cap != cudaStreamCaptureStatusNone)
+        return noalloc_fail(DFSPH_E_STATE, "dfsph_sort_cell_keys_noalloc cannot run under stream capture");
+    // Device address of the scratch array on the current device (the host-side name
+    // g_noalloc_scratch is only a stand-in and must never be handed to a kernel). Looked up on every
+    // call, a host-side lookup, so that it stays valid after a device reset reloads the module.
+    void* sym = nullptr;
+    e = cudaGetSymbolAddress(&sym, g_noalloc_scratch);
+    if (e != cudaSuccess) return noalloc_fail(DFSPH_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    uint32_t* scratch = (uint32_t*)sym;
     const int passes = (key_bits + 7) / 8;
+    const uint32_t key_mask = key_bits == 32 ? 0xFFFFFFFFu : ((1u << key_bits) - 1u);
     const size_t tiles = (n + kSortTile - 1) / kSortTile;
     uint32_t* counters = scratch + kNoAllocCounters;
     uint32_t* status = scratch + kNoAllocStatus;
@@ -282,7 +285,7 @@ extern "C" int dfsph_sort_cell_keys_noalloc(const uint32_t* keys_in, uint32_t* k
     if (e != cudaSuccess) return noalloc_fail(DFSPH_E_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
     int hist_blocks = (int)((n + kSortThreads * 16 - 1) / (kSortThreads * 16));
     if (hist_blocks > 148 * 4) hist_blocks = 148 * 4;
-    launch_pdl(histogram_kernel, hist_blocks, kSortThreads, 0, s, keys_in, n, passes, hist);
+    launch_pdl(histogram_kernel, hist_blocks, kSortThreads, 0, s, keys_in, n, passes, key_mask, hist);
     launch_pdl(scan_kernel, 1, 256, 0, s, hist, passes, offsets);
     // The last pass must write the caller's buffers: with an odd pass count the first pass writes
     // them, with an even count the first pass writes the scratch pair.
@@ -292,13 +295,14 @@ extern "C" int dfsph_sort_cell_keys_noalloc(const uint32_t* keys_in, uint32_t* k
     for (int p = 0; p < passes; ++p) {
         uint32_t* kout = to_out ? keys_out : pk;
         uint32_t* vout = to_out ? perm_out : pv;
-        launch_pdl(onesweep_kernel, (unsigned)tiles, kSortThreads, 0, s, kin, vin, kout, vout, n, 8 * p, offsets + p * 256,
-                                                                flags + (size_t)p * tiles * 256, counters + p, status,
-                                                                kNoWithheldTile);
+        launch_pdl(onesweep_kernel, (unsigned)tiles, kSortThreads, 0, s, kin, vin, kout, vout, n, 8 * p, key_mask,
+                   offsets + p * 256, flags + (size_t)p * tiles * 256, counters + p, status, kNoWithheldTile);
         kin = kout;
         vin = vout;
         to_out = !to_out;
     }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return noalloc_fail(DFSPH_E_CUDA, std::string("sort launch: ") + cudaGetErrorString(e));
     uint32_t st = 0;
     e = cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -14,6 +14,7 @@ from oracle import mlp_oracle as M
 from splishsplash_for_cuda_b200 import _capi
 from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
 from splishsplash_for_cuda_b200.scene import column_scene, synthetic_scene
+from tests._compare import assert_field
 
 pytestmark = pytest.mark.gpu
 
@@ -235,3 +236,84 @@ def test_gate_parameters_and_divergence_off(cuda_lib):
         assert sa.iterations == sd.iterations and sd.iterations_v == 0 and sd.warm_start == 0
     assert np.array_equal(a.positions(), d.positions())
     assert d.get_param("gate_plain_steps") == 20 and d.get_param("gate_last_excess") >= 0.0
+
+
+def _oracle_features(o, needed_p, needed_v):
+    """The five network inputs of the density + alpha pass, restated from the oracle's fields:
+    (rho - rho0)/rho0, rho_dot * alpha, neighbours / 64, and the previous step's needed kappa and
+    kappa_v (solver.cu density_alpha_kernel)."""
+    counts, _ = o.get_neighbors()
+    rho0 = o.scene.config.density0
+    return np.stack([(o.field("density") - rho0) / rho0, o.field("density_adv") * o.field("factor"),
+                     counts.sum(axis=1) / 64.0, needed_p, needed_v], axis=1)
+
+
+def test_features_match_oracle(cuda_lib):
+    """The warm-start network's inputs written by the density + alpha pass, against the oracle on
+    the same state: step 1 of a scene with random velocities (+-0.5 m/s), and step 2, whose last two
+    inputs are the coefficients step 1 needed. The learned mode runs with the network's correction
+    fixed at zero, which makes its first step the plain step (the oracle's). Bars: the neighbour count
+    exactly; the other inputs within 1e-4 relative, floored at 1e-3 of each input's largest value
+    (the network rounds its inputs to BF16, 2^-8 relative; rho_dot and the needed coefficients are
+    sums of velocity differences that cancel, where FP32 itself errs by ~1e-4)."""
+    from oracle import Oracle
+
+    s = synthetic_scene(1, counts=(14, 14, 14))
+    rng = np.random.default_rng(7)
+    s.fluid_velocity = rng.uniform(-0.5, 0.5, size=s.fluid.shape).astype(np.float32)
+    d = DFSPHCUDA(s)
+    d.set_learned_warm_start(True, train_interval=0)
+    d.set_param("learned_base_only", 1)
+    o = Oracle(s, 64)
+    zeros = np.zeros(s.n_fluid)
+    for step in (1, 2):
+        if step == 1:
+            o.neighbors()
+            o.density_alpha(True)
+            ref = _oracle_features(o, zeros, zeros)
+            o2 = Oracle(s, 64)
+            ro = o2.step()
+        else:
+            need_p, need_v = o2.field("kappa_needed"), o2.field("kappa_v_needed")
+            assert np.abs(need_p).max() > 0 and np.abs(need_v).max() > 0
+            o2.neighbors()
+            o2.density_alpha(True)
+            ref = _oracle_features(o2, need_p, need_v)
+        st = d.step()
+        if step == 1:
+            assert st.iterations == ro["iterations"] and st.iterations_v == ro["iterations_v"]
+        got = d.field("features").astype(np.float64)
+        assert got.shape == (s.n_fluid, 5)
+        assert np.array_equal(got[:, 2], ref[:, 2]), step
+        for k in (0, 1, 3, 4):
+            assert_field(f"feature {k} step {step}", got[:, k], ref[:, k], 1e-4, 1e-3)
+
+
+def test_network_contribution_ablation(cuda_lib):
+    """Three arms on the stiff resting column, same scene and tolerance: the reference warm start,
+    the needed-coefficient base with the network's correction fixed at zero, and the online-trained
+    network on top of that base. Every solve converges in every arm; the base alone cuts the
+    pressure iterations by >= 30 %; the trained network's own contribution (base minus trained
+    iterations) is measured and must not cost more than 10 % of the base's iterations."""
+    s = column_scene(counts=(10, 40, 10), time_step=0.002, max_error=0.01)
+    steps = 300
+    _, ip, _, _, bp = _run(s, steps, False)
+    db = DFSPHCUDA(s)
+    db.set_learned_warm_start(True, train_interval=25)
+    db.set_param("learned_base_only", 1)
+    ib, bb = [], 0
+    for _ in range(steps):
+        st = db.step()
+        ib.append(st.iterations)
+        bb |= st.status
+    ib = np.array(ib)
+    dl, il, _, _, bl = _run(s, steps, True, train_interval=25)
+    for bits in (bp, bb, bl):
+        assert bits & (_capi.ST_PRESSURE_NOT_CONVERGED | _capi.ST_NONFINITE) == 0
+    assert db.get_param("mlp_trainings") == 0 and dl.get_param("mlp_trainings") >= 10
+    win = slice(150, steps)
+    mp, mb, ml = ip[win].mean(), ib[win].mean(), il[win].mean()
+    print(f"pressure iterations: plain {mp:.2f}, base (network output 0) {mb:.2f}, trained {ml:.2f}; "
+          f"network contribution {mb - ml:+.2f} iterations/step ({(mb - ml) / mb:+.1%} of the base)")
+    assert mb <= 0.7 * mp
+    assert ml <= 1.1 * mb

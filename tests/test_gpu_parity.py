@@ -1,8 +1,10 @@
 """GPU parity tests: the sm_100a kernels, called through the C ABI, against the CPU oracle.
 
-Bars: neighbour sets bit-exact; one-step fields within 1e-5 relative of the FP64 oracle for the FP32
-build (relative error floored at 1e-3 of the field's max, see tests/_compare.py) and within 1e-9 for
-the FP64 build of the same kernels; identical iteration counts; bit-identical reruns."""
+Bars: neighbour sets bit-exact; one step from rest of the full configurations (27,000, 250,047 and
+1,000,000 particles): density, alpha, kappa, kappa_v, velocity, position and acceleration of every
+particle within a plain 1e-5 relative of the FP64 oracle for the FP32 build (no floor: a value that
+is exactly zero in the oracle must be exactly zero), and within 1e-9 for the FP64 build of the same
+kernels; identical iteration counts; bit-identical reruns."""
 import numpy as np
 import pytest
 
@@ -15,15 +17,21 @@ from tests._compare import assert_field, field_error, neighbor_sets
 pytestmark = pytest.mark.gpu
 
 FIELDS_ONE_STEP = ["density", "factor", "kappa", "kappa_v", "velocity", "position", "acceleration"]
-# Relative-error floor per field (fraction of the field's maximum magnitude). Velocities of particles
-# that nearly stop after the pressure solve carry the FP32 rounding of v_i - v_j taken after gravity
-# added a common ~g*h to every particle; the FP32 oracle shows the same ~1e-5 there, so velocity and
-# acceleration are compared per particle against max(|v_i|, 1 % of the maximum speed).
+# Relative-error floor (fraction of the field's maximum magnitude) of the multi-step and stress
+# comparisons below; the one-step parity tests from rest use none.
 FLOOR = {"velocity": 1e-2, "acceleration": 1e-2}
 
 
 def check_field(name, got, ref, rtol):
     return assert_field(name, got, ref, rtol, FLOOR.get(name, 1e-3))
+
+
+def _sloshing_walls(scene):
+    """The sloshing tank's walls at t = 0: in place, moving at 0.1 (2 pi / 2) m/s along x."""
+    b = scene.boundary.astype(np.float32)
+    v = np.zeros_like(b)
+    v[:, 0] = 0.1 * np.pi
+    return b, v
 
 
 def _moving_scene(counts=(14, 14, 14), seed=7, vmax=0.5):
@@ -68,25 +76,47 @@ def test_boundary_psi_matches_fp64_oracle():
     assert_field("psi", d.field("boundary_psi", np.float64), o.field("boundary_psi"), 1e-6)
 
 
-@pytest.mark.parametrize("scene_fn", [lambda: synthetic_scene(1, counts=(14, 14, 14)), lambda: synthetic_scene(1),
-                                      lambda: synthetic_scene(2, counts=(40, 30, 30), cfl=True)])
-def test_one_step_fp32_matches_fp64_oracle(scene_fn):
-    """Physical scenes (dam breaks from rest): every field within 1e-5 of the FP64 oracle, or within
-    2x the error of plain FP32 arithmetic of the same formulation (the FP32 oracle, division form)
-    where that is larger: velocities that nearly cancel after the first pressure solve sit at ~1.2e-5
-    in plain FP32, ~2e-5 in the device kernels (reciprocal square root instead of two divisions)."""
-    s = scene_fn()
+@pytest.mark.parametrize("config,counts", [(1, (14, 14, 14)), (1, None), (2, None), (3, None)])
+def test_one_step_fp32_within_1e5_of_fp64_oracle(config, counts):
+    """One CFL step from rest of the full dam break (27,000), precision (250,047) and sloshing-tank
+    (1,000,000 particles, walls at rest) configurations: every field of every particle within a plain
+    1e-5 relative of the FP64 oracle. What makes the velocity bar reachable in FP32 is the density
+    pass's double-float terms: the particles next to the few compressed ones get a pressure
+    correction that cancels most of gravity's g h, so their velocity carries the relative error of
+    rho - rho0 amplified ~3x, and plain FP32 terms (~1e-4 kg/m^3 on rho) put it at 1-2e-5."""
+    s = synthetic_scene(config, counts=counts, cfl=True)
     d = DFSPHCUDA(s)
-    o, o32 = Oracle(s, 64), Oracle(s, 32)
+    o = Oracle(s, 64)
     st = d.step()
     ro = o.step()
-    o32.step()
+    assert st.status == 0
     assert st.iterations == ro["iterations"]
     assert st.iterations_v == ro["iterations_v"]
-    assert st.density_error == pytest.approx(ro["density_error"], rel=1e-4, abs=1e-7)
-    for name in FIELDS_ONE_STEP:
-        budget = field_error(o32.field(name), o.field(name), FLOOR.get(name, 1e-3))
-        check_field(name, d.field(name, np.float64), o.field(name), max(1e-5, 2.0 * budget))
+    assert st.density_error == pytest.approx(ro["density_error"], rel=1e-5)
+    errs = {name: assert_field(name, d.field(name, np.float64), o.field(name), 1e-5, 0.0) for name in FIELDS_ONE_STEP}
+    print(config, s.n_fluid, {k: f"{v:.2e}" for k, v in errs.items()})
+
+
+def test_one_step_sloshing_moving_walls():
+    """First step of the 1,000,000-particle sloshing workload, walls moving at 0.314 m/s: density,
+    alpha, velocity and position of every particle within a plain 1e-5 relative of the FP64 oracle.
+    kappa and kappa_v within 1e-5 relative where they are at least 5 % of the field's largest value;
+    below that within 5e-7 of the largest value (the same 1e-5 floored at 5 %): there a coefficient
+    is the sum of a solve's last residuals, each a difference of nearly equal FP32 neighbour sums
+    (the FP32 oracle shows 2e-4 relative on kappa values ~1e-3 of the largest, 2e-7 of it)."""
+    s = synthetic_scene(3, cfl=True)
+    d = DFSPHCUDA(s)
+    o = Oracle(s, 64)
+    b, v = _sloshing_walls(s)
+    d.move_boundary(b, v)
+    o.move_boundary(b, v)
+    st, ro = d.step(), o.step()
+    assert st.status == 0
+    assert st.iterations == ro["iterations"] and st.iterations_v == ro["iterations_v"]
+    for name in ("density", "factor", "velocity", "position", "acceleration"):
+        assert_field(name, d.field(name, np.float64), o.field(name), 1e-5, 0.0)
+    for name in ("kappa", "kappa_v"):
+        assert_field(name, d.field(name, np.float64), o.field(name), 1e-5, 0.05)
 
 
 def test_one_step_stress_scene_within_fp32_budget():

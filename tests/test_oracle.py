@@ -64,15 +64,21 @@ def test_boundary_psi_planar_lattice(oracle_lib):
     assert psi.min() > 0 and psi.max() < 2 * expected
 
 
-def test_fp32_error_budget_one_step(oracle_lib):
-    s = synthetic_scene(1, counts=(14, 14, 14))
+@pytest.mark.parametrize("config,counts", [(1, (14, 14, 14)), (1, None), (2, None)])
+def test_fp32_formulation_meets_one_step_bar(oracle_lib, config, counts):
+    """The FP32 instance of the restated formulation (the device's arithmetic: compensated FP32
+    sums, double-float density terms) against the FP64 instance, one CFL step from rest: every field
+    of every particle within a plain 1e-5 relative (no floor). Measured: density 6e-8, alpha 7e-7,
+    kappa 3e-8, velocity 5e-7 on the 250,047-particle configuration; with plain FP32 density terms
+    the velocity was 1.1e-5."""
+    s = synthetic_scene(config, counts=counts, cfl=True)
     o64, o32 = Oracle(s, 64), Oracle(s, 32)
     r64, r32 = o64.step(), o32.step()
     assert r64["iterations"] == r32["iterations"]
     assert r64["iterations_v"] == r32["iterations_v"]
-    for name, tol in [("density", 1e-6), ("factor", 1e-5), ("velocity", 1e-5), ("position", 1e-6), ("kappa", 1e-4)]:
-        err = field_error(o32.field(name), o64.field(name))
-        assert err < tol, (name, err)
+    for name in ("density", "factor", "kappa", "kappa_v", "velocity", "position", "acceleration"):
+        err = field_error(o32.field(name), o64.field(name), 0.0)
+        assert err < 1e-5, (name, err)
 
 
 def test_dam_break_stays_bounded(oracle_lib):

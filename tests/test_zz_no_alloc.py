@@ -65,6 +65,76 @@ def test_noalloc_sort_matches_solver_sorted_order():
     d.close()
 
 
+def _noalloc_sort(keys: np.ndarray, key_bits: int):
+    import torch
+
+    lib = _capi.load()
+    dev = torch.device("cuda", 0)
+    n = keys.size
+    keys_in = torch.from_numpy(keys.view(np.int32)).to(dev)
+    keys_out = torch.full((n,), -1, dtype=torch.int32, device=dev)
+    perm_out = torch.full((n,), -1, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    code = lib.dfsph_sort_cell_keys_noalloc(C.c_void_p(keys_in.data_ptr()), C.c_void_p(keys_out.data_ptr()),
+                                            C.c_void_p(perm_out.data_ptr()), n, key_bits,
+                                            C.c_void_p(stream.cuda_stream))
+    assert code == _capi.DFSPH_OK, lib.dfsph_last_error(None)
+    return keys_out.cpu().numpy().view(np.uint32), perm_out.cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("n,key_bits,high", [(1, 8, False), (2047, 8, False), (2049, 24, False),
+                                             (100_003, 24, True), (262_144, 30, True), (77_777, 32, False),
+                                             (5000, 13, True)])
+def test_noalloc_sort_equals_stable_argsort(n, key_bits, high):
+    """1, 2, 3 and 4 digit passes (odd counts write the caller's buffers on the first pass), one key,
+    partial tiles and a full last tile, and keys with bits set above key_bits (carried, not
+    ordered): equal to numpy's stable argsort of the low key_bits bits, twice in a row."""
+    rng = np.random.default_rng(n + key_bits)
+    low = rng.integers(0, 1 << min(key_bits, 31), size=n, dtype=np.int64)
+    if key_bits == 32:
+        low = rng.integers(0, 1 << 32, size=n, dtype=np.int64)
+    low[: n // 3] = low[n // 3: 2 * (n // 3)]  # many equal keys: stability matters
+    keys = low.astype(np.uint64)
+    if high and key_bits < 32:
+        keys |= rng.integers(0, 1 << (32 - key_bits), size=n).astype(np.uint64) << key_bits
+    keys = keys.astype(np.uint32)
+    mask = np.uint32(0xFFFFFFFF if key_bits == 32 else (1 << key_bits) - 1)
+    ref = np.argsort(keys & mask, kind="stable").astype(np.uint32)
+    for _ in range(2):
+        ko, po = _noalloc_sort(keys, key_bits)
+        assert np.array_equal(po, ref)
+        assert np.array_equal(ko, keys[ref])
+
+
+def test_noalloc_sort_rejects_overlap_and_capture():
+    import torch
+
+    lib = _capi.load()
+    dev = torch.device("cuda", 0)
+    buf = torch.zeros(3000, dtype=torch.int32, device=dev)
+    p = buf.data_ptr()
+    # keys_out overlapping keys_in
+    code = lib.dfsph_sort_cell_keys_noalloc(C.c_void_p(p), C.c_void_p(p + 4 * 500), C.c_void_p(p + 4 * 2000), 1000,
+                                            8, None)
+    assert code == _capi.DFSPH_E_INVALID and b"overlap" in lib.dfsph_last_error(None)
+    keys = torch.zeros(1000, dtype=torch.int32, device=dev)
+    ko = torch.zeros(1000, dtype=torch.int32, device=dev)
+    po = torch.zeros(1000, dtype=torch.int32, device=dev)
+    s = torch.cuda.Stream(dev)
+    g = torch.cuda.CUDAGraph()
+    codes = []
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            codes.append(lib.dfsph_sort_cell_keys_noalloc(C.c_void_p(keys.data_ptr()), C.c_void_p(ko.data_ptr()),
+                                                          C.c_void_p(po.data_ptr()), 1000, 8,
+                                                          C.c_void_p(s.cuda_stream)))
+            ko.add_(1)  # the captured graph must not be empty
+    assert codes == [_capi.DFSPH_E_STATE]
+    assert b"stream capture" in lib.dfsph_last_error(None)
+    del g
+    torch.cuda.synchronize()
+
+
 def test_noalloc_sort_rejects_oversize_input():
     lib = _capi.load()
     n = _capi.NOALLOC_MAX_KEYS + 1
