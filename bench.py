@@ -1,9 +1,13 @@
 """Benchmark of the DFSPH time step on B200 (one JSON line on rank 0).
 
-Workload (default): the 250,047-particle dam break (63^3 lattice, r = 0.0125 m, 4 x 2 x 2 m box,
-64,002 wall particles, CFL 0.4 with dt_max 5 ms, density tolerance 0.01 %, divergence 0.1 %),
-synthetic seeded input. A step is one DFSPHCUDA::step() equivalent: neighbour search, divergence
-solve, XSPH + gravity, CFL dt, pressure solve, position update.
+Workload (default, --config 3): the 1,000,000-particle sloshing tank (100^3 lattice, r = 0.01 m,
+8 x 4 x 4 m box, 400,002 wall particles translating rigidly as x = 0.1 sin(2 pi t / 2) m, CFL 0.4
+with dt_max 5 ms, density tolerance 0.01 %, divergence 0.1 %), synthetic seeded input. A step is
+one DFSPHCUDA::step() equivalent: the walls' rigid motion (on the device), neighbour search,
+divergence solve, XSPH + gravity, CFL dt, pressure solve, position update. `value` is the plain
+(reference) warm start; the learned-vs-plain comparison of the metric runs the same workload and the
+2,000,000-particle column collapse (0.005 %, dt_max 8 ms) in every mode, and the stiff resting
+column where the solver needs many iterations.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 1..5]
 
@@ -106,10 +110,24 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml"}
 
 
-def make_scene(config: int):
-    from splishsplash_for_cuda_b200.scene import synthetic_scene
+def make_workload(config: int):
+    """(scene, wall motion or None) of benchmark configuration `config`. The sloshing tank's walls
+    move rigidly (sloshing_wall_motion); motion(d, t) applies their state at simulated time t."""
+    from splishsplash_for_cuda_b200.scene import sloshing_wall_motion, synthetic_scene
 
-    return synthetic_scene(config, cfl=True)
+    scene = synthetic_scene(config, cfl=True)
+    if config != 3:
+        return scene, None
+
+    def motion(d, t):
+        p, v = sloshing_wall_motion(t)
+        d.move_boundary_rigid(0, scene.n_boundary, None, p, v, None)
+
+    return scene, motion
+
+
+def make_scene(config: int):
+    return make_workload(config)[0]
 
 
 # Algorithmic bytes per launch of each kernel (FP32 layout: float4 pos+mass, float4 vel, 4-byte
@@ -210,6 +228,8 @@ def run_reference_arm(args, world, rank):
         "steps": done, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": scene.name, "fluid_particles": scene.n_fluid, "boundary_particles": scene.n_boundary,
+                   "walls": "static (the reference CPU solver's boundary is a static rigid body; the per-step cost "
+                            "of a moving wall is its rebinning)" if args.config == 3 else "static",
                    "parallelism": "cpu"},
         "cpu_baseline": {"value": round(ms, 3), "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"{done} steps after {args.warmup} warm-up steps of {scene.name}"},
@@ -218,7 +238,7 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-ABLATION_WORKLOADS = ("column_64", "sloshing_1m", "column_2m")
+ABLATION_WORKLOADS = ("sloshing_1m", "column_2m", "column_64")
 
 
 def ablation_scene(workload: str):
@@ -232,17 +252,7 @@ def ablation_scene(workload: str):
     if workload == "column_64":
         return column_scene(counts=(64, 64, 64), time_step=0.002, max_error=0.01), None
     if workload == "sloshing_1m":
-        scene = synthetic_scene(3, cfl=True)
-        b0 = scene.boundary.astype(np.float64)
-
-        def walls(t):
-            x = b0.copy()
-            x[:, 0] += 0.1 * np.sin(2 * np.pi * t / 2.0)
-            v = np.zeros_like(b0)
-            v[:, 0] = 0.1 * (2 * np.pi / 2.0) * np.cos(2 * np.pi * t / 2.0)
-            return x.astype(np.float32), v.astype(np.float32)
-
-        return scene, walls
+        return make_workload(3)
     if workload == "column_2m":
         return synthetic_scene(4, cfl=True), None
     raise ValueError(workload)
@@ -251,9 +261,12 @@ def ablation_scene(workload: str):
 def learned_ablation(local, steps: int, workload: str = "column_64"):
     """Plain vs learned warm start on the same scene from the same state, each for `steps` steps;
     the second half is measured (the flow has developed by then). ms/step is the device time of each
-    step (CUDA events inside dfsph_step), online training rounds included. "gated" is the learned
-    warm start behind its cost gate (learned passes only while the plain solver needs at least one
-    iteration per step above the minimum counts; plain probe windows included in the average)."""
+    step (CUDA events inside dfsph_step), online training rounds included. "base" is the learned
+    warm start with the network's correction fixed at zero (the needed-coefficient base alone, no
+    inference, no training), so "learned" vs "base" is the trained network's own contribution.
+    "gated" is the learned warm start behind its cost gate (learned passes only while the plain
+    solver needs at least one iteration per step above the minimum counts; plain probe windows
+    included in the average)."""
     from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
 
     scene, walls = ablation_scene(workload)
@@ -261,17 +274,19 @@ def learned_ablation(local, steps: int, workload: str = "column_64"):
            "steps": steps, "measured_steps": f"{steps // 2}..{steps - 1}",
            "max_error_pct": scene.config.maxError, "moving_walls": walls is not None,
            "cfl": bool(scene.config.cflMethod)}
-    for mode in ("plain", "learned", "gated"):
+    for mode in ("plain", "base", "learned", "gated"):
         d = DFSPHCUDA(scene, device=local)
         d.set_param("timing", 1)
         if walls is not None:  # the fluid follows the walls past the initial box: keep every particle
             d.set_param("remove_escaped", 0)
         if mode != "plain":
             d.set_learned_warm_start(True, gate=mode == "gated")
+        if mode == "base":
+            d.set_param("learned_base_only", 1)
         its, itv, ms, bits, t = [], [], [], 0, 0.0
         for _ in range(steps):
             if walls is not None:
-                d.move_boundary(*walls(t))
+                walls(d, t)
             st = d.step()
             t += st.h
             its.append(st.iterations)
@@ -298,6 +313,8 @@ def learned_ablation(local, steps: int, workload: str = "column_64"):
         d.close()
     out["pressure_iteration_reduction"] = round(1 - out["learned"]["pressure_iterations"]
                                                 / out["plain"]["pressure_iterations"], 4)
+    out["network_contribution_iterations"] = round(out["base"]["pressure_iterations"]
+                                                   - out["learned"]["pressure_iterations"], 3)
     out["ms_per_step_reduction"] = round(1 - out["learned"]["ms_per_step"] / out["plain"]["ms_per_step"], 4)
     out["gated_ms_per_step_reduction"] = round(1 - out["gated"]["ms_per_step"] / out["plain"]["ms_per_step"], 4)
     return out
@@ -308,23 +325,36 @@ def run_ours(args, world, rank, local):
 
     from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
 
-    scene = make_scene(args.config)
+    scene, motion = make_workload(args.config)
     n = scene.n_fluid
     d = DFSPHCUDA(scene, device=local, use_graphs=not args.host_loops)
     d.set_param("timing", 0)
+    if motion is not None:  # the fluid follows the walls past the initial box: keep every particle
+        d.set_param("remove_escaped", 0)
     stream = torch.cuda.ExternalStream(d.stream_handle(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    sim_t = [0.0]
+
+    def advance():
+        """One step of the workload: the walls' motion at the current simulated time (on the device),
+        then the step. With moving walls the step returns its statistics (the next motion needs its
+        dt); otherwise it is only enqueued."""
+        if motion is None:
+            d.step_async()
+            return
+        motion(d, sim_t[0])
+        sim_t[0] += d.step().h
 
     for _ in range(args.warmup):
-        d.step()
+        advance()
     d.synchronize()
 
     def timed_steps(k, e2e=False, host=None):
         """k steps, each bracketed by CUDA events on the solver's stream after a 256 MiB write that
-        evicts L2. Steps are enqueued without host round trips (the step runs on the device, dt
-        included); iterations come from the device counters. e2e: each step also uploads its inputs
-        from pinned host memory and reads positions and velocities back (readDynamicData, which
-        waits)."""
+        evicts L2. Without moving walls steps are enqueued without host round trips (the step runs
+        on the device, dt included); iterations come from the device counters. e2e: each step also
+        uploads its inputs from pinned host memory and reads positions and velocities back
+        (readDynamicData, which waits)."""
         tot = 0.0
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
@@ -335,7 +365,7 @@ def run_ours(args, world, rank, local):
                 starts[s].record(stream)
             if e2e:
                 d.update_fluid(host["x"], host["v"])
-            d.step_async()
+            advance()
             if e2e:  # DFSPHCData::readDynamicData: positions and velocities, one wait
                 d.m_data.readDynamicData(host["x"], host["v"])
             with torch.cuda.stream(stream):
@@ -412,7 +442,7 @@ def run_ours(args, world, rank, local):
 
     ablation = None
     if rank == 0 and world == 1 and args.ablation_steps > 0:
-        ablation = learned_ablation(local, args.ablation_steps, args.ablation_workload)
+        ablation = {w: learned_ablation(local, args.ablation_steps, w) for w in args.ablation_workloads}
 
     if rank == 0:
         line = {
@@ -420,9 +450,13 @@ def run_ours(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice + xoshiro256** jitter)",
             "config": {"workload": scene.name, "fluid_particles": n, "boundary_particles": scene.n_boundary,
-                       "radius": scene.config.particleRadius, "cfl": "0.4, dt_max 5 ms",
+                       "radius": scene.config.particleRadius, "cfl": f"0.4, dt_max {scene.config.cflMaxTimeStepSize * 1e3:g} ms",
                        "max_error_pct": scene.config.maxError, "max_error_v_pct": scene.config.maxErrorV,
-                       "warm_start": "plain", "l2": "256 MiB write before every timed step",
+                       "warm_start": "plain",
+                       "walls": "rigid translation x = 0.1 sin(pi t) m, moved on the device every step"
+                       if motion is not None else "static",
+                       "l2": "256 MiB write before every timed step"
+                       + ("; the step's working set exceeds L2" if n >= 1_000_000 else ""),
                        "parallelism": "replicas" if world > 1 else "single"},
             "iterations_per_step": round(mean_it, 2), "iterations_v_per_step": round(mean_itv, 2),
             "status_bits": int(status_bits),
@@ -451,7 +485,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--config", type=int, default=3)
     ap.add_argument("--host-loops", action="store_true", help="solver loops driven from the host")
     ap.add_argument("--kernel-reps", type=int, default=5)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
@@ -459,7 +493,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ablation-steps", type=int, default=300,
                     help="steps per mode of the plain vs learned warm-start comparison (0: skip)")
-    ap.add_argument("--ablation-workload", choices=ABLATION_WORKLOADS, default="column_64")
+    ap.add_argument("--ablation-workloads", nargs="*", choices=ABLATION_WORKLOADS, default=list(ABLATION_WORKLOADS))
     ap.add_argument("--ablation-only", action="store_true",
                     help="print only the plain vs learned comparison as one JSON line")
     args = ap.parse_args()
@@ -469,8 +503,8 @@ def main():
     try:
         if args.ablation_only:
             if rank == 0:
-                print(json.dumps({"learned_warm_start": learned_ablation(local, args.ablation_steps,
-                                                                         args.ablation_workload)}), flush=True)
+                print(json.dumps({"learned_warm_start": {w: learned_ablation(local, args.ablation_steps, w)
+                                                         for w in args.ablation_workloads}}), flush=True)
         elif args.impl == "reference":
             run_reference_arm(args, world, rank)
         else:

@@ -155,6 +155,16 @@ int dfsph_set_boundary(dfsph_ctx* ctx, const float* xyz, const float* psi, uint3
  * the order of dfsph_set_boundary. psi is kept. The boundary cell structure is rebuilt. */
 int dfsph_move_boundary(dfsph_ctx* ctx, const float* xyz, const float* vxyz);
 
+/* Rigid motion of one body of the boundary, on the device (update_dynamicObject_UnifiedParticleSet_cuda,
+ * SPlisHSPlasH/DFSPH/DFSPH_core_cuda.cu:3426-3449): the particles of upload indices
+ * [first, first + count) go to x = R(q) x0 + position with velocity angular_velocity x (x - position)
+ * + velocity, where x0 is each particle's position as given to dfsph_set_boundary (its rest frame)
+ * and q = (w, x, y, z) a rotation quaternion (normalised here). Null pointers mean the identity /
+ * zero. psi is kept, the other particles keep their state, and the boundary cell structure is
+ * rebuilt; no particle data crosses the host link. */
+int dfsph_move_boundary_rigid(dfsph_ctx* ctx, uint32_t first, uint32_t count, const double* q, const double* position,
+                              const double* velocity, const double* angular_velocity);
+
 /* Fluid particles (fluid_data->reset<FluidModel>). vxyz may be null (zero velocity). mass may be
  * null: every particle then gets the reference default mass 0.8 * rho0 * (2r)^3
  * (FluidModel::initMasses, FluidModel.cpp:94-107). Resets kappa, kappa_v and the dt history

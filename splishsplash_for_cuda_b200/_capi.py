@@ -121,6 +121,7 @@ SIGNATURES = {
     "dfsph_last_error": (C.c_char_p, [_P]),
     "dfsph_set_boundary": (C.c_int, [_P, _F, _F, C.c_uint32]),
     "dfsph_move_boundary": (C.c_int, [_P, _F, _F]),
+    "dfsph_move_boundary_rigid": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, _P, _P]),
     "dfsph_upload_fluid": (C.c_int, [_P, _F, _F, _F, C.c_uint32]),
     "dfsph_update_fluid": (C.c_int, [_P, _F, _F]),
     "dfsph_download": (C.c_int, [_P, C.c_int, C.c_int, _P, C.c_size_t, C.c_int]),

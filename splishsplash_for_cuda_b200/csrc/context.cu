@@ -99,6 +99,7 @@ public:
     size_t cells = 0;
     Vec4<Real>* bpos[2] = {nullptr, nullptr};
     Vec4<Real>* bvel[2] = {nullptr, nullptr};
+    float* brest = nullptr;  // boundary positions as given to set_boundary (upload order), for rigid moves
     Real* bforce = nullptr;  // boundary forces (4 per particle, sorted order), allocated when enabled
     bool boundary_forces = false;
     uint32_t* bid = nullptr;
@@ -229,6 +230,7 @@ public:
         DF_TRY(dalloc(&counts, Nc));
         DF_TRY(dalloc(&nbr, (size_t)cap * stride));
         DF_TRY(dalloc(&bid, Bc));
+        DF_TRY(dalloc(&brest, (size_t)Bc * 3));
         const uint32_t nmax = std::max(Nc, Bc);
         DF_TRY(dalloc(&sb.keys_a, nmax));
         DF_TRY(dalloc(&sb.keys_b, nmax));
@@ -514,6 +516,7 @@ public:
         boundary_moving = false;
         if (count) {
             DF_CUDA(cudaMemcpyAsync(stage, xyz, (size_t)count * 3 * sizeof(float), cudaMemcpyHostToDevice, stream));
+            DF_CUDA(cudaMemcpyAsync(brest, stage, (size_t)count * 3 * sizeof(float), cudaMemcpyDeviceToDevice, stream));
             if (psi)
                 DF_CUDA(cudaMemcpyAsync(stage + (size_t)count * 3, psi, (size_t)count * sizeof(float),
                                         cudaMemcpyHostToDevice, stream));
@@ -538,6 +541,45 @@ public:
         // positions in original order -> staging set [1] in original order, then re-sort
         launch_move_boundary<Real>(stage, vxyz ? stage + (size_t)nb * 3 : nullptr, nb, bid, bpos[0], bvel[0], stream);
         // bring the moved set back to original order in [1]: slot i holds original bid[i]
+        launch_pack_field<Real, Real>((const Real*)bpos[0], 4, 4, bid, nb, (Real*)bpos[1], stream);
+        launch_pack_field<Real, Real>((const Real*)bvel[0], 4, 4, bid, nb, (Real*)bvel[1], stream);
+        launches += 3;
+        boundary_moving = true;
+        DF_TRY(sort_boundary(false));
+        return sync_state();
+    }
+
+    // update_dynamicObject_UnifiedParticleSet_cuda (DFSPH_core_cuda.cu:3426-3449) for the boundary
+    // particles of upload indices [first, first + count): x = R(q) x0 + position with x0 the
+    // positions given to set_boundary, v = angular_velocity x (x - position) + velocity. Every
+    // argument stays on the device path (no host copy of the particles); the cell structure is rebuilt.
+    int move_boundary_rigid(uint32_t first, uint32_t count, const double* q, const double* position,
+                            const double* velocity, const double* angular_velocity) {
+        DF_CHECK(nb > 0, DFSPH_E_STATE, "no boundary set");
+        DF_CHECK(first <= nb && count <= nb - first, DFSPH_E_INVALID, "boundary range out of bounds");
+        RigidMotion m{};
+        double w = 1, x = 0, y = 0, z = 0;
+        if (q) {
+            const double len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+            DF_CHECK(len > 0 && std::isfinite(len), DFSPH_E_INVALID, "quaternion must be finite and non-zero");
+            w = q[0] / len; x = q[1] / len; y = q[2] / len; z = q[3] / len;
+        }
+        const double R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
+                             2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                             2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)};
+        for (int k = 0; k < 9; ++k) m.R[k] = R[k];
+        for (int k = 0; k < 3; ++k) {
+            m.p[k] = position ? position[k] : 0.0;
+            m.v[k] = velocity ? velocity[k] : 0.0;
+            m.w[k] = angular_velocity ? angular_velocity[k] : 0.0;
+            DF_CHECK(std::isfinite(m.p[k]) && std::isfinite(m.v[k]) && std::isfinite(m.w[k]), DFSPH_E_INVALID,
+                     "rigid motion must be finite");
+        }
+        m.first = first;
+        m.count = count;
+        if (!count) return DFSPH_OK;
+        if (!boundary_moving) DF_CUDA(cudaMemsetAsync(bvel[0], 0, (size_t)nb * sizeof(Vec4<Real>), stream));
+        launch_rigid_boundary<Real>(brest, nb, bid, m, bpos[0], bvel[0], stream);
         launch_pack_field<Real, Real>((const Real*)bpos[0], 4, 4, bid, nb, (Real*)bpos[1], stream);
         launch_pack_field<Real, Real>((const Real*)bvel[0], 4, 4, bid, nb, (Real*)bvel[1], stream);
         launches += 3;
@@ -2363,6 +2405,10 @@ int dfsph_set_boundary(dfsph_ctx* ctx, const float* xyz, const float* psi, uint3
 }
 int dfsph_move_boundary(dfsph_ctx* ctx, const float* xyz, const float* vxyz) {
     DFSPH_DISPATCH(ctx, move_boundary(xyz, vxyz));
+}
+int dfsph_move_boundary_rigid(dfsph_ctx* ctx, uint32_t first, uint32_t count, const double* q, const double* position,
+                              const double* velocity, const double* angular_velocity) {
+    DFSPH_DISPATCH(ctx, move_boundary_rigid(first, count, q, position, velocity, angular_velocity));
 }
 int dfsph_upload_fluid(dfsph_ctx* ctx, const float* xyz, const float* vxyz, const float* mass, uint32_t n) {
     DFSPH_DISPATCH(ctx, upload_fluid(xyz, vxyz, mass, n));

@@ -121,6 +121,39 @@ __global__ void __launch_bounds__(kBlock) move_boundary_kernel(const float* __re
     bvel[i] = v;
 }
 
+// Rigid motion of the boundary particles whose upload index lies in [first, first + count), the
+// reference's update of a dynamic object's particles (DFSPH_updateDynamicObjectParticles_kernel,
+// DFSPH_core_cuda.cu:3412-3423): x = R x0 + p, v = w x (x - p) + v_lin, with x0 the particle's
+// position given at dfsph_set_boundary (upload order); psi is kept. i runs over the sorted slots.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) rigid_boundary_kernel(const float* __restrict__ rest, uint32_t n,
+                                                                const uint32_t* __restrict__ bid, RigidMotion m,
+                                                                Vec4<Real>* __restrict__ bpos,
+                                                                Vec4<Real>* __restrict__ bvel) {
+    DFSPH_PDL_ENTER;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = bid[i];
+    if (t - m.first >= m.count) return;  // unsigned: also t < first
+    const Real x0 = (Real)rest[3 * (size_t)t], y0 = (Real)rest[3 * (size_t)t + 1], z0 = (Real)rest[3 * (size_t)t + 2];
+    const Real R[9] = {(Real)m.R[0], (Real)m.R[1], (Real)m.R[2], (Real)m.R[3], (Real)m.R[4],
+                       (Real)m.R[5], (Real)m.R[6], (Real)m.R[7], (Real)m.R[8]};
+    const Real px = (Real)m.p[0], py = (Real)m.p[1], pz = (Real)m.p[2];
+    Vec4<Real> x = bpos[i];
+    x.x = R[0] * x0 + R[1] * y0 + R[2] * z0 + px;
+    x.y = R[3] * x0 + R[4] * y0 + R[5] * z0 + py;
+    x.z = R[6] * x0 + R[7] * y0 + R[8] * z0 + pz;
+    bpos[i] = x;
+    const Real rx = x.x - px, ry = x.y - py, rz = x.z - pz;
+    const Real wx = (Real)m.w[0], wy = (Real)m.w[1], wz = (Real)m.w[2];
+    Vec4<Real> v;
+    v.x = wy * rz - wz * ry + (Real)m.v[0];
+    v.y = wz * rx - wx * rz + (Real)m.v[1];
+    v.z = wx * ry - wy * rx + (Real)m.v[2];
+    v.w = Real(0);
+    bvel[i] = v;
+}
+
 // Field download: element c of slot i of src (stride src_stride Real elements) goes to
 // dst[(id ? id[i] : i) * comps + c], converted to Out.
 template <class Real, class Out>
@@ -245,6 +278,11 @@ void launch_move_boundary(const float* xyz, const float* vxyz, uint32_t n, const
                           Vec4<Real>* bvel, cudaStream_t s) {
     if (n) launch_pdl(move_boundary_kernel<Real>, grid_for(n), kBlock, 0, s, xyz, vxyz, n, bid, bpos, bvel);
 }
+template <class Real>
+void launch_rigid_boundary(const float* rest, uint32_t n, const uint32_t* bid, const RigidMotion& m, Vec4<Real>* bpos,
+                           Vec4<Real>* bvel, cudaStream_t s) {
+    if (n) launch_pdl(rigid_boundary_kernel<Real>, grid_for(n), kBlock, 0, s, rest, n, bid, m, bpos, bvel);
+}
 template <class Real, class Out>
 void launch_pack_field(const Real* src, int src_stride, int comps, const uint32_t* id, uint32_t n, Out* dst,
                        cudaStream_t s) {
@@ -269,6 +307,8 @@ void launch_unpack_counts(const uint32_t* counts, const uint32_t* id, uint32_t n
                                              Vec4<R>*, uint32_t*, cudaStream_t);                                     \
     template void launch_move_boundary<R>(const float*, const float*, uint32_t, const uint32_t*, Vec4<R>*, Vec4<R>*, \
                                           cudaStream_t);                                                             \
+    template void launch_rigid_boundary<R>(const float*, uint32_t, const uint32_t*, const RigidMotion&, Vec4<R>*,    \
+                                           Vec4<R>*, cudaStream_t);                                                  \
     template void launch_pack_field<R, float>(const R*, int, int, const uint32_t*, uint32_t, float*, cudaStream_t);  \
     template void launch_pack_field<R, double>(const R*, int, int, const uint32_t*, uint32_t, double*, cudaStream_t);
 

@@ -38,6 +38,15 @@ void launch_reorder_boundary(const uint32_t* perm, uint32_t n, const Vec4<Real>*
 template <class Real>
 void launch_move_boundary(const float* xyz, const float* vxyz, uint32_t n, const uint32_t* bid, Vec4<Real>* bpos,
                           Vec4<Real>* bvel, cudaStream_t s);
+// Rotation (row-major), translation, linear and angular velocity of one rigid range of boundary
+// particles (upload indices [first, first + count)).
+struct RigidMotion {
+    double R[9], p[3], v[3], w[3];
+    uint32_t first, count;
+};
+template <class Real>
+void launch_rigid_boundary(const float* rest, uint32_t n, const uint32_t* bid, const RigidMotion& m, Vec4<Real>* bpos,
+                           Vec4<Real>* bvel, cudaStream_t s);
 template <class Real, class Out>
 void launch_pack_field(const Real* src, int src_stride, int comps, const uint32_t* id, uint32_t n, Out* dst,
                        cudaStream_t s);

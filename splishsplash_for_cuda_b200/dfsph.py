@@ -370,6 +370,18 @@ class DFSPHCUDA:
         v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32)
         self._call(self._lib.dfsph_move_boundary(self._ctx, _fptr(x), _fptr(v)))
 
+    def move_boundary_rigid(self, first: int = 0, count: int | None = None, q=None, position=None, velocity=None,
+                            angular_velocity=None) -> None:
+        """Rigid motion of the boundary particles [first, first + count) on the device
+        (update_dynamicObject_UnifiedParticleSet_cuda): x = R(q) x0 + position, v = angular_velocity x
+        (x - position) + velocity, x0 the positions given to set_boundary; q = (w, x, y, z)."""
+        if count is None:
+            count = int(self.get_param("num_boundary")) - first
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in
+                (q, position, velocity, angular_velocity)]
+        ptrs = [None if a is None else a.ctypes.data_as(C.c_void_p) for a in arrs]
+        self._call(self._lib.dfsph_move_boundary_rigid(self._ctx, int(first), int(count), *ptrs))
+
     # ---- snapshots (DFSPHCUDA::handleSimulationSave / handleSimulationLoad) ----------------------
     def save_snapshot(self, folder, fluid: bool = True, boundary: bool = True) -> None:
         """Writes fluid_file.txt, general_data.txt and boundaries_file.txt (reference text format)."""

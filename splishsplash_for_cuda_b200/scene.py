@@ -319,6 +319,14 @@ def synthetic_scene(config: int, jitter: float = 0.01, time_step: float | None =
                  box_min=(0.0, 0.0, 0.0), box_max=tuple(box), meta=dict(config=config, seed=spec["seed"]))
 
 
+def sloshing_wall_motion(t: float, amplitude: float = 0.1, period: float = 2.0):
+    """The sloshing tank's prescribed wall motion at simulated time t: a rigid translation along x,
+    x(t) = amplitude sin(2 pi t / period). Returns (position, velocity) of the walls' frame, for
+    DFSPHCUDA.move_boundary_rigid."""
+    w = 2.0 * np.pi / period
+    return (amplitude * np.sin(w * t), 0.0, 0.0), (amplitude * w * np.cos(w * t), 0.0, 0.0)
+
+
 def column_scene(counts=(10, 80, 10), radius: float = 0.008, time_step: float = 0.004, max_error: float = 0.005,
                  jitter: float = 0.01, seed: int = 4, headroom: float = 1.25) -> Scene:
     """A tall resting water column in a tank that fits its footprint (the lid `headroom` times the

@@ -297,6 +297,40 @@ def test_moving_boundary_lockstep_with_oracle():
         check_field(name, d.field(name, np.float64), o.field(name), 1e-4)
 
 
+def test_rigid_boundary_motion_equals_host_motion():
+    """dfsph_move_boundary_rigid moves a range of boundary particles on the device as the reference's
+    update_dynamicObject does (x = R x0 + p, v = w x (x - p) + v_lin). Against the same motion computed
+    on the host and uploaded with dfsph_move_boundary: boundary positions within 1e-6 m and
+    velocities within 1e-6 m/s (FP32 rounding of R x0 + p), particles outside the range untouched,
+    and five steps of fluid in lockstep (same iteration counts, positions within 1e-5 m)."""
+    s = synthetic_scene(1, counts=(12, 12, 12))
+    a, b = DFSPHCUDA(s), DFSPHCUDA(s)
+    b0 = s.boundary.astype(np.float64)
+    nb = b0.shape[0]
+    first, count = nb // 3, nb // 2
+    theta = 0.05
+    q = np.array([np.cos(theta / 2), 0.0, np.sin(theta / 2), 0.0])
+    R = np.array([[np.cos(theta), 0.0, np.sin(theta)], [0.0, 1.0, 0.0], [-np.sin(theta), 0.0, np.cos(theta)]])
+    for k in range(5):
+        p = np.array([0.02 * k, 0.0, -0.01 * k])
+        v = np.array([0.2, 0.0, -0.1])
+        w = np.array([0.0, 0.3, 0.0])
+        a.move_boundary_rigid(first, count, q, p, v, w)
+        x = b0.copy()
+        vel = np.zeros_like(b0)
+        x[first:first + count] = b0[first:first + count] @ R.T + p
+        vel[first:first + count] = np.cross(w, x[first:first + count] - p) + v
+        b.move_boundary(x.astype(np.float32), vel.astype(np.float32))
+        xa, xb = a.field("boundary_position", np.float64), b.field("boundary_position", np.float64)
+        assert np.abs(xa - xb).max() <= 1e-6
+        assert np.array_equal(xa[:first], b0[:first]) and np.array_equal(xa[first + count:], b0[first + count:])
+        va, vb = a.field("boundary_velocity", np.float64), b.field("boundary_velocity", np.float64)
+        assert np.abs(va - vb).max() <= 1e-6
+        sa, sb = a.step(), b.step()
+        assert (sa.iterations, sa.iterations_v) == (sb.iterations, sb.iterations_v), k
+    assert np.abs(a.positions(np.float64) - b.positions(np.float64)).max() <= 1e-5
+
+
 def test_particles_outside_domain_box_removed_like_reference():
     """DFSPHCUDA::step ends with checkParticlesPositions(2): particles outside the boundary's box are
     removed, the others keep their order (ids renumbered densely). Seven particles start outside the
