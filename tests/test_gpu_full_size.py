@@ -55,3 +55,46 @@ def test_full_size_fp32_tracks_fp64(cuda_lib):
     e = np.abs(xa - xb).max(1)
     assert np.median(e) <= 2e-4 and np.quantile(e, 0.99) <= 2e-3
     assert np.abs(xa.mean(0) - xb.mean(0)).max() <= 2e-5
+
+
+def test_fp32_vs_fp64_build_500_steps(cuda_lib):
+    """The 250,047-particle dam break over 500 CFL steps, FP32 and FP64 builds of the same kernels
+    (0.36 s of flow: release, impact on the far wall, run-up). Measured per field (one B200):
+
+    step | position median / 99 % / max [m] | velocity median / max [m/s] | density median / max [kg/m^3]
+       1 | 2.3e-8 / 3.7e-8 / 3.7e-8         | 4.4e-10 / 1.7e-8            | 4.3e-6 / 2.9e-5
+       5 | 4.4e-8 / 1.2e-7 / 6.5e-6         | 1.6e-9 / 5.2e-4             | 6.9e-6 / 3.4e-2
+      20 | 4.4e-5 / 3.9e-4 / 1.9e-3         | 3.7e-3 / 0.13               | 0.22 / 33
+     100 | 2.1e-3 / 2.1e-2 / 4.6e-2         | 5.8e-2 / 1.1                | 4.1 / 232
+     500 | 1.4e-2 / 7.7e-2 / 0.80           | 0.17 / 10                   | 4.7 / 745
+
+    Until the front reaches the wall the builds agree to rounding; afterwards each build's solves
+    stop at their own residuals below the 0.01 % tolerance and the splash (velocities up to 11 m/s)
+    amplifies those differences like any chaotic flow, so single particles separate while the flow
+    stays the same: every one of the 500 steps took the same iteration counts in both builds, and
+    at step 500 the centres of mass differ by 3.0e-3 m (at most 3.7e-3 m over the run), the kinetic
+    energies by 0.8 % (at most 1.4 %), the mean densities by 0.12 %. Bounds: rounding-level
+    agreement through step 5, then the aggregates within about 3x the measured gaps."""
+    s = synthetic_scene(2, cfl=True)
+    a, b = DFSPHCUDA(s, precision=32), DFSPHCUDA(s, precision=64)
+    same, com, ke = 0, [], []
+    for k in range(500):
+        sa, sb = a.step(), b.step()
+        assert sa.status & BAD == 0 and sb.status & BAD == 0, k
+        same += (sa.iterations, sa.iterations_v) == (sb.iterations, sb.iterations_v)
+        if k == 4:
+            e = np.linalg.norm(a.positions(np.float64) - b.positions(np.float64), axis=1)
+            assert np.median(e) <= 1e-6 and e.max() <= 5e-5
+        if k % 50 == 49:
+            xa, xb = a.positions(np.float64), b.positions(np.float64)
+            va, vb = a.velocities(np.float64), b.velocities(np.float64)
+            com.append(np.abs(xa.mean(0) - xb.mean(0)).max())
+            kb = (vb ** 2).sum(1).mean()
+            ke.append(abs((va ** 2).sum(1).mean() - kb) / kb)
+    assert same >= 475
+    assert max(com) <= 1.2e-2
+    assert max(ke) <= 0.05
+    ra, rb = a.field("density", np.float64), b.field("density", np.float64)
+    assert abs(ra.mean() - rb.mean()) <= 5e-3 * rb.mean()
+    e = np.linalg.norm(a.positions(np.float64) - b.positions(np.float64), axis=1)
+    assert np.median(e) <= 5e-2
