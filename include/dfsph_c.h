@@ -52,6 +52,8 @@ typedef struct dfsph_ctx dfsph_ctx;
 #define DFSPH_ST_FLUID_CAPACITY 0x80u    /* an open-boundary inflow was cut at fluid_capacity        */
 #define DFSPH_ST_MMA_TIMEOUT 0x100u      /* a bounded wait for the warm-start network's tensor-core MMA
                                             gave up (no hang; that call's predictions are unspecified) */
+#define DFSPH_ST_INDEX 0x200u            /* checked build only: a neighbour-list entry, a list count or a
+                                            cell-table run was out of range and was skipped, not read */
 
 /* ---- scene / solver parameters ---------------------------------------------------------------- */
 /* Mirrors the "Configuration" keys of the reference JSON scene (Utilities/SceneLoader.cpp:39-160)

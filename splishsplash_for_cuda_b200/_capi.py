@@ -9,6 +9,7 @@ import os
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libdfsph_b200.so"
+CHECKED_LIB_PATH = Path(__file__).resolve().parent / "libdfsph_b200_checked.so"  # range-checked variant
 
 DFSPH_OK = 0
 DFSPH_E_INVALID = -1
@@ -26,6 +27,7 @@ ST_SORT_TIMEOUT = 0x20
 ST_BOUNDARY_OVERFLOW = 0x40
 ST_FLUID_CAPACITY = 0x80
 ST_MMA_TIMEOUT = 0x100
+ST_INDEX = 0x200
 
 SURFACE_PLANE, SURFACE_CUBOID, SURFACE_CYLINDER, SURFACE_SPHERE, SURFACE_STAR = 0, 1, 2, 4, 5
 

@@ -21,6 +21,10 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libdfsph_b200.so"
 OBJ = PKG / "_build"
+# The checked variant: every neighbour-list entry, list count and cell-table run is range-checked on
+# the device (DFSPH_ST_INDEX instead of an out-of-range read); for debugging and the tests.
+CHECKED_OUT = PKG / "libdfsph_b200_checked.so"
+CHECKED_OBJ = PKG / "_build_checked"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -99,14 +103,23 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
     return OUT_
 
 
+def build_checked(force: bool = False, verbose: bool = False) -> Path:
+    """Builds libdfsph_b200_checked.so (-DDFSPH_CHECKED) beside the product library."""
+    return build(force=force, verbose=verbose, extra_flags=["-DDFSPH_CHECKED"], out=CHECKED_OUT,
+                 obj_dir=CHECKED_OBJ)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-v", "--verbose", action="store_true")
     ap.add_argument("--ptxas-info", action="store_true", help="print registers/spills per kernel")
+    ap.add_argument("--checked", action="store_true", help="also build libdfsph_b200_checked.so")
     a = ap.parse_args()
     extra = ["-Xptxas", "-v"] if a.ptxas_info else None
     print(build(force=a.force or a.ptxas_info, verbose=a.verbose or a.ptxas_info, extra_flags=extra))
+    if a.checked:
+        print(build_checked(force=a.force, verbose=a.verbose))
 
 
 if __name__ == "__main__":

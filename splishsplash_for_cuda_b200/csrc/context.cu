@@ -140,6 +140,9 @@ public:
     // Ablation of the learned warm start: the needed-coefficient base with the network's correction
     // fixed at zero (no inference, no training).
     bool base_only = false;
+    // Test hook of the checked build: the next neighbour search writes index n + corrupt_neighbor - 1
+    // into particle 0's list (0: off).
+    uint32_t corrupt_neighbor = 0;
     Real* kappaT[2] = {nullptr, nullptr};
     Real* kappaVT[2] = {nullptr, nullptr};
     Real *kappaW = nullptr, *kappaVW = nullptr, *kappaP = nullptr, *kappaVP = nullptr;
@@ -685,6 +688,11 @@ public:
         DF_TRY(bin_fluid());
         launch_build_neighbors<Real>(ds, n, ftab, btab, stream);
         launches += 1;
+        if (corrupt_neighbor) {  // checked builds only (the key is rejected otherwise); one search
+            launch_corrupt_first_neighbor(nbr, counts, n + corrupt_neighbor - 1u, stream);
+            corrupt_neighbor = 0;
+            launches += 1;
+        }
         DF_CUDA(cudaGetLastError());
         return DFSPH_OK;
     }
@@ -2077,6 +2085,15 @@ public:
         else if (k == "learned_warm_start") return enable_learned(v != 0);
         else if (k == "warm_start_probe") probe = v != 0;
         else if (k == "learned_base_only") base_only = v != 0;
+        else if (k == "checked_corrupt_neighbor") {
+#ifdef DFSPH_CHECKED
+            DF_CHECK(v >= 1 && v <= 64 && n + (uint32_t)v <= Nc, DFSPH_E_INVALID,
+                     "checked_corrupt_neighbor must be in [1, 64] and stay inside fluid_capacity");
+            corrupt_neighbor = (uint32_t)v;
+#else
+            DF_CHECK(false, DFSPH_E_INVALID, "checked_corrupt_neighbor exists only in the checked build");
+#endif
+        }
         else if (k == "sort_withhold_tile") sort_withheld_tile = v < 0 ? kNoWithheldTile : (uint32_t)v;
         else if (k == "remove_escaped") remove_escaped = v != 0;
         else if (k == "boundary_forces") {
@@ -2166,6 +2183,13 @@ public:
         else if (k == "learned_warm_start") *v = learned ? 1 : 0;
         else if (k == "warm_start_probe") *v = probe ? 1 : 0;
         else if (k == "learned_base_only") *v = base_only ? 1 : 0;
+        else if (k == "checked_build") {
+#ifdef DFSPH_CHECKED
+            *v = 1;
+#else
+            *v = 0;
+#endif
+        }
         else if (k == "boundary_forces") *v = boundary_forces ? 1 : 0;
         else if (k == "remove_escaped") *v = remove_escaped ? 1 : 0;
         else if (k == "escaped_removed") *v = (double)escaped_removed;

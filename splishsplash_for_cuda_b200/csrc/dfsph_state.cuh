@@ -75,6 +75,8 @@ void launch_cell_bounds(const uint32_t* sorted_keys, uint32_t n, int dim_x, int 
 template <class Real>
 void launch_build_neighbors(const DevState<Real>* d, uint32_t n, const uint2* fluid_table, const uint2* boundary_table,
                             cudaStream_t s);
+// Checked builds only (a no-op otherwise): particle 0's first list entry := value.
+void launch_corrupt_first_neighbor(uint32_t* nbr, const uint32_t* counts, uint32_t value, cudaStream_t s);
 template <class Real>
 void launch_boundary_psi(const Vec4<Real>* bpos_in, Vec4<Real>* bpos_out, uint32_t nb, const StepParams<Real>& p,
                          const uint2* boundary_table, uint32_t* status, cudaStream_t s);

@@ -100,6 +100,31 @@ __global__ void __launch_bounds__(kBlock) cell_bounds_kernel(const uint32_t* __r
     if (i == n - 1 || keys[i + 1] != k) table[lin].y = i + 1;
 }
 
+// A cell-table run [r.x, r.y) of a set of `limit` particles. Checked builds verify it and raise
+// DFSPH_ST_INDEX instead of scanning a run out of range; the unchecked build trusts the table.
+__device__ __forceinline__ bool run_in_range(uint2 r, uint32_t limit, uint32_t* status) {
+#ifdef DFSPH_CHECKED
+    if (r.x > r.y || r.y > limit) {
+        atomicOr(status, DFSPH_ST_INDEX);
+        return false;
+    }
+#else
+    (void)r;
+    (void)limit;
+    (void)status;
+#endif
+    return true;
+}
+
+#ifdef DFSPH_CHECKED
+// Test hook of the checked build: replaces particle 0's first list entry by `value` (an index past the
+// fluid count, inside the allocation), which the checked gathers must report and skip.
+__global__ void corrupt_first_neighbor_kernel(uint32_t* __restrict__ nbr, const uint32_t* __restrict__ counts,
+                                              uint32_t value) {
+    if (threadIdx.x == 0 && (counts[0] & 0xFFFFu) > 0) nbr[0] = value;
+}
+#endif
+
 // One thread per fluid particle: fluid neighbours (self excluded) then boundary neighbours, cells in
 // a fixed order (z, y, x from -1 to +1), particles of a cell in sorted order. Lists are written
 // interleaved (nbr[k * stride + i]) so that the gathers read them coalesced.
@@ -159,6 +184,7 @@ __global__ void __launch_bounds__(kBlock) build_neighbors_kernel(const DevState<
                     const int x = cx + dx;
                     if (x < 0 || x >= p.dim_x) continue;
                     const uint2 r = ftab[cell_linear(x, y, z, p.dim_x, p.dim_y)];
+                    if (!run_in_range(r, n, ds->status)) continue;
                     scan_cell<Real, true>(pos, r.x, r.y, i, xi, H2, nbr, stride, cap, total, nf, overflow);
                 }
             }
@@ -174,6 +200,7 @@ __global__ void __launch_bounds__(kBlock) build_neighbors_kernel(const DevState<
                         const int x = cx + dx;
                         if (x < 0 || x >= p.dim_x) continue;
                         const uint2 r = btab[cell_linear(x, y, z, p.dim_x, p.dim_y)];
+                        if (!run_in_range(r, p.n_boundary, ds->status)) continue;
                         scan_cell<Real, false>(bpos, r.x, r.y, i, xi, H2, nbr, stride, cap, total, nb, overflow);
                     }
                 }
@@ -210,6 +237,7 @@ __global__ void __launch_bounds__(kBlock) boundary_psi_kernel(const Vec4<Real>* 
                     const int x = cx + dx;
                     if (x < 0 || x >= p.dim_x) continue;
                     const uint2 r = btab[cell_linear(x, y, z, p.dim_x, p.dim_y)];
+                    if (!run_in_range(r, nb, status)) continue;
                     for (uint32_t j = r.x; j < r.y; ++j) {
                         if (j == b) continue;
                         const Vec4<Real> xj = bpos_in[j];
@@ -282,6 +310,16 @@ template <class Real>
 void launch_build_neighbors(const DevState<Real>* d, uint32_t n, const uint2* fluid_table, const uint2* boundary_table,
                             cudaStream_t s) {
     if (n) launch_pdl(build_neighbors_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, fluid_table, boundary_table);
+}
+void launch_corrupt_first_neighbor(uint32_t* nbr, const uint32_t* counts, uint32_t value, cudaStream_t s) {
+#ifdef DFSPH_CHECKED
+    corrupt_first_neighbor_kernel<<<1, 32, 0, s>>>(nbr, counts, value);
+#else
+    (void)nbr;
+    (void)counts;
+    (void)value;
+    (void)s;
+#endif
 }
 template <class Real>
 void launch_boundary_psi(const Vec4<Real>* bpos_in, Vec4<Real>* bpos_out, uint32_t nb, const StepParams<Real>& p,

@@ -30,6 +30,13 @@ def test_library_exports_every_declared_symbol(cuda_lib):
         assert hasattr(cuda_lib, name), name
 
 
+def test_checked_library_exports_every_declared_symbol():
+    """The range-checked variant (libdfsph_b200_checked.so) offers the same C ABI."""
+    lib = _capi.load(_capi.CHECKED_LIB_PATH)
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+
+
 def test_scene_defaults_match_reference_timestep(cuda_lib):
     s = _capi.DfsphScene()
     assert cuda_lib.dfsph_scene_defaults(C.byref(s)) == 0
