@@ -9,6 +9,9 @@
  *                                                        onSimulationStepEnd, readDynamicData,
  *                                                        getFluidParticlesCount, h / h_future / h_past
  *   cuda_* host functions (DFSPH_core_cuda.h:27-74)     dfsph::cuda_* with the same arguments
+ *   SPH::TimeStepDFSPH (TimeStepDFSPH.h:20-48)          dfsph::TimeStepDFSPH: the same TimeStep
+ *                                                        interface on the device time step
+ *   SceneLoader::readScene (SceneLoader.cpp:39-320)     dfsph::SceneData::load (dfsph_scene_load)
  *
  * Header-only; link with libdfsph_b200.so. Errors throw dfsph::Error (code + dfsph_last_error
  * message) where the reference calls exit(). The scene is given as plain arrays (the reference builds
@@ -87,9 +90,39 @@ private:
     dfsph_ctx* ctx_;
 };
 
+/* A reference JSON scene read by the library (dfsph_scene_load): the solver parameters and the
+ * particle arrays (SceneLoader::readScene + the scene part of DemoBase::buildModel). */
+struct SceneData {
+    dfsph_scene scene{};
+    std::vector<float> fluid, fluid_vel, boundary;  // fluid_vel empty when the scene gives none
+
+    static SceneData load(const std::string& json_path) {
+        SceneData d;
+        dfsph_scene_file* f = nullptr;
+        check(nullptr, dfsph_scene_load(json_path.c_str(), &d.scene, &f));
+        uint32_t n = 0, nb = 0;
+        int has_vel = 0;
+        int code = dfsph_scene_file_counts(f, &n, &nb, &has_vel);
+        if (code == DFSPH_OK) {
+            d.fluid.resize(3 * (size_t)n);
+            d.boundary.resize(3 * (size_t)nb);
+            if (has_vel) d.fluid_vel.resize(3 * (size_t)n);
+            code = dfsph_scene_file_fluid(f, d.fluid.data(), has_vel ? d.fluid_vel.data() : nullptr);
+        }
+        if (code == DFSPH_OK) code = dfsph_scene_file_boundary(f, d.boundary.data());
+        dfsph_scene_file_free(f);
+        check(nullptr, code);
+        return d;
+    }
+};
+
 /* SPH::DFSPHCUDA over one context. The arrays passed to the constructor are kept for reset(). */
 class DFSPHCUDA {
 public:
+    /* From a reference JSON scene (its learnedWarmStart block is applied by
+     * dfsph_create_from_scene_file; here the learned mode is set with set()). */
+    explicit DFSPHCUDA(const std::string& scene_json) : DFSPHCUDA(SceneData::load(scene_json)) {}
+    explicit DFSPHCUDA(const SceneData& d) : DFSPHCUDA(d.scene, d.fluid, d.boundary, d.fluid_vel) {}
     DFSPHCUDA(const dfsph_scene& scene, std::vector<float> fluid_xyz, std::vector<float> boundary_xyz,
               std::vector<float> fluid_vel = {}, std::vector<float> boundary_psi = {})
         : fluid_(std::move(fluid_xyz)), vel_(std::move(fluid_vel)), boundary_(std::move(boundary_xyz)),
@@ -156,11 +189,7 @@ public:
 
     const dfsph_step_stats& lastStats() const { return stats_; }
     dfsph_ctx* handle() const { return ctx_; }
-
-    DFSPHCData m_data;
-    unsigned int m_iterations = 0, m_iterationsV = 0;
-
-private:
+    /* Any dfsph_set_param / dfsph_get_param key (e.g. "learned_warm_start", "boundary_forces"). */
     double get(const char* key) const {
         double v = 0;
         check(ctx_, dfsph_get_param(ctx_, key, &v));
@@ -168,9 +197,23 @@ private:
     }
     void set(const char* key, double v) { check(ctx_, dfsph_set_param(ctx_, key, v)); }
 
+    DFSPHCData m_data;
+    unsigned int m_iterations = 0, m_iterationsV = 0;
+
+private:
+
     dfsph_ctx* ctx_ = nullptr;
     dfsph_step_stats stats_{};
     std::vector<float> fluid_, vel_, boundary_, psi_;
+};
+
+/* SPH::TimeStepDFSPH (TimeStepDFSPH.h:20-48), the reference's CPU solver class, on the device time
+ * step: the same public methods (step, reset, get/setEnableDivergenceSolver and the TimeStep
+ * parameters of TimeStep.h:70-103), so code written against TimeStepDFSPH runs unchanged apart from
+ * its construction, which takes the scene (arrays or a JSON scene file) instead of a FluidModel. */
+class TimeStepDFSPH : public DFSPHCUDA {
+public:
+    using DFSPHCUDA::DFSPHCUDA;
 };
 
 /* The host functions of DFSPH_core_cuda.h:27-74 (same arguments; RealCuda -> double). */

@@ -83,6 +83,26 @@ typedef struct dfsph_scene {
     double grid_max[3];           /*   grid_max on every axis, otherwise the boundary bounding box    */
 } dfsph_scene;
 
+/* ---- scene files (reference JSON format) --------------------------------------------------------- */
+/* A reference JSON scene read by the library (Utilities/SceneLoader.cpp:39-320 keys: Configuration,
+ * FluidBlocks in dense mode, FluidModels and RigidBodies with .bgeo particle files, box walls sampled
+ * as a single-layer lattice of spacing 2r; extension keys seed, jitter, precision, learnedWarmStart),
+ * so that C and C++ callers need no other reader. Replaces SceneLoader::readScene + the scene part of
+ * DemoBase::buildModel (Demos/Common/DemoBase.cpp:539-603). */
+typedef struct dfsph_scene_file dfsph_scene_file;
+/* Reads json_path; scene (nullable) receives the solver parameters with capacities equal to the
+ * particle counts. *out must be released with dfsph_scene_file_free. Errors: DFSPH_E_INVALID with
+ * the reason in dfsph_last_error(NULL). */
+int dfsph_scene_load(const char* json_path, dfsph_scene* scene, dfsph_scene_file** out);
+int dfsph_scene_file_counts(const dfsph_scene_file* f, uint32_t* n_fluid, uint32_t* n_boundary, int* has_velocity);
+/* 3 floats per particle; vxyz (nullable) is zero where the scene gives no velocity. */
+int dfsph_scene_file_fluid(const dfsph_scene_file* f, float* xyz, float* vxyz);
+int dfsph_scene_file_boundary(const dfsph_scene_file* f, float* xyz);
+void dfsph_scene_file_free(dfsph_scene_file* f);
+/* dfsph_scene_load + dfsph_create + dfsph_set_boundary + dfsph_upload_fluid, and the scene's
+ * learnedWarmStart block applied (DemoBase::buildModel + DFSPHCUDA(FluidModel*), DFSPH_CUDA.cpp:38). */
+int dfsph_create_from_scene_file(const char* json_path, dfsph_ctx** out);
+
 /* ---- per-step statistics ---------------------------------------------------------------------- */
 typedef struct dfsph_step_stats {
     int32_t iterations;           /* pressure iterations (TimeStep::getIterationCount)               */

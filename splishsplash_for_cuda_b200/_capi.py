@@ -171,6 +171,12 @@ SIGNATURES = {
     "dfsph_mlp_train": (C.c_int, [_P, _F, _F, C.c_uint32, C.c_int32, C.c_double, C.POINTER(C.c_double)]),
     "dfsph_mlp_reset": (C.c_int, [_P, C.c_uint32]),
     "dfsph_sort_cell_keys_noalloc": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_int, _P]),
+    "dfsph_scene_load": (C.c_int, [C.c_char_p, C.POINTER(DfsphScene), C.POINTER(C.c_void_p)]),
+    "dfsph_scene_file_counts": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int)]),
+    "dfsph_scene_file_fluid": (C.c_int, [_P, _P, _P]),
+    "dfsph_scene_file_boundary": (C.c_int, [_P, _P]),
+    "dfsph_scene_file_free": (None, [_P]),
+    "dfsph_create_from_scene_file": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
 }
 
 MLP_INPUTS, MLP_OUTPUTS, MLP_PARAMS = 8, 2, 4866

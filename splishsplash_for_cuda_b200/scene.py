@@ -270,6 +270,31 @@ def load_scene(path: str | Path) -> Scene:
     )
 
 
+def load_scene_native(path: str | Path) -> tuple:
+    """Reads a reference JSON scene with the library's own reader (dfsph_scene_load, the path C and
+    C++ callers use). Returns (dfsph_scene struct, fluid (N, 3) float32, fluid velocity (N, 3) float32
+    or None, boundary (B, 3) float32)."""
+    import ctypes as C
+
+    from . import _capi
+
+    lib = _capi.load()
+    sc = _capi.DfsphScene()
+    h = C.c_void_p()
+    _capi.check(lib, None, lib.dfsph_scene_load(str(path).encode(), C.byref(sc), C.byref(h)))
+    try:
+        n, nb, hv = C.c_uint32(), C.c_uint32(), C.c_int()
+        _capi.check(lib, None, lib.dfsph_scene_file_counts(h, C.byref(n), C.byref(nb), C.byref(hv)))
+        x = np.zeros((n.value, 3), np.float32)
+        v = np.zeros((n.value, 3), np.float32)
+        b = np.zeros((nb.value, 3), np.float32)
+        _capi.check(lib, None, lib.dfsph_scene_file_fluid(h, x.ctypes.data_as(C.c_void_p), v.ctypes.data_as(C.c_void_p)))
+        _capi.check(lib, None, lib.dfsph_scene_file_boundary(h, b.ctypes.data_as(C.c_void_p)))
+    finally:
+        lib.dfsph_scene_file_free(h)
+    return sc, x, (v if hv.value else None), b
+
+
 # Synthetic scenes of the five benchmark configurations. Every box dimension is twice the stated
 # one because a lattice of spacing 2r with the stated particle counts does not fit the stated boxes
 # (e.g. 30 x 2r = 1.5 m of fluid for a 1 m box); N, r, spacing, h = 4r, mass, dt and tolerances are

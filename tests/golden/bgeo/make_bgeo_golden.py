@@ -24,7 +24,8 @@ ROOT = HERE.parents[2]
 sys.path.insert(0, str(ROOT))
 from splishsplash_for_cuda_b200.scene import read_bgeo  # noqa: E402
 
-REF_DIR = Path(os.environ.get("REF_DIR", "/root/reference"))
+# the reference checkout: REF_DIR, else a directory named "reference" beside this repository
+REF_DIR = Path(os.environ.get("REF_DIR", str(ROOT.parent / "reference")))
 
 
 def pin():

@@ -88,3 +88,63 @@ def test_facade_matches_python_facade(tmp_path, cuda_lib, cfl):
     assert (its, itv) == (ti, tv)
     assert np.array_equal(xf, d.positions()) and np.array_equal(vf, d.velocities())
     assert np.array_equal(xp, xf) and np.array_equal(vp, vf)
+
+
+def build_timestep_demo(tmp_path: Path) -> Path:
+    _capi.load()
+    exe = tmp_path / "timestep_demo"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"),
+                    str(ROOT / "tests" / "cpp" / "timestep_demo.cpp"), "-L", str(LIBDIR), "-ldfsph_b200",
+                    f"-Wl,-rpath,{LIBDIR}", "-o", str(exe)], check=True)
+    return exe
+
+
+def _scene_json(tmp_path: Path, cfl: int = 1) -> Path:
+    import json
+
+    r = 0.025
+    scene = {"Configuration": {"particleRadius": r, "timeStepSize": 0.005, "cflMethod": cfl, "cflFactor": 0.4,
+                               "cflMaxTimeStepSize": 0.005, "maxError": 0.01, "maxErrorV": 0.1, "jitter": 0.01,
+                               "seed": 4},
+             "FluidBlocks": [{"denseMode": 0, "start": [0.0, 0.0, 0.0], "end": [13 * 2 * r] * 3}],
+             "RigidBodies": [{"geometryFile": "../models/UnitBox.obj", "translation": [0.5, 0.5, 0.5],
+                              "scale": [1.0, 1.0, 1.0]}]}
+    p = tmp_path / "scene.json"
+    p.write_text(json.dumps(scene))
+    return p
+
+
+def test_timestep_facade_reads_scene_without_python(tmp_path):
+    """The C++ TimeStepDFSPH facade's scene reader (dfsph_scene_load) needs no GPU and no Python."""
+    from splishsplash_for_cuda_b200.scene import load_scene
+
+    exe = build_timestep_demo(tmp_path)
+    p = _scene_json(tmp_path)
+    r = subprocess.run([str(exe), "--load", str(p)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    s = load_scene(p)
+    assert r.stdout.split() == ["fluid", str(s.n_fluid), "boundary", str(s.n_boundary), "radius", "0.025"]
+
+
+@pytest.mark.gpu
+def test_timestep_facade_from_json_matches_python_facade(tmp_path, cuda_lib):
+    from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
+    from splishsplash_for_cuda_b200.scene import load_scene
+
+    exe = build_timestep_demo(tmp_path)
+    p = _scene_json(tmp_path)
+    r = subprocess.run([str(exe), str(p), "10", str(tmp_path / "o.bin")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    b = (tmp_path / "o.bin").read_bytes()
+    (n,) = struct.unpack_from("<i", b, 0)
+    x = np.frombuffer(b, np.float32, 3 * n, 4).reshape(n, 3)
+    v = np.frombuffer(b, np.float32, 3 * n, 4 + 12 * n).reshape(n, 3)
+    its, itv = struct.unpack_from("<ii", b, 4 + 24 * n)
+    d = DFSPHCUDA(load_scene(p))
+    ti = tv = 0
+    for _ in range(10):
+        st = d.step()
+        ti += st.iterations
+        tv += st.iterations_v
+    assert (its, itv) == (ti, tv)
+    assert np.array_equal(x, d.positions()) and np.array_equal(v, d.velocities())

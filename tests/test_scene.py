@@ -69,3 +69,113 @@ def test_json_extensions_configure_the_solver(cuda_lib, tmp_path):
     assert d.get_param("learned_warm_start") == 1 and d.get_param("train_interval") == 25
     assert d.get_param("warm_start_damping") == 0.9
     assert d.step().status == 0
+
+
+# ---- the library's own JSON reader (dfsph_scene_load), for C and C++ callers -------------------------
+def _check_native_equals_python(path, atol=0.0):
+    from splishsplash_for_cuda_b200.scene import load_scene_native
+
+    s = load_scene(path)
+    sc, x, v, b = load_scene_native(path)
+    assert x.shape == s.fluid.shape and b.shape == s.boundary.shape
+    if atol == 0.0:
+        assert np.array_equal(x, s.fluid) and np.array_equal(b, s.boundary)
+    else:
+        assert np.abs(x - s.fluid).max() <= atol and np.abs(b - s.boundary).max() <= atol
+    if s.fluid_velocity is None:
+        assert v is None
+    else:
+        assert np.array_equal(v, s.fluid_velocity)
+    c = s.config
+    assert (sc.particle_radius, sc.density0, sc.viscosity, tuple(sc.gravitation), sc.time_step) == \
+        (c.particleRadius, c.density0, c.viscosity, tuple(c.gravitation), c.timeStepSize)
+    assert (sc.max_iterations, sc.max_error, sc.max_iterations_v, sc.max_error_v) == \
+        (c.maxIterations, c.maxError, c.maxIterationsV, c.maxErrorV)
+    assert (sc.cfl_method, sc.cfl_factor, sc.cfl_max_time_step) == (c.cflMethod, c.cflFactor, c.cflMaxTimeStepSize)
+    assert sc.enable_divergence_solver == (1 if c.enableDivergenceSolver else 0) and sc.precision == c.precision
+    assert sc.fluid_capacity == max(1, s.n_fluid) and sc.boundary_capacity == max(1, s.n_boundary)
+    return s
+
+
+@pytest.mark.parametrize("extra", [{}, {"jitter": 0.01, "seed": 3}, {"cflMethod": 1, "precision": 64,
+                                                                    "gravitation": [0.5, -9.0, 0.25]}])
+def test_native_reader_equals_python_reader(tmp_path, extra):
+    _check_native_equals_python(_dam_break_json(tmp_path, extra))
+
+
+def test_native_reader_particle_files_and_rotation(tmp_path):
+    """FluidModels and RigidBodies from .bgeo particle files, rotated and scaled (x = R (s x) + t)."""
+    from splishsplash_for_cuda_b200.scene import write_bgeo
+
+    rng = np.random.default_rng(5)
+    xf = rng.uniform(0.2, 0.8, size=(500, 3)).astype(np.float32)
+    vf = rng.uniform(-1, 1, size=(500, 3)).astype(np.float32)
+    xb = rng.uniform(0.0, 1.0, size=(300, 3)).astype(np.float32)
+    write_bgeo(tmp_path / "fluid.bgeo", xf, vf, 0.025)
+    write_bgeo(tmp_path / "walls.bgeo", xb, None, 0.025)
+    p = _dam_break_json(tmp_path, {"jitter": 0.02, "seed": 9})
+    j = json.loads(p.read_text())
+    j["FluidModels"] = [{"particleFile": "fluid.bgeo", "translation": [0.1, 0.2, 0.3], "scale": 1.5,
+                         "rotationAxis": [0, 1, 0], "rotationAngle": 0.3}]
+    j["RigidBodies"].append({"particleFile": "walls.bgeo", "translation": [0.0, -0.5, 0.0], "scale": [2.0, 2.0, 2.0],
+                             "rotationAxis": [1, 0, 0], "rotationAngle": 1.1})
+    p.write_text(json.dumps(j))
+    s = _check_native_equals_python(p, atol=1e-6)
+    assert s.n_fluid == 27000 + 500 and s.fluid_velocity is not None
+
+
+@pytest.mark.parametrize("change,message", [
+    (lambda j: j["FluidBlocks"][0].update(denseMode=1), b"denseMode"),
+    (lambda j: j["Configuration"].update(precision=16), b"precision"),
+    (lambda j: j["Configuration"].update(learnedWarmStart={"epochs": 3}), b"learnedWarmStart"),
+    (lambda j: j["RigidBodies"][0].update(geometryFile="sphere.obj"), b"box"),
+])
+def test_native_reader_rejects_like_python(tmp_path, change, message):
+    import ctypes as C
+
+    from splishsplash_for_cuda_b200 import _capi
+
+    p = _dam_break_json(tmp_path)
+    j = json.loads(p.read_text())
+    change(j)
+    p.write_text(json.dumps(j))
+    with pytest.raises(ValueError):
+        load_scene(p)
+    lib = _capi.load()
+    h = C.c_void_p()
+    assert lib.dfsph_scene_load(str(p).encode(), None, C.byref(h)) == _capi.DFSPH_E_INVALID
+    assert message in lib.dfsph_last_error(None)
+    p.write_text('{"Configuration": {"particleRadius": 0.025,}')
+    assert lib.dfsph_scene_load(str(p).encode(), None, C.byref(h)) == _capi.DFSPH_E_INVALID
+
+
+@pytest.mark.gpu
+def test_create_from_scene_file_equals_python_facade(cuda_lib, tmp_path):
+    """dfsph_create_from_scene_file (the C path: read, create, upload, learned block) steps exactly
+    like the Python facade on the Python reader's scene."""
+    import ctypes as C
+
+    from splishsplash_for_cuda_b200 import _capi
+    from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
+
+    p = _dam_break_json(tmp_path, {"jitter": 0.01, "seed": 2, "learnedWarmStart": {"trainInterval": 5}})
+    ref = DFSPHCUDA(load_scene(p))
+    lib = _capi.load()
+    ctx = C.c_void_p()
+    assert lib.dfsph_create_from_scene_file(str(p).encode(), C.byref(ctx)) == _capi.DFSPH_OK
+    try:
+        v = C.c_double()
+        assert lib.dfsph_get_param(ctx, b"learned_warm_start", C.byref(v)) == 0 and v.value == 1
+        assert lib.dfsph_get_param(ctx, b"train_interval", C.byref(v)) == 0 and v.value == 5
+        st = _capi.DfsphStepStats()
+        for _ in range(12):
+            assert lib.dfsph_step(ctx, C.byref(st)) == 0
+            sr = ref.step()
+            assert (st.iterations, st.iterations_v) == (sr.iterations, sr.iterations_v)
+        n = ref.num_fluid()
+        x = np.empty((n, 3), np.float32)
+        vv = np.empty((n, 3), np.float32)
+        assert lib.dfsph_read_dynamic_data(ctx, x.ctypes.data, vv.ctypes.data) == 0
+        assert np.array_equal(x, ref.positions()) and np.array_equal(vv, ref.velocities())
+    finally:
+        lib.dfsph_destroy(ctx)
