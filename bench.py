@@ -391,6 +391,12 @@ def run_ours(args, world, rank, local):
         dist.barrier()
     ms = reduce_max(total_ms / args.steps, world)
     agg_pps = reduce_sum(n * args.steps / (total_ms / 1e3), world)
+    if args.steps_only:  # profiling runs: the warm-up and the timed steps, nothing else
+        if rank == 0:
+            print(json.dumps({"workload": scene.name, "ms_per_step": round(ms, 4), "iterations_per_step": mean_it,
+                              "iterations_v_per_step": mean_itv, "status_bits": int(status_bits)}), flush=True)
+        d.close()
+        return
 
     # end-to-end through the public API with host buffers (pinned), copies inside the timed region
     xh = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
@@ -491,6 +497,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--steps-only", action="store_true",
+                    help="profiling: run the warm-up and the timed steps only and print a short line")
     ap.add_argument("--ablation-steps", type=int, default=300,
                     help="steps per mode of the plain vs learned warm-start comparison (0: skip)")
     ap.add_argument("--ablation-workloads", nargs="*", choices=ABLATION_WORKLOADS, default=list(ABLATION_WORKLOADS))
