@@ -53,7 +53,8 @@ typedef struct dfsph_ctx dfsph_ctx;
 #define DFSPH_ST_MMA_TIMEOUT 0x100u      /* a bounded wait for the warm-start network's tensor-core MMA
                                             gave up (no hang; that call's predictions are unspecified) */
 #define DFSPH_ST_INDEX 0x200u            /* checked build only: a neighbour-list entry, a list count or a
-                                            cell-table run was out of range and was skipped, not read */
+                                            cell-table run was out of range; it was not read (the run is
+                                            skipped, the particle's list emptied) */
 
 /* ---- scene / solver parameters ---------------------------------------------------------------- */
 /* Mirrors the "Configuration" keys of the reference JSON scene (Utilities/SceneLoader.cpp:39-160)

@@ -21,8 +21,9 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libdfsph_b200.so"
 OBJ = PKG / "_build"
-# The checked variant: every neighbour-list entry, list count and cell-table run is range-checked on
-# the device (DFSPH_ST_INDEX instead of an out-of-range read); for debugging and the tests.
+# The checked variant: every cell-table run, neighbour-list entry and list count is range-checked on
+# the device after each neighbour search (DFSPH_ST_INDEX instead of an out-of-range read); the solver
+# passes are the product's code. For debugging and the tests.
 CHECKED_OUT = PKG / "libdfsph_b200_checked.so"
 CHECKED_OBJ = PKG / "_build_checked"
 

@@ -100,6 +100,7 @@ public:
     Vec4<Real>* bpos[2] = {nullptr, nullptr};
     Vec4<Real>* bvel[2] = {nullptr, nullptr};
     float* brest = nullptr;  // boundary positions as given to set_boundary (upload order), for rigid moves
+    unsigned long long* bforce_fx = nullptr;  // boundary forces, fixed-point sums (converted into bforce)
     Real* bforce = nullptr;  // boundary forces (4 per particle, sorted order), allocated when enabled
     bool boundary_forces = false;
     uint32_t* bid = nullptr;
@@ -277,7 +278,7 @@ public:
         for (int b = 0; b < 2; ++b) {
             f(pos[b]); f(vel[b]); f(kappa[b]); f(kappaV[b]); f(id[b]); f(bpos[b]); f(bvel[b]);
         }
-        f(density); f(factor); f(densityAdv); f(kcoef); f(acc); f(counts); f(nbr); f(bid); f(bforce);
+        f(density); f(factor); f(densityAdv); f(kcoef); f(acc); f(counts); f(nbr); f(bid); f(bforce); f(bforce_fx);
         f(sb.keys_a); f(sb.keys_b); f(sb.vals_a); f(sb.vals_b); f(sb.workspace);
         f(partials); f(cfl_partials); f(ctl); f(status); f(stage); f(dl); f(ds); f(ftab); f(btab);
         for (int b = 0; b < 2; ++b) {
@@ -393,7 +394,7 @@ public:
         hs.status = status;
         hs.cfl_partials = cfl_partials;
         hs.dtd = dtd;
-        hs.bforce = boundary_forces ? bforce : nullptr;
+        hs.bforce = boundary_forces ? bforce_fx : nullptr;
         hs.features = features;
         hs.pred = pred;
         hs.kappaT = kappaT[cur];
@@ -683,7 +684,8 @@ public:
         DF_CHECK(grid_ready, DFSPH_E_STATE, "no grid: set a boundary or upload fluid first");
         // forces on the boundary are per step (the reference clears them when it moves the dynamic
         // bodies at the start of a step, DFSPH_core_cuda.cu:3413)
-        if (boundary_forces && nb) DF_CUDA(cudaMemsetAsync(bforce, 0, (size_t)nb * 4 * sizeof(Real), stream));
+        if (boundary_forces && nb)
+            DF_CUDA(cudaMemsetAsync(bforce_fx, 0, (size_t)nb * 3 * sizeof(unsigned long long), stream));
         if (!n) return DFSPH_OK;
         DF_TRY(bin_fluid());
         launch_build_neighbors<Real>(ds, n, ftab, btab, stream);
@@ -691,6 +693,10 @@ public:
         if (corrupt_neighbor) {  // checked builds only (the key is rejected otherwise); one search
             launch_corrupt_first_neighbor(nbr, counts, n + corrupt_neighbor - 1u, stream);
             corrupt_neighbor = 0;
+            launches += 1;
+        }
+        if (kCheckedBuild) {
+            launch_validate_neighbors(counts, nbr, n, nb, stride, cap, status, stream);
             launches += 1;
         }
         DF_CUDA(cudaGetLastError());
@@ -1611,6 +1617,8 @@ public:
                 break;
             case DFSPH_F_BOUNDARY_FORCE:
                 DF_CHECK(bforce, DFSPH_E_STATE, "boundary forces are off (set_param boundary_forces 1)");
+                launch_force_from_fx<Real>(bforce_fx, nb, bforce, stream);
+                launches += 1;
                 src = bforce; sstride = 4; comps = 3; count = nb;
                 idmap = (order == DFSPH_ORDER_ID) ? bid : nullptr;
                 break;
@@ -1729,6 +1737,7 @@ public:
         double* dout = dcent + 3 * (size_t)nbod;
         if (nb) {
             launch_pack_field<Real, double>((const Real*)bpos[0], 4, 3, bid, nb, xp, stream);
+            launch_force_from_fx<Real>(bforce_fx, nb, bforce, stream);
             launch_pack_field<Real, double>(bforce, 4, 3, bid, nb, fp, stream);
         }
         DF_CUDA(cudaMemcpyAsync(dfirst, first, nbod * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
@@ -2099,7 +2108,9 @@ public:
         else if (k == "boundary_forces") {
             if (v != 0 && !bforce) {
                 DF_TRY(dalloc(&bforce, (size_t)Bc * 4));
+                DF_TRY(dalloc(&bforce_fx, (size_t)Bc * 3));
                 DF_CUDA(cudaMemsetAsync(bforce, 0, (size_t)Bc * 4 * sizeof(Real), stream));
+                DF_CUDA(cudaMemsetAsync(bforce_fx, 0, (size_t)Bc * 3 * sizeof(unsigned long long), stream));
             }
             boundary_forces = v != 0;
             invalidate_graphs();  // the loop graphs read the DevState block; rebuilt for clarity

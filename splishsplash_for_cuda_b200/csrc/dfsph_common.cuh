@@ -117,6 +117,15 @@ template <class Real> struct KSum3 {
 };
 
 // ---------------------------------------------------------------------------------------------
+// Boundary forces in 64-bit fixed point: 2^32 units per newton, +-2^31 N range. Each contribution is
+// rounded once to 2^-32 N (2.3e-10 N) and added with an integer atomic, so the accumulated force is
+// the same whatever the order of the additions (an FP32 atomicAdd sum is not).
+constexpr double kForceScale = 4294967296.0;
+__device__ __forceinline__ void add_force_fx(unsigned long long* p, double f) {
+    atomicAdd(p, (unsigned long long)llrint(f * kForceScale));
+}
+
+// ---------------------------------------------------------------------------------------------
 // Canonical pair predicate. The reference tests (pos_i - pos_j).squaredNorm() < H*H
 // (SPlisHSPlasH/DFSPH/DFSPH_macro_cuda.h:149, squaredNorm at SPlisHSPlasH/Vector.h:137). Its
 // rounding depends on how the compiler contracts x*x+y*y+z*z; this library fixes one order with
@@ -320,36 +329,9 @@ constexpr int kGatherBatch = DFSPH_GATHER_BATCH;
 #endif
 constexpr uint32_t kNoNeighbor = 0xFFFFFFFFu;
 
-// Checked builds (-DDFSPH_CHECKED, libdfsph_b200_checked.so): every list entry is compared with the
-// particle count of its set (limit) and every count with the table's capacity (cap); an entry or a
-// count out of range raises DFSPH_ST_INDEX in *status and is skipped instead of read. The unchecked
-// build trusts the lists (they come from the library's own neighbour search).
 template <int B, class Load, class Use>
 __device__ __forceinline__ void visit_neighbors(const uint32_t* __restrict__ nbr, uint32_t stride, uint32_t i,
-                                                uint32_t k0, uint32_t k1, uint32_t fallback, uint32_t limit,
-                                                uint32_t cap, uint32_t* status, Load&& load, Use&& use) {
-#ifdef DFSPH_CHECKED
-    if (k1 > cap) {
-        atomicOr(status, DFSPH_ST_INDEX);
-        k1 = cap;
-        if (k0 > k1) k0 = k1;
-    }
-    bool bad[B];
-    auto check = [&](int u, uint32_t j) {
-        bad[u] = j != kNoNeighbor && j >= limit;
-        if (bad[u]) atomicOr(status, DFSPH_ST_INDEX);
-        return (j == kNoNeighbor || bad[u]) ? fallback : j;
-    };
-#define DFSPH_VISIT_LOAD(u, j) load(u, check(u, j))
-#define DFSPH_VISIT_USE(u) \
-    if (!bad[u]) use(u)
-#else
-    (void)limit;
-    (void)cap;
-    (void)status;
-#define DFSPH_VISIT_LOAD(u, j) load(u, (j) == kNoNeighbor ? fallback : (j))
-#define DFSPH_VISIT_USE(u) use(u)
-#endif
+                                                uint32_t k0, uint32_t k1, uint32_t fallback, Load&& load, Use&& use) {
 #if DFSPH_PREFETCH_IDX
     // The index loads of the next batch are issued before the gathers of this one, so that their
     // latency (a coalesced stream, usually from DRAM) overlaps the dependent gathers.
@@ -364,12 +346,10 @@ __device__ __forceinline__ void visit_neighbors(const uint32_t* __restrict__ nbr
             jn[u] = k < k1 ? __ldg(nbr + (size_t)k * stride + i) : kNoNeighbor;
         }
 #pragma unroll
-        for (int u = 0; u < B; ++u) DFSPH_VISIT_LOAD(u, jj[u]);
+        for (int u = 0; u < B; ++u) load(u, jj[u] == kNoNeighbor ? fallback : jj[u]);
 #pragma unroll
         for (int u = 0; u < B; ++u)
-            if (kb + u < k1) {
-                DFSPH_VISIT_USE(u);
-            }
+            if (kb + u < k1) use(u);
 #pragma unroll
         for (int u = 0; u < B; ++u) jj[u] = jn[u];
     }
@@ -382,16 +362,12 @@ __device__ __forceinline__ void visit_neighbors(const uint32_t* __restrict__ nbr
             jj[u] = k < k1 ? __ldg(nbr + (size_t)k * stride + i) : kNoNeighbor;
         }
 #pragma unroll
-        for (int u = 0; u < B; ++u) DFSPH_VISIT_LOAD(u, jj[u]);
+        for (int u = 0; u < B; ++u) load(u, jj[u] == kNoNeighbor ? fallback : jj[u]);
 #pragma unroll
         for (int u = 0; u < B; ++u)
-            if (kb + u < k1) {
-                DFSPH_VISIT_USE(u);
-            }
+            if (kb + u < k1) use(u);
     }
 #endif
-#undef DFSPH_VISIT_LOAD
-#undef DFSPH_VISIT_USE
 }
 
 // ---------------------------------------------------------------------------------------------

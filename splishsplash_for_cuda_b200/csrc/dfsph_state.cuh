@@ -30,7 +30,10 @@ template <class Real> struct DevState {
     // boundary, cell-sorted order
     const Vec4<Real>* bpos;  // x, y, z, psi
     const Vec4<Real>* bvel;  // vx, vy, vz, (unused)
-    Real* bforce;            // fx, fy, fz, - per boundary particle (null: not accumulated)
+    // Force of the fluid on each boundary particle, x, y, z, accumulated as 64-bit fixed point
+    // (kForceScale units per newton): integer additions commute, so the sums do not depend on the
+    // order in which the atomics land (null: not accumulated).
+    unsigned long long* bforce;
     // reductions and control
     double* partials;      // one FP64 partial per block
     LoopCtl* ctl;          // [0] divergence loop, [1] pressure loop, [2] CFL / misc, [3] candidate probe
@@ -75,8 +78,17 @@ void launch_cell_bounds(const uint32_t* sorted_keys, uint32_t n, int dim_x, int 
 template <class Real>
 void launch_build_neighbors(const DevState<Real>* d, uint32_t n, const uint2* fluid_table, const uint2* boundary_table,
                             cudaStream_t s);
-// Checked builds only (a no-op otherwise): particle 0's first list entry := value.
+// Checked builds only (no-ops otherwise): particle 0's first list entry := value; the range check of
+// every list entry and count (DFSPH_ST_INDEX, the offending particle's list emptied).
 void launch_corrupt_first_neighbor(uint32_t* nbr, const uint32_t* counts, uint32_t value, cudaStream_t s);
+void launch_validate_neighbors(uint32_t* counts, const uint32_t* nbr, uint32_t n, uint32_t n_boundary, uint32_t stride,
+                               uint32_t cap, uint32_t* status, cudaStream_t s);
+constexpr bool kCheckedBuild =
+#ifdef DFSPH_CHECKED
+    true;
+#else
+    false;
+#endif
 template <class Real>
 void launch_boundary_psi(const Vec4<Real>* bpos_in, Vec4<Real>* bpos_out, uint32_t nb, const StepParams<Real>& p,
                          const uint2* boundary_table, uint32_t* status, cudaStream_t s);

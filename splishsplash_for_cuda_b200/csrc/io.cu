@@ -154,6 +154,18 @@ __global__ void __launch_bounds__(kBlock) rigid_boundary_kernel(const float* __r
     bvel[i] = v;
 }
 
+// Boundary forces: 64-bit fixed-point sums (kForceScale units per newton) -> Real x, y, z, 0.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) force_from_fx_kernel(const unsigned long long* __restrict__ fx, uint32_t n,
+                                                               Real* __restrict__ out) {
+    DFSPH_PDL_ENTER;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[4 * (size_t)i + c] = (Real)((double)(long long)fx[3 * (size_t)i + c] / kForceScale);
+    out[4 * (size_t)i + 3] = Real(0);
+}
+
 // Field download: element c of slot i of src (stride src_stride Real elements) goes to
 // dst[(id ? id[i] : i) * comps + c], converted to Out.
 template <class Real, class Out>
@@ -283,6 +295,10 @@ void launch_rigid_boundary(const float* rest, uint32_t n, const uint32_t* bid, c
                            Vec4<Real>* bvel, cudaStream_t s) {
     if (n) launch_pdl(rigid_boundary_kernel<Real>, grid_for(n), kBlock, 0, s, rest, n, bid, m, bpos, bvel);
 }
+template <class Real>
+void launch_force_from_fx(const unsigned long long* fx, uint32_t n, Real* out, cudaStream_t s) {
+    if (n) launch_pdl(force_from_fx_kernel<Real>, grid_for(n), kBlock, 0, s, fx, n, out);
+}
 template <class Real, class Out>
 void launch_pack_field(const Real* src, int src_stride, int comps, const uint32_t* id, uint32_t n, Out* dst,
                        cudaStream_t s) {
@@ -309,6 +325,7 @@ void launch_unpack_counts(const uint32_t* counts, const uint32_t* id, uint32_t n
                                           cudaStream_t);                                                             \
     template void launch_rigid_boundary<R>(const float*, uint32_t, const uint32_t*, const RigidMotion&, Vec4<R>*,    \
                                            Vec4<R>*, cudaStream_t);                                                  \
+    template void launch_force_from_fx<R>(const unsigned long long*, uint32_t, R*, cudaStream_t);                    \
     template void launch_pack_field<R, float>(const R*, int, int, const uint32_t*, uint32_t, float*, cudaStream_t);  \
     template void launch_pack_field<R, double>(const R*, int, int, const uint32_t*, uint32_t, double*, cudaStream_t);
 

@@ -47,6 +47,9 @@ struct RigidMotion {
 template <class Real>
 void launch_rigid_boundary(const float* rest, uint32_t n, const uint32_t* bid, const RigidMotion& m, Vec4<Real>* bpos,
                            Vec4<Real>* bvel, cudaStream_t s);
+// Boundary forces from their fixed-point sums (x, y, z, 0 per particle).
+template <class Real>
+void launch_force_from_fx(const unsigned long long* fx, uint32_t n, Real* out, cudaStream_t s);
 template <class Real, class Out>
 void launch_pack_field(const Real* src, int src_stride, int comps, const uint32_t* id, uint32_t n, Out* dst,
                        cudaStream_t s);

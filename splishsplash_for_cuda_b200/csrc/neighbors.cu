@@ -118,10 +118,30 @@ __device__ __forceinline__ bool run_in_range(uint2 r, uint32_t limit, uint32_t* 
 
 #ifdef DFSPH_CHECKED
 // Test hook of the checked build: replaces particle 0's first list entry by `value` (an index past the
-// fluid count, inside the allocation), which the checked gathers must report and skip.
+// fluid count, inside the allocation), which the validation below must report.
 __global__ void corrupt_first_neighbor_kernel(uint32_t* __restrict__ nbr, const uint32_t* __restrict__ counts,
                                               uint32_t value) {
     if (threadIdx.x == 0 && (counts[0] & 0xFFFFu) > 0) nbr[0] = value;
+}
+
+// Validation of the lists before any pass gathers through them (checked build): a count past the
+// table's capacity, a fluid entry >= n or a boundary entry >= n_boundary raises DFSPH_ST_INDEX and
+// empties that particle's list, so no pass reads out of range. The passes themselves are the
+// unchecked build's code, so a clean run gives the same bits.
+__global__ void __launch_bounds__(kBlock) validate_neighbors_kernel(uint32_t* __restrict__ counts,
+                                                                    const uint32_t* __restrict__ nbr, uint32_t n,
+                                                                    uint32_t n_boundary, uint32_t stride, uint32_t cap,
+                                                                    uint32_t* __restrict__ status) {
+    DFSPH_PDL_ENTER;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t c = counts[i], nf = c & 0xFFFFu, nb = c >> 16;
+    bool bad = nf + nb > cap;
+    for (uint32_t k = 0; k < nf + nb && !bad; ++k) bad = nbr[(size_t)k * stride + i] >= (k < nf ? n : n_boundary);
+    if (bad) {
+        atomicOr(status, DFSPH_ST_INDEX);
+        counts[i] = 0u;
+    }
 }
 #endif
 
@@ -310,6 +330,21 @@ template <class Real>
 void launch_build_neighbors(const DevState<Real>* d, uint32_t n, const uint2* fluid_table, const uint2* boundary_table,
                             cudaStream_t s) {
     if (n) launch_pdl(build_neighbors_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, fluid_table, boundary_table);
+}
+void launch_validate_neighbors(uint32_t* counts, const uint32_t* nbr, uint32_t n, uint32_t n_boundary, uint32_t stride,
+                               uint32_t cap, uint32_t* status, cudaStream_t s) {
+#ifdef DFSPH_CHECKED
+    if (n) launch_pdl(validate_neighbors_kernel, grid_for(n), kBlock, 0, s, counts, nbr, n, n_boundary, stride, cap, status);
+#else
+    (void)counts;
+    (void)nbr;
+    (void)n;
+    (void)n_boundary;
+    (void)stride;
+    (void)cap;
+    (void)status;
+    (void)s;
+#endif
 }
 void launch_corrupt_first_neighbor(uint32_t* nbr, const uint32_t* counts, uint32_t value, cudaStream_t s) {
 #ifdef DFSPH_CHECKED

@@ -169,7 +169,7 @@ __device__ __forceinline__ Real velocity_divergence(const DevState<Real>* __rest
     KSum<Real> s;
     Vec4<Real> xj[kGatherBatch], vj[kGatherBatch];
     visit_neighbors<kGatherBatch>(
-        nbr, stride, i, 0, nf, i, p.n_fluid, p.nbr_cap, ds->status,
+        nbr, stride, i, 0, nf, i,
         [&](int u, uint32_t j) {
             xj[u] = ld4<Real>(pos + j);
             vj[u] = ld4<Real>(vel + j);
@@ -183,7 +183,7 @@ __device__ __forceinline__ Real velocity_divergence(const DevState<Real>* __rest
         const bool moving = p.boundary_moving != 0;
         BNbr<Real> b[kGatherBatch];
         visit_neighbors<kGatherBatch>(
-            nbr, stride, i, nf, nf + nb, 0u, p.n_boundary, p.nbr_cap, ds->status, [&](int u, uint32_t j) { load_bnbr(b[u], ds->bpos, ds->bvel, j, moving); },
+            nbr, stride, i, nf, nf + nb, 0u, [&](int u, uint32_t j) { load_bnbr(b[u], ds->bpos, ds->bvel, j, moving); },
             [&](int u) {
                 Real gx, gy, gz;
                 K.gradW(xi.x - b[u].x.x, xi.y - b[u].x.y, xi.z - b[u].x.z, gx, gy, gz);
@@ -208,7 +208,7 @@ __device__ __forceinline__ void velocity_divergence2(const DevState<Real>* __res
     KSum<Real> sa, sb;
     Vec4<Real> xj[kDualBatch], va[kDualBatch], vb[kDualBatch];
     visit_neighbors<kDualBatch>(
-        nbr, stride, i, 0, nf, i, p.n_fluid, p.nbr_cap, ds->status,
+        nbr, stride, i, 0, nf, i,
         [&](int u, uint32_t j) {
             xj[u] = ld4<Real>(pos + j);
             va[u] = ld4<Real>(vela + j);
@@ -224,7 +224,7 @@ __device__ __forceinline__ void velocity_divergence2(const DevState<Real>* __res
         const bool moving = p.boundary_moving != 0;
         BNbr<Real> b[kDualBatch];
         visit_neighbors<kDualBatch>(
-            nbr, stride, i, nf, nf + nb, 0u, p.n_boundary, p.nbr_cap, ds->status, [&](int u, uint32_t j) { load_bnbr(b[u], ds->bpos, ds->bvel, j, moving); },
+            nbr, stride, i, nf, nf + nb, 0u, [&](int u, uint32_t j) { load_bnbr(b[u], ds->bpos, ds->bvel, j, moving); },
             [&](int u) {
                 Real gx, gy, gz;
                 K.gradW(xi.x - b[u].x.x, xi.y - b[u].x.y, xi.z - b[u].x.z, gx, gy, gz);
@@ -252,7 +252,7 @@ __device__ __forceinline__ void jacobi_sum(const DevState<Real>* __restrict__ ds
     Vec4<Real> xj[kGatherBatch];
     Real kj[kGatherBatch];
     visit_neighbors<kGatherBatch>(
-        nbr, stride, i, 0, nf, i, p.n_fluid, p.nbr_cap, ds->status,
+        nbr, stride, i, 0, nf, i,
         [&](int u, uint32_t j) {
             xj[u] = ld4<Real>(pos + j);
             kj[u] = kof(j);
@@ -268,11 +268,11 @@ __device__ __forceinline__ void jacobi_sum(const DevState<Real>* __restrict__ ds
         });
     if (nb && above_eps(ki)) {
         const Vec4<Real>* __restrict__ bpos = ds->bpos;
-        Real* __restrict__ bf = (kForces && forces) ? ds->bforce : nullptr;
+        unsigned long long* __restrict__ bf = (kForces && forces) ? ds->bforce : nullptr;
         Vec4<Real> xb[kGatherBatch];
         uint32_t jb[kGatherBatch];
         visit_neighbors<kGatherBatch>(
-            nbr, stride, i, nf, nf + nb, 0u, p.n_boundary, p.nbr_cap, ds->status,
+            nbr, stride, i, nf, nf + nb, 0u,
             [&](int u, uint32_t j) {
                 xb[u] = ld4<Real>(bpos + j);
                 jb[u] = j;
@@ -284,10 +284,10 @@ __device__ __forceinline__ void jacobi_sum(const DevState<Real>* __restrict__ ds
                 acc.add(sc * gx, sc * gy, sc * gz);
                 if (kForces && bf) {
                     const Real f = -xi.w * sc;
-                    Real* fb = bf + 4 * (size_t)jb[u];
-                    atomicAdd(fb, f * gx);
-                    atomicAdd(fb + 1, f * gy);
-                    atomicAdd(fb + 2, f * gz);
+                    unsigned long long* fb = bf + 3 * (size_t)jb[u];
+                    add_force_fx(fb, (double)(f * gx));
+                    add_force_fx(fb + 1, (double)(f * gy));
+                    add_force_fx(fb + 2, (double)(f * gz));
                 }
             });
     }
@@ -309,7 +309,7 @@ __device__ __forceinline__ void jacobi_sum2(const DevState<Real>* __restrict__ d
     Vec4<Real> xj[kDualBatch];
     Real kja[kDualBatch], kjb[kDualBatch];
     visit_neighbors<kDualBatch>(
-        nbr, stride, i, 0, nf, i, p.n_fluid, p.nbr_cap, ds->status,
+        nbr, stride, i, 0, nf, i,
         [&](int u, uint32_t j) {
             xj[u] = ld4<Real>(pos + j);
             kja[u] = kofa(j);
@@ -334,11 +334,11 @@ __device__ __forceinline__ void jacobi_sum2(const DevState<Real>* __restrict__ d
     const bool ba = above_eps(kia), bb = above_eps(kib);
     if (nb && (ba || bb)) {
         const Vec4<Real>* __restrict__ bpos = ds->bpos;
-        Real* __restrict__ bf = kForces ? ds->bforce : nullptr;
+        unsigned long long* __restrict__ bf = kForces ? ds->bforce : nullptr;
         Vec4<Real> xb[kDualBatch];
         uint32_t jb[kDualBatch];
         visit_neighbors<kDualBatch>(
-            nbr, stride, i, nf, nf + nb, 0u, p.n_boundary, p.nbr_cap, ds->status,
+            nbr, stride, i, nf, nf + nb, 0u,
             [&](int u, uint32_t j) {
                 xb[u] = ld4<Real>(bpos + j);
                 jb[u] = j;
@@ -355,10 +355,10 @@ __device__ __forceinline__ void jacobi_sum2(const DevState<Real>* __restrict__ d
                     accb.add(sc * gx, sc * gy, sc * gz);
                     if (kForces && bf) {
                         const Real f = -xi.w * sc;
-                        Real* fb = bf + 4 * (size_t)jb[u];
-                        atomicAdd(fb, f * gx);
-                        atomicAdd(fb + 1, f * gy);
-                        atomicAdd(fb + 2, f * gz);
+                        unsigned long long* fb = bf + 3 * (size_t)jb[u];
+                        add_force_fx(fb, (double)(f * gx));
+                        add_force_fx(fb + 1, (double)(f * gy));
+                        add_force_fx(fb + 2, (double)(f * gz));
                     }
                 }
             });
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
     {
         Vec4<Real> xj[kGatherBatch], vj[kGatherBatch];
         visit_neighbors<kGatherBatch>(
-            nbr, stride, i, 0, nf, i, p.n_fluid, p.nbr_cap, ds->status,
+            nbr, stride, i, 0, nf, i,
             [&](int u, uint32_t j) {
                 xj[u] = ld4<Real>(pos + j);
                 vj[u] = ld4<Real>(vel + j);
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
         const bool moving = p.boundary_moving != 0;
         BNbr<Real> b[kGatherBatch];
         visit_neighbors<kGatherBatch>(
-            nbr, stride, i, nf, nf + nb, 0u, p.n_boundary, p.nbr_cap, ds->status, [&](int u, uint32_t j) { load_bnbr(b[u], ds->bpos, ds->bvel, j, moving); },
+            nbr, stride, i, nf, nf + nb, 0u, [&](int u, uint32_t j) { load_bnbr(b[u], ds->bpos, ds->bvel, j, moving); },
             [&](int u) { accumulate(b[u].x, b[u].vx, b[u].vy, b[u].vz); });
     }
     const Real gx = gpi.x.value(), gy = gpi.y.value(), gz = gpi.z.value();
@@ -596,7 +596,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) viscosity_kernel(con
         Vec4<Real> xj[kGatherBatch], vj[kGatherBatch];
         Real rj[kGatherBatch];
         visit_neighbors<kGatherBatch>(
-            ds->nbr, p.nbr_stride, i, 0, nf, i, p.n_fluid, p.nbr_cap, ds->status,
+            ds->nbr, p.nbr_stride, i, 0, nf, i,
             [&](int u, uint32_t j) {
                 xj[u] = ld4<Real>(pos + j);
                 vj[u] = ld4<Real>(vel + j);

@@ -1,9 +1,10 @@
-"""The checked build (libdfsph_b200_checked.so, compiled with -DDFSPH_CHECKED): every neighbour-list
-entry, list count and cell-table run is range-checked on the device, and an entry out of range raises
-DFSPH_ST_INDEX and is skipped instead of read. It stands in for a memory checker on the small parity
-cases: they must run with the bit clear and give exactly the unchecked build's bits, and an index
-planted past the fluid count (inside the allocation, so that no access could leave it even
-unchecked) must be reported."""
+"""The checked build (libdfsph_b200_checked.so, compiled with -DDFSPH_CHECKED): every cell-table run
+is range-checked while the lists are built, and every list entry and count after each neighbour
+search, before any pass gathers through them; a value out of range raises DFSPH_ST_INDEX and is not
+read (the run skipped, the particle's list emptied). It stands in for a memory checker on the small
+parity cases: they must run with the bit clear and give exactly the unchecked build's bits (the
+solver passes are the same code), and an index planted past the fluid count (inside the allocation,
+so that no access could leave it even unchecked) must be reported."""
 import numpy as np
 import pytest
 

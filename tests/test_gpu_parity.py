@@ -473,6 +473,28 @@ def test_boundary_forces_match_oracle():
     assert abs(np.mean(fy) + weight) <= 0.05 * weight
 
 
+def test_boundary_forces_rerun_bit_identical():
+    """The fluid's forces on the boundary are accumulated in 64-bit fixed point (integer atomics
+    commute), so two runs give the same force on every boundary particle, bit for bit, and so the same
+    body wrench."""
+    from splishsplash_for_cuda_b200.scene import column_scene
+
+    s = column_scene(counts=(8, 16, 8), time_step=0.002)
+    a, b = DFSPHCUDA(s), DFSPHCUDA(s)
+    for d in (a, b):
+        d.set_param("boundary_forces", 1)
+    for _ in range(15):
+        a.step()
+        b.step()
+        fa, fb = a.field("boundary_force", np.float64), b.field("boundary_force", np.float64)
+        assert np.array_equal(fa, fb)
+    assert np.abs(fa).max() > 0
+    nb = s.n_boundary
+    fa_, ta = a.body_wrench([0], [nb], [(0.0, 0.0, 0.0)])
+    fb_, tb = b.body_wrench([0], [nb], [(0.0, 0.0, 0.0)])
+    assert np.array_equal(fa_, fb_) and np.array_equal(ta, tb)
+
+
 def test_async_steps_equal_waiting_steps():
     """The step runs on the device, CFL dt included: enqueued steps without read-back give the same
     state, dt history and iteration totals as steps that wait for their statistics."""
