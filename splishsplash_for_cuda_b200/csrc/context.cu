@@ -444,10 +444,16 @@ public:
 
     // Cell tables for the current off / dim (also used when a checkpoint restores them).
     int alloc_grid() {
-        const int maxdim = std::max(dim[0], std::max(dim[1], dim[2]));
-        int bits = 1;
-        while ((1 << bits) < maxdim) ++bits;
-        key_passes = std::min(4, (3 * bits + 1 + 7) / 8);
+        // Digit passes of the key sort: the highest bit a valid Morton key can set (axis a's top bit
+        // lands on key bit 3 (bits_a - 1) + a), plus one so that the escaped-particle key (all ones)
+        // still sorts after every valid key in the bits sorted.
+        int key_bits = 1;
+        for (int a = 0; a < 3; ++a) {
+            int bits = 1;
+            while ((1 << bits) < dim[a]) ++bits;
+            key_bits = std::max(key_bits, 3 * (bits - 1) + a + 1);
+        }
+        key_passes = std::min(4, (key_bits + 1 + 7) / 8);
         const size_t c = (size_t)dim[0] * dim[1] * dim[2];
         if (c != cells) {
             if (ftab) cudaFree(ftab);
