@@ -409,6 +409,28 @@ int dfsph_open_boundary_samples(dfsph_ctx* ctx, float* xyz, uint32_t capacity, u
  * displacement this way, OpenBoundariesSimple.cu:527-553). */
 int dfsph_open_boundary_shift(dfsph_ctx* ctx, const float* delta);
 
+/* ---- dynamic window (own design after DynamicWindowInterface, SPlisHSPlasH/DFSPH/DynamicWindow.h:
+ * 31-200, driven like DFSPHCUDA::applyDynamicWindow, DFSPH_CUDA.cpp:3988-4139) ---------------------
+ * The simulated region is the box [lo, hi] walled by the boundary particles [wall_first, wall_first +
+ * wall_count) (upload order, given to dfsph_set_boundary in the window's initial place); rest_xyz are
+ * n_rest positions of a fluid at rest tiling the window (the reference's rest-fluid file). The cell
+ * grid does not move: the scene's grid box must cover the window's whole path.
+ * dfsph_dynamic_window_shift moves the window by displacement[3], between steps: the walls translate
+ * rigidly on the device; fluid particles outside the moved box are removed (ids renumbered densely in
+ * their previous order); the rest samples move with the window and those in the region it newly
+ * covers become fluid particles by the open boundary's inflow rule (no fluid particle closer than
+ * allowed_distance, density estimate at most allowed_density, velocity the kernel-weighted velocity of
+ * the fluid around it, kappa = kappa_v = 0, the next ids in sample order); the domain box of the
+ * end-of-step removal moves with the window. The reference's tagging by density levels and its
+ * damped stabilisation iterations are not reproduced: the pressure solve of the next step takes the
+ * seam. added / removed (nullable) receive the counts; synchronises the context's stream. */
+int dfsph_dynamic_window_init(dfsph_ctx* ctx, const double* lo, const double* hi, uint32_t wall_first,
+                              uint32_t wall_count, const float* rest_xyz, uint32_t n_rest);
+int dfsph_dynamic_window_shift(dfsph_ctx* ctx, const double* displacement, double allowed_distance,
+                               double allowed_density, uint32_t* added, uint32_t* removed);
+/* Total displacement of the window since dfsph_dynamic_window_init. */
+int dfsph_dynamic_window_displacement(dfsph_ctx* ctx, double* displacement);
+
 /* Force and torque of the fluid on boundary bodies during the last step (needs "boundary_forces" 1):
  * the per-particle forces the reference hands to its rigid-body solver (readDynamicObjectsData,
  * DFSPH_c_arrays_structure.cpp:1177-1193), summed on the device. Body b is the range

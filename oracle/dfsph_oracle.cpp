@@ -1064,6 +1064,24 @@ int oracle_open_boundary_apply(void* h, double dist, double rho, int inflow, int
 
 int oracle_open_boundary_shift(void* h, const float* d) { return ORACLE_DO(h, (o.ob_shift(d), 0)); }
 
+// Removes the fluid particles with a coordinate outside [lo, hi] (compared as the device's box tag,
+// open_boundary.cu box_tag_kernel), keeping the order of the others; the dynamic window's removal
+// behind a moved window.
+int oracle_remove_outside_box(void* h, const float* lo, const float* hi, uint32_t* removed) {
+    return ORACLE_DO(h, ([&] {
+        using R = typename std::remove_reference<decltype(o.x[0])>::type;
+        const uint32_t r = o.compact([&](uint32_t i) {
+            for (int a = 0; a < 3; ++a) {
+                const R c = o.x[3 * i + a];
+                if (c > (R)hi[a] || c < (R)lo[a]) return false;
+            }
+            return true;
+        });
+        if (removed) *removed = r;
+        return 0;
+    })());
+}
+
 // inside[i] and normal[3 i..] of the restated BufferFluidSurface::isinside / getNormal.
 int oracle_surface_eval(const Surface* s, const float* p, uint32_t n, uint8_t* inside, float* normal) {
     for (uint32_t i = 0; i < n; ++i) {

@@ -105,6 +105,7 @@ def _load():
             "oracle_open_boundary_apply": (C.c_int, [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_uint32, up,
                                                      up]),
             "oracle_open_boundary_shift": (C.c_int, [vp, fp]),
+            "oracle_remove_outside_box": (C.c_int, [vp, fp, fp, up]),
             "oracle_surface_eval": (C.c_int, [C.POINTER(OracleSurface), fp, C.c_uint32, C.c_void_p, fp]),
         }
         for name, (res, args) in sig.items():
@@ -123,7 +124,7 @@ class Oracle:
     """CPU restatement of the DFSPH step on one scene (fluid in original order)."""
 
     def __init__(self, scene, precision: int = 64, brute_force: bool = False, neighbor_capacity: int = 96,
-                 boundary_psi=None):
+                 boundary_psi=None, grid_box=None):
         self.lib = _load()
         cfg = scene.config
         p = OracleParams()
@@ -152,7 +153,10 @@ class Oracle:
         b = np.ascontiguousarray(scene.boundary, dtype=np.float32)
         psi = None if boundary_psi is None else np.ascontiguousarray(boundary_psi, dtype=np.float32)
         self._keep = (b, psi)
-        if self.lib.oracle_set_boundary(self.h, _f(b), _f(psi), b.shape[0], None) != 0:
+        gb = None if grid_box is None else np.ascontiguousarray(np.asarray(grid_box, np.float64).reshape(6))
+        self._keep = (b, psi, gb)
+        if self.lib.oracle_set_boundary(self.h, _f(b), _f(psi), b.shape[0],
+                                        None if gb is None else gb.ctypes.data_as(C.POINTER(C.c_double))) != 0:
             raise RuntimeError("oracle_set_boundary failed")
         x = np.ascontiguousarray(scene.fluid, dtype=np.float32)
         v = None if scene.fluid_velocity is None else np.ascontiguousarray(scene.fluid_velocity, dtype=np.float32)
@@ -268,6 +272,14 @@ class Oracle:
                                                       int(use_outflow), capacity, C.byref(a), C.byref(r))
         self.n = self.n + a.value - r.value
         return a.value, r.value, bool(clipped)
+
+    def remove_outside_box(self, lo, hi) -> int:
+        """Removes the fluid particles outside [lo, hi] (float32 bounds), keeping the others' order."""
+        r = C.c_uint32()
+        self.lib.oracle_remove_outside_box(self.h, _f(np.asarray(lo, np.float32).reshape(3)),
+                                           _f(np.asarray(hi, np.float32).reshape(3)), C.byref(r))
+        self.n = int(self.scalar("n"))
+        return int(r.value)
 
     def open_boundary_shift(self, delta) -> None:
         self.lib.oracle_open_boundary_shift(self.h, _f(np.asarray(delta, np.float32).reshape(3)))

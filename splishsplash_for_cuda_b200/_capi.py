@@ -158,6 +158,10 @@ SIGNATURES = {
     "dfsph_open_boundary_apply": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_uint32),
                                             C.POINTER(C.c_uint32)]),
     "dfsph_open_boundary_shift": (C.c_int, [_P, _P]),
+    "dfsph_dynamic_window_init": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32]),
+    "dfsph_dynamic_window_shift": (C.c_int, [_P, _P, C.c_double, C.c_double, C.POINTER(C.c_uint32),
+                                             C.POINTER(C.c_uint32)]),
+    "dfsph_dynamic_window_displacement": (C.c_int, [_P, _P]),
     "dfsph_open_boundary_samples": (C.c_int, [_P, _P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "dfsph_bgeo_write": (C.c_int, [C.c_char_p, _P, _P, C.c_uint64, C.c_float]),
     "dfsph_bgeo_read": (C.c_int, [C.c_char_p, _P, _P, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_int)]),

@@ -190,6 +190,18 @@ public:
     uint32_t* ob_total = nullptr;  // device scan totals
     uint32_t* h_ob = nullptr;      // pinned copy of a scan total
     uint32_t ob_ns = 0, ob_cap = 0;
+    uint32_t ob_scan_inputs = 0;   // inputs ob_scan was sized for
+
+    // dynamic window: the window box and its total displacement, the walls that move with it, and
+    // the rest-fluid samples (in the window's current place) with their scratch
+    bool dw_ready = false;
+    double dw_lo[3] = {0, 0, 0}, dw_hi[3] = {0, 0, 0}, dw_disp[3] = {0, 0, 0};
+    uint32_t dw_wall_first = 0, dw_wall_count = 0, dw_ns = 0, dw_cap = 0;
+    float4* dw_samples = nullptr;  // rest samples, moved with the window
+    float4* dw_sel = nullptr;      // the samples of the newly covered region
+    float4* dw_vel = nullptr;      // their candidate velocities
+    uint32_t* dw_flag = nullptr;
+    uint32_t* dw_rank = nullptr;
 
     // end-of-step removal of particles outside the domain box (checkParticlesPositions(2))
     float bb_lo[3] = {0, 0, 0}, bb_hi[3] = {0, 0, 0};
@@ -290,6 +302,7 @@ public:
         f(mlp.params); f(mlp.adam_m); f(mlp.adam_v); f(mlp.grad); f(mlp.partials);
         f(mlp.w1_bf16); f(mlp.w2_bf16); f(mlp.w3_bf16); f(mlp.scales); f(mlp.loss);
         f(ob_samples); f(ob_vel); f(ob_flag); f(ob_rank); f(ob_scan); f(ob_total); f(wrench_buf);
+        f(brest); f(dw_samples); f(dw_sel); f(dw_vel); f(dw_flag); f(dw_rank);
         if (h_ob) cudaFreeHost(h_ob);
         if (h_ctl) cudaFreeHost(h_ctl);
         if (h_status) cudaFreeHost(h_status);
@@ -770,10 +783,12 @@ public:
             DF_TRY(dalloc(&ob_vel, ob_cap));
             DF_TRY(dalloc(&ob_flag, ob_cap));
             DF_TRY(dalloc(&ob_rank, ob_cap));
-            DF_TRY(dalloc(&ob_scan, scan_scratch_words(std::max(ob_cap, Nc))));
+            ob_scan_inputs = std::max(ob_cap, Nc);
+            DF_TRY(dalloc(&ob_scan, scan_scratch_words(ob_scan_inputs)));
             if (!ob_total) DF_TRY(dalloc(&ob_total, 2));
             if (!h_ob) DF_CUDA(cudaMallocHost((void**)&h_ob, 2 * sizeof(uint32_t)));
         }
+        DF_TRY(ensure_scan_scratch(std::max(dw_cap, ns)));
         ob_boundary = *bnd;
         ob_interior = *interior;
         ob_surface = *surf;
@@ -848,8 +863,16 @@ public:
         return DFSPH_OK;
     }
 
-    int ensure_scan_scratch() {
-        if (!ob_scan) DF_TRY(dalloc(&ob_scan, scan_scratch_words(std::max(ob_cap, Nc))));
+    int ensure_scan_scratch(uint32_t inputs = 0) {
+        inputs = std::max(inputs, std::max(ob_cap, Nc));
+        if (ob_scan && inputs > ob_scan_inputs) {
+            cudaFree(ob_scan);
+            ob_scan = nullptr;
+        }
+        if (!ob_scan) {
+            DF_TRY(dalloc(&ob_scan, scan_scratch_words(inputs)));
+            ob_scan_inputs = inputs;
+        }
         if (!ob_total) DF_TRY(dalloc(&ob_total, 2));
         if (!h_ob) DF_CUDA(cudaMallocHost((void**)&h_ob, 2 * sizeof(uint32_t)));
         return DFSPH_OK;
@@ -885,6 +908,159 @@ public:
         DF_TRY(sync_state());
         DF_CUDA(cudaStreamSynchronize(stream));
         DF_CUDA(cudaGetLastError());
+        return DFSPH_OK;
+    }
+
+    // ---- dynamic window (after DynamicWindowInterface, DynamicWindow.h:31-200, driven like
+    // DFSPHCUDA::applyDynamicWindow, DFSPH_CUDA.cpp:3988-4139) ------------------------------------
+    int dynamic_window_init(const double* lo, const double* hi, uint32_t wall_first, uint32_t wall_count,
+                            const float* xyz, uint32_t ns) {
+        DF_CHECK(lo && hi, DFSPH_E_INVALID, "null window box");
+        DF_CHECK(lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2], DFSPH_E_INVALID, "empty window box");
+        DF_CHECK(wall_first <= nb && wall_count <= nb - wall_first, DFSPH_E_INVALID, "wall range out of bounds");
+        DF_CHECK(xyz || ns == 0, DFSPH_E_INVALID, "null rest samples");
+        DF_CHECK(grid_ready, DFSPH_E_STATE, "no grid: set a boundary first");
+        if (ns > dw_cap) {
+            for (void* q : {(void*)dw_samples, (void*)dw_sel, (void*)dw_vel, (void*)dw_flag, (void*)dw_rank})
+                if (q) cudaFree(q);
+            dw_samples = dw_sel = dw_vel = nullptr;
+            dw_flag = dw_rank = nullptr;
+            dw_cap = ns;
+            DF_TRY(dalloc(&dw_samples, dw_cap));
+            DF_TRY(dalloc(&dw_sel, dw_cap));
+            DF_TRY(dalloc(&dw_vel, dw_cap));
+            DF_TRY(dalloc(&dw_flag, dw_cap));
+            DF_TRY(dalloc(&dw_rank, dw_cap));
+        }
+        DF_TRY(ensure_scan_scratch(std::max(dw_cap, Nc)));
+        if (ns) {
+            std::vector<float4> h(ns);
+            for (uint32_t i = 0; i < ns; ++i) h[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.f);
+            DF_CUDA(cudaMemcpyAsync(dw_samples, h.data(), (size_t)ns * sizeof(float4), cudaMemcpyHostToDevice, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+        }
+        for (int a = 0; a < 3; ++a) {
+            dw_lo[a] = lo[a];
+            dw_hi[a] = hi[a];
+            dw_disp[a] = 0.0;
+        }
+        dw_wall_first = wall_first;
+        dw_wall_count = wall_count;
+        dw_ns = ns;
+        dw_ready = true;
+        return DFSPH_OK;
+    }
+
+    // Moves the window by d: (1) its walls translate rigidly to their set_boundary place + the total
+    // displacement (on the device); (2) fluid particles outside the moved box are removed (stable
+    // compaction, ids renumbered); (3) the rest samples move with the window, and those in the region
+    // the window newly covers become fluid particles by the open boundary's inflow rule (no fluid
+    // particle closer than allowed_distance, density estimate at most allowed_density; velocity the
+    // kernel-weighted velocity of the fluid around it). The domain box of the end-of-step removal moves
+    // with the window. The cell grid stays where it is: it must cover the window's whole path.
+    int dynamic_window_shift(const double* d, double allowed_distance, double allowed_density, uint32_t* added,
+                             uint32_t* removed) {
+        DF_CHECK(dw_ready, DFSPH_E_STATE, "dynamic window not initialised (dfsph_dynamic_window_init)");
+        DF_CHECK(d && std::isfinite(d[0]) && std::isfinite(d[1]) && std::isfinite(d[2]), DFSPH_E_INVALID,
+                 "displacement must be finite");
+        DF_CHECK(allowed_distance > 0 && allowed_density > 0, DFSPH_E_INVALID,
+                 "the window's inflow needs allowed_distance > 0 and allowed_density > 0");
+        double old_lo[3], old_hi[3];
+        for (int a = 0; a < 3; ++a) {
+            old_lo[a] = dw_lo[a] + dw_disp[a];
+            old_hi[a] = dw_hi[a] + dw_disp[a];
+            dw_disp[a] += d[a];
+            bb_lo[a] += (float)d[a];
+            bb_hi[a] += (float)d[a];
+        }
+        if (dw_wall_count) DF_TRY(move_boundary_rigid(dw_wall_first, dw_wall_count, nullptr, dw_disp, nullptr, nullptr));
+        // (2) removal outside the moved box
+        uint32_t n_rm = 0;
+        if (n) {
+            float lo[3], hi[3];
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = (float)(dw_lo[a] + dw_disp[a]);
+                hi[a] = (float)(dw_hi[a] + dw_disp[a]);
+            }
+            DF_CUDA(cudaMemsetAsync(status + 3, 0, sizeof(uint32_t), stream));
+            launch_box_tag<Real>(pos[cur], n, lo, hi, sb.keys_a, status + 3, stream);
+            DF_CUDA(cudaMemcpyAsync(h_status + 3, status + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+            launches += 1;
+            n_rm = h_status[3];
+            if (n_rm) {
+                exclusive_scan_u32(sb.keys_a, sb.vals_a, n, ob_scan, ob_total, stream);
+                launches += 3;
+                DF_TRY(compact_fluid(sb.keys_a, sb.vals_a, n - n_rm));
+            }
+        }
+        // (3) the samples of the newly covered region: outside the previous box, inside the grid
+        uint32_t n_add = 0;
+        bool clipped = false;
+        if (dw_ns) {
+            launch_shift_samples(dw_samples, dw_ns, (float)d[0], (float)d[1], (float)d[2], stream);
+            dfsph_surface prev{};
+            prev.type = DFSPH_SURFACE_CUBOID;
+            dfsph_surface all{};  // every point: the half space below y = 3e38
+            all.type = DFSPH_SURFACE_PLANE;
+            all.origin[1] = 3.0e38f;
+            all.normal[1] = -1.0f;
+            for (int a = 0; a < 3; ++a) {
+                prev.center[a] = (float)(0.5 * (old_lo[a] + old_hi[a]));
+                prev.half_lengths[a] = (float)(0.5 * (old_hi[a] - old_lo[a]));
+            }
+            launch_open_boundary_select<Real>(dw_samples, dw_ns, prev, all, params(), dw_flag, stream);
+            exclusive_scan_u32(dw_flag, dw_rank, dw_ns, ob_scan, ob_total, stream);
+            launch_compact_samples(dw_samples, dw_flag, dw_rank, dw_ns, dw_sel, stream);
+            DF_CUDA(cudaMemcpyAsync(h_ob, ob_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+            const uint32_t nsel = h_ob[0];
+            launches += 5;
+            if (nsel) {
+                DF_TRY(bin_fluid());
+                const double dd = 2.0 * sc.particle_radius;
+                const Real mass = (Real)(float)(0.8 * dd * dd * dd * sc.density0);
+                dfsph_surface box{};
+                box.type = DFSPH_SURFACE_CUBOID;
+                for (int a = 0; a < 3; ++a) {
+                    box.center[a] = (float)(0.5 * (dw_lo[a] + dw_hi[a]) + dw_disp[a]);
+                    box.half_lengths[a] = (float)(0.5 * (dw_hi[a] - dw_lo[a]));
+                }
+                launch_inflow<Real>(ds, dw_sel, nsel, (float)allowed_distance, (float)allowed_density, mass, box, ftab,
+                                    btab, dw_flag, dw_vel, stream);
+                exclusive_scan_u32(dw_flag, dw_rank, nsel, ob_scan, ob_total, stream);
+                DF_CUDA(cudaMemcpyAsync(h_ob, ob_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+                DF_CUDA(cudaStreamSynchronize(stream));
+                const uint32_t want = h_ob[0];
+                n_add = std::min<uint32_t>(want, Nc - n);
+                clipped = n_add < want;
+                launch_append_inflow<Real>(dw_sel, dw_vel, dw_flag, dw_rank, nsel, n, Nc, mass, pos[cur], vel[cur],
+                                           kappa[cur], kappaV[cur], id[cur], learned ? kappaT[cur] : nullptr,
+                                           learned ? kappaVT[cur] : nullptr, stream);
+                n += n_add;
+                launches += 5;
+            }
+        }
+        if (n_add || n_rm) invalidate_graphs();
+        DF_TRY(sync_state());
+        if (clipped) {
+            uint32_t st = 0;
+            DF_CUDA(cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+            st |= DFSPH_ST_FLUID_CAPACITY;
+            DF_CUDA(cudaMemcpyAsync(status, &st, sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        }
+        DF_CUDA(cudaStreamSynchronize(stream));
+        DF_CUDA(cudaGetLastError());
+        if (added) *added = n_add;
+        if (removed) *removed = n_rm;
+        return DFSPH_OK;
+    }
+
+    int dynamic_window_state(double* displacement) {
+        DF_CHECK(displacement, DFSPH_E_INVALID, "null output");
+        DF_CHECK(dw_ready, DFSPH_E_STATE, "dynamic window not initialised (dfsph_dynamic_window_init)");
+        for (int a = 0; a < 3; ++a) displacement[a] = dw_disp[a];
         return DFSPH_OK;
     }
 
@@ -2542,6 +2718,17 @@ int dfsph_open_boundary_apply(dfsph_ctx* ctx, double allowed_distance, double al
                                             added, removed));
 }
 int dfsph_open_boundary_shift(dfsph_ctx* ctx, const float* delta) { DFSPH_DISPATCH(ctx, open_boundary_shift(delta)); }
+int dfsph_dynamic_window_init(dfsph_ctx* ctx, const double* lo, const double* hi, uint32_t wall_first,
+                              uint32_t wall_count, const float* rest_xyz, uint32_t n_rest) {
+    DFSPH_DISPATCH(ctx, dynamic_window_init(lo, hi, wall_first, wall_count, rest_xyz, n_rest));
+}
+int dfsph_dynamic_window_shift(dfsph_ctx* ctx, const double* displacement, double allowed_distance,
+                               double allowed_density, uint32_t* added, uint32_t* removed) {
+    DFSPH_DISPATCH(ctx, dynamic_window_shift(displacement, allowed_distance, allowed_density, added, removed));
+}
+int dfsph_dynamic_window_displacement(dfsph_ctx* ctx, double* displacement) {
+    DFSPH_DISPATCH(ctx, dynamic_window_state(displacement));
+}
 int dfsph_open_boundary_samples(dfsph_ctx* ctx, float* xyz, uint32_t capacity, uint32_t* count) {
     DFSPH_DISPATCH(ctx, open_boundary_samples(xyz, capacity, count));
 }

@@ -26,7 +26,8 @@ def _fptr(a: np.ndarray | None):
 
 def scene_struct(scene: Scene, precision: int = 32, device: int = 0, use_graphs: bool = True,
                  neighbor_capacity: int = 96, fluid_capacity: int | None = None,
-                 boundary_capacity: int | None = None, lib_path: str | None = None) -> _capi.DfsphScene:
+                 boundary_capacity: int | None = None, lib_path: str | None = None,
+                 grid_box=None) -> _capi.DfsphScene:
     lib = _capi.load(lib_path)
     s = _capi.DfsphScene()
     _capi.check(lib, None, lib.dfsph_scene_defaults(C.byref(s)))
@@ -51,6 +52,11 @@ def scene_struct(scene: Scene, precision: int = 32, device: int = 0, use_graphs:
     s.precision = precision
     s.device = device
     s.use_graphs = 1 if use_graphs else 0
+    if grid_box is not None:  # (min x, y, z, max x, y, z): the cell grid's domain (else the boundary's box)
+        g = np.asarray(grid_box, np.float64).reshape(6)
+        for a in range(3):
+            s.grid_min[a] = g[a]
+            s.grid_max[a] = g[3 + a]
     return s
 
 
@@ -101,7 +107,7 @@ class DFSPHCUDA:
 
     def __init__(self, scene: Scene, precision: int | None = None, device: int = 0, use_graphs: bool = True,
                  neighbor_capacity: int = 96, boundary_psi: np.ndarray | None = None,
-                 fluid_capacity: int | None = None, lib_path: str | None = None):
+                 fluid_capacity: int | None = None, lib_path: str | None = None, grid_box=None):
         """precision None takes the scene's (Configuration "precision", default 32); the scene's
         "learnedWarmStart" block, when present, configures the learned warm start."""
         self._lib = _capi.load(lib_path)
@@ -110,7 +116,7 @@ class DFSPHCUDA:
             precision = int(getattr(scene.config, "precision", 32) or 32)
         self.precision = precision
         self._struct = scene_struct(scene, precision, device, use_graphs, neighbor_capacity, fluid_capacity,
-                                    lib_path=lib_path)
+                                    lib_path=lib_path, grid_box=grid_box)
         ctx = C.c_void_p()
         code = self._lib.dfsph_create(C.byref(self._struct), C.byref(ctx))
         if code != _capi.DFSPH_OK:
@@ -381,6 +387,29 @@ class DFSPHCUDA:
                 (q, position, velocity, angular_velocity)]
         ptrs = [None if a is None else a.ctypes.data_as(C.c_void_p) for a in arrs]
         self._call(self._lib.dfsph_move_boundary_rigid(self._ctx, int(first), int(count), *ptrs))
+
+    # ---- dynamic window (DynamicWindowInterface, driven like DFSPHCUDA::applyDynamicWindow) ----------
+    def init_dynamic_window(self, lo, hi, wall_first: int, wall_count: int, rest_positions) -> None:
+        """The window box [lo, hi] walled by boundary particles [wall_first, wall_first + wall_count),
+        and a fluid at rest tiling it (rest_positions (n, 3))."""
+        lo_ = np.ascontiguousarray(lo, dtype=np.float64).reshape(3)
+        hi_ = np.ascontiguousarray(hi, dtype=np.float64).reshape(3)
+        x = np.ascontiguousarray(rest_positions, dtype=np.float32).reshape(-1, 3)
+        self._call(self._lib.dfsph_dynamic_window_init(self._ctx, lo_.ctypes.data, hi_.ctypes.data, int(wall_first),
+                                                       int(wall_count), x.ctypes.data, x.shape[0]))
+
+    def shift_dynamic_window(self, displacement, allowed_distance: float, allowed_density: float) -> tuple:
+        """Moves the window by displacement (between steps). Returns (added, removed)."""
+        d = np.ascontiguousarray(displacement, dtype=np.float64).reshape(3)
+        a, r = C.c_uint32(), C.c_uint32()
+        self._call(self._lib.dfsph_dynamic_window_shift(self._ctx, d.ctypes.data, float(allowed_distance),
+                                                        float(allowed_density), C.byref(a), C.byref(r)))
+        return int(a.value), int(r.value)
+
+    def dynamic_window_displacement(self) -> np.ndarray:
+        out = np.zeros(3, np.float64)
+        self._call(self._lib.dfsph_dynamic_window_displacement(self._ctx, out.ctypes.data))
+        return out
 
     # ---- snapshots (DFSPHCUDA::handleSimulationSave / handleSimulationLoad) ----------------------
     def save_snapshot(self, folder, fluid: bool = True, boundary: bool = True) -> None:
