@@ -305,6 +305,8 @@ def learned_ablation(local, steps: int, workload: str = "column_64"):
         if mode == "learned":
             solves = int(d.get_param("learned_solves_p"))
             kept = int(d.get_param("learned_kept_p"))
+            rec.update(network_used_at_end=int(d.get_param("network_used")),
+                       heldout_loss_ratio=round(d.get_param("mlp_heldout_ratio"), 4))
             rec.update(trainings=int(d.get_param("mlp_trainings")), kept_pressure=kept, solves_pressure=solves,
                        kept_divergence=int(d.get_param("learned_kept_v")),
                        fallback_rate_pressure=round(1 - kept / solves, 4) if solves else None,
@@ -318,6 +320,62 @@ def learned_ablation(local, steps: int, workload: str = "column_64"):
     out["ms_per_step_reduction"] = round(1 - out["learned"]["ms_per_step"] / out["plain"]["ms_per_step"], 4)
     out["gated_ms_per_step_reduction"] = round(1 - out["gated"]["ms_per_step"] / out["plain"]["ms_per_step"], 4)
     return out
+
+
+def run_wave_tank(args, world, rank, local):
+    """--config 5: the 4,000,000-particle wave tank (piston, absorbing open boundary, floating box,
+    dynamic window; splishsplash_for_cuda_b200/wave_tank.py) for W + K steps. ms_per_step is the
+    device time of each whole step, the workload's host-side coupling (piston and body motion, body
+    wrench, open boundary, window) included, from CUDA events on the solver's stream."""
+    import torch
+
+    from splishsplash_for_cuda_b200.wave_tank import WaveTank, wave_tank_scene
+
+    scene, layout = wave_tank_scene()
+    tank = WaveTank(scene, layout, device=local, learned=not args.plain_wave_tank)
+    d = tank.d
+    d.set_param("timing", 1)
+    stream = torch.cuda.ExternalStream(d.stream_handle(), device=torch.device("cuda", local))
+    for _ in range(args.warmup):
+        tank.step()
+    d.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    its, itv, solver_ms, n_max = [], [], [], 0
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                starts[k].record(stream)
+            st = tank.step()
+            with torch.cuda.stream(stream):
+                ends[k].record(stream)
+            its.append(st.iterations)
+            itv.append(st.iterations_v)
+            solver_ms.append(st.ms_total)
+            n_max = max(n_max, st.num_fluid)
+        torch.cuda.synchronize(local)
+    total = sum(starts[k].elapsed_time(ends[k]) for k in range(args.steps))
+    ms = reduce_max(total / args.steps, world)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": round(ms, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice + xoshiro256** jitter)",
+            "config": {"workload": scene.name, "fluid_particles": scene.n_fluid, "boundary_particles": scene.n_boundary,
+                       "warm_start": "plain" if args.plain_wave_tank else "learned (gated)",
+                       "piston": "0.2 m, 1.5 s", "absorbing_layer_m": 0.3, "window_shift_m": 0.5,
+                       "window_every_steps": tank.window_every, "floating_box": "0.4 x 0.2 x 0.2 m, 500 kg/m^3",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "iterations_per_step": round(float(np.mean(its)), 2), "iterations_v_per_step": round(float(np.mean(itv)), 2),
+            "solver_ms_per_step": round(float(np.mean(solver_ms)), 4), "status_bits": int(tank.status),
+            "simulated_s": round(tank.t, 4), "window_shifts": tank.shifts, "added": tank.added, "removed": tank.removed,
+            "fluid_particles_max": n_max, "fluid_particles_end": d.num_fluid(),
+            "body_center": [round(float(c), 4) for c in tank.body.x], "clocks": clk.summary()}), flush=True)
+    d.close()
 
 
 def run_ours(args, world, rank, local):
@@ -497,6 +555,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-wave-tank", action="store_true", help="--config 5 with the plain warm start")
     ap.add_argument("--steps-only", action="store_true",
                     help="profiling: run the warm-up and the timed steps only and print a short line")
     ap.add_argument("--ablation-steps", type=int, default=300,
@@ -515,6 +574,8 @@ def main():
                                                          for w in args.ablation_workloads}}), flush=True)
         elif args.impl == "reference":
             run_reference_arm(args, world, rank)
+        elif args.config == 5:
+            run_wave_tank(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

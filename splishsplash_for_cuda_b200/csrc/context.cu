@@ -141,6 +141,14 @@ public:
     // Ablation of the learned warm start: the needed-coefficient base with the network's correction
     // fixed at zero (no inference, no training).
     bool base_only = false;
+    bool last_lp = false;  // the previous dfsph_step ran the learned passes
+    // The network's correction is applied only while it predicts better than no correction: each
+    // training round first evaluates the current network on the round's fresh batch (data it has not
+    // trained on) and keeps its correction on for the next rounds if that loss is below
+    // useful_ratio x the loss of predicting zero (the batch's mean squared target).
+    bool net_useful = false;
+    double useful_ratio = 0.8, zero_loss = 0.0, heldout_loss = 0.0;
+    double* h_loss = nullptr;  // pinned copy of the first training step's loss
     // Test hook of the checked build: the next neighbour search writes index n + corrupt_neighbor - 1
     // into particle 0's list (0: off).
     uint32_t corrupt_neighbor = 0;
@@ -307,6 +315,7 @@ public:
         if (h_ctl) cudaFreeHost(h_ctl);
         if (h_status) cudaFreeHost(h_status);
         if (h_dt) cudaFreeHost(h_dt);
+        if (h_loss) cudaFreeHost(h_loss);
         f(dtd);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -630,6 +639,7 @@ public:
         if (count != n) invalidate_graphs();
         n = count;
         cur = 0;
+        last_lp = false;  // the uploaded state carries no learned warm start
         if (count) {
             float* sx = stage;
             float* sv = stage + (size_t)count * 3;
@@ -1246,7 +1256,7 @@ public:
             launch_divergence_residual<Real>(ds, n, true, eta, kMinItersV, max_iter, 0, false, stream);
             launches += 3;
         } else {
-            const bool infer = mlp_ready && !base_only, use = infer || base_only;
+            const bool infer = mlp_ready && !base_only && net_useful, use = mlp_ready || base_only;
             launch_density_alpha<Real>(ds, n, false, true, stream);
             if (infer) launch_mlp_forward(mlp, features, n, pred, status, stream);
             launch_warm_values<Real>(ds, n, 0, use, infer, damping, stream);
@@ -1279,7 +1289,7 @@ public:
             launch_pressure_residual<Real>(ds, n, true, eta, kMinItersP, max_iter, 0, false, stream);
             launches += 2;
         } else {
-            const bool infer = mlp_ready && !base_only, use = infer || base_only;
+            const bool infer = mlp_ready && !base_only && net_useful, use = mlp_ready || base_only;
             launch_warm_values<Real>(ds, n, 1, use, infer, damping, stream);
             launches += 1;
             if (use && probe) {
@@ -1438,6 +1448,11 @@ public:
         forced_warm = 0;
         step_trained = false;
         if (lp) DF_CUDA(cudaMemsetAsync(status + 2, 0, sizeof(uint32_t), stream));
+        if (learned && !lp && last_lp && n) {  // the gate's first plain step after learned ones
+            launch_restore_totals<Real>(ds, n, stream);
+            launches += 1;
+        }
+        last_lp = lp;
         DF_TRY(neighbors_search());
         const bool div = sc.enable_divergence_solver != 0;
         if (div) {
@@ -1448,7 +1463,7 @@ public:
             if (lp) {  // no divergence solve: its warm-start arrays stay zero
                 DF_CUDA(cudaMemsetAsync(kappaVW, 0, (size_t)n * sizeof(Real), stream));
                 DF_CUDA(cudaMemsetAsync(kappaV[cur], 0, (size_t)n * sizeof(Real), stream));
-                if (mlp_ready && !base_only) {
+                if (mlp_ready && !base_only && net_useful) {
                     launch_mlp_forward(mlp, features, n, pred, status, stream);
                     launches += 1;
                 }
@@ -1549,6 +1564,7 @@ public:
         launches += 2;
         adam_t = 0;
         mlp_ready = false;
+        net_useful = false;
         scales_set = false;
         DF_CUDA(cudaGetLastError());
         return DFSPH_OK;
@@ -1628,6 +1644,16 @@ public:
             }
         }
         scales_set = true;
+        {  // loss of predicting zero on this batch, in the units the network trains in (new scales)
+            double z = 0.0;
+            for (uint32_t k = 0; k < B; ++k)
+                for (int o = 0; o < kMlpOut; ++o) {
+                    const double e = (double)t[(size_t)k * kMlpOut + o] * (double)h_scales.out_scale[o] /
+                                     (double)ns.out_scale[o];
+                    z += e * e;
+                }
+            zero_loss = z / (double)B;
+        }
         if (!changed) return DFSPH_OK;
         std::vector<float> prm(kMlpParams);
         DF_CUDA(cudaMemcpyAsync(prm.data(), mlp.params, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, stream));
@@ -1661,10 +1687,20 @@ public:
         launch_gather_training<Real>(ds, n, B, offset, div, tx, tt, stream);
         launches += 1;
         DF_TRY(adapt_scales(B, offset, div));
-        for (int it = 0; it < train_iters; ++it)
+        if (!h_loss) DF_CUDA(cudaMallocHost((void**)&h_loss, sizeof(double)));
+        const bool evaluated = mlp_ready && train_iters > 0;
+        for (int it = 0; it < train_iters; ++it) {
             launch_mlp_train_step(mlp, tx, tt, B, 1, (float)lr, 0.9f, 0.999f, 1e-8f, ++adam_t, stream);
+            // the first step's loss is the current network's, before it has seen this batch
+            if (it == 0) DF_CUDA(cudaMemcpyAsync(h_loss, mlp.loss, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        }
         launch_mlp_pack(mlp, stream);
         launches += 1 + 2ull * (uint64_t)train_iters;
+        DF_CUDA(cudaStreamSynchronize(stream));
+        if (evaluated) {
+            heldout_loss = *h_loss;
+            net_useful = zero_loss > 0.0 && heldout_loss < useful_ratio * zero_loss;
+        }
         mlp_ready = true;
         step_trained = true;
         ++trainings;
@@ -1700,6 +1736,7 @@ public:
         DF_CUDA(cudaStreamSynchronize(stream));
         adam_t = 0;
         mlp_ready = true;
+        net_useful = true;  // a network given by the caller is used as given
         return DFSPH_OK;
     }
 
@@ -1764,6 +1801,7 @@ public:
         DF_CUDA(cudaGetLastError());
         if (loss) *loss = l;
         mlp_ready = true;
+        net_useful = true;  // trained by the caller on its own data: used as given
         return DFSPH_OK;
     }
 
@@ -1953,7 +1991,7 @@ public:
         std::ofstream f(path, std::ios::binary | std::ios::trunc);
         DF_CHECK(f.is_open(), DFSPH_E_INVALID, std::string("cannot open ") + path);
         f.write(kCkptMagic, 8);
-        put(f, (int32_t)2);
+        put(f, (int32_t)3);
         put(f, (int32_t)sizeof(Real));
         put(f, n);
         put(f, nb);
@@ -1992,6 +2030,10 @@ public:
             for (uint32_t v : {it - gate_it0, itv - gate_itv0}) put(f, v);
             for (double v : {gate_margin, gate_last_excess}) put(f, v);
             for (uint64_t v : {gate_learned_steps, gate_plain_steps}) put(f, v);
+            // version 3: whether the network's correction is in use, and the losses that decided it
+            put(f, (int32_t)(net_useful ? 1 : 0));
+            put(f, (int32_t)(last_lp ? 1 : 0));
+            for (double v : {useful_ratio, zero_loss, heldout_loss}) put(f, v);
         }
         DF_CHECK(f.good(), DFSPH_E_INVALID, std::string("write failed: ") + path);
         return DFSPH_OK;
@@ -2007,7 +2049,7 @@ public:
         int32_t version = 0, rbytes = 0;
         uint32_t cn = 0, cnb = 0;
         dfsph_scene csc{};
-        DF_CHECK(get(f, version) && (version == 1 || version == 2) && get(f, rbytes) && get(f, cn) && get(f, cnb) &&
+        DF_CHECK(get(f, version) && version >= 1 && version <= 3 && get(f, rbytes) && get(f, cn) && get(f, cnb) &&
                      get(f, csc),
                  DFSPH_E_INVALID, "bad checkpoint header");
         DF_CHECK(rbytes == (int32_t)sizeof(Real), DFSPH_E_INVALID, "checkpoint precision differs from the context's");
@@ -2103,6 +2145,17 @@ public:
                 DF_TRY(gate_sums(it, itv));
                 gate_it0 = it - part[0];
                 gate_itv0 = itv - part[1];
+            }
+            if (version >= 3) {
+                int32_t used = 0, prev = 0;
+                DF_CHECK(get(f, used) && get(f, prev) && get(f, useful_ratio) && get(f, zero_loss) &&
+                             get(f, heldout_loss),
+                         DFSPH_E_INVALID, "truncated checkpoint");
+                net_useful = used != 0;
+                last_lp = prev != 0;
+            } else {
+                net_useful = mlp_ready;  // earlier files: the network was used whenever trained
+                last_lp = false;
             }
             DF_TRY(upload_scales());
             launch_mlp_pack(mlp, stream);
@@ -2276,6 +2329,10 @@ public:
         else if (k == "learned_warm_start") return enable_learned(v != 0);
         else if (k == "warm_start_probe") probe = v != 0;
         else if (k == "learned_base_only") base_only = v != 0;
+        else if (k == "network_useful_ratio") {
+            DF_CHECK(v >= 0, DFSPH_E_INVALID, "network_useful_ratio must be >= 0");
+            useful_ratio = v;
+        }
         else if (k == "checked_corrupt_neighbor") {
 #ifdef DFSPH_CHECKED
             DF_CHECK(v >= 1 && v <= 64 && n + (uint32_t)v <= Nc, DFSPH_E_INVALID,
@@ -2376,6 +2433,9 @@ public:
         else if (k == "learned_warm_start") *v = learned ? 1 : 0;
         else if (k == "warm_start_probe") *v = probe ? 1 : 0;
         else if (k == "learned_base_only") *v = base_only ? 1 : 0;
+        else if (k == "network_useful_ratio") *v = useful_ratio;
+        else if (k == "network_used") *v = net_useful ? 1 : 0;
+        else if (k == "mlp_heldout_ratio") *v = zero_loss > 0 ? heldout_loss / zero_loss : -1.0;
         else if (k == "checked_build") {
 #ifdef DFSPH_CHECKED
             *v = 1;

@@ -116,6 +116,7 @@ void launch_warm_values(const DevState<Real>* d, uint32_t n, int which, bool lea
                         cudaStream_t s);
 // kappaT / kappaVT = the pressure / divergence coefficients this step's solves needed: applied
 // totals (warm start + corrections) less the excess the unclamped final residuals show.
+template <class Real> void launch_restore_totals(const DevState<Real>* d, uint32_t n, cudaStream_t s);
 template <class Real> void launch_totals(const DevState<Real>* d, uint32_t n, bool div_ran, cudaStream_t s);
 // Training pairs of `batch` particles spread over [0, n): x = features, t = targets
 // [(needed kappa)/r2 - kappaT_prev, (needed kappa_v)/hr - kappaVT_prev] / out_scale.

@@ -1055,6 +1055,18 @@ __device__ __forceinline__ void needed_totals(const DevState<Real>* __restrict__
                   : Real(0);
 }
 
+// A plain step after a learned one (the cost gate's probe windows): the reference warm start carries
+// a solve's corrections only, and after a learned step those miss the learned warm start the solve
+// began from; the applied warm start is added back so that the plain step starts from the total.
+template <class Real>
+__global__ void __launch_bounds__(kBlock) restore_totals_kernel(const DevState<Real>* __restrict__ ds, uint32_t n) {
+    DFSPH_PDL_ENTER;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ds->kappa[i] = ds->kappa[i] + ds->kappaW[i];
+    ds->kappaV[i] = ds->kappaV[i] + ds->kappaVW[i];
+}
+
 template <class Real>
 __global__ void __launch_bounds__(kBlock) totals_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                         bool div_ran) {
@@ -1110,6 +1122,9 @@ template <class Real>
 void launch_warm_values(const DevState<Real>* d, uint32_t n, int which, bool learned, bool use_pred, double damping,
                         cudaStream_t s) {
     if (n) launch_pdl(warm_values_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, which, learned, use_pred, (Real)damping);
+}
+template <class Real> void launch_restore_totals(const DevState<Real>* d, uint32_t n, cudaStream_t s) {
+    if (n) launch_pdl(restore_totals_kernel<Real>, grid_for(n), kBlock, 0, s, d, n);
 }
 template <class Real> void launch_totals(const DevState<Real>* d, uint32_t n, bool div_ran, cudaStream_t s) {
     if (n) launch_pdl(totals_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, div_ran);
@@ -1217,6 +1232,7 @@ template <class Real> void launch_cfl_reduce(const DevState<Real>* d, uint32_t n
     template void launch_probe_residual<R>(const DevState<R>*, uint32_t, int, const Vec4<R>*, cudaStream_t);        \
     template void launch_warm_values<R>(const DevState<R>*, uint32_t, int, bool, bool, double, cudaStream_t);       \
     template void launch_totals<R>(const DevState<R>*, uint32_t, bool, cudaStream_t);                               \
+    template void launch_restore_totals<R>(const DevState<R>*, uint32_t, cudaStream_t);                              \
     template void launch_gather_training<R>(const DevState<R>*, uint32_t, uint32_t, uint32_t, bool, float*, float*, \
                                             cudaStream_t);                                                           \
     template void launch_divergence_residual<R>(const DevState<R>*, uint32_t, bool, double, int, int,               \
