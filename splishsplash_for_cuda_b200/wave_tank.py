@@ -138,7 +138,7 @@ class WaveTank:
             return
         step = np.sign(gap) * WINDOW_STEP
         a, r = self.d.shift_dynamic_window((step, 0.0, 0.0), 0.9 * 2 * R, 1100.0)
-        self.d.open_boundary_shift((step, 0.0, 0.0))
+        self.d.shift_open_boundary((step, 0.0, 0.0))
         self.window_x += step
         self.shifts += 1
         self.added += a
