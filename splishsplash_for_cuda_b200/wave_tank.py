@@ -61,8 +61,12 @@ def wave_tank_scene(counts=(400, 100, 100), seed: int = 5, box_offset: float = 1
     rng = np.random.default_rng(seed)
     center = np.array([0.5 * (2 * PISTON_REST + length) + box_offset + rng.uniform(-0.1, 0.1), level,
                        0.5 * width + rng.uniform(-0.1, 0.1)])
-    body = RigidBody.box(center, (0.4, 0.2, 0.2), 500.0, d)
+    size = np.array([0.4, 0.2, 0.2])
+    body = RigidBody.box(center, size, 500.0, d)
     bx, _ = body.particles()
+    # the box displaces its volume: no fluid particle inside it or closer than 2r to its faces
+    inside = np.all(np.abs(fluid - center) < 0.5 * size + d, axis=1)
+    fluid = fluid[~inside]
     boundary = np.concatenate([walls, bx]).astype(np.float32)
     cfg = Configuration(timeStepSize=0.005, particleRadius=R, density0=1000.0, viscosity=0.01, cflMethod=1,
                         cflFactor=0.4, cflMaxTimeStepSize=0.005, maxIterations=100, maxError=0.01,

@@ -14,7 +14,7 @@ BAD = _capi.ST_NONFINITE | _capi.ST_PRESSURE_NOT_CONVERGED | _capi.ST_NEIGHBOR_O
 
 
 def test_wave_tank_runs_clean():
-    scene, layout = wave_tank_scene(counts=(80, 20, 20), box_offset=0.6)
+    scene, layout = wave_tank_scene(counts=(120, 20, 20), box_offset=0.4)
     tank = WaveTank(scene, layout, window_every=30, open_boundary_every=5)
     y0 = tank.body.x[1]
     for _ in range(120):
