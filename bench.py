@@ -258,7 +258,7 @@ def ablation_scene(workload: str):
     raise ValueError(workload)
 
 
-def learned_ablation(local, steps: int, workload: str = "column_64"):
+def learned_ablation(local, steps: int, workload: str = "column_64", window: int = 0):
     """Plain vs learned warm start on the same scene from the same state, each for `steps` steps;
     the second half is measured (the flow has developed by then). ms/step is the device time of each
     step (CUDA events inside dfsph_step), online training rounds included. "base" is the learned
@@ -266,7 +266,8 @@ def learned_ablation(local, steps: int, workload: str = "column_64"):
     inference, no training), so "learned" vs "base" is the trained network's own contribution.
     "gated" is the learned warm start behind its cost gate (learned passes only while the plain
     solver needs at least one iteration per step above the minimum counts; plain probe windows
-    included in the average)."""
+    included in the average). window > 0 adds, per mode, the means over consecutive windows of that
+    many steps across the whole run (the full horizon) and the mean over all steps."""
     from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
 
     scene, walls = ablation_scene(workload)
@@ -283,7 +284,7 @@ def learned_ablation(local, steps: int, workload: str = "column_64"):
             d.set_learned_warm_start(True, gate=mode == "gated")
         if mode == "base":
             d.set_param("learned_base_only", 1)
-        its, itv, ms, bits, t = [], [], [], 0, 0.0
+        its, itv, ms, hs, bits, t = [], [], [], [], 0, 0.0
         for _ in range(steps):
             if walls is not None:
                 walls(d, t)
@@ -292,12 +293,21 @@ def learned_ablation(local, steps: int, workload: str = "column_64"):
             its.append(st.iterations)
             itv.append(st.iterations_v)
             ms.append(st.ms_total)
+            hs.append(st.h)
             bits |= st.status
         w = slice(steps // 2, steps)
         rec = {"pressure_iterations": round(float(np.mean(its[w])), 2),
                "divergence_iterations": round(float(np.mean(itv[w])), 2),
                "ms_per_step": round(float(np.mean(ms[w])), 4), "status_bits": int(bits),
                "simulated_s": round(t, 4)}
+        if window > 0:
+            rec["windows"] = [{"steps": f"{a}..{min(a + window, steps) - 1}",
+                               "pressure_iterations": round(float(np.mean(its[a:a + window])), 2),
+                               "divergence_iterations": round(float(np.mean(itv[a:a + window])), 2),
+                               "ms_per_step": round(float(np.mean(ms[a:a + window])), 3),
+                               "dt_ms": round(1e3 * float(np.mean(hs[a:a + window])), 3)}
+                              for a in range(0, steps, window)]
+            rec["ms_per_step_all"] = round(float(np.mean(ms)), 4)
         if mode == "gated":
             rec.update(learned_steps=int(d.get_param("gate_learned_steps")),
                        plain_steps=int(d.get_param("gate_plain_steps")),
@@ -506,7 +516,7 @@ def run_ours(args, world, rank, local):
 
     ablation = None
     if rank == 0 and world == 1 and args.ablation_steps > 0:
-        ablation = {w: learned_ablation(local, args.ablation_steps, w) for w in args.ablation_workloads}
+        ablation = {w: learned_ablation(local, args.ablation_steps, w, args.ablation_window) for w in args.ablation_workloads}
 
     if rank == 0:
         line = {
@@ -561,6 +571,8 @@ def main():
     ap.add_argument("--ablation-steps", type=int, default=300,
                     help="steps per mode of the plain vs learned warm-start comparison (0: skip)")
     ap.add_argument("--ablation-workloads", nargs="*", choices=ABLATION_WORKLOADS, default=list(ABLATION_WORKLOADS))
+    ap.add_argument("--ablation-window", type=int, default=0,
+                    help="with --ablation-only: also report means over windows of this many steps")
     ap.add_argument("--ablation-only", action="store_true",
                     help="print only the plain vs learned comparison as one JSON line")
     args = ap.parse_args()
@@ -570,7 +582,8 @@ def main():
     try:
         if args.ablation_only:
             if rank == 0:
-                print(json.dumps({"learned_warm_start": {w: learned_ablation(local, args.ablation_steps, w)
+                print(json.dumps({"learned_warm_start": {w: learned_ablation(local, args.ablation_steps, w,
+                                                                            args.ablation_window)
                                                          for w in args.ablation_workloads}}), flush=True)
         elif args.impl == "reference":
             run_reference_arm(args, world, rank)
