@@ -2,9 +2,10 @@
 open boundary, floating box of density 500 and the dynamic window together, through the C ABI. Over
 450 steps (dt at most 1 ms), the window checked at most every 30 steps at the piston's furthest
 advance: no non-finite, escaped or non-converged state, no particle faster than 5 m/s (the piston
-moves at most 0.84 m/s), the fluid count within 5 % of the initial one, the window shifts toward the
-box, the layer and the window exchange particles, and the box keeps floating near the rest level
-(density 500: half submerged)."""
+moves at most 0.9 m/s), the fluid count within 15 % of the initial one (a shift removes a 0.5 m slab,
+a fifth of this short tank, that the piston's stroke has raised; the new slab is at rest), the window
+shifts toward the box, the layer and the window exchange particles, and the box keeps floating near
+the rest level (density 500: half submerged)."""
 import numpy as np
 import pytest
 
@@ -27,7 +28,7 @@ def test_wave_tank_runs_clean():
         if tank.steps % 10 == 0:
             speed = np.linalg.norm(tank.d.velocities(), axis=1)
             assert speed.max() < 5.0, (tank.steps, float(speed.max()))
-            assert abs(tank.d.num_fluid() - n0) < 0.05 * n0, (tank.steps, tank.d.num_fluid())
+            assert abs(tank.d.num_fluid() - n0) < 0.15 * n0, (tank.steps, tank.d.num_fluid())
     assert tank.shifts >= 1
     assert tank.added > 0 and tank.removed > 0
     assert abs(tank.body.x[1] - y0) < 0.1
