@@ -377,8 +377,10 @@ def run_wave_tank(args, world, rank, local):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice + xoshiro256** jitter)",
             "config": {"workload": scene.name, "fluid_particles": scene.n_fluid, "boundary_particles": scene.n_boundary,
                        "warm_start": "plain" if args.plain_wave_tank else "learned (gated)",
-                       "piston": "0.2 m, 1.5 s", "absorbing_layer_m": 0.3, "window_shift_m": 0.5,
-                       "window_every_steps": tank.window_every, "floating_box": "0.4 x 0.2 x 0.2 m, 500 kg/m^3",
+                       "lattice_spacing_mm": 18.59, "piston": "0.2 m, 1.5 s", "absorbing_layer_m": 0.3,
+                       "window_shift_m": 0.5, "window_check_every_steps": tank.window_every,
+                       "window_shift_when": "piston at its furthest advance",
+                       "floating_box": "0.403 x 0.199 x 0.199 m, 500 kg/m^3", "dt_max_ms": 1.0,
                        "parallelism": "replicas" if world > 1 else "single"},
             "iterations_per_step": round(float(np.mean(its)), 2), "iterations_v_per_step": round(float(np.mean(itv)), 2),
             "solver_ms_per_step": round(float(np.mean(solver_ms)), 4), "status_bits": int(tank.status),
