@@ -356,18 +356,25 @@ int dfsph_bgeo_read(const char* path, float* xyz, float* vxyz, uint64_t capacity
 
 /* ---- simple open boundary (OpenBoundariesSimpleInterface, OpenBoundariesSimple.{h,cu}) ----------
  * Surfaces are the reference's BufferFluidSurface shapes (BufferFluidSurface.cu:421-900) with its
- * type numbers; the triangle-mesh shape (3) is not offered. "Inside" follows isinside(): plane
+ * type numbers. "Inside" follows isinside(): plane
  * (x - origin) . normal >= 0; cuboid |x - center| < half_lengths component-wise; cylinder (axis y)
  * |dy| <= half_lengths[1] and horizontal distance < radius; sphere distance < radius; star (axis y,
  * `points` linear-sided points, the first along `direction`) |dy| <= half_lengths[1] and inside the
- * star outline between radius_internal and radius. reversed != 0 swaps inside and outside. The
- * normal used by the inflow is center - x (cylinder, sphere, star; negated when reversed,
- * normalised) and zero for planes and cuboids. All surface arithmetic is FP32. */
+ * star outline between radius_internal and radius; mesh (3): the closed triangle mesh registered
+ * with dfsph_set_surface_mesh under the id `points`, translated by `center` (MeshPerso, :49-410):
+ * outside the box of its vertices and the origin (translated) a point is outside, inside that box it
+ * is inside when the ray from it along normalise(2.575, 6.19763, 5.986) crosses an odd number of
+ * triangles ahead of it (Moller-Trumbore with the reference's 1e-7 parallel cut-off, :14-47).
+ * reversed != 0 swaps inside and outside. The normal used by the inflow is center - x (cylinder,
+ * sphere, star; negated when reversed, normalised) and zero for planes, cuboids and meshes. All
+ * surface arithmetic is FP32 (1/a of the ray test in FP64, as the reference divides 1.0 by it). */
 #define DFSPH_SURFACE_PLANE 0
 #define DFSPH_SURFACE_CUBOID 1
 #define DFSPH_SURFACE_CYLINDER 2
+#define DFSPH_SURFACE_MESH 3
 #define DFSPH_SURFACE_SPHERE 4
 #define DFSPH_SURFACE_STAR 5
+#define DFSPH_MAX_SURFACE_MESHES 8
 typedef struct dfsph_surface {
     int32_t type;            /* DFSPH_SURFACE_*                                                   */
     int32_t reversed;        /* != 0: inside and outside swapped                                  */
@@ -380,6 +387,19 @@ typedef struct dfsph_surface {
     uint32_t points;         /* star: number of points (>= 1)                                     */
     float direction[3];      /* star: direction of the first point (horizontal)                   */
 } dfsph_surface;
+
+/* Registers (or replaces) the triangle mesh `mesh_id` (< DFSPH_MAX_SURFACE_MESHES) for surfaces of
+ * type DFSPH_SURFACE_MESH: n_vertices positions (xyz[3 n]) and n_triangles vertex-index triples. The
+ * mesh should be closed. Surfaces already given to dfsph_open_boundary_init see the new mesh from
+ * their next use. Errors: DFSPH_E_INVALID for an index out of range or no triangles. */
+int dfsph_set_surface_mesh(dfsph_ctx* ctx, uint32_t mesh_id, const float* vertices, uint32_t n_vertices,
+                           const uint32_t* triangles, uint32_t n_triangles);
+/* Wavefront OBJ reader for such meshes (the reference loads them with OBJ_Loader, MeshPerso::
+ * loadFromFile): `v x y z` vertices and `f` faces (indices 1-based or negative, `i/t/n` forms),
+ * polygons split into fans from their first vertex; other records are skipped. With null arrays only
+ * the counts are returned; otherwise the capacities must hold them. No GPU is needed. */
+int dfsph_read_obj(const char* path, float* vertices, uint32_t vertex_capacity, uint32_t* n_vertices,
+                   uint32_t* triangles, uint32_t triangle_capacity, uint32_t* n_triangles);
 
 /* OpenBoundariesSimpleInterface::init (OpenBoundariesSimple.cu:105-350): boundary is the simulation
  * boundary, interior a slightly smaller copy (the reference uses 3 r less), fluid_surface the

@@ -187,10 +187,72 @@ struct Surface {
 float sdot(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 float snorm(const float* a) { return std::sqrt(sdot(a, a)); }
 
+// Triangle meshes of type-3 surfaces by id (MeshPerso, BufferFluidSurface.cu:49-410): triangles as
+// vertex triples, the box of the vertices and the origin, the ray direction.
+struct OracleMesh {
+    std::vector<float> tri;  // 9 per triangle
+    float bmin[3] = {0.f, 0.f, 0.f}, bmax[3] = {0.f, 0.f, 0.f};
+};
+OracleMesh g_meshes[8];
+
+void ray_direction(float d[3]) {  // normalise((2.575, 6.19763, 5.986)) in FP32, each operation rounded
+    const float x = (float)2.575, y = (float)6.19763, z = (float)5.986;
+    const float n = std::sqrt(x * x + y * y + z * z);
+    d[0] = x / n;
+    d[1] = y / n;
+    d[2] = z / n;
+}
+void scross(const float* a, const float* b, float* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+// RayIntersectsTriangle<true, false> (BufferFluidSurface.cu:14-47) followed by the t > 0 test of
+// MeshPerso::isInside.
+bool ray_hits_ahead(const float* o, const float* d, const float* v0, const float* v1, const float* v2) {
+    const float eps = 1e-7f;
+    float e1[3], e2[3], h[3], s[3], q[3];
+    for (int a = 0; a < 3; ++a) {
+        e1[a] = v1[a] - v0[a];
+        e2[a] = v2[a] - v0[a];
+    }
+    scross(d, e2, h);
+    const float a = sdot(e1, h);
+    if (a > -eps && a < eps) return false;
+    const float f = (float)(1.0 / (double)a);
+    for (int k = 0; k < 3; ++k) s[k] = o[k] - v0[k];
+    const float u = f * sdot(s, h);
+    if (u < 0.0f || u > 1.0f) return false;
+    scross(s, e1, q);
+    const float v = f * sdot(d, q);
+    if (v < 0.0f || u + v > 1.0f) return false;
+    return f * sdot(e2, q) > 0.0f;
+}
+bool mesh_inside(const Surface& S, const float* p) {
+    const OracleMesh& m = g_meshes[S.points];
+    for (int a = 0; a < 3; ++a)
+        if (p[a] < m.bmin[a] + S.center[a]) return false;
+    for (int a = 0; a < 3; ++a)
+        if (p[a] > m.bmax[a] + S.center[a]) return false;
+    float d[3];
+    ray_direction(d);
+    uint32_t hits = 0;
+    const size_t nt = m.tri.size() / 9;
+    for (size_t t = 0; t < nt; ++t) {
+        float v[9];
+        for (int k = 0; k < 9; ++k) v[k] = m.tri[9 * t + k] + S.center[k % 3];
+        if (ray_hits_ahead(p, d, v, v + 3, v + 6)) ++hits;
+    }
+    return (hits & 1u) != 0u;
+}
+
 bool surface_inside(const Surface& S, const float* p) {
     bool r = false;
     float v[3];
     switch (S.type) {
+        case 3:
+            r = S.points < 8 && mesh_inside(S, p);
+            break;
         case 0:
             for (int a = 0; a < 3; ++a) v[a] = p[a] - S.origin[a];
             r = !(sdot(v, S.normal) < 0.0f);
@@ -1083,6 +1145,24 @@ int oracle_remove_outside_box(void* h, const float* lo, const float* hi, uint32_
 }
 
 // inside[i] and normal[3 i..] of the restated BufferFluidSurface::isinside / getNormal.
+int oracle_set_surface_mesh(uint32_t id, const float* v, uint32_t nv, const uint32_t* t, uint32_t nt) {
+    if (id >= 8 || nt == 0) return -1;
+    OracleMesh& m = g_meshes[id];
+    m = OracleMesh{};
+    for (uint32_t i = 0; i < nv; ++i)
+        for (int a = 0; a < 3; ++a) {
+            const float x = v[3 * (size_t)i + a];
+            if (m.bmin[a] > x) m.bmin[a] = x;
+            if (m.bmax[a] < x) m.bmax[a] = x;
+        }
+    m.tri.resize(9 * (size_t)nt);
+    for (size_t k = 0; k < 3 * (size_t)nt; ++k) {
+        if (t[k] >= nv) return -1;
+        for (int a = 0; a < 3; ++a) m.tri[3 * k + a] = v[3 * (size_t)t[k] + a];
+    }
+    return 0;
+}
+
 int oracle_surface_eval(const Surface* s, const float* p, uint32_t n, uint8_t* inside, float* normal) {
     for (uint32_t i = 0; i < n; ++i) {
         inside[i] = surface_inside(*s, p + 3 * (size_t)i) ? 1 : 0;

@@ -107,6 +107,7 @@ def _load():
             "oracle_open_boundary_shift": (C.c_int, [vp, fp]),
             "oracle_remove_outside_box": (C.c_int, [vp, fp, fp, up]),
             "oracle_surface_eval": (C.c_int, [C.POINTER(OracleSurface), fp, C.c_uint32, C.c_void_p, fp]),
+            "oracle_set_surface_mesh": (C.c_int, [C.c_uint32, fp, C.c_uint32, up, C.c_uint32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -283,6 +284,16 @@ class Oracle:
 
     def open_boundary_shift(self, delta) -> None:
         self.lib.oracle_open_boundary_shift(self.h, _f(np.asarray(delta, np.float32).reshape(3)))
+
+
+def set_surface_mesh(mesh_id: int, vertices, triangles) -> None:
+    """Registers the triangle mesh mesh_id for the oracle's type-3 surfaces (one table per process)."""
+    lib = _load()
+    v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+    if lib.oracle_set_surface_mesh(int(mesh_id), _f(v), v.shape[0], t.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                   t.shape[0]) != 0:
+        raise ValueError("invalid mesh")
 
 
 def surface_eval(surface, points):

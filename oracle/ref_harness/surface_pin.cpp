@@ -1,11 +1,14 @@
 // surface_pin.cpp — runs the reference's own BufferFluidSurface (SPlisHSPlasH/DFSPH/BufferFluidSurface.cu,
 // the shapes of the simple open boundary) on the host: its __host__ __device__ members compile as host
 // code. Test infrastructure only: the open-boundary pins compare the oracle's restatement of
-// isinside / getNormal with it. The mesh shape is not used (it needs managed memory).
+// isinside / getNormal with it. The mesh shape's class needs managed memory, so pin_mesh_inside runs
+// the steps of MeshPerso::isInside (BufferFluidSurface.cu:224-270: the box of the vertices and the
+// origin, the fixed ray, the reference's own RayIntersectsTriangle) on host arrays.
 #include <cstdint>
 #include <cstring>
 #include <sstream>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -47,6 +50,39 @@ int pin_surface_eval(const PinSurface* s, const float* p, uint32_t n, uint8_t* i
         normal[3 * i] = nr.x;
         normal[3 * i + 1] = nr.y;
         normal[3 * i + 2] = nr.z;
+    }
+    return 0;
+}
+
+// MeshPerso::isInside for the mesh (vertices v[3 nv], triangles t[3 nt]) moved by offset[3].
+int pin_mesh_inside(const float* v, uint32_t nv, const uint32_t* t, uint32_t nt, const float* offset,
+                    const float* p, uint32_t n, uint8_t* inside) {
+    Vector3d bmin(0, 0, 0), bmax(0, 0, 0);
+    std::vector<Vector3d> V(nv);
+    for (uint32_t i = 0; i < nv; ++i) {
+        V[i] = Vector3d(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+        bmin.toMin(V[i]);
+        bmax.toMax(V[i]);
+    }
+    const Vector3d off(offset[0], offset[1], offset[2]);
+    Vector3d u(2.575, 6.19763, 5.986);
+    u.toUnit();
+    for (uint32_t k = 0; k < n; ++k) {
+        const Vector3d x(p[3 * k], p[3 * k + 1], p[3 * k + 2]);
+        if ((x < bmin + off) || x > bmax + off) {
+            inside[k] = 0;
+            continue;
+        }
+        int count = 0;
+        for (uint32_t f = 0; f < nt; ++f) {
+            Vector3d ip(0);
+            RealCuda dist = 0;
+            if (RayIntersectsTriangle<true, false>(x, u, V[t[3 * f]] + off, V[t[3 * f + 1]] + off, V[t[3 * f + 2]] + off,
+                                                   ip, dist)) {
+                if (dist > 0) count++;
+            }
+        }
+        inside[k] = (count & 1) ? 1 : 0;
     }
     return 0;
 }

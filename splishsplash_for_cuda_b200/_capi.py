@@ -29,7 +29,8 @@ ST_FLUID_CAPACITY = 0x80
 ST_MMA_TIMEOUT = 0x100
 ST_INDEX = 0x200
 
-SURFACE_PLANE, SURFACE_CUBOID, SURFACE_CYLINDER, SURFACE_SPHERE, SURFACE_STAR = 0, 1, 2, 4, 5
+SURFACE_PLANE, SURFACE_CUBOID, SURFACE_CYLINDER, SURFACE_MESH, SURFACE_SPHERE, SURFACE_STAR = 0, 1, 2, 3, 4, 5
+MAX_SURFACE_MESHES = 8
 
 
 class Surface(C.Structure):
@@ -158,6 +159,9 @@ SIGNATURES = {
     "dfsph_open_boundary_apply": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_uint32),
                                             C.POINTER(C.c_uint32)]),
     "dfsph_open_boundary_shift": (C.c_int, [_P, _P]),
+    "dfsph_set_surface_mesh": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32]),
+    "dfsph_read_obj": (C.c_int, [C.c_char_p, _P, C.c_uint32, C.POINTER(C.c_uint32), _P, C.c_uint32,
+                                 C.POINTER(C.c_uint32)]),
     "dfsph_dynamic_window_init": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32]),
     "dfsph_dynamic_window_shift": (C.c_int, [_P, _P, C.c_double, C.c_double, C.POINTER(C.c_uint32),
                                              C.POINTER(C.c_uint32)]),

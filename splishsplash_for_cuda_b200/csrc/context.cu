@@ -68,8 +68,10 @@ public:
     dfsph_scene sc{};
     cudaStream_t stream = nullptr;
     // Velocities given to update_fluid travel on a copy stream and are applied inside the next
-    // step's binning, after the sort (which does not read them): their upload overlaps the key pass
-    // and the radix sort. Any other call applies them first (flush_pending).
+    // step's neighbour search, after the neighbour build (the key pass, the sort, the reorder and
+    // the build do not read them; the reorder moves stale values that the flush overwrites in the
+    // new order): their upload overlaps those passes. Any other call applies them first
+    // (flush_pending).
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_vel_ready = nullptr, ev_vel_free = nullptr;
     bool pending_vel = false;
@@ -311,6 +313,10 @@ public:
         f(mlp.w1_bf16); f(mlp.w2_bf16); f(mlp.w3_bf16); f(mlp.scales); f(mlp.loss);
         f(ob_samples); f(ob_vel); f(ob_flag); f(ob_rank); f(ob_scan); f(ob_total); f(wrench_buf);
         f(brest); f(dw_samples); f(dw_sel); f(dw_vel); f(dw_flag); f(dw_rank);
+        for (MeshSlot& m : meshes) {
+            f(m.tri);
+            m = MeshSlot{};
+        }
         if (h_ob) cudaFreeHost(h_ob);
         if (h_ctl) cudaFreeHost(h_ctl);
         if (h_status) cudaFreeHost(h_status);
@@ -716,9 +722,10 @@ public:
         if (boundary_forces && nb)
             DF_CUDA(cudaMemsetAsync(bforce_fx, 0, (size_t)nb * 3 * sizeof(unsigned long long), stream));
         if (!n) return DFSPH_OK;
-        DF_TRY(bin_fluid());
+        DF_TRY(bin_fluid(true));
         launch_build_neighbors<Real>(ds, n, ftab, btab, stream);
         launches += 1;
+        DF_TRY(flush_pending());  // velocities uploaded during the binning and the build
         if (corrupt_neighbor) {  // checked builds only (the key is rejected otherwise); one search
             launch_corrupt_first_neighbor(nbr, counts, n + corrupt_neighbor - 1u, stream);
             corrupt_neighbor = 0;
@@ -732,8 +739,9 @@ public:
         return DFSPH_OK;
     }
 
-    // Cell keys -> stable radix sort -> reorder (double buffer) -> cell table of the fluid.
-    int bin_fluid() {
+    // Cell keys -> stable radix sort -> reorder (double buffer) -> cell table of the fluid. With
+    // defer_velocities the caller applies velocities pending from update_fluid afterwards.
+    int bin_fluid(bool defer_velocities = false) {
         if (!n) {
             DF_CUDA(cudaMemsetAsync(ftab, 0, cells * sizeof(uint2), stream));
             return sync_state();
@@ -745,7 +753,7 @@ public:
                                radix_sort_workspace_words(n, key_passes));
         uint32_t *skeys, *perm;
         radix_sort_pairs(sb, n, key_passes, true, stream, status, &launches, &skeys, &perm, sort_withheld_tile, true);
-        DF_TRY(flush_pending());  // velocities uploaded during the key pass and the sort
+        if (!defer_velocities) DF_TRY(flush_pending());  // velocities uploaded during the key pass and the sort
         const int nx = 1 - cur;
         launch_reorder_fluid<Real>(perm, n, pos[cur], vel[cur], kappa[cur], kappaV[cur], id[cur], pos[nx], vel[nx],
                                    kappa[nx], kappaV[nx], id[nx], stream);
@@ -762,7 +770,63 @@ public:
 
     // ------------------------------------------------------------------------------------------
     // Simple open boundary (OpenBoundariesSimple.cu).
-    static bool surface_valid(const dfsph_surface& S) {
+    // Triangle meshes of DFSPH_SURFACE_MESH surfaces, by id.
+    struct MeshSlot {
+        float4* tri = nullptr;  // 3 per triangle
+        uint32_t nt = 0, cap = 0;
+        float bmin[3] = {0.f, 0.f, 0.f}, bmax[3] = {0.f, 0.f, 0.f};
+    };
+    MeshSlot meshes[DFSPH_MAX_SURFACE_MESHES];
+
+    int set_surface_mesh(uint32_t id, const float* v, uint32_t nv, const uint32_t* t, uint32_t nt) {
+        DF_CHECK(id < DFSPH_MAX_SURFACE_MESHES, DFSPH_E_INVALID, "mesh id beyond DFSPH_MAX_SURFACE_MESHES");
+        DF_CHECK(nt > 0 && v && t, DFSPH_E_INVALID, "a mesh needs vertices and at least one triangle");
+        for (size_t k = 0; k < 3 * (size_t)nt; ++k)
+            DF_CHECK(t[k] < nv, DFSPH_E_INVALID, "triangle vertex index out of range");
+        for (size_t k = 0; k < 3 * (size_t)nv; ++k)
+            DF_CHECK(std::isfinite(v[k]), DFSPH_E_INVALID, "mesh vertices must be finite");
+        MeshSlot& m = meshes[id];
+        if (nt > m.cap) {
+            if (m.tri) DF_CUDA(cudaFree(m.tri));
+            m.tri = nullptr;
+            m.cap = 0;
+            DF_TRY(dalloc(&m.tri, 3 * (size_t)nt));
+            m.cap = nt;
+        }
+        // MeshPerso::loadFromFile (BufferFluidSurface.cu:150-165): the box starts at the origin
+        for (int a = 0; a < 3; ++a) m.bmin[a] = m.bmax[a] = 0.0f;
+        for (uint32_t i = 0; i < nv; ++i)
+            for (int a = 0; a < 3; ++a) {
+                const float x = v[3 * (size_t)i + a];
+                if (m.bmin[a] > x) m.bmin[a] = x;
+                if (m.bmax[a] < x) m.bmax[a] = x;
+            }
+        std::vector<float4> h(3 * (size_t)nt);
+        for (size_t k = 0; k < 3 * (size_t)nt; ++k) {
+            const float* p = v + 3 * (size_t)t[k];
+            h[k] = make_float4(p[0], p[1], p[2], 0.f);
+        }
+        DF_CUDA(cudaMemcpyAsync(m.tri, h.data(), h.size() * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        m.nt = nt;
+        return DFSPH_OK;
+    }
+    DevSurface dev_surface(const dfsph_surface& s) const {
+        DevSurface d = plain_surface(s);
+        if (s.type == DFSPH_SURFACE_MESH && s.points < DFSPH_MAX_SURFACE_MESHES) {
+            const MeshSlot& m = meshes[s.points];
+            d.m.tri = m.tri;
+            d.m.nt = m.nt;
+            for (int a = 0; a < 3; ++a) {
+                d.m.bmin[a] = m.bmin[a];
+                d.m.bmax[a] = m.bmax[a];
+            }
+            mesh_ray_direction(d.m.dir);
+        }
+        return d;
+    }
+
+    bool surface_valid(const dfsph_surface& S) const {
         switch (S.type) {
             case DFSPH_SURFACE_PLANE:
             case DFSPH_SURFACE_CUBOID:
@@ -771,6 +835,8 @@ public:
                 return true;
             case DFSPH_SURFACE_STAR:
                 return S.points >= 1;
+            case DFSPH_SURFACE_MESH:
+                return S.points < DFSPH_MAX_SURFACE_MESHES && meshes[S.points].nt > 0;
             default:
                 return false;
         }
@@ -780,7 +846,8 @@ public:
                            const float* xyz, uint32_t ns, uint32_t* n_kept) {
         DF_CHECK(bnd && interior && surf, DFSPH_E_INVALID, "null surface");
         DF_CHECK(surface_valid(*bnd) && surface_valid(*interior) && surface_valid(*surf), DFSPH_E_INVALID,
-                 "unsupported surface (types: plane 0, cuboid 1, cylinder 2, sphere 4, star 5 with points >= 1)");
+                 "unsupported surface (types: plane 0, cuboid 1, cylinder 2, mesh 3 with a registered mesh id, "
+                 "sphere 4, star 5 with points >= 1)");
         DF_CHECK(xyz || ns == 0, DFSPH_E_INVALID, "null sample positions");
         DF_CHECK(grid_ready, DFSPH_E_STATE, "no grid: set a boundary or upload fluid first");
         if (ns > ob_cap || !ob_total) {
@@ -807,7 +874,8 @@ public:
             std::vector<float4> h(ns);
             for (uint32_t i = 0; i < ns; ++i) h[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.f);
             DF_CUDA(cudaMemcpyAsync(ob_vel, h.data(), (size_t)ns * sizeof(float4), cudaMemcpyHostToDevice, stream));
-            launch_open_boundary_select<Real>(ob_vel, ns, ob_interior, ob_surface, params(), ob_flag, stream);
+            launch_open_boundary_select<Real>(ob_vel, ns, dev_surface(ob_interior), dev_surface(ob_surface), params(),
+                                              ob_flag, stream);
             exclusive_scan_u32(ob_flag, ob_rank, ns, ob_scan, ob_total, stream);
             launch_compact_samples(ob_vel, ob_flag, ob_rank, ns, ob_samples, stream);
             DF_CUDA(cudaMemcpyAsync(h_ob, ob_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
@@ -1019,7 +1087,8 @@ public:
                 prev.center[a] = (float)(0.5 * (old_lo[a] + old_hi[a]));
                 prev.half_lengths[a] = (float)(0.5 * (old_hi[a] - old_lo[a]));
             }
-            launch_open_boundary_select<Real>(dw_samples, dw_ns, prev, all, params(), dw_flag, stream);
+            launch_open_boundary_select<Real>(dw_samples, dw_ns, plain_surface(prev), plain_surface(all), params(), dw_flag,
+                                              stream);
             exclusive_scan_u32(dw_flag, dw_rank, dw_ns, ob_scan, ob_total, stream);
             launch_compact_samples(dw_samples, dw_flag, dw_rank, dw_ns, dw_sel, stream);
             DF_CUDA(cudaMemcpyAsync(h_ob, ob_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
@@ -1036,8 +1105,8 @@ public:
                     box.center[a] = (float)(0.5 * (dw_lo[a] + dw_hi[a]) + dw_disp[a]);
                     box.half_lengths[a] = (float)(0.5 * (dw_hi[a] - dw_lo[a]));
                 }
-                launch_inflow<Real>(ds, dw_sel, nsel, (float)allowed_distance, (float)allowed_density, mass, box, ftab,
-                                    btab, dw_flag, dw_vel, stream);
+                launch_inflow<Real>(ds, dw_sel, nsel, (float)allowed_distance, (float)allowed_density, mass,
+                                    plain_surface(box), ftab, btab, dw_flag, dw_vel, stream);
                 exclusive_scan_u32(dw_flag, dw_rank, nsel, ob_scan, ob_total, stream);
                 DF_CUDA(cudaMemcpyAsync(h_ob, ob_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
                 DF_CUDA(cudaStreamSynchronize(stream));
@@ -1088,7 +1157,7 @@ public:
             const double d = 2.0 * sc.particle_radius;
             const Real mass = (Real)(float)(0.8 * d * d * d * sc.density0);
             launch_inflow<Real>(ds, ob_samples, ob_ns, (float)allowed_distance, (float)allowed_density, mass,
-                                ob_boundary, ftab, btab, ob_flag, ob_vel, stream);
+                                dev_surface(ob_boundary), ftab, btab, ob_flag, ob_vel, stream);
             exclusive_scan_u32(ob_flag, ob_rank, ob_ns, ob_scan, ob_total, stream);
             DF_CUDA(cudaMemcpyAsync(h_ob, ob_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
             DF_CUDA(cudaStreamSynchronize(stream));
@@ -1104,7 +1173,7 @@ public:
         if (outflow && n) {
             uint32_t* alive = sb.keys_a;
             uint32_t* dst = sb.vals_a;
-            launch_outflow_tag<Real>(pos[cur], n, ob_interior, ob_surface, alive, stream);
+            launch_outflow_tag<Real>(pos[cur], n, dev_surface(ob_interior), dev_surface(ob_surface), alive, stream);
             exclusive_scan_u32(alive, dst, n, ob_scan, ob_total, stream);
             DF_CUDA(cudaMemcpyAsync(h_ob, ob_total, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
             DF_CUDA(cudaStreamSynchronize(stream));
@@ -2778,6 +2847,10 @@ int dfsph_open_boundary_apply(dfsph_ctx* ctx, double allowed_distance, double al
                                             added, removed));
 }
 int dfsph_open_boundary_shift(dfsph_ctx* ctx, const float* delta) { DFSPH_DISPATCH(ctx, open_boundary_shift(delta)); }
+int dfsph_set_surface_mesh(dfsph_ctx* ctx, uint32_t mesh_id, const float* vertices, uint32_t n_vertices,
+                           const uint32_t* triangles, uint32_t n_triangles) {
+    DFSPH_DISPATCH(ctx, set_surface_mesh(mesh_id, vertices, n_vertices, triangles, n_triangles));
+}
 int dfsph_dynamic_window_init(dfsph_ctx* ctx, const double* lo, const double* hi, uint32_t wall_first,
                               uint32_t wall_count, const float* rest_xyz, uint32_t n_rest) {
     DFSPH_DISPATCH(ctx, dynamic_window_init(lo, hi, wall_first, wall_count, rest_xyz, n_rest));

@@ -13,6 +13,8 @@
 // written with explicit round-to-nearest operations so that no multiply-add is contracted.
 #include "open_boundary.cuh"
 
+#include <cmath>
+
 namespace dfsph {
 
 namespace {
@@ -66,7 +68,53 @@ __device__ bool star_inside(const dfsph_surface& S, F3 v, float nv) {
     return nv <= d;
 }
 
-__device__ bool surface_inside(const dfsph_surface& S, F3 p) {
+// Moller-Trumbore ray / triangle test as BufferFluidSurface.cu:14-47 evaluates it (RayIntersectsTriangle
+// <true, false>): FP32 throughout, products and sums in the written order, 1/a in FP64; a ray crossing
+// counts when the triangle's plane is not parallel to it (|a| >= 1e-7), the hit lies inside the
+// triangle (u, v >= 0, u <= 1, u + v <= 1) and ahead of the point (t > 0).
+__device__ __forceinline__ F3 cross3(F3 a, F3 b) {
+    return {__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+}
+__device__ __forceinline__ bool ray_hits_triangle_ahead(F3 o, F3 d, F3 v0, F3 v1, F3 v2) {
+    const float eps = 1e-7f;
+    const F3 e1 = sub3(v1, v0), e2 = sub3(v2, v0);
+    const F3 h = cross3(d, e2);
+    const float a = dot3(e1, h);
+    if (a > -eps && a < eps) return false;
+    const float f = (float)__ddiv_rn(1.0, (double)a);
+    const F3 s = sub3(o, v0);
+    const float u = __fmul_rn(f, dot3(s, h));
+    if (u < 0.0f || u > 1.0f) return false;
+    const F3 q = cross3(s, e1);
+    const float v = __fmul_rn(f, dot3(d, q));
+    if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return false;
+    return __fmul_rn(f, dot3(e2, q)) > 0.0f;
+}
+
+// MeshPerso::isInside (BufferFluidSurface.cu:224-270): outside the bounding box (vertices and the
+// origin, translated) a point is outside; inside it, inside when the ray along the fixed direction
+// crosses an odd number of triangles.
+__device__ bool mesh_inside(const DevSurface& S, F3 p) {
+    const float* c = S.s.center;
+    const F3 lo = {__fadd_rn(S.m.bmin[0], c[0]), __fadd_rn(S.m.bmin[1], c[1]), __fadd_rn(S.m.bmin[2], c[2])};
+    const F3 hi = {__fadd_rn(S.m.bmax[0], c[0]), __fadd_rn(S.m.bmax[1], c[1]), __fadd_rn(S.m.bmax[2], c[2])};
+    if (p.x < lo.x || p.y < lo.y || p.z < lo.z || p.x > hi.x || p.y > hi.y || p.z > hi.z) return false;
+    const F3 d = {S.m.dir[0], S.m.dir[1], S.m.dir[2]};
+    const F3 off = {c[0], c[1], c[2]};
+    uint32_t hits = 0;
+    for (uint32_t t = 0; t < S.m.nt; ++t) {
+        const float4 a = S.m.tri[3 * (size_t)t], b = S.m.tri[3 * (size_t)t + 1], e = S.m.tri[3 * (size_t)t + 2];
+        const F3 v0 = {__fadd_rn(a.x, off.x), __fadd_rn(a.y, off.y), __fadd_rn(a.z, off.z)};
+        const F3 v1 = {__fadd_rn(b.x, off.x), __fadd_rn(b.y, off.y), __fadd_rn(b.z, off.z)};
+        const F3 v2 = {__fadd_rn(e.x, off.x), __fadd_rn(e.y, off.y), __fadd_rn(e.z, off.z)};
+        if (ray_hits_triangle_ahead(p, d, v0, v1, v2)) ++hits;
+    }
+    return (hits & 1u) != 0u;
+}
+
+__device__ bool surface_inside(const DevSurface& D, F3 p) {
+    const dfsph_surface& S = D.s;
     bool r = false;
     switch (S.type) {
         case DFSPH_SURFACE_PLANE:
@@ -97,15 +145,19 @@ __device__ bool surface_inside(const dfsph_surface& S, F3 p) {
             else r = star_inside(S, v, nv);
             break;
         }
+        case DFSPH_SURFACE_MESH:
+            r = mesh_inside(D, p);
+            break;
         default:
             break;
     }
     return S.reversed ? !r : r;
 }
 
-// Inward normal: center - p for the round shapes, zero for planes and cuboids
+// Inward normal: center - p for the round shapes, zero for planes, cuboids and meshes
 // (BufferFluidSurface::getNormal).
-__device__ F3 surface_normal(const dfsph_surface& S, F3 p) {
+__device__ F3 surface_normal(const DevSurface& D, F3 p) {
+    const dfsph_surface& S = D.s;
     F3 r = {0.0f, 0.0f, 0.0f};
     if (S.type == DFSPH_SURFACE_CYLINDER || S.type == DFSPH_SURFACE_SPHERE || S.type == DFSPH_SURFACE_STAR)
         r = sub3(f3(S.center), p);
@@ -224,7 +276,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const uint32_t
 // ---- open boundary kernels -----------------------------------------------------------------------
 template <class Real>
 __global__ void __launch_bounds__(kBlock) select_kernel(const float4* __restrict__ samples, uint32_t ns,
-                                                        dfsph_surface interior, dfsph_surface surface,
+                                                        DevSurface interior, DevSurface surface,
                                                         StepParams<Real> p, uint32_t* __restrict__ keep) {
     DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -263,7 +315,7 @@ template <class Real>
 __global__ void __launch_bounds__(kBlock) inflow_kernel(const DevState<Real>* __restrict__ ds,
                                                         const float4* __restrict__ samples, uint32_t ns,
                                                         float allowed_distance, float allowed_density, Real mass,
-                                                        dfsph_surface boundary, const uint2* __restrict__ ftab,
+                                                        DevSurface boundary, const uint2* __restrict__ ftab,
                                                         const uint2* __restrict__ btab, uint32_t* __restrict__ flag,
                                                         float4* __restrict__ vout) {
     DFSPH_PDL_ENTER;
@@ -379,7 +431,7 @@ __global__ void __launch_bounds__(kBlock) append_kernel(const float4* __restrict
 
 template <class Real>
 __global__ void __launch_bounds__(kBlock) outflow_tag_kernel(const Vec4<Real>* __restrict__ pos, uint32_t n,
-                                                             dfsph_surface interior, dfsph_surface surface,
+                                                             DevSurface interior, DevSurface surface,
                                                              uint32_t* __restrict__ alive) {
     DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -457,8 +509,21 @@ void exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t*
     launch_pdl(scan_apply_kernel, tiles, kScanThreads, 0, s, in, n, scratch, out);
 }
 
+void mesh_ray_direction(float dir[3]) {
+    // the constants are doubles rounded to float, as Vector3d(2.575, 6.19763, 5.986) rounds them;
+    // volatile: no contraction, no reassociation
+    volatile float x = (float)2.575, y = (float)6.19763, z = (float)5.986;
+    volatile float xx = x * x, yy = y * y, zz = z * z;
+    volatile float s = xx + yy;
+    s = s + zz;
+    const float nrm = std::sqrt((float)s);
+    dir[0] = x / nrm;
+    dir[1] = y / nrm;
+    dir[2] = z / nrm;
+}
+
 template <class Real>
-void launch_open_boundary_select(const float4* samples, uint32_t ns, dfsph_surface interior, dfsph_surface fluid_surface,
+void launch_open_boundary_select(const float4* samples, uint32_t ns, DevSurface interior, DevSurface fluid_surface,
                                  const StepParams<Real>& p, uint32_t* keep, cudaStream_t s) {
     if (ns) launch_pdl(select_kernel<Real>, grid_for(ns), kBlock, 0, s, samples, ns, interior, fluid_surface, p, keep);
 }
@@ -471,7 +536,7 @@ void launch_shift_samples(float4* samples, uint32_t ns, float dx, float dy, floa
 }
 template <class Real>
 void launch_inflow(const DevState<Real>* d, const float4* samples, uint32_t ns, float allowed_distance,
-                   float allowed_density, Real mass, dfsph_surface boundary, const uint2* fluid_table,
+                   float allowed_density, Real mass, DevSurface boundary, const uint2* fluid_table,
                    const uint2* boundary_table, uint32_t* flag, float4* vel, cudaStream_t s) {
     if (ns)
         launch_pdl(inflow_kernel<Real>, grid_for(ns), kBlock, 0, s, d, samples, ns, allowed_distance, allowed_density, mass,
@@ -486,7 +551,7 @@ void launch_append_inflow(const float4* samples, const float4* svel, const uint3
                                                             kappa, kappaV, id, kappaT, kappaVT);
 }
 template <class Real>
-void launch_outflow_tag(const Vec4<Real>* pos, uint32_t n, dfsph_surface interior, dfsph_surface fluid_surface,
+void launch_outflow_tag(const Vec4<Real>* pos, uint32_t n, DevSurface interior, DevSurface fluid_surface,
                         uint32_t* alive, cudaStream_t s) {
     if (n) launch_pdl(outflow_tag_kernel<Real>, grid_for(n), kBlock, 0, s, pos, n, interior, fluid_surface, alive);
 }
@@ -516,14 +581,14 @@ void launch_renumber_ids(uint32_t* id, uint32_t n, const uint32_t* new_id, cudaS
 }
 
 #define DFSPH_INSTANTIATE_OPEN_BOUNDARY(R)                                                                        \
-    template void launch_open_boundary_select<R>(const float4*, uint32_t, dfsph_surface, dfsph_surface,           \
+    template void launch_open_boundary_select<R>(const float4*, uint32_t, DevSurface, DevSurface,           \
                                                  const StepParams<R>&, uint32_t*, cudaStream_t);                  \
-    template void launch_inflow<R>(const DevState<R>*, const float4*, uint32_t, float, float, R, dfsph_surface,   \
+    template void launch_inflow<R>(const DevState<R>*, const float4*, uint32_t, float, float, R, DevSurface,   \
                                    const uint2*, const uint2*, uint32_t*, float4*, cudaStream_t);                 \
     template void launch_append_inflow<R>(const float4*, const float4*, const uint32_t*, const uint32_t*,         \
                                           uint32_t, uint32_t, uint32_t, R, Vec4<R>*, Vec4<R>*, R*, R*, uint32_t*, \
                                           R*, R*, cudaStream_t);                                                  \
-    template void launch_outflow_tag<R>(const Vec4<R>*, uint32_t, dfsph_surface, dfsph_surface, uint32_t*,        \
+    template void launch_outflow_tag<R>(const Vec4<R>*, uint32_t, DevSurface, DevSurface, uint32_t*,        \
                                         cudaStream_t);                                                            \
     template void launch_compact_fluid<R>(const uint32_t*, const uint32_t*, uint32_t, const Vec4<R>*,             \
                                           const Vec4<R>*, const R*, const R*, const uint32_t*, const R*, const R*, \

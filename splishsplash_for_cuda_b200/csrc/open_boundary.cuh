@@ -6,6 +6,28 @@
 
 namespace dfsph {
 
+// A surface as the kernels see it: the C ABI's description and, for DFSPH_SURFACE_MESH, the mesh
+// registered under its id (`points`) in device memory. The mesh is translated by the surface's
+// `center` (the reference's MeshPerso offset).
+struct SurfaceMesh {
+    const float4* tri = nullptr;  // 3 per triangle: vertices 0, 1, 2 (w unused), untranslated
+    uint32_t nt = 0;
+    float bmin[3] = {0.f, 0.f, 0.f}, bmax[3] = {0.f, 0.f, 0.f};  // box of the vertices and the origin
+    float dir[3] = {0.f, 0.f, 0.f};                              // the ray's direction (unit)
+};
+struct DevSurface {
+    dfsph_surface s;
+    SurfaceMesh m;
+};
+inline DevSurface plain_surface(const dfsph_surface& s) {
+    DevSurface d;
+    d.s = s;
+    return d;
+}
+// The ray direction of the mesh inside test, normalise((2.575, 6.19763, 5.986)) in FP32 with each
+// operation rounded (BufferFluidSurface.cu:242-243).
+void mesh_ray_direction(float dir[3]);
+
 // Scratch words of exclusive_scan_u32 for n inputs.
 inline size_t scan_scratch_words(uint32_t n) { return (size_t)(n / 4096u) + 2u; }
 
@@ -17,7 +39,7 @@ void exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t*
 // keep[i] = 1 for samples outside `interior` and inside `fluid_surface` whose cell lies in the grid
 // (OpenBoundariesSimple::init, OpenBoundariesSimple.cu:283-318).
 template <class Real>
-void launch_open_boundary_select(const float4* samples, uint32_t ns, dfsph_surface interior, dfsph_surface fluid_surface,
+void launch_open_boundary_select(const float4* samples, uint32_t ns, DevSurface interior, DevSurface fluid_surface,
                                  const StepParams<Real>& p, uint32_t* keep, cudaStream_t s);
 
 // Compacts samples[i] with keep[i] to out[rank[i]].
@@ -33,7 +55,7 @@ void launch_shift_samples(float4* samples, uint32_t ns, float dx, float dy, floa
 // density estimate is at most allowed_density and the velocity does not point out of `boundary`.
 template <class Real>
 void launch_inflow(const DevState<Real>* d, const float4* samples, uint32_t ns, float allowed_distance,
-                   float allowed_density, Real mass, dfsph_surface boundary, const uint2* fluid_table,
+                   float allowed_density, Real mass, DevSurface boundary, const uint2* fluid_table,
                    const uint2* boundary_table, uint32_t* flag, float4* vel, cudaStream_t s);
 
 // Appends the flagged samples at n + rank (ranks past capacity are dropped): position, velocity,
@@ -46,7 +68,7 @@ void launch_append_inflow(const float4* samples, const float4* svel, const uint3
 // alive[i] = 0 for particles outside `interior` and outside `fluid_surface` (outflow_basic_kernel,
 // OpenBoundariesSimple.cu:475-492), 1 otherwise.
 template <class Real>
-void launch_outflow_tag(const Vec4<Real>* pos, uint32_t n, dfsph_surface interior, dfsph_surface fluid_surface,
+void launch_outflow_tag(const Vec4<Real>* pos, uint32_t n, DevSurface interior, DevSurface fluid_surface,
                         uint32_t* alive, cudaStream_t s);
 
 // Stable compaction of the fluid state (cur -> nxt) keeping the particles with alive[i], and the

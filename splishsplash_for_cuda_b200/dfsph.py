@@ -366,6 +366,14 @@ class DFSPHCUDA:
         self._call(self._lib.dfsph_open_boundary_samples(self._ctx, _fptr(x), cnt.value, C.byref(cnt)))
         return x
 
+    def set_surface_mesh(self, mesh_id: int, vertices, triangles) -> None:
+        """Registers the triangle mesh mesh_id for open-boundary surfaces of type mesh
+        (open_boundary.mesh): vertices (V, 3), triangles (T, 3) vertex indices."""
+        v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        self._call(self._lib.dfsph_set_surface_mesh(self._ctx, int(mesh_id), v.ctypes.data_as(C.c_void_p), v.shape[0],
+                                                    t.ctypes.data_as(C.c_void_p), t.shape[0]))
+
     def shift_open_boundary(self, delta) -> None:
         """Moves the open boundary's surfaces and samples (dynamic-window displacement)."""
         d = np.ascontiguousarray(delta, dtype=np.float32).reshape(3)

@@ -11,7 +11,8 @@ from pathlib import Path
 
 import numpy as np
 
-from ._capi import (SURFACE_CUBOID, SURFACE_CYLINDER, SURFACE_PLANE, SURFACE_SPHERE, SURFACE_STAR, Surface)
+from ._capi import (MAX_SURFACE_MESHES, SURFACE_CUBOID, SURFACE_CYLINDER, SURFACE_MESH, SURFACE_PLANE, SURFACE_SPHERE,
+                    SURFACE_STAR, Surface)
 
 
 def _v3(dst, v) -> None:
@@ -62,6 +63,46 @@ def star(center, half_height: float, radius: float, radius_internal: float, poin
     _v3(s.half_lengths, (0.0, half_height, 0.0))
     _v3(s.direction, direction)
     return s
+
+
+def mesh(mesh_id: int = 0, offset=(0.0, 0.0, 0.0), reversed: bool = False) -> Surface:
+    """The closed triangle mesh registered under mesh_id (DFSPHCUDA.set_surface_mesh), translated by
+    offset (MeshPerso with its offset): inside = an odd number of crossings of the fixed ray with its
+    triangles."""
+    if not 0 <= mesh_id < MAX_SURFACE_MESHES:
+        raise ValueError(f"mesh id must be in [0, {MAX_SURFACE_MESHES})")
+    s = Surface(type=SURFACE_MESH, reversed=int(reversed), points=int(mesh_id))
+    _v3(s.center, offset)
+    return s
+
+
+def read_obj(path, lib_path=None) -> tuple[np.ndarray, np.ndarray]:
+    """(vertices (V, 3) float32, triangles (T, 3) uint32) of a Wavefront OBJ file, read by the
+    library's dfsph_read_obj (no GPU needed): faces split into fans, other records skipped."""
+    import ctypes as C
+
+    from . import _capi
+
+    lib = _capi.load(lib_path)
+    nv, nt = C.c_uint32(), C.c_uint32()
+    p = str(path).encode()
+    _capi.check(lib, None, lib.dfsph_read_obj(p, None, 0, C.byref(nv), None, 0, C.byref(nt)))
+    v = np.zeros((nv.value, 3), np.float32)
+    t = np.zeros((nt.value, 3), np.uint32)
+    _capi.check(lib, None, lib.dfsph_read_obj(p, v.ctypes.data_as(C.c_void_p), nv.value, C.byref(nv),
+                                              t.ctypes.data_as(C.c_void_p), nt.value, C.byref(nt)))
+    return v, t
+
+
+def box_mesh(lo, hi) -> tuple[np.ndarray, np.ndarray]:
+    """(vertices, triangles) of the closed axis-aligned box [lo, hi]: 8 vertices, 12 triangles with
+    outward normals."""
+    lo, hi = np.asarray(lo, np.float32), np.asarray(hi, np.float32)
+    v = np.array([[lo[0] if i & 1 == 0 else hi[0], lo[1] if i & 2 == 0 else hi[1], lo[2] if i & 4 == 0 else hi[2]]
+                  for i in range(8)], np.float32)
+    quads = [(0, 2, 3, 1), (4, 5, 7, 6), (0, 1, 5, 4), (2, 6, 7, 3), (0, 4, 6, 2), (1, 3, 7, 5)]
+    t = np.array([tri for a, b, c, d in quads for tri in ((a, b, c), (a, c, d))], np.uint32)
+    return v, t
 
 
 def _f32(x) -> float:

@@ -20,6 +20,7 @@ from test_open_boundary import R, tank_samples, tank_scene, tank_surfaces
 
 pytestmark = pytest.mark.gpu
 GOLD = Path(__file__).resolve().parent / "golden" / "open_boundary" / "surfaces.npz"
+MESH_GOLD = Path(__file__).resolve().parent / "golden" / "open_boundary" / "meshes.npz"
 
 
 def check(name, a, b, tol):
@@ -53,6 +54,72 @@ def test_device_surfaces_match_reference(cuda_lib):
         if not (got.shape == exp.shape and np.array_equal(got, exp)):
             mism.append((k, int(s.type), got.shape[0], exp.shape[0]))
     assert not mism, mism
+
+
+def test_device_mesh_surfaces_match_reference(cuda_lib):
+    """Mesh surfaces (type 3) on the device: the samples kept outside each fixture mesh equal the
+    reference's MeshPerso::isInside answers (fixture made from its own RayIntersectsTriangle)."""
+    z = np.load(MESH_GOLD)
+    cfg = Configuration()
+    cfg.particleRadius = 0.05
+    corners = np.array([[x, y, z_] for x in (-4.5, 4.5) for y in (-4.5, 4.5) for z_ in (-4.5, 4.5)], np.float32)
+    d = DFSPHCUDA(Scene(config=cfg, fluid=np.zeros((1, 3), np.float32), boundary=corners))
+    everything = ob.plane((0.0, -100.0, 0.0), (0.0, 1.0, 0.0))
+    for k in range(int(z["cases"])):
+        d.set_surface_mesh(k % _capi.MAX_SURFACE_MESHES, z[f"v{k}"], z[f"t{k}"])
+        pts = z[f"p{k}"]
+        d.init_open_boundary(everything, ob.mesh(k % _capi.MAX_SURFACE_MESHES, offset=z[f"off{k}"]), everything, pts)
+        assert np.array_equal(d.open_boundary_samples(), pts[~z[f"in{k}"].astype(bool)]), k
+
+
+def test_mesh_surfaces_in_the_open_boundary(cuda_lib):
+    """The tank's open boundary with box meshes in place of its cuboids runs exactly as with the
+    cuboids (kept samples, added / removed particles, the state after three steps); with a non-convex
+    interior (an L-shaped prism) and a shift, the device matches the oracle."""
+    s = tank_scene(vx=0.3)
+    b, i, f = tank_surfaces()
+    runs = []
+    for meshes in (False, True):
+        d = DFSPHCUDA(s, fluid_capacity=2 * s.n_fluid)
+        d.step()
+        if meshes:
+            d.set_surface_mesh(0, *ob.box_mesh((0.0, 0.0, 0.0), (1.0, 1.0, 0.5)))
+            d.set_surface_mesh(1, *ob.box_mesh((0.075, 0.075, 0.075), (0.925, 0.925, 0.425)))
+            kept = d.init_open_boundary(ob.mesh(0), ob.mesh(1), f, tank_samples())
+        else:
+            kept = d.init_open_boundary(b, i, f, tank_samples())
+        added = d.apply_open_boundary(1.75 * R, 700.0)
+        for _ in range(3):
+            d.step()
+        runs.append((kept, added, d.open_boundary_samples(), d.positions(), d.velocities()))
+    assert runs[0][0] == runs[1][0] and runs[0][1] == runs[1][1] and runs[0][1][0] > 0
+    for a, c in zip(runs[0][2:], runs[1][2:]):
+        assert np.array_equal(a, c)
+    # non-convex interior: the tank without the L-shaped prism over x, y in [0.1, 0.9], z in [0.1, 0.4]
+    outline = np.array([(0.1, 0.1), (0.9, 0.1), (0.9, 0.5), (0.5, 0.5), (0.5, 0.9), (0.1, 0.9)], np.float32)
+    n = len(outline)
+    v = np.concatenate([np.c_[outline, np.full(n, 0.1)], np.c_[outline, np.full(n, 0.4)]]).astype(np.float32)
+    t = []
+    for a_, b_, c_ in [(0, 1, 2), (0, 2, 3), (0, 3, 5), (3, 4, 5)]:
+        t += [(a_, c_, b_), (a_ + n, b_ + n, c_ + n)]
+    for k in range(n):
+        j = (k + 1) % n
+        t += [(k, j, j + n), (k, j + n, k + n)]
+    t = np.array(t, np.uint32)
+    from oracle.oracle import set_surface_mesh
+    set_surface_mesh(2, v, t)
+    d = DFSPHCUDA(s, fluid_capacity=2 * s.n_fluid)
+    d.set_surface_mesh(2, v, t)
+    o = Oracle(s, 64)
+    interior = ob.mesh(2)
+    assert d.init_open_boundary(b, interior, f, tank_samples()) == o.open_boundary_init(b, interior, f, tank_samples())
+    delta = np.array([0.02, 0.0, -0.01], np.float32)
+    d.shift_open_boundary(delta)
+    o.open_boundary_shift(delta)
+    ad, rd = d.apply_open_boundary(1.75 * R, 700.0)
+    ao, ro, _ = o.open_boundary_apply(1.75 * R, 700.0)
+    assert (ad, rd) == (ao, ro) and ad > 0 and rd > 0
+    assert np.array_equal(d.positions(), o.field("position").astype(np.float32))
 
 
 @pytest.mark.parametrize("precision", [32, 64])
@@ -181,10 +248,16 @@ def test_errors(cuda_lib):
     assert e.value.code == _capi.DFSPH_E_STATE
     b, i, f = tank_surfaces()
     bad = _capi.Surface.from_buffer_copy(bytes(b))
-    bad.type = 3  # the mesh shape is not offered
+    bad.type = 3  # a mesh id with no mesh registered
     with pytest.raises(_capi.DfsphError) as e:
         d.init_open_boundary(bad, i, f, tank_samples())
     assert e.value.code == _capi.DFSPH_E_INVALID
+    for args in [(_capi.MAX_SURFACE_MESHES, *ob.box_mesh((0, 0, 0), (1, 1, 1))),
+                 (0, np.zeros((3, 3), np.float32), np.array([[0, 1, 3]], np.uint32)),
+                 (0, np.zeros((3, 3), np.float32), np.zeros((0, 3), np.uint32))]:
+        with pytest.raises(_capi.DfsphError) as e:
+            d.set_surface_mesh(*args)
+        assert e.value.code == _capi.DFSPH_E_INVALID
     d.init_open_boundary(b, i, f, tank_samples())
     with pytest.raises(_capi.DfsphError) as e:
         d.apply_open_boundary(allowed_distance=0.0)

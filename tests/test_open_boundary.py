@@ -10,11 +10,12 @@ import numpy as np
 import pytest
 
 from oracle import Oracle
-from oracle.oracle import OracleSurface, surface_eval
+from oracle.oracle import OracleSurface, set_surface_mesh, surface_eval
 from splishsplash_for_cuda_b200 import open_boundary as ob
 from splishsplash_for_cuda_b200.scene import Configuration, Scene, box_wall, lattice_block
 
 GOLD = Path(__file__).resolve().parent / "golden" / "open_boundary" / "surfaces.npz"
+MESH_GOLD = Path(__file__).resolve().parent / "golden" / "open_boundary" / "meshes.npz"
 PIN = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "libsurface_pin.so"
 
 
@@ -42,6 +43,80 @@ def test_oracle_surfaces_match_reference_live():
         assert lib.pin_surface_eval(C.addressof(s), p.ctypes.data, p.shape[0], ins.ctypes.data, nrm.ctypes.data) == 0
         oi, on = surface_eval(s, p)
         assert np.array_equal(oi, ins.astype(bool)) and np.array_equal(on, nrm)
+
+
+def test_oracle_mesh_surfaces_match_reference_fixture():
+    """Type-3 (mesh) surfaces: the oracle's isinside against MeshPerso::isInside run on the reference's
+    own RayIntersectsTriangle (fixture: an L-shaped prism, a box and an octahedron, two offsets each,
+    random points and lattice points on planes through vertices), bit for bit; reversed flips it."""
+    z = np.load(MESH_GOLD)
+    for k in range(int(z["cases"])):
+        set_surface_mesh(3, z[f"v{k}"], z[f"t{k}"])
+        inside, normal = surface_eval(ob.mesh(3, offset=z[f"off{k}"]), z[f"p{k}"])
+        assert np.array_equal(inside, z[f"in{k}"].astype(bool)), k
+        assert not normal.any()
+        rev, _ = surface_eval(ob.mesh(3, offset=z[f"off{k}"], reversed=True), z[f"p{k}"])
+        assert np.array_equal(rev, ~z[f"in{k}"].astype(bool)), k
+
+
+@pytest.mark.skipif(not PIN.exists(), reason="BufferFluidSurface compiled from the reference sources is not present")
+def test_oracle_mesh_surfaces_match_reference_live():
+    lib = C.CDLL(str(PIN))
+    lib.pin_mesh_inside.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                    C.c_uint32, C.c_void_p]
+    z = np.load(MESH_GOLD)
+    rng = np.random.default_rng(31)
+    for k in range(int(z["cases"])):
+        v, t = z[f"v{k}"], z[f"t{k}"]
+        off = rng.uniform(-0.3, 0.3, size=3).astype(np.float32)
+        p = rng.uniform(-0.5, 3.0, size=(4000, 3)).astype(np.float32)
+        ins = np.zeros(p.shape[0], np.uint8)
+        assert lib.pin_mesh_inside(v.ctypes.data, v.shape[0], t.ctypes.data, t.shape[0], off.ctypes.data,
+                                   p.ctypes.data, p.shape[0], ins.ctypes.data) == 0
+        set_surface_mesh(4, v, t)
+        got, _ = surface_eval(ob.mesh(4, offset=off), p)
+        assert np.array_equal(got, ins.astype(bool)), k
+
+
+def test_box_mesh_equals_cuboid():
+    lo, hi = np.array([0.1, -0.2, 0.3]), np.array([0.9, 0.6, 1.4])
+    set_surface_mesh(5, *ob.box_mesh(lo, hi))
+    rng = np.random.default_rng(2)
+    p = rng.uniform(-0.5, 2.0, size=(20000, 3)).astype(np.float32)
+    c = 0.5 * (lo + hi)
+    gap = np.min(np.abs(np.abs(p - c) - 0.5 * (hi - lo)), axis=1)
+    p = p[gap > 1e-4]  # not on a face
+    a, _ = surface_eval(ob.mesh(5), p)
+    b, _ = surface_eval(ob.cuboid(c, 0.5 * (hi - lo)), p)
+    assert np.array_equal(a, b) and a.sum() > 500
+
+
+def test_read_obj(tmp_path):
+    """The library's OBJ reader (no GPU): quads split into two triangles, negative and v/t/n
+    references, other records skipped; bad references are errors."""
+    from splishsplash_for_cuda_b200 import _capi
+
+    f = tmp_path / "m.obj"
+    f.write_text("# box face and a triangle\no thing\nv 0 0 0\nv 1 0 0\nvt 0 0\nv 1 1 0\nv 0 1 0\n"
+                 "vn 0 0 1\nf 1/1/1 2/1/1 3/1/1 4/1/1\nv 0.5 0.5 1\nf -1 1//1 2\ns off\n")
+    v, t = ob.read_obj(f)
+    assert v.shape == (5, 3) and v.dtype == np.float32
+    assert np.array_equal(v[4], np.float32([0.5, 0.5, 1.0]))
+    assert t.tolist() == [[0, 1, 2], [0, 2, 3], [4, 0, 1]]
+    bad = tmp_path / "bad.obj"
+    bad.write_text("v 0 0 0\nv 1 0 0\nf 1 2 3\n")
+    with pytest.raises(_capi.DfsphError):
+        ob.read_obj(bad)
+    v2, t2 = ob.read_obj(_write_box_obj(tmp_path / "box.obj"))
+    a, b = ob.box_mesh((0, 0, 0), (1, 2, 3))
+    assert np.array_equal(v2, a) and np.array_equal(t2, b)
+
+
+def _write_box_obj(path):
+    v, t = ob.box_mesh((0, 0, 0), (1, 2, 3))
+    lines = [f"v {x:.9g} {y:.9g} {z:.9g}" for x, y, z in v] + [f"f {a + 1} {b + 1} {c + 1}" for a, b, c in t]
+    path.write_text("\n".join(lines) + "\n")
+    return path
 
 
 def test_presets():
