@@ -190,8 +190,11 @@ int dfsph_move_boundary_rigid(dfsph_ctx* ctx, uint32_t first, uint32_t count, co
 
 /* Fluid particles (fluid_data->reset<FluidModel>). vxyz may be null (zero velocity). mass may be
  * null: every particle then gets the reference default mass 0.8 * rho0 * (2r)^3
- * (FluidModel::initMasses, FluidModel.cpp:94-107). Resets kappa, kappa_v and the dt history
- * (h = h_future = h_past = time_step, h_ratio = 1) and assigns ids 0..n-1 in upload order. */
+ * (FluidModel::initMasses, FluidModel.cpp:94-107). Particles that the open boundary or the dynamic
+ * window add later get the first uploaded particle's mass (the reference gives them fluid->mass[0],
+ * OpenBoundariesSimple.cu:457); parameter "inflow_mass" reads or overrides it. Resets kappa,
+ * kappa_v and the dt history (h = h_future = h_past = time_step, h_ratio = 1) and assigns ids
+ * 0..n-1 in upload order. */
 int dfsph_upload_fluid(dfsph_ctx* ctx, const float* xyz, const float* vxyz, const float* mass, uint32_t n);
 
 /* Overwrites positions and velocities of the current n particles (given in id order) but keeps
@@ -259,7 +262,9 @@ int dfsph_on_step_end(dfsph_ctx* ctx);                                    /* onS
  * "escaped_removed" (read-only: particles removed that way so far),
  * "boundary_forces" (1: accumulate the fluid's force on every boundary particle in each Jacobi pass,
  * -m_i k_i psi_b grad W_ib summed over both solves of a step, as the reference does for dynamic
- * bodies; cleared by each neighbour search; atomics, so the summation order varies),
+ * bodies; cleared by each neighbour search; summed with 64-bit fixed-point atomics in units of
+ * 2^-32 N, so the sums do not depend on the order), "inflow_mass" (the mass of particles the open
+ * boundary and the dynamic window add; default: the first uploaded particle's),
  * "sort_withhold_tile" (failure-detection tests: the fluid sort's tile with this id never publishes
  * its look-back flags, so the bounded waits of the tiles after it run out, about a second, and the
  * step reports DFSPH_ST_SORT_TIMEOUT with an unspecified particle order; -1 turns it off).
@@ -465,8 +470,8 @@ int dfsph_body_wrench(dfsph_ctx* ctx, uint32_t n_bodies, const uint32_t* first, 
  * kappa and kappa_v, the boundary with psi, the dt history, the grid, the scene parameters and, when
  * the learned warm start is on, its totals, network weights, Adam state, scales and cost-gate
  * schedule. Loading into a context created with at least the same capacities, the same
- * neighbor_capacity and precision resumes bit-identically. Files of format version 1 (no gate
- * schedule) still load. */
+ * neighbor_capacity and precision resumes bit-identically. Files of format versions 1 to 3 (no
+ * gate schedule, no network-usefulness state, no inflow mass) still load. */
 int dfsph_checkpoint_save(dfsph_ctx* ctx, const char* path);
 int dfsph_checkpoint_load(dfsph_ctx* ctx, const char* path);
 

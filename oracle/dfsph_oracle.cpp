@@ -400,14 +400,15 @@ template <class Real> struct Oracle {
         for (size_t k = 0; k < ob_x.size(); ++k) ob_x[k] += d[k % 3];
     }
 
+    float inflow_mass = 0.0f;  // mass of the particles the inflow adds: the first uploaded particle's
+
     // applyOpenBoundary: inflow decisions against the current fluid (all of them, in sample order),
     // then the outflow over every particle, new ones included.
     void ob_apply(double allowed_distance, double allowed_density, bool inflow, bool outflow, uint32_t capacity,
                   uint32_t& added, uint32_t& removed, bool& clipped) {
         added = removed = 0;
         clipped = false;
-        const double d2r = 2.0 * prm.particle_radius;
-        const Real mass = (Real)(float)(0.8 * d2r * d2r * d2r * prm.density0);
+        const Real mass = (Real)inflow_mass;
         if (inflow && !ob_x.empty()) {
             const std::vector<float> fp = fpos(), fb = fbpos();
             const Buckets bf = bucket(fp, n), bbk = bucket(fb, nb);
@@ -1005,6 +1006,7 @@ template <class O> void set_fluid(O& o, const float* xyz, const float* vxyz, con
         o.v[k] = vxyz ? (Real)vxyz[k] : Real(0);
     }
     for (uint32_t i = 0; i < n; ++i) o.m[i] = (Real)(mass ? mass[i] : default_mass);
+    o.inflow_mass = (n && mass) ? mass[0] : default_mass;  // the new particles' mass (fluid->mass[0])
     for (auto* vec : {&o.rho, &o.alpha, &o.dadv, &o.kap, &o.kapv, &o.kc}) vec->assign(n, 0);
     o.a.assign(3 * (size_t)n, 0);
     o.nf.assign(n, {});

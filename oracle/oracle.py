@@ -163,7 +163,9 @@ class Oracle:
         v = None if scene.fluid_velocity is None else np.ascontiguousarray(scene.fluid_velocity, dtype=np.float32)
         self.n = x.shape[0]
         self.nb = b.shape[0]
-        self.lib.oracle_set_fluid(self.h, _f(x), _f(v), None, self.n)
+        m = getattr(scene, "fluid_mass", None)
+        self._keep_m = None if m is None else np.ascontiguousarray(m, dtype=np.float32)
+        self.lib.oracle_set_fluid(self.h, _f(x), _f(v), _f(self._keep_m), self.n)
 
     def close(self):
         if self.h:

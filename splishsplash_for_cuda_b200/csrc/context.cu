@@ -75,6 +75,14 @@ public:
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_vel_ready = nullptr, ev_vel_free = nullptr;
     bool pending_vel = false;
+    // Mass of the particles the open boundary and the dynamic window add: the first uploaded
+    // particle's (the reference gives new particles fluid->mass[0], OpenBoundariesSimple.cu:457).
+    float inflow_mass = 0.0f;
+    float new_particle_mass() const {
+        if (inflow_mass > 0.0f) return inflow_mass;
+        const double d = 2.0 * sc.particle_radius;  // nothing uploaded yet: FluidModel's default
+        return (float)(0.8 * d * d * d * sc.density0);
+    }
     uint32_t Nc = 0, Bc = 0, cap = 0, stride = 0;
     uint32_t n = 0, nb = 0;
     int cur = 0;
@@ -646,6 +654,10 @@ public:
         n = count;
         cur = 0;
         last_lp = false;  // the uploaded state carries no learned warm start
+        {
+            const double d = 2.0 * sc.particle_radius;
+            inflow_mass = (count && mass) ? mass[0] : (float)(0.8 * d * d * d * sc.density0);
+        }
         if (count) {
             float* sx = stage;
             float* sv = stage + (size_t)count * 3;
@@ -1097,8 +1109,7 @@ public:
             launches += 5;
             if (nsel) {
                 DF_TRY(bin_fluid());
-                const double dd = 2.0 * sc.particle_radius;
-                const Real mass = (Real)(float)(0.8 * dd * dd * dd * sc.density0);
+                const Real mass = (Real)new_particle_mass();
                 dfsph_surface box{};
                 box.type = DFSPH_SURFACE_CUBOID;
                 for (int a = 0; a < 3; ++a) {
@@ -1154,8 +1165,7 @@ public:
         const uint32_t n0 = n;
         if (inflow && ob_ns) {
             DF_TRY(bin_fluid());
-            const double d = 2.0 * sc.particle_radius;
-            const Real mass = (Real)(float)(0.8 * d * d * d * sc.density0);
+            const Real mass = (Real)new_particle_mass();
             launch_inflow<Real>(ds, ob_samples, ob_ns, (float)allowed_distance, (float)allowed_density, mass,
                                 dev_surface(ob_boundary), ftab, btab, ob_flag, ob_vel, stream);
             exclusive_scan_u32(ob_flag, ob_rank, ob_ns, ob_scan, ob_total, stream);
@@ -2060,7 +2070,7 @@ public:
         std::ofstream f(path, std::ios::binary | std::ios::trunc);
         DF_CHECK(f.is_open(), DFSPH_E_INVALID, std::string("cannot open ") + path);
         f.write(kCkptMagic, 8);
-        put(f, (int32_t)3);
+        put(f, (int32_t)4);
         put(f, (int32_t)sizeof(Real));
         put(f, n);
         put(f, nb);
@@ -2104,6 +2114,7 @@ public:
             put(f, (int32_t)(last_lp ? 1 : 0));
             for (double v : {useful_ratio, zero_loss, heldout_loss}) put(f, v);
         }
+        put(f, inflow_mass);  // version 4
         DF_CHECK(f.good(), DFSPH_E_INVALID, std::string("write failed: ") + path);
         return DFSPH_OK;
     }
@@ -2118,7 +2129,7 @@ public:
         int32_t version = 0, rbytes = 0;
         uint32_t cn = 0, cnb = 0;
         dfsph_scene csc{};
-        DF_CHECK(get(f, version) && version >= 1 && version <= 3 && get(f, rbytes) && get(f, cn) && get(f, cnb) &&
+        DF_CHECK(get(f, version) && version >= 1 && version <= 4 && get(f, rbytes) && get(f, cn) && get(f, cnb) &&
                      get(f, csc),
                  DFSPH_E_INVALID, "bad checkpoint header");
         DF_CHECK(rbytes == (int32_t)sizeof(Real), DFSPH_E_INVALID, "checkpoint precision differs from the context's");
@@ -2231,6 +2242,12 @@ public:
             launches += 1;
         } else if (learned) {
             DF_TRY(enable_learned(false));
+        }
+        if (version >= 4) {
+            DF_CHECK(get(f, inflow_mass), DFSPH_E_INVALID, "truncated checkpoint");
+        } else {  // earlier files: the default mass
+            const double d = 2.0 * sc.particle_radius;
+            inflow_mass = (float)(0.8 * d * d * d * sc.density0);
         }
         h = dt[0]; h_future = dt[1]; h_past = dt[2]; inv_h = dt[3]; inv_h_future = dt[4];
         h_ratio = dt[5]; h_ratio2 = dt[6]; time_step = dt[7];
@@ -2413,6 +2430,10 @@ public:
         }
         else if (k == "sort_withhold_tile") sort_withheld_tile = v < 0 ? kNoWithheldTile : (uint32_t)v;
         else if (k == "remove_escaped") remove_escaped = v != 0;
+        else if (k == "inflow_mass") {
+            DF_CHECK(v > 0 && std::isfinite(v), DFSPH_E_INVALID, "inflow_mass must be positive");
+            inflow_mass = (float)v;
+        }
         else if (k == "boundary_forces") {
             if (v != 0 && !bforce) {
                 DF_TRY(dalloc(&bforce, (size_t)Bc * 4));
@@ -2514,6 +2535,7 @@ public:
         }
         else if (k == "boundary_forces") *v = boundary_forces ? 1 : 0;
         else if (k == "remove_escaped") *v = remove_escaped ? 1 : 0;
+        else if (k == "inflow_mass") *v = new_particle_mass();
         else if (k == "escaped_removed") *v = (double)escaped_removed;
         else if (k == "warm_start_damping") *v = damping;
         else if (k == "learned_gate") *v = gate ? 1 : 0;

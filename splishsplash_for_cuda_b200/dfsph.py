@@ -158,7 +158,8 @@ class DFSPHCUDA:
         x = np.ascontiguousarray(self.scene.fluid, dtype=np.float32)
         v = None if self.scene.fluid_velocity is None else np.ascontiguousarray(self.scene.fluid_velocity,
                                                                                  dtype=np.float32)
-        self._call(self._lib.dfsph_upload_fluid(self._ctx, _fptr(x), _fptr(v), None, x.shape[0]))
+        m = None if self.scene.fluid_mass is None else np.ascontiguousarray(self.scene.fluid_mass, dtype=np.float32)
+        self._call(self._lib.dfsph_upload_fluid(self._ctx, _fptr(x), _fptr(v), _fptr(m), x.shape[0]))
         self.m_iterations = 0
         self.m_iterationsV = 0
 

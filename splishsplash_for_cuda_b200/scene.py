@@ -155,6 +155,7 @@ class Scene:
     box_min: tuple | None = None
     box_max: tuple | None = None
     meta: dict = field(default_factory=dict)
+    fluid_mass: np.ndarray | None = None  # (N,) float32; None: FluidModel's default 0.8 rho0 (2r)^3
 
     @property
     def n_fluid(self) -> int:

@@ -201,6 +201,28 @@ def test_learned_mode_matches_plain_through_open_boundary(cuda_lib):
     assert np.array_equal(runs[0][0], runs[1][0]) and np.array_equal(runs[0][1], runs[1][1])
 
 
+def test_inflow_mass_follows_the_fluid(cuda_lib):
+    """With masses given at upload, the particles the inflow adds get the first uploaded particle's
+    mass (the reference gives them fluid->mass[0]), on the device as in the oracle; "inflow_mass"
+    reads and overrides it."""
+    s = tank_scene(vx=0.3)
+    m0 = np.float32(1000.0 * (2 * R) ** 3)
+    s.fluid_mass = np.full(s.n_fluid, m0, np.float32)
+    b, i, f = tank_surfaces()
+    d = DFSPHCUDA(s, fluid_capacity=2 * s.n_fluid)
+    o = Oracle(s, 64)
+    assert d.get_param("inflow_mass") == pytest.approx(float(m0), rel=1e-7)
+    d.init_open_boundary(b, i, f, tank_samples())
+    o.open_boundary_init(b, i, f, tank_samples())
+    ad, rd = d.apply_open_boundary(1.75 * R, 700.0)
+    ao, ro, _ = o.open_boundary_apply(1.75 * R, 700.0)
+    assert (ad, rd) == (ao, ro) and ad > 0
+    assert np.array_equal(d.field("mass", np.float64), o.field("mass"))
+    assert np.all(d.field("mass") == m0)
+    d.set_param("inflow_mass", 0.5 * float(m0))
+    assert d.get_param("inflow_mass") == pytest.approx(0.5 * float(m0), rel=1e-7)
+
+
 def test_capacity_cut_and_status(cuda_lib):
     s = tank_scene()
     d = DFSPHCUDA(s, fluid_capacity=s.n_fluid + 5)

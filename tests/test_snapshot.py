@@ -116,8 +116,10 @@ def test_checkpoint_resume_bit_identical(cuda_lib, tmp_path, mode):
     a.checkpoint_save(path)
     sa = [a.step() for _ in range(10)]
     b = DFSPHCUDA(s)
+    b.set_param("inflow_mass", 1.0)  # replaced by the checkpoint's (format version 4)
     b.step()  # the resumed context's own counters differ from the saved run's
     b.checkpoint_load(path)
+    assert b.get_param("inflow_mass") == a.get_param("inflow_mass")
     sb = [b.step() for _ in range(10)]
     if mode == "gated":
         for key in ("gate_learned_steps", "gate_plain_steps", "gate_last_excess"):
