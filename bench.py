@@ -134,20 +134,25 @@ def make_scene(config: int):
 # scalars, 4-byte neighbour indices, one packed 4-byte count word). Each particle's own data is
 # counted once per launch, neighbour data is other particles' own data (perfect reuse), and every
 # stored neighbour costs its 4-byte index. nf / nb are the mean fluid / boundary neighbour counts.
-def kernel_bytes(name: str, n: int, nb_particles: int, nf: float, nb: float) -> float:
+def kernel_bytes(name: str, n: int, nb_particles: int, nf: float, nb: float, real: int = 4) -> float:
+    """Algorithmic bytes of one launch: every per-particle array read or written once, the neighbour
+    lists once, the boundary positions once. real = 4 (FP32 build) or 8 (FP64 build): a position,
+    velocity or acceleration record is 4 reals, a scalar field one real; counts and list entries
+    are 4 bytes."""
     nn = nf + nb
+    v, r = 4 * real, real
     per = {
-        "density_alpha": 16 + 16 + 4 + 4 + 4 + 4 + 4 + 4 + 4 * nn,      # pos, vel, counts, kv r/w, rho, alpha, dadv
-        "divergence_jacobi": 16 + 4 + 4 + 4 + 4 + 16 + 16 + 4 * nn,     # pos, k, counts, kv r/w, vel r/w
-        "divergence_residual": 16 + 16 + 4 + 4 + 4 + 4 + 4 * nn,        # pos, vel, counts, alpha, dadv, k
-        "viscosity": 16 + 16 + 4 + 4 + 16 + 4 * nf,                      # pos, vel, counts, rho, acc
-        "pressure_warm_jacobi": 16 + 4 + 4 + 16 + 16 + 4 * nn,           # pos, kappa, counts, vel r/w
-        "pressure_residual": 16 + 16 + 4 + 4 + 4 + 4 + 4 + 4 + 4 * nn,   # pos, vel, counts, rho, alpha, kappa r/w, dadv, k
-        "pressure_jacobi": 16 + 4 + 4 + 16 + 16 + 4 * nn,                # pos, k, counts, vel r/w
-        "neighbor_build": 16 + 4 + 4 * nn,                               # pos, counts, lists written
-        "update_pos": 16 + 16 + 16,                                      # pos r/w, vel
+        "density_alpha": v + v + 4 + r + r + r + r + r + 4 * nn,        # pos, vel, counts, kv r/w, rho, alpha, dadv
+        "divergence_jacobi": v + r + 4 + r + r + v + v + 4 * nn,        # pos, k, counts, kv r/w, vel r/w
+        "divergence_residual": v + v + 4 + r + r + r + 4 * nn,          # pos, vel, counts, alpha, dadv, k
+        "viscosity": v + v + 4 + r + v + 4 * nf,                        # pos, vel, counts, rho, acc
+        "pressure_warm_jacobi": v + r + 4 + v + v + 4 * nn,             # pos, kappa, counts, vel r/w
+        "pressure_residual": v + v + 4 + r + r + r + r + r + r + 4 * nn,  # pos, vel, counts, rho, alpha, kappa r/w, dadv, k
+        "pressure_jacobi": v + r + 4 + v + v + 4 * nn,                  # pos, k, counts, vel r/w
+        "neighbor_build": v + 4 + 4 * nn,                               # pos, counts, lists written
+        "update_pos": v + v + v,                                        # pos r/w, vel
     }[name]
-    extra = 16 * nb_particles if name not in ("viscosity", "update_pos") else 0  # boundary pos+psi once
+    extra = v * nb_particles if name not in ("viscosity", "update_pos") else 0  # boundary pos+psi once
     return per * n + extra
 
 
@@ -397,7 +402,7 @@ def run_ours(args, world, rank, local):
 
     scene, motion = make_workload(args.config)
     n = scene.n_fluid
-    d = DFSPHCUDA(scene, device=local, use_graphs=not args.host_loops)
+    d = DFSPHCUDA(scene, device=local, use_graphs=not args.host_loops, precision=args.precision)
     d.set_param("timing", 0)
     if motion is not None:  # the fluid follows the walls past the initial box: keep every particle
         d.set_param("remove_escaped", 0)
@@ -495,7 +500,7 @@ def run_ours(args, world, rank, local):
     share = {k: kt[k] * per_step_launches[k] for k in kt}
     dom = max(share, key=share.get)
     peak, peak_kind = _peaks()
-    alg = kernel_bytes(dom, n, scene.n_boundary, nf, nbn)
+    alg = kernel_bytes(dom, n, scene.n_boundary, nf, nbn, 8 if args.precision == 64 else 4)
     achieved = alg / (kt[dom] * 1e-3) / 1e9
     # The same kernel back to back without the flush: when its working set fits the 126 MB L2 (the
     # 250 k configurations) this is the rate it sustains inside a step, served from L2.
@@ -504,7 +509,7 @@ def run_ours(args, world, rank, local):
     l2_resident = alg < 0.75 * 126e6
     traffic = None
     tf = ROOT / "profiles" / "ncu_traffic.json"
-    if tf.exists():
+    if tf.exists() and args.precision == 32:  # the captures are of the FP32 build
         tj = json.loads(tf.read_text())
         rec = tj.get("kernels", {}).get(dom)
         if rec and rec.get("n_particles"):
@@ -524,7 +529,8 @@ def run_ours(args, world, rank, local):
         line = {
             "metric": METRIC, "value": round(ms, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice + xoshiro256** jitter)",
+            "vs_baseline": None, "dtype": "f32" if args.precision == 32 else "f64",
+            "data": "synthetic (seeded lattice + xoshiro256** jitter)",
             "config": {"workload": scene.name, "fluid_particles": n, "boundary_particles": scene.n_boundary,
                        "radius": scene.config.particleRadius, "cfl": f"0.4, dt_max {scene.config.cflMaxTimeStepSize * 1e3:g} ms",
                        "max_error_pct": scene.config.maxError, "max_error_v_pct": scene.config.maxErrorV,
@@ -563,6 +569,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", type=int, default=3)
     ap.add_argument("--host-loops", action="store_true", help="solver loops driven from the host")
+    ap.add_argument("--precision", type=int, choices=[32, 64], default=32,
+                    help="64: the FP64 build of the same kernels (the precision comparison of config 2)")
     ap.add_argument("--kernel-reps", type=int, default=5)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
