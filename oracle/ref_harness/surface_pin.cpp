@@ -54,6 +54,26 @@ int pin_surface_eval(const PinSurface* s, const float* p, uint32_t n, uint8_t* i
     return 0;
 }
 
+// The triangles MeshPerso::loadFromFile reads (OBJ_Loader, its first mesh): 9 floats per triangle,
+// the three vertex positions in index order. out null: only the count.
+int pin_obj_triangles(const char* path, float* out, uint32_t cap, uint32_t* count) {
+    objl::Loader L;
+    if (!L.LoadFile(path) || L.LoadedMeshes.empty()) return -1;
+    const objl::Mesh& m = L.LoadedMeshes[0];
+    const uint32_t nt = (uint32_t)(m.Indices.size() / 3);
+    *count = nt;
+    if (!out) return 0;
+    if (cap < nt) return -2;
+    for (uint32_t t = 0; t < nt; ++t)
+        for (int k = 0; k < 3; ++k) {
+            const objl::Vector3& q = m.Vertices[m.Indices[3 * t + k]].Position;
+            out[9 * t + 3 * k] = q.X;
+            out[9 * t + 3 * k + 1] = q.Y;
+            out[9 * t + 3 * k + 2] = q.Z;
+        }
+    return 0;
+}
+
 // MeshPerso::isInside for the mesh (vertices v[3 nv], triangles t[3 nt]) moved by offset[3].
 int pin_mesh_inside(const float* v, uint32_t nv, const uint32_t* t, uint32_t nt, const float* offset,
                     const float* p, uint32_t n, uint8_t* inside) {

@@ -47,11 +47,11 @@ extern "C" int dfsph_read_obj(const char* path, float* vertices, uint32_t vertex
         std::string kind;
         if (!(ls >> kind)) continue;
         if (kind == "v") {
-            double x, y, z;
+            float x, y, z;  // read as float directly (rounded once, as OBJ_Loader's std::stof does)
             if (!(ls >> x >> y >> z)) return DFSPH_E_INVALID;
-            v.push_back((float)x);
-            v.push_back((float)y);
-            v.push_back((float)z);
+            v.push_back(x);
+            v.push_back(y);
+            v.push_back(z);
         } else if (kind == "f") {
             std::vector<uint32_t> poly;
             std::string tok;

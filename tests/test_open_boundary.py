@@ -4,6 +4,7 @@ SPlisHSPlasH/DFSPH/BufferFluidSurface.cu compiled as host code; the live pin whe
 reference's configuration table, and the oracle's inflow / outflow against a brute-force numpy
 restatement of OpenBoundariesSimple.cu:352-492 on a small tank. No GPU is needed."""
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -110,6 +111,27 @@ def test_read_obj(tmp_path):
     v2, t2 = ob.read_obj(_write_box_obj(tmp_path / "box.obj"))
     a, b = ob.box_mesh((0, 0, 0), (1, 2, 3))
     assert np.array_equal(v2, a) and np.array_equal(t2, b)
+
+
+REF_DIR = Path(os.environ.get("REF_DIR", str(Path(__file__).resolve().parents[2] / "reference")))
+REF_MODELS = ["UnitBox.obj", "EmitterBox.obj", "EmitterCylinder.obj", "2mBox_rotated45.obj", "Dragon_50k.obj"]
+
+
+@pytest.mark.skipif(not PIN.exists() or not (REF_DIR / "data" / "models").is_dir(),
+                    reason="the reference's OBJ_Loader pin or its models are not present")
+def test_read_obj_matches_reference_loader():
+    """dfsph_read_obj against the reference's own OBJ_Loader (as MeshPerso::loadFromFile calls it) on
+    the reference's models: the same triangles, vertex positions bit for bit, in the same order."""
+    lib = C.CDLL(str(PIN))
+    lib.pin_obj_triangles.argtypes = [C.c_char_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]
+    for name in REF_MODELS:
+        path = REF_DIR / "data" / "models" / name
+        n = C.c_uint32()
+        assert lib.pin_obj_triangles(str(path).encode(), None, 0, C.byref(n)) == 0
+        want = np.zeros((n.value, 9), np.float32)
+        assert lib.pin_obj_triangles(str(path).encode(), want.ctypes.data, n.value, C.byref(n)) == 0
+        v, t = ob.read_obj(path)
+        assert np.array_equal(v[t].reshape(-1, 9), want), name
 
 
 def _write_box_obj(path):
