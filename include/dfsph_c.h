@@ -453,6 +453,17 @@ int dfsph_dynamic_window_init(dfsph_ctx* ctx, const double* lo, const double* hi
                               uint32_t wall_count, const float* rest_xyz, uint32_t n_rest);
 int dfsph_dynamic_window_shift(dfsph_ctx* ctx, const double* displacement, double allowed_distance,
                                double allowed_density, uint32_t* added, uint32_t* removed);
+/* DynamicWindowInterface::stabilizeFluid, method 0 (DynamicWindow.cu:3160-3700), between steps after
+ * dfsph_dynamic_window_shift: `iterations` steps of the fixed time step `time_step` (the reference's
+ * default: 5 steps of 3 ms) with kappa and kappa_v cleared before and after; each runs the neighbour
+ * search, the divergence solve, viscosity and gravity, the pressure solve with the velocity update,
+ * multiplies the velocities of the particles the last shift added by `damping` (in [0, 1]; 1: none)
+ * and updates the positions. With tagged_only the other particles keep their positions and velocities
+ * (they act as neighbours only); particles count as added by the last shift until the fluid is
+ * compacted or uploaded again. The dt history is restored afterwards. Synchronises the context's
+ * stream. */
+int dfsph_dynamic_window_stabilize(dfsph_ctx* ctx, uint32_t iterations, double time_step, double damping,
+                                   int tagged_only);
 /* Total displacement of the window since dfsph_dynamic_window_init. */
 int dfsph_dynamic_window_displacement(dfsph_ctx* ctx, double* displacement);
 

@@ -961,6 +961,39 @@ template <class Real> struct Oracle {
         return clampk((double)(kw_v[i] + kapv[i] + std::min<Real>(raw_v[i], Real(0)) * (alpha[i] * (Real)h_future)));
     }
 
+    // dfsph_dynamic_window_stabilize (DynamicWindow::stabilizeFluid method 0, DynamicWindow.cu:
+    // 3160-3700): `iters` steps of the fixed step `dt` with the warm starts cleared before and after;
+    // the particles before `first` keep their positions and velocities, the others' velocities are
+    // multiplied by `damping` before each position update; the dt history is restored afterwards.
+    void stabilize(uint32_t iters, double dt, double damping, uint32_t first) {
+        const double sh = h, shf = h_future, shp = h_past, sih = inv_h, sihf = inv_h_future, sr = h_ratio,
+                     sr2 = h_ratio2;
+        h = h_future = dt;
+        inv_h = inv_h_future = 1.0 / dt;
+        h_ratio = h_ratio2 = 1.0;
+        std::fill(kap.begin(), kap.end(), Real(0));
+        std::fill(kapv.begin(), kapv.end(), Real(0));
+        first = std::min(first, n);
+        const std::vector<Real> sx(x.begin(), x.begin() + 3 * (size_t)first), sv(v.begin(), v.begin() + 3 * (size_t)first);
+        for (uint32_t it = 0; it < iters; ++it) {
+            neighbors();
+            if (prm.enable_divergence_solver) divergence_solve(prm.max_iterations_v, prm.max_error_v);
+            else density_alpha(false);
+            viscosity();
+            update_vel();
+            pressure_solve(prm.max_iterations, prm.max_error);
+            if (damping < 1.0)
+                for (size_t k = 3 * (size_t)first; k < 3 * (size_t)n; ++k) v[k] *= (Real)damping;
+            update_pos();
+            std::copy(sx.begin(), sx.end(), x.begin());
+            std::copy(sv.begin(), sv.end(), v.begin());
+            on_step_end();
+        }
+        std::fill(kap.begin(), kap.end(), Real(0));
+        std::fill(kapv.begin(), kapv.end(), Real(0));
+        h = sh; h_future = shf; h_past = shp; inv_h = sih; inv_h_future = sihf; h_ratio = sr; h_ratio2 = sr2;
+    }
+
     void step() {
         div_ran = false;
         neighbors();
@@ -1131,6 +1164,10 @@ int oracle_open_boundary_shift(void* h, const float* d) { return ORACLE_DO(h, (o
 // Removes the fluid particles with a coordinate outside [lo, hi] (compared as the device's box tag,
 // open_boundary.cu box_tag_kernel), keeping the order of the others; the dynamic window's removal
 // behind a moved window.
+int oracle_dynamic_window_stabilize(void* h, uint32_t iters, double dt, double damping, uint32_t first) {
+    return ORACLE_DO(h, (o.stabilize(iters, dt, damping, first), 0));
+}
+
 int oracle_remove_outside_box(void* h, const float* lo, const float* hi, uint32_t* removed) {
     return ORACLE_DO(h, ([&] {
         using R = typename std::remove_reference<decltype(o.x[0])>::type;

@@ -108,6 +108,7 @@ def _load():
             "oracle_remove_outside_box": (C.c_int, [vp, fp, fp, up]),
             "oracle_surface_eval": (C.c_int, [C.POINTER(OracleSurface), fp, C.c_uint32, C.c_void_p, fp]),
             "oracle_set_surface_mesh": (C.c_int, [C.c_uint32, fp, C.c_uint32, up, C.c_uint32]),
+            "oracle_dynamic_window_stabilize": (C.c_int, [vp, C.c_uint32, C.c_double, C.c_double, C.c_uint32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -283,6 +284,10 @@ class Oracle:
                                            _f(np.asarray(hi, np.float32).reshape(3)), C.byref(r))
         self.n = int(self.scalar("n"))
         return int(r.value)
+
+    def dynamic_window_stabilize(self, iterations: int, time_step: float, damping: float, first: int) -> None:
+        """The device's dfsph_dynamic_window_stabilize with the particles of ids >= first tagged."""
+        self.lib.oracle_dynamic_window_stabilize(self.h, int(iterations), float(time_step), float(damping), int(first))
 
     def open_boundary_shift(self, delta) -> None:
         self.lib.oracle_open_boundary_shift(self.h, _f(np.asarray(delta, np.float32).reshape(3)))

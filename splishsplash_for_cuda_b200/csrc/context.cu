@@ -213,6 +213,11 @@ public:
     // dynamic window: the window box and its total displacement, the walls that move with it, and
     // the rest-fluid samples (in the window's current place) with their scratch
     bool dw_ready = false;
+    // ids >= dw_first_new were added by the last window shift (the stabilisation's tagged particles;
+    // none once the fluid is compacted or uploaded again); dw_spos / dw_svel keep the others' state
+    uint32_t dw_first_new = 0;
+    Vec4<Real>* dw_spos = nullptr;
+    Vec4<Real>* dw_svel = nullptr;
     double dw_lo[3] = {0, 0, 0}, dw_hi[3] = {0, 0, 0}, dw_disp[3] = {0, 0, 0};
     uint32_t dw_wall_first = 0, dw_wall_count = 0, dw_ns = 0, dw_cap = 0;
     float4* dw_samples = nullptr;  // rest samples, moved with the window
@@ -320,7 +325,7 @@ public:
         f(mlp.params); f(mlp.adam_m); f(mlp.adam_v); f(mlp.grad); f(mlp.partials);
         f(mlp.w1_bf16); f(mlp.w2_bf16); f(mlp.w3_bf16); f(mlp.scales); f(mlp.loss);
         f(ob_samples); f(ob_vel); f(ob_flag); f(ob_rank); f(ob_scan); f(ob_total); f(wrench_buf);
-        f(brest); f(dw_samples); f(dw_sel); f(dw_vel); f(dw_flag); f(dw_rank);
+        f(brest); f(dw_samples); f(dw_sel); f(dw_vel); f(dw_flag); f(dw_rank); f(dw_spos); f(dw_svel);
         for (MeshSlot& m : meshes) {
             f(m.tri);
             m = MeshSlot{};
@@ -653,6 +658,7 @@ public:
         if (count != n) invalidate_graphs();
         n = count;
         cur = 0;
+        dw_first_new = count;
         last_lp = false;  // the uploaded state carries no learned warm start
         {
             const double d = 2.0 * sc.particle_radius;
@@ -937,6 +943,7 @@ public:
     // Stable removal of the particles with alive[i] == 0 (dst = exclusive scan of alive, kept
     // survivors): the state moves to the other buffer; ids stay dense and keep their relative order.
     int compact_fluid(const uint32_t* alive, const uint32_t* dst, uint32_t kept) {
+        dw_first_new = kept;  // ids are renumbered: nothing counts as added by the window any more
         const int nx = 1 - cur;
         launch_compact_fluid<Real>(alive, dst, n, pos[cur], vel[cur], kappa[cur], kappaV[cur], id[cur],
                                    learned ? kappaT[cur] : nullptr, learned ? kappaVT[cur] : nullptr, pos[nx],
@@ -1131,6 +1138,7 @@ public:
                 launches += 5;
             }
         }
+        dw_first_new = n - n_add;
         if (n_add || n_rm) invalidate_graphs();
         DF_TRY(sync_state());
         if (clipped) {
@@ -1144,6 +1152,72 @@ public:
         DF_CUDA(cudaGetLastError());
         if (added) *added = n_add;
         if (removed) *removed = n_rm;
+        return DFSPH_OK;
+    }
+
+    // DynamicWindowInterface::stabilizeFluid, method 0 (DynamicWindow.cu:3160-3700: the fluid simulated
+    // for a few steps of a fixed time step with the warm starts cleared before and after, restricted
+    // to the tagged particles, their velocities damped before each position update). Here the tagged
+    // particles are the ones the last shift added; the others, with tagged_only, keep their positions
+    // and velocities (they take part as neighbours). Each iteration is the plain step's sequence:
+    // neighbour search, divergence solve, viscosity and gravity, pressure solve with the velocity
+    // update, damping, position update. The dt history is restored afterwards (the reference sets the
+    // previous time step again).
+    int dynamic_window_stabilize(uint32_t iterations, double step, double damping, int tagged_only) {
+        DF_CHECK(dw_ready, DFSPH_E_STATE, "dynamic window not initialised (dfsph_dynamic_window_init)");
+        DF_CHECK(step > 0 && std::isfinite(step), DFSPH_E_INVALID, "stabilisation time step must be finite and > 0");
+        DF_CHECK(damping >= 0 && damping <= 1, DFSPH_E_INVALID, "damping must be in [0, 1]");
+        if (!n || !iterations) return DFSPH_OK;
+        const uint32_t first = tagged_only ? std::min(dw_first_new, n) : 0u;
+        std::vector<double> saved(kDtSlots);
+        DF_CUDA(cudaMemcpyAsync(saved.data(), dtd, kDtSlots * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        DtArgs a{};
+        for (int k = 0; k < kDtSlots; ++k) a.v[k] = saved[k];
+        a.v[kDtH] = a.v[kDtHFuture] = step;
+        a.v[kDtInvH] = a.v[kDtInvHFuture] = 1.0 / step;
+        a.v[kDtRatio] = a.v[kDtRatio2] = 1.0;
+        launch_dt<Real>(ds, 0, a, stream);
+        DF_CUDA(cudaMemsetAsync(kappa[cur], 0, (size_t)n * sizeof(Real), stream));
+        DF_CUDA(cudaMemsetAsync(kappaV[cur], 0, (size_t)n * sizeof(Real), stream));
+        launches += 1;
+        if (first) {
+            if (!dw_spos) {
+                DF_TRY(dalloc(&dw_spos, Nc));
+                DF_TRY(dalloc(&dw_svel, Nc));
+            }
+            launch_save_untagged<Real>(pos[cur], vel[cur], id[cur], n, first, dw_spos, dw_svel, stream);
+            launches += 1;
+        }
+        for (uint32_t it = 0; it < iterations; ++it) {
+            DF_TRY(neighbors_search());
+            if (sc.enable_divergence_solver) {
+                DF_TRY(divergence_solve(sc.max_iterations_v, sc.max_error_v));
+            } else {
+                launch_density_alpha<Real>(ds, n, false, false, stream);
+                launches += 1;
+            }
+            DF_TRY(external_forces(false));
+            DF_TRY(pressure_solve(sc.max_iterations, sc.max_error, true));
+            if (damping < 1.0) {
+                launch_damp_tagged<Real>(vel[cur], id[cur], n, first, (Real)damping, stream);
+                launches += 1;
+            }
+            DF_TRY(update_pos());
+            if (first) {
+                launch_restore_untagged<Real>(pos[cur], vel[cur], id[cur], n, first, dw_spos, dw_svel, stream);
+                launches += 1;
+            }
+            DF_TRY(on_step_end());
+        }
+        DF_CUDA(cudaMemsetAsync(kappa[cur], 0, (size_t)n * sizeof(Real), stream));
+        DF_CUDA(cudaMemsetAsync(kappaV[cur], 0, (size_t)n * sizeof(Real), stream));
+        for (int k = 0; k < kDtSlots; ++k) a.v[k] = saved[k];
+        launch_dt<Real>(ds, 0, a, stream);
+        launches += 1;
+        dt_stale = true;
+        DF_CUDA(cudaStreamSynchronize(stream));
+        DF_CUDA(cudaGetLastError());
         return DFSPH_OK;
     }
 
@@ -2880,6 +2954,10 @@ int dfsph_dynamic_window_init(dfsph_ctx* ctx, const double* lo, const double* hi
 int dfsph_dynamic_window_shift(dfsph_ctx* ctx, const double* displacement, double allowed_distance,
                                double allowed_density, uint32_t* added, uint32_t* removed) {
     DFSPH_DISPATCH(ctx, dynamic_window_shift(displacement, allowed_distance, allowed_density, added, removed));
+}
+int dfsph_dynamic_window_stabilize(dfsph_ctx* ctx, uint32_t iterations, double time_step, double damping,
+                                   int tagged_only) {
+    DFSPH_DISPATCH(ctx, dynamic_window_stabilize(iterations, time_step, damping, tagged_only));
 }
 int dfsph_dynamic_window_displacement(dfsph_ctx* ctx, double* displacement) {
     DFSPH_DISPATCH(ctx, dynamic_window_state(displacement));

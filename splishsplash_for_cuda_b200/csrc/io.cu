@@ -218,6 +218,50 @@ template <class Real> __global__ void set_state_kernel(DevState<Real>* __restric
         for (int k = 0; k < 4; ++k) v.ctl[k].ticket = 0;
 }
 
+template <class Real>
+__global__ void __launch_bounds__(kBlock) save_untagged_kernel(const Vec4<Real>* __restrict__ pos,
+                                                               const Vec4<Real>* __restrict__ vel,
+                                                               const uint32_t* __restrict__ id, uint32_t n,
+                                                               uint32_t first, Vec4<Real>* __restrict__ spos,
+                                                               Vec4<Real>* __restrict__ svel) {
+    DFSPH_PDL_ENTER;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = id[i];
+    if (t >= first) return;
+    spos[t] = pos[i];
+    svel[t] = vel[i];
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock) restore_untagged_kernel(Vec4<Real>* __restrict__ pos,
+                                                                  Vec4<Real>* __restrict__ vel,
+                                                                  const uint32_t* __restrict__ id, uint32_t n,
+                                                                  uint32_t first, const Vec4<Real>* __restrict__ spos,
+                                                                  const Vec4<Real>* __restrict__ svel) {
+    DFSPH_PDL_ENTER;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = id[i];
+    if (t >= first) return;
+    pos[i] = spos[t];
+    vel[i] = svel[t];
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBlock) damp_tagged_kernel(Vec4<Real>* __restrict__ vel,
+                                                             const uint32_t* __restrict__ id, uint32_t n,
+                                                             uint32_t first, Real f) {
+    DFSPH_PDL_ENTER;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || id[i] < first) return;
+    Vec4<Real> v = vel[i];
+    v.x *= f;
+    v.y *= f;
+    v.z *= f;
+    vel[i] = v;
+}
+
 template <class Real> __global__ void dt_kernel(DevState<Real>* __restrict__ ds, int op, DtArgs a) {
     DFSPH_PDL_ENTER;
     double* t = ds->dtd;
@@ -299,6 +343,20 @@ template <class Real>
 void launch_force_from_fx(const unsigned long long* fx, uint32_t n, Real* out, cudaStream_t s) {
     if (n) launch_pdl(force_from_fx_kernel<Real>, grid_for(n), kBlock, 0, s, fx, n, out);
 }
+template <class Real>
+void launch_save_untagged(const Vec4<Real>* pos, const Vec4<Real>* vel, const uint32_t* id, uint32_t n, uint32_t first,
+                          Vec4<Real>* spos, Vec4<Real>* svel, cudaStream_t s) {
+    if (n) launch_pdl(save_untagged_kernel<Real>, grid_for(n), kBlock, 0, s, pos, vel, id, n, first, spos, svel);
+}
+template <class Real>
+void launch_restore_untagged(Vec4<Real>* pos, Vec4<Real>* vel, const uint32_t* id, uint32_t n, uint32_t first,
+                             const Vec4<Real>* spos, const Vec4<Real>* svel, cudaStream_t s) {
+    if (n) launch_pdl(restore_untagged_kernel<Real>, grid_for(n), kBlock, 0, s, pos, vel, id, n, first, spos, svel);
+}
+template <class Real>
+void launch_damp_tagged(Vec4<Real>* vel, const uint32_t* id, uint32_t n, uint32_t first, Real f, cudaStream_t s) {
+    if (n) launch_pdl(damp_tagged_kernel<Real>, grid_for(n), kBlock, 0, s, vel, id, n, first, f);
+}
 template <class Real, class Out>
 void launch_pack_field(const Real* src, int src_stride, int comps, const uint32_t* id, uint32_t n, Out* dst,
                        cudaStream_t s) {
@@ -326,6 +384,11 @@ void launch_unpack_counts(const uint32_t* counts, const uint32_t* id, uint32_t n
     template void launch_rigid_boundary<R>(const float*, uint32_t, const uint32_t*, const RigidMotion&, Vec4<R>*,    \
                                            Vec4<R>*, cudaStream_t);                                                  \
     template void launch_force_from_fx<R>(const unsigned long long*, uint32_t, R*, cudaStream_t);                    \
+    template void launch_save_untagged<R>(const Vec4<R>*, const Vec4<R>*, const uint32_t*, uint32_t, uint32_t,       \
+                                          Vec4<R>*, Vec4<R>*, cudaStream_t);                                         \
+    template void launch_restore_untagged<R>(Vec4<R>*, Vec4<R>*, const uint32_t*, uint32_t, uint32_t,                \
+                                             const Vec4<R>*, const Vec4<R>*, cudaStream_t);                          \
+    template void launch_damp_tagged<R>(Vec4<R>*, const uint32_t*, uint32_t, uint32_t, R, cudaStream_t);             \
     template void launch_pack_field<R, float>(const R*, int, int, const uint32_t*, uint32_t, float*, cudaStream_t);  \
     template void launch_pack_field<R, double>(const R*, int, int, const uint32_t*, uint32_t, double*, cudaStream_t);
 

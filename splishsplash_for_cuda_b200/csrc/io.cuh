@@ -50,6 +50,17 @@ void launch_rigid_boundary(const float* rest, uint32_t n, const uint32_t* bid, c
 // Boundary forces from their fixed-point sums (x, y, z, 0 per particle).
 template <class Real>
 void launch_force_from_fx(const unsigned long long* fx, uint32_t n, Real* out, cudaStream_t s);
+// The dynamic window's stabilisation: particles with id >= first (the ones the last shift added) are
+// the tagged ones. save: spos[id] = pos, svel[id] = vel for the untagged; restore: the untagged get
+// their saved position and velocity back; damp: the tagged velocities are multiplied by f.
+template <class Real>
+void launch_save_untagged(const Vec4<Real>* pos, const Vec4<Real>* vel, const uint32_t* id, uint32_t n, uint32_t first,
+                          Vec4<Real>* spos, Vec4<Real>* svel, cudaStream_t s);
+template <class Real>
+void launch_restore_untagged(Vec4<Real>* pos, Vec4<Real>* vel, const uint32_t* id, uint32_t n, uint32_t first,
+                             const Vec4<Real>* spos, const Vec4<Real>* svel, cudaStream_t s);
+template <class Real>
+void launch_damp_tagged(Vec4<Real>* vel, const uint32_t* id, uint32_t n, uint32_t first, Real f, cudaStream_t s);
 template <class Real, class Out>
 void launch_pack_field(const Real* src, int src_stride, int comps, const uint32_t* id, uint32_t n, Out* dst,
                        cudaStream_t s);

@@ -415,6 +415,14 @@ class DFSPHCUDA:
                                                         float(allowed_density), C.byref(a), C.byref(r)))
         return int(a.value), int(r.value)
 
+    def stabilize_dynamic_window(self, iterations: int = 5, time_step: float = 0.003, damping: float = 1.0,
+                                 tagged_only: bool = True) -> None:
+        """DynamicWindowInterface::stabilizeFluid, method 0: after a shift, `iterations` steps of the
+        fixed `time_step` with the warm starts cleared, the particles the shift added damped by
+        `damping` before each position update and, with tagged_only, the others held in place."""
+        self._call(self._lib.dfsph_dynamic_window_stabilize(self._ctx, int(iterations), float(time_step),
+                                                            float(damping), 1 if tagged_only else 0))
+
     def dynamic_window_displacement(self) -> np.ndarray:
         out = np.zeros(3, np.float64)
         self._call(self._lib.dfsph_dynamic_window_displacement(self._ctx, out.ctypes.data))

@@ -78,6 +78,54 @@ def test_dynamic_window_lockstep_with_oracle():
     assert np.array_equal(bx.astype(np.float32), (walls0 + disp.astype(np.float32)).astype(np.float32))
 
 
+@pytest.mark.parametrize("tagged_only", [True, False])
+def test_window_stabilisation_lockstep_with_oracle(tagged_only):
+    """dfsph_dynamic_window_stabilize after a shift against the oracle's restatement: 4 steps of 3 ms
+    with the added particles damped by 0.5; with tagged_only the other particles do not move (bit
+    for bit) and only the added ones settle; afterwards the warm starts are clear, the dt history is
+    back and the run continues in lockstep (positions within 2e-4 m, FP32 vs FP64)."""
+    s, lo, hi, rest, grid = _window_scene()
+    nb = s.n_boundary
+    d = DFSPHCUDA(s, grid_box=grid, fluid_capacity=s.n_fluid + 4000)
+    d.set_param("remove_escaped", 0)
+    d.init_dynamic_window(lo, hi, 0, nb, rest)
+    o = Oracle(s, 64, grid_box=grid)
+    o.set_scalar("remove_escaped", 0)
+    for _ in range(3):
+        d.step()
+        o.step()
+    shift = np.array([0.1, 0.0, 0.0])
+    added, removed = d.shift_dynamic_window(shift, 0.9 * 2 * R, 1100.0)
+    walls = (s.boundary.astype(np.float32) + shift.astype(np.float32)).astype(np.float32)
+    o.move_boundary(walls, np.zeros_like(walls))
+    blo, bhi = _f32box(lo, hi, shift)
+    r_o = o.remove_outside_box(blo, bhi)
+    samples = (rest + np.float32(shift[0]) * np.array([1, 0, 0], np.float32)).astype(np.float32)
+    prev = cuboid(0.5 * (lo + hi), 0.5 * (hi - lo))
+    box = cuboid(0.5 * (lo + hi) + shift, 0.5 * (hi - lo))
+    o.open_boundary_init(box, prev, plane((0.0, 3.0e38, 0.0), (0.0, -1.0, 0.0)), samples)
+    a_o, _, _ = o.open_boundary_apply(0.9 * 2 * R, 1100.0, use_inflow=True, use_outflow=False)
+    assert (added, removed) == (a_o, r_o) and added > 0
+    n = d.num_fluid()
+    first = n - added if tagged_only else 0
+    h0 = d.get_param("h")
+    x_before = d.positions()
+    d.stabilize_dynamic_window(4, 0.003, 0.5, tagged_only)
+    o.dynamic_window_stabilize(4, 0.003, 0.5, first)
+    x_after = d.positions()
+    if tagged_only:
+        assert np.array_equal(x_after[:first], x_before[:first])
+    assert not np.array_equal(x_after[n - added:], x_before[n - added:])
+    assert d.get_param("h") == h0
+    assert not d.field("kappa").any() and not d.field("kappa_v").any()
+    xd, xo = d.field("position", np.float64), o.field("position")
+    assert np.abs(xd - xo).max() <= 2e-4
+    for k in range(4):
+        st, ro = d.step(), o.step()
+        assert (st.iterations, st.iterations_v) == (ro["iterations"], ro["iterations_v"]), k
+    assert np.abs(d.field("position", np.float64) - o.field("position")).max() <= 2e-4
+
+
 def test_dynamic_window_arguments_are_checked():
     s, lo, hi, rest, grid = _window_scene()
     d = DFSPHCUDA(s, grid_box=grid)
@@ -91,3 +139,6 @@ def test_dynamic_window_arguments_are_checked():
     d.init_dynamic_window(lo, hi, 0, s.n_boundary, rest)
     with pytest.raises(_capi.DfsphError):
         d.shift_dynamic_window((0.1, 0, 0), 0.0, 1100.0)
+    for args in [(2, 0.0, 1.0), (2, 0.003, 1.5), (2, float("nan"), 1.0)]:
+        with pytest.raises(_capi.DfsphError):
+            d.stabilize_dynamic_window(*args)
