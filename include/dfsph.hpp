@@ -20,6 +20,7 @@
 #ifndef DFSPH_HPP
 #define DFSPH_HPP
 
+#include <array>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -131,6 +132,7 @@ public:
             (!psi_.empty() && psi_.size() * 3 != boundary_.size()))
             throw Error(DFSPH_E_INVALID, "DFSPHCUDA: array sizes do not match");
         dfsph_scene s = scene;
+        radius_ = scene.particle_radius;
         if (s.fluid_capacity < fluid_.size() / 3) s.fluid_capacity = (uint32_t)(fluid_.size() / 3);
         if (s.boundary_capacity < boundary_.size() / 3) s.boundary_capacity = (uint32_t)(boundary_.size() / 3);
         check(nullptr, dfsph_create(&s, &ctx_));
@@ -187,6 +189,106 @@ public:
     double getViscosity() const { return get("viscosity"); }
     void setViscosity(double v) { set("viscosity", v); }
 
+    /* ---- the host-side operations of the reference's DFSPHCUDA (DFSPH_CUDA.cpp:1885-1979, 3889-4210) */
+
+    /* DFSPHCData::fluid_files_folder: where handleSimulationSave / handleSimulationLoad write and read. */
+    std::string fluid_files_folder = "file_data/";
+    /* handleSimulationSave: the fluid (with general_data.txt) and the boundary in the reference's text
+     * format. Dynamic bodies are ranges of the boundary here, so save_solids adds nothing of its own. */
+    void handleSimulationSave(bool save_liquid, bool save_solids, bool save_boundaries) {
+        (void)save_solids;
+        const int what = (save_liquid ? DFSPH_SNAP_FLUID : 0) | (save_boundaries ? DFSPH_SNAP_BOUNDARY : 0);
+        if (what) check(ctx_, dfsph_save_snapshot(ctx_, fluid_files_folder.c_str(), what));
+    }
+    /* handleSimulationLoad (dynamic bodies: as handleSimulationSave). */
+    void handleSimulationLoad(bool load_liquid, bool load_liquid_velocities, bool load_solids,
+                              bool load_solids_velocities, bool load_boundaries) {
+        (void)load_solids;
+        (void)load_solids_velocities;
+        const int what = (load_liquid ? DFSPH_SNAP_FLUID : 0) | (load_boundaries ? DFSPH_SNAP_BOUNDARY : 0);
+        if (what)
+            check(ctx_, dfsph_load_snapshot(ctx_, fluid_files_folder.c_str(), what, load_liquid_velocities ? 1 : 0));
+    }
+    /* zeroFluidVelocities (DFSPHCData::zeroFluidVelocities): positions kept, velocities zero. */
+    void zeroFluidVelocities() {
+        std::vector<float> x, v;
+        m_data.readDynamicData(x, v);
+        if (!x.empty()) check(ctx_, dfsph_update_fluid(ctx_, x.data(), nullptr));
+    }
+    /* updateTimeStepDuration: the time step used while the CFL condition is off. */
+    void updateTimeStepDuration(double duration) { set("time_step", duration); }
+    /* applyOpenBoundaries (DFSPH_CUDA.cpp:3889-3986) with the reference's thresholds (1.75 r,
+     * 700 kg/m^3, :3903-3906) once dfsph_open_boundary_init has set the surfaces and samples. */
+    void applyOpenBoundaries() {
+        check(ctx_, dfsph_open_boundary_apply(ctx_, 1.75 * radius_, 700.0, 1, 1, nullptr, nullptr));
+    }
+    /* The dynamic window (DynamicWindowInterface): its box and walls, then handleSimulationMovement
+     * (DFSPH_CUDA.cpp:4142-4147: movements of more than 0.5 m shift it, with the open boundary's inflow
+     * thresholds for the newly covered region) and getSimulationCenter (the box's centre). */
+    void dynamicWindowInit(const double lo[3], const double hi[3], uint32_t wall_first, uint32_t wall_count,
+                           const std::vector<float>& rest_xyz) {
+        check(ctx_, dfsph_dynamic_window_init(ctx_, lo, hi, wall_first, wall_count, rest_xyz.data(),
+                                              (uint32_t)(rest_xyz.size() / 3)));
+        for (int a = 0; a < 3; ++a) window_center_[a] = 0.5 * (lo[a] + hi[a]);
+    }
+    void handleSimulationMovement(const double movement[3]) {
+        const double m2 = movement[0] * movement[0] + movement[1] * movement[1] + movement[2] * movement[2];
+        if (m2 > 0.25)
+            check(ctx_, dfsph_dynamic_window_shift(ctx_, movement, 1.75 * radius_, 700.0, nullptr, nullptr));
+    }
+    std::array<double, 3> getSimulationCenter() const {
+        double d[3] = {0, 0, 0};
+        if (dfsph_dynamic_window_displacement(ctx_, d) != DFSPH_OK) d[0] = d[1] = d[2] = 0.0;
+        return {window_center_[0] + d[0], window_center_[1] + d[1], window_center_[2] + d[2]};
+    }
+    /* Dynamic bodies as ranges of the boundary (upload order) with their centres, for
+     * getFluidImpactOnDynamicBodies (needs set("boundary_forces", 1)). */
+    struct DynamicBody {
+        uint32_t first, count;
+        std::array<double, 3> position;
+    };
+    std::vector<DynamicBody> dynamic_bodies;
+    /* getFluidImpactOnDynamicBodies (compute_fluid_impact_on_dynamic_body_kernel,
+     * DFSPH_memory_management_cuda.cu:688-705): per body, the sum of its particles' fluid forces
+     * multiplied component-wise by the body's reduction factor, and the moment of those forces about
+     * the body's position; appended to sph_forces / sph_moments, summed in FP64 on the host. */
+    void getFluidImpactOnDynamicBodies(std::vector<std::array<double, 3>>& sph_forces,
+                                       std::vector<std::array<double, 3>>& sph_moments,
+                                       const std::vector<std::array<double, 3>>& reduction_factors) {
+        uint32_t nb = 0;
+        {
+            double v = 0;
+            check(ctx_, dfsph_get_param(ctx_, "num_boundary", &v));
+            nb = (uint32_t)v;
+        }
+        std::vector<double> f(3 * (size_t)nb), x(3 * (size_t)nb);
+        if (nb) {
+            check(ctx_, dfsph_download(ctx_, DFSPH_F_BOUNDARY_FORCE, DFSPH_DTYPE_F64, f.data(), f.size(), DFSPH_ORDER_ID));
+            check(ctx_, dfsph_download(ctx_, DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F64, x.data(), x.size(),
+                                       DFSPH_ORDER_ID));
+        }
+        for (size_t b = 0; b < dynamic_bodies.size(); ++b) {
+            const DynamicBody& body = dynamic_bodies[b];
+            if ((uint64_t)body.first + body.count > nb) throw Error(DFSPH_E_INVALID, "dynamic body beyond the boundary");
+            const std::array<double, 3> r =
+                b < reduction_factors.size() ? reduction_factors[b] : std::array<double, 3>{1.0, 1.0, 1.0};
+            std::array<double, 3> F{0, 0, 0}, M{0, 0, 0};
+            for (uint32_t i = body.first; i < body.first + body.count; ++i) {
+                const double fx = f[3 * (size_t)i] * r[0], fy = f[3 * (size_t)i + 1] * r[1], fz = f[3 * (size_t)i + 2] * r[2];
+                const double px = x[3 * (size_t)i] - body.position[0], py = x[3 * (size_t)i + 1] - body.position[1],
+                             pz = x[3 * (size_t)i + 2] - body.position[2];
+                F[0] += fx;
+                F[1] += fy;
+                F[2] += fz;
+                M[0] += py * fz - pz * fy;
+                M[1] += pz * fx - px * fz;
+                M[2] += px * fy - py * fx;
+            }
+            sph_forces.push_back(F);
+            sph_moments.push_back(M);
+        }
+    }
+
     const dfsph_step_stats& lastStats() const { return stats_; }
     dfsph_ctx* handle() const { return ctx_; }
     /* Any dfsph_set_param / dfsph_get_param key (e.g. "learned_warm_start", "boundary_forces"). */
@@ -205,6 +307,8 @@ private:
     dfsph_ctx* ctx_ = nullptr;
     dfsph_step_stats stats_{};
     std::vector<float> fluid_, vel_, boundary_, psi_;
+    double radius_ = 0.0;
+    double window_center_[3] = {0.0, 0.0, 0.0};
 };
 
 /* SPH::TimeStepDFSPH (TimeStepDFSPH.h:20-48), the reference's CPU solver class, on the device time

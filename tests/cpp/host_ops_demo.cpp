@@ -1,0 +1,99 @@
+// host_ops_demo.cpp — the host-side operations of the reference's SPH::DFSPHCUDA through the C++
+// facade (include/dfsph.hpp): handleSimulationSave / handleSimulationLoad, zeroFluidVelocities,
+// updateTimeStepDuration and getFluidImpactOnDynamicBodies. Test program: tests/test_cpp_facade.py
+// writes the scene, runs this and reads its exit code; the checks are made here.
+//
+//   host_ops_demo <scene.bin> <folder/>
+//
+// scene.bin as for facade_demo. Exit codes: 0 ok, 1 a check failed (message on stderr), 2 usage /
+// input error, 3 dfsph::Error.
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <vector>
+
+#include "dfsph.hpp"
+
+namespace {
+template <class T> bool rd(std::ifstream& f, T* p, size_t n) {
+    return (bool)f.read(reinterpret_cast<char*>(p), (std::streamsize)(n * sizeof(T)));
+}
+int fail(const char* what) {
+    std::cerr << "check failed: " << what << "\n";
+    return 1;
+}
+bool close(double a, double b, double tol) { return std::fabs(a - b) <= tol * std::max(1.0, std::fabs(b)); }
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc != 3) {
+        std::cerr << "usage: host_ops_demo <scene.bin> <folder/>\n";
+        return 2;
+    }
+    std::ifstream in(argv[1], std::ios::binary);
+    int32_t n = 0, nb = 0;
+    double cfg[10];
+    if (!rd(in, &n, 1) || !rd(in, &nb, 1) || !rd(in, cfg, 10) || n <= 0 || nb <= 0) {
+        std::cerr << "bad scene file\n";
+        return 2;
+    }
+    std::vector<float> fluid(3 * (size_t)n), boundary(3 * (size_t)nb);
+    if (!rd(in, fluid.data(), fluid.size()) || !rd(in, boundary.data(), boundary.size())) {
+        std::cerr << "truncated scene file\n";
+        return 2;
+    }
+    try {
+        dfsph_scene s;
+        dfsph::check(nullptr, dfsph_scene_defaults(&s));
+        s.particle_radius = cfg[0];
+        s.time_step = cfg[3];
+        dfsph::DFSPHCUDA sim(s, fluid, boundary);
+        sim.set("boundary_forces", 1);
+        for (int k = 0; k < 8; ++k) sim.step();
+
+        // getFluidImpactOnDynamicBodies: the whole boundary as one body, against dfsph_body_wrench
+        const double c[3] = {0.5, 0.25, 0.5};
+        sim.dynamic_bodies = {{0u, (uint32_t)nb, {c[0], c[1], c[2]}}};
+        std::vector<std::array<double, 3>> F, M;
+        sim.getFluidImpactOnDynamicBodies(F, M, {{1.0, 1.0, 1.0}});
+        const uint32_t first = 0, count = (uint32_t)nb;
+        double ft[6];
+        dfsph::check(sim.handle(), dfsph_body_wrench(sim.handle(), 1, &first, &count, c, ft));
+        for (int a = 0; a < 3; ++a)
+            if (!close(F[0][a], ft[a], 1e-9) || !close(M[0][a], ft[3 + a], 1e-9)) return fail("wrench");
+        if (!(F[0][1] < 0.0)) return fail("the fluid pushes the walls down");
+        std::vector<std::array<double, 3>> F2, M2;
+        sim.getFluidImpactOnDynamicBodies(F2, M2, {{0.5, 1.0, 2.0}});
+        if (!close(F2[0][0], 0.5 * F[0][0], 1e-12) || !close(F2[0][1], F[0][1], 1e-12) ||
+            !close(F2[0][2], 2.0 * F[0][2], 1e-12))
+            return fail("reduction factor");
+
+        // handleSimulationSave / zeroFluidVelocities / handleSimulationLoad
+        std::vector<float> x0, v0, x1, v1, x2, v2;
+        sim.m_data.readDynamicData(x0, v0);
+        sim.fluid_files_folder = argv[2];
+        sim.handleSimulationSave(true, false, true);
+        sim.zeroFluidVelocities();
+        sim.m_data.readDynamicData(x1, v1);
+        if (x1 != x0) return fail("zeroFluidVelocities keeps the positions");
+        for (float q : v1)
+            if (q != 0.0f) return fail("zeroFluidVelocities");
+        sim.handleSimulationLoad(true, true, false, false, false);
+        sim.m_data.readDynamicData(x2, v2);
+        if (x2.size() != x0.size()) return fail("loaded count");
+        for (size_t k = 0; k < x0.size(); ++k)
+            if (!close(x2[k], x0[k], 1e-6) || !close(v2[k], v0[k], 1e-6)) return fail("load round trip");
+
+        // updateTimeStepDuration
+        sim.updateTimeStepDuration(0.00125);
+        if (sim.get("time_step") != 0.00125) return fail("updateTimeStepDuration");
+        sim.step();
+        std::cout << "ok: force " << F[0][0] << " " << F[0][1] << " " << F[0][2] << "\n";
+    } catch (const dfsph::Error& e) {
+        std::cerr << e.what() << "\n";
+        return 3;
+    }
+    return 0;
+}

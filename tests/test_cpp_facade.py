@@ -148,3 +148,22 @@ def test_timestep_facade_from_json_matches_python_facade(tmp_path, cuda_lib):
         tv += st.iterations_v
     assert (its, itv) == (ti, tv)
     assert np.array_equal(x, d.positions()) and np.array_equal(v, d.velocities())
+
+
+@pytest.mark.gpu
+def test_host_operations(tmp_path, cuda_lib):
+    """tests/cpp/host_ops_demo.cpp: the reference's host-side DFSPHCUDA operations through the facade
+    (snapshot save and load, zeroFluidVelocities, updateTimeStepDuration, the fluid's impact on a
+    dynamic body with reduction factors against dfsph_body_wrench); the program checks itself."""
+    _capi.load()
+    exe = tmp_path / "host_ops_demo"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"),
+                    str(ROOT / "tests" / "cpp" / "host_ops_demo.cpp"), "-L", str(LIBDIR), "-ldfsph_b200",
+                    f"-Wl,-rpath,{LIBDIR}", "-o", str(exe)], check=True)
+    s = synthetic_scene(1, counts=(10, 10, 10))
+    write_scene(tmp_path / "s.bin", s)
+    folder = tmp_path / "snap"
+    folder.mkdir()
+    r = subprocess.run([str(exe), str(tmp_path / "s.bin"), str(folder) + "/"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert (folder / "fluid_file.txt").exists() and (folder / "boundaries_file.txt").exists()
