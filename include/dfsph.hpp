@@ -21,6 +21,7 @@
 #define DFSPH_HPP
 
 #include <array>
+#include <cmath>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -241,13 +242,52 @@ public:
         if (dfsph_dynamic_window_displacement(ctx_, d) != DFSPH_OK) d[0] = d[1] = d[2] = 0.0;
         return {window_center_[0] + d[0], window_center_[1] + d[1], window_center_[2] + d[2]};
     }
-    /* Dynamic bodies as ranges of the boundary (upload order) with their centres, for
-     * getFluidImpactOnDynamicBodies (needs set("boundary_forces", 1)). */
+    /* Dynamic bodies as ranges of the boundary (upload order): the centre of their samples as
+     * uploaded (rest_position) and their current position, for updateRigidBodies and
+     * getFluidImpactOnDynamicBodies (which needs set("boundary_forces", 1)). */
     struct DynamicBody {
         uint32_t first, count;
         std::array<double, 3> position;
+        std::array<double, 3> rest_position;
     };
     std::vector<DynamicBody> dynamic_bodies;
+    void addDynamicBody(uint32_t first, uint32_t count, const std::array<double, 3>& center) {
+        dynamic_bodies.push_back({first, count, center, center});
+    }
+    /* The state the reference's rigid-body solver hands back each step (DynamicBody: position,
+     * velocity, orientation q = (w, x, y, z), angular velocity). */
+    struct DynamicBodyState {
+        std::array<double, 3> position, velocity, angular_velocity;
+        std::array<double, 4> q;
+    };
+    /* updateRigidBodies (DFSPHCData::update_solids; update_dynamicObject_UnifiedParticleSet_cuda,
+     * DFSPH_core_cuda.cu:3407-3449): body b's samples go to R(q) (x0 - rest) + position with the rigid
+     * velocity field v + w x (x - position), on the device. */
+    void updateRigidBodies(const std::vector<DynamicBodyState>& states) {
+        if (states.size() != dynamic_bodies.size()) throw Error(DFSPH_E_INVALID, "one state per dynamic body");
+        for (size_t b = 0; b < states.size(); ++b) {
+            DynamicBody& body = dynamic_bodies[b];
+            const DynamicBodyState& st = states[b];
+            const double w = st.q[0], x = st.q[1], y = st.q[2], z = st.q[3];
+            const double len = std::sqrt(w * w + x * x + y * y + z * z);
+            if (!(len > 0)) throw Error(DFSPH_E_INVALID, "quaternion must be non-zero");
+            const double qw = w / len, qx = x / len, qy = y / len, qz = z / len;
+            const double R[9] = {1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qw * qz), 2 * (qx * qz + qw * qy),
+                                 2 * (qx * qy + qw * qz), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qw * qx),
+                                 2 * (qx * qz - qw * qy), 2 * (qy * qz + qw * qx), 1 - 2 * (qx * qx + qy * qy)};
+            const std::array<double, 3>& c = body.rest_position;
+            double arm[3], p[3], v[3];  // x = R x0 + p with p = position - R c; v passed about p
+            for (int i = 0; i < 3; ++i) arm[i] = R[3 * i] * c[0] + R[3 * i + 1] * c[1] + R[3 * i + 2] * c[2];
+            for (int i = 0; i < 3; ++i) p[i] = st.position[i] - arm[i];
+            const std::array<double, 3>& om = st.angular_velocity;
+            v[0] = st.velocity[0] - (om[1] * arm[2] - om[2] * arm[1]);
+            v[1] = st.velocity[1] - (om[2] * arm[0] - om[0] * arm[2]);
+            v[2] = st.velocity[2] - (om[0] * arm[1] - om[1] * arm[0]);
+            const double q4[4] = {qw, qx, qy, qz};
+            check(ctx_, dfsph_move_boundary_rigid(ctx_, body.first, body.count, q4, p, v, om.data()));
+            body.position = st.position;
+        }
+    }
     /* getFluidImpactOnDynamicBodies (compute_fluid_impact_on_dynamic_body_kernel,
      * DFSPH_memory_management_cuda.cu:688-705): per body, the sum of its particles' fluid forces
      * multiplied component-wise by the body's reduction factor, and the moment of those forces about

@@ -1,7 +1,8 @@
 // host_ops_demo.cpp — the host-side operations of the reference's SPH::DFSPHCUDA through the C++
 // facade (include/dfsph.hpp): handleSimulationSave / handleSimulationLoad, zeroFluidVelocities,
-// updateTimeStepDuration and getFluidImpactOnDynamicBodies. Test program: tests/test_cpp_facade.py
-// writes the scene, runs this and reads its exit code; the checks are made here.
+// updateTimeStepDuration, updateRigidBodies and getFluidImpactOnDynamicBodies. Test program:
+// tests/test_cpp_facade.py writes the scene, runs this and reads its exit code; the checks are made
+// here.
 //
 //   host_ops_demo <scene.bin> <folder/>
 //
@@ -55,7 +56,7 @@ int main(int argc, char** argv) {
 
         // getFluidImpactOnDynamicBodies: the whole boundary as one body, against dfsph_body_wrench
         const double c[3] = {0.5, 0.25, 0.5};
-        sim.dynamic_bodies = {{0u, (uint32_t)nb, {c[0], c[1], c[2]}}};
+        sim.addDynamicBody(0u, (uint32_t)nb, {c[0], c[1], c[2]});
         std::vector<std::array<double, 3>> F, M;
         sim.getFluidImpactOnDynamicBodies(F, M, {{1.0, 1.0, 1.0}});
         const uint32_t first = 0, count = (uint32_t)nb;
@@ -85,6 +86,17 @@ int main(int argc, char** argv) {
         if (x2.size() != x0.size()) return fail("loaded count");
         for (size_t k = 0; k < x0.size(); ++k)
             if (!close(x2[k], x0[k], 1e-6) || !close(v2[k], v0[k], 1e-6)) return fail("load round trip");
+
+        // updateRigidBodies: the whole boundary translated by 1 mm, no rotation, at rest
+        std::vector<double> b0(3 * (size_t)nb), b1(3 * (size_t)nb);
+        dfsph::check(sim.handle(), dfsph_download(sim.handle(), DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F64, b0.data(),
+                                                  b0.size(), DFSPH_ORDER_ID));
+        sim.updateRigidBodies({{{c[0] + 0.001, c[1], c[2]}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {1.0, 0.0, 0.0, 0.0}}});
+        dfsph::check(sim.handle(), dfsph_download(sim.handle(), DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F64, b1.data(),
+                                                  b1.size(), DFSPH_ORDER_ID));
+        for (size_t k = 0; k < b0.size(); ++k)
+            if (!close(b1[k], b0[k] + (k % 3 == 0 ? 0.001 : 0.0), 1e-6)) return fail("updateRigidBodies");
+        if (sim.dynamic_bodies[0].position[0] != c[0] + 0.001) return fail("body position");
 
         // updateTimeStepDuration
         sim.updateTimeStepDuration(0.00125);
