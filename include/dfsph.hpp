@@ -295,18 +295,9 @@ public:
     void getFluidImpactOnDynamicBodies(std::vector<std::array<double, 3>>& sph_forces,
                                        std::vector<std::array<double, 3>>& sph_moments,
                                        const std::vector<std::array<double, 3>>& reduction_factors) {
-        uint32_t nb = 0;
-        {
-            double v = 0;
-            check(ctx_, dfsph_get_param(ctx_, "num_boundary", &v));
-            nb = (uint32_t)v;
-        }
-        std::vector<double> f(3 * (size_t)nb), x(3 * (size_t)nb);
-        if (nb) {
-            check(ctx_, dfsph_download(ctx_, DFSPH_F_BOUNDARY_FORCE, DFSPH_DTYPE_F64, f.data(), f.size(), DFSPH_ORDER_ID));
-            check(ctx_, dfsph_download(ctx_, DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F64, x.data(), x.size(),
-                                       DFSPH_ORDER_ID));
-        }
+        std::vector<double> f, x;
+        boundary_force_and_position(f, x);
+        const size_t nb = f.size() / 3;
         for (size_t b = 0; b < dynamic_bodies.size(); ++b) {
             const DynamicBody& body = dynamic_bodies[b];
             if ((uint64_t)body.first + body.count > nb) throw Error(DFSPH_E_INVALID, "dynamic body beyond the boundary");
@@ -329,6 +320,36 @@ public:
         }
     }
 
+    /* getFluidBoyancyOnDynamicBodies (compute_fluid_Boyancy_on_dynamic_body_cuda,
+     * DFSPH_memory_management_cuda.cu:729-776): per body, the vertical component of its particles'
+     * fluid forces as the buoyancy (0, sum F_y, 0) and the point where it applies, the particles'
+     * positions weighted by |F_y|; both zero when no particle feels a vertical force. */
+    void getFluidBoyancyOnDynamicBodies(std::vector<std::array<double, 3>>& forces,
+                                        std::vector<std::array<double, 3>>& pts_appli) {
+        std::vector<double> f, x;
+        boundary_force_and_position(f, x);
+        for (const DynamicBody& body : dynamic_bodies) {
+            if ((uint64_t)body.first + body.count > f.size() / 3)
+                throw Error(DFSPH_E_INVALID, "dynamic body beyond the boundary");
+            double fy = 0, wsum = 0, p[3] = {0, 0, 0};
+            for (uint32_t i = body.first; i < body.first + body.count; ++i) {
+                const double b = f[3 * (size_t)i + 1], a = std::fabs(b);
+                if (a > 0) {
+                    wsum += a;
+                    fy += b;
+                    for (int k = 0; k < 3; ++k) p[k] += x[3 * (size_t)i + k] * a;
+                }
+            }
+            if (std::fabs(fy) > 0) {
+                forces.push_back({0.0, fy, 0.0});
+                pts_appli.push_back({p[0] / wsum, p[1] / wsum, p[2] / wsum});
+            } else {
+                forces.push_back({0.0, 0.0, 0.0});
+                pts_appli.push_back({0.0, 0.0, 0.0});
+            }
+        }
+    }
+
     const dfsph_step_stats& lastStats() const { return stats_; }
     dfsph_ctx* handle() const { return ctx_; }
     /* Any dfsph_set_param / dfsph_get_param key (e.g. "learned_warm_start", "boundary_forces"). */
@@ -343,6 +364,18 @@ public:
     unsigned int m_iterations = 0, m_iterationsV = 0;
 
 private:
+    // The fluid's force on every boundary particle during the last step and the particles' positions,
+    // 3 FP64 values each in upload order.
+    void boundary_force_and_position(std::vector<double>& f, std::vector<double>& x) const {
+        double v = 0;
+        check(ctx_, dfsph_get_param(ctx_, "num_boundary", &v));
+        const size_t nb = (size_t)v;
+        f.assign(3 * nb, 0.0);
+        x.assign(3 * nb, 0.0);
+        if (!nb) return;
+        check(ctx_, dfsph_download(ctx_, DFSPH_F_BOUNDARY_FORCE, DFSPH_DTYPE_F64, f.data(), f.size(), DFSPH_ORDER_ID));
+        check(ctx_, dfsph_download(ctx_, DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F64, x.data(), x.size(), DFSPH_ORDER_ID));
+    }
 
     dfsph_ctx* ctx_ = nullptr;
     dfsph_step_stats stats_{};

@@ -1,6 +1,7 @@
 // host_ops_demo.cpp — the host-side operations of the reference's SPH::DFSPHCUDA through the C++
 // facade (include/dfsph.hpp): handleSimulationSave / handleSimulationLoad, zeroFluidVelocities,
-// updateTimeStepDuration, updateRigidBodies and getFluidImpactOnDynamicBodies. Test program:
+// updateTimeStepDuration, updateRigidBodies, getFluidImpactOnDynamicBodies and
+// getFluidBoyancyOnDynamicBodies. Test program:
 // tests/test_cpp_facade.py writes the scene, runs this and reads its exit code; the checks are made
 // here.
 //
@@ -8,6 +9,7 @@
 //
 // scene.bin as for facade_demo. Exit codes: 0 ok, 1 a check failed (message on stderr), 2 usage /
 // input error, 3 dfsph::Error.
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdio>
@@ -70,6 +72,19 @@ int main(int argc, char** argv) {
         if (!close(F2[0][0], 0.5 * F[0][0], 1e-12) || !close(F2[0][1], F[0][1], 1e-12) ||
             !close(F2[0][2], 2.0 * F[0][2], 1e-12))
             return fail("reduction factor");
+
+        // getFluidBoyancyOnDynamicBodies: the vertical force, applied inside the box of the samples
+        std::vector<std::array<double, 3>> B, P;
+        sim.getFluidBoyancyOnDynamicBodies(B, P);
+        if (B[0][0] != 0.0 || B[0][2] != 0.0 || !close(B[0][1], F[0][1], 1e-9)) return fail("buoyancy force");
+        for (int a = 0; a < 3; ++a) {
+            float lo = boundary[a], hi = boundary[a];
+            for (size_t k = a; k < boundary.size(); k += 3) {
+                lo = std::min(lo, boundary[k]);
+                hi = std::max(hi, boundary[k]);
+            }
+            if (!(P[0][a] >= lo && P[0][a] <= hi)) return fail("buoyancy point");
+        }
 
         // handleSimulationSave / zeroFluidVelocities / handleSimulationLoad
         std::vector<float> x0, v0, x1, v1, x2, v2;
