@@ -453,6 +453,18 @@ int dfsph_dynamic_window_init(dfsph_ctx* ctx, const double* lo, const double* hi
                               uint32_t wall_count, const float* rest_xyz, uint32_t n_rest);
 int dfsph_dynamic_window_shift(dfsph_ctx* ctx, const double* displacement, double allowed_distance,
                                double allowed_density, uint32_t* added, uint32_t* removed);
+/* DFSPHCData::computeFluidLevel (find_fluid_height_cuda, SPH_other_systems_cuda.cu:149-260): per
+ * column of cells (x, z), the cells are read from the top down until at least three particles have
+ * been seen and the column's height is the middle one of the three highest (a lone splash does not
+ * count); *level is the highest column's (-1: no column holds three particles). Computed on the host
+ * from the device's binning; synchronises the context's stream. */
+int dfsph_fluid_level(dfsph_ctx* ctx, double* level);
+/* DFSPHCData::handleFLuidLevelControl (control_fluid_height_cuda, :414-440), between steps: when the
+ * level is more than 5 cm above target (> 0), the particles above target are removed (stable, ids
+ * renumbered densely); *removed (nullable) receives their count. Raising a low level (the reference
+ * places new particles above the columns) is not offered: the call then changes nothing. */
+int dfsph_fluid_level_control(dfsph_ctx* ctx, double target, uint32_t* removed);
+
 /* DynamicWindowInterface::stabilizeFluid, method 0 (DynamicWindow.cu:3160-3700), between steps after
  * dfsph_dynamic_window_shift: `iterations` steps of the fixed time step `time_step` (the reference's
  * default: 5 steps of 3 ms) with kappa and kappa_v cleared before and after; each runs the neighbour

@@ -315,6 +315,52 @@ def surface_eval(surface, points):
     return inside.astype(bool), normal
 
 
+def fluid_level(positions, particle_radius: float, grid_offset, grid_dims) -> float:
+    """DFSPHCData::computeFluidLevel restated on the CPU (pure Python, small cases).
+
+    find_splashless_column_max_height_kernel (SPlisHSPlasH/DFSPH/SPH_other_systems_cuda.cu:144-187):
+    for every column (x, z) of the cell grid, the cells are read from the top (y = dims - 1) down; every
+    particle of a cell is inserted into an ascending array of the three highest heights (initially
+    -2); after a cell, the walk stops once more than two particles have been seen. The column's height
+    is the middle entry when more than two were seen, else -2. find_fluid_height_cuda (:192-260): the
+    level is the highest column height, starting from -1. Cells: floor(x / (4 r) + offset) in FP32.
+    """
+    x = np.asarray(positions, np.float32).reshape(-1, 3)
+    H = np.float32(4.0 * particle_radius)
+    off = np.asarray(grid_offset, np.float32).reshape(3)
+    dims = [int(d) for d in grid_dims]
+    cells: dict[tuple[int, int, int], list[float]] = {}
+    for p in x:
+        c = np.floor(p / H + off).astype(np.int64)
+        if np.any(c < 0) or c[0] >= dims[0] or c[1] >= dims[1] or c[2] >= dims[2]:
+            continue
+        cells.setdefault((int(c[0]), int(c[1]), int(c[2])), []).append(float(p[1]))
+    columns: dict[tuple[int, int], list[int]] = {}
+    for (cx, cy, cz) in cells:
+        columns.setdefault((cx, cz), []).append(cy)
+    ranking = -1.0
+    for (cx, cz), ys in columns.items():
+        top = [-2.0, -2.0, -2.0]
+        count = 0
+        for cy in sorted(ys, reverse=True):
+            for h in cells[(cx, cy, cz)]:
+                count += 1
+                sup = -1
+                for k in range(3):
+                    if h > top[k]:
+                        sup = k
+                if sup > -1:
+                    for k in range(sup):
+                        top[k] = top[k + 1]
+                    top[sup] = h
+            if count > 2:
+                break
+        col = top[1] if count > 2 else -2.0
+        if ranking < col:
+            ranking = col
+    return ranking
+
+
 def kernel_values(H: float, r: np.ndarray, precision: int = 32):
     lib = _load()
     r = np.ascontiguousarray(r, dtype=np.float64)

@@ -1221,6 +1221,101 @@ public:
         return DFSPH_OK;
     }
 
+    // DFSPHCData::computeFluidLevel (find_fluid_height_cuda, SPH_other_systems_cuda.cu:149-260): per
+    // column of cells (x, z), the cells are read from the top down until at least three particles
+    // have been seen; the column's height is the middle one of the three highest (a lone splash
+    // particle above the surface does not count); the level is the highest column's. Columns of
+    // fewer than three particles count -2; no such column at all gives -1; particles off the grid are
+    // not read. On the host, from the positions and the cells of the device's binning (FP32,
+    // floor(x / H + offset)).
+    int fluid_level(double* out) {
+        DF_CHECK(out, DFSPH_E_INVALID, "null output");
+        *out = -1.0;
+        if (!n || !grid_ready) return DFSPH_OK;
+        std::vector<Vec4<Real>> hp(n);
+        DF_CUDA(cudaMemcpyAsync(hp.data(), pos[cur], (size_t)n * sizeof(Vec4<Real>), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        const float H = (float)(4.0 * sc.particle_radius);
+        struct Cell {
+            int64_t column;
+            int32_t y;
+            Real h;
+        };
+        std::vector<Cell> cells;
+        cells.reserve(n);
+        for (const Vec4<Real>& q : hp) {
+            const float x = (float)q.x, y = (float)q.y, z = (float)q.z;
+            if (!(std::isfinite(x) && std::isfinite(y) && std::isfinite(z))) continue;
+            const int cx = (int)std::floor(x / H + (float)off[0]), cy = (int)std::floor(y / H + (float)off[1]),
+                      cz = (int)std::floor(z / H + (float)off[2]);
+            if (cx < 0 || cy < 0 || cz < 0 || cx >= dim[0] || cy >= dim[1] || cz >= dim[2]) continue;  // off the grid
+            cells.push_back({(int64_t)cz * (int64_t)(1 << 30) + cx, cy, q.y});
+        }
+        std::sort(cells.begin(), cells.end(), [](const Cell& a, const Cell& b) {
+            return a.column != b.column ? a.column < b.column : a.y > b.y;
+        });
+        double level = -1.0;
+        for (size_t a = 0; a < cells.size();) {
+            size_t b = a;
+            while (b < cells.size() && cells[b].column == cells[a].column) ++b;
+            Real top[3] = {Real(-2), Real(-2), Real(-2)};  // ascending, as the reference keeps them
+            int count = 0;
+            for (size_t c = a; c < b;) {
+                size_t e = c;
+                while (e < b && cells[e].y == cells[c].y) ++e;  // one cell
+                for (size_t k = c; k < e; ++k) {
+                    ++count;
+                    int sup = -1;
+                    for (int m = 0; m < 3; ++m)
+                        if (cells[k].h > top[m]) sup = m;
+                    if (sup > -1) {
+                        for (int m = 0; m < sup; ++m) top[m] = top[m + 1];
+                        top[sup] = cells[k].h;
+                    }
+                }
+                c = e;
+                if (count > 2) break;
+            }
+            const double col = count > 2 ? (double)top[1] : -2.0;
+            if (col > level) level = col;
+            a = b;
+        }
+        *out = level;
+        return DFSPH_OK;
+    }
+
+    // DFSPHCData::handleFLuidLevelControl (control_fluid_height_cuda, SPH_other_systems_cuda.cu:
+    // 414-440): when the level is more than 5 cm above the target, the particles above the target are
+    // removed (y > target, the target rounded to FP32; stable compaction, ids renumbered densely).
+    // Raising a low level (the reference places
+    // a lattice of new particles above the columns) is not offered: the call then changes nothing.
+    int fluid_level_control(double target, uint32_t* removed) {
+        if (removed) *removed = 0;
+        if (!(target > 0) || !n) return DFSPH_OK;
+        double level = 0;
+        DF_TRY(fluid_level(&level));
+        if (std::fabs(level - target) < 0.05 || level < target) return DFSPH_OK;
+        DF_TRY(ensure_scan_scratch());
+        const float lo[3] = {-3.0e38f, -3.0e38f, -3.0e38f}, hi[3] = {3.0e38f, (float)target, 3.0e38f};
+        DF_CUDA(cudaMemsetAsync(status + 3, 0, sizeof(uint32_t), stream));
+        launch_box_tag<Real>(pos[cur], n, lo, hi, sb.keys_a, status + 3, stream);
+        DF_CUDA(cudaMemcpyAsync(h_status + 3, status + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        DF_CUDA(cudaStreamSynchronize(stream));
+        launches += 1;
+        const uint32_t n_rm = h_status[3];
+        if (n_rm) {
+            exclusive_scan_u32(sb.keys_a, sb.vals_a, n, ob_scan, ob_total, stream);
+            launches += 3;
+            DF_TRY(compact_fluid(sb.keys_a, sb.vals_a, n - n_rm));
+            invalidate_graphs();
+            DF_TRY(sync_state());
+            DF_CUDA(cudaStreamSynchronize(stream));
+            DF_CUDA(cudaGetLastError());
+        }
+        if (removed) *removed = n_rm;
+        return DFSPH_OK;
+    }
+
     int dynamic_window_state(double* displacement) {
         DF_CHECK(displacement, DFSPH_E_INVALID, "null output");
         DF_CHECK(dw_ready, DFSPH_E_STATE, "dynamic window not initialised (dfsph_dynamic_window_init)");
@@ -2958,6 +3053,10 @@ int dfsph_dynamic_window_shift(dfsph_ctx* ctx, const double* displacement, doubl
 int dfsph_dynamic_window_stabilize(dfsph_ctx* ctx, uint32_t iterations, double time_step, double damping,
                                    int tagged_only) {
     DFSPH_DISPATCH(ctx, dynamic_window_stabilize(iterations, time_step, damping, tagged_only));
+}
+int dfsph_fluid_level(dfsph_ctx* ctx, double* level) { DFSPH_DISPATCH(ctx, fluid_level(level)); }
+int dfsph_fluid_level_control(dfsph_ctx* ctx, double target, uint32_t* removed) {
+    DFSPH_DISPATCH(ctx, fluid_level_control(target, removed));
 }
 int dfsph_dynamic_window_displacement(dfsph_ctx* ctx, double* displacement) {
     DFSPH_DISPATCH(ctx, dynamic_window_state(displacement));

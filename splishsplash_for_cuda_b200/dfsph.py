@@ -423,6 +423,19 @@ class DFSPHCUDA:
         self._call(self._lib.dfsph_dynamic_window_stabilize(self._ctx, int(iterations), float(time_step),
                                                             float(damping), 1 if tagged_only else 0))
 
+    def fluid_level(self) -> float:
+        """DFSPHCData::computeFluidLevel: the highest splash-free column height (-1: none)."""
+        v = C.c_double()
+        self._call(self._lib.dfsph_fluid_level(self._ctx, C.byref(v)))
+        return v.value
+
+    def fluid_level_control(self, target: float) -> int:
+        """DFSPHCData::handleFLuidLevelControl: removes the particles above target when the level is
+        more than 5 cm above it; returns how many."""
+        r = C.c_uint32()
+        self._call(self._lib.dfsph_fluid_level_control(self._ctx, float(target), C.byref(r)))
+        return r.value
+
     def dynamic_window_displacement(self) -> np.ndarray:
         out = np.zeros(3, np.float64)
         self._call(self._lib.dfsph_dynamic_window_displacement(self._ctx, out.ctypes.data))

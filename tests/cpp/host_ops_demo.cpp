@@ -1,7 +1,7 @@
 // host_ops_demo.cpp — the host-side operations of the reference's SPH::DFSPHCUDA through the C++
 // facade (include/dfsph.hpp): handleSimulationSave / handleSimulationLoad, zeroFluidVelocities,
-// updateTimeStepDuration, updateRigidBodies, getFluidImpactOnDynamicBodies and
-// getFluidBoyancyOnDynamicBodies. Test program:
+// updateTimeStepDuration, updateRigidBodies, getFluidImpactOnDynamicBodies,
+// getFluidBoyancyOnDynamicBodies, getFluidLevel and handleFLuidLevelControl. Test program:
 // tests/test_cpp_facade.py writes the scene, runs this and reads its exit code; the checks are made
 // here.
 //
@@ -112,6 +112,20 @@ int main(int argc, char** argv) {
         for (size_t k = 0; k < b0.size(); ++k)
             if (!close(b1[k], b0[k] + (k % 3 == 0 ? 0.001 : 0.0), 1e-6)) return fail("updateRigidBodies");
         if (sim.dynamic_bodies[0].position[0] != c[0] + 0.001) return fail("body position");
+
+        // getFluidLevel / handleFLuidLevelControl: a target above the level changes nothing, one 5 cm
+        // below it removes every particle above it
+        const double level = sim.getFluidLevel();
+        if (!(level > 0.0)) return fail("getFluidLevel");
+        const uint32_t n_before = sim.m_data.getFluidParticlesCount();
+        sim.handleFLuidLevelControl(level + 0.5);
+        if (sim.m_data.getFluidParticlesCount() != n_before) return fail("level control above the level");
+        sim.handleFLuidLevelControl(level - 0.06);
+        std::vector<float> x3, v3;
+        sim.m_data.readDynamicData(x3, v3);
+        if (!(sim.m_data.getFluidParticlesCount() < n_before)) return fail("level control removal");
+        for (size_t k = 1; k < x3.size(); k += 3)
+            if (x3[k] > (float)(level - 0.06)) return fail("a particle above the target remains");
 
         // updateTimeStepDuration
         sim.updateTimeStepDuration(0.00125);

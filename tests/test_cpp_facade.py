@@ -154,7 +154,8 @@ def test_timestep_facade_from_json_matches_python_facade(tmp_path, cuda_lib):
 def test_host_operations(tmp_path, cuda_lib):
     """tests/cpp/host_ops_demo.cpp: the reference's host-side DFSPHCUDA operations through the facade
     (snapshot save and load, zeroFluidVelocities, updateTimeStepDuration, the fluid's impact on a
-    dynamic body with reduction factors against dfsph_body_wrench); the program checks itself."""
+    dynamic body with reduction factors against dfsph_body_wrench, the fluid level and its control);
+    the program checks itself."""
     _capi.load()
     exe = tmp_path / "host_ops_demo"
     subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"),
