@@ -217,14 +217,14 @@ public:
         if (!x.empty()) check(ctx_, dfsph_update_fluid(ctx_, x.data(), nullptr));
     }
     /* getFluidLevel / handleFLuidLevelControl (DFSPH_CUDA.cpp:4150-4160; dfsph_fluid_level,
-     * dfsph_fluid_level_control: only lowering a high level is offered). */
+     * dfsph_fluid_level_control). */
     double getFluidLevel() const {
         double v = -1;
         check(ctx_, dfsph_fluid_level(ctx_, &v));
         return v;
     }
     void handleFLuidLevelControl(double level) {
-        if (level > 0) check(ctx_, dfsph_fluid_level_control(ctx_, level, nullptr));
+        if (level > 0) check(ctx_, dfsph_fluid_level_control(ctx_, level, nullptr, nullptr));
     }
     /* updateTimeStepDuration: the time step used while the CFL condition is off. */
     void updateTimeStepDuration(double duration) { set("time_step", duration); }

@@ -459,11 +459,16 @@ int dfsph_dynamic_window_shift(dfsph_ctx* ctx, const double* displacement, doubl
  * count); *level is the highest column's (-1: no column holds three particles). Computed on the host
  * from the device's binning; synchronises the context's stream. */
 int dfsph_fluid_level(dfsph_ctx* ctx, double* level);
-/* DFSPHCData::handleFLuidLevelControl (control_fluid_height_cuda, :414-440), between steps: when the
- * level is more than 5 cm above target (> 0), the particles above target are removed (stable, ids
- * renumbered densely); *removed (nullable) receives their count. Raising a low level (the reference
- * places new particles above the columns) is not offered: the call then changes nothing. */
-int dfsph_fluid_level_control(dfsph_ctx* ctx, double target, uint32_t* removed);
+/* DFSPHCData::handleFLuidLevelControl (control_fluid_height_cuda, :414-547), between steps; nothing
+ * when the level is within 5 cm of target (> 0). Above it, the particles above target are removed
+ * (stable, ids renumbered densely). Below it, a lattice of new particles (spacing 2r, layers 0.8 * 2r
+ * apart, floor((target - level) / 2r) + 1 layers) spanning the domain box taken from the first and
+ * last ten boundary particles in the reference's boundary order (shrunk by 2r) is placed, outside the
+ * box's central third in x or z, each point lifted to its column's highest fluid particle + 2.5 r;
+ * appended at rest with the inflow mass, in lattice order (ids n, n + 1, ...); past fluid_capacity
+ * the rest is dropped and DFSPH_ST_FLUID_CAPACITY set. *removed / *added (nullable) receive the
+ * counts. */
+int dfsph_fluid_level_control(dfsph_ctx* ctx, double target, uint32_t* removed, uint32_t* added);
 
 /* DynamicWindowInterface::stabilizeFluid, method 0 (DynamicWindow.cu:3160-3700), between steps after
  * dfsph_dynamic_window_shift: `iterations` steps of the fixed time step `time_step` (the reference's

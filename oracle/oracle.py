@@ -361,6 +361,84 @@ def fluid_level(positions, particle_radius: float, grid_offset, grid_dims) -> fl
     return ranking
 
 
+def column_tops(positions, particle_radius: float, grid_offset, grid_dims) -> dict:
+    """find_column_max_height_kernel (SPlisHSPlasH/DFSPH/SPH_other_systems_cuda.cu:292-318): per column
+    (x, z) the highest particle of its top occupied cell, as float32."""
+    x = np.asarray(positions, np.float32).reshape(-1, 3)
+    H = np.float32(4.0 * particle_radius)
+    off = np.asarray(grid_offset, np.float32).reshape(3)
+    dims = [int(d) for d in grid_dims]
+    best: dict[tuple[int, int], tuple[int, np.float32]] = {}
+    for p in x:
+        c = np.floor(p / H + off).astype(np.int64)
+        if np.any(c < 0) or c[0] >= dims[0] or c[1] >= dims[1] or c[2] >= dims[2]:
+            continue
+        key = (int(c[0]), int(c[2]))
+        cy, h = int(c[1]), np.float32(p[1])
+        cur = best.get(key)
+        if cur is None or cy > cur[0]:
+            best[key] = (cy, max(np.float32(-2.0), h))
+        elif cy == cur[0] and h > cur[1]:
+            best[key] = (cy, h)
+    return {k: v[1] for k, v in best.items()}
+
+
+def fluid_level_raise(fluid_positions, boundary_positions, particle_radius: float, grid_offset, grid_dims,
+                      target: float, level: float) -> np.ndarray:
+    """The particles the raising branch of control_fluid_height_cuda places (float32, lattice order).
+
+    SPlisHSPlasH/DFSPH/SPH_other_systems_cuda.cu: get_min_max_pos_kernel (:282-304) on the boundary
+    in the reference's order (stable by the linear cell index x + 256 z + 65536 y; boundary_positions
+    in upload order), the host's lattice size (:486-516), place_additional_particles_right_above_kernel
+    (:321-408) with border_range = width / 3 (y 0), in its FP32 / FP64 operation order.
+    """
+    f32, f64 = np.float32, float
+    b = np.asarray(boundary_positions, np.float32).reshape(-1, 3)
+    H = f32(4.0 * particle_radius)
+    off = np.asarray(grid_offset, np.float32).reshape(3)
+    cells = np.floor(b / H + off).astype(np.int64)
+    order = sorted(range(len(b)), key=lambda k: (cells[k][1], cells[k][2], cells[k][0]))
+    mn = b[order[0]].copy()
+    mx = b[order[-1]].copy()
+    for k in range(min(10, len(b))):
+        mn = np.minimum(mn, b[order[k]])
+        mx = np.maximum(mx, b[order[len(b) - 1 - k]])
+    r = f32(particle_radius)
+    p = f32(r * f32(2))
+    mn = (mn + f32(2) * r).astype(np.float32)
+    mx = (mx - f32(2) * r).astype(np.float32)
+    width = (mx - mn).astype(np.float32)
+    host_x = f32(np.floor(width[0] / p) + f32(1))
+    host_z = f32(np.floor(width[2] / p) + f32(1))
+    layers = f32(np.floor((f32(target) - f32(level)) / p) + f32(1))
+    want = int(f32(f32(host_x * layers) * host_z))
+    cw_x = f32(np.floor(abs(width[0]) / p) + f32(1))
+    cw_z = f32(np.floor(abs(width[2]) / p) + f32(1))
+    border = np.array([width[0] / f32(3), 0, width[2] / f32(3)], np.float32)
+    bordered = f32(border[0] * border[0]) + f32(border[2] * border[2]) > 0
+    tops = column_tops(fluid_positions, particle_radius, grid_offset, grid_dims)
+    out = []
+    for i in range(want):
+        row = int(f32(f32(i) / cw_x))
+        lev = int(f32(f32(row) / cw_z))
+        lx = f32(f32(f32(i) - f32(f32(row) * cw_x)) * p)
+        ly = f32(f64(lev) * (f64(p) * 0.80))
+        lz = f32(f32(f32(row) - f32(f32(lev) * cw_z)) * p)
+        if lev & 1:
+            lx = f32(lx + f32(p / f32(2)))
+            lz = f32(lz + f32(p / f32(2)))
+        tx, tz = f32(mn[0] + lx), f32(mn[2] + lz)
+        if bordered and not (tx < f32(mn[0] + border[0]) or tz < f32(mn[2] + border[2]) or
+                             tx > f32(mx[0] - border[0]) or tz > f32(mx[2] - border[2])):
+            continue
+        cx = int(np.floor(f32(f32(tx / H) + off[0])))
+        cz = int(np.floor(f32(f32(tz / H) + off[2])))
+        top = tops.get((cx, cz), f32(-2.0))
+        y0 = f32(f64(f32(top + p)) + f64(p) / 4.0)
+        out.append((f32(mn[0] + lx), f32(y0 + ly), f32(mn[2] + lz)))
+    return np.array(out, np.float32).reshape(-1, 3)
+
+
 def kernel_values(H: float, r: np.ndarray, precision: int = 32):
     lib = _load()
     r = np.ascontiguousarray(r, dtype=np.float64)

@@ -162,7 +162,7 @@ SIGNATURES = {
     "dfsph_set_surface_mesh": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32]),
     "dfsph_dynamic_window_stabilize": (C.c_int, [_P, C.c_uint32, C.c_double, C.c_double, C.c_int]),
     "dfsph_fluid_level": (C.c_int, [_P, C.POINTER(C.c_double)]),
-    "dfsph_fluid_level_control": (C.c_int, [_P, C.c_double, C.POINTER(C.c_uint32)]),
+    "dfsph_fluid_level_control": (C.c_int, [_P, C.c_double, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "dfsph_read_obj": (C.c_int, [C.c_char_p, _P, C.c_uint32, C.POINTER(C.c_uint32), _P, C.c_uint32,
                                  C.POINTER(C.c_uint32)]),
     "dfsph_dynamic_window_init": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32]),

@@ -7,6 +7,7 @@
 // static, so several contexts may coexist (the reference keeps statics in cuda_neighborsSearch
 // and cuda_CFL, DFSPH_core_cuda.cu:2653-2663, :3333-3348, and is one instance per process).
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstddef>
@@ -16,6 +17,7 @@
 #include <memory>
 #include <sstream>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "bgeo.h"
@@ -1221,14 +1223,16 @@ public:
         return DFSPH_OK;
     }
 
-    // DFSPHCData::computeFluidLevel (find_fluid_height_cuda, SPH_other_systems_cuda.cu:149-260): per
+    // DFSPHCData::computeFluidLevel (find_fluid_height_cuda, SPH_other_systems_cuda.cu:144-260): per
     // column of cells (x, z), the cells are read from the top down until at least three particles
     // have been seen; the column's height is the middle one of the three highest (a lone splash
     // particle above the surface does not count); the level is the highest column's. Columns of
     // fewer than three particles count -2; no such column at all gives -1; particles off the grid are
     // not read. On the host, from the positions and the cells of the device's binning (FP32,
-    // floor(x / H + offset)).
-    int fluid_level(double* out) {
+    // floor(x / H + offset)). `tops` (nullable) receives each column's highest particle in its top
+    // occupied cell (find_column_max_height_kernel, :292-318), keyed by column_key.
+    static int64_t column_key(int cx, int cz) { return (int64_t)cz * (int64_t)(1 << 30) + cx; }
+    int fluid_level(double* out, std::unordered_map<int64_t, float>* tops = nullptr) {
         DF_CHECK(out, DFSPH_E_INVALID, "null output");
         *out = -1.0;
         if (!n || !grid_ready) return DFSPH_OK;
@@ -1249,7 +1253,7 @@ public:
             const int cx = (int)std::floor(x / H + (float)off[0]), cy = (int)std::floor(y / H + (float)off[1]),
                       cz = (int)std::floor(z / H + (float)off[2]);
             if (cx < 0 || cy < 0 || cz < 0 || cx >= dim[0] || cy >= dim[1] || cz >= dim[2]) continue;  // off the grid
-            cells.push_back({(int64_t)cz * (int64_t)(1 << 30) + cx, cy, q.y});
+            cells.push_back({column_key(cx, cz), cy, q.y});
         }
         std::sort(cells.begin(), cells.end(), [](const Cell& a, const Cell& b) {
             return a.column != b.column ? a.column < b.column : a.y > b.y;
@@ -1258,6 +1262,11 @@ public:
         for (size_t a = 0; a < cells.size();) {
             size_t b = a;
             while (b < cells.size() && cells[b].column == cells[a].column) ++b;
+            if (tops) {  // the top occupied cell's highest particle
+                float t = -2.0f;
+                for (size_t c = a; c < b && cells[c].y == cells[a].y; ++c) t = std::max(t, (float)cells[c].h);
+                (*tops)[cells[a].column] = t;
+            }
             Real top[3] = {Real(-2), Real(-2), Real(-2)};  // ascending, as the reference keeps them
             int count = 0;
             for (size_t c = a; c < b;) {
@@ -1285,16 +1294,18 @@ public:
     }
 
     // DFSPHCData::handleFLuidLevelControl (control_fluid_height_cuda, SPH_other_systems_cuda.cu:
-    // 414-440): when the level is more than 5 cm above the target, the particles above the target are
-    // removed (y > target, the target rounded to FP32; stable compaction, ids renumbered densely).
-    // Raising a low level (the reference places
-    // a lattice of new particles above the columns) is not offered: the call then changes nothing.
-    int fluid_level_control(double target, uint32_t* removed) {
+    // 414-547): nothing when the level is within 5 cm of the target. Above it, the particles above the
+    // target are removed (y > target, the target rounded to FP32; stable compaction, ids renumbered
+    // densely). Below it, new particles are placed above the fluid near the walls (raise_fluid_level).
+    int fluid_level_control(double target, uint32_t* removed, uint32_t* added) {
         if (removed) *removed = 0;
+        if (added) *added = 0;
         if (!(target > 0) || !n) return DFSPH_OK;
         double level = 0;
-        DF_TRY(fluid_level(&level));
-        if (std::fabs(level - target) < 0.05 || level < target) return DFSPH_OK;
+        std::unordered_map<int64_t, float> tops;
+        DF_TRY(fluid_level(&level, &tops));
+        if (std::fabs(level - target) < 0.05) return DFSPH_OK;
+        if (level < target) return raise_fluid_level(target, level, tops, added);
         DF_TRY(ensure_scan_scratch());
         const float lo[3] = {-3.0e38f, -3.0e38f, -3.0e38f}, hi[3] = {3.0e38f, (float)target, 3.0e38f};
         DF_CUDA(cudaMemsetAsync(status + 3, 0, sizeof(uint32_t), stream));
@@ -1313,6 +1324,114 @@ public:
             DF_CUDA(cudaGetLastError());
         }
         if (removed) *removed = n_rm;
+        return DFSPH_OK;
+    }
+
+    // The raising branch of control_fluid_height_cuda (SPH_other_systems_cuda.cu:486-545) with
+    // get_min_max_pos_kernel (:282-304) and place_additional_particles_right_above_kernel (:321-408),
+    // in the reference's FP32/FP64 operation order. The domain box: component-wise min (max) of the
+    // first (last) ten boundary particles in the reference's boundary order (stable by linear cell
+    // index x + 256 z + 65536 y, from the boundary's current positions), shrunk by 2r. A lattice of
+    // spacing 2r spans the box (layers 0.8 * 2r apart, odd layers shifted by r in x and z) with
+    // floor((target - level) / 2r) + 1 layers; only the points outside the central third of the box
+    // (in x or z) are kept, and each is lifted to its column's highest particle + 2.5 r (a column
+    // without fluid counts -2). Appended in lattice order (the reference's atomic counter gives an
+    // arbitrary order), velocity zero, the inflow mass; past fluid_capacity the rest is dropped and
+    // DFSPH_ST_FLUID_CAPACITY is set.
+    int raise_fluid_level(double target, double level, const std::unordered_map<int64_t, float>& tops,
+                          uint32_t* added) {
+        DF_CHECK(nb > 0, DFSPH_E_STATE, "raising the fluid level needs the boundary (the domain's extent)");
+        std::vector<float> b((size_t)nb * 3);
+        DF_TRY(download(DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F32, b.data(), b.size(), DFSPH_ORDER_ID));
+        const float H = (float)(4.0 * sc.particle_radius);
+        std::vector<std::array<int, 3>> key(nb);
+        for (uint32_t k = 0; k < nb; ++k)
+            for (int a = 0; a < 3; ++a) key[k][a] = (int)std::floor(b[3 * k + a] / H + (float)off[a]);
+        std::vector<uint32_t> order(nb);
+        for (uint32_t k = 0; k < nb; ++k) order[k] = k;
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t p, uint32_t q) {
+            const auto &kp = key[p], &kq = key[q];
+            if (kp[1] != kq[1]) return kp[1] < kq[1];
+            if (kp[2] != kq[2]) return kp[2] < kq[2];
+            return kp[0] < kq[0];
+        });
+        float mn[3], mx[3];
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = b[3 * order[0] + a];
+            mx[a] = b[3 * order[nb - 1] + a];
+        }
+        for (uint32_t k = 0; k < 10 && k < nb; ++k)
+            for (int a = 0; a < 3; ++a) {
+                mn[a] = std::min(mn[a], b[3 * order[k] + a]);
+                mx[a] = std::max(mx[a], b[3 * order[nb - 1 - k] + a]);
+            }
+        const float r = (float)sc.particle_radius, p = r * 2.0f;
+        for (int a = 0; a < 3; ++a) {
+            mn[a] += 2.0f * r;
+            mx[a] -= 2.0f * r;
+        }
+        float width[3], count_w[3], border[3];
+        for (int a = 0; a < 3; ++a) {
+            width[a] = mx[a] - mn[a];
+            count_w[a] = std::floor(std::fabs(width[a]) / p) + 1.0f;  // the kernel's |width|
+            border[a] = a == 1 ? 0.0f : width[a] / 3.0f;
+        }
+        // the lattice size as the host computes it (from width itself, y from the missing height)
+        const float host_x = std::floor(width[0] / p) + 1.0f, host_z = std::floor(width[2] / p) + 1.0f;
+        const float layers = std::floor(((float)target - (float)level) / p) + 1.0f;
+        const float want_f = host_x * layers * host_z;
+        if (!(want_f >= 1.0f)) return DFSPH_OK;  // the reference stops the program here
+        DF_CHECK(want_f < 2.0e9f, DFSPH_E_INVALID, "fluid level control: lattice too large");
+        const int want = (int)want_f;
+        const bool bordered = border[0] * border[0] + border[2] * border[2] > 0.0f;
+        std::vector<float> xyz;
+        for (int id = 0; id < want; ++id) {
+            const int row = (int)((float)id / count_w[0]);
+            const int lev = (int)((float)row / count_w[2]);
+            float lx = ((float)id - (float)row * count_w[0]) * p;
+            float ly = (float)((double)lev * ((double)p * 0.80));
+            float lz = ((float)row - (float)lev * count_w[2]) * p;
+            if (lev & 1) {
+                lx += p / 2.0f;
+                lz += p / 2.0f;
+            }
+            const float tx = mn[0] + lx, tz = mn[2] + lz;
+            if (bordered && !(tx < mn[0] + border[0] || tz < mn[2] + border[2] || tx > mx[0] - border[0] ||
+                              tz > mx[2] - border[2]))
+                continue;
+            const int cx = (int)std::floor(tx / H + (float)off[0]), cz = (int)std::floor(tz / H + (float)off[2]);
+            const auto it = tops.find(column_key(cx, cz));
+            const float top = it == tops.end() ? -2.0f : it->second;
+            const float y0 = (float)((double)(top + p) + (double)p / 4.0);
+            xyz.push_back(mn[0] + lx);
+            xyz.push_back(y0 + ly);
+            xyz.push_back(mn[2] + lz);
+        }
+        const uint32_t kept = (uint32_t)(xyz.size() / 3);
+        const uint32_t n_add = std::min<uint32_t>(kept, Nc - n);
+        if (n_add) {
+            DF_CUDA(cudaMemcpyAsync(stage, xyz.data(), (size_t)n_add * 3 * sizeof(float), cudaMemcpyHostToDevice, stream));
+            launch_unpack_fluid<Real>(stage, nullptr, nullptr, new_particle_mass(), n_add, pos[cur] + n, vel[cur] + n,
+                                      kappa[cur] + n, kappaV[cur] + n, id[cur] + n, stream, n);
+            if (learned && kappaT[cur]) {
+                DF_CUDA(cudaMemsetAsync(kappaT[cur] + n, 0, (size_t)n_add * sizeof(Real), stream));
+                DF_CUDA(cudaMemsetAsync(kappaVT[cur] + n, 0, (size_t)n_add * sizeof(Real), stream));
+            }
+            launches += 1;
+            n += n_add;
+            invalidate_graphs();
+            DF_TRY(sync_state());
+        }
+        if (n_add < kept) {
+            uint32_t st = 0;
+            DF_CUDA(cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+            DF_CUDA(cudaStreamSynchronize(stream));
+            st |= DFSPH_ST_FLUID_CAPACITY;
+            DF_CUDA(cudaMemcpyAsync(status, &st, sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        }
+        DF_CUDA(cudaStreamSynchronize(stream));
+        DF_CUDA(cudaGetLastError());
+        if (added) *added = n_add;
         return DFSPH_OK;
     }
 
@@ -3055,8 +3174,8 @@ int dfsph_dynamic_window_stabilize(dfsph_ctx* ctx, uint32_t iterations, double t
     DFSPH_DISPATCH(ctx, dynamic_window_stabilize(iterations, time_step, damping, tagged_only));
 }
 int dfsph_fluid_level(dfsph_ctx* ctx, double* level) { DFSPH_DISPATCH(ctx, fluid_level(level)); }
-int dfsph_fluid_level_control(dfsph_ctx* ctx, double target, uint32_t* removed) {
-    DFSPH_DISPATCH(ctx, fluid_level_control(target, removed));
+int dfsph_fluid_level_control(dfsph_ctx* ctx, double target, uint32_t* removed, uint32_t* added) {
+    DFSPH_DISPATCH(ctx, fluid_level_control(target, removed, added));
 }
 int dfsph_dynamic_window_displacement(dfsph_ctx* ctx, double* displacement) {
     DFSPH_DISPATCH(ctx, dynamic_window_state(displacement));

@@ -14,7 +14,8 @@ __global__ void __launch_bounds__(kBlock) unpack_fluid_kernel(const float* __res
                                                               const float* __restrict__ mass, float default_mass,
                                                               uint32_t n, Vec4<Real>* __restrict__ pos,
                                                               Vec4<Real>* __restrict__ vel, Real* __restrict__ kappa,
-                                                              Real* __restrict__ kappaV, uint32_t* __restrict__ id) {
+                                                              Real* __restrict__ kappaV, uint32_t* __restrict__ id,
+                                                              uint32_t id0) {
     DFSPH_PDL_ENTER;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -31,7 +32,7 @@ __global__ void __launch_bounds__(kBlock) unpack_fluid_kernel(const float* __res
     vel[i] = v;
     kappa[i] = Real(0);
     kappaV[i] = Real(0);
-    id[i] = i;
+    id[i] = id0 + i;
 }
 
 // Overwrites positions/velocities of each slot from the caller's arrays indexed by particle id.
@@ -307,10 +308,11 @@ template <class Real> void launch_dt(DevState<Real>* d, int op, const DtArgs& a,
 
 template <class Real>
 void launch_unpack_fluid(const float* xyz, const float* vxyz, const float* mass, float default_mass, uint32_t n,
-                         Vec4<Real>* pos, Vec4<Real>* vel, Real* kappa, Real* kappaV, uint32_t* id, cudaStream_t s) {
+                         Vec4<Real>* pos, Vec4<Real>* vel, Real* kappa, Real* kappaV, uint32_t* id, cudaStream_t s,
+                         uint32_t id0) {
     if (n)
         launch_pdl(unpack_fluid_kernel<Real>, grid_for(n), kBlock, 0, s, xyz, vxyz, mass, default_mass, n, pos, vel, kappa,
-                                                                 kappaV, id);
+                                                                 kappaV, id, id0);
 }
 template <class Real>
 void launch_update_fluid(const float* xyz, const float* vxyz, uint32_t n, const uint32_t* id, Vec4<Real>* pos,
@@ -373,7 +375,7 @@ void launch_unpack_counts(const uint32_t* counts, const uint32_t* id, uint32_t n
     template void launch_set_state<R>(DevState<R>*, const DevState<R>&, cudaStream_t);                               \
     template void launch_dt<R>(DevState<R>*, int, const DtArgs&, cudaStream_t);                                       \
     template void launch_unpack_fluid<R>(const float*, const float*, const float*, float, uint32_t, Vec4<R>*,        \
-                                         Vec4<R>*, R*, R*, uint32_t*, cudaStream_t);                                 \
+                                         Vec4<R>*, R*, R*, uint32_t*, cudaStream_t, uint32_t);                                 \
     template void launch_update_fluid<R>(const float*, const float*, uint32_t, const uint32_t*, Vec4<R>*, Vec4<R>*,  \
                                          cudaStream_t, bool);                                                        \
     template void launch_unpack_boundary<R>(const float*, const float*, uint32_t, Vec4<R>*, Vec4<R>*, cudaStream_t); \

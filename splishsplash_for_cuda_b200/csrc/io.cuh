@@ -21,9 +21,12 @@ struct DtArgs {
 // DFSPH_c_arrays_structure.cpp:1100-1112), all in FP64, and refresh the Real copies in p.
 template <class Real> void launch_dt(DevState<Real>* d, int op, const DtArgs& a, cudaStream_t s);
 
+// Writes n particles (positions, optional velocities and masses; kappa and kappa_v zero) at pos..,
+// with ids id0, id0 + 1, ...
 template <class Real>
 void launch_unpack_fluid(const float* xyz, const float* vxyz, const float* mass, float default_mass, uint32_t n,
-                         Vec4<Real>* pos, Vec4<Real>* vel, Real* kappa, Real* kappaV, uint32_t* id, cudaStream_t s);
+                         Vec4<Real>* pos, Vec4<Real>* vel, Real* kappa, Real* kappaV, uint32_t* id, cudaStream_t s,
+                         uint32_t id0 = 0);
 // Overwrites positions (xyz not null) and, with set_vel, velocities (zero for a null vxyz) of the
 // particles, both given in id order.
 template <class Real>

@@ -429,12 +429,13 @@ class DFSPHCUDA:
         self._call(self._lib.dfsph_fluid_level(self._ctx, C.byref(v)))
         return v.value
 
-    def fluid_level_control(self, target: float) -> int:
+    def fluid_level_control(self, target: float) -> tuple[int, int]:
         """DFSPHCData::handleFLuidLevelControl: removes the particles above target when the level is
-        more than 5 cm above it; returns how many."""
-        r = C.c_uint32()
-        self._call(self._lib.dfsph_fluid_level_control(self._ctx, float(target), C.byref(r)))
-        return r.value
+        more than 5 cm above it, places new ones near the walls when it is more than 5 cm below;
+        returns (removed, added)."""
+        r, a = C.c_uint32(), C.c_uint32()
+        self._call(self._lib.dfsph_fluid_level_control(self._ctx, float(target), C.byref(r), C.byref(a)))
+        return r.value, a.value
 
     def dynamic_window_displacement(self) -> np.ndarray:
         out = np.zeros(3, np.float64)

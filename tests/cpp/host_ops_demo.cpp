@@ -113,13 +113,13 @@ int main(int argc, char** argv) {
             if (!close(b1[k], b0[k] + (k % 3 == 0 ? 0.001 : 0.0), 1e-6)) return fail("updateRigidBodies");
         if (sim.dynamic_bodies[0].position[0] != c[0] + 0.001) return fail("body position");
 
-        // getFluidLevel / handleFLuidLevelControl: a target above the level changes nothing, one 5 cm
-        // below it removes every particle above it
+        // getFluidLevel / handleFLuidLevelControl: a target within 5 cm of the level changes nothing,
+        // one 6 cm below it removes every particle above it
         const double level = sim.getFluidLevel();
         if (!(level > 0.0)) return fail("getFluidLevel");
         const uint32_t n_before = sim.m_data.getFluidParticlesCount();
-        sim.handleFLuidLevelControl(level + 0.5);
-        if (sim.m_data.getFluidParticlesCount() != n_before) return fail("level control above the level");
+        sim.handleFLuidLevelControl(level + 0.04);
+        if (sim.m_data.getFluidParticlesCount() != n_before) return fail("level control near the level");
         sim.handleFLuidLevelControl(level - 0.06);
         std::vector<float> x3, v3;
         sim.m_data.readDynamicData(x3, v3);

@@ -1,11 +1,12 @@
 """Fluid level (DFSPHCData::computeFluidLevel / handleFLuidLevelControl, SPH_other_systems_cuda.cu:
-144-260 and 414-470): the oracle's column rule on hand-built columns (CPU), then the device's level
-against the oracle on a settled tank and the removal of the particles above a lowered target, called
-through the C ABI (GPU)."""
+144-547): the oracle's column rule on hand-built columns and its raising lattice (CPU), then the
+device's level against the oracle on a settled tank, the removal of the particles above a lowered
+target and the particles placed to raise it again, equal to the oracle's, called through the C ABI
+(GPU)."""
 import numpy as np
 import pytest
 
-from oracle.oracle import fluid_level
+from oracle.oracle import fluid_level, fluid_level_raise
 from splishsplash_for_cuda_b200.scene import Configuration, Scene, box_wall, lattice_block
 
 R = 0.025
@@ -42,6 +43,30 @@ def test_oracle_ignores_particles_off_the_grid():
     assert fluid_level(pts, R, (0, 0, 0), (4, 10, 4)) == pytest.approx(np.float32(0.25))
 
 
+def test_oracle_raise_lattice():
+    # a closed box of boundary particles, fluid up to y = 0.3: three layers of spacing 2r over the box
+    # shrunk by 2r, only outside its central third in x or z, each lifted to its column's top + 2.5 r
+    r = 0.025
+    walls = box_wall(np.array([0.0, 0.0, 0.0]), np.array([0.6, 0.9, 0.4]), 2 * r).astype(np.float32)
+    fluid = lattice_block((10, 6, 6), r).astype(np.float32)  # y up to 0.3
+    off, dims = (2, 2, 2), (12, 14, 10)
+    new = fluid_level_raise(fluid, walls, r, off, dims, target=0.4, level=0.3)
+    assert len(new) > 0
+    lo, hi = walls.min(0) + 2 * r, walls.max(0) - 2 * r
+    w = hi - lo
+    inner = ((new[:, 0] >= lo[0] + w[0] / 3) & (new[:, 0] <= hi[0] - w[0] / 3) &
+             (new[:, 2] >= lo[2] + w[2] / 3) & (new[:, 2] <= hi[2] - w[2] / 3))
+    assert not inner.any()
+    # three layers 0.8 * 2r apart; odd layers shifted by r in x and z
+    assert np.unique(np.round((new[:, 0] - lo[0]) / r, 3) % 2).size == 2
+    # every point sits 2.5 r + a layer offset above its column's top (-2 where no fluid)
+    over = fluid[:, 1].max() + 2.5 * r
+    ys = np.unique(np.round(new[:, 1], 4))
+    for y in ys:
+        assert any(abs(y - (t + 2.5 * r + k * 0.8 * 2 * r)) < 1e-4 for t in (fluid[:, 1].max(), -2.0) for k in range(3)), y
+    assert ys.max() <= over + 2 * 0.8 * 2 * r + 1e-4
+
+
 def _tank():
     lo, hi = np.array([0.0, 0.0, 0.0]), np.array([0.6, 0.9, 0.4])
     walls = box_wall(lo, hi, 2 * R)
@@ -62,7 +87,7 @@ def test_level_matches_oracle_and_control_removes_above_target():
     from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
 
     s = _tank()
-    d = DFSPHCUDA(s)
+    d = DFSPHCUDA(s, fluid_capacity=s.n_fluid + 1000)
     levels = []
     for k in range(60):
         d.step()
@@ -75,19 +100,33 @@ def test_level_matches_oracle_and_control_removes_above_target():
     level = levels[-1]
     assert 0.45 < level < 0.65
     n0 = d.num_fluid()
-    # within 5 cm of the level, or above it: nothing changes
-    assert d.fluid_level_control(level - 0.04) == 0
-    assert d.fluid_level_control(level + 0.2) == 0
+    # within 5 cm of the level: nothing changes
+    assert d.fluid_level_control(level - 0.04) == (0, 0)
+    assert d.fluid_level_control(level + 0.04) == (0, 0)
     assert d.num_fluid() == n0
     # lowered by 10 cm: every particle above the target (rounded to FP32) goes
     target = level - 0.1
     y = d.positions()[:, 1]
     above = int(np.count_nonzero(y > np.float32(target)))
     assert above > 0
-    assert d.fluid_level_control(target) == above
+    assert d.fluid_level_control(target) == (above, 0)
     assert d.num_fluid() == n0 - above
     assert d.positions()[:, 1].max() <= np.float32(target)
     bad = _capi.ST_NONFINITE | _capi.ST_NEIGHBOR_OVERFLOW | _capi.ST_PRESSURE_NOT_CONVERGED | _capi.ST_ESCAPED
     for _ in range(10):
         assert d.step().status & bad == 0
-    assert d.fluid_level() < level - 0.05
+    low = d.fluid_level()
+    assert low < level - 0.05
+    # raised back to the first level: the oracle's lattice, appended in lattice order
+    n1 = d.num_fluid()
+    off, dims = _device_level_inputs(d)
+    want = fluid_level_raise(d.positions(), d.field("boundary_position"), R, off, dims, level, low)
+    assert len(want) > 0
+    assert d.fluid_level_control(level) == (0, len(want))
+    x = d.positions()
+    assert len(x) == n1 + len(want)
+    assert np.array_equal(x[n1:], want)
+    assert np.array_equal(x[:n1], d.positions()[:n1])
+    assert np.all(d.field("velocity")[n1:] == 0)
+    for _ in range(10):
+        assert d.step().status & bad == 0
