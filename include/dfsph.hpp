@@ -21,10 +21,15 @@
 #define DFSPH_HPP
 
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -259,10 +264,21 @@ public:
         uint32_t first, count;
         std::array<double, 3> position;
         std::array<double, 3> rest_position;
+        std::array<double, 4> q{{1.0, 0.0, 0.0, 0.0}};  // orientation (w, x, y, z), unit
     };
     std::vector<DynamicBody> dynamic_bodies;
     void addDynamicBody(uint32_t first, uint32_t count, const std::array<double, 3>& center) {
-        dynamic_bodies.push_back({first, count, center, center});
+        dynamic_bodies.push_back({first, count, center, center, {{1.0, 0.0, 0.0, 0.0}}});
+    }
+    /* DFSPHCUDA::is_dynamic_bodies_paused / handleDynamicBodiesPause (DFSPH_CUDA.cpp:1860-1883,
+     * DFSPHCData::pause_solids): pausing sets every dynamic body's particle velocities (and so its
+     * rigid velocity field) to zero, keeping its pose. */
+    bool is_dynamic_bodies_paused = false;
+    void handleDynamicBodiesPause(bool pause) {
+        is_dynamic_bodies_paused = pause;
+        if (!pause) return;
+        const std::array<double, 3> zero{{0.0, 0.0, 0.0}};
+        for (DynamicBody& body : dynamic_bodies) apply_pose(body, body.position, body.q, zero, zero);
     }
     /* The state the reference's rigid-body solver hands back each step (DynamicBody: position,
      * velocity, orientation q = (w, x, y, z), angular velocity). */
@@ -275,28 +291,75 @@ public:
      * velocity field v + w x (x - position), on the device. */
     void updateRigidBodies(const std::vector<DynamicBodyState>& states) {
         if (states.size() != dynamic_bodies.size()) throw Error(DFSPH_E_INVALID, "one state per dynamic body");
-        for (size_t b = 0; b < states.size(); ++b) {
-            DynamicBody& body = dynamic_bodies[b];
-            const DynamicBodyState& st = states[b];
-            const double w = st.q[0], x = st.q[1], y = st.q[2], z = st.q[3];
-            const double len = std::sqrt(w * w + x * x + y * y + z * z);
-            if (!(len > 0)) throw Error(DFSPH_E_INVALID, "quaternion must be non-zero");
-            const double qw = w / len, qx = x / len, qy = y / len, qz = z / len;
-            const double R[9] = {1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qw * qz), 2 * (qx * qz + qw * qy),
-                                 2 * (qx * qy + qw * qz), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qw * qx),
-                                 2 * (qx * qz - qw * qy), 2 * (qy * qz + qw * qx), 1 - 2 * (qx * qx + qy * qy)};
-            const std::array<double, 3>& c = body.rest_position;
-            double arm[3], p[3], v[3];  // x = R x0 + p with p = position - R c; v passed about p
-            for (int i = 0; i < 3; ++i) arm[i] = R[3 * i] * c[0] + R[3 * i + 1] * c[1] + R[3 * i + 2] * c[2];
-            for (int i = 0; i < 3; ++i) p[i] = st.position[i] - arm[i];
-            const std::array<double, 3>& om = st.angular_velocity;
-            v[0] = st.velocity[0] - (om[1] * arm[2] - om[2] * arm[1]);
-            v[1] = st.velocity[1] - (om[2] * arm[0] - om[0] * arm[2]);
-            v[2] = st.velocity[2] - (om[0] * arm[1] - om[1] * arm[0]);
-            const double q4[4] = {qw, qx, qy, qz};
-            check(ctx_, dfsph_move_boundary_rigid(ctx_, body.first, body.count, q4, p, v, om.data()));
-            body.position = st.position;
+        for (size_t b = 0; b < states.size(); ++b)
+            apply_pose(dynamic_bodies[b], states[b].position, states[b].q, states[b].velocity,
+                       states[b].angular_velocity);
+    }
+    /* updateRigidBodiesStatefromFile (DFSPHCData::update_solids_from_file, DFSPH_c_arrays_structure.cpp:
+     * 1445-1479): waits for `solids_files_folder` + "update_solids.txt", reads per dynamic body its
+     * position, velocity, orientation (x y z w) and angular velocity (13 numbers), applies them as
+     * updateRigidBodies does and removes the file. The reference waits without limit; this wait gives
+     * up after timeout_s seconds (Error DFSPH_E_STATE). */
+    std::string solids_files_folder;
+    void updateRigidBodiesStatefromFile(double timeout_s = 60.0) {
+        const std::string path = solids_files_folder + "update_solids.txt";
+        std::ifstream f;
+        const auto t0 = std::chrono::steady_clock::now();
+        for (;;) {
+            f.open(path);
+            if (f.is_open()) break;
+            if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > timeout_s)
+                throw Error(DFSPH_E_STATE, "no " + path + " within the time limit");
+            std::this_thread::sleep_for(std::chrono::milliseconds(100));
         }
+        std::vector<DynamicBodyState> states(dynamic_bodies.size());
+        for (DynamicBodyState& st : states) {
+            double qx, qy, qz, qs;
+            f >> st.position[0] >> st.position[1] >> st.position[2] >> st.velocity[0] >> st.velocity[1] >>
+                st.velocity[2] >> qx >> qy >> qz >> qs >> st.angular_velocity[0] >> st.angular_velocity[1] >>
+                st.angular_velocity[2];
+            if (!f) throw Error(DFSPH_E_INVALID, "truncated " + path);
+            st.q = {{qs, qx, qy, qz}};
+        }
+        f.close();
+        updateRigidBodies(states);
+        std::remove(path.c_str());
+    }
+    /* updateRigidBodiesStateToFile (DFSPHCData::update_solids_to_file, UnifiedParticleSet::
+     * write_forces_to_file, DFSPH_c_arrays_structure.cpp:1422-1443, 681-712): per dynamic body i,
+     * "solid_forces_file_<i>.txt" holds its particle count, then one line per particle with its
+     * position in the body frame and the fluid's force on it; "solids_file.txt" the number of bodies;
+     * all in `solids_files_folder` (needs set("boundary_forces", 1)). */
+    void updateRigidBodiesStateToFile() {
+        std::vector<double> f, x;
+        boundary_force_and_position(f, x);
+        std::remove((solids_files_folder + "solids_file.txt").c_str());
+        for (size_t b = 0; b < dynamic_bodies.size(); ++b) {
+            const DynamicBody& body = dynamic_bodies[b];
+            if ((uint64_t)body.first + body.count > f.size() / 3)
+                throw Error(DFSPH_E_INVALID, "dynamic body beyond the boundary");
+            double R[9];
+            rotation(body.q, R);
+            std::ostringstream oss;
+            oss << body.count << std::endl;
+            for (uint32_t i = body.first; i < body.first + body.count; ++i) {
+                double d[3], x0[3];
+                for (int a = 0; a < 3; ++a) d[a] = x[3 * (size_t)i + a] - body.position[a];
+                for (int a = 0; a < 3; ++a) x0[a] = R[a] * d[0] + R[3 + a] * d[1] + R[6 + a] * d[2];  // R^T d
+                oss << (float)x0[0] << " " << (float)x0[1] << " " << (float)x0[2] << " ";
+                oss << (float)f[3 * (size_t)i] << " " << (float)f[3 * (size_t)i + 1] << " " << (float)f[3 * (size_t)i + 2]
+                    << " ";
+                oss << std::endl;
+            }
+            const std::string name = solids_files_folder + "solid_forces_file_" + std::to_string(b) + ".txt";
+            std::remove(name.c_str());
+            std::ofstream out(name, std::ios_base::app);
+            if (!out) throw Error(DFSPH_E_INVALID, "cannot write " + name);
+            out << oss.str();
+        }
+        std::ofstream main(solids_files_folder + "solids_file.txt");
+        if (!main) throw Error(DFSPH_E_INVALID, "cannot write " + solids_files_folder + "solids_file.txt");
+        main << dynamic_bodies.size();
     }
     /* getFluidImpactOnDynamicBodies (compute_fluid_impact_on_dynamic_body_kernel,
      * DFSPH_memory_management_cuda.cu:688-705): per body, the sum of its particles' fluid forces
@@ -374,6 +437,35 @@ public:
     unsigned int m_iterations = 0, m_iterationsV = 0;
 
 private:
+    // Rotation matrix (row-major) of the unit quaternion q = (w, x, y, z).
+    static void rotation(const std::array<double, 4>& q, double R[9]) {
+        const double qw = q[0], qx = q[1], qy = q[2], qz = q[3];
+        const double M[9] = {1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qw * qz), 2 * (qx * qz + qw * qy),
+                             2 * (qx * qy + qw * qz), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qw * qx),
+                             2 * (qx * qz - qw * qy), 2 * (qy * qz + qw * qx), 1 - 2 * (qx * qx + qy * qy)};
+        for (int k = 0; k < 9; ++k) R[k] = M[k];
+    }
+    // update_dynamicObject_UnifiedParticleSet_cuda (DFSPH_core_cuda.cu:3407-3449) for one body: its
+    // samples go to R(q) (x0 - rest) + position with the rigid velocity field v + w x (x - position),
+    // on the device; the body keeps the pose.
+    void apply_pose(DynamicBody& body, const std::array<double, 3>& position, const std::array<double, 4>& q,
+                    const std::array<double, 3>& velocity, const std::array<double, 3>& om) {
+        const double len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        if (!(len > 0)) throw Error(DFSPH_E_INVALID, "quaternion must be non-zero");
+        const std::array<double, 4> u{{q[0] / len, q[1] / len, q[2] / len, q[3] / len}};
+        double R[9];
+        rotation(u, R);
+        const std::array<double, 3>& c = body.rest_position;
+        double arm[3], p[3], v[3];  // x = R x0 + p with p = position - R c; v passed about p
+        for (int i = 0; i < 3; ++i) arm[i] = R[3 * i] * c[0] + R[3 * i + 1] * c[1] + R[3 * i + 2] * c[2];
+        for (int i = 0; i < 3; ++i) p[i] = position[i] - arm[i];
+        v[0] = velocity[0] - (om[1] * arm[2] - om[2] * arm[1]);
+        v[1] = velocity[1] - (om[2] * arm[0] - om[0] * arm[2]);
+        v[2] = velocity[2] - (om[0] * arm[1] - om[1] * arm[0]);
+        check(ctx_, dfsph_move_boundary_rigid(ctx_, body.first, body.count, u.data(), p, v, om.data()));
+        body.position = position;
+        body.q = u;
+    }
     // The fluid's force on every boundary particle during the last step and the particles' positions,
     // 3 FP64 values each in upload order.
     void boundary_force_and_position(std::vector<double>& f, std::vector<double>& x) const {

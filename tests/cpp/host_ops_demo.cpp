@@ -1,7 +1,8 @@
 // host_ops_demo.cpp — the host-side operations of the reference's SPH::DFSPHCUDA through the C++
 // facade (include/dfsph.hpp): handleSimulationSave / handleSimulationLoad, zeroFluidVelocities,
-// updateTimeStepDuration, updateRigidBodies, getFluidImpactOnDynamicBodies,
-// getFluidBoyancyOnDynamicBodies, getFluidLevel and handleFLuidLevelControl. Test program:
+// updateTimeStepDuration, updateRigidBodies, handleDynamicBodiesPause, updateRigidBodiesStateToFile /
+// updateRigidBodiesStatefromFile, getFluidImpactOnDynamicBodies, getFluidBoyancyOnDynamicBodies,
+// getFluidLevel and handleFLuidLevelControl. Test program:
 // tests/test_cpp_facade.py writes the scene, runs this and reads its exit code; the checks are made
 // here.
 //
@@ -14,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <fstream>
+#include <string>
 #include <iostream>
 #include <vector>
 
@@ -106,12 +108,73 @@ int main(int argc, char** argv) {
         std::vector<double> b0(3 * (size_t)nb), b1(3 * (size_t)nb);
         dfsph::check(sim.handle(), dfsph_download(sim.handle(), DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F64, b0.data(),
                                                   b0.size(), DFSPH_ORDER_ID));
-        sim.updateRigidBodies({{{c[0] + 0.001, c[1], c[2]}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {1.0, 0.0, 0.0, 0.0}}});
+        sim.updateRigidBodies({{{c[0] + 0.001, c[1], c[2]}, {0.1, 0.0, 0.0}, {0.0, 0.0, 0.0}, {1.0, 0.0, 0.0, 0.0}}});
         dfsph::check(sim.handle(), dfsph_download(sim.handle(), DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F64, b1.data(),
                                                   b1.size(), DFSPH_ORDER_ID));
         for (size_t k = 0; k < b0.size(); ++k)
             if (!close(b1[k], b0[k] + (k % 3 == 0 ? 0.001 : 0.0), 1e-6)) return fail("updateRigidBodies");
         if (sim.dynamic_bodies[0].position[0] != c[0] + 0.001) return fail("body position");
+        std::vector<double> bv(3 * (size_t)nb), b2(3 * (size_t)nb);
+        dfsph::check(sim.handle(), dfsph_download(sim.handle(), DFSPH_F_BOUNDARY_VELOCITY, DFSPH_DTYPE_F64, bv.data(),
+                                                  bv.size(), DFSPH_ORDER_ID));
+        for (size_t k = 0; k < bv.size(); ++k)
+            if (!close(bv[k], k % 3 == 0 ? 0.1 : 0.0, 1e-6)) return fail("rigid velocity");
+
+        // handleDynamicBodiesPause: velocities zero, pose kept
+        sim.handleDynamicBodiesPause(true);
+        if (!sim.is_dynamic_bodies_paused) return fail("pause flag");
+        dfsph::check(sim.handle(), dfsph_download(sim.handle(), DFSPH_F_BOUNDARY_VELOCITY, DFSPH_DTYPE_F64, bv.data(),
+                                                  bv.size(), DFSPH_ORDER_ID));
+        dfsph::check(sim.handle(), dfsph_download(sim.handle(), DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F64, b2.data(),
+                                                  b2.size(), DFSPH_ORDER_ID));
+        for (size_t k = 0; k < bv.size(); ++k)
+            if (bv[k] != 0.0 || !close(b2[k], b1[k], 1e-7)) return fail("handleDynamicBodiesPause");
+
+        // updateRigidBodiesStateToFile: the body-frame positions and the fluid's forces, per particle
+        sim.solids_files_folder = argv[2];
+        sim.step();
+        sim.updateRigidBodiesStateToFile();
+        {
+            std::vector<double> f(3 * (size_t)nb), x(3 * (size_t)nb);
+            dfsph::check(sim.handle(), dfsph_download(sim.handle(), DFSPH_F_BOUNDARY_FORCE, DFSPH_DTYPE_F64, f.data(),
+                                                      f.size(), DFSPH_ORDER_ID));
+            dfsph::check(sim.handle(), dfsph_download(sim.handle(), DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F64,
+                                                      x.data(), x.size(), DFSPH_ORDER_ID));
+            std::ifstream sf(std::string(argv[2]) + "solids_file.txt");
+            int bodies = 0;
+            if (!(sf >> bodies) || bodies != 1) return fail("solids_file.txt");
+            std::ifstream ff(std::string(argv[2]) + "solid_forces_file_0.txt");
+            uint32_t count = 0;
+            if (!(ff >> count) || count != (uint32_t)nb) return fail("solid_forces_file_0.txt count");
+            double fmax = 0;
+            for (double q : f) fmax = std::max(fmax, std::fabs(q));
+            for (uint32_t i = 0; i < count; ++i) {
+                double v[6];
+                for (double& q : v)
+                    if (!(ff >> q)) return fail("solid_forces_file_0.txt line");
+                for (int a = 0; a < 3; ++a) {
+                    const double x0 = x[3 * (size_t)i + a] - sim.dynamic_bodies[0].position[a];
+                    if (std::fabs(v[a] - x0) > 1e-5 * std::max(1.0, std::fabs(x0))) return fail("body-frame position");
+                    if (std::fabs(v[3 + a] - f[3 * (size_t)i + a]) > 1e-5 * std::fabs(f[3 * (size_t)i + a]) + 1e-9 * fmax)
+                        return fail("particle force");
+                }
+            }
+        }
+
+        // updateRigidBodiesStatefromFile: position x y z, velocity, q as x y z w, angular velocity
+        {
+            const std::string path = std::string(argv[2]) + "update_solids.txt";
+            std::ofstream uf(path);
+            uf.precision(17);
+            uf << c[0] + 0.002 << " " << c[1] << " " << c[2] << " 0 0 0  0 0 0 1  0 0 0\n";
+            uf.close();
+            sim.updateRigidBodiesStatefromFile(5.0);
+            if (std::ifstream(path).good()) return fail("update_solids.txt not removed");
+            dfsph::check(sim.handle(), dfsph_download(sim.handle(), DFSPH_F_BOUNDARY_POSITION, DFSPH_DTYPE_F64,
+                                                      b2.data(), b2.size(), DFSPH_ORDER_ID));
+            for (size_t k = 0; k < b0.size(); ++k)
+                if (!close(b2[k], b0[k] + (k % 3 == 0 ? 0.002 : 0.0), 1e-6)) return fail("updateRigidBodiesStatefromFile");
+        }
 
         // getFluidLevel / handleFLuidLevelControl: a target within 5 cm of the level changes nothing,
         // one 6 cm below it removes every particle above it
