@@ -107,70 +107,30 @@ template <class Real> struct Cubic {
     }
 };
 
-// Density terms m_j W_ij of the FP32 instance as double-float pairs (hi + lo), the same
-// error-free transformations as the device's density_term (dfsph_common.cuh): TwoSum, Fast2Sum and
-// the FMA product error on FP32 values. The FP64 instance evaluates the terms directly.
-struct F2 {
-    float h, l;
-};
-inline F2 f2_two_sum(float a, float b) {
-    const float s = a + b, bb = s - a;
-    return {s, (a - (s - bb)) + (b - bb)};
-}
-inline F2 f2_fast_two_sum(float a, float b) {
-    const float s = a + b;
-    return {s, b - (s - a)};
-}
-inline F2 f2_mul(F2 a, F2 b) {
-    const float p = a.h * b.h;
-    float e = std::fmaf(a.h, b.h, -p);
-    e = std::fmaf(a.h, b.l, e);
-    e = std::fmaf(a.l, b.h, e);
-    return f2_fast_two_sum(p, e);
-}
-inline F2 f2_mul_f(F2 a, float b) {
-    const float p = a.h * b;
-    return f2_fast_two_sum(p, std::fmaf(a.l, b, std::fmaf(a.h, b, -p)));
-}
-inline F2 f2_split(double v) {
-    const float h = (float)v;
-    return {h, (float)(v - (double)h)};
-}
+// Density terms m_j W_ij of the FP32 instance, evaluated in FP64 from the FP32 distance components
+// and summed in FP64, as the device's density_term (dfsph_common.cuh). The FP64 instance evaluates
+// the terms with its kernel.
 struct DensityTerms {
-    F2 ih2{}, k{}, k2{};
+    double ih2 = 0, k = 0;
     void set(double H) {
-        ih2 = f2_split(1.0 / (H * H));
-        k = f2_split(8.0 / (M_PI * H * H * H));
-        k2 = f2_split(16.0 / (M_PI * H * H * H));
+        ih2 = 1.0 / (H * H);
+        k = 8.0 / (M_PI * H * H * H);
     }
-    // m W(r): |r|^2, q^2, q (one Newton correction of the FP32 root), the cubic and the product with
-    // m, each as a pair.
-    F2 term(float rx, float ry, float rz, float m) const {
-        const float a = rx * rx, b = ry * ry, c = rz * rz;
-        const float ea = std::fmaf(rx, rx, -a), eb = std::fmaf(ry, ry, -b), ec = std::fmaf(rz, rz, -c);
-        const F2 s1 = f2_two_sum(a, b), s2 = f2_two_sum(s1.h, c);
-        const F2 r2 = f2_fast_two_sum(s2.h, ((ea + eb) + ec) + (s1.l + s2.l));
-        const F2 q2 = f2_mul(r2, ih2);
-        if (q2.h > 1.0f) return {0.0f, 0.0f};
-        F2 W = k;
-        if (q2.h > 0.0f) {
-            const float qh = std::sqrt(q2.h);
-            const F2 q = f2_fast_two_sum(qh, (std::fmaf(-qh, qh, q2.h) + q2.l) * (0.5f / qh));
-            if (q.h > 1.0f) return {0.0f, 0.0f};
-            if (q.h <= 0.5f) {
-                F2 t = f2_two_sum(q.h, -1.0f);
-                t = f2_fast_two_sum(t.h, t.l + q.l);
-                const F2 v = f2_mul_f(f2_mul(q2, t), 6.0f);
-                F2 P = f2_two_sum(1.0f, v.h);
-                P = f2_fast_two_sum(P.h, P.l + v.l);
-                W = f2_mul(P, k);
+    double term(float rx, float ry, float rz, float m) const {
+        const double dx = rx, dy = ry, dz = rz;
+        const double q2 = (dx * dx + dy * dy + dz * dz) * ih2;
+        if (q2 > 1.0) return 0.0;
+        double w = k;
+        if (q2 > 0.0) {
+            const double q = std::sqrt(q2);
+            if (q <= 0.5) {
+                w = k * (1.0 + 6.0 * q2 * (q - 1.0));
             } else {
-                F2 f = f2_two_sum(1.0f, -q.h);
-                f = f2_fast_two_sum(f.h, f.l - q.l);
-                W = f2_mul(f2_mul(f2_mul(f, f), f), k2);
+                const double f = 1.0 - q;
+                w = 2.0 * k * (f * f * f);
             }
         }
-        return f2_mul_f(W, m);
+        return w * (double)m;
     }
 };
 
@@ -696,14 +656,12 @@ template <class Real> struct Oracle {
             if (warm_v) kapv[i] = std::max<Real>(kapv[i] * hr / Real(2), Real(-0.5));
             // rho - rho0 accumulated directly (the device kernels do the same; see density_alpha_kernel)
             Neumaier<Real> r;
-            float r_lo = 0.0f;
+            double r64 = -(double)(Real)prm.density0;
             Kahan<Real> sgk, dr, gx, gy, gz;
             r.add((Real)-prm.density0);
             auto add_term = [&](Real rx, Real ry, Real rz, Real mj, Real w) {
                 if (sizeof(Real) == 4) {
-                    const F2 t = DT.term((float)rx, (float)ry, (float)rz, (float)mj);
-                    r.add((Real)t.h);
-                    r_lo += t.l;
+                    r64 += DT.term((float)rx, (float)ry, (float)rz, (float)mj);
                 } else {
                     r.add(mj * w);
                 }
@@ -734,7 +692,7 @@ template <class Real> struct Oracle {
             const Real Gx = gx.value(), Gy = gy.value(), Gz = gz.value();
             const Real sg = sgk.value() + (Gx * Gx + Gy * Gy + Gz * Gz);
             alpha[i] = -invh / std::max<Real>(sg, (Real)kEps);
-            rho[i] = r.value() + (Real)r_lo;  // rho - rho0
+            rho[i] = sizeof(Real) == 4 ? (Real)r64 : r.value();  // rho - rho0
             uint32_t num = (uint32_t)nf[i].size();
             if (num < kMinNeighbors) num += (uint32_t)nbd[i].size();
             dadv[i] = (num < kMinNeighbors) ? Real(0) : std::max<Real>(dr.value(), Real(0));

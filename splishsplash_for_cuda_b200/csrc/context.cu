@@ -387,13 +387,8 @@ public:
         p.kern.k = (Real)(8.0 / (M_PI * H * H * H));
         p.kern.l = (Real)(48.0 / (M_PI * H * H * H));
         p.kern.W0 = p.kern.k;
-        auto split = [](double v, float& hi, float& lo) {
-            hi = (float)v;
-            lo = (float)(v - (double)hi);
-        };
-        split(1.0 / (H * H), p.kern.ih2_h, p.kern.ih2_l);
-        split(8.0 / (M_PI * H * H * H), p.kern.k_h, p.kern.k_l);
-        split(16.0 / (M_PI * H * H * H), p.kern.k2_h, p.kern.k2_l);
+        p.kern.ih2_d = 1.0 / (H * H);
+        p.kern.k_d = 8.0 / (M_PI * H * H * H);
         p.H2 = (Real)(Hf * Hf);
         p.density0 = (Real)sc.density0;
         p.viscosity = (Real)sc.viscosity;

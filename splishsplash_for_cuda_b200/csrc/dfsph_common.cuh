@@ -185,9 +185,9 @@ constexpr uint32_t kEscapedKey = 0xFFFFFFFFu;  // sorts after every valid 30-bit
 // and the parity tests bound the difference).
 template <class Real> struct Cubic {
     Real H, invH, k, l, W0;
-    // Double-float (hi + lo) splits of 1/H^2, k and 2k for the density terms of the FP32 build
-    // (density_term below); unused by the FP64 build.
-    float ih2_h, ih2_l, k_h, k_l, k2_h, k2_l;
+    // 1/H^2 and k in FP64 for the density terms of the FP32 build (density_term below); unused by
+    // the FP64 build.
+    double ih2_d, k_d;
     static __device__ __forceinline__ float rsqrt_(float v) { return rsqrtf(v); }
     static __device__ __forceinline__ double rsqrt_(double v) { return rsqrt(v); }
     __device__ __forceinline__ Real W_of_q(Real q) const {
@@ -254,63 +254,25 @@ template <class Real> struct Cubic {
 // pairs keeps each term within ~2^-40 of the exact value for the given FP32 coordinates; the sum
 // itself stays an FP32 compensated sum (hi parts in Neumaier's sum, lo parts in a plain FP32 sum).
 // Every operation is an explicit round-to-nearest intrinsic so nothing is contracted.
-struct F2 {
-    float h, l;
-};
-__device__ __forceinline__ F2 f2_two_sum(float a, float b) {
-    const float s = __fadd_rn(a, b);
-    const float bb = __fsub_rn(s, a);
-    return {s, __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb))};
-}
-__device__ __forceinline__ F2 f2_fast_two_sum(float a, float b) {  // |a| >= |b|
-    const float s = __fadd_rn(a, b);
-    return {s, __fsub_rn(b, __fsub_rn(s, a))};
-}
-__device__ __forceinline__ F2 f2_mul(F2 a, F2 b) {
-    const float p = __fmul_rn(a.h, b.h);
-    float e = __fmaf_rn(a.h, b.h, -p);
-    e = __fmaf_rn(a.h, b.l, e);
-    e = __fmaf_rn(a.l, b.h, e);
-    return f2_fast_two_sum(p, e);
-}
-__device__ __forceinline__ F2 f2_mul_f(F2 a, float b) {
-    const float p = __fmul_rn(a.h, b);
-    return f2_fast_two_sum(p, __fmaf_rn(a.l, b, __fmaf_rn(a.h, b, -p)));
-}
-// m W(r) for FP32 r and m: hi + lo. The self term (r = 0) is m k.
-__device__ __forceinline__ F2 density_term(const Cubic<float>& K, float rx, float ry, float rz, float m) {
-    const float a = __fmul_rn(rx, rx), b = __fmul_rn(ry, ry), c = __fmul_rn(rz, rz);
-    const float ea = __fmaf_rn(rx, rx, -a), eb = __fmaf_rn(ry, ry, -b), ec = __fmaf_rn(rz, rz, -c);
-    const F2 s1 = f2_two_sum(a, b);
-    const F2 s2 = f2_two_sum(s1.h, c);
-    const F2 r2 = f2_fast_two_sum(s2.h, __fadd_rn(__fadd_rn(__fadd_rn(ea, eb), ec), __fadd_rn(s1.l, s2.l)));
-    const F2 q2 = f2_mul(r2, F2{K.ih2_h, K.ih2_l});
-    if (q2.h > 1.0f) return {0.0f, 0.0f};
-    F2 W;
-    if (q2.h > 0.0f) {
-        // q = sqrt(q^2): a few-ulp FP32 root, then one Newton correction on the pair (the residual
-        // q^2 - qh^2 is exact through the FMA, so the pair is accurate whatever qh's last bits).
-        const float rs = rsqrtf(q2.h);
-        const float qh = __fmul_rn(q2.h, rs);
-        const float ql = __fmul_rn(__fadd_rn(__fmaf_rn(-qh, qh, q2.h), q2.l), __fmul_rn(0.5f, rs));
-        const F2 q = f2_fast_two_sum(qh, ql);
-        if (q.h > 1.0f) return {0.0f, 0.0f};
-        if (q.h <= 0.5f) {  // k (1 + 6 q^2 (q - 1))
-            F2 t = f2_two_sum(q.h, -1.0f);
-            t = f2_fast_two_sum(t.h, __fadd_rn(t.l, q.l));
-            const F2 v = f2_mul_f(f2_mul(q2, t), 6.0f);
-            F2 P = f2_two_sum(1.0f, v.h);
-            P = f2_fast_two_sum(P.h, __fadd_rn(P.l, v.l));
-            W = f2_mul(P, F2{K.k_h, K.k_l});
-        } else {  // 2 k (1 - q)^3
-            F2 f = f2_two_sum(1.0f, -q.h);
-            f = f2_fast_two_sum(f.h, __fsub_rn(f.l, q.l));
-            W = f2_mul(f2_mul(f2_mul(f, f), f), F2{K.k2_h, K.k2_l});
+// Density term m_j W(r_ij) of the FP32 build, evaluated in native FP64 from the FP32 distance
+// components (their squares are exact in FP64): the FP32 build sums rho - rho0 in FP64 from these
+// terms, so the density residual keeps the accuracy of the FP64 build where rho ~ rho0 cancels.
+// The self term (r = 0) is m k.
+__device__ __forceinline__ double density_term(const Cubic<float>& K, float rx, float ry, float rz, float m) {
+    const double dx = rx, dy = ry, dz = rz;
+    const double q2 = (dx * dx + dy * dy + dz * dz) * K.ih2_d;
+    if (q2 > 1.0) return 0.0;
+    double w = K.k_d;
+    if (q2 > 0.0) {
+        const double q = sqrt(q2);
+        if (q <= 0.5) {
+            w = K.k_d * (1.0 + 6.0 * q2 * (q - 1.0));
+        } else {
+            const double f = 1.0 - q;
+            w = 2.0 * K.k_d * (f * f * f);
         }
-    } else {
-        W = F2{K.k_h, K.k_l};
     }
-    return f2_mul_f(W, m);
+    return w * (double)m;
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -392,19 +392,17 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
     // rho - rho0 is accumulated directly (rest density first, then the self term and the neighbour
     // terms) so that the density residual rho + h*div - rho0 of the pressure solve never subtracts
     // two numbers of ~1e3 in FP32 (the reference forms rho, then rho + h*div - rho0).
-    // FP32 build: each density term m_j W_ij is formed as a double-float pair (density_term); the
-    // hi parts go to the compensated sum, the lo parts to rho_lo. FP64 build: plain terms.
-    constexpr bool kPairTerms = std::is_same<Real, float>::value;
+    // FP32 build: each density term m_j W_ij is formed and summed in FP64 (density_term). FP64
+    // build: plain terms, compensated sum.
+    constexpr bool kF64Terms = std::is_same<Real, float>::value;
     NSum<Real> rho;
-    float rho_lo = 0.0f;
+    double rho64 = -(double)p.density0;
     KSum<Real> sgk, drho;
     KSum3<Real> gpi;
     rho.add(-p.density0);
     auto add_term = [&](Real rx, Real ry, Real rz, Real m, Real w) {
-        if constexpr (kPairTerms) {
-            const F2 t = density_term(K, rx, ry, rz, m);
-            rho.add(t.h);
-            rho_lo = __fadd_rn(rho_lo, t.l);
+        if constexpr (kF64Terms) {
+            rho64 += density_term(K, rx, ry, rz, m);
         } else {
             rho.add(m * w);
         }
@@ -413,7 +411,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
     auto accumulate = [&](const Vec4<Real>& xj, Real vx, Real vy, Real vz) {
         Real w, gx, gy, gz;
         const Real rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-        if constexpr (kPairTerms) K.gradW(rx, ry, rz, gx, gy, gz), w = Real(0);
+        if constexpr (kF64Terms) K.gradW(rx, ry, rz, gx, gy, gz), w = Real(0);
         else K.W_gradW(rx, ry, rz, w, gx, gy, gz);
         add_term(rx, ry, rz, xj.w, w);
         const Real px = xj.w * gx, py = xj.w * gy, pz = xj.w * gz;
@@ -441,7 +439,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) density_alpha_kernel
     const Real gx = gpi.x.value(), gy = gpi.y.value(), gz = gpi.z.value();
     const Real sg = sgk.value() + (gx * gx + gy * gy + gz * gz);
     const Real alpha = -p.inv_h / rmax<Real>(sg, Real(kEps));
-    const Real density = rho.value() + Real(rho_lo);
+    const Real density = kF64Terms ? (Real)rho64 : rho.value();
     ds->factor[i] = alpha;
     ds->density[i] = density;
     uint32_t num = nf;

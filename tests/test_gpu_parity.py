@@ -81,7 +81,7 @@ def test_one_step_fp32_within_1e5_of_fp64_oracle(config, counts):
     """One CFL step from rest of the full dam break (27,000), precision (250,047) and sloshing-tank
     (1,000,000 particles, walls at rest) configurations: every field of every particle within a plain
     1e-5 relative of the FP64 oracle. What makes the velocity bar reachable in FP32 is the density
-    pass's double-float terms: the particles next to the few compressed ones get a pressure
+    pass's FP64 terms: the particles next to the few compressed ones get a pressure
     correction that cancels most of gravity's g h, so their velocity carries the relative error of
     rho - rho0 amplified ~3x, and plain FP32 terms (~1e-4 kg/m^3 on rho) put it at 1-2e-5."""
     s = synthetic_scene(config, counts=counts, cfl=True)

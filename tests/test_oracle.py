@@ -67,10 +67,9 @@ def test_boundary_psi_planar_lattice(oracle_lib):
 @pytest.mark.parametrize("config,counts", [(1, (14, 14, 14)), (1, None), (2, None)])
 def test_fp32_formulation_meets_one_step_bar(oracle_lib, config, counts):
     """The FP32 instance of the restated formulation (the device's arithmetic: compensated FP32
-    sums, double-float density terms) against the FP64 instance, one CFL step from rest: every field
-    of every particle within a plain 1e-5 relative (no floor). Measured: density 6e-8, alpha 7e-7,
-    kappa 3e-8, velocity 5e-7 on the 250,047-particle configuration; with plain FP32 density terms
-    the velocity was 1.1e-5."""
+    sums, density terms formed and summed in FP64) against the FP64 instance, one CFL step from rest:
+    every field of every particle within a plain 1e-5 relative (no floor). With plain FP32 density
+    terms the velocity was 1.1e-5 on the 250,047-particle configuration."""
     s = synthetic_scene(config, counts=counts, cfl=True)
     o64, o32 = Oracle(s, 64), Oracle(s, 32)
     r64, r32 = o64.step(), o32.step()
