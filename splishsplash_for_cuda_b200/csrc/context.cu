@@ -2947,7 +2947,8 @@ struct dfsph_ctx {
         if (pre != DFSPH_OK) return pre;                                                       \
         return (ctx)->f32 ? (ctx)->f32->call : (ctx)->f64->call;                               \
     } while (0)
-// The step applies velocities pending from dfsph_update_fluid inside its binning.
+// The step applies velocities pending from dfsph_update_fluid inside its binning; a rigid boundary
+// motion touches neither the fluid nor the upload staging, so the pending copy keeps overlapping.
 #define DFSPH_DISPATCH_STEP(ctx, call)                                                         \
     do {                                                                                       \
         if (!(ctx)) return DFSPH_E_INVALID;                                                    \
@@ -3059,7 +3060,7 @@ int dfsph_move_boundary(dfsph_ctx* ctx, const float* xyz, const float* vxyz) {
 }
 int dfsph_move_boundary_rigid(dfsph_ctx* ctx, uint32_t first, uint32_t count, const double* q, const double* position,
                               const double* velocity, const double* angular_velocity) {
-    DFSPH_DISPATCH(ctx, move_boundary_rigid(first, count, q, position, velocity, angular_velocity));
+    DFSPH_DISPATCH_STEP(ctx, move_boundary_rigid(first, count, q, position, velocity, angular_velocity));
 }
 int dfsph_upload_fluid(dfsph_ctx* ctx, const float* xyz, const float* vxyz, const float* mass, uint32_t n) {
     DFSPH_DISPATCH(ctx, upload_fluid(xyz, vxyz, mass, n));

@@ -88,3 +88,21 @@ def test_update_with_unchanged_state_changes_nothing(cuda_lib):
         sa, sb = a.step(), b.step()
         assert sa.iterations == sb.iterations and sa.iterations_v == sb.iterations_v
     assert np.array_equal(a.positions(), b.positions()) and np.array_equal(a.velocities(), b.velocities())
+
+
+def test_rigid_wall_motion_keeps_the_pending_velocities(cuda_lib):
+    """A rigid boundary motion between the update and the step leaves the velocity copy in flight
+    (it touches neither the fluid nor the upload staging): same bits as applying them first."""
+    runs = []
+    for flush_first in (False, True):
+        d = advanced()
+        nb = int(d.get_param("num_boundary"))
+        x2, v2 = new_state(d)
+        d.update_fluid(x2, v2)
+        if flush_first:
+            d.synchronize()
+        d.move_boundary_rigid(0, nb, position=(0.002, 0.0, 0.0), velocity=(0.1, 0.0, 0.0))
+        st = d.step()
+        runs.append((st.iterations, st.iterations_v, d.positions(), d.velocities()))
+    assert runs[0][:2] == runs[1][:2]
+    assert np.array_equal(runs[0][2], runs[1][2]) and np.array_equal(runs[0][3], runs[1][3])
