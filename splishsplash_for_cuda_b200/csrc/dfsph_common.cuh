@@ -258,21 +258,24 @@ template <class Real> struct Cubic {
 // components (their squares are exact in FP64): the FP32 build sums rho - rho0 in FP64 from these
 // terms, so the density residual keeps the accuracy of the FP64 build where rho ~ rho0 cancels.
 // The self term (r = 0) is m k.
+// Every FP64 operation is rounded on its own (no contraction), in the order the oracle's FP32
+// instance evaluates it, so the two agree bit for bit on the same inputs.
 __device__ __forceinline__ double density_term(const Cubic<float>& K, float rx, float ry, float rz, float m) {
     const double dx = rx, dy = ry, dz = rz;
-    const double q2 = (dx * dx + dy * dy + dz * dz) * K.ih2_d;
+    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    const double q2 = __dmul_rn(r2, K.ih2_d);
     if (q2 > 1.0) return 0.0;
     double w = K.k_d;
     if (q2 > 0.0) {
-        const double q = sqrt(q2);
+        const double q = __dsqrt_rn(q2);
         if (q <= 0.5) {
-            w = K.k_d * (1.0 + 6.0 * q2 * (q - 1.0));
+            w = __dmul_rn(K.k_d, __dadd_rn(1.0, __dmul_rn(__dmul_rn(6.0, q2), __dadd_rn(q, -1.0))));
         } else {
-            const double f = 1.0 - q;
-            w = 2.0 * K.k_d * (f * f * f);
+            const double f = __dadd_rn(1.0, -q);
+            w = __dmul_rn(__dmul_rn(2.0, K.k_d), __dmul_rn(__dmul_rn(f, f), f));
         }
     }
-    return w * (double)m;
+    return __dmul_rn(w, (double)m);
 }
 
 // ---------------------------------------------------------------------------------------------
