@@ -130,3 +130,26 @@ def test_level_matches_oracle_and_control_removes_above_target():
     assert np.all(d.field("velocity")[n1:] == 0)
     for _ in range(10):
         assert d.step().status & bad == 0
+
+
+@pytest.mark.gpu
+def test_raise_stops_at_fluid_capacity():
+    """Raising past fluid_capacity appends what fits, in lattice order, and sets
+    DFSPH_ST_FLUID_CAPACITY; calls with a target <= 0 or within 5 cm change nothing."""
+    from splishsplash_for_cuda_b200 import _capi
+    from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
+
+    s = _tank()
+    d = DFSPHCUDA(s, fluid_capacity=s.n_fluid + 10)
+    d.step()
+    level = d.fluid_level()
+    assert d.fluid_level_control(0.0) == (0, 0)
+    assert d.fluid_level_control(-1.0) == (0, 0)
+    off, dims = _device_level_inputs(d)
+    want = fluid_level_raise(d.positions(), d.field("boundary_position"), R, off, dims, level + 0.2, level)
+    assert len(want) > 10
+    d.status(clear=True)
+    assert d.fluid_level_control(level + 0.2) == (0, 10)
+    assert d.num_fluid() == s.n_fluid + 10
+    assert np.array_equal(d.positions()[s.n_fluid:], want[:10])
+    assert d.status() & _capi.ST_FLUID_CAPACITY
