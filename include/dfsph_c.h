@@ -477,7 +477,8 @@ int dfsph_fluid_level_control(dfsph_ctx* ctx, double target, uint32_t* removed, 
  * multiplies the velocities of the particles the last shift added by `damping` (in [0, 1]; 1: none)
  * and updates the positions. With tagged_only the other particles keep their positions and velocities
  * (they act as neighbours only); particles count as added by the last shift until the fluid is
- * compacted or uploaded again. The dt history is restored afterwards. Synchronises the context's
+ * compacted or uploaded again, and particles appended after the shift (open-boundary inflow, a fluid
+ * level raise) count with them. The dt history is restored afterwards. Synchronises the context's
  * stream. */
 int dfsph_dynamic_window_stabilize(dfsph_ctx* ctx, uint32_t iterations, double time_step, double damping,
                                    int tagged_only);

@@ -215,8 +215,9 @@ public:
     // dynamic window: the window box and its total displacement, the walls that move with it, and
     // the rest-fluid samples (in the window's current place) with their scratch
     bool dw_ready = false;
-    // ids >= dw_first_new were added by the last window shift (the stabilisation's tagged particles;
-    // none once the fluid is compacted or uploaded again); dw_spos / dw_svel keep the others' state
+    // ids >= dw_first_new were added by the last window shift or appended since (the stabilisation's
+    // tagged particles; none once the fluid is compacted or uploaded again); dw_spos / dw_svel keep
+    // the others' state
     uint32_t dw_first_new = 0;
     Vec4<Real>* dw_spos = nullptr;
     Vec4<Real>* dw_svel = nullptr;
