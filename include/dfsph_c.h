@@ -184,7 +184,12 @@ int dfsph_move_boundary(dfsph_ctx* ctx, const float* xyz, const float* vxyz);
  * + velocity, where x0 is each particle's position as given to dfsph_set_boundary (its rest frame)
  * and q = (w, x, y, z) a rotation quaternion (normalised here). Null pointers mean the identity /
  * zero. psi is kept, the other particles keep their state, and the boundary cell structure is
- * rebuilt; no particle data crosses the host link. */
+ * rebuilt; no particle data crosses the host link. A pure translation of the whole boundary (first 0,
+ * count all, no rotation) that stays within half a cell of the positions the boundary was last binned
+ * at is not re-binned: the neighbour search then looks the boundary up at each fluid particle's
+ * position minus the translation (one more cell layer near cell faces) and tests the pairs at the
+ * current positions, so the neighbour sets are the same; only the order of the boundary entries in a
+ * list may differ. */
 int dfsph_move_boundary_rigid(dfsph_ctx* ctx, uint32_t first, uint32_t count, const double* q, const double* position,
                               const double* velocity, const double* angular_velocity);
 
@@ -267,7 +272,10 @@ int dfsph_on_step_end(dfsph_ctx* ctx);                                    /* onS
  * boundary and the dynamic window add; default: the first uploaded particle's),
  * "sort_withhold_tile" (failure-detection tests: the fluid sort's tile with this id never publishes
  * its look-back flags, so the bounded waits of the tiles after it run out, about a second, and the
- * step reports DFSPH_ST_SORT_TIMEOUT with an unspecified particle order; -1 turns it off).
+ * step reports DFSPH_ST_SORT_TIMEOUT with an unspecified particle order; -1 turns it off),
+ * "boundary_shift_active" (read-only: 1 while a translation of the whole boundary by
+ * dfsph_move_boundary_rigid, less than half a cell since the boundary was last binned, is applied by
+ * querying the binned cells at the shifted position instead of re-binning).
  *
  * Learned warm start (no reference counterpart; off by default, dfsph_step only):
  * "learned_warm_start" (1: on), "warm_start_probe" (1: per solve, keep the learned candidate only if

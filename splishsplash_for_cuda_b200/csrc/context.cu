@@ -115,6 +115,11 @@ public:
     unsigned long long* bforce_fx = nullptr;  // boundary forces, fixed-point sums (converted into bforce)
     Real* bforce = nullptr;  // boundary forces (4 per particle, sorted order), allocated when enabled
     bool boundary_forces = false;
+    // Rigid translation of the whole boundary without re-binning: bin_rigid when the binned positions
+    // are the rest positions translated by bin_p; bshift_d the translation since (used while every
+    // component stays below one cell); bshifted when it is not zero.
+    bool bin_rigid = false, bshifted = false;
+    double bin_p[3] = {0.0, 0.0, 0.0}, bshift_d[3] = {0.0, 0.0, 0.0};
     uint32_t* bid = nullptr;
     double* partials = nullptr;
     LoopCtl* ctl = nullptr;
@@ -409,6 +414,10 @@ public:
         p.nbr_stride = stride;
         p.nbr_cap = cap;
         p.boundary_moving = boundary_moving ? 1 : 0;
+        p.bshift = bshifted ? 1 : 0;
+        p.bsx = (Real)bshift_d[0];
+        p.bsy = (Real)bshift_d[1];
+        p.bsz = (Real)bshift_d[2];
         return p;
     }
 
@@ -574,6 +583,9 @@ public:
             launches += 1;
             DF_TRY(sort_boundary(psi == nullptr));
         }
+        bin_rigid = true;  // binned at the rest positions
+        bshifted = false;
+        for (int a = 0; a < 3; ++a) bin_p[a] = bshift_d[a] = 0.0;
         invalidate_graphs();
         DF_TRY(sync_state());
         DF_CUDA(cudaStreamSynchronize(stream));
@@ -595,6 +607,7 @@ public:
         launches += 3;
         boundary_moving = true;
         DF_TRY(sort_boundary(false));
+        bin_rigid = bshifted = false;
         return sync_state();
     }
 
@@ -629,11 +642,50 @@ public:
         if (!count) return DFSPH_OK;
         if (!boundary_moving) DF_CUDA(cudaMemsetAsync(bvel[0], 0, (size_t)nb * sizeof(Vec4<Real>), stream));
         launch_rigid_boundary<Real>(brest, nb, bid, m, bpos[0], bvel[0], stream);
+        // A translation of the whole boundary keeps the binning while it stays within a cell of the
+        // binned positions: the neighbour search queries the binned cells at x_i minus the shift.
+        bool pure = first == 0 && count == nb;
+        for (int k = 0; k < 9; ++k) pure = pure && m.R[k] == (k % 4 == 0 ? 1.0 : 0.0);
+        const double Hd = 4.0 * sc.particle_radius;
+        double d[3];
+        bool near = pure && bin_rigid;
+        for (int a = 0; a < 3; ++a) {
+            d[a] = m.p[a] - bin_p[a];
+            near = near && std::fabs(d[a]) < 0.5 * Hd;
+        }
+        boundary_moving = true;
+        if (near) {
+            for (int a = 0; a < 3; ++a) bshift_d[a] = d[a];
+            bshifted = d[0] != 0.0 || d[1] != 0.0 || d[2] != 0.0;
+            launches += 1;
+            return sync_state();
+        }
         launch_pack_field<Real, Real>((const Real*)bpos[0], 4, 4, bid, nb, (Real*)bpos[1], stream);
         launch_pack_field<Real, Real>((const Real*)bvel[0], 4, 4, bid, nb, (Real*)bvel[1], stream);
         launches += 3;
-        boundary_moving = true;
         DF_TRY(sort_boundary(false));
+        bin_rigid = pure;
+        bshifted = false;
+        for (int a = 0; a < 3; ++a) {
+            bin_p[a] = pure ? m.p[a] : 0.0;
+            bshift_d[a] = 0.0;
+        }
+        return sync_state();
+    }
+
+    // Re-bins the boundary at its current positions when a rigid translation has been left pending
+    // (before anything other than the neighbour search reads the boundary's cell table or order).
+    int bin_boundary_now() {
+        if (!bshifted) return DFSPH_OK;
+        launch_pack_field<Real, Real>((const Real*)bpos[0], 4, 4, bid, nb, (Real*)bpos[1], stream);
+        launch_pack_field<Real, Real>((const Real*)bvel[0], 4, 4, bid, nb, (Real*)bvel[1], stream);
+        launches += 2;
+        DF_TRY(sort_boundary(false));
+        for (int a = 0; a < 3; ++a) {
+            bin_p[a] += bshift_d[a];
+            bshift_d[a] = 0.0;
+        }
+        bshifted = false;
         return sync_state();
     }
 
@@ -1069,6 +1121,7 @@ public:
             bb_hi[a] += (float)d[a];
         }
         if (dw_wall_count) DF_TRY(move_boundary_rigid(dw_wall_first, dw_wall_count, nullptr, dw_disp, nullptr, nullptr));
+        DF_TRY(bin_boundary_now());  // the inflow below reads the boundary's cell table
         // (2) removal outside the moved box
         uint32_t n_rm = 0;
         if (n) {
@@ -1441,6 +1494,7 @@ public:
     int open_boundary_apply(double allowed_distance, double allowed_density, bool inflow, bool outflow,
                             uint32_t* added, uint32_t* removed) {
         DF_CHECK(ob_ready, DFSPH_E_STATE, "open boundary not initialised (dfsph_open_boundary_init)");
+        DF_TRY(bin_boundary_now());  // the inflow reads the boundary's cell table
         if (inflow)
             DF_CHECK(allowed_distance > 0 && allowed_density > 0, DFSPH_E_INVALID,
                      "open boundary inflow needs allowed_distance > 0 and allowed_density > 0");
@@ -2350,6 +2404,7 @@ public:
     int save_checkpoint(const char* path) {
         DF_CHECK(path, DFSPH_E_INVALID, "null path");
         DF_CHECK(grid_ready, DFSPH_E_STATE, "nothing to checkpoint");
+        DF_TRY(bin_boundary_now());  // the file keeps the boundary in its sorted order
         DF_TRY(pull_dt());
         std::ofstream f(path, std::ios::binary | std::ios::trunc);
         DF_CHECK(f.is_open(), DFSPH_E_INVALID, std::string("cannot open ") + path);
@@ -2456,6 +2511,8 @@ public:
             DF_CUDA(cudaMemcpyAsync(bid, saved_bid.data(), nb * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
         }
         boundary_moving = moving != 0;
+        bin_rigid = bshifted = false;  // the next rigid motion re-bins
+        for (int a = 0; a < 3; ++a) bin_p[a] = bshift_d[a] = 0.0;
         DF_CUDA(cudaMemsetAsync(counts, 0, (size_t)Nc * sizeof(uint32_t), stream));
         DF_CUDA(cudaMemsetAsync(status, 0, 4 * sizeof(uint32_t), stream));
         if (was_learned) {
@@ -2819,6 +2876,7 @@ public:
         }
         else if (k == "boundary_forces") *v = boundary_forces ? 1 : 0;
         else if (k == "remove_escaped") *v = remove_escaped ? 1 : 0;
+        else if (k == "boundary_shift_active") *v = bshifted ? 1 : 0;
         else if (k == "inflow_mass") *v = new_particle_mass();
         else if (k == "escaped_removed") *v = (double)escaped_removed;
         else if (k == "warm_start_damping") *v = damping;

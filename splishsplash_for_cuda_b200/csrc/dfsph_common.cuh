@@ -370,6 +370,8 @@ template <class Real> struct StepParams {
     uint32_t nbr_stride;         // row stride of the interleaved neighbour table
     uint32_t nbr_cap;            // stored neighbours per particle
     int boundary_moving;         // 1: boundary velocities are read (else zero)
+    int bshift;                  // 1: the boundary translated rigidly by (bsx, bsy, bsz) since its binning
+    Real bsx, bsy, bsz;
 };
 
 // Device-side control block of one solver loop (divergence or pressure).

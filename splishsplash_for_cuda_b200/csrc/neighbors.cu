@@ -210,14 +210,33 @@ __global__ void __launch_bounds__(kBlock) build_neighbors_kernel(const DevState<
             }
         }
         if (p.n_boundary > 0) {
-            for (int dz = -1; dz <= 1; ++dz) {
-                const int z = cz + dz;
+            // Boundary cells: the 27 around the particle's cell, or, while the whole boundary has only
+            // translated by s since it was binned, the cells around x_i - s in the binned frame, one
+            // more layer on a side where x_i - s lies within 1e-3 of a cell face (the binned and the
+            // current positions differ from s by rounding; the pair test uses the current positions).
+            int lo[3] = {cx - 1, cy - 1, cz - 1}, hi[3] = {cx + 1, cy + 1, cz + 1};
+            bool query = true;
+            if (p.bshift) {
+                const float q[3] = {__fsub_rn((float)xi.x, (float)p.bsx), __fsub_rn((float)xi.y, (float)p.bsy),
+                                    __fsub_rn((float)xi.z, (float)p.bsz)};
+                const int off[3] = {p.off_x, p.off_y, p.off_z};
+                const float Hf = (float)p.kern.H;
+                for (int a = 0; a < 3 && query; ++a) {
+                    const float t = __fadd_rn(__fdiv_rn(q[a], Hf), (float)off[a]);
+                    if (!(fabsf(t) < 1.0e8f)) {  // also NaN: no boundary neighbours, as off the grid
+                        query = false;
+                        break;
+                    }
+                    const float c = floorf(t), frac = t - c;
+                    lo[a] = (int)c - 1 - (frac < 1e-3f ? 1 : 0);
+                    hi[a] = (int)c + 1 + (frac > 1.0f - 1e-3f ? 1 : 0);
+                }
+            }
+            for (int z = lo[2]; query && z <= hi[2]; ++z) {
                 if (z < 0 || z >= p.dim_z) continue;
-                for (int dy = -1; dy <= 1; ++dy) {
-                    const int y = cy + dy;
+                for (int y = lo[1]; y <= hi[1]; ++y) {
                     if (y < 0 || y >= p.dim_y) continue;
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        const int x = cx + dx;
+                    for (int x = lo[0]; x <= hi[0]; ++x) {
                         if (x < 0 || x >= p.dim_x) continue;
                         const uint2 r = btab[cell_linear(x, y, z, p.dim_x, p.dim_y)];
                         if (!run_in_range(r, p.n_boundary, ds->status)) continue;

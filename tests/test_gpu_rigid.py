@@ -6,7 +6,8 @@ import pytest
 
 from splishsplash_for_cuda_b200.dfsph import DFSPHCUDA
 from splishsplash_for_cuda_b200.rigid import RigidBody, RigidCoupling
-from splishsplash_for_cuda_b200.scene import Configuration, Scene, box_wall, lattice_block
+from splishsplash_for_cuda_b200.scene import Configuration, Scene, box_wall, lattice_block, synthetic_scene
+from tests._compare import neighbor_sets
 
 pytestmark = pytest.mark.gpu
 R = 0.01
@@ -103,3 +104,46 @@ def test_free_box_floats_at_rest(cuda_lib):
     assert abs(np.mean(fy) - weight) <= 0.1 * weight, (np.mean(fy), weight)
     assert 0.2 * size[1] <= depth <= 0.8 * size[1], (depth, surface)
     assert np.linalg.norm(body.v) < 0.05 and np.linalg.norm(body.w) < 0.5
+
+
+def test_whole_boundary_translation_keeps_neighbour_sets():
+    """A translation of the whole boundary within half a cell of its binning is applied without
+    re-binning (the neighbour search looks the boundary up at x_i minus the shift): against the same
+    positions uploaded with dfsph_move_boundary (a full re-binning each step), the same neighbour
+    sets, the same iteration counts and positions within 1e-5 m over ten steps; a larger translation
+    re-bins; a checkpoint taken while shifted reloads to the same state."""
+    import tempfile
+
+    s = synthetic_scene(1, counts=(14, 14, 14))
+    a, b = DFSPHCUDA(s), DFSPHCUDA(s)
+    b0 = s.boundary.astype(np.float64)
+    nb = b0.shape[0]
+    H = 4 * s.config.particleRadius
+    for k in range(10):
+        p = np.array([0.3 * H * np.sin(0.7 * k), 0.0, -0.2 * H * np.sin(0.4 * k)])
+        v = np.array([0.1, 0.0, -0.05])
+        a.move_boundary_rigid(0, nb, None, p, v, None)
+        assert a.get_param("boundary_shift_active") == (1.0 if np.any(p != 0.0) else 0.0)
+        b.move_boundary((b0 + p).astype(np.float32), np.tile(v, (nb, 1)).astype(np.float32))
+        assert np.abs(a.field("boundary_position", np.float64) - b.field("boundary_position", np.float64)).max() <= 1e-6
+        a.neighbors_search()
+        b.neighbors_search()
+        ca, la = a.neighbors()
+        cb, lb = b.neighbors()
+        assert np.array_equal(ca, cb), k
+        assert neighbor_sets(ca, la) == neighbor_sets(cb, lb), k
+        sa, sb = a.step(), b.step()
+        assert (sa.iterations, sa.iterations_v) == (sb.iterations, sb.iterations_v), k
+    assert np.abs(a.positions(np.float64) - b.positions(np.float64)).max() <= 1e-5
+    a.move_boundary_rigid(0, nb, None, np.array([0.6 * H, 0.0, 0.0]), None, None)
+    assert a.get_param("boundary_shift_active") == 0.0
+    a.move_boundary_rigid(0, nb, None, np.array([0.7 * H, 0.0, 0.0]), None, None)
+    assert a.get_param("boundary_shift_active") == 1.0
+    with tempfile.TemporaryDirectory() as tmp:
+        a.checkpoint_save(f"{tmp}/c.bin")
+        assert a.get_param("boundary_shift_active") == 0.0
+        c = DFSPHCUDA(s)
+        c.checkpoint_load(f"{tmp}/c.bin")
+        sa, sc = a.step(), c.step()
+        assert (sa.iterations, sa.iterations_v) == (sc.iterations, sc.iterations_v)
+        assert np.array_equal(a.positions(), c.positions())
