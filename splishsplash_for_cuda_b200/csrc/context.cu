@@ -791,7 +791,7 @@ public:
             DF_CUDA(cudaMemsetAsync(bforce_fx, 0, (size_t)nb * 3 * sizeof(unsigned long long), stream));
         if (!n) return DFSPH_OK;
         DF_TRY(bin_fluid(true));
-        launch_build_neighbors<Real>(ds, n, ftab, btab, stream);
+        launch_build_neighbors<Real>(ds, n, ftab, btab, stream, bshifted);
         launches += 1;
         DF_TRY(flush_pending());  // velocities uploaded during the binning and the build
         if (corrupt_neighbor) {  // checked builds only (the key is rejected otherwise); one search
@@ -2915,7 +2915,7 @@ public:
 
     void launch_kernel(int k) {
         switch (k) {
-            case DFSPH_K_NEIGHBOR_BUILD: launch_build_neighbors<Real>(ds, n, ftab, btab, stream); break;
+            case DFSPH_K_NEIGHBOR_BUILD: launch_build_neighbors<Real>(ds, n, ftab, btab, stream, bshifted); break;
             case DFSPH_K_DENSITY_ALPHA: launch_density_alpha<Real>(ds, n, false, false, stream); break;
             case DFSPH_K_DIVERGENCE_JACOBI: launch_divergence_jacobi<Real>(ds, n, 0, false, stream); break;
             case DFSPH_K_DIVERGENCE_RESIDUAL:

@@ -77,7 +77,7 @@ void launch_cell_bounds(const uint32_t* sorted_keys, uint32_t n, int dim_x, int 
                         cudaStream_t s);
 template <class Real>
 void launch_build_neighbors(const DevState<Real>* d, uint32_t n, const uint2* fluid_table, const uint2* boundary_table,
-                            cudaStream_t s);
+                            cudaStream_t s, bool boundary_shifted = false);
 // Checked builds only (no-ops otherwise): particle 0's first list entry := value; the range check of
 // every list entry and count (DFSPH_ST_INDEX, the offending particle's list emptied).
 void launch_corrupt_first_neighbor(uint32_t* nbr, const uint32_t* counts, uint32_t value, cudaStream_t s);

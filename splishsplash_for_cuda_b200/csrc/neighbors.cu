@@ -176,7 +176,7 @@ __device__ __forceinline__ void scan_cell(const Vec4<Real>* __restrict__ src, ui
     }
 }
 
-template <class Real>
+template <class Real, bool kShift>
 __global__ void __launch_bounds__(kBlock) build_neighbors_kernel(const DevState<Real>* __restrict__ ds, uint32_t n,
                                                                  const uint2* __restrict__ ftab,
                                                                  const uint2* __restrict__ btab) {
@@ -209,30 +209,45 @@ __global__ void __launch_bounds__(kBlock) build_neighbors_kernel(const DevState<
                 }
             }
         }
-        if (p.n_boundary > 0) {
-            // Boundary cells: the 27 around the particle's cell, or, while the whole boundary has only
-            // translated by s since it was binned, the cells around x_i - s in the binned frame, one
-            // more layer on a side where x_i - s lies within 1e-3 of a cell face (the binned and the
-            // current positions differ from s by rounding; the pair test uses the current positions).
-            int lo[3] = {cx - 1, cy - 1, cz - 1}, hi[3] = {cx + 1, cy + 1, cz + 1};
-            bool query = true;
-            if (p.bshift) {
-                const float q[3] = {__fsub_rn((float)xi.x, (float)p.bsx), __fsub_rn((float)xi.y, (float)p.bsy),
-                                    __fsub_rn((float)xi.z, (float)p.bsz)};
-                const int off[3] = {p.off_x, p.off_y, p.off_z};
-                const float Hf = (float)p.kern.H;
-                for (int a = 0; a < 3 && query; ++a) {
-                    const float t = __fadd_rn(__fdiv_rn(q[a], Hf), (float)off[a]);
-                    if (!(fabsf(t) < 1.0e8f)) {  // also NaN: no boundary neighbours, as off the grid
-                        query = false;
-                        break;
+        if (p.n_boundary > 0 && !kShift) {
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int z = cz + dz;
+                if (z < 0 || z >= p.dim_z) continue;
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const int y = cy + dy;
+                    if (y < 0 || y >= p.dim_y) continue;
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        const int x = cx + dx;
+                        if (x < 0 || x >= p.dim_x) continue;
+                        const uint2 r = btab[cell_linear(x, y, z, p.dim_x, p.dim_y)];
+                        if (!run_in_range(r, p.n_boundary, ds->status)) continue;
+                        scan_cell<Real, false>(bpos, r.x, r.y, i, xi, H2, nbr, stride, cap, total, nb, overflow);
                     }
-                    const float c = floorf(t), frac = t - c;
-                    lo[a] = (int)c - 1 - (frac < 1e-3f ? 1 : 0);
-                    hi[a] = (int)c + 1 + (frac > 1.0f - 1e-3f ? 1 : 0);
                 }
             }
-            for (int z = lo[2]; query && z <= hi[2]; ++z) {
+        }
+        if (p.n_boundary > 0 && kShift) {
+            // The whole boundary has only translated by s since it was binned: the cells around the
+            // binned cell of x_i - s, with one more layer on a side where x_i - s lies within 1e-3 of a
+            // cell face (the binned and the current positions differ from s by rounding; the pair test
+            // uses the current positions).
+            int lo[3], hi[3];
+            bool query = true;
+            const float q[3] = {__fsub_rn((float)xi.x, (float)p.bsx), __fsub_rn((float)xi.y, (float)p.bsy),
+                                __fsub_rn((float)xi.z, (float)p.bsz)};
+            const int off[3] = {p.off_x, p.off_y, p.off_z};
+            const float Hf = (float)p.kern.H;
+            for (int a = 0; a < 3 && query; ++a) {
+                const float t = __fadd_rn(__fdiv_rn(q[a], Hf), (float)off[a]);
+                if (!(fabsf(t) < 1.0e8f)) {  // also NaN: no boundary neighbours, as off the grid
+                    query = false;
+                    break;
+                }
+                const float c = floorf(t), frac = t - c;
+                lo[a] = (int)c - 1 - (frac < 1e-3f ? 1 : 0);
+                hi[a] = (int)c + 1 + (frac > 1.0f - 1e-3f ? 1 : 0);
+            }
+            for (int z = query ? lo[2] : 1; query && z <= hi[2]; ++z) {
                 if (z < 0 || z >= p.dim_z) continue;
                 for (int y = lo[1]; y <= hi[1]; ++y) {
                     if (y < 0 || y >= p.dim_y) continue;
@@ -347,8 +362,12 @@ void launch_cell_bounds(const uint32_t* sorted_keys, uint32_t n, int dim_x, int 
 }
 template <class Real>
 void launch_build_neighbors(const DevState<Real>* d, uint32_t n, const uint2* fluid_table, const uint2* boundary_table,
-                            cudaStream_t s) {
-    if (n) launch_pdl(build_neighbors_kernel<Real>, grid_for(n), kBlock, 0, s, d, n, fluid_table, boundary_table);
+                            cudaStream_t s, bool boundary_shifted) {
+    if (!n) return;
+    if (boundary_shifted)
+        launch_pdl(build_neighbors_kernel<Real, true>, grid_for(n), kBlock, 0, s, d, n, fluid_table, boundary_table);
+    else
+        launch_pdl(build_neighbors_kernel<Real, false>, grid_for(n), kBlock, 0, s, d, n, fluid_table, boundary_table);
 }
 void launch_validate_neighbors(uint32_t* counts, const uint32_t* nbr, uint32_t n, uint32_t n_boundary, uint32_t stride,
                                uint32_t cap, uint32_t* status, cudaStream_t s) {
@@ -392,7 +411,8 @@ void launch_scatter_by_id(const uint32_t* id, uint32_t n, const Real* src, int c
     template void launch_reorder_fluid<R>(const uint32_t*, uint32_t, const Vec4<R>*, const Vec4<R>*, const R*,       \
                                           const R*, const uint32_t*, Vec4<R>*, Vec4<R>*, R*, R*, uint32_t*,          \
                                           cudaStream_t);                                                             \
-    template void launch_build_neighbors<R>(const DevState<R>*, uint32_t, const uint2*, const uint2*, cudaStream_t); \
+    template void launch_build_neighbors<R>(const DevState<R>*, uint32_t, const uint2*, const uint2*, cudaStream_t,   \
+                                            bool);                                                                   \
     template void launch_reorder_pair<R>(const uint32_t*, uint32_t, const R*, const R*, R*, R*, cudaStream_t);       \
     template void launch_boundary_psi<R>(const Vec4<R>*, Vec4<R>*, uint32_t, const StepParams<R>&, const uint2*,     \
                                          uint32_t*, cudaStream_t);                                                   \
